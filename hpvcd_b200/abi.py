@@ -1,0 +1,246 @@
+"""ctypes mirror of include/hpvcd_gpu.h and the library loaders.
+
+The structs here must match the C header byte for byte; tests/test_abi.py
+checks every size and field offset against the compiled library's own
+`sizeof` report.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+LIB_PATH = os.path.join(HERE, "libhpvcd_b200.so")
+SYNTH_PATH = os.path.join(HERE, "libhpvcd_synth.so")
+
+# status codes (hpvcd_status)
+OK = 0
+ERR_BITSTREAM = 1
+ERR_ALLOC = 2
+ERR_LIMIT = 3
+ERR_UNSUPPORTED = 4
+ERR_TIMEOUT = 5
+ERR_CUDA = 6
+ERR_INVALID_ARG = 7
+ERR_BUSY = 8
+
+STATUS_NAMES = {
+    OK: "OK",
+    ERR_BITSTREAM: "Bitstream",
+    ERR_ALLOC: "AllocationFailed",
+    ERR_LIMIT: "LimitExceeded",
+    ERR_UNSUPPORTED: "Unsupported",
+    ERR_TIMEOUT: "Timeout",
+    ERR_CUDA: "Cuda",
+    ERR_INVALID_ARG: "InvalidArgument",
+    ERR_BUSY: "Busy",
+}
+
+TU_CBF, TU_TSKIP, TU_INTRA, TU_TQB = 0x01, 0x02, 0x04, 0x08
+CELL_EXEMPT = 0x01
+PU_L0, PU_L1 = 0x01, 0x02
+MAX_REFS = 16
+
+PIC_STRONG_SMOOTHING = 0x0001
+PIC_SMOOTHING_DISABLED = 0x0002
+PIC_DEBLOCK = 0x0004
+PIC_SAO_LUMA = 0x0008
+PIC_SAO_CHROMA = 0x0010
+PIC_PRED_IN_PLANE = 0x0020
+PIC_INTER = 0x0040
+
+OUT_YUV, OUT_RGB8 = 0, 1
+MATRIX_IDENTITY, MATRIX_BT709, MATRIX_BT470BG = 0, 1, 5
+MATRIX_SMPTE170M, MATRIX_YCGCO, MATRIX_BT2020NCL = 6, 8, 9
+
+STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_OUTPUT = 0x1, 0x2, 0x4, 0x8
+STAGE_ALL = 0xF
+
+SYNTH_RESIDUAL, SYNTH_INTRA, SYNTH_INTER = 0, 1, 2
+
+
+class HpvcdError(RuntimeError):
+    """Error raised for a non-zero hpvcd_status (maps to the reference's DecodeError)."""
+
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {STATUS_NAMES.get(status, status)} ({status})")
+
+
+class Tu(C.Structure):
+    _fields_ = [
+        ("x", C.c_uint16), ("y", C.c_uint16), ("coeff_off", C.c_uint32),
+        ("log2n", C.c_uint8), ("comp", C.c_uint8), ("flags", C.c_uint8), ("mode", C.c_uint8),
+        ("qp_y", C.c_int8), ("cqp_off", C.c_int8), ("nx", C.c_uint8), ("rsvd", C.c_uint8),
+    ]
+
+
+TU_DTYPE = np.dtype([
+    ("x", "<u2"), ("y", "<u2"), ("coeff_off", "<u4"), ("log2n", "u1"), ("comp", "u1"),
+    ("flags", "u1"), ("mode", "u1"), ("qp_y", "i1"), ("cqp_off", "i1"), ("nx", "u1"), ("rsvd", "u1"),
+])
+
+
+class Cell(C.Structure):
+    _fields_ = [("bs_v", C.c_uint8), ("bs_h", C.c_uint8), ("qp_y", C.c_int8), ("flags", C.c_uint8)]
+
+
+CELL_DTYPE = np.dtype([("bs_v", "u1"), ("bs_h", "u1"), ("qp_y", "i1"), ("flags", "u1")])
+
+
+class SaoComp(C.Structure):
+    _fields_ = [
+        ("type_idx", C.c_uint8), ("band_pos", C.c_uint8), ("eo_class", C.c_uint8),
+        ("rsvd", C.c_uint8), ("offsets", C.c_int16 * 4),
+    ]
+
+
+class SaoCtb(C.Structure):
+    _fields_ = [("comp", SaoComp * 3)]
+
+
+SAO_DTYPE = np.dtype([("comp", [("type_idx", "u1"), ("band_pos", "u1"), ("eo_class", "u1"),
+                                ("rsvd", "u1"), ("offsets", "<i2", (4,))], (3,))])
+
+
+class Pu(C.Structure):
+    _fields_ = [
+        ("x", C.c_uint16), ("y", C.c_uint16), ("w", C.c_uint16), ("h", C.c_uint16),
+        ("mv", (C.c_int16 * 2) * 2), ("ref_idx", C.c_int8 * 2), ("flags", C.c_uint8),
+        ("rsvd", C.c_uint8),
+    ]
+
+
+class WpEntry(C.Structure):
+    _fields_ = [("luma_w", C.c_int16), ("luma_o", C.c_int16), ("cb_w", C.c_int16),
+                ("cb_o", C.c_int16), ("cr_w", C.c_int16), ("cr_o", C.c_int16)]
+
+
+class WpTable(C.Structure):
+    _fields_ = [("luma_log2_denom", C.c_uint8), ("chroma_log2_denom", C.c_uint8),
+                ("rsvd", C.c_uint8 * 2), ("e", (WpEntry * MAX_REFS) * 2)]
+
+
+class Picture(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32), ("height", C.c_uint32),
+        ("chroma_idc", C.c_uint8), ("bit_depth_y", C.c_uint8), ("bit_depth_c", C.c_uint8),
+        ("log2_ctb", C.c_uint8), ("flags", C.c_uint32),
+        ("beta_offset_div2", C.c_int8), ("tc_offset_div2", C.c_int8),
+        ("pps_cb_qp_offset", C.c_int8), ("pps_cr_qp_offset", C.c_int8),
+        ("n_tus", C.c_uint32), ("n_pus", C.c_uint32), ("n_coeffs", C.c_uint64),
+        ("tus", C.c_void_p), ("ctu_tu_start", C.c_void_p), ("coeffs", C.c_void_p),
+        ("cells", C.c_void_p), ("sao", C.c_void_p), ("pus", C.c_void_p), ("wp", C.c_void_p),
+        ("ref_slot", (C.c_int32 * MAX_REFS) * 2),
+        ("pred", C.c_void_p * 3),
+    ]
+
+
+class TilePlace(C.Structure):
+    _fields_ = [("dst_x", C.c_uint32), ("dst_y", C.c_uint32), ("crop_w", C.c_uint32),
+                ("crop_h", C.c_uint32)]
+
+
+class Output(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("matrix", C.c_uint32), ("full_range", C.c_uint32),
+                ("canvas_w", C.c_uint32), ("canvas_h", C.c_uint32), ("place", C.c_void_p)]
+
+
+class GpuCfg(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_inflight", C.c_uint32), ("hbm_budget", C.c_uint64)]
+
+
+class Sched(C.Structure):
+    _fields_ = [("recon_threads", C.c_uint32), ("recon_ctas_per_sm", C.c_uint32),
+                ("filter_tile", C.c_uint32), ("fuse_filters", C.c_uint32)]
+
+
+class SynthCfg(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32),
+        ("kind", C.c_uint32), ("chroma_idc", C.c_uint32), ("bit_depth", C.c_uint32),
+        ("log2_ctb", C.c_uint32), ("pic_flags", C.c_uint32),
+        ("cu_split_p", C.c_float), ("tu_split_p", C.c_float), ("cbf_p", C.c_float),
+        ("zero_frac", C.c_float), ("laplace_scale", C.c_float), ("tskip_p", C.c_float),
+        ("tqb_p", C.c_float), ("sao_p", C.c_float),
+        ("qp_min", C.c_int32), ("qp_max", C.c_int32),
+        ("beta_offset_div2", C.c_int32), ("tc_offset_div2", C.c_int32),
+        ("cb_qp_offset", C.c_int32), ("cr_qp_offset", C.c_int32),
+        ("intra_cu_p", C.c_float), ("bi_p", C.c_float), ("mv_sd", C.c_float),
+        ("mv_pad", C.c_float), ("weighted", C.c_uint32), ("n_refs", C.c_uint32),
+    ]
+
+
+def _load(path: str, what: str) -> C.CDLL:
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{what} not built: {path} is missing (run `python -c 'import __graft_entry__ as g; g.build()'`)"
+        )
+    return C.CDLL(path)
+
+
+_lib = None
+_synth = None
+
+
+def lib() -> C.CDLL:
+    """The CUDA back end (libhpvcd_b200.so).  Raises ImportError when it is not built."""
+    global _lib
+    if _lib is None:
+        L = _load(LIB_PATH, "CUDA back end")
+        vp, u32, i32, u64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64
+        sig = {
+            "hpvcd_abi_version": (u32, []),
+            "hpvcd_status_string": (C.c_char_p, [C.c_int]),
+            "hpvcd_kernel_launch_count": (u64, []),
+            "hpvcd_gpu_create": (i32, [C.POINTER(GpuCfg), C.POINTER(vp)]),
+            "hpvcd_gpu_destroy": (i32, [vp]),
+            "hpvcd_gpu_submit": (i32, [vp, C.POINTER(Picture), u32, C.POINTER(Output), C.POINTER(u64)]),
+            "hpvcd_gpu_wait": (i32, [vp, u64, i32]),
+            "hpvcd_gpu_output_size": (i32, [vp, u64, C.POINTER(u64)]),
+            "hpvcd_gpu_read": (i32, [vp, u64, vp, u64]),
+            "hpvcd_plan_create": (i32, [C.POINTER(Picture), u32, C.POINTER(Output), C.POINTER(Sched), C.POINTER(vp)]),
+            "hpvcd_plan_destroy": (i32, [vp]),
+            "hpvcd_plan_launch": (i32, [vp, u32, vp]),
+            "hpvcd_plan_planes": (i32, [vp, u32, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+            "hpvcd_plan_canvas": (i32, [vp, C.POINTER(vp), C.POINTER(u64)]),
+            "hpvcd_plan_device_status": (i32, [vp, vp]),
+            "hpvcd_plan_launches_per_run": (u32, [vp]),
+            "hpvcd_abi_sizeof": (u64, [C.c_char_p]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def synth_lib() -> C.CDLL:
+    """The host-only synthetic input generator (libhpvcd_synth.so)."""
+    global _synth
+    if _synth is None:
+        L = _load(SYNTH_PATH, "synthetic generator")
+        L.hpvcd_synth_default_cfg.argtypes = [C.POINTER(SynthCfg)]
+        L.hpvcd_synth_default_cfg.restype = None
+        L.hpvcd_synth_new.restype = C.c_void_p
+        L.hpvcd_synth_new.argtypes = []
+        L.hpvcd_synth_free.argtypes = [C.c_void_p]
+        L.hpvcd_synth_free.restype = None
+        L.hpvcd_synth_add.argtypes = [C.c_void_p, C.POINTER(SynthCfg)]
+        L.hpvcd_synth_add.restype = C.c_int32
+        L.hpvcd_synth_count.argtypes = [C.c_void_p]
+        L.hpvcd_synth_count.restype = C.c_uint32
+        L.hpvcd_synth_get.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(Picture)]
+        L.hpvcd_synth_get.restype = C.c_int32
+        _synth = L
+    return _synth
+
+
+def check(status: int, what: str) -> None:
+    if status != OK:
+        raise HpvcdError(status, what)

@@ -1,0 +1,309 @@
+/*
+ * hpvcd_gpu.h -- C ABI of the B200 reconstruction back end for hpvcd.
+ *
+ * The reference decoder (hpvcd, Rust) keeps bitstream demux, parameter sets,
+ * CABAC and syntax decode on the host.  Everything that turns parsed syntax
+ * into pixels -- dequantisation, inverse DCT/DST and transform skip, intra
+ * prediction with reconstruction, motion compensation with weighted
+ * prediction, deblocking, SAO and YCbCr->RGB -- runs behind this ABI on the
+ * GPU.  In the reference those steps are the function-pointer slots of
+ * `ExecContext` (src/exec.rs:31-77), called once per transform block from
+ * `FullDecoder::transform_unit` (src/decode.rs:3478) and once per picture from
+ * `FullDecoder::finish_with` (src/decode.rs:1440) and
+ * `yuv_to_rgb_window_with_color_pool` (src/yuv.rs:533).  A GPU launch per TU
+ * would be hopeless, so the seam here is per picture / per batch of pictures:
+ * the host fills the flat buffers below while parsing and hands a whole
+ * picture (or a whole HEIC grid) over in one call.
+ *
+ * Everything is plain C: fixed-size integer structs, pointers and sizes.  No
+ * function here throws, aborts or panics; every entry point returns an
+ * `hpvcd_status`, which maps onto the reference's `DecodeError`
+ * (src/error.rs:30-60).
+ */
+#ifndef HPVCD_GPU_H
+#define HPVCD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPVCD_ABI_VERSION 1u
+
+/* ------------------------------------------------------------------------ */
+/* Status codes.  Mapping onto src/error.rs `DecodeError`:                   */
+/*   HPVCD_ERR_BITSTREAM   -> DecodeError::Bitstream (malformed flat buffers) */
+/*   HPVCD_ERR_ALLOC       -> DecodeError::AllocationFailed { what, bytes }   */
+/*   HPVCD_ERR_LIMIT       -> DecodeError::LimitExceeded                      */
+/*   HPVCD_ERR_UNSUPPORTED -> DecodeError::Unsupported                        */
+/* The remaining codes have no reference counterpart (device-side failures). */
+/* ------------------------------------------------------------------------ */
+typedef enum hpvcd_status {
+    HPVCD_OK = 0,
+    HPVCD_ERR_BITSTREAM = 1,
+    HPVCD_ERR_ALLOC = 2,
+    HPVCD_ERR_LIMIT = 3,
+    HPVCD_ERR_UNSUPPORTED = 4,
+    HPVCD_ERR_TIMEOUT = 5,     /* a bounded device-side wait ran out          */
+    HPVCD_ERR_CUDA = 6,        /* a CUDA runtime call failed                  */
+    HPVCD_ERR_INVALID_ARG = 7, /* NULL pointer, bad handle, bad size          */
+    HPVCD_ERR_BUSY = 8         /* ticket not finished within the wait budget  */
+} hpvcd_status;
+
+/* ------------------------------------------------------------------------ */
+/* Flat per-picture buffers (the output contract of the host syntax decode). */
+/* ------------------------------------------------------------------------ */
+
+/* hpvcd_tu.flags */
+#define HPVCD_TU_CBF 0x01u   /* coded residual present (cbf_luma / cbf_cb / cbf_cr) */
+#define HPVCD_TU_TSKIP 0x02u /* transform_skip_flag                                  */
+#define HPVCD_TU_INTRA 0x04u /* block of an intra CU (prediction from neighbours)    */
+#define HPVCD_TU_TQB 0x08u   /* cu_transquant_bypass: residual = levels verbatim     */
+
+/*
+ * One transform block, or one "mark decoded" record.  Records of a picture are
+ * stored in decode order, grouped per CTU in raster order (ctu_tu_start).
+ *
+ * - Intra luma TB      : predict (intra.rs), dequant + inverse transform, add,
+ *                        mark the luma 4x4 cells decoded (decode.rs:4724-4907).
+ * - Intra chroma TB    : predict, dequant + inverse DCT, add (decode.rs:5280).
+ * - Inter TB with CBF  : prediction already in the plane (motion compensation),
+ *                        add residual, mark decoded (decode.rs:4738-4745).
+ * - Record without CBF and without INTRA: marks its square decoded only; this
+ *   is how the end of an inter CU is signalled (decode.rs:6546-6548).  Such a
+ *   record may have log2n up to 6.
+ *
+ * x, y are in samples of the component plane.  For 4:2:0, a group of four 4x4
+ * luma TBs is followed by one 4x4 chroma TB per chroma component at the
+ * parent's position (decode.rs:3601-3609).
+ */
+typedef struct hpvcd_tu {
+    uint16_t x, y;
+    uint32_t coeff_off; /* element offset of the n*n row-major int16 levels   */
+    uint8_t log2n;      /* 2..5 for coded TBs                                  */
+    uint8_t comp;       /* 0 = Y, 1 = Cb, 2 = Cr                               */
+    uint8_t flags;      /* HPVCD_TU_*                                          */
+    uint8_t mode;       /* intra prediction mode 0..34 (chroma: resolved mode) */
+    int8_t qp_y;        /* QpY of the coding unit (may be negative, bd > 8)    */
+    int8_t cqp_off;     /* chroma TBs: slice + CU chroma QP offset             */
+    uint8_t nx;         /* max_x + 1 from residual_coding (columns >= nx zero) */
+    uint8_t rsvd;
+} hpvcd_tu; /* 16 bytes */
+
+/* hpvcd_cell.flags */
+#define HPVCD_CELL_EXEMPT 0x01u /* tqb CU, or I_PCM CU with pcm_loop_filter_disabled */
+
+/*
+ * Per 4x4 luma cell deblocking metadata (decode.rs:101-335 maps qp_y_map,
+ * edge_v/bs_v, edge_h/bs_h, tqb/pcm).  bs_v / bs_h hold the boundary strength
+ * of the cell's left / top edge after the host applied the edge flag and the
+ * slice / tile gating of `deblock_bs_v` / `deblock_bs_h` (decode.rs:1670-1712):
+ * 0 means "not a filtered edge".
+ */
+typedef struct hpvcd_cell {
+    uint8_t bs_v;
+    uint8_t bs_h;
+    int8_t qp_y;
+    uint8_t flags;
+} hpvcd_cell; /* 4 bytes */
+
+/* SAO parameters of one CTB component (decode.rs:66-72 `SaoCtb`). */
+typedef struct hpvcd_sao_comp {
+    uint8_t type_idx; /* 0 off, 1 band offset, 2 edge offset                */
+    uint8_t band_pos; /* band offset: first of the four bands (0..31)        */
+    uint8_t eo_class; /* edge offset: 0 hor, 1 ver, 2 135 deg, 3 45 deg      */
+    uint8_t rsvd;
+    int16_t offsets[4]; /* already sign-resolved and scaled (decode.rs:1560-1612) */
+} hpvcd_sao_comp; /* 12 bytes */
+
+typedef struct hpvcd_sao_ctb {
+    hpvcd_sao_comp comp[3];
+} hpvcd_sao_ctb; /* 36 bytes */
+
+/* hpvcd_pu.flags */
+#define HPVCD_PU_L0 0x01u
+#define HPVCD_PU_L1 0x02u
+
+/* One inter prediction block (decode.rs:7000 `motion_compensate`). */
+typedef struct hpvcd_pu {
+    uint16_t x, y, w, h;  /* luma samples                                     */
+    int16_t mv[2][2];     /* [list][x,y], quarter-pel luma units              */
+    int8_t ref_idx[2];    /* index into the picture's reference lists          */
+    uint8_t flags;        /* HPVCD_PU_L0 | HPVCD_PU_L1                         */
+    uint8_t rsvd;
+} hpvcd_pu; /* 20 bytes */
+
+/* Explicit weighted prediction (inter.rs:141 `PredWeightTable`), offsets in
+ * reconstructed-sample units (already normalised as inter.rs:33-58 does). */
+#define HPVCD_MAX_REFS 16
+typedef struct hpvcd_wp_entry {
+    int16_t luma_w, luma_o;
+    int16_t cb_w, cb_o;
+    int16_t cr_w, cr_o;
+} hpvcd_wp_entry; /* 12 bytes */
+
+typedef struct hpvcd_wp_table {
+    uint8_t luma_log2_denom;
+    uint8_t chroma_log2_denom;
+    uint8_t rsvd[2];
+    hpvcd_wp_entry e[2][HPVCD_MAX_REFS];
+} hpvcd_wp_table;
+
+/* hpvcd_picture.flags */
+#define HPVCD_PIC_STRONG_SMOOTHING 0x0001u   /* strong_intra_smoothing_enabled_flag   */
+#define HPVCD_PIC_SMOOTHING_DISABLED 0x0002u /* RExt intra_smoothing_disabled_flag     */
+#define HPVCD_PIC_DEBLOCK 0x0004u            /* run the deblocking filter              */
+#define HPVCD_PIC_SAO_LUMA 0x0008u           /* slice_sao_luma_flag                    */
+#define HPVCD_PIC_SAO_CHROMA 0x0010u         /* slice_sao_chroma_flag                  */
+#define HPVCD_PIC_PRED_IN_PLANE 0x0020u      /* planes hold the prediction on entry:   */
+                                             /* every TB only adds its residual        */
+#define HPVCD_PIC_INTER 0x0040u              /* picture has motion-compensated PUs     */
+
+/*
+ * One coded picture (one HEIC grid tile, one still image, or one video frame).
+ * Pointers are host pointers for hpvcd_gpu_submit and device pointers for the
+ * hpvcd_plan_* entry points.  Planes are stored without padding: luma stride =
+ * width, chroma stride = width / SubWidthC, one byte per sample when the bit
+ * depth is 8 and two bytes otherwise.
+ */
+typedef struct hpvcd_picture {
+    uint32_t width, height; /* coded luma size (multiple of the minimum CB)   */
+    uint8_t chroma_idc;     /* 0 mono, 1 4:2:0, 3 4:4:4 (2 -> UNSUPPORTED)     */
+    uint8_t bit_depth_y;    /* 8..12                                           */
+    uint8_t bit_depth_c;
+    uint8_t log2_ctb; /* 4..6                                              */
+    uint32_t flags;   /* HPVCD_PIC_*                                       */
+    int8_t beta_offset_div2;
+    int8_t tc_offset_div2;
+    int8_t pps_cb_qp_offset;
+    int8_t pps_cr_qp_offset;
+    uint32_t n_tus;
+    uint32_t n_pus;
+    uint64_t n_coeffs;
+    const hpvcd_tu* tus;           /* n_tus                                  */
+    const uint32_t* ctu_tu_start;  /* ctb_cols * ctb_rows + 1 prefix offsets  */
+    const int16_t* coeffs;         /* n_coeffs                               */
+    const hpvcd_cell* cells;       /* ceil(w/4) * ceil(h/4), NULL -> no deblock */
+    const hpvcd_sao_ctb* sao;      /* ctb_cols * ctb_rows, NULL -> no SAO     */
+    const hpvcd_pu* pus;           /* n_pus, inter pictures only              */
+    const hpvcd_wp_table* wp;      /* NULL -> default weighted prediction     */
+    int32_t ref_slot[2][HPVCD_MAX_REFS]; /* reference list -> DPB slot         */
+    const void* pred[3];           /* PRED_IN_PLANE: initial Y/Cb/Cr planes   */
+} hpvcd_picture;
+
+/* Output of a batch.  RGB8 is the `decode_heic_rgb8` path (lib.rs:1964):
+ * Q13 YCbCr->RGB (yuv.rs:187-393) then `>> (bit_depth - 8)`.  Pictures are
+ * placed on an output canvas as grid tiles (lib.rs:1610 `stitch_grid_band`);
+ * the part of a tile outside the canvas is cropped. */
+#define HPVCD_OUT_YUV 0u  /* per-picture planes                              */
+#define HPVCD_OUT_RGB8 1u /* packed RGB8 canvas                               */
+
+/* Matrix coefficients as in src/color.rs `MatrixCoefficients` (H.273 values). */
+#define HPVCD_MATRIX_IDENTITY 0u
+#define HPVCD_MATRIX_BT709 1u
+#define HPVCD_MATRIX_BT470BG 5u
+#define HPVCD_MATRIX_SMPTE170M 6u
+#define HPVCD_MATRIX_YCGCO 8u
+#define HPVCD_MATRIX_BT2020NCL 9u
+
+typedef struct hpvcd_tile_place {
+    uint32_t dst_x, dst_y;   /* top-left on the canvas                         */
+    uint32_t crop_w, crop_h; /* visible tile size (SPS conformance window size) */
+} hpvcd_tile_place;
+
+typedef struct hpvcd_output {
+    uint32_t kind;           /* HPVCD_OUT_*                                    */
+    uint32_t matrix;         /* HPVCD_MATRIX_*                                 */
+    uint32_t full_range;     /* video_full_range_flag                          */
+    uint32_t canvas_w, canvas_h;
+    const hpvcd_tile_place* place; /* one per picture (RGB8 only)              */
+} hpvcd_output;
+
+/* ------------------------------------------------------------------------ */
+/* Library information.                                                     */
+/* ------------------------------------------------------------------------ */
+uint32_t hpvcd_abi_version(void);
+const char* hpvcd_status_string(int status);
+/* Number of kernel launches issued by this process so far (all entry points). */
+uint64_t hpvcd_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------------ */
+/* Host-buffer API: the drop-in under `decode_heic` / `VideoDecoder`.        */
+/* Replaces, per picture batch, the per-TU ExecContext calls made from       */
+/* decode.rs:3478-5426, `finish_with` (decode.rs:1440) and the grid stitch   */
+/* `fill_grid_bands` / `stitch_grid_band` (lib.rs:1680 / lib.rs:1610).       */
+/* A context is internally synchronised: any thread may submit.             */
+/* ------------------------------------------------------------------------ */
+typedef struct hpvcd_gpu hpvcd_gpu;
+typedef uint64_t hpvcd_ticket;
+
+typedef struct hpvcd_gpu_cfg {
+    int32_t device;           /* CUDA device ordinal                          */
+    uint32_t max_inflight;    /* concurrent tickets (streams), 0 -> 4         */
+    uint64_t hbm_budget;      /* bytes this context may hold, 0 -> 80% free   */
+} hpvcd_gpu_cfg;
+
+hpvcd_status hpvcd_gpu_create(const hpvcd_gpu_cfg* cfg, hpvcd_gpu** out);
+hpvcd_status hpvcd_gpu_destroy(hpvcd_gpu* ctx);
+/* Copy the host buffers of `n` pictures to the device, reconstruct them and
+ * start the copy of the requested output back.  Host buffers are only read
+ * during the call.  Returns HPVCD_ERR_ALLOC when the batch does not fit the
+ * HBM budget (the caller may retry later). */
+hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* ctx, const hpvcd_picture* pics, uint32_t n,
+                              const hpvcd_output* out, hpvcd_ticket* ticket);
+/* Wait at most timeout_ms (negative: forever) for a ticket. */
+hpvcd_status hpvcd_gpu_wait(hpvcd_gpu* ctx, hpvcd_ticket ticket, int32_t timeout_ms);
+/* Bytes of output a finished ticket holds (RGB8 canvas, or all YUV planes
+ * of all pictures concatenated). */
+hpvcd_status hpvcd_gpu_output_size(hpvcd_gpu* ctx, hpvcd_ticket ticket, uint64_t* bytes);
+/* Copy a finished ticket's output into caller memory and release the ticket. */
+hpvcd_status hpvcd_gpu_read(hpvcd_gpu* ctx, hpvcd_ticket ticket, void* dst, uint64_t bytes);
+
+/* ------------------------------------------------------------------------ */
+/* Device-buffer API (plans).  The picture descriptors point at device      */
+/* memory that stays valid while the plan lives.  A plan owns its own        */
+/* device scratch (work queues, ready flags, ping-pong planes) and output.   */
+/* hpvcd_plan_launch only enqueues kernels on `stream` (no allocation, no    */
+/* synchronisation), so it can be captured into a CUDA graph.               */
+/* ------------------------------------------------------------------------ */
+typedef struct hpvcd_plan hpvcd_plan;
+
+/* Stage selection for hpvcd_plan_launch. */
+#define HPVCD_STAGE_RECON 0x01u   /* residual / intra / inter reconstruction    */
+#define HPVCD_STAGE_DEBLOCK 0x02u /* deblocking filter                          */
+#define HPVCD_STAGE_SAO 0x04u     /* sample adaptive offset                     */
+#define HPVCD_STAGE_OUTPUT 0x08u  /* RGB8 canvas conversion                     */
+#define HPVCD_STAGE_ALL 0x0Fu
+
+/* Variant knobs chosen by the autotuner / schedule selector.  They never
+ * change pixels, only speed. */
+typedef struct hpvcd_sched {
+    uint32_t recon_threads; /* threads per CTU worker of the intra wavefront: 32|64|128 */
+    uint32_t recon_ctas_per_sm; /* persistent CTAs per SM (0 -> occupancy max) */
+    uint32_t filter_tile;   /* post-filter tile edge in luma samples: 32|64   */
+    uint32_t fuse_filters;  /* 1: fused deblock+SAO+RGB kernel, 0: separate passes */
+} hpvcd_sched;
+
+hpvcd_status hpvcd_plan_create(const hpvcd_picture* dev_pics, uint32_t n,
+                               const hpvcd_output* out, const hpvcd_sched* sched,
+                               hpvcd_plan** plan);
+hpvcd_status hpvcd_plan_destroy(hpvcd_plan* plan);
+/* Enqueue the selected stages on `stream` (a cudaStream_t, NULL = default). */
+hpvcd_status hpvcd_plan_launch(hpvcd_plan* plan, uint32_t stages, void* stream);
+/* Device pointers of the reconstructed planes of picture i (valid after the
+ * launch completes) and of the RGB8 canvas. */
+hpvcd_status hpvcd_plan_planes(hpvcd_plan* plan, uint32_t i, void** y, void** cb, void** cr);
+hpvcd_status hpvcd_plan_canvas(hpvcd_plan* plan, void** rgb, uint64_t* bytes);
+/* Device-side error word of the last launch (0 = none); HPVCD_ERR_TIMEOUT when
+ * a wavefront wait gave up.  Synchronises with the plan's last launch. */
+hpvcd_status hpvcd_plan_device_status(hpvcd_plan* plan, void* stream);
+/* Number of kernel launches one hpvcd_plan_launch(HPVCD_STAGE_ALL) issues. */
+uint32_t hpvcd_plan_launches_per_run(const hpvcd_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPVCD_GPU_H */
