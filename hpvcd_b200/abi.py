@@ -211,6 +211,7 @@ def lib() -> C.CDLL:
             "hpvcd_plan_device_status": (i32, [vp, vp]),
             "hpvcd_plan_launches_per_run": (u32, [vp]),
             "hpvcd_abi_sizeof": (u64, [C.c_char_p]),
+            "hpvcd_copy": (i32, [vp, vp, u64, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

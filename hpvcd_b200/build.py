@@ -68,7 +68,9 @@ def build_cuda(force: bool = False, verbose_ptxas: bool = False) -> str:
         if force or _stale(obj, [cu] + deps):
             _run(flags)
         objs.append(obj)
-    _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-lcudart", "-lpthread"])
+    # static CUDA runtime (nvcc's default): no dependency on a libcudart on
+    # the library path; the driver's primary context is shared with torch.
+    _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", out, *objs, "-lpthread"])
     return out
 
 

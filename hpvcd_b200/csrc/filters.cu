@@ -1,0 +1,354 @@
+// filters.cu -- in-loop filters and output conversion.
+//
+// Deblocking (deblock.rs + the serial driver decode.rs:1774-2146): every
+// 4-line edge segment is independent within a pass, so one thread owns one
+// segment; the vertical-edge pass runs to completion before the
+// horizontal-edge pass.  Samples of exempt cells (transquant bypass, or PCM
+// with pcm_loop_filter_disabled) are never written, which equals the
+// reference's filter-then-restore (decode.rs:1831-1880).
+//
+// SAO (sao.rs + decode.rs:2258-2493): out-of-place, every sample reads the
+// deblocked picture (the reference's snapshot) and writes the final plane.
+//
+// RGB (yuv.rs:187-393 Q13 matrix, lib.rs:1964-1978 rgb8 narrowing,
+// lib.rs:1610-1660 tile placement and cropping on the canvas).
+#include "common.cuh"
+
+namespace hpvcd {
+
+// deblock.rs:34-50 (H.265 Table 8-12)
+__constant__ uint8_t c_beta[52] = {0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  0,  6,  7,
+                                   8,  9,  10, 11, 12, 13, 14, 15, 16, 17, 18, 20, 22, 24, 26, 28, 30, 32,
+                                   34, 36, 38, 40, 42, 44, 46, 48, 50, 52, 54, 56, 58, 60, 62, 64};
+__constant__ uint8_t c_tc[54] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,  0,  0,  0,  0,  0,
+                                 1, 1, 1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2,  3,  3,  3,  3,  4,
+                                 4, 4, 5, 5, 6, 6, 7, 8, 9, 10, 11, 13, 14, 16, 18, 20, 22, 24};
+
+__device__ __forceinline__ const hpvcd_cell& cell_at(const DevPic& P, int px, int py) {
+    return P.cells[(size_t)(py >> 2) * P.gw + (px >> 2)];
+}
+__device__ __forceinline__ int qp_at(const DevPic& P, int px, int py) {
+    const int gx = min(px >> 2, P.gw - 1), gy = min(py >> 2, P.gh - 1);
+    return P.cells[(size_t)gy * P.gw + gx].qp_y;
+}
+__device__ __forceinline__ bool exempt_at(const DevPic& P, int lx, int ly) {
+    return (cell_at(P, lx, ly).flags & HPVCD_CELL_EXEMPT) != 0;
+}
+
+// Luma segment: 8 taps x 4 lines around the edge, in registers.
+// v[line][tap+4] with tap -4..3 (p3..p0, q0..q3).
+__device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan) {
+    const int mid = scan + 1;
+    const hpvcd_cell& q = vertical ? cell_at(P, edge, mid) : cell_at(P, mid, edge);
+    const int bs = vertical ? q.bs_v : q.bs_h;
+    if (bs == 0) return;
+    const int qp_p = vertical ? qp_at(P, edge - 1, mid) : qp_at(P, mid, edge - 1);
+    const int qp_q = q.qp_y;
+    const int avg = (qp_p + qp_q + 1) >> 1;
+    const int sh = P.bd - 8;
+    const int beta = c_beta[clamp3i(avg + 2 * P.beta_offset_div2, 0, 51)] << sh;
+    const int tc = c_tc[clamp3i(avg + 2 * (bs - 1) + 2 * P.tc_offset_div2, 0, 53)] << sh;
+    if (tc == 0) return;
+    const int w = P.w;
+    void* pl = P.rec[0];
+    const int bps = P.bps;
+    int v[4][8];
+    auto idx = [&](int line, int tap) -> size_t {
+        return vertical ? (size_t)(scan + line) * w + (edge + tap) : (size_t)(edge + tap) * w + (scan + line);
+    };
+#pragma unroll
+    for (int l = 0; l < 4; ++l)
+#pragma unroll
+        for (int t = 0; t < 8; ++t) v[l][t] = load_sample(pl, bps, idx(l, t - 4));
+    // deblock.rs:216-238 luma_decision (lines 0 and 3)
+    auto g = [&](int l, int tap) { return v[l][tap + 4]; };
+    const int dp0 = abs(g(0, -3) - 2 * g(0, -2) + g(0, -1));
+    const int dp3 = abs(g(3, -3) - 2 * g(3, -2) + g(3, -1));
+    const int dq0 = abs(g(0, 2) - 2 * g(0, 1) + g(0, 0));
+    const int dq3 = abs(g(3, 2) - 2 * g(3, 1) + g(3, 0));
+    if (dp0 + dp3 + dq0 + dq3 >= beta) return;
+    auto dsam = [&](int l, int dpq) {
+        return 2 * dpq < (beta >> 2) && abs(g(l, -4) - g(l, -1)) + abs(g(l, 0) - g(l, 3)) < (beta >> 3) &&
+               abs(g(l, -1) - g(l, 0)) < ((5 * tc + 1) >> 1);
+    };
+    const bool strong = dsam(0, dp0 + dq0) && dsam(3, dp3 + dq3);
+    const int side_thr = (beta + (beta >> 1)) >> 3;
+    const bool do_p1 = dp0 + dp3 < side_thr, do_q1 = dq0 + dq3 < side_thr;
+    const int maxv = (1 << P.bd) - 1;
+    // exemption of the P / Q side (whole 4x4 cells)
+    const bool ex_p = vertical ? exempt_at(P, edge - 1, mid) : exempt_at(P, mid, edge - 1);
+    const bool ex_q = (q.flags & HPVCD_CELL_EXEMPT) != 0;
+    const int tc2 = tc >> 1;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+        const int p0 = g(l, -1), p1 = g(l, -2), p2 = g(l, -3), p3 = g(l, -4);
+        const int q0 = g(l, 0), q1 = g(l, 1), q2 = g(l, 2), q3 = g(l, 3);
+        if (strong) {  // deblock.rs:605-616
+            auto c = [&](int o, int x) { return clamp3i(clamp3i(x, o - 2 * tc, o + 2 * tc), 0, maxv); };
+            if (!ex_p) {
+                store_sample(pl, bps, idx(l, -1), c(p0, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3));
+                store_sample(pl, bps, idx(l, -2), c(p1, (p2 + p1 + p0 + q0 + 2) >> 2));
+                store_sample(pl, bps, idx(l, -3), c(p2, (2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3));
+            }
+            if (!ex_q) {
+                store_sample(pl, bps, idx(l, 0), c(q0, (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3));
+                store_sample(pl, bps, idx(l, 1), c(q1, (p0 + q0 + q1 + q2 + 2) >> 2));
+                store_sample(pl, bps, idx(l, 2), c(q2, (p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3));
+            }
+        } else {  // deblock.rs:617-631
+            const int delta0 = (9 * (q0 - p0) - 3 * (q1 - p1) + 8) >> 4;
+            if (abs(delta0) < tc * 10) {
+                const int delta = clamp3i(delta0, -tc, tc);
+                if (!ex_p) {
+                    store_sample(pl, bps, idx(l, -1), clamp3i(p0 + delta, 0, maxv));
+                    if (do_p1) {
+                        const int dp1 = clamp3i((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -tc2, tc2);
+                        store_sample(pl, bps, idx(l, -2), clamp3i(p1 + dp1, 0, maxv));
+                    }
+                }
+                if (!ex_q) {
+                    store_sample(pl, bps, idx(l, 0), clamp3i(q0 - delta, 0, maxv));
+                    if (do_q1) {
+                        const int dq1 = clamp3i((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -tc2, tc2);
+                        store_sample(pl, bps, idx(l, 1), clamp3i(q1 + dq1, 0, maxv));
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Chroma segment (decode.rs:2036-2137): 4 chroma lines, both Cb and Cr.
+__device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int scan) {
+    const int mid = scan + 1;
+    const int lex = vertical ? edge * P.sub_w : mid * P.sub_w;
+    const int ley = vertical ? mid * P.sub_h : edge * P.sub_h;
+    if (lex >= P.w || ley >= P.h) return;
+    const hpvcd_cell& q = cell_at(P, lex, ley);
+    const int bs = vertical ? q.bs_v : q.bs_h;
+    if (bs < 2) return;
+    const int lqx = min(lex, P.w - 1), lqy = min(ley, P.h - 1);
+    int ppx, ppy;
+    if (vertical) {
+        ppx = min(max(lex - 1, 0), P.w - 1);
+        ppy = min(ley, P.h - 1);
+    } else {
+        ppx = min(lex, P.w - 1);
+        ppy = min(max(ley - 1, 0), P.h - 1);
+    }
+    const int avg = (qp_at(P, ppx, ppy) + qp_at(P, lqx, lqy) + 1) >> 1;
+    const int sh = P.bd_c - 8;
+    const int maxv = (1 << P.bd_c) - 1;
+    const int cw = P.cw;
+    const int scan_max = vertical ? P.ch : P.cw;
+    for (int plane = 0; plane < 2; ++plane) {
+        const int off = plane == 0 ? P.pps_cb_qp_offset : P.pps_cr_qp_offset;
+        const int qc = qpc_map(avg + off, P.idc, P.bd_c);
+        const int tc = c_tc[clamp3i(qc + 2 + 2 * P.tc_offset_div2, 0, 53)] << sh;
+        if (tc == 0) continue;
+        void* pl = P.rec[1 + plane];
+        for (int s = scan; s < scan + 4; ++s) {
+            if (s >= scan_max) continue;
+            size_t ip0, ip1, iq0, iq1;
+            int pxl, pyl, qxl, qyl;  // luma positions of p0 / q0 for exemption
+            if (vertical) {
+                ip0 = (size_t)s * cw + edge - 1;
+                ip1 = ip0 - 1;
+                iq0 = (size_t)s * cw + edge;
+                iq1 = iq0 + 1;
+                pxl = (edge - 1) * P.sub_w; pyl = s * P.sub_h;
+                qxl = edge * P.sub_w; qyl = s * P.sub_h;
+            } else {
+                ip0 = (size_t)(edge - 1) * cw + s;
+                ip1 = (size_t)(edge - 2) * cw + s;
+                iq0 = (size_t)edge * cw + s;
+                iq1 = (size_t)(edge + 1) * cw + s;
+                pxl = s * P.sub_w; pyl = (edge - 1) * P.sub_h;
+                qxl = s * P.sub_w; qyl = edge * P.sub_h;
+            }
+            const int p0 = load_sample(pl, P.bps, ip0), p1 = load_sample(pl, P.bps, ip1);
+            const int q0 = load_sample(pl, P.bps, iq0), q1 = load_sample(pl, P.bps, iq1);
+            const int delta = clamp3i((((q0 - p0) * 4 + p1 - q1 + 4) >> 3), -tc, tc);
+            if (delta != 0) {
+                if (!exempt_at(P, pxl, pyl)) store_sample(pl, P.bps, ip0, clamp3i(p0 + delta, 0, maxv));
+                if (!exempt_at(P, qxl, qyl)) store_sample(pl, P.bps, iq0, clamp3i(q0 - delta, 0, maxv));
+            }
+        }
+    }
+}
+
+// blockIdx.y = picture, blockIdx.z = 0 luma / 1 chroma.
+__global__ void k_deblock(const DevPic* __restrict__ pics, int vertical) {
+    const DevPic& P = pics[blockIdx.y];
+    if (!(P.flags & HPVCD_PIC_DEBLOCK) || !P.cells) return;
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (blockIdx.z == 0) {
+        const int edge_max = vertical ? P.w : P.h, scan_max = vertical ? P.h : P.w;
+        const int n_edges = edge_max >= 12 ? (edge_max - 4) / 8 : 0;  // edges 8, 16, ... <= max - 4
+        const int n_segs = scan_max / 4;
+        if (id >= n_edges * n_segs) return;
+        const int e = id / n_segs, s = id % n_segs;
+        luma_segment(P, vertical != 0, 8 * (e + 1), 4 * s);
+    } else {
+        if (P.idc == 0) return;
+        const int edge_max = vertical ? P.cw : P.ch, scan_max = vertical ? P.ch : P.cw;
+        const int n_edges = edge_max >= 10 ? (edge_max - 2) / 8 : 0;  // edges 8, 16, ... <= max - 2
+        const int n_segs = scan_max / 4;  // decode.rs:2042 `while scan + 4 <= scan_max`
+        if (id >= n_edges * n_segs) return;
+        const int e = id / n_segs, s = id % n_segs;
+        chroma_segment(P, vertical != 0, 8 * (e + 1), 4 * s);
+    }
+}
+
+// SAO: one thread per sample.  blockIdx.y = picture, blockIdx.z = component.
+__global__ void k_sao(const DevPic* __restrict__ pics) {
+    const DevPic& P = pics[blockIdx.y];
+    const int c = blockIdx.z;
+    if (P.rec[0] == P.fin[0]) return;  // no SAO for this picture
+    if (c > 0 && P.idc == 0) return;
+    const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= pw * ph) return;
+    const int x = id % pw, y = id / pw;
+    const void* src = P.rec[c];
+    void* dst = P.fin[c];
+    const int bps = P.bps;
+    const int s = load_sample(src, bps, (size_t)y * pw + x);
+    int out = s;
+    const bool on = c == 0 ? (P.flags & HPVCD_PIC_SAO_LUMA) != 0 : (P.flags & HPVCD_PIC_SAO_CHROMA) != 0;
+    const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
+    const int lx = x * sw, ly = y * sh;
+    const bool exempt = P.cells && exempt_at(P, lx, ly);
+    if (on && P.sao && !exempt) {
+        const int rx = lx >> P.log2_ctb, ry = ly >> P.log2_ctb;
+        const hpvcd_sao_comp sc = P.sao[(size_t)ry * P.ctb_cols + rx].comp[c];
+        const int bd = c ? P.bd_c : P.bd;
+        const int mx = (1 << bd) - 1;
+        if (sc.type_idx == 1) {  // sao.rs:205-233
+            const uint8_t rel = (uint8_t)((uint8_t)(s >> (bd - 5)) - sc.band_pos);
+            if (rel < 4) out = clamp3i(s + sc.offsets[rel], 0, mx);
+        } else if (sc.type_idx == 2) {  // sao.rs:266-330
+            int dx, dy;
+            switch (sc.eo_class) {
+                case 0: dx = 1; dy = 0; break;
+                case 1: dx = 0; dy = 1; break;
+                case 2: dx = 1; dy = 1; break;
+                default: dx = 1; dy = -1; break;
+            }
+            const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
+            if (x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph) {
+                const int n1 = load_sample(src, bps, (size_t)y1 * pw + x1);
+                const int n2 = load_sample(src, bps, (size_t)y2 * pw + x2);
+                const int e = ((s > n1) - (s < n1)) + ((s > n2) - (s < n2)) + 2;
+                int o = 0;
+                if (e == 0) o = sc.offsets[0];
+                else if (e == 1) o = sc.offsets[1];
+                else if (e == 3) o = sc.offsets[2];
+                else if (e == 4) o = sc.offsets[3];
+                if (o) out = clamp3i(s + o, 0, mx);
+            }
+        }
+    }
+    store_sample(dst, bps, (size_t)y * pw + x, out);
+}
+
+// Q13 YCbCr -> RGB8 onto the canvas.  blockIdx.y = picture.
+struct RgbParams {
+    int matrix, full_range, canvas_w, canvas_h;
+};
+
+__global__ void k_rgb(const DevPic* __restrict__ pics, RgbParams rp, uint8_t* __restrict__ canvas) {
+    const DevPic& P = pics[blockIdx.y];
+    const int tw = P.crop_w, th = P.crop_h;
+    const int copy_w = min(tw, max(rp.canvas_w - P.dst_x, 0));
+    const int copy_h = min(th, max(rp.canvas_h - P.dst_y, 0));
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= copy_w * copy_h) return;
+    const int xx = id % copy_w, yy = id / copy_w;
+    const int bd = P.bd;
+    const long long Q13 = 13, ONE = 1 << 13, ROUND = 1 << 12;
+    const long long scale = 1ll << (bd - 8);
+    const bool full = rp.full_range != 0;
+    const long long k_y = full ? ONE : 9539, k_uv = full ? ONE : 9326;
+    long long cr_r0, cb_g0, cr_g0, cb_b0;
+    switch (rp.matrix) {
+        case HPVCD_MATRIX_BT470BG:
+        case HPVCD_MATRIX_SMPTE170M: cr_r0 = 11485; cb_g0 = -2819; cr_g0 = -5851; cb_b0 = 14516; break;
+        case HPVCD_MATRIX_BT2020NCL: cr_r0 = 12080; cb_g0 = -1348; cr_g0 = -4681; cb_b0 = 17546; break;
+        case HPVCD_MATRIX_IDENTITY: cr_r0 = cb_g0 = cr_g0 = cb_b0 = 0; break;
+        default: cr_r0 = 12901; cb_g0 = -1534; cr_g0 = -3835; cb_b0 = 15201; break;
+    }
+    const long long cmax = (1 << bd) - 1;
+    const long long y_black = full ? 0 : 16 * scale, c_black = y_black, neutral = 128 * scale;
+    const int yr = min(yy, P.h - 1), xc = min(xx, P.w - 1);
+    const long long luma = load_sample(P.fin[0], P.bps, (size_t)yr * P.w + xc);
+    long long r, g, b;
+    if (P.idc == 0) {
+        r = g = b = (k_y * (luma - y_black) + ROUND) >> Q13;
+    } else {
+        const int crow = min(yy / P.sub_h, P.ch - 1), ccol = min(xx / P.sub_w, P.cw - 1);
+        const long long cb = load_sample(P.fin[1], P.bps, (size_t)crow * P.cw + ccol);
+        const long long cr = load_sample(P.fin[2], P.bps, (size_t)crow * P.cw + ccol);
+        if (rp.matrix == HPVCD_MATRIX_IDENTITY) {
+            if (full) {
+                r = cr; g = luma; b = cb;
+            } else {
+                r = (k_uv * (cr - c_black) + ROUND) >> Q13;
+                g = (k_y * (luma - y_black) + ROUND) >> Q13;
+                b = (k_uv * (cb - c_black) + ROUND) >> Q13;
+            }
+        } else if (rp.matrix == HPVCD_MATRIX_YCGCO) {
+            const long long cg = cb - neutral, co = cr - neutral, t = luma - cg;
+            r = t + co; g = luma + cg; b = t - co;
+        } else {
+            const long long cr_to_r = (cr_r0 * k_uv + ROUND) >> Q13, cb_to_g = (cb_g0 * k_uv + ROUND) >> Q13;
+            const long long cr_to_g = (cr_g0 * k_uv + ROUND) >> Q13, cb_to_b = (cb_b0 * k_uv + ROUND) >> Q13;
+            const long long yv = k_y * (luma - y_black), cbc = cb - neutral, crc = cr - neutral;
+            r = (yv + cr_to_r * crc + ROUND) >> Q13;
+            g = (yv + cb_to_g * cbc + cr_to_g * crc + ROUND) >> Q13;
+            b = (yv + cb_to_b * cbc + ROUND) >> Q13;
+        }
+    }
+    const int sh = bd - 8;
+    r = r < 0 ? 0 : (r > cmax ? cmax : r);
+    g = g < 0 ? 0 : (g > cmax ? cmax : g);
+    b = b < 0 ? 0 : (b > cmax ? cmax : b);
+    uint8_t* o = canvas + ((size_t)(P.dst_y + yy) * rp.canvas_w + P.dst_x + xx) * 3;
+    o[0] = (uint8_t)(r >> sh);
+    o[1] = (uint8_t)(g >> sh);
+    o[2] = (uint8_t)(b >> sh);
+}
+
+}  // namespace hpvcd
+
+extern "C" cudaError_t hpvcd_launch_deblock(const hpvcd::DevPic* pics, int n_pics, int max_segments,
+                                            int vertical, cudaStream_t stream) {
+    if (n_pics <= 0 || max_segments <= 0) return cudaSuccess;
+    const int threads = 256;
+    dim3 grid((max_segments + threads - 1) / threads, n_pics, 2);
+    hpvcd::k_deblock<<<grid, threads, 0, stream>>>(pics, vertical);
+    hpvcd_note_launches(1);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t hpvcd_launch_sao(const hpvcd::DevPic* pics, int n_pics, int max_samples,
+                                        cudaStream_t stream) {
+    if (n_pics <= 0 || max_samples <= 0) return cudaSuccess;
+    const int threads = 256;
+    dim3 grid((max_samples + threads - 1) / threads, n_pics, 3);
+    hpvcd::k_sao<<<grid, threads, 0, stream>>>(pics);
+    hpvcd_note_launches(1);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t hpvcd_launch_rgb(const hpvcd::DevPic* pics, int n_pics, int max_pixels, int matrix,
+                                        int full_range, int canvas_w, int canvas_h, uint8_t* canvas,
+                                        cudaStream_t stream) {
+    if (n_pics <= 0 || max_pixels <= 0) return cudaSuccess;
+    const int threads = 256;
+    dim3 grid((max_pixels + threads - 1) / threads, n_pics, 1);
+    hpvcd::RgbParams rp{matrix, full_range, canvas_w, canvas_h};
+    hpvcd::k_rgb<<<grid, threads, 0, stream>>>(pics, rp, canvas);
+    hpvcd_note_launches(1);
+    return cudaGetLastError();
+}

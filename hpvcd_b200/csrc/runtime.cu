@@ -1,0 +1,834 @@
+// runtime.cu -- host runtime behind include/hpvcd_gpu.h: plans (device
+// buffers, kernel schedule), contexts (host buffers, staging, streams,
+// tickets, HBM admission) and the exported C entry points.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "common.cuh"
+
+#define HPVCD_API extern "C" __attribute__((visibility("default")))
+
+using hpvcd::CtuItem;
+using hpvcd::DevPic;
+
+extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int,
+                                          int, cudaStream_t);
+extern "C" int hpvcd_recon_occupancy(int c444);
+extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, int, int, int, int, uint8_t*, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_mc(const DevPic*, int, int, int, cudaStream_t);
+
+static std::atomic<uint64_t> g_launches{0};
+extern "C" void hpvcd_note_launches(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct Geo {
+    int w, h, cw, ch, gw, gh, sub_w, sub_h, bps, ctb_cols, ctb_rows;
+    size_t luma_bytes, chroma_bytes;
+};
+
+Geo geo_of(const hpvcd_picture& p) {
+    Geo g;
+    g.w = (int)p.width;
+    g.h = (int)p.height;
+    g.sub_w = p.chroma_idc == 1 ? 2 : 1;
+    g.sub_h = p.chroma_idc == 1 ? 2 : 1;
+    g.cw = p.chroma_idc ? (g.w + g.sub_w - 1) / g.sub_w : 0;
+    g.ch = p.chroma_idc ? (g.h + g.sub_h - 1) / g.sub_h : 0;
+    g.gw = (g.w + 3) / 4;
+    g.gh = (g.h + 3) / 4;
+    g.bps = p.bit_depth_y <= 8 && p.bit_depth_c <= 8 ? 1 : 2;
+    const int ctb = 1 << p.log2_ctb;
+    g.ctb_cols = (g.w + ctb - 1) / ctb;
+    g.ctb_rows = (g.h + ctb - 1) / ctb;
+    g.luma_bytes = (size_t)g.w * g.h * g.bps;
+    g.chroma_bytes = (size_t)g.cw * g.ch * g.bps;
+    return g;
+}
+
+hpvcd_status validate(const hpvcd_picture& p) {
+    if (p.width == 0 || p.height == 0 || p.width > 16384 || p.height > 16384) return HPVCD_ERR_LIMIT;
+    if ((p.width & 7) || (p.height & 7)) return HPVCD_ERR_BITSTREAM;
+    if (p.chroma_idc == 2 || p.chroma_idc > 3) return HPVCD_ERR_UNSUPPORTED;
+    if (p.bit_depth_y < 8 || p.bit_depth_y > 12 || p.bit_depth_c < 8 || p.bit_depth_c > 12)
+        return HPVCD_ERR_UNSUPPORTED;
+    if ((p.bit_depth_y == 8) != (p.bit_depth_c == 8)) return HPVCD_ERR_UNSUPPORTED;
+    if (p.log2_ctb < 4 || p.log2_ctb > 6) return HPVCD_ERR_BITSTREAM;
+    if (p.n_tus && (!p.tus || !p.ctu_tu_start)) return HPVCD_ERR_INVALID_ARG;
+    if (p.n_coeffs && !p.coeffs) return HPVCD_ERR_INVALID_ARG;
+    if (p.n_pus && !p.pus) return HPVCD_ERR_INVALID_ARG;
+    if (!p.ctu_tu_start) return HPVCD_ERR_INVALID_ARG;
+    if ((p.flags & HPVCD_PIC_DEBLOCK) && !p.cells) return HPVCD_ERR_INVALID_ARG;
+    if ((p.flags & HPVCD_PIC_PRED_IN_PLANE) && !p.pred[0]) return HPVCD_ERR_INVALID_ARG;
+    return HPVCD_OK;
+}
+
+bool sao_active(const hpvcd_picture& p) {
+    return p.sao && (p.flags & (HPVCD_PIC_SAO_LUMA | HPVCD_PIC_SAO_CHROMA));
+}
+
+struct Segment {
+    uint32_t first_pic, n_pics;
+    uint32_t item_off, n_items;
+    int max_dbk_v, max_dbk_h, max_sao;
+};
+
+}  // namespace
+
+struct hpvcd_plan {
+    int device = 0;
+    std::vector<hpvcd_picture> src;
+    std::vector<DevPic> pics;
+    DevPic* d_pics = nullptr;
+    std::vector<CtuItem> items;
+    CtuItem* d_items = nullptr;
+    std::vector<Segment> segs;
+    uint32_t* d_scratch = nullptr;  // [seg counters][err][ready flags...]
+    size_t scratch_words = 0;
+    unsigned char* d_planes = nullptr;
+    size_t plane_bytes = 0;
+    uint8_t* d_canvas = nullptr;
+    size_t canvas_bytes = 0;
+    hpvcd_output out{};
+    std::vector<hpvcd_tile_place> places;
+    hpvcd_sched sched{};
+    int c444 = 0;
+    int recon_grid = 0;
+    int max_rgb = 0;
+    uint32_t launches_per_run = 0;
+
+    ~hpvcd_plan() {
+        cudaFree(d_pics);
+        cudaFree(d_items);
+        cudaFree(d_scratch);
+        cudaFree(d_planes);
+        cudaFree(d_canvas);
+    }
+};
+
+namespace {
+
+hpvcd_status cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return HPVCD_OK;
+    if (e == cudaErrorMemoryAllocation) return HPVCD_ERR_ALLOC;
+    return HPVCD_ERR_CUDA;
+}
+
+// Device bytes a plan for these pictures needs (planes, scratch, canvas).
+size_t plan_footprint(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out) {
+    size_t bytes = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const Geo g = geo_of(pics[i]);
+        const size_t one = align_up(g.luma_bytes, 256) + 2 * align_up(g.chroma_bytes, 256);
+        bytes += one * (sao_active(pics[i]) ? 2 : 1);
+        bytes += (size_t)g.ctb_cols * g.ctb_rows * (4 + sizeof(CtuItem));
+    }
+    bytes += n * sizeof(DevPic);
+    if (out && out->kind == HPVCD_OUT_RGB8) bytes += (size_t)out->canvas_w * out->canvas_h * 3;
+    return bytes;
+}
+
+// Rebuild the input-pointer fields of the device table from descriptors.
+void fill_inputs(DevPic& d, const hpvcd_picture& p) {
+    d.tus = p.tus;
+    d.ctu_start = p.ctu_tu_start;
+    d.coeffs = p.coeffs;
+    d.cells = p.cells;
+    d.sao = p.sao;
+    d.pus = p.pus;
+    d.n_tus = p.n_tus;
+    d.n_pus = p.n_pus;
+    d.n_coeffs = p.n_coeffs;
+}
+
+hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out,
+                        const hpvcd_sched* sched, const hpvcd_wp_table* host_wp, hpvcd_plan** result) {
+    if (!pics || n == 0 || !result) return HPVCD_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < n; ++i) {
+        const hpvcd_status s = validate(pics[i]);
+        if (s != HPVCD_OK) return s;
+    }
+    if (out && out->kind == HPVCD_OUT_RGB8 && (!out->place || out->canvas_w == 0 || out->canvas_h == 0))
+        return HPVCD_ERR_INVALID_ARG;
+    hpvcd_plan* P = new (std::nothrow) hpvcd_plan();
+    if (!P) return HPVCD_ERR_ALLOC;
+    cudaGetDevice(&P->device);
+    P->src.assign(pics, pics + n);
+    if (out) {
+        P->out = *out;
+        if (out->kind == HPVCD_OUT_RGB8) {
+            P->places.assign(out->place, out->place + n);
+            P->out.place = nullptr;
+        }
+    } else {
+        P->out.kind = HPVCD_OUT_YUV;
+    }
+    if (sched) P->sched = *sched;
+    bool any_inter = false;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (pics[i].chroma_idc == 3) P->c444 = 1;
+        if (pics[i].flags & HPVCD_PIC_INTER) any_inter = true;
+    }
+    // ---- planes + scratch layout ----
+    size_t plane_bytes = 0;
+    std::vector<size_t> rec_off(n), fin_off(n);
+    size_t ready_words = 0;
+    std::vector<size_t> ready_off(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const Geo g = geo_of(pics[i]);
+        const size_t one = align_up(g.luma_bytes, 256) + 2 * align_up(g.chroma_bytes, 256);
+        rec_off[i] = plane_bytes;
+        plane_bytes += one;
+        if (sao_active(pics[i])) {
+            fin_off[i] = plane_bytes;
+            plane_bytes += one;
+        } else {
+            fin_off[i] = rec_off[i];
+        }
+        ready_off[i] = ready_words;
+        ready_words += (size_t)g.ctb_cols * g.ctb_rows;
+    }
+    // segments: all pictures at once, or one per picture when any picture
+    // predicts from another (its references must be final first).
+    if (any_inter) {
+        for (uint32_t i = 0; i < n; ++i) P->segs.push_back(Segment{i, 1, 0, 0, 0, 0, 0});
+    } else {
+        P->segs.push_back(Segment{0, n, 0, 0, 0, 0, 0});
+    }
+    const size_t n_seg = P->segs.size();
+    P->scratch_words = n_seg + 1 + ready_words;
+    cudaError_t e = cudaMalloc(&P->d_planes, std::max<size_t>(plane_bytes, 256));
+    if (e == cudaSuccess) e = cudaMalloc(&P->d_scratch, P->scratch_words * sizeof(uint32_t));
+    if (e == cudaSuccess && P->out.kind == HPVCD_OUT_RGB8) {
+        P->canvas_bytes = (size_t)P->out.canvas_w * P->out.canvas_h * 3;
+        e = cudaMalloc(&P->d_canvas, P->canvas_bytes);
+        if (e == cudaSuccess) e = cudaMemset(P->d_canvas, 0, P->canvas_bytes);
+    }
+    if (e != cudaSuccess) {
+        delete P;
+        cudaGetLastError();
+        return cuda_status(e);
+    }
+    P->plane_bytes = plane_bytes;
+    // ---- device picture table ----
+    P->pics.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const hpvcd_picture& p = pics[i];
+        const Geo g = geo_of(p);
+        DevPic& d = P->pics[i];
+        std::memset(&d, 0, sizeof(d));
+        d.w = g.w; d.h = g.h; d.cw = g.cw; d.ch = g.ch; d.gw = g.gw; d.gh = g.gh;
+        d.idc = p.chroma_idc; d.sub_w = g.sub_w; d.sub_h = g.sub_h;
+        d.bd = p.bit_depth_y; d.bd_c = p.bit_depth_c; d.bps = g.bps;
+        d.log2_ctb = p.log2_ctb; d.ctb_cols = g.ctb_cols; d.ctb_rows = g.ctb_rows;
+        d.flags = p.flags;
+        d.beta_offset_div2 = p.beta_offset_div2;
+        d.tc_offset_div2 = p.tc_offset_div2;
+        d.pps_cb_qp_offset = p.pps_cb_qp_offset;
+        d.pps_cr_qp_offset = p.pps_cr_qp_offset;
+        fill_inputs(d, p);
+        if (host_wp && p.wp) {
+            d.wp = host_wp[i];
+            d.has_wp = 1;
+        }
+        for (int l = 0; l < 2; ++l)
+            for (int r = 0; r < HPVCD_MAX_REFS; ++r) {
+                const int s = p.ref_slot[l][r];
+                d.ref_pic[l][r] = (s >= 0 && (uint32_t)s < i) ? s : -1;
+            }
+        unsigned char* base = P->d_planes + rec_off[i];
+        d.rec[0] = base;
+        d.rec[1] = base + align_up(g.luma_bytes, 256);
+        d.rec[2] = base + align_up(g.luma_bytes, 256) + align_up(g.chroma_bytes, 256);
+        unsigned char* fb = P->d_planes + fin_off[i];
+        d.fin[0] = fb;
+        d.fin[1] = fb + align_up(g.luma_bytes, 256);
+        d.fin[2] = fb + align_up(g.luma_bytes, 256) + align_up(g.chroma_bytes, 256);
+        if (!p.chroma_idc) d.rec[1] = d.rec[2] = d.fin[1] = d.fin[2] = nullptr;
+        d.ready = P->d_scratch + n_seg + 1 + ready_off[i];
+        d.needs_wavefront = (p.flags & HPVCD_PIC_PRED_IN_PLANE) ? 0 : 1;
+        if (P->out.kind == HPVCD_OUT_RGB8) {
+            const hpvcd_tile_place& tp = P->places[i];
+            d.dst_x = (int)tp.dst_x; d.dst_y = (int)tp.dst_y;
+            d.crop_w = (int)std::min<uint32_t>(tp.crop_w, p.width);
+            d.crop_h = (int)std::min<uint32_t>(tp.crop_h, p.height);
+            P->max_rgb = std::max(P->max_rgb, d.crop_w * d.crop_h);
+        }
+    }
+    // ---- wavefront schedule per segment: sort CTUs by (x + 2y, picture, x) ----
+    for (Segment& s : P->segs) {
+        s.item_off = (uint32_t)P->items.size();
+        int max_t = 0;
+        for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
+            max_t = std::max(max_t, P->pics[i].ctb_cols + 2 * P->pics[i].ctb_rows);
+        for (int t = 0; t <= max_t; ++t)
+            for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
+                const DevPic& d = P->pics[i];
+                for (int y = 0; y < d.ctb_rows; ++y) {
+                    const int x = t - 2 * y;
+                    if (x >= 0 && x < d.ctb_cols) P->items.push_back(CtuItem{i, (uint16_t)x, (uint16_t)y});
+                }
+            }
+        s.n_items = (uint32_t)P->items.size() - s.item_off;
+        for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
+            const DevPic& d = P->pics[i];
+            const int lv = (d.w >= 12 ? (d.w - 4) / 8 : 0) * (d.h / 4);
+            const int lh = (d.h >= 12 ? (d.h - 4) / 8 : 0) * (d.w / 4);
+            const int cv = d.idc ? (d.cw >= 10 ? (d.cw - 2) / 8 : 0) * (d.ch / 4) : 0;
+            const int ch = d.idc ? (d.ch >= 10 ? (d.ch - 2) / 8 : 0) * (d.cw / 4) : 0;
+            s.max_dbk_v = std::max(s.max_dbk_v, std::max(lv, cv));
+            s.max_dbk_h = std::max(s.max_dbk_h, std::max(lh, ch));
+            if (d.rec[0] != d.fin[0]) s.max_sao = std::max(s.max_sao, d.w * d.h);
+        }
+    }
+    e = cudaMalloc(&P->d_pics, sizeof(DevPic) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&P->d_items, sizeof(CtuItem) * std::max<size_t>(P->items.size(), 1));
+    if (e == cudaSuccess) e = cudaMemcpy(P->d_pics, P->pics.data(), sizeof(DevPic) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !P->items.empty())
+        e = cudaMemcpy(P->d_items, P->items.data(), sizeof(CtuItem) * P->items.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        delete P;
+        cudaGetLastError();
+        return cuda_status(e);
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
+    int occ = hpvcd_recon_occupancy(P->c444);
+    if (occ <= 0) occ = 1;
+    if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
+    P->recon_grid = sms * occ;
+    // launches per full run
+    uint32_t L = 0;
+    for (const Segment& s : P->segs) {
+        for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
+            if ((P->src[i].flags & HPVCD_PIC_INTER) && P->src[i].n_pus) ++L;
+        L += 1;                             // recon
+        if (s.max_dbk_v > 0) L += 1;
+        if (s.max_dbk_h > 0) L += 1;
+        if (s.max_sao > 0) L += 1;
+    }
+    if (P->out.kind == HPVCD_OUT_RGB8 && P->max_rgb > 0) L += 1;
+    P->launches_per_run = L;
+    *result = P;
+    return HPVCD_OK;
+}
+
+hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(P->d_scratch, 0, P->scratch_words * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return cuda_status(e);
+    const uint32_t n_seg = (uint32_t)P->segs.size();
+    uint32_t* d_err = P->d_scratch + n_seg;
+    if (stages & HPVCD_STAGE_RECON) {
+        for (size_t i = 0; i < P->src.size(); ++i) {
+            const hpvcd_picture& p = P->src[i];
+            if (!(p.flags & HPVCD_PIC_PRED_IN_PLANE)) continue;
+            const Geo g = geo_of(p);
+            const DevPic& d = P->pics[i];
+            for (int c = 0; c < (p.chroma_idc ? 3 : 1); ++c) {
+                if (!p.pred[c]) continue;
+                e = cudaMemcpyAsync(d.rec[c], p.pred[c], c ? g.chroma_bytes : g.luma_bytes,
+                                    cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
+        }
+    }
+    for (uint32_t si = 0; si < n_seg; ++si) {
+        const Segment& s = P->segs[si];
+        const DevPic* dp = P->d_pics + s.first_pic;
+        if (stages & HPVCD_STAGE_RECON) {
+            for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
+                if ((P->src[i].flags & HPVCD_PIC_INTER) && P->src[i].n_pus) {
+                    e = hpvcd_launch_mc(P->d_pics, (int)i, (int)P->src[i].n_pus, P->src[i].chroma_idc ? 3 : 1, st);
+                    if (e != cudaSuccess) return cuda_status(e);
+                }
+            const int grid = std::max(1, std::min<int>(P->recon_grid, (int)s.n_items));
+            e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
+                                   P->c444, grid, st);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        if (stages & HPVCD_STAGE_DEBLOCK) {
+            e = hpvcd_launch_deblock(dp, (int)s.n_pics, s.max_dbk_v, 1, st);
+            if (e == cudaSuccess) e = hpvcd_launch_deblock(dp, (int)s.n_pics, s.max_dbk_h, 0, st);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+        if (stages & HPVCD_STAGE_SAO) {
+            e = hpvcd_launch_sao(dp, (int)s.n_pics, s.max_sao, st);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+    }
+    if ((stages & HPVCD_STAGE_OUTPUT) && P->out.kind == HPVCD_OUT_RGB8) {
+        e = hpvcd_launch_rgb(P->d_pics, (int)P->pics.size(), P->max_rgb, (int)P->out.matrix,
+                             (int)P->out.full_range, (int)P->out.canvas_w, (int)P->out.canvas_h, P->d_canvas,
+                             st);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    return HPVCD_OK;
+}
+
+// Re-point the input fields of an existing plan at new device buffers of a
+// batch with identical geometry (same layout key).
+hpvcd_status plan_rebind(hpvcd_plan* P, const hpvcd_picture* pics, const hpvcd_wp_table* host_wp,
+                         cudaStream_t st) {
+    for (size_t i = 0; i < P->pics.size(); ++i) {
+        P->src[i] = pics[i];
+        fill_inputs(P->pics[i], pics[i]);
+        if (host_wp && pics[i].wp) {
+            P->pics[i].wp = host_wp[i];
+            P->pics[i].has_wp = 1;
+        } else {
+            P->pics[i].has_wp = 0;
+        }
+    }
+    return cuda_status(cudaMemcpyAsync(P->d_pics, P->pics.data(), sizeof(DevPic) * P->pics.size(),
+                                       cudaMemcpyHostToDevice, st));
+}
+
+bool same_layout(const hpvcd_plan* P, const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out) {
+    if (P->src.size() != n) return false;
+    for (uint32_t i = 0; i < n; ++i) {
+        const hpvcd_picture& a = P->src[i];
+        const hpvcd_picture& b = pics[i];
+        if (a.width != b.width || a.height != b.height || a.chroma_idc != b.chroma_idc ||
+            a.bit_depth_y != b.bit_depth_y || a.bit_depth_c != b.bit_depth_c || a.log2_ctb != b.log2_ctb ||
+            a.flags != b.flags || a.beta_offset_div2 != b.beta_offset_div2 ||
+            a.tc_offset_div2 != b.tc_offset_div2 || a.pps_cb_qp_offset != b.pps_cb_qp_offset ||
+            a.pps_cr_qp_offset != b.pps_cr_qp_offset || (a.sao != nullptr) != (b.sao != nullptr) ||
+            (a.n_pus != 0) != (b.n_pus != 0) ||
+            std::memcmp(a.ref_slot, b.ref_slot, sizeof(a.ref_slot)) != 0)
+            return false;
+    }
+    const uint32_t kind = out ? out->kind : HPVCD_OUT_YUV;
+    if (kind != P->out.kind) return false;
+    if (kind == HPVCD_OUT_RGB8) {
+        if (out->matrix != P->out.matrix || out->full_range != P->out.full_range ||
+            out->canvas_w != P->out.canvas_w || out->canvas_h != P->out.canvas_h)
+            return false;
+        for (uint32_t i = 0; i < n; ++i)
+            if (std::memcmp(&out->place[i], &P->places[i], sizeof(hpvcd_tile_place)) != 0) return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Contexts (host-buffer API)
+// ---------------------------------------------------------------------------
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    unsigned char* h_in = nullptr;  // pinned staging of the inputs
+    size_t h_in_cap = 0;
+    unsigned char* d_in = nullptr;  // device input arena
+    size_t d_in_cap = 0;
+    unsigned char* h_out = nullptr;  // pinned output
+    size_t h_out_cap = 0;
+    hpvcd_plan* plan = nullptr;
+    uint64_t ticket = 0;  // 0 = free
+    uint64_t out_bytes = 0;
+    uint64_t plan_bytes = 0;  // device bytes of `plan`
+    uint64_t held = 0;        // device bytes this slot holds (arena + plan)
+    bool busy = false;
+    std::vector<hpvcd_wp_table> wp;
+};
+
+}  // namespace
+
+struct hpvcd_gpu {
+    int device = 0;
+    std::mutex mu;
+    std::vector<Slot> slots;
+    uint64_t next_ticket = 1;
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    ~hpvcd_gpu() {
+        for (Slot& s : slots) {
+            if (s.stream) cudaStreamSynchronize(s.stream);
+            delete s.plan;
+            cudaFreeHost(s.h_in);
+            cudaFreeHost(s.h_out);
+            cudaFree(s.d_in);
+            if (s.done) cudaEventDestroy(s.done);
+            if (s.stream) cudaStreamDestroy(s.stream);
+        }
+    }
+};
+
+namespace {
+
+hpvcd_status grow_pinned(unsigned char** p, size_t* cap, size_t need) {
+    if (*cap >= need) return HPVCD_OK;
+    cudaFreeHost(*p);
+    *p = nullptr;
+    *cap = 0;
+    const size_t sz = align_up(need + need / 4, 1 << 20);
+    if (cudaMallocHost(p, sz) != cudaSuccess) {
+        cudaGetLastError();
+        return HPVCD_ERR_ALLOC;
+    }
+    *cap = sz;
+    return HPVCD_OK;
+}
+
+hpvcd_status grow_device(unsigned char** p, size_t* cap, size_t need) {
+    if (*cap >= need) return HPVCD_OK;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    const size_t sz = align_up(need + need / 4, 1 << 20);
+    if (cudaMalloc(p, sz) != cudaSuccess) {
+        cudaGetLastError();
+        return HPVCD_ERR_ALLOC;
+    }
+    *cap = sz;
+    return HPVCD_OK;
+}
+
+Slot* find_ticket(hpvcd_gpu* g, hpvcd_ticket t) {
+    for (Slot& s : g->slots)
+        if (s.busy && s.ticket == t) return &s;
+    return nullptr;
+}
+
+hpvcd_status device_status(hpvcd_plan* P, cudaStream_t st) {
+    uint32_t err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, P->d_scratch + P->segs.size(), sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (err & hpvcd::DEV_ERR_TIMEOUT) return HPVCD_ERR_TIMEOUT;
+    if (err & hpvcd::DEV_ERR_BITSTREAM) return HPVCD_ERR_BITSTREAM;
+    return HPVCD_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Exported C ABI
+// ===========================================================================
+HPVCD_API uint32_t hpvcd_abi_version(void) { return HPVCD_ABI_VERSION; }
+
+HPVCD_API const char* hpvcd_status_string(int s) {
+    switch (s) {
+        case HPVCD_OK: return "ok";
+        case HPVCD_ERR_BITSTREAM: return "bitstream: malformed reconstruction buffers";
+        case HPVCD_ERR_ALLOC: return "allocation failed (HBM budget or device memory)";
+        case HPVCD_ERR_LIMIT: return "limit exceeded";
+        case HPVCD_ERR_UNSUPPORTED: return "unsupported feature";
+        case HPVCD_ERR_TIMEOUT: return "device-side wait timed out";
+        case HPVCD_ERR_CUDA: return "CUDA runtime error";
+        case HPVCD_ERR_INVALID_ARG: return "invalid argument";
+        case HPVCD_ERR_BUSY: return "ticket not finished";
+        default: return "unknown status";
+    }
+}
+
+HPVCD_API uint64_t hpvcd_kernel_launch_count(void) { return g_launches.load(); }
+
+HPVCD_API hpvcd_status hpvcd_copy(void* dst, const void* src, uint64_t bytes, void* stream) {
+    if ((!dst || !src) && bytes) return HPVCD_ERR_INVALID_ARG;
+    if (!bytes) return HPVCD_OK;
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    return cuda_status(e);
+}
+
+// sizeof of ABI structs, for the binding layout test.
+HPVCD_API uint64_t hpvcd_abi_sizeof(const char* name) {
+    if (!name) return 0;
+    const struct {
+        const char* n;
+        size_t s;
+    } t[] = {{"hpvcd_tu", sizeof(hpvcd_tu)},           {"hpvcd_cell", sizeof(hpvcd_cell)},
+             {"hpvcd_sao_comp", sizeof(hpvcd_sao_comp)}, {"hpvcd_sao_ctb", sizeof(hpvcd_sao_ctb)},
+             {"hpvcd_pu", sizeof(hpvcd_pu)},           {"hpvcd_wp_entry", sizeof(hpvcd_wp_entry)},
+             {"hpvcd_wp_table", sizeof(hpvcd_wp_table)}, {"hpvcd_picture", sizeof(hpvcd_picture)},
+             {"hpvcd_tile_place", sizeof(hpvcd_tile_place)}, {"hpvcd_output", sizeof(hpvcd_output)},
+             {"hpvcd_gpu_cfg", sizeof(hpvcd_gpu_cfg)}, {"hpvcd_sched", sizeof(hpvcd_sched)}};
+    for (const auto& e : t)
+        if (std::strcmp(e.n, name) == 0) return e.s;
+    return 0;
+}
+
+HPVCD_API hpvcd_status hpvcd_plan_create(const hpvcd_picture* dev_pics, uint32_t n, const hpvcd_output* out,
+                                         const hpvcd_sched* sched, hpvcd_plan** plan) {
+    if (!dev_pics || !plan) return HPVCD_ERR_INVALID_ARG;
+    // Device-pointer descriptors: weighted-prediction tables are read from
+    // device memory once here.
+    std::vector<hpvcd_wp_table> wp(n);
+    bool any = false;
+    for (uint32_t i = 0; i < n; ++i)
+        if (dev_pics[i].wp) {
+            if (cudaMemcpy(&wp[i], dev_pics[i].wp, sizeof(hpvcd_wp_table), cudaMemcpyDeviceToHost) != cudaSuccess) {
+                cudaGetLastError();
+                return HPVCD_ERR_INVALID_ARG;
+            }
+            any = true;
+        }
+    return plan_build(dev_pics, n, out, sched, any ? wp.data() : nullptr, plan);
+}
+
+HPVCD_API hpvcd_status hpvcd_plan_destroy(hpvcd_plan* plan) {
+    if (!plan) return HPVCD_ERR_INVALID_ARG;
+    cudaDeviceSynchronize();
+    delete plan;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_plan_launch(hpvcd_plan* plan, uint32_t stages, void* stream) {
+    if (!plan) return HPVCD_ERR_INVALID_ARG;
+    return plan_launch(plan, stages, (cudaStream_t)stream);
+}
+
+HPVCD_API hpvcd_status hpvcd_plan_planes(hpvcd_plan* plan, uint32_t i, void** y, void** cb, void** cr) {
+    if (!plan || i >= plan->pics.size()) return HPVCD_ERR_INVALID_ARG;
+    if (y) *y = plan->pics[i].fin[0];
+    if (cb) *cb = plan->pics[i].fin[1];
+    if (cr) *cr = plan->pics[i].fin[2];
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_plan_canvas(hpvcd_plan* plan, void** rgb, uint64_t* bytes) {
+    if (!plan) return HPVCD_ERR_INVALID_ARG;
+    if (rgb) *rgb = plan->d_canvas;
+    if (bytes) *bytes = plan->canvas_bytes;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_plan_device_status(hpvcd_plan* plan, void* stream) {
+    if (!plan) return HPVCD_ERR_INVALID_ARG;
+    return device_status(plan, (cudaStream_t)stream);
+}
+
+HPVCD_API uint32_t hpvcd_plan_launches_per_run(const hpvcd_plan* plan) {
+    return plan ? plan->launches_per_run : 0;
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_create(const hpvcd_gpu_cfg* cfg, hpvcd_gpu** out) {
+    if (!out) return HPVCD_ERR_INVALID_ARG;
+    *out = nullptr;
+    hpvcd_gpu_cfg c{};
+    if (cfg) c = *cfg;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return HPVCD_ERR_CUDA;
+    }
+    if (c.device < 0 || c.device >= ndev) return HPVCD_ERR_INVALID_ARG;
+    if (cudaSetDevice(c.device) != cudaSuccess) return HPVCD_ERR_CUDA;
+    hpvcd_gpu* g = new (std::nothrow) hpvcd_gpu();
+    if (!g) return HPVCD_ERR_ALLOC;
+    g->device = c.device;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    g->budget = c.hbm_budget ? c.hbm_budget : (uint64_t)(free_b * 0.8);
+    const uint32_t inflight = c.max_inflight ? std::min<uint32_t>(c.max_inflight, 64) : 4;
+    g->slots.resize(inflight);
+    for (Slot& s : g->slots) {
+        if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) {
+            delete g;
+            cudaGetLastError();
+            return HPVCD_ERR_CUDA;
+        }
+    }
+    *out = g;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_destroy(hpvcd_gpu* g) {
+    if (!g) return HPVCD_ERR_INVALID_ARG;
+    cudaSetDevice(g->device);
+    delete g;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics, uint32_t n,
+                                        const hpvcd_output* out, hpvcd_ticket* ticket) {
+    if (!g || !pics || n == 0 || !ticket) return HPVCD_ERR_INVALID_ARG;
+    for (uint32_t i = 0; i < n; ++i) {
+        const hpvcd_status s = validate(pics[i]);
+        if (s != HPVCD_OK) return s;
+    }
+    if (out && out->kind == HPVCD_OUT_RGB8 && (!out->place || !out->canvas_w || !out->canvas_h))
+        return HPVCD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g->mu);
+    cudaSetDevice(g->device);
+    Slot* slot = nullptr;
+    for (Slot& s : g->slots)
+        if (!s.busy) {
+            slot = &s;
+            break;
+        }
+    if (!slot) return HPVCD_ERR_BUSY;
+    // ---- input layout in one arena ----
+    struct Part {
+        const void* src;
+        size_t bytes;
+        size_t off;
+    };
+    std::vector<Part> parts;
+    size_t total = 0;
+    auto add = [&](const void* src, size_t bytes) -> size_t {
+        const size_t off = total;
+        parts.push_back(Part{src, bytes, off});
+        total = align_up(total + bytes, 256);
+        return off;
+    };
+    std::vector<hpvcd_picture> dev(pics, pics + n);
+    std::vector<size_t> offs(n * 9, (size_t)-1);
+    for (uint32_t i = 0; i < n; ++i) {
+        const hpvcd_picture& p = pics[i];
+        const Geo geo = geo_of(p);
+        const size_t ctbs = (size_t)geo.ctb_cols * geo.ctb_rows;
+        if (p.n_tus) offs[i * 9 + 0] = add(p.tus, p.n_tus * sizeof(hpvcd_tu));
+        offs[i * 9 + 1] = add(p.ctu_tu_start, (ctbs + 1) * sizeof(uint32_t));
+        if (p.n_coeffs) offs[i * 9 + 2] = add(p.coeffs, p.n_coeffs * sizeof(int16_t));
+        if (p.cells) offs[i * 9 + 3] = add(p.cells, (size_t)geo.gw * geo.gh * sizeof(hpvcd_cell));
+        if (p.sao) offs[i * 9 + 4] = add(p.sao, ctbs * sizeof(hpvcd_sao_ctb));
+        if (p.n_pus) offs[i * 9 + 5] = add(p.pus, p.n_pus * sizeof(hpvcd_pu));
+        if (p.flags & HPVCD_PIC_PRED_IN_PLANE)
+            for (int c = 0; c < (p.chroma_idc ? 3 : 1); ++c)
+                if (p.pred[c]) offs[i * 9 + 6 + c] = add(p.pred[c], c ? geo.chroma_bytes : geo.luma_bytes);
+    }
+    // ---- HBM admission ----
+    const size_t out_bytes = [&]() -> size_t {
+        if (out && out->kind == HPVCD_OUT_RGB8) return (size_t)out->canvas_w * out->canvas_h * 3;
+        size_t b = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const Geo geo = geo_of(pics[i]);
+            b += geo.luma_bytes + 2 * geo.chroma_bytes;
+        }
+        return b;
+    }();
+    const bool reuse = slot->plan && same_layout(slot->plan, pics, n, out);
+    // HBM admission: what this slot would hold after the call (input arena +
+    // plan) against what it holds now; refuse when the context budget would
+    // be exceeded (the caller may retry once other tickets are read).
+    const uint64_t held = slot->held;
+    const uint64_t plan_bytes = reuse ? slot->plan_bytes : plan_footprint(pics, n, out);
+    const uint64_t need = std::max<uint64_t>(slot->d_in_cap, align_up(total + total / 4, 1 << 20)) + plan_bytes;
+    if (g->in_use - held + need > g->budget) return HPVCD_ERR_ALLOC;
+    hpvcd_status st = grow_pinned(&slot->h_in, &slot->h_in_cap, total);
+    if (st == HPVCD_OK) st = grow_device(&slot->d_in, &slot->d_in_cap, total);
+    if (st == HPVCD_OK) st = grow_pinned(&slot->h_out, &slot->h_out_cap, out_bytes);
+    if (st != HPVCD_OK) return st;
+    for (const Part& pt : parts) std::memcpy(slot->h_in + pt.off, pt.src, pt.bytes);
+    cudaError_t e = cudaMemcpyAsync(slot->d_in, slot->h_in, total, cudaMemcpyHostToDevice, slot->stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    slot->wp.assign(n, hpvcd_wp_table{});
+    bool any_wp = false;
+    for (uint32_t i = 0; i < n; ++i) {
+        hpvcd_picture& d = dev[i];
+        auto at = [&](int k) -> unsigned char* {
+            return offs[i * 9 + k] == (size_t)-1 ? nullptr : slot->d_in + offs[i * 9 + k];
+        };
+        d.tus = (const hpvcd_tu*)at(0);
+        d.ctu_tu_start = (const uint32_t*)at(1);
+        d.coeffs = (const int16_t*)at(2);
+        d.cells = (const hpvcd_cell*)at(3);
+        d.sao = (const hpvcd_sao_ctb*)at(4);
+        d.pus = (const hpvcd_pu*)at(5);
+        for (int c = 0; c < 3; ++c) d.pred[c] = at(6 + c);
+        if (pics[i].wp) {
+            slot->wp[i] = *pics[i].wp;
+            any_wp = true;
+        }
+        d.wp = pics[i].wp;  // only tested for NULL; the table itself is passed by value
+    }
+    if (reuse) {
+        st = plan_rebind(slot->plan, dev.data(), any_wp ? slot->wp.data() : nullptr, slot->stream);
+    } else {
+        if (slot->plan) {
+            cudaStreamSynchronize(slot->stream);
+            delete slot->plan;
+            slot->plan = nullptr;
+            slot->plan_bytes = 0;
+        }
+        st = plan_build(dev.data(), n, out, nullptr, any_wp ? slot->wp.data() : nullptr, &slot->plan);
+        slot->plan_bytes = st == HPVCD_OK ? plan_bytes : 0;
+    }
+    g->in_use = g->in_use - held + slot->d_in_cap + slot->plan_bytes;
+    slot->held = slot->d_in_cap + slot->plan_bytes;
+    if (st != HPVCD_OK) return st;
+    st = plan_launch(slot->plan, HPVCD_STAGE_ALL, slot->stream);
+    if (st != HPVCD_OK) return st;
+    // ---- output copy back ----
+    hpvcd_plan* P = slot->plan;
+    if (P->out.kind == HPVCD_OUT_RGB8) {
+        e = cudaMemcpyAsync(slot->h_out, P->d_canvas, P->canvas_bytes, cudaMemcpyDeviceToHost, slot->stream);
+    } else {
+        size_t o = 0;
+        for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) {
+            const Geo geo = geo_of(pics[i]);
+            for (int c = 0; c < (pics[i].chroma_idc ? 3 : 1) && e == cudaSuccess; ++c) {
+                const size_t b = c ? geo.chroma_bytes : geo.luma_bytes;
+                e = cudaMemcpyAsync(slot->h_out + o, P->pics[i].fin[c], b, cudaMemcpyDeviceToHost, slot->stream);
+                o += b;
+            }
+        }
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(slot->done, slot->stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    slot->busy = true;
+    slot->ticket = g->next_ticket++;
+    slot->out_bytes = out_bytes;
+    *ticket = slot->ticket;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_wait(hpvcd_gpu* g, hpvcd_ticket t, int32_t timeout_ms) {
+    if (!g) return HPVCD_ERR_INVALID_ARG;
+    cudaEvent_t ev;
+    {
+        std::lock_guard<std::mutex> lock(g->mu);
+        Slot* s = find_ticket(g, t);
+        if (!s) return HPVCD_ERR_INVALID_ARG;
+        ev = s->done;
+    }
+    cudaSetDevice(g->device);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return HPVCD_OK;
+        if (e != cudaErrorNotReady) return cuda_status(e);
+        if (timeout_ms >= 0 &&
+            std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(timeout_ms))
+            return HPVCD_ERR_BUSY;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_output_size(hpvcd_gpu* g, hpvcd_ticket t, uint64_t* bytes) {
+    if (!g || !bytes) return HPVCD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g->mu);
+    Slot* s = find_ticket(g, t);
+    if (!s) return HPVCD_ERR_INVALID_ARG;
+    *bytes = s->out_bytes;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_read(hpvcd_gpu* g, hpvcd_ticket t, void* dst, uint64_t bytes) {
+    if (!g || !dst) return HPVCD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g->mu);
+    Slot* s = find_ticket(g, t);
+    if (!s) return HPVCD_ERR_INVALID_ARG;
+    if (bytes < s->out_bytes) return HPVCD_ERR_INVALID_ARG;
+    cudaSetDevice(g->device);
+    cudaError_t e = cudaEventSynchronize(s->done);
+    hpvcd_status st = cuda_status(e);
+    if (st == HPVCD_OK) st = device_status(s->plan, s->stream);
+    if (st == HPVCD_OK) std::memcpy(dst, s->h_out, s->out_bytes);
+    s->busy = false;
+    s->ticket = 0;
+    return st;
+}

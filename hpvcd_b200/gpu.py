@@ -1,0 +1,232 @@
+"""Python host side of the B200 reconstruction back end.
+
+Two layers over the C ABI (include/hpvcd_gpu.h, libhpvcd_b200.so):
+
+* `GpuDecoder` -- the host-buffer drop-in that sits where the reference's
+  `decode_heic` grid path (lib.rs:1724 `decode_grid` -> lib.rs:1680
+  `fill_grid_bands` -> lib.rs:1610 `stitch_grid_band`) and `finish_with`
+  (decode.rs:1440) run: flat per-picture buffers in host memory go in, an RGB8
+  canvas or YUV planes come out.  Errors raise `HpvcdError`, the analogue of
+  the reference's `DecodeError`.
+* `DevicePlan` -- the same reconstruction over buffers already resident in
+  HBM (uploaded once through torch), launched on a CUDA stream; this is what
+  the kernel-level timing uses.
+
+There is no CPU fallback: when the CUDA library is missing these classes
+raise ImportError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .synth import geometry
+
+
+def _check(status: int, what: str) -> None:
+    abi.check(status, what)
+
+
+def _pic_array(pics):
+    return (abi.Picture * len(pics))(*pics)
+
+
+class GpuDecoder:
+    """Host-buffer API (hpvcd_gpu_*): submit / wait / read tickets."""
+
+    def __init__(self, device: int = 0, max_inflight: int = 4, hbm_budget: int = 0):
+        self._L = abi.lib()
+        cfg = abi.GpuCfg(device, max_inflight, hbm_budget)
+        h = C.c_void_p()
+        _check(self._L.hpvcd_gpu_create(C.byref(cfg), C.byref(h)), "hpvcd_gpu_create")
+        self._h = h
+
+    def submit(self, pics, output: abi.Output | None = None) -> int:
+        arr = _pic_array(pics)
+        t = C.c_uint64()
+        _check(self._L.hpvcd_gpu_submit(self._h, arr, len(pics),
+                                        C.byref(output) if output is not None else None, C.byref(t)),
+               "hpvcd_gpu_submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> bool:
+        s = self._L.hpvcd_gpu_wait(self._h, ticket, timeout_ms)
+        if s == abi.ERR_BUSY:
+            return False
+        _check(s, "hpvcd_gpu_wait")
+        return True
+
+    def output_size(self, ticket: int) -> int:
+        b = C.c_uint64()
+        _check(self._L.hpvcd_gpu_output_size(self._h, ticket, C.byref(b)), "hpvcd_gpu_output_size")
+        return b.value
+
+    def read(self, ticket: int, dst: np.ndarray | None = None) -> np.ndarray:
+        n = self.output_size(ticket)
+        if dst is None:
+            dst = np.empty(n, np.uint8)
+        assert dst.nbytes >= n and dst.flags["C_CONTIGUOUS"]
+        _check(self._L.hpvcd_gpu_read(self._h, ticket, dst.ctypes.data_as(C.c_void_p), dst.nbytes),
+               "hpvcd_gpu_read")
+        return dst
+
+    def decode_rgb8(self, pics, output: abi.Output, dst: np.ndarray | None = None) -> np.ndarray:
+        """Decode a grid of pictures onto an RGB8 canvas (decode_heic_rgb8)."""
+        t = self.submit(pics, output)
+        self.wait(t)
+        out = self.read(t, dst)
+        return out.reshape(output.canvas_h, output.canvas_w, 3)
+
+    def decode_yuv(self, pics):
+        """Decode pictures to their final planes (decode_heic_yuv); returns a
+        list of (Y, Cb, Cr) numpy arrays in native sample type."""
+        t = self.submit(pics, None)
+        self.wait(t)
+        raw = self.read(t)
+        return split_planes(pics, raw)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.hpvcd_gpu_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def split_planes(pics, raw: np.ndarray):
+    out = []
+    o = 0
+    for p in pics:
+        g = geometry(p)
+        dt = np.uint8 if g["bytes_per_sample"] == 1 else np.uint16
+        planes = []
+        for c in range(3 if p.chroma_idc else 1):
+            w, h = (g["w"], g["h"]) if c == 0 else (g["cw"], g["ch"])
+            nb = w * h * g["bytes_per_sample"]
+            planes.append(raw[o:o + nb].view(dt).reshape(h, w).copy())
+            o += nb
+        while len(planes) < 3:
+            planes.append(np.zeros((0, 0), dt))
+        out.append(tuple(planes))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Device-resident plans (torch provides the device memory and streams).
+# ---------------------------------------------------------------------------
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("DevicePlan needs a CUDA device")
+    return torch
+
+
+class DevicePlan:
+    """Upload the flat buffers of `pics` to HBM once and build a plan."""
+
+    def __init__(self, pics, output: abi.Output | None = None, sched: abi.Sched | None = None,
+                 device: int = 0):
+        torch = _torch()
+        self._L = abi.lib()
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        self._keep = []
+        self.host_pics = list(pics)
+        dev = []
+        self.input_bytes = 0
+        for p in pics:
+            g = geometry(p)
+            ctbs = g["ctb_cols"] * g["ctb_rows"]
+            d = abi.Picture()
+            C.pointer(d)[0] = p
+            d.tus = self._upload(p.tus, p.n_tus * 16)
+            d.ctu_tu_start = self._upload(p.ctu_tu_start, (ctbs + 1) * 4)
+            d.coeffs = self._upload(p.coeffs, p.n_coeffs * 2)
+            d.cells = self._upload(p.cells, g["gw"] * g["gh"] * 4)
+            d.sao = self._upload(p.sao, ctbs * 36)
+            d.pus = self._upload(p.pus, p.n_pus * 20)
+            d.wp = self._upload(p.wp, C.sizeof(abi.WpTable))
+            for c in range(3):
+                if p.pred[c]:
+                    nb = (g["w"] * g["h"] if c == 0 else g["cw"] * g["ch"]) * g["bytes_per_sample"]
+                    d.pred[c] = self._upload(p.pred[c], nb)
+            dev.append(d)
+        self.dev_pics = dev
+        arr = _pic_array(dev)
+        h = C.c_void_p()
+        _check(self._L.hpvcd_plan_create(arr, len(dev), C.byref(output) if output is not None else None,
+                                         C.byref(sched) if sched is not None else None, C.byref(h)),
+               "hpvcd_plan_create")
+        self._h = h
+        self.output = output
+        self.launches_per_run = self._L.hpvcd_plan_launches_per_run(h)
+
+    def _upload(self, host_ptr, nbytes: int):
+        if not host_ptr or nbytes == 0:
+            return None
+        torch = self.torch
+        src = np.ctypeslib.as_array((C.c_uint8 * nbytes).from_address(host_ptr))
+        t = torch.from_numpy(src.copy()).to(self.device)
+        self._keep.append(t)
+        self.input_bytes += nbytes
+        return t.data_ptr()
+
+    def launch(self, stages: int = abi.STAGE_ALL, stream=None) -> None:
+        s = stream if stream is not None else self.torch.cuda.current_stream(self.device)
+        _check(self._L.hpvcd_plan_launch(self._h, stages, C.c_void_p(s.cuda_stream)), "hpvcd_plan_launch")
+
+    def status(self, stream=None) -> int:
+        s = stream if stream is not None else self.torch.cuda.current_stream(self.device)
+        return self._L.hpvcd_plan_device_status(self._h, C.c_void_p(s.cuda_stream))
+
+    def canvas(self) -> np.ndarray:
+        ptr, nb = C.c_void_p(), C.c_uint64()
+        _check(self._L.hpvcd_plan_canvas(self._h, C.byref(ptr), C.byref(nb)), "hpvcd_plan_canvas")
+        out = np.empty(nb.value, np.uint8)
+        _check(self._L.hpvcd_copy(out.ctypes.data_as(C.c_void_p), ptr, nb.value, None), "hpvcd_copy")
+        return out.reshape(self.output.canvas_h, self.output.canvas_w, 3)
+
+    def canvas_ptr(self) -> tuple[int, int]:
+        ptr, nb = C.c_void_p(), C.c_uint64()
+        _check(self._L.hpvcd_plan_canvas(self._h, C.byref(ptr), C.byref(nb)), "hpvcd_plan_canvas")
+        return ptr.value, nb.value
+
+    def planes(self, i: int):
+        p = self.host_pics[i]
+        g = geometry(p)
+        ptrs = [C.c_void_p() for _ in range(3)]
+        _check(self._L.hpvcd_plan_planes(self._h, i, *(C.byref(x) for x in ptrs)), "hpvcd_plan_planes")
+        dt = np.uint8 if g["bytes_per_sample"] == 1 else np.uint16
+        res = []
+        for c in range(3):
+            w, h = (g["w"], g["h"]) if c == 0 else (g["cw"], g["ch"])
+            a = np.zeros((h, w), dt)
+            if ptrs[c].value and a.size:
+                _check(self._L.hpvcd_copy(a.ctypes.data_as(C.c_void_p), ptrs[c], a.nbytes, None), "hpvcd_copy")
+            res.append(a)
+        return tuple(res)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.hpvcd_plan_destroy(self._h)
+            self._h = None
+        self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -302,6 +302,16 @@ hpvcd_status hpvcd_plan_device_status(hpvcd_plan* plan, void* stream);
 /* Number of kernel launches one hpvcd_plan_launch(HPVCD_STAGE_ALL) issues. */
 uint32_t hpvcd_plan_launches_per_run(const hpvcd_plan* plan);
 
+/* ------------------------------------------------------------------------ */
+/* Utilities (no reference counterpart).                                    */
+/* ------------------------------------------------------------------------ */
+/* Copy `bytes` between host and/or device pointers on `stream` and wait for
+ * it (the direction is inferred from the pointers). */
+hpvcd_status hpvcd_copy(void* dst, const void* src, uint64_t bytes, void* stream);
+/* sizeof() of an ABI struct by name ("hpvcd_tu", ...), 0 if unknown; lets a
+ * binding check its layout against this library. */
+uint64_t hpvcd_abi_sizeof(const char* name);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,238 @@
+"""Bit-exact parity of the CUDA reconstruction path against the CPU oracle.
+
+Every test calls through the C ABI (libhpvcd_b200.so) with seeded synthetic
+flat buffers and compares plane for plane (and the RGB8 canvas) with the
+oracle restatement of the reference's scalar decode.  Integer work: the
+tolerance is zero.
+"""
+import numpy as np
+import pytest
+
+from hpvcd_b200 import abi, synth
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():  # pragma: no cover
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+from hpvcd_b200.gpu import DevicePlan, GpuDecoder  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def dec():
+    d = GpuDecoder(0)
+    yield d
+    d.close()
+
+
+def assert_planes_equal(gpu_planes, ref_planes, what=""):
+    for i, (g, r) in enumerate(zip(gpu_planes, ref_planes)):
+        for c in range(3):
+            gc = g[c].astype(np.uint16)
+            rc = r[c]
+            if rc.size == 0:
+                continue
+            if not np.array_equal(gc, rc):
+                diff = np.argwhere(gc != rc)
+                y, x = diff[0]
+                raise AssertionError(
+                    f"{what} picture {i} comp {c}: {len(diff)} samples differ, first at (x={x}, y={y}) "
+                    f"gpu={gc[y, x]} oracle={rc[y, x]}")
+
+
+def run_yuv(dec, pics, what):
+    gpu = dec.decode_yuv(pics)
+    ref, _ = O.decode_batch(pics)
+    assert_planes_equal(gpu, ref, what)
+
+
+# --- residual-only reconstruction (512x512 8-bit, seeded prediction) -------
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_residual_picture(dec, seed):
+    s = synth.SynthSet()
+    s.add(synth.residual_cfg(seed))
+    run_yuv(dec, s.pictures(), "residual")
+
+
+def test_residual_picture_10bit_444(dec):
+    s = synth.SynthSet()
+    s.add(synth.residual_cfg(5, 256, 192, bit_depth=10, chroma_idc=3))
+    run_yuv(dec, s.pictures(), "residual 10-bit 4:4:4")
+
+
+# --- intra pictures: prediction + residual + deblock + SAO -----------------
+@pytest.mark.parametrize("bd,idc", [(8, 1), (10, 1), (8, 3), (10, 3), (8, 0)])
+def test_intra_tile(dec, bd, idc):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(10 + bd + idc, 512, 512, bit_depth=bd, chroma_idc=idc))
+    run_yuv(dec, s.pictures(), f"intra bd={bd} idc={idc}")
+
+
+def test_intra_recon_only(dec):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(21, 256, 256, bit_depth=10, sao=False, deblock=False))
+    run_yuv(dec, s.pictures(), "intra recon only")
+
+
+def test_intra_tskip_tqb_exempt(dec):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(22, 256, 256, bit_depth=8, tskip_p=0.5, tqb_p=0.2))
+    s.add(synth.intra_cfg(23, 256, 256, bit_depth=10, tskip_p=0.5, tqb_p=0.2))
+    run_yuv(dec, s.pictures(), "tskip/tqb")
+
+
+@pytest.mark.parametrize("w,h,log2_ctb", [(200, 136, 6), (96, 64, 4), (328, 168, 5), (8, 8, 6), (1080 // 4 * 4, 72, 6)])
+def test_intra_odd_sizes_and_ctb(dec, w, h, log2_ctb):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(30 + w, w, h, bit_depth=10)
+    c.log2_ctb = log2_ctb
+    s.add(c)
+    run_yuv(dec, s.pictures(), f"intra {w}x{h} ctb {1 << log2_ctb}")
+
+
+def test_intra_qp_offsets_and_deblock_offsets(dec):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(40, 256, 256, bit_depth=10)
+    c.cb_qp_offset, c.cr_qp_offset = -5, 7
+    c.beta_offset_div2, c.tc_offset_div2 = 3, -2
+    c.qp_min, c.qp_max = 0, 51
+    s.add(c)
+    c2 = synth.intra_cfg(41, 128, 128, bit_depth=10)
+    c2.qp_min, c2.qp_max = -12, 51  # negative QpY allowed at 10-bit
+    s.add(c2)
+    run_yuv(dec, s.pictures(), "qp offsets")
+
+
+def test_intra_no_strong_smoothing_and_smoothing_disabled(dec):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(42, 256, 256)
+    c.pic_flags &= ~abi.PIC_STRONG_SMOOTHING
+    s.add(c)
+    c = synth.intra_cfg(43, 256, 256)
+    c.pic_flags |= abi.PIC_SMOOTHING_DISABLED
+    s.add(c)
+    run_yuv(dec, s.pictures(), "smoothing flags")
+
+
+def test_batch_of_mixed_pictures(dec):
+    s = synth.SynthSet()
+    for i, (w, h, bd, idc) in enumerate([(512, 512, 8, 1), (256, 384, 10, 3), (192, 128, 8, 3),
+                                         (512, 320, 10, 1), (64, 64, 8, 1)]):
+        s.add(synth.intra_cfg(50 + i, w, h, bit_depth=bd, chroma_idc=idc))
+    run_yuv(dec, s.pictures(), "mixed batch")
+
+
+# --- RGB8 canvas of a grid (decode_heic_rgb8 path) --------------------------
+@pytest.mark.parametrize("matrix,full", [(abi.MATRIX_SMPTE170M, True), (abi.MATRIX_BT709, False),
+                                         (abi.MATRIX_BT2020NCL, True), (abi.MATRIX_IDENTITY, True),
+                                         (abi.MATRIX_YCGCO, True)])
+def test_grid_rgb8(dec, matrix, full):
+    g = synth.make_grid(1000, 700, seed=3, bit_depth=10, chroma_idc=1)
+    out, keep = synth.grid_output(g, matrix=matrix, full_range=full)
+    pics = g.synth.pictures()
+    rgb = dec.decode_rgb8(pics, out)
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    assert np.array_equal(rgb, ref)
+
+
+def test_full_4032x3024_grid_rgb8(dec):
+    g = synth.config1_grid(seed=7)
+    out, keep = synth.grid_output(g)
+    pics = g.synth.pictures()
+    rgb = dec.decode_rgb8(pics, out)
+    _, ref = O.decode_batch(pics, out, want_planes=False, threads=8)
+    assert rgb.shape == (3024, 4032, 3)
+    assert np.array_equal(rgb, ref)
+
+
+def test_grid_8bit_444_and_mono(dec):
+    for bd, idc in ((8, 3), (8, 0), (12, 1)):
+        g = synth.make_grid(700, 600, seed=9 + idc, bit_depth=bd, chroma_idc=idc)
+        out, keep = synth.grid_output(g)
+        pics = g.synth.pictures()
+        rgb = dec.decode_rgb8(pics, out)
+        _, ref = O.decode_batch(pics, out, want_planes=False)
+        assert np.array_equal(rgb, ref), (bd, idc)
+
+
+# --- inter: motion compensation with bi / weighted prediction --------------
+@pytest.mark.parametrize("weighted", [False, True])
+def test_inter_sequence(dec, weighted):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(60, 320, 192, bit_depth=8))
+    for i in range(1, 5):
+        s.add(synth.inter_cfg(60 + i, 320, 192, weighted=weighted))
+    run_yuv(dec, s.pictures(), f"inter weighted={weighted}")
+
+
+def test_inter_10bit(dec):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(70, 256, 136, bit_depth=10))
+    for i in range(1, 4):
+        s.add(synth.inter_cfg(70 + i, 256, 136, bit_depth=10, weighted=(i == 2)))
+    run_yuv(dec, s.pictures(), "inter 10-bit")
+
+
+# --- device plans: repeated launches give identical output ----------------
+def test_device_plan_repeat_and_status():
+    g = synth.make_grid(1024, 512, seed=11, bit_depth=10)
+    out, keep = synth.grid_output(g)
+    pics = g.synth.pictures()
+    plan = DevicePlan(pics, out)
+    plan.launch()
+    a = plan.canvas()
+    plan.launch()
+    plan.launch()
+    b = plan.canvas()
+    assert plan.status() == abi.OK
+    assert np.array_equal(a, b)
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    assert np.array_equal(a, ref)
+    plan.close()
+
+
+def test_ticket_reuse_same_layout(dec):
+    # Same layout, different content: the cached plan is rebound.
+    outs = []
+    for seed in (1, 2):
+        g = synth.make_grid(600, 600, seed=seed, bit_depth=8)
+        out, keep = synth.grid_output(g)
+        pics = g.synth.pictures()
+        rgb = dec.decode_rgb8(pics, out)
+        _, ref = O.decode_batch(pics, out, want_planes=False)
+        assert np.array_equal(rgb, ref)
+        outs.append(rgb)
+    assert not np.array_equal(outs[0], outs[1])
+
+
+def test_errors_map_to_status(dec):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(80, 64, 64))
+    bad = s.picture(0)
+    bad.chroma_idc = 2
+    with pytest.raises(abi.HpvcdError) as e:
+        dec.submit([bad])
+    assert e.value.status == abi.ERR_UNSUPPORTED
+    p2 = s.picture(0)
+    p2.width = 0
+    with pytest.raises(abi.HpvcdError) as e:
+        dec.submit([p2])
+    assert e.value.status == abi.ERR_LIMIT
+
+
+def test_malformed_tb_is_reported(dec):
+    # A TB record pointing outside its CTU must not be reconstructed; the
+    # device reports a Bitstream error instead of writing out of bounds.
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(81, 128, 128))
+    p = s.picture(0)
+    tus = synth.tus_of(p)
+    coded = np.nonzero(tus["flags"] & abi.TU_CBF)[0]
+    tus[coded[0]]["x"] = 4000  # far outside
+    t = dec.submit([p])
+    dec.wait(t)
+    with pytest.raises(abi.HpvcdError) as e:
+        dec.read(t)
+    assert e.value.status == abi.ERR_BITSTREAM
