@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 HEVC reconstruction back end.
+
+Workload (one step): full decode of a 4032x3024 10-bit 4:2:0 HEIC still
+stored as an 8x6 grid of 512x512 tiles (edge tiles cropped) from the flat
+per-tile buffers the host syntax decode produces, to a packed RGB8 canvas
+(BT.601 full range, `decode_heic_rgb8`): intra prediction + dequant +
+inverse DCT/DST + add, deblocking, SAO, YCbCr->RGB and stitching.  Inputs are
+seeded synthetic buffers with the benchmark's distributions (there is no
+public corpus for this path).
+
+Metric: decoded megapixels (output luma pixels) per second, higher is better.
+  value  -- device time of the reconstruction with inputs resident in HBM,
+            L2 flushed between steps, CUDA events on the launching stream.
+  e2e    -- the same decode through the C-ABI host-buffer entry points
+            (hpvcd_gpu_submit / wait / read) with the inputs in page-locked
+            host memory and the RGB8 canvas copied back every step.
+`--impl reference` times the CPU reference path (the oracle restatement of
+the reference decoder, all host threads) on the same workload.
+
+One process per GPU (torchrun for N > 1); every rank decodes its own image
+(replicas, weak scaling); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "heic_grid_4032x3024_10bit_420_48x512_tiles_to_rgb8"
+OUT_W, OUT_H = 4032, 3024
+MPIX = OUT_W * OUT_H / 1e6
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM traffic of the dominant kernel from the committed ncu
+    summary (profiles/recon_traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "recon_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(device_index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(rows), "reasons": reasons}
+
+
+def cpu_baseline(pics, out, threads: int, min_seconds: float = 2.0) -> dict:
+    """The oracle (C++ restatement of the reference CPU path) on the host
+    cores: repeated full decodes of the workload for ~min_seconds."""
+    from oracle import oracle as O
+    O.decode_batch(pics, out, want_planes=False, threads=threads)  # warm
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.decode_batch(pics, out, want_planes=False, threads=threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= min_seconds and reps >= 2:
+            break
+    return {"value": round(MPIX * reps / el, 2), "unit": "MPix/s", "cores": threads, "kind": "port",
+            "sample": f"{reps} full {OUT_W}x{OUT_H} decodes (48 tiles, recon+deblock+SAO+RGB8) "
+                      f"in {el:.2f} s, {threads} threads"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return 0
+    from hpvcd_b200 import synth
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    g = synth.config1_grid(seed=0)
+    out, keep = synth.grid_output(g)
+    pics = g.synth.pictures()
+    for _ in range(max(args.warmup, 1)):
+        O.decode_batch(pics, out, want_planes=False, threads=threads)
+    steps = max(1, min(args.steps, 20))
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.decode_batch(pics, out, want_planes=False, threads=threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = MPIX * steps / total
+    times_ms = sorted(t * 1e3 for t in times)
+    line = {
+        "impl": "reference", "metric": "decoded MPix/s", "value": round(value, 2), "unit": "MPix/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": round(total / steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "tiles": 48, "out": f"{OUT_W}x{OUT_H} RGB8",
+                   "implementation": "C++ restatement of the hpvcd CPU reconstruction path "
+                                     "(Rust toolchain absent; scalar kernels, one tile per thread)"},
+        "latency_ms": {"p50": round(times_ms[len(times_ms) // 2], 3),
+                       "p99": round(times_ms[min(len(times_ms) - 1, int(0.99 * len(times_ms)))], 3)},
+        "cpu_baseline": {"value": round(value, 2), "unit": "MPix/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full decodes of the workload, {threads} threads"},
+        "e2e": {"value": round(value, 2), "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from hpvcd_b200 import abi, synth
+    from hpvcd_b200.gpu import DevicePlan, GpuDecoder, pack_pinned, pinned_empty
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=dev)
+    L = abi.lib()
+
+    g = synth.config1_grid(seed=rank)
+    out, keep = synth.grid_output(g)
+    pics = g.synth.pictures()
+    plan = DevicePlan(pics, out, device=local)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    stages = [abi.STAGE_RECON, abi.STAGE_DEBLOCK, abi.STAGE_SAO, abi.STAGE_OUTPUT]
+    for _ in range(args.warmup):
+        flush.zero_()
+        plan.launch(abi.STAGE_ALL, stream)
+    torch.cuda.synchronize(dev)
+    st = plan.status(stream)
+    if st != abi.OK:
+        raise abi.HpvcdError(st, "device status after warm-up")
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(stages) + 1)] for _ in range(K)]
+    launches0 = L.hpvcd_kernel_launch_count()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(local)
+    for k in range(K):
+        flush.zero_()
+        ev[k][0].record(stream)
+        for i, s in enumerate(stages):
+            plan.launch(s, stream)
+            ev[k][i + 1].record(stream)
+    torch.cuda.synchronize(dev)
+    clock_rec = clocks.stop()
+    if world > 1:
+        torch.distributed.barrier()
+    launches = L.hpvcd_kernel_launch_count() - launches0
+    st = plan.status(stream)
+    if st != abi.OK:
+        raise abi.HpvcdError(st, "device status after timed region")
+
+    step_ms = [ev[k][0].elapsed_time(ev[k][-1]) for k in range(K)]
+    stage_ms = [sum(ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(K)) / K for i in range(len(stages))]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * MPIX * K / (total_ms / 1e3)
+    lat = sorted(step_ms)
+
+    # Roofline of the dominant kernel (the reconstruction kernel): algorithmic
+    # bytes per launch = dense int16 levels of the coded TBs + TB records +
+    # CTU index + the reconstructed samples written once.
+    n_coeffs = sum(p.n_coeffs for p in pics)
+    n_tus = sum(p.n_tus for p in pics)
+    ctus = sum(synth.geometry(p)["ctb_cols"] * synth.geometry(p)["ctb_rows"] + 1 for p in pics)
+    written = sum(p.width * p.height * 3 // 2 * synth.geometry(p)["bytes_per_sample"] for p in pics)
+    recon_bytes = n_coeffs * 2 + n_tus * 16 + ctus * 4 + written
+    peak, peak_kind = measured_peaks()
+    recon_s = stage_ms[0] / 1e3
+    achieved = recon_bytes / recon_s / 1e9
+    traffic = profile_traffic()
+    roofline = {"kernel": "k_recon", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": recon_bytes,
+                "traffic": traffic.get("dram_bytes_per_launch") if traffic else None}
+    # whole-pipeline bytes (reconstruction + filters + RGB), for context
+    pipe_bytes = recon_bytes + 2 * written * 2 + written + OUT_W * OUT_H * 3
+
+    # ---- end to end through the C ABI (host buffers) ----
+    e2e = None
+    K2 = args.e2e_steps if args.e2e_steps is not None else max(5, min(K, 50))
+    packed, pkeep = pack_pinned(pics)
+    h2d = pkeep[2]
+    canvas_bytes = OUT_W * OUT_H * 3
+    dst, dkeep = pinned_empty(canvas_bytes)
+    out2, keep2 = synth.grid_output(g)
+    out2.host_dst = dst.ctypes.data
+    out2.host_dst_bytes = canvas_bytes
+    with GpuDecoder(local, max_inflight=2) as decd:
+        for _ in range(max(3, args.warmup // 2)):
+            t = decd.submit(packed, out2)
+            decd.wait(t)
+            decd.read(t, dst)
+        if world > 1:
+            torch.distributed.barrier()
+        times = []
+        for _ in range(K2):
+            t0 = time.perf_counter()
+            t = decd.submit(packed, out2)
+            decd.wait(t)
+            decd.read(t, dst)
+            times.append(time.perf_counter() - t0)
+        e2e_total = sum(times)
+        if world > 1:
+            tt = torch.tensor([e2e_total], device=dev)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            e2e_total = float(tt.item())
+        e2e = {"value": round(world * MPIX * K2 / e2e_total, 2), "unit": "MPix/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": canvas_bytes,
+               "steps": K2, "ms_per_step": round(e2e_total / K2 * 1e3, 3),
+               "api": "hpvcd_gpu_submit/wait/read, pinned packed inputs, pinned RGB8 output"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(pics, out, os.cpu_count() or 1)
+
+    line = {
+        "metric": "decoded MPix/s", "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
+        "steps": K, "warmup": args.warmup, "ms_per_step": round(total_ms / K, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "tiles": 48, "tile": "512x512 (edge tiles cropped)",
+                   "out": f"{OUT_W}x{OUT_H} RGB8 BT.601 full range", "bit_depth": 10, "chroma": "4:2:0",
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                   "inputs": "seeded synthetic flat buffers (CU/TU quadtrees, modes, QP 22-37, "
+                             "85% zero levels, Laplacian(8), deblock on, random SAO)"},
+        "latency_ms": {"p50": round(lat[len(lat) // 2], 4),
+                       "p99": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 4)},
+        "stages_ms": {"recon": round(stage_ms[0], 4), "deblock": round(stage_ms[1], 4),
+                      "sao": round(stage_ms[2], 4), "rgb": round(stage_ms[3], 4)},
+        "pipeline_gbs": round(pipe_bytes / (total_ms / K / 1e3) / 1e9, 1),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "launches_per_step": int(launches // K),
+        "clocks": clock_rec,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

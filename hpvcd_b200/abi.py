@@ -147,7 +147,8 @@ class TilePlace(C.Structure):
 
 class Output(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("matrix", C.c_uint32), ("full_range", C.c_uint32),
-                ("canvas_w", C.c_uint32), ("canvas_h", C.c_uint32), ("place", C.c_void_p)]
+                ("canvas_w", C.c_uint32), ("canvas_h", C.c_uint32), ("place", C.c_void_p),
+                ("host_dst", C.c_void_p), ("host_dst_bytes", C.c_uint64)]
 
 
 class GpuCfg(C.Structure):
@@ -212,6 +213,8 @@ def lib() -> C.CDLL:
             "hpvcd_plan_launches_per_run": (u32, [vp]),
             "hpvcd_abi_sizeof": (u64, [C.c_char_p]),
             "hpvcd_copy": (i32, [vp, vp, u64, vp]),
+            "hpvcd_gpu_packed_size": (u64, [C.POINTER(Picture), u32]),
+            "hpvcd_gpu_pack_inputs": (i32, [C.POINTER(Picture), u32, vp, u64, C.POINTER(Picture)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

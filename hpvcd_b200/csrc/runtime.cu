@@ -325,8 +325,13 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
 }
 
 hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(P->d_scratch, 0, P->scratch_words * sizeof(uint32_t), st);
-    if (e != cudaSuccess) return cuda_status(e);
+    cudaError_t e = cudaSuccess;
+    // Work counters, the device error word and the wavefront ready flags are
+    // reset by every launch that reconstructs.
+    if (stages & HPVCD_STAGE_RECON) {
+        e = cudaMemsetAsync(P->d_scratch, 0, P->scratch_words * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
     const uint32_t n_seg = (uint32_t)P->segs.size();
     uint32_t* d_err = P->d_scratch + n_seg;
     if (stages & HPVCD_STAGE_RECON) {
@@ -437,6 +442,7 @@ struct Slot {
     uint64_t out_bytes = 0;
     uint64_t plan_bytes = 0;  // device bytes of `plan`
     uint64_t held = 0;        // device bytes this slot holds (arena + plan)
+    void* direct_out = nullptr;  // caller's pinned output buffer of the ticket, if any
     bool busy = false;
     std::vector<hpvcd_wp_table> wp;
 };
@@ -508,6 +514,62 @@ hpvcd_status device_status(hpvcd_plan* P, cudaStream_t st) {
     if (err & hpvcd::DEV_ERR_TIMEOUT) return HPVCD_ERR_TIMEOUT;
     if (err & hpvcd::DEV_ERR_BITSTREAM) return HPVCD_ERR_BITSTREAM;
     return HPVCD_OK;
+}
+
+// Layout of the inputs of a batch in one arena (256-byte aligned parts in a
+// fixed order per picture: tus, ctu starts, coefficients, cells, SAO, PUs,
+// prediction planes).  Shared by hpvcd_gpu_pack_inputs and submit.
+struct InputPart {
+    const void* src;
+    size_t bytes;
+    size_t off;
+    uint32_t pic;
+    int kind;  // 0..8 as above (6..8 = prediction planes Y/Cb/Cr)
+};
+
+size_t input_layout(const hpvcd_picture* pics, uint32_t n, std::vector<InputPart>* parts) {
+    size_t total = 0;
+    auto add = [&](uint32_t i, int kind, const void* src, size_t bytes) {
+        if (!src || !bytes) return;
+        parts->push_back(InputPart{src, bytes, total, i, kind});
+        total = align_up(total + bytes, 256);
+    };
+    for (uint32_t i = 0; i < n; ++i) {
+        const hpvcd_picture& p = pics[i];
+        const Geo geo = geo_of(p);
+        const size_t ctbs = (size_t)geo.ctb_cols * geo.ctb_rows;
+        add(i, 0, p.tus, (size_t)p.n_tus * sizeof(hpvcd_tu));
+        add(i, 1, p.ctu_tu_start, (ctbs + 1) * sizeof(uint32_t));
+        add(i, 2, p.coeffs, (size_t)p.n_coeffs * sizeof(int16_t));
+        add(i, 3, p.cells, (size_t)geo.gw * geo.gh * sizeof(hpvcd_cell));
+        add(i, 4, p.sao, ctbs * sizeof(hpvcd_sao_ctb));
+        add(i, 5, p.pus, (size_t)p.n_pus * sizeof(hpvcd_pu));
+        if (p.flags & HPVCD_PIC_PRED_IN_PLANE)
+            for (int c = 0; c < (p.chroma_idc ? 3 : 1); ++c)
+                add(i, 6 + c, p.pred[c], c ? geo.chroma_bytes : geo.luma_bytes);
+    }
+    return total;
+}
+
+void point_at(hpvcd_picture& d, int kind, const void* ptr) {
+    switch (kind) {
+        case 0: d.tus = (const hpvcd_tu*)ptr; break;
+        case 1: d.ctu_tu_start = (const uint32_t*)ptr; break;
+        case 2: d.coeffs = (const int16_t*)ptr; break;
+        case 3: d.cells = (const hpvcd_cell*)ptr; break;
+        case 4: d.sao = (const hpvcd_sao_ctb*)ptr; break;
+        case 5: d.pus = (const hpvcd_pu*)ptr; break;
+        default: d.pred[kind - 6] = ptr; break;
+    }
+}
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
 }
 
 }  // namespace
@@ -671,34 +733,24 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         }
     if (!slot) return HPVCD_ERR_BUSY;
     // ---- input layout in one arena ----
-    struct Part {
-        const void* src;
-        size_t bytes;
-        size_t off;
-    };
-    std::vector<Part> parts;
-    size_t total = 0;
-    auto add = [&](const void* src, size_t bytes) -> size_t {
-        const size_t off = total;
-        parts.push_back(Part{src, bytes, off});
-        total = align_up(total + bytes, 256);
-        return off;
-    };
+    std::vector<InputPart> parts;
+    const size_t total = input_layout(pics, n, &parts);
     std::vector<hpvcd_picture> dev(pics, pics + n);
-    std::vector<size_t> offs(n * 9, (size_t)-1);
-    for (uint32_t i = 0; i < n; ++i) {
-        const hpvcd_picture& p = pics[i];
-        const Geo geo = geo_of(p);
-        const size_t ctbs = (size_t)geo.ctb_cols * geo.ctb_rows;
-        if (p.n_tus) offs[i * 9 + 0] = add(p.tus, p.n_tus * sizeof(hpvcd_tu));
-        offs[i * 9 + 1] = add(p.ctu_tu_start, (ctbs + 1) * sizeof(uint32_t));
-        if (p.n_coeffs) offs[i * 9 + 2] = add(p.coeffs, p.n_coeffs * sizeof(int16_t));
-        if (p.cells) offs[i * 9 + 3] = add(p.cells, (size_t)geo.gw * geo.gh * sizeof(hpvcd_cell));
-        if (p.sao) offs[i * 9 + 4] = add(p.sao, ctbs * sizeof(hpvcd_sao_ctb));
-        if (p.n_pus) offs[i * 9 + 5] = add(p.pus, p.n_pus * sizeof(hpvcd_pu));
-        if (p.flags & HPVCD_PIC_PRED_IN_PLANE)
-            for (int c = 0; c < (p.chroma_idc ? 3 : 1); ++c)
-                if (p.pred[c]) offs[i * 9 + 6 + c] = add(p.pred[c], c ? geo.chroma_bytes : geo.luma_bytes);
+    for (hpvcd_picture& d : dev) {
+        d.tus = nullptr; d.ctu_tu_start = nullptr; d.coeffs = nullptr; d.cells = nullptr;
+        d.sao = nullptr; d.pus = nullptr; d.pred[0] = d.pred[1] = d.pred[2] = nullptr;
+    }
+    // A packed batch in page-locked memory goes up in one DMA.
+    const unsigned char* packed_base = nullptr;
+    if (!parts.empty()) {
+        const unsigned char* base = (const unsigned char*)parts[0].src - parts[0].off;
+        bool packed = true;
+        for (const InputPart& pt : parts)
+            if ((const unsigned char*)pt.src - pt.off != base) {
+                packed = false;
+                break;
+            }
+        if (packed && is_pinned(base)) packed_base = base;
     }
     // ---- HBM admission ----
     const size_t out_bytes = [&]() -> size_t {
@@ -718,32 +770,28 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     const uint64_t plan_bytes = reuse ? slot->plan_bytes : plan_footprint(pics, n, out);
     const uint64_t need = std::max<uint64_t>(slot->d_in_cap, align_up(total + total / 4, 1 << 20)) + plan_bytes;
     if (g->in_use - held + need > g->budget) return HPVCD_ERR_ALLOC;
-    hpvcd_status st = grow_pinned(&slot->h_in, &slot->h_in_cap, total);
-    if (st == HPVCD_OK) st = grow_device(&slot->d_in, &slot->d_in_cap, total);
-    if (st == HPVCD_OK) st = grow_pinned(&slot->h_out, &slot->h_out_cap, out_bytes);
+    const bool direct_out = out && out->host_dst && out->host_dst_bytes >= out_bytes && is_pinned(out->host_dst);
+    hpvcd_status st = packed_base ? HPVCD_OK : grow_pinned(&slot->h_in, &slot->h_in_cap, total);
+    if (st == HPVCD_OK) st = grow_device(&slot->d_in, &slot->d_in_cap, std::max<size_t>(total, 256));
+    if (st == HPVCD_OK && !direct_out) st = grow_pinned(&slot->h_out, &slot->h_out_cap, out_bytes);
     if (st != HPVCD_OK) return st;
-    for (const Part& pt : parts) std::memcpy(slot->h_in + pt.off, pt.src, pt.bytes);
-    cudaError_t e = cudaMemcpyAsync(slot->d_in, slot->h_in, total, cudaMemcpyHostToDevice, slot->stream);
+    cudaError_t e;
+    if (packed_base) {
+        e = cudaMemcpyAsync(slot->d_in, packed_base, total, cudaMemcpyHostToDevice, slot->stream);
+    } else {
+        for (const InputPart& pt : parts) std::memcpy(slot->h_in + pt.off, pt.src, pt.bytes);
+        e = cudaMemcpyAsync(slot->d_in, slot->h_in, total, cudaMemcpyHostToDevice, slot->stream);
+    }
     if (e != cudaSuccess) return cuda_status(e);
+    for (const InputPart& pt : parts) point_at(dev[pt.pic], pt.kind, slot->d_in + pt.off);
     slot->wp.assign(n, hpvcd_wp_table{});
     bool any_wp = false;
     for (uint32_t i = 0; i < n; ++i) {
-        hpvcd_picture& d = dev[i];
-        auto at = [&](int k) -> unsigned char* {
-            return offs[i * 9 + k] == (size_t)-1 ? nullptr : slot->d_in + offs[i * 9 + k];
-        };
-        d.tus = (const hpvcd_tu*)at(0);
-        d.ctu_tu_start = (const uint32_t*)at(1);
-        d.coeffs = (const int16_t*)at(2);
-        d.cells = (const hpvcd_cell*)at(3);
-        d.sao = (const hpvcd_sao_ctb*)at(4);
-        d.pus = (const hpvcd_pu*)at(5);
-        for (int c = 0; c < 3; ++c) d.pred[c] = at(6 + c);
         if (pics[i].wp) {
             slot->wp[i] = *pics[i].wp;
             any_wp = true;
         }
-        d.wp = pics[i].wp;  // only tested for NULL; the table itself is passed by value
+        dev[i].wp = pics[i].wp;  // only tested for NULL; the table itself is passed by value
     }
     if (reuse) {
         st = plan_rebind(slot->plan, dev.data(), any_wp ? slot->wp.data() : nullptr, slot->stream);
@@ -764,15 +812,17 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     if (st != HPVCD_OK) return st;
     // ---- output copy back ----
     hpvcd_plan* P = slot->plan;
+    unsigned char* host_out = direct_out ? (unsigned char*)out->host_dst : slot->h_out;
+    slot->direct_out = direct_out ? out->host_dst : nullptr;
     if (P->out.kind == HPVCD_OUT_RGB8) {
-        e = cudaMemcpyAsync(slot->h_out, P->d_canvas, P->canvas_bytes, cudaMemcpyDeviceToHost, slot->stream);
+        e = cudaMemcpyAsync(host_out, P->d_canvas, P->canvas_bytes, cudaMemcpyDeviceToHost, slot->stream);
     } else {
         size_t o = 0;
         for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) {
             const Geo geo = geo_of(pics[i]);
             for (int c = 0; c < (pics[i].chroma_idc ? 3 : 1) && e == cudaSuccess; ++c) {
                 const size_t b = c ? geo.chroma_bytes : geo.luma_bytes;
-                e = cudaMemcpyAsync(slot->h_out + o, P->pics[i].fin[c], b, cudaMemcpyDeviceToHost, slot->stream);
+                e = cudaMemcpyAsync(host_out + o, P->pics[i].fin[c], b, cudaMemcpyDeviceToHost, slot->stream);
                 o += b;
             }
         }
@@ -783,6 +833,27 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     slot->ticket = g->next_ticket++;
     slot->out_bytes = out_bytes;
     *ticket = slot->ticket;
+    return HPVCD_OK;
+}
+
+HPVCD_API uint64_t hpvcd_gpu_packed_size(const hpvcd_picture* pics, uint32_t n) {
+    if (!pics) return 0;
+    std::vector<InputPart> parts;
+    return input_layout(pics, n, &parts);
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_pack_inputs(const hpvcd_picture* pics, uint32_t n, void* dst, uint64_t bytes,
+                                             hpvcd_picture* out_pics) {
+    if (!pics || !dst || !out_pics) return HPVCD_ERR_INVALID_ARG;
+    std::vector<InputPart> parts;
+    const size_t total = input_layout(pics, n, &parts);
+    if (bytes < total) return HPVCD_ERR_INVALID_ARG;
+    std::vector<hpvcd_picture> res(pics, pics + n);
+    for (const InputPart& pt : parts) {
+        std::memcpy((unsigned char*)dst + pt.off, pt.src, pt.bytes);
+        point_at(res[pt.pic], pt.kind, (unsigned char*)dst + pt.off);
+    }
+    std::memcpy(out_pics, res.data(), sizeof(hpvcd_picture) * n);
     return HPVCD_OK;
 }
 
@@ -827,7 +898,8 @@ HPVCD_API hpvcd_status hpvcd_gpu_read(hpvcd_gpu* g, hpvcd_ticket t, void* dst, u
     cudaError_t e = cudaEventSynchronize(s->done);
     hpvcd_status st = cuda_status(e);
     if (st == HPVCD_OK) st = device_status(s->plan, s->stream);
-    if (st == HPVCD_OK) std::memcpy(dst, s->h_out, s->out_bytes);
+    if (st == HPVCD_OK && dst != s->direct_out)
+        std::memcpy(dst, s->direct_out ? (const unsigned char*)s->direct_out : s->h_out, s->out_bytes);
     s->busy = false;
     s->ticket = 0;
     return st;

@@ -105,6 +105,28 @@ class GpuDecoder:
             pass
 
 
+def pinned_empty(nbytes: int):
+    """Page-locked host buffer (torch provides the allocation); returns
+    (numpy view, keepalive)."""
+    import torch
+    t = torch.empty(max(int(nbytes), 1), dtype=torch.uint8, pin_memory=True)
+    return t.numpy()[:nbytes], t
+
+
+def pack_pinned(pics):
+    """Copy the host buffers of `pics` into one page-locked arena laid out as
+    the device input arena, so hpvcd_gpu_submit uploads them with one DMA.
+    Returns (new descriptors, keepalive)."""
+    L = abi.lib()
+    arr = _pic_array(pics)
+    nb = L.hpvcd_gpu_packed_size(arr, len(pics))
+    buf, keep = pinned_empty(nb)
+    out = (abi.Picture * len(pics))()
+    _check(L.hpvcd_gpu_pack_inputs(arr, len(pics), buf.ctypes.data_as(C.c_void_p), nb, out),
+           "hpvcd_gpu_pack_inputs")
+    return list(out), (keep, buf, nb)
+
+
 def split_planes(pics, raw: np.ndarray):
     out = []
     o = 0

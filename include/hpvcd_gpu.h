@@ -219,6 +219,10 @@ typedef struct hpvcd_output {
     uint32_t full_range;     /* video_full_range_flag                          */
     uint32_t canvas_w, canvas_h;
     const hpvcd_tile_place* place; /* one per picture (RGB8 only)              */
+    void* host_dst;          /* optional: page-locked caller buffer that       */
+                             /* receives the output directly (then             */
+                             /* hpvcd_gpu_read copies nothing)                 */
+    uint64_t host_dst_bytes;
 } hpvcd_output;
 
 /* ------------------------------------------------------------------------ */
@@ -249,10 +253,20 @@ hpvcd_status hpvcd_gpu_create(const hpvcd_gpu_cfg* cfg, hpvcd_gpu** out);
 hpvcd_status hpvcd_gpu_destroy(hpvcd_gpu* ctx);
 /* Copy the host buffers of `n` pictures to the device, reconstruct them and
  * start the copy of the requested output back.  Host buffers are only read
- * during the call.  Returns HPVCD_ERR_ALLOC when the batch does not fit the
- * HBM budget (the caller may retry later). */
+ * during the call.  Buffers in page-locked memory are copied by DMA straight
+ * from where they are (and in one transfer when they are laid out as
+ * hpvcd_gpu_pack_inputs lays them out); pageable ones go through a staging
+ * copy.  Returns HPVCD_ERR_ALLOC when the batch does not fit the HBM budget
+ * (the caller may retry later). */
 hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* ctx, const hpvcd_picture* pics, uint32_t n,
                               const hpvcd_output* out, hpvcd_ticket* ticket);
+/* Size of the packed input layout of a batch, and the packing itself: copies
+ * every host buffer of `pics` into `dst` (bytes >= the size) and rewrites
+ * `out_pics` to point there.  A packed batch in page-locked memory is
+ * uploaded with one DMA by hpvcd_gpu_submit. */
+uint64_t hpvcd_gpu_packed_size(const hpvcd_picture* pics, uint32_t n);
+hpvcd_status hpvcd_gpu_pack_inputs(const hpvcd_picture* pics, uint32_t n, void* dst, uint64_t bytes,
+                                   hpvcd_picture* out_pics);
 /* Wait at most timeout_ms (negative: forever) for a ticket. */
 hpvcd_status hpvcd_gpu_wait(hpvcd_gpu* ctx, hpvcd_ticket ticket, int32_t timeout_ms);
 /* Bytes of output a finished ticket holds (RGB8 canvas, or all YUV planes

@@ -236,3 +236,20 @@ def test_malformed_tb_is_reported(dec):
     with pytest.raises(abi.HpvcdError) as e:
         dec.read(t)
     assert e.value.status == abi.ERR_BITSTREAM
+
+
+def test_packed_pinned_inputs_and_direct_output(dec):
+    from hpvcd_b200.gpu import pack_pinned, pinned_empty
+    g = synth.make_grid(1100, 900, seed=12, bit_depth=10)
+    out, keep = synth.grid_output(g)
+    pics = g.synth.pictures()
+    packed, pkeep = pack_pinned(pics)
+    nb = out.canvas_w * out.canvas_h * 3
+    dst, dkeep = pinned_empty(nb)
+    out.host_dst = dst.ctypes.data
+    out.host_dst_bytes = nb
+    t = dec.submit(packed, out)
+    dec.wait(t)
+    dec.read(t, dst)
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    assert np.array_equal(dst.reshape(ref.shape), ref)
