@@ -36,7 +36,7 @@ extern "C" {
 /* Status codes.  Mapping onto src/error.rs `DecodeError`:                   */
 /*   HPVCD_ERR_BITSTREAM   -> DecodeError::Bitstream (malformed flat buffers) */
 /*   HPVCD_ERR_ALLOC       -> DecodeError::AllocationFailed { what, bytes }   */
-/*   HPVCD_ERR_LIMIT       -> DecodeError::LimitExceeded                      */
+/*   HPVCD_ERR_LIMIT       -> DecodeError::LimitExceeded { what, .. }         */
 /*   HPVCD_ERR_UNSUPPORTED -> DecodeError::Unsupported                        */
 /* The remaining codes have no reference counterpart (device-side failures). */
 /* ------------------------------------------------------------------------ */
