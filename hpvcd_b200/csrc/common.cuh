@@ -34,6 +34,8 @@ struct DevPic {
     // final picture after SAO (equal to `rec` when SAO does not run).
     void* rec[3];
     void* fin[3];
+    int16_t* res[3];        // int16 residual planes of intra TBs (k_residual -> k_recon)
+    int32_t res_stride[3];  // row stride of res[c] in samples (multiple of 16)
     uint32_t* ready;  // per-CTU ready flags (wavefront)
     // output placement on the RGB canvas
     int32_t dst_x, dst_y, crop_w, crop_h;

@@ -187,7 +187,10 @@ __global__ void k_deblock(const DevPic* __restrict__ pics, int vertical) {
         const int n_edges = edge_max >= 12 ? (edge_max - 4) / 8 : 0;  // edges 8, 16, ... <= max - 4
         const int n_segs = scan_max / 4;
         if (id >= n_edges * n_segs) return;
-        const int e = id / n_segs, s = id % n_segs;
+        // vertical edges: neighbouring threads take neighbouring edges of the
+        // same rows; horizontal edges: neighbouring segments of the same edge
+        const int e = vertical ? id % n_edges : id / n_segs;
+        const int s = vertical ? id / n_edges : id % n_segs;
         luma_segment(P, vertical != 0, 8 * (e + 1), 4 * s);
     } else {
         if (P.idc == 0) return;
@@ -195,7 +198,8 @@ __global__ void k_deblock(const DevPic* __restrict__ pics, int vertical) {
         const int n_edges = edge_max >= 10 ? (edge_max - 2) / 8 : 0;  // edges 8, 16, ... <= max - 2
         const int n_segs = scan_max / 4;  // decode.rs:2042 `while scan + 4 <= scan_max`
         if (id >= n_edges * n_segs) return;
-        const int e = id / n_segs, s = id % n_segs;
+        const int e = vertical ? id % n_edges : id / n_segs;
+        const int s = vertical ? id / n_edges : id % n_segs;
         chroma_segment(P, vertical != 0, 8 * (e + 1), 4 * s);
     }
 }

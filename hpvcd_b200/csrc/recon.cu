@@ -3,28 +3,29 @@
 // bypass (transform.rs), intra prediction (intra.rs) and residual add + clip
 // (reconstruct.rs), in the decode order of decode.rs:3478-5426.
 //
-// One CTA reconstructs one CTU at a time; CTUs are claimed from a global
-// queue sorted by wavefront index (x + 2y) across all pictures, so a CTU is
-// only claimed after every CTU it depends on (left, above-left, above,
-// above-right) has been claimed by a running CTA -> no deadlock for any grid
-// size.  Per CTU:
-//   A. all coded TBs of the CTU are inverse-transformed in parallel (one warp
-//      per TB) into a shared-memory residual canvas -- this needs no
-//      neighbour and overlaps the wavefront wait;
-//   B. wait (bounded) for the neighbour CTUs, load their edge samples, then
-//      one warp walks the records in decode order: reference gathering with
-//      z-order availability, substitution, filtering, prediction, add+clip,
-//      all in shared memory;
-//   C. the CTU interior is written to the plane and its ready flag released.
-#include <cstdio>
-
+// Two kernels:
+//
+//  k_residual -- every coded TB of every picture, fully parallel (one warp
+//     per TB).  TBs whose prediction is already in the plane (inter TBs,
+//     prediction-in-plane pictures) are added and clipped into the plane
+//     right away; intra TBs leave an int16 residual in a residual plane.
+//     (int16 is exact: for 8-bit the reference itself truncates to i16,
+//     transform.rs:55-63; above 8 bits a residual outside +-32767 saturates
+//     the clip to [0, 2^bd - 1] exactly as the unsaturated one does.)
+//
+//  k_recon -- the intra wavefront.  One CTA reconstructs one CTU at a time;
+//     CTUs are claimed from a global queue sorted by wavefront index
+//     (x + 2y) across all pictures, so a CTU is only claimed after every CTU
+//     it depends on (left, above-left, above, above-right) was claimed by a
+//     running CTA: no deadlock for any grid size.  Per CTU the residuals are
+//     prefetched with cp.async while thread 0 waits (bounded) for the
+//     neighbours; then luma, Cb and Cr are walked by three warps in parallel
+//     (chroma availability only depends on the luma `decoded` map, which
+//     each warp replays from the records), all in shared memory; finally
+//     the CTU is written out and its ready flag released.
 #include "common.cuh"
 
 namespace hpvcd {
-
-constexpr int kReconWarps = 4;
-constexpr int kReconThreads = kReconWarps * 32;
-constexpr int kScr = 33;  // padded row stride of the per-warp transform scratch
 
 // intra.rs:30-38 (H.265 Tables 8-4 / 8-5)
 __constant__ int8_t c_intra_angle[33] = {32,  26,  21,  17,  13,  9,  5,  2,  0,  -2, -5,
@@ -40,48 +41,7 @@ __constant__ int8_t c_dst4[4][4] = {{29, 55, 74, 84}, {74, 74, 0, -74}, {84, -29
 __constant__ int8_t c_dct_mag[33] = {64, 90, 90, 90, 89, 88, 87, 85, 83, 82, 80, 78, 75, 73, 70, 67, 64,
                                      61, 57, 54, 50, 46, 43, 38, 36, 31, 25, 22, 18, 13, 9,  4,  0};
 
-// Shared-memory layout of one CTA.  Sizes are for the largest CTB (64) and
-// the largest chroma canvas of the batch (64 for 4:4:4, 32 otherwise).
-struct ReconLayout {
-    int cs;          // chroma canvas side
-    size_t off_dct, off_res_y, off_res_c, off_int_y, off_int_c, off_top, off_left, off_scr,
-        off_misc, total;
-    __host__ __device__ explicit ReconLayout(int c444) {
-        cs = c444 ? 64 : 32;
-        size_t o = 0;
-        off_dct = o;   o += 32 * 32 * sizeof(int16_t);
-        off_res_y = o; o += 64 * 64 * sizeof(int32_t);
-        off_res_c = o; o += 2 * (size_t)cs * cs * sizeof(int32_t);
-        off_int_y = o; o += 64 * 64 * sizeof(uint16_t);
-        off_int_c = o; o += 2 * (size_t)cs * cs * sizeof(uint16_t);
-        off_top = o;   o += 3 * 136 * sizeof(uint16_t);
-        off_left = o;  o += 3 * 64 * sizeof(uint16_t);
-        off_scr = o;   o += (size_t)kReconWarps * 2 * 32 * kScr * sizeof(int16_t);
-        off_misc = o;  o += 2048;
-        total = o;
-    }
-};
-
-// Phase-B scratch (used by warp 0 only).
-struct PredScratch {
-    int32_t s[132];        // substituted reference line (4n+1), -1 = unavailable
-    uint16_t above[68];    // 2n+1
-    uint16_t left[68];
-    uint16_t fa[68];
-    uint16_t fl[68];
-    int32_t refs[100];     // 3n+1 angular projection
-    uint32_t decoded[16];  // 16x16 luma 4x4 cells of the CTU, bit x of word y
-    uint32_t item;
-    int32_t err;
-};
-
-struct Canvas {
-    uint16_t* interior[3];
-    uint16_t* top[3];   // x = -1 .. 2S-1 stored at [x + 1]
-    uint16_t* left[3];  // y = 0 .. S-1
-    int32_t* res[3];
-    int side[3];        // S per component
-};
+constexpr int kScr = 33;  // padded row stride of the transform scratch
 
 __device__ __forceinline__ int dct_entry(int n, int k, int m) {
     if (k == 0) return 64;
@@ -96,19 +56,26 @@ __device__ __forceinline__ int dct_entry(int n, int k, int m) {
     return sign * c_dct_mag[j];
 }
 
-// ---------------------------------------------------------------------------
+__device__ __forceinline__ int sat16(int v) { return v < -32768 ? -32768 : (v > 32767 ? 32767 : v); }
+
+// ===========================================================================
+// k_residual
+// ===========================================================================
+constexpr int kResWarps = 8;
+
 // Residual of one coded TB by one warp (transform.rs:489-858, decode.rs
-// :4754-4903 luma and :5313-5417 chroma), written into `res` (stride rs).
-// ---------------------------------------------------------------------------
-__device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, int32_t* res, int rs,
-                                 const int16_t* dct, int16_t* buf, int16_t* tmp, int lane) {
+// :4754-4903 luma, :5313-5417 chroma).  `emit(r, m, v)` receives every
+// residual sample (row r, column m) in the reference's storage semantics.
+template <typename Emit>
+__device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16_t* dct, int16_t* buf,
+                                 int16_t* tmp, int lane, Emit emit) {
     const int n = 1 << t.log2n;
     const bool luma = t.comp == 0;
     const int bd = luma ? P.bd : P.bd_c;
     const bool i16s = bd <= 8;
     const int16_t* lv = P.coeffs + t.coeff_off;
     if (t.flags & HPVCD_TU_TQB) {  // decode.rs:4754-4757 / :4830-4834: residual = levels
-        for (int i = lane; i < n * n; i += 32) res[(i / n) * rs + (i % n)] = lv[i];
+        for (int i = lane; i < n * n; i += 32) emit(i / n, i % n, (int)lv[i]);
         return;
     }
     int qpp;
@@ -120,38 +87,36 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, int32_t* re
     }
     // transform.rs:701-725 dequant_params (non-extended precision: range 15)
     const int bd_shift = bd + t.log2n + 10 - 15;
-    const int max_qpp = 51 + 6 * (bd - 8);
-    const int qs = clamp3i(qpp, 0, max_qpp);
+    const int qs = clamp3i(qpp, 0, 51 + 6 * (bd - 8));
     const long long factor = (long long)c_dequant_scale[qs % 6] * (1ll << (qs / 6)) * 16;
     const long long add = 1ll << (bd_shift - 1);
     if (t.flags & HPVCD_TU_TSKIP) {  // transform.rs:728-792
         const int tr_shift = 15 - bd - t.log2n;
         const int tr_add = tr_shift > 0 ? 1 << (tr_shift - 1) : 0;
         for (int i = lane; i < n * n; i += 32) {
-            long long l = lv[i];
-            long long v = (l * factor + add) >> bd_shift;
+            long long v = ((long long)lv[i] * factor + add) >> bd_shift;
             v = v < -32768 ? -32768 : (v > 32767 ? 32767 : v);
-            int r = tr_shift >= 0 ? ((int)v + tr_add) >> tr_shift : (int)((unsigned)v << (-tr_shift));
-            res[(i / n) * rs + (i % n)] = i16s ? (int)(int16_t)r : r;
+            const int r = tr_shift >= 0 ? ((int)v + tr_add) >> tr_shift : (int)((unsigned)v << (-tr_shift));
+            emit(i / n, i % n, i16s ? (int)(int16_t)r : r);
         }
         return;
     }
     const int nx = (t.nx == 0 || t.nx > n) ? n : t.nx;
-    // dequantise into buf (row-major, padded); columns >= nx are zero
-    // (transform.rs:510-511: stage 1 skips them).  Track the last non-zero row.
+    // dequantise into buf; columns >= nx are zero (transform.rs:510-511);
+    // track the last non-zero row so stage 1 skips all-zero rows.
     int my_rows = 0;
     for (int i = lane; i < n * n; i += 32) {
         const int r = i / n, c = i % n;
         int v = 0;
         if (c < nx) {
-            const long long l = lv[i];
-            long long d = (l * factor + add) >> bd_shift;
+            const long long d = ((long long)lv[i] * factor + add) >> bd_shift;
             v = (int)(d < -32768 ? -32768 : (d > 32767 ? 32767 : d));
         }
         buf[r * kScr + c] = (int16_t)v;
         if (v) my_rows = r + 1;
     }
     int rows = my_rows;
+#pragma unroll
     for (int o = 16; o; o >>= 1) rows = max(rows, __shfl_xor_sync(0xffffffffu, rows, o));
     __syncwarp();
     const bool dst = luma && n == 4 && (t.flags & HPVCD_TU_INTRA);
@@ -161,6 +126,7 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, int32_t* re
         const int m = i / n, c = i % n;
         int acc = 0;
         if (dst) {
+#pragma unroll
             for (int k = 0; k < 4; ++k) acc += c_dst4[k][m] * buf[k * kScr + c];
         } else {
             for (int k = 0; k < rows; ++k) acc += dct[(k * step) * 32 + m] * buf[k * kScr + c];
@@ -176,312 +142,430 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, int32_t* re
         const int r = i / n, m = i % n;
         int acc = 0;
         if (dst) {
+#pragma unroll
             for (int k = 0; k < 4; ++k) acc += c_dst4[k][m] * tmp[r * kScr + k];
         } else {
             for (int k = 0; k < kmax; ++k) acc += dct[(k * step) * 32 + m] * tmp[r * kScr + k];
         }
         const int v = (acc + add2) >> shift2;
-        res[r * rs + m] = i16s ? (int)(int16_t)v : v;
+        emit(r, m, i16s ? (int)(int16_t)v : v);
     }
     __syncwarp();
 }
 
-// ---------------------------------------------------------------------------
-// Availability and sample access for component c at CTU-relative coords.
-// ---------------------------------------------------------------------------
-struct CtuGeo {
-    int ox[3], oy[3];  // CTU origin in component samples
-    int pw[3], ph[3];  // plane size
-    int S[3];
-    int sub_w, sub_h;
-    int w, h;
+__global__ void __launch_bounds__(kResWarps * 32)
+k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_prefix, uint32_t n_pics,
+           uint32_t* dev_err) {
+    __shared__ int16_t dct[32 * 32];
+    __shared__ int16_t scr[kResWarps][2][32 * kScr];
+    for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) dct[i] = (int16_t)dct_entry(32, i / 32, i % 32);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t total = rec_prefix[n_pics];
+    for (uint32_t g = rec_prefix[0] + blockIdx.x * kResWarps + warp; g < total; g += gridDim.x * kResWarps) {
+        // picture of global record g (binary search in the prefix)
+        uint32_t lo = 0, hi = n_pics;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (rec_prefix[mid] <= g) lo = mid; else hi = mid;
+        }
+        const DevPic& P = pics[lo];
+        const hpvcd_tu t = P.tus[g - rec_prefix[lo]];
+        if (!(t.flags & HPVCD_TU_CBF)) continue;
+        const int c = t.comp;
+        const int ncomp = P.idc ? 3 : 1;
+        const int n = 1 << t.log2n;
+        const int pw = c < 3 && c ? P.cw : P.w, ph = c < 3 && c ? P.ch : P.h;
+        if (c >= ncomp || t.log2n < 2 || t.log2n > 5 || (int)t.x >= pw || (int)t.y >= ph ||
+            (uint64_t)t.coeff_off + (uint64_t)n * n > P.n_coeffs) {
+            if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+            continue;
+        }
+        const int x0 = t.x, y0 = t.y;
+        const bool in_plane = (P.flags & HPVCD_PIC_PRED_IN_PLANE) || !(t.flags & HPVCD_TU_INTRA);
+        if (in_plane) {  // prediction already in the plane: add + clip (reconstruct.rs:214-251)
+            void* pl = P.rec[c];
+            const int mx = (1 << (c ? P.bd_c : P.bd)) - 1;
+            tb_residual_warp(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
+                const int x = x0 + m, y = y0 + r;
+                if (x < pw && y < ph) {
+                    const size_t idx = (size_t)y * pw + x;
+                    store_sample(pl, P.bps, idx, clamp3i(load_sample(pl, P.bps, idx) + v, 0, mx));
+                }
+            });
+        } else {
+            int16_t* rp = P.res[c];
+            const int rs = P.res_stride[c];
+            tb_residual_warp(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
+                const int x = x0 + m, y = y0 + r;
+                if (x < pw && y < ph) rp[(size_t)y * rs + x] = (int16_t)sat16(v);
+            });
+        }
+    }
+}
+
+// ===========================================================================
+// k_recon
+// ===========================================================================
+constexpr int kReconWarps = 4;
+constexpr int kReconThreads = kReconWarps * 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Per-warp scratch of the decode-order walk.
+struct WalkScratch {
+    int32_t s[132];   // substituted reference line: s[2n+q] = above[q], s[2n-q] = left[q]
+    int32_t f[132];   // filtered line (same layout); also holds available values before substitution
+    int32_t refs[100];  // angular projection, refs[n + k] for k in [-n, 2n]
+    uint4 recs[32];   // staged TB records
 };
 
-// decode.rs:4651-4690 luma_avail / chroma_avail with the `decoded` map
-// restricted to this CTU and its (already reconstructed) neighbours.
-__device__ __forceinline__ bool avail(const CtuGeo& g, const PredScratch& ps, int c, int x, int y) {
-    const int ax = g.ox[c] + x, ay = g.oy[c] + y;
-    if (ax < 0 || ay < 0 || ax >= g.pw[c] || ay >= g.ph[c]) return false;
-    const int sw = c ? g.sub_w : 1, sh = c ? g.sub_h : 1;
-    if (ax * sw >= g.w || ay * sh >= g.h) return false;
-    const int S = g.S[c];
-    if (y < 0) return true;          // CTU row above: fully reconstructed
-    if (x < 0) return y < S;         // left CTU yes, below-left CTU not yet
-    if (x >= S || y >= S) return false;
-    const int lx = (x * sw) >> 2, ly = (y * sh) >> 2;
-    return (ps.decoded[ly] >> lx) & 1u;
+// Shared-memory layout of one CTA.  Each component has one bordered canvas:
+// row 0 is the row above the CTU (x = -1 .. 2S-1), rows 1..S the CTU, column
+// 7 the column left of the CTU; sample (x, y) is at (y + 1) * CW + x + 8, so
+// the interior rows start 16-byte aligned.
+struct ReconLayout {
+    int cs;  // chroma canvas side
+    size_t off_can_y, off_can_c, off_res_y, off_res_c, off_ws, off_misc, total;
+    static __host__ __device__ int cw_of(int S) { return 2 * S + 8; }
+    __host__ __device__ explicit ReconLayout(int c444) {
+        cs = c444 ? 64 : 32;
+        size_t o = 0;
+        off_can_y = o; o += (size_t)65 * cw_of(64) * sizeof(uint16_t);
+        o = (o + 15) & ~(size_t)15;
+        off_can_c = o; o += 2 * (size_t)(cs + 1) * cw_of(cs) * sizeof(uint16_t);
+        o = (o + 15) & ~(size_t)15;
+        off_res_y = o; o += 64 * 64 * sizeof(int16_t);
+        off_res_c = o; o += 2 * (size_t)cs * cs * sizeof(int16_t);
+        off_ws = o;    o += kReconWarps * sizeof(WalkScratch);
+        o = (o + 15) & ~(size_t)15;
+        off_misc = o;  o += 16;
+        total = o;
+    }
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Everything one warp needs about one component of the current CTU.
+struct Comp {
+    int ox, oy;   // CTU origin in component samples
+    int pw, ph;   // plane size
+    int S, CW;    // CTU side in component samples, canvas row stride
+    int sw, sh;   // luma samples per component sample (1 or 2)
+    int bd, max_v;
+    bool luma, filt, smoothing, strong;
+    uint16_t* can;       // bordered canvas
+    const int16_t* res;  // S x S residual canvas
+};
+
+__device__ __forceinline__ int cidx(const Comp& k, int x, int y) { return (y + 1) * k.CW + x + 8; }
+
+// Reference sample i of the line (i < 2n: left column bottom-up, 2n: the
+// corner, > 2n: above row) with its availability (decode.rs:4651-4690
+// luma_avail / chroma_avail restricted to this CTU and its already
+// reconstructed neighbours; single slice and tile per picture).  `dec` is
+// this lane's row of the CTU's `decoded` map (lane r holds cell row r).
+__device__ __forceinline__ bool gather_ref(const Comp& k, uint32_t dec, uint32_t wabove, int n2, int x0, int y0,
+                                           int i, int* v) {
+    const bool left_side = i < n2;
+    const int x = left_side ? x0 - 1 : x0 + (i - n2 - 1);
+    const int y = left_side ? y0 + (n2 - 1 - i) : y0 - 1;
+    // decoded word of this sample's cell row (left column: differs per lane)
+    const int row = (min(max(y, 0), k.S - 1) * k.sh) >> 2;
+    const uint32_t wl = __shfl_sync(kFull, dec, row);
+    const int ax = k.ox + x, ay = k.oy + y;
+    bool a = ax >= 0 && ay >= 0 && ax < k.pw && ay < k.ph;
+    if (y >= 0) {
+        if (x < 0)
+            a = a && y < k.S;  // left CTU (below-left CTU is not reconstructed yet)
+        else
+            a = a && x < k.S && y < k.S && ((wl >> ((x * k.sw) >> 2)) & 1u);
+    }
+    (void)wabove;
+    *v = a ? (int)k.can[cidx(k, x, y)] : 0;
+    return a;
 }
 
-__device__ __forceinline__ int fetch(const Canvas& cv, int c, int x, int y) {
-    if (y < 0) return cv.top[c][x + 1];
-    if (x < 0) return cv.left[c][y];
-    return cv.interior[c][y * cv.side[c] + x];
+// The angular reference projection of intra.rs:305-318: position in the
+// reference line of refs[k] (k in [-n, 2n]).
+__device__ __forceinline__ int ref_pos(int k, bool vertical, int n2, int inv) {
+    if (k >= 0) return vertical ? n2 + k : n2 - k;
+    const int idx = max(min((k * inv + 128) >> 8, n2), 0);
+    return vertical ? n2 - idx : n2 + idx;
 }
 
-// intra.rs:84-148 substitution, :151-219 filtering, :257-372 prediction, and
-// the residual add of reconstruct.rs:214-251, for one TB by one warp.
-__device__ void predict_tb_warp(const DevPic& P, const hpvcd_tu& t, int c, int x0, int y0,
-                                const CtuGeo& g, const Canvas& cv, PredScratch& ps, int lane,
-                                bool coded) {
-    const int n = 1 << t.log2n;
-    const bool luma = c == 0;
-    const int bd = luma ? P.bd : P.bd_c;
-    const int total = 4 * n + 1;
-    // gather: s[i] = left[2n-1-i] (i < 2n), s[2n] = corner, s[2n+1+i] = above[i]
-    for (int i = lane; i < total; i += 32) {
-        int x, y;
-        if (i < 2 * n) {
-            x = x0 - 1;
-            y = y0 + (2 * n - 1 - i);
-        } else if (i == 2 * n) {
-            x = x0 - 1;
-            y = y0 - 1;
-        } else {
-            x = x0 + (i - 2 * n - 1);
-            y = y0 - 1;
-        }
-        ps.s[i] = avail(g, ps, c, x, y) ? fetch(cv, c, x, y) : -1;
+// 4x4 intra TB entirely in registers: the 17 reference samples live in
+// lanes 0..16 (intra.rs:84-148 substitution via shuffles; no filtering for
+// n = 4, intra.rs:174), prediction (intra.rs:257-372) by lanes 0..15.
+__device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y0, bool coded, uint32_t dec,
+                                          int lane) {
+    constexpr int n = 4, n2 = 8, total = 17;
+    int v = 0;
+    // every lane joins the shuffle inside gather_ref; lanes past the line
+    // repeat the last position and drop it
+    bool a = gather_ref(k, dec, 0u, n2, x0, y0, min(lane, total - 1), &v);
+    a = a && lane < total;
+    const uint32_t mask = __ballot_sync(kFull, a);
+    int sv;
+    if (!mask) {
+        sv = 1 << (k.bd - 1);
+    } else {
+        const uint32_t m0 = mask & ((2u << lane) - 1u);
+        const int j = m0 ? 31 - __clz(m0) : __ffs(mask) - 1;
+        sv = __shfl_sync(kFull, v, j);
     }
-    __syncwarp();
-    uint32_t mask[5];
-#pragma unroll
-    for (int wd = 0; wd < 5; ++wd) {
-        const int i = wd * 32 + lane;
-        mask[wd] = __ballot_sync(0xffffffffu, i < total && ps.s[i] >= 0);
-    }
-    int first = -1;
-#pragma unroll
-    for (int wd = 4; wd >= 0; --wd)
-        if (mask[wd]) first = wd * 32 + __ffs(mask[wd]) - 1;
-    const int neutral = 1 << (bd - 1);
-    // substituted value of position i (last available j <= i, or `first`)
-    int subst[5];
-#pragma unroll
-    for (int wd = 0; wd < 5; ++wd) {
-        const int i = wd * 32 + lane;
-        int v = neutral;
-        if (i < total && first >= 0) {
-            int j = -1;
-            const uint32_t m0 = mask[wd] & (0xffffffffu >> (31 - lane));
-            if (m0) {
-                j = wd * 32 + 31 - __clz(m0);
-            } else {
-                for (int q = wd - 1; q >= 0; --q)
-                    if (mask[q]) {
-                        j = q * 32 + 31 - __clz(mask[q]);
-                        break;
-                    }
-            }
-            if (j < 0) j = first;
-            v = ps.s[j];
-        }
-        subst[wd] = v;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int wd = 0; wd < 5; ++wd) {
-        const int i = wd * 32 + lane;
-        if (i < total) {
-            // above_out[k] = s[2n + k], left_out[k] = s[2n - k]
-            if (i >= 2 * n) ps.above[i - 2 * n] = (uint16_t)subst[wd];
-            if (i <= 2 * n) ps.left[2 * n - i] = (uint16_t)subst[wd];
-        }
-    }
-    __syncwarp();
-    // filtering (luma, or 4:4:4 chroma without strong smoothing)
-    const int mode = t.mode;
-    const uint16_t* A = ps.above;
-    const uint16_t* L = ps.left;
-    const bool smoothing = !(P.flags & HPVCD_PIC_SMOOTHING_DISABLED);
-    const bool filt_ok = luma || P.idc == 3;
-    bool do_filter = false;
-    if (filt_ok && smoothing && n != 4 && mode != 1) {
-        const int md = min(abs(mode - 26), abs(mode - 10));
-        const int thresh = n == 8 ? 7 : (n == 16 ? 1 : (n == 32 ? 0 : 8));
-        do_filter = mode == 0 || md > thresh;
-    }
-    if (do_filter) {
-        bool strong = false;
-        if (luma && (P.flags & HPVCD_PIC_STRONG_SMOOTHING) && n == 32) {
-            const int thr = 1 << (bd - 5);
-            const int bl = L[2 * n], tl = A[0], tr = A[2 * n], cl = L[n], ct = A[n];
-            strong = abs(bl + tl - 2 * cl) < thr && abs(tr + tl - 2 * ct) < thr;
-        }
-        for (int i = lane; i <= 2 * n; i += 32) {
-            int fa, fl;
-            if (strong) {
-                const int tl = A[0], tr = A[2 * n], bl = L[2 * n];
-                if (i == 0 || i == 2 * n) {
-                    fa = A[i];
-                    fl = L[i];
-                } else {
-                    fa = ((2 * n - i) * tl + i * tr + n) >> 6;
-                    fl = ((2 * n - i) * tl + i * bl + n) >> 6;
-                }
-            } else if (i == 0) {
-                fa = fl = (L[1] + 2 * A[0] + A[1] + 2) >> 2;
-            } else if (i == 2 * n) {
-                fa = A[i];
-                fl = L[i];
-            } else {
-                fa = (A[i - 1] + 2 * A[i] + A[i + 1] + 2) >> 2;
-                fl = (L[i - 1] + 2 * L[i] + L[i + 1] + 2) >> 2;
-            }
-            ps.fa[i] = (uint16_t)fa;
-            ps.fl[i] = (uint16_t)fl;
-        }
-        __syncwarp();
-        A = ps.fa;
-        L = ps.fl;
-    }
-    const int max_v = (1 << bd) - 1;
-    const bool edge_filters = luma && n < 32;  // is_luma gate of predict_into
-    const int log2n = t.log2n;
-    const int S = cv.side[c];
-    uint16_t* out = cv.interior[c];
-    const int32_t* res = cv.res[c];
-    const int vw = min(n, g.pw[c] - (g.ox[c] + x0)), vh = min(n, g.ph[c] - (g.oy[c] + y0));
+    // sv in lane i = s[i]
+    const int yy = lane >> 2, xx = lane & 3;
+    int pred;
     if (mode >= 2) {
         const int angle = c_intra_angle[mode - 2];
         const bool vertical = mode >= 18;
-        const uint16_t* mainr = vertical ? A : L;
-        const uint16_t* side = vertical ? L : A;
-        for (int i = lane; i <= 2 * n; i += 32) ps.refs[n + i] = mainr[i];
+        const int inv = angle < 0 ? c_inv_angle[mode - 11] : 0;
+        const int a_ = vertical ? yy : xx, b = vertical ? xx : yy;
+        const int pos = (a_ + 1) * angle;
+        const int iidx = pos >> 5, frac = pos & 31;
+        const int r0 = __shfl_sync(kFull, sv, ref_pos(b + iidx + 1, vertical, n2, inv));
+        const int r1 = __shfl_sync(kFull, sv, ref_pos(min(b + iidx + 2, 2 * n), vertical, n2, inv));
+        pred = clamp3i(frac ? ((32 - frac) * r0 + frac * r1 + 16) >> 5 : r0, 0, k.max_v);
+        if (k.luma) {  // DC / vertical / horizontal edge filters (n < 32)
+            const int c0 = __shfl_sync(kFull, sv, n2);
+            const int a0 = __shfl_sync(kFull, sv, vertical ? n2 + 1 : n2 - 1);
+            const int e = __shfl_sync(kFull, sv, mode == 26 ? n2 - (yy + 1) : n2 + xx + 1);
+            if ((mode == 26 && xx == 0) || (mode == 10 && yy == 0)) pred = clamp3i(a0 + ((e - c0) >> 1), 0, k.max_v);
+        }
+    } else if (mode == 1) {  // DC
+        int part = ((lane >= n2 - n && lane < n2) || (lane > n2 && lane <= n2 + n)) ? sv : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+        const int dc = (part + n) >> 3;
+        const int l1 = __shfl_sync(kFull, sv, n2 - 1), a1 = __shfl_sync(kFull, sv, n2 + 1);
+        const int e = __shfl_sync(kFull, sv, yy == 0 ? n2 + xx + 1 : n2 - yy - 1);
+        pred = dc;
+        if (k.luma) {
+            if (xx == 0 && yy == 0)
+                pred = (l1 + 2 * dc + a1 + 2) >> 2;
+            else if (yy == 0 || xx == 0)
+                pred = (e + 3 * dc + 2) >> 2;
+        }
+    } else {  // planar
+        const int lft = __shfl_sync(kFull, sv, n2 - yy - 1), abv = __shfl_sync(kFull, sv, n2 + xx + 1);
+        const int tr = __shfl_sync(kFull, sv, n2 + n + 1), bl = __shfl_sync(kFull, sv, n2 - n - 1);
+        pred = ((n - 1 - xx) * lft + (xx + 1) * tr + (n - 1 - yy) * abv + (yy + 1) * bl + n) >> 3;
+    }
+    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    if (lane < 16 && xx < vw && yy < vh) {
+        if (coded) pred = clamp3i(pred + k.res[(y0 + yy) * k.S + x0 + xx], 0, k.max_v);
+        k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)pred;
+    }
+    __syncwarp();
+}
+
+// Intra TB of size 8..32 by one warp through shared memory: gather,
+// substitution (intra.rs:84-148), filtering (:151-219), prediction
+// (:257-372), add residual + clip (reconstruct.rs:214-251).
+__device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
+                                             uint32_t dec, WalkScratch& ws, int lane) {
+    const int n = 1 << log2n;
+    const int total = 4 * n + 1;
+    const int n2 = 2 * n;
+    uint32_t mask[5];
+    int val[5];
+#pragma unroll
+    for (int wd = 0; wd < 5; ++wd) {
+        const int i = wd * 32 + lane;
+        int v = 0;
+        bool a = false;
+        if (wd * 32 < total) {  // warp-uniform: every lane joins the shuffle inside
+            a = gather_ref(k, dec, 0u, n2, x0, y0, min(i, total - 1), &v);
+            a = a && i < total;
+        }
+        val[wd] = v;
+        mask[wd] = __ballot_sync(kFull, a);
+    }
+    int last_upto[5];
+    int first = -1, run = -1;
+#pragma unroll
+    for (int wd = 0; wd < 5; ++wd) {
+        if (mask[wd]) run = wd * 32 + 31 - __clz(mask[wd]);
+        last_upto[wd] = run;
+        if (first < 0 && mask[wd]) first = wd * 32 + __ffs(mask[wd]) - 1;
+    }
+#pragma unroll
+    for (int wd = 0; wd < 5; ++wd) {
+        const int i = wd * 32 + lane;
+        if (i < total && ((mask[wd] >> lane) & 1u)) ws.f[i] = val[wd];
+    }
+    __syncwarp();
+    const int neutral = 1 << (k.bd - 1);
+#pragma unroll
+    for (int wd = 0; wd < 5; ++wd) {
+        const int i = wd * 32 + lane;
+        if (i >= total) continue;
+        int v;
+        if (first < 0) {
+            v = neutral;
+        } else if ((mask[wd] >> lane) & 1u) {
+            v = val[wd];
+        } else {
+            const uint32_t m0 = mask[wd] & ((2u << lane) - 1u);
+            int j = m0 ? wd * 32 + 31 - __clz(m0) : (wd ? last_upto[wd - 1] : -1);
+            if (j < 0) j = first;
+            v = ws.f[j];
+        }
+        ws.s[i] = v;
+    }
+    __syncwarp();
+    // ---- filtering (luma, or 4:4:4 chroma without strong smoothing) ----
+    bool do_filter = false;
+    if (k.filt && k.smoothing && mode != 1) {
+        const int md = min(abs(mode - 26), abs(mode - 10));
+        const int thresh = n == 8 ? 7 : (n == 16 ? 1 : 0);
+        do_filter = mode == 0 || md > thresh;
+    }
+    const int32_t* R = ws.s;
+    if (do_filter) {
+        bool strong = false;
+        const int tl = ws.s[n2], tr = ws.s[2 * n2], bl = ws.s[0];
+        if (k.luma && k.strong && n == 32) {
+            const int thr = 1 << (k.bd - 5);
+            strong = abs(bl + tl - 2 * ws.s[n2 - n]) < thr && abs(tr + tl - 2 * ws.s[n2 + n]) < thr;
+        }
+        for (int i = lane; i < total; i += 32) {
+            int v;
+            if (i == 0 || i == 2 * n2) {
+                v = ws.s[i];
+            } else if (strong) {
+                if (i == n2) {
+                    v = ws.s[i];
+                } else if (i > n2) {
+                    const int q = i - n2;  // above[q]
+                    v = ((n2 - q) * tl + q * tr + n) >> 6;
+                } else {
+                    const int q = n2 - i;  // left[q]
+                    v = ((n2 - q) * tl + q * bl + n) >> 6;
+                }
+            } else {
+                v = (ws.s[i - 1] + 2 * ws.s[i] + ws.s[i + 1] + 2) >> 2;
+            }
+            ws.f[i] = v;
+        }
+        __syncwarp();
+        R = ws.f;
+    }
+    // A(q) = R[n2 + q], L(q) = R[n2 - q]
+    const int max_v = k.max_v;
+    const bool edge_filters = k.luma && n < 32;  // is_luma gate of predict_into
+    const int S = k.S;
+    const int16_t* res = k.res;
+    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    if (mode >= 2) {
+        const int angle = c_intra_angle[mode - 2];
+        const bool vertical = mode >= 18;
+        for (int q = lane; q <= n2; q += 32) ws.refs[n + q] = vertical ? R[n2 + q] : R[n2 - q];
         if (angle < 0) {
             const int inv = c_inv_angle[mode - 11];
             const int lim = (n * angle) >> 5;
-            for (int k = -1 - lane; k >= lim; k -= 32) {
-                const int idx = min((k * inv + 128) >> 8, 2 * n);
-                ps.refs[k + n] = side[max(idx, 0)];
+            for (int q = -1 - lane; q >= lim; q -= 32) {
+                const int idx = max(min((q * inv + 128) >> 8, n2), 0);
+                ws.refs[q + n] = vertical ? R[n2 - idx] : R[n2 + idx];  // side(idx)
             }
         }
         __syncwarp();
+        const int a0 = vertical ? R[n2 + 1] : R[n2 - 1];  // above[1] / left[1]
+        const int c0 = R[n2];
+#pragma unroll 4
         for (int i = lane; i < n * n; i += 32) {
             const int yy = i >> log2n, xx = i & (n - 1);
-            const int a = vertical ? yy : xx;  // index whose (a+1)*angle gives the position
-            const int b = vertical ? xx : yy;  // index along the main reference
+            const int a = vertical ? yy : xx;
+            const int b = vertical ? xx : yy;
             const int pos = (a + 1) * angle;
             const int iidx = pos >> 5, frac = pos & 31;
-            const int r0 = ps.refs[b + iidx + 1 + n];
-            int v = r0;
-            if (frac) v = ((32 - frac) * r0 + frac * ps.refs[b + iidx + 2 + n] + 16) >> 5;
+            const int r0 = ws.refs[b + iidx + 1 + n];
+            const int r1 = ws.refs[min(b + iidx + 2, 2 * n) + n];
+            int v = frac ? ((32 - frac) * r0 + frac * r1 + 16) >> 5 : r0;
             v = clamp3i(v, 0, max_v);
             if (edge_filters) {
-                if (mode == 26 && xx == 0) v = clamp3i(A[1] + ((L[yy + 1] - A[0]) >> 1), 0, max_v);
-                if (mode == 10 && yy == 0) v = clamp3i(L[1] + ((A[xx + 1] - A[0]) >> 1), 0, max_v);
+                if (mode == 26 && xx == 0) v = clamp3i(a0 + ((R[n2 - (yy + 1)] - c0) >> 1), 0, max_v);
+                if (mode == 10 && yy == 0) v = clamp3i(a0 + ((R[n2 + xx + 1] - c0) >> 1), 0, max_v);
             }
             if (xx < vw && yy < vh) {
                 if (coded) v = clamp3i(v + res[(y0 + yy) * S + x0 + xx], 0, max_v);
-                out[(y0 + yy) * S + x0 + xx] = (uint16_t)v;
+                k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
     } else if (mode == 1) {  // DC
-        int sum = 0;
-        for (int i = 1; i <= n; ++i) sum += A[i] + L[i];
-        const int dc = (sum + n) >> (log2n + 1);
+        int part = lane < n ? R[n2 + 1 + lane] + R[n2 - 1 - lane] : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+        const int dc = (part + n) >> (log2n + 1);
+#pragma unroll 4
         for (int i = lane; i < n * n; i += 32) {
             const int yy = i >> log2n, xx = i & (n - 1);
             int v = dc;
             if (edge_filters) {
                 if (xx == 0 && yy == 0)
-                    v = (L[1] + 2 * dc + A[1] + 2) >> 2;
+                    v = (R[n2 - 1] + 2 * dc + R[n2 + 1] + 2) >> 2;
                 else if (yy == 0)
-                    v = (A[xx + 1] + 3 * dc + 2) >> 2;
+                    v = (R[n2 + xx + 1] + 3 * dc + 2) >> 2;
                 else if (xx == 0)
-                    v = (L[yy + 1] + 3 * dc + 2) >> 2;
+                    v = (R[n2 - yy - 1] + 3 * dc + 2) >> 2;
             }
             if (xx < vw && yy < vh) {
                 if (coded) v = clamp3i(v + res[(y0 + yy) * S + x0 + xx], 0, max_v);
-                out[(y0 + yy) * S + x0 + xx] = (uint16_t)v;
+                k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
     } else {  // planar
-        const int tr = A[n + 1], bl = L[n + 1];
+        const int tr = R[n2 + n + 1], bl = R[n2 - n - 1];
+#pragma unroll 4
         for (int i = lane; i < n * n; i += 32) {
             const int yy = i >> log2n, xx = i & (n - 1);
-            const int hh = (n - 1 - xx) * L[yy + 1] + (xx + 1) * tr;
-            const int vv = (n - 1 - yy) * A[xx + 1] + (yy + 1) * bl;
+            const int hh = (n - 1 - xx) * R[n2 - yy - 1] + (xx + 1) * tr;
+            const int vv = (n - 1 - yy) * R[n2 + xx + 1] + (yy + 1) * bl;
             int v = (hh + vv + n) >> (log2n + 1);
             if (xx < vw && yy < vh) {
                 if (coded) v = clamp3i(v + res[(y0 + yy) * S + x0 + xx], 0, max_v);
-                out[(y0 + yy) * S + x0 + xx] = (uint16_t)v;
+                k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
     }
     __syncwarp();
 }
 
-__device__ __forceinline__ void mark_decoded(const CtuGeo& g, PredScratch& ps, int x0, int y0, int n,
-                                             int lane) {
-    // luma CTU-relative square; cells outside the picture stay unmarked
-    // (decode.rs:3170-3189 via fill_grid_rect clipped to the grid).
-    for (int i = lane; i < 16; i += 32) {
-        const int cy = i;
-        const int y = cy * 4;
-        if (y < y0 || y >= y0 + n || g.oy[0] + y >= g.h) continue;
-        uint32_t bits = 0;
-        for (int x = x0; x < x0 + n && x < 64; x += 4)
-            if (g.ox[0] + x < g.w) bits |= 1u << (x >> 2);
-        ps.decoded[cy] |= bits;
+// Mark a luma square decoded (decode.rs:3170-3189; cells outside the
+// picture stay unmarked).  Lane r holds cell row r; no synchronisation.
+__device__ __forceinline__ uint32_t mark_rows(uint32_t dec, int x0, int y0, int n, int lane, int vis_w, int vis_h) {
+    const int r0 = y0 >> 2, r1 = (min(y0 + n, vis_h) + 3) >> 2;
+    const int x1 = min(x0 + n, vis_w);
+    if (lane >= r0 && lane < r1 && x1 > x0) {
+        const int c0 = x0 >> 2, c1 = (x1 + 3) >> 2;
+        dec |= (c1 - c0 >= 32 ? kFull : ((1u << (c1 - c0)) - 1u)) << c0;
     }
-    __syncwarp();
+    return dec;
 }
 
-// ---------------------------------------------------------------------------
-// The kernel.
-// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kReconThreads)
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
         uint32_t* work_counter, uint32_t* dev_err, int c444, uint32_t spin_limit) {
     extern __shared__ __align__(16) unsigned char smem[];
     const ReconLayout lay(c444);
-    int16_t* dct = (int16_t*)(smem + lay.off_dct);
-    PredScratch& ps = *(PredScratch*)(smem + lay.off_misc);
+    uint32_t* s_item = (uint32_t*)(smem + lay.off_misc);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int16_t* wbuf = (int16_t*)(smem + lay.off_scr) + (size_t)warp * 2 * 32 * kScr;
-    int16_t* wtmp = wbuf + 32 * kScr;
-
-    for (int i = tid; i < 32 * 32; i += kReconThreads) dct[i] = (int16_t)dct_entry(32, i / 32, i % 32);
-
     for (;;) {
         __syncthreads();
-        if (tid == 0) ps.item = atomicAdd(work_counter, 1u);
+        if (tid == 0) *s_item = atomicAdd(work_counter, 1u);
         __syncthreads();
-        const uint32_t item = ps.item;
+        const uint32_t item = *s_item;
         if (item >= n_items) break;
         const CtuItem it = items[item];
         const DevPic& P = pics[it.pic];
         const int ctb = 1 << P.log2_ctb;
-        CtuGeo g;
-        g.w = P.w;
-        g.h = P.h;
-        g.sub_w = P.sub_w;
-        g.sub_h = P.sub_h;
-        g.ox[0] = it.cx * ctb;
-        g.oy[0] = it.cy * ctb;
-        g.pw[0] = P.w;
-        g.ph[0] = P.h;
-        g.S[0] = ctb;
-        for (int c = 1; c < 3; ++c) {
-            g.ox[c] = g.ox[0] / P.sub_w;
-            g.oy[c] = g.oy[0] / P.sub_h;
-            g.pw[c] = P.cw;
-            g.ph[c] = P.ch;
-            g.S[c] = ctb / P.sub_w;
-        }
-        Canvas cv;
-        cv.interior[0] = (uint16_t*)(smem + lay.off_int_y);
-        cv.interior[1] = (uint16_t*)(smem + lay.off_int_c);
-        cv.interior[2] = cv.interior[1] + lay.cs * lay.cs;
-        cv.res[0] = (int32_t*)(smem + lay.off_res_y);
-        cv.res[1] = (int32_t*)(smem + lay.off_res_c);
-        cv.res[2] = cv.res[1] + lay.cs * lay.cs;
-        for (int c = 0; c < 3; ++c) {
-            cv.top[c] = (uint16_t*)(smem + lay.off_top) + c * 136;
-            cv.left[c] = (uint16_t*)(smem + lay.off_left) + c * 64;
-            cv.side[c] = g.S[c];
-        }
         const int ncomp = P.idc ? 3 : 1;
+        const int oxl = it.cx * ctb, oyl = it.cy * ctb;
+        const int ocx = oxl / P.sub_w, ocy = oyl / P.sub_h, Sc = ctb / P.sub_w;
         const uint32_t ci = (uint32_t)it.cy * P.ctb_cols + it.cx;
         uint32_t r0 = P.ctu_start[ci], r1 = P.ctu_start[ci + 1];
         if (r1 > P.n_tus || r0 > r1) {  // malformed CTU range: report, reconstruct nothing
@@ -489,50 +573,55 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             r1 = min(r1, P.n_tus);
             r0 = min(r0, r1);
         }
-        if (tid < 16) ps.decoded[tid] = 0;
-        if (tid == 0) ps.err = 0;
-        // Inter / prediction-in-plane pictures: the plane already holds the
-        // prediction; load the CTU interior.
-        const bool pred_plane = (P.flags & (HPVCD_PIC_PRED_IN_PLANE | HPVCD_PIC_INTER)) != 0;
-        if (pred_plane) {
+        auto can_of = [&](int c) -> uint16_t* {
+            return c == 0 ? (uint16_t*)(smem + lay.off_can_y)
+                          : (uint16_t*)(smem + lay.off_can_c) +
+                                (size_t)(c - 1) * (lay.cs + 1) * ReconLayout::cw_of(lay.cs);
+        };
+        auto res_of = [&](int c) -> int16_t* {
+            return c == 0 ? (int16_t*)(smem + lay.off_res_y)
+                          : (int16_t*)(smem + lay.off_res_c) + (size_t)(c - 1) * lay.cs * lay.cs;
+        };
+        // ---- prefetch the residual canvases (cp.async, 8 samples per copy) ----
+        for (int c = 0; c < ncomp; ++c) {
+            const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+            const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+            const int rows = min(S, ph - oy), cols = min(S, pw - ox);
+            const int chunks = (cols + 7) >> 3;
+            const int16_t* src = P.res[c] + (size_t)oy * P.res_stride[c] + ox;
+            int16_t* dst = res_of(c);
+            for (int i = tid; i < rows * chunks; i += kReconThreads) {
+                const int y = i / chunks, q = i % chunks;
+                // residual rows are padded to 16 samples, so a 16-byte copy never
+                // leaves the allocation; samples beyond `cols` are unused
+                cp_async16(dst + y * S + 8 * q, src + (size_t)y * P.res_stride[c] + 8 * q);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        // Inter pictures: the plane holds motion-compensated + residual
+        // samples; load the CTU interior so intra TBs can predict from it.
+        if (P.flags & HPVCD_PIC_INTER) {
             for (int c = 0; c < ncomp; ++c) {
-                const int S = g.S[c];
+                const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+                const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+                uint16_t* can = can_of(c);
+                const int CW = ReconLayout::cw_of(S);
                 for (int i = tid; i < S * S; i += kReconThreads) {
                     const int y = i / S, x = i % S;
-                    const int ax = g.ox[c] + x, ay = g.oy[c] + y;
+                    const int ax = ox + x, ay = oy + y;
                     int v = 0;
-                    if (ax < g.pw[c] && ay < g.ph[c])
-                        v = load_sample(P.rec[c], P.bps, (size_t)ay * g.pw[c] + ax);
-                    cv.interior[c][i] = (uint16_t)v;
+                    if (ax < pw && ay < ph) v = load_sample(P.rec[c], P.bps, (size_t)ay * pw + ax);
+                    can[(y + 1) * CW + x + 8] = (uint16_t)v;
                 }
             }
         }
-        // ---- Phase A: residuals of all coded TBs, one warp per TB ----
-        {
-            int k = 0;
-            for (uint32_t r = r0; r < r1; ++r) {
-                const hpvcd_tu t = P.tus[r];
-                if (!(t.flags & HPVCD_TU_CBF)) continue;
-                if ((k++ % kReconWarps) != warp) continue;
-                const int c = t.comp;
-                const int n = 1 << t.log2n;
-                const int x = (int)t.x - g.ox[c < 3 ? c : 0], y = (int)t.y - g.oy[c < 3 ? c : 0];
-                const bool bad = c >= ncomp || t.log2n < 2 || t.log2n > 5 || x < 0 || y < 0 ||
-                                 x + n > g.S[c] || y + n > g.S[c] ||
-                                 (uint64_t)t.coeff_off + (uint64_t)n * n > P.n_coeffs;
-                if (bad) {
-                    if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
-                    continue;
-                }
-                tb_residual_warp(P, t, cv.res[c] + y * g.S[c] + x, g.S[c], dct, wbuf, wtmp, lane);
-            }
-        }
-        // ---- Phase B prologue: wait for the neighbours and load their edges ----
-        if (P.needs_wavefront && tid == 0) {
+        // ---- wait for the neighbours (bounded) and load their edges ----
+        if (tid == 0) {
             const int cx = it.cx, cy = it.cy;
             const int nb[4][2] = {{cx - 1, cy}, {cx - 1, cy - 1}, {cx, cy - 1}, {cx + 1, cy - 1}};
-            for (int k = 0; k < 4; ++k) {
-                const int nx = nb[k][0], ny = nb[k][1];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int nx = nb[q][0], ny = nb[q][1];
                 if (nx < 0 || ny < 0 || nx >= P.ctb_cols) continue;
                 const uint32_t* f = P.ready + (size_t)ny * P.ctb_cols + nx;
                 uint32_t spins = 0;
@@ -546,78 +635,118 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             }
         }
         __syncthreads();
-        if (P.needs_wavefront) {
-            for (int c = 0; c < ncomp; ++c) {
-                const int S = g.S[c];
-                for (int i = tid; i < 2 * S + 1; i += kReconThreads) {
-                    const int x = i - 1;
-                    const int ax = g.ox[c] + x, ay = g.oy[c] - 1;
+        for (int c = 0; c < ncomp; ++c) {
+            const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+            const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+            uint16_t* can = can_of(c);
+            const int CW = ReconLayout::cw_of(S);
+            for (int i = tid; i < 3 * S + 1; i += kReconThreads) {
+                if (i < 2 * S + 1) {  // row above: x = i - 1
+                    const int ax = ox + i - 1, ay = oy - 1;
                     int v = 0;
-                    if (ay >= 0 && ax >= 0 && ax < g.pw[c])
-                        v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * g.pw[c] + ax);
-                    cv.top[c][i] = (uint16_t)v;
-                }
-                for (int i = tid; i < S; i += kReconThreads) {
-                    const int ax = g.ox[c] - 1, ay = g.oy[c] + i;
+                    if (ay >= 0 && ax >= 0 && ax < pw) v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * pw + ax);
+                    can[i + 7] = (uint16_t)v;
+                } else {  // column left: y = i - (2S + 1)
+                    const int y = i - (2 * S + 1);
+                    const int ax = ox - 1, ay = oy + y;
                     int v = 0;
-                    if (ax >= 0 && ay < g.ph[c])
-                        v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * g.pw[c] + ax);
-                    cv.left[c][i] = (uint16_t)v;
+                    if (ax >= 0 && ay < ph) v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * pw + ax);
+                    can[(y + 1) * CW + 7] = (uint16_t)v;
                 }
             }
         }
+        cp_async_wait_all();
         __syncthreads();
-        // ---- Phase B: decode-order walk by warp 0 ----
-        if (warp == 0) {
+        // ---- decode-order walk: warp c reconstructs component c ----
+        if (warp < ncomp) {
+            const int c = warp;
+            WalkScratch& ws = ((WalkScratch*)(smem + lay.off_ws))[c];
+            Comp k;
+            k.S = c ? Sc : ctb;
+            k.CW = ReconLayout::cw_of(k.S);
+            k.ox = c ? ocx : oxl;
+            k.oy = c ? ocy : oyl;
+            k.pw = c ? P.cw : P.w;
+            k.ph = c ? P.ch : P.h;
+            k.sw = c ? P.sub_w : 1;
+            k.sh = c ? P.sub_h : 1;
+            k.bd = c ? P.bd_c : P.bd;
+            k.max_v = (1 << k.bd) - 1;
+            k.luma = c == 0;
+            k.filt = c == 0 || P.idc == 3;
+            k.smoothing = !(P.flags & HPVCD_PIC_SMOOTHING_DISABLED);
+            k.strong = (P.flags & HPVCD_PIC_STRONG_SMOOTHING) != 0;
+            k.can = can_of(c);
+            k.res = res_of(c);
+            const int vis_w = min(64, P.w - oxl), vis_h = min(64, P.h - oyl);
             const bool intra_pred_ok = !(P.flags & HPVCD_PIC_PRED_IN_PLANE);
-            for (uint32_t r = r0; r < r1; ++r) {
-                const hpvcd_tu t = P.tus[r];
-                const int c = t.comp;
-                const int n = 1 << t.log2n;
-                if (c >= ncomp || t.log2n < 2 || t.log2n > 6) continue;
-                const int x = (int)t.x - g.ox[c], y = (int)t.y - g.oy[c];
-                if (x < 0 || y < 0 || x + n > g.S[c] || y + n > g.S[c]) continue;
-                const bool coded = (t.flags & HPVCD_TU_CBF) != 0 && t.log2n <= 5 &&
-                                   (uint64_t)t.coeff_off + (uint64_t)n * n <= P.n_coeffs;
-                const bool intra = (t.flags & HPVCD_TU_INTRA) != 0;
-                if (intra && intra_pred_ok) {
-                    if (t.log2n <= 5 && t.mode <= 34)
-                        predict_tb_warp(P, t, c, x, y, g, cv, ps, lane, coded);
-                    else if (lane == 0)
-                        atomicOr(dev_err, DEV_ERR_BITSTREAM);
-                } else if (coded) {
-                    // prediction already in the canvas: add + clip (reconstruct.rs:214-251)
-                    const int S = g.S[c];
-                    const int bd = c ? P.bd_c : P.bd;
-                    const int mx = (1 << bd) - 1;
-                    const int vw = min(n, g.pw[c] - (g.ox[c] + x)), vh = min(n, g.ph[c] - (g.oy[c] + y));
-                    for (int i = lane; i < n * n; i += 32) {
-                        const int yy = i / n, xx = i % n;
-                        if (xx < vw && yy < vh) {
-                            const int idx = (y + yy) * S + x + xx;
-                            cv.interior[c][idx] =
-                                (uint16_t)clamp3i((int)cv.interior[c][idx] + cv.res[c][idx], 0, mx);
+            uint32_t dec = 0;  // lane r: cell row r of the CTU's `decoded` map
+            for (uint32_t base = r0; base < r1; base += 32) {
+                if (base + lane < r1) ws.recs[lane] = *(const uint4*)(P.tus + base + lane);
+                __syncwarp();
+                const int cnt = (int)min(32u, r1 - base);
+                for (int j = 0; j < cnt; ++j) {
+                    const uint4 w = ws.recs[j];
+                    hpvcd_tu t;
+                    memcpy(&t, &w, sizeof(t));
+                    const int tc = t.comp;
+                    if (tc >= ncomp || t.log2n < 2 || t.log2n > 6) continue;
+                    const int n = 1 << t.log2n;
+                    const int x = (int)t.x - (tc ? ocx : oxl), y = (int)t.y - (tc ? ocy : oyl);
+                    const int St = tc ? Sc : ctb;
+                    if (x < 0 || y < 0 || x + n > St || y + n > St) {
+                        if (lane == 0 && c == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+                        continue;
+                    }
+                    if (tc == c && (t.flags & HPVCD_TU_INTRA) && intra_pred_ok) {
+                        const bool coded = (t.flags & HPVCD_TU_CBF) != 0;
+                        if (t.mode > 34 || t.log2n > 5) {
+                            if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+                        } else if (t.log2n == 2) {
+                            intra_tb4(k, t.mode, x, y, coded, dec, lane);
+                        } else {
+                            intra_tb_big(k, t.log2n, t.mode, x, y, coded, dec, ws, lane);
                         }
                     }
-                    __syncwarp();
+                    if (tc == 0) dec = mark_rows(dec, x, y, n, lane, vis_w, vis_h);
                 }
-                if (c == 0) mark_decoded(g, ps, x, y, n, lane);
+                __syncwarp();
             }
         }
         __syncthreads();
-        // ---- Phase C: publish the CTU ----
+        // ---- publish the CTU (8 samples per store when rows allow) ----
         for (int c = 0; c < ncomp; ++c) {
-            const int S = g.S[c];
-            for (int i = tid; i < S * S; i += kReconThreads) {
-                const int y = i / S, x = i % S;
-                const int ax = g.ox[c] + x, ay = g.oy[c] + y;
-                if (ax < g.pw[c] && ay < g.ph[c])
-                    store_sample(P.rec[c], P.bps, (size_t)ay * g.pw[c] + ax, cv.interior[c][i]);
+            const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+            const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+            const uint16_t* can = can_of(c);
+            const int CW = ReconLayout::cw_of(S);
+            const int rows = min(S, ph - oy), cols = min(S, pw - ox);
+            if ((pw & 7) == 0 && (cols & 7) == 0) {
+                const int chunks = cols >> 3;
+                for (int i = tid; i < rows * chunks; i += kReconThreads) {
+                    const int y = i / chunks, q = i % chunks;
+                    const uint4 v = *(const uint4*)(can + (y + 1) * CW + 8 + 8 * q);
+                    const size_t off = (size_t)(oy + y) * pw + ox + 8 * q;
+                    if (P.bps == 2) {
+                        *(uint4*)((uint16_t*)P.rec[c] + off) = v;
+                    } else {
+                        const uint32_t lo = (v.x & 0xffu) | ((v.x >> 8) & 0xff00u) | ((v.y & 0xffu) << 16) |
+                                            ((v.y & 0xff0000u) << 8);
+                        const uint32_t hi = (v.z & 0xffu) | ((v.z >> 8) & 0xff00u) | ((v.w & 0xffu) << 16) |
+                                            ((v.w & 0xff0000u) << 8);
+                        *(uint2*)((uint8_t*)P.rec[c] + off) = make_uint2(lo, hi);
+                    }
+                }
+            } else {
+                for (int i = tid; i < rows * cols; i += kReconThreads) {
+                    const int y = i / cols, x = i % cols;
+                    store_sample(P.rec[c], P.bps, (size_t)(oy + y) * pw + ox + x, can[(y + 1) * CW + 8 + x]);
+                }
             }
         }
         __threadfence();
         __syncthreads();
-        if (tid == 0 && P.needs_wavefront) st_release(P.ready + ci, 1u);
+        if (tid == 0) st_release(P.ready + ci, 1u);
     }
 }
 
@@ -625,9 +754,25 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
 
 extern "C" size_t hpvcd_recon_smem_bytes(int c444) { return hpvcd::ReconLayout(c444).total; }
 
+extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const uint32_t* rec_prefix,
+                                             uint32_t n_pics, uint32_t total_records, uint32_t* dev_err,
+                                             cudaStream_t stream) {
+    if (total_records == 0) return cudaSuccess;
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t blocks_needed = (total_records + hpvcd::kResWarps - 1) / hpvcd::kResWarps;
+    const uint32_t cap = (uint32_t)sms * 8u;
+    const int grid = (int)(blocks_needed < cap ? blocks_needed : cap);
+    hpvcd::k_residual<<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix, n_pics, dev_err);
+    hpvcd_note_launches(1);
+    return cudaGetLastError();
+}
+
 extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd::CtuItem* items,
                                           uint32_t n_items, uint32_t* work_counter, uint32_t* dev_err,
                                           int c444, int grid, cudaStream_t stream) {
+    if (n_items == 0) return cudaSuccess;
     const size_t smem = hpvcd::ReconLayout(c444).total;
     static bool configured[2] = {false, false};
     if (!configured[c444 ? 1 : 0]) {

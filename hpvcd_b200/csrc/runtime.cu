@@ -18,6 +18,8 @@
 using hpvcd::CtuItem;
 using hpvcd::DevPic;
 
+extern "C" cudaError_t hpvcd_launch_residual(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*,
+                                             cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int,
                                           int, cudaStream_t);
 extern "C" int hpvcd_recon_occupancy(int c444);
@@ -94,6 +96,9 @@ struct hpvcd_plan {
     std::vector<CtuItem> items;
     CtuItem* d_items = nullptr;
     std::vector<Segment> segs;
+    std::vector<uint32_t> rec_prefix;  // TB records of pictures [0, i)
+    uint32_t* d_prefix = nullptr;
+    unsigned char* d_res = nullptr;    // int16 residual planes
     uint32_t* d_scratch = nullptr;  // [seg counters][err][ready flags...]
     size_t scratch_words = 0;
     unsigned char* d_planes = nullptr;
@@ -112,6 +117,8 @@ struct hpvcd_plan {
         cudaFree(d_pics);
         cudaFree(d_items);
         cudaFree(d_scratch);
+        cudaFree(d_prefix);
+        cudaFree(d_res);
         cudaFree(d_planes);
         cudaFree(d_canvas);
     }
@@ -125,6 +132,13 @@ hpvcd_status cuda_status(cudaError_t e) {
     return HPVCD_ERR_CUDA;
 }
 
+// int16 residual planes of a picture, rows padded to 16 samples.
+inline int res_stride_of(int w) { return (w + 15) & ~15; }
+size_t res_plane_bytes(const Geo& g) {
+    return align_up((size_t)res_stride_of(g.w) * g.h * 2, 256) +
+           2 * align_up((size_t)res_stride_of(g.cw) * g.ch * 2, 256);
+}
+
 // Device bytes a plan for these pictures needs (planes, scratch, canvas).
 size_t plan_footprint(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out) {
     size_t bytes = 0;
@@ -132,6 +146,7 @@ size_t plan_footprint(const hpvcd_picture* pics, uint32_t n, const hpvcd_output*
         const Geo g = geo_of(pics[i]);
         const size_t one = align_up(g.luma_bytes, 256) + 2 * align_up(g.chroma_bytes, 256);
         bytes += one * (sao_active(pics[i]) ? 2 : 1);
+        bytes += res_plane_bytes(g);
         bytes += (size_t)g.ctb_cols * g.ctb_rows * (4 + sizeof(CtuItem));
     }
     bytes += n * sizeof(DevPic);
@@ -208,7 +223,19 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     }
     const size_t n_seg = P->segs.size();
     P->scratch_words = n_seg + 1 + ready_words;
+    size_t res_bytes = 0;
+    std::vector<size_t> res_off(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        res_off[i] = res_bytes;
+        res_bytes += res_plane_bytes(geo_of(pics[i]));
+    }
+    P->rec_prefix.assign(n + 1, 0);
+    for (uint32_t i = 0; i < n; ++i) P->rec_prefix[i + 1] = P->rec_prefix[i] + pics[i].n_tus;
     cudaError_t e = cudaMalloc(&P->d_planes, std::max<size_t>(plane_bytes, 256));
+    if (e == cudaSuccess) e = cudaMalloc(&P->d_res, std::max<size_t>(res_bytes, 256));
+    if (e == cudaSuccess) e = cudaMalloc(&P->d_prefix, sizeof(uint32_t) * (n + 1));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(P->d_prefix, P->rec_prefix.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&P->d_scratch, P->scratch_words * sizeof(uint32_t));
     if (e == cudaSuccess && P->out.kind == HPVCD_OUT_RGB8) {
         P->canvas_bytes = (size_t)P->out.canvas_w * P->out.canvas_h * 3;
@@ -257,6 +284,16 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         d.fin[2] = fb + align_up(g.luma_bytes, 256) + align_up(g.chroma_bytes, 256);
         if (!p.chroma_idc) d.rec[1] = d.rec[2] = d.fin[1] = d.fin[2] = nullptr;
         d.ready = P->d_scratch + n_seg + 1 + ready_off[i];
+        {
+            unsigned char* rb = P->d_res + res_off[i];
+            d.res_stride[0] = res_stride_of(g.w);
+            d.res_stride[1] = d.res_stride[2] = res_stride_of(g.cw);
+            const size_t ly = align_up((size_t)d.res_stride[0] * g.h * 2, 256);
+            const size_t lc = align_up((size_t)d.res_stride[1] * g.ch * 2, 256);
+            d.res[0] = (int16_t*)rb;
+            d.res[1] = p.chroma_idc ? (int16_t*)(rb + ly) : nullptr;
+            d.res[2] = p.chroma_idc ? (int16_t*)(rb + ly + lc) : nullptr;
+        }
         d.needs_wavefront = (p.flags & HPVCD_PIC_PRED_IN_PLANE) ? 0 : 1;
         if (P->out.kind == HPVCD_OUT_RGB8) {
             const hpvcd_tile_place& tp = P->places[i];
@@ -275,6 +312,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         for (int t = 0; t <= max_t; ++t)
             for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
                 const DevPic& d = P->pics[i];
+                if (!d.needs_wavefront) continue;  // prediction in plane: k_residual did it all
                 for (int y = 0; y < d.ctb_rows; ++y) {
                     const int x = t - 2 * y;
                     if (x >= 0 && x < d.ctb_cols) P->items.push_back(CtuItem{i, (uint16_t)x, (uint16_t)y});
@@ -313,7 +351,8 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     for (const Segment& s : P->segs) {
         for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
             if ((P->src[i].flags & HPVCD_PIC_INTER) && P->src[i].n_pus) ++L;
-        L += 1;                             // recon
+        if (P->rec_prefix[s.first_pic + s.n_pics] > P->rec_prefix[s.first_pic]) L += 1;  // residual
+        if (s.n_items) L += 1;                                                           // recon
         if (s.max_dbk_v > 0) L += 1;
         if (s.max_dbk_h > 0) L += 1;
         if (s.max_sao > 0) L += 1;
@@ -357,6 +396,9 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
                     e = hpvcd_launch_mc(P->d_pics, (int)i, (int)P->src[i].n_pus, P->src[i].chroma_idc ? 3 : 1, st);
                     if (e != cudaSuccess) return cuda_status(e);
                 }
+            const uint32_t nrec = P->rec_prefix[s.first_pic + s.n_pics] - P->rec_prefix[s.first_pic];
+            e = hpvcd_launch_residual(P->d_pics + s.first_pic, P->d_prefix + s.first_pic, s.n_pics, nrec, d_err, st);
+            if (e != cudaSuccess) return cuda_status(e);
             const int grid = std::max(1, std::min<int>(P->recon_grid, (int)s.n_items));
             e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
                                    P->c444, grid, st);
@@ -387,6 +429,7 @@ hpvcd_status plan_rebind(hpvcd_plan* P, const hpvcd_picture* pics, const hpvcd_w
                          cudaStream_t st) {
     for (size_t i = 0; i < P->pics.size(); ++i) {
         P->src[i] = pics[i];
+        P->rec_prefix[i + 1] = P->rec_prefix[i] + pics[i].n_tus;
         fill_inputs(P->pics[i], pics[i]);
         if (host_wp && pics[i].wp) {
             P->pics[i].wp = host_wp[i];
@@ -395,8 +438,11 @@ hpvcd_status plan_rebind(hpvcd_plan* P, const hpvcd_picture* pics, const hpvcd_w
             P->pics[i].has_wp = 0;
         }
     }
-    return cuda_status(cudaMemcpyAsync(P->d_pics, P->pics.data(), sizeof(DevPic) * P->pics.size(),
-                                       cudaMemcpyHostToDevice, st));
+    cudaError_t e = cudaMemcpyAsync(P->d_prefix, P->rec_prefix.data(), sizeof(uint32_t) * P->rec_prefix.size(),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(P->d_pics, P->pics.data(), sizeof(DevPic) * P->pics.size(), cudaMemcpyHostToDevice, st);
+    return cuda_status(e);
 }
 
 bool same_layout(const hpvcd_plan* P, const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out) {
