@@ -59,6 +59,7 @@ MATRIX_SMPTE170M, MATRIX_YCGCO, MATRIX_BT2020NCL = 6, 8, 9
 
 STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_OUTPUT = 0x1, 0x2, 0x4, 0x8
 STAGE_ALL = 0xF
+STAGE_GRAPH = 0x100
 
 SYNTH_RESIDUAL, SYNTH_INTRA, SYNTH_INTER = 0, 1, 2
 
@@ -142,13 +143,39 @@ class Picture(C.Structure):
 
 class TilePlace(C.Structure):
     _fields_ = [("dst_x", C.c_uint32), ("dst_y", C.c_uint32), ("crop_w", C.c_uint32),
-                ("crop_h", C.c_uint32)]
+                ("crop_h", C.c_uint32), ("canvas", C.c_uint32)]
+
+
+class Canvas(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("matrix", C.c_uint32),
+                ("full_range", C.c_uint32)]
 
 
 class Output(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("matrix", C.c_uint32), ("full_range", C.c_uint32),
                 ("canvas_w", C.c_uint32), ("canvas_h", C.c_uint32), ("place", C.c_void_p),
-                ("host_dst", C.c_void_p), ("host_dst_bytes", C.c_uint64)]
+                ("host_dst", C.c_void_p), ("host_dst_bytes", C.c_uint64),
+                ("n_canvases", C.c_uint32), ("canvases", C.c_void_p), ("canvas_dst", C.c_void_p)]
+
+
+class ServerCfg(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_inflight", C.c_uint32), ("max_batch_pictures", C.c_uint32),
+                ("max_batch_bytes", C.c_uint64), ("hbm_budget", C.c_uint64), ("batching", C.c_uint32),
+                ("batch_window_us", C.c_uint32)]
+
+
+class Request(C.Structure):
+    _fields_ = [("pics", C.c_void_p), ("n_pics", C.c_uint32), ("place", C.c_void_p),
+                ("canvas", Canvas), ("dst", C.c_void_p), ("dst_bytes", C.c_uint64), ("user", C.c_uint64),
+                ("flags", C.c_uint32)]
+
+
+REQ_ZERO_COPY = 0x1
+
+
+class Completion(C.Structure):
+    _fields_ = [("user", C.c_uint64), ("status", C.c_int32), ("batch_pictures", C.c_uint32),
+                ("latency_ms", C.c_double), ("queue_ms", C.c_double)]
 
 
 class GpuCfg(C.Structure):
@@ -198,6 +225,7 @@ def lib() -> C.CDLL:
             "hpvcd_abi_version": (u32, []),
             "hpvcd_status_string": (C.c_char_p, [C.c_int]),
             "hpvcd_kernel_launch_count": (u64, []),
+            "hpvcd_last_error_string": (C.c_char_p, []),
             "hpvcd_gpu_create": (i32, [C.POINTER(GpuCfg), C.POINTER(vp)]),
             "hpvcd_gpu_destroy": (i32, [vp]),
             "hpvcd_gpu_submit": (i32, [vp, C.POINTER(Picture), u32, C.POINTER(Output), C.POINTER(u64)]),
@@ -214,6 +242,11 @@ def lib() -> C.CDLL:
             "hpvcd_abi_sizeof": (u64, [C.c_char_p]),
             "hpvcd_copy": (i32, [vp, vp, u64, vp]),
             "hpvcd_gpu_packed_size": (u64, [C.POINTER(Picture), u32]),
+            "hpvcd_server_create": (i32, [C.POINTER(ServerCfg), C.POINTER(vp)]),
+            "hpvcd_server_submit": (i32, [vp, C.POINTER(Request)]),
+            "hpvcd_server_poll": (u32, [vp, C.POINTER(Completion), u32, i32]),
+            "hpvcd_server_pending": (u32, [vp]),
+            "hpvcd_server_destroy": (i32, [vp]),
             "hpvcd_gpu_pack_inputs": (i32, [C.POINTER(Picture), u32, vp, u64, C.POINTER(Picture)]),
         }
         for name, (res, args) in sig.items():
@@ -247,4 +280,7 @@ def synth_lib() -> C.CDLL:
 
 def check(status: int, what: str) -> None:
     if status != OK:
-        raise HpvcdError(status, what)
+        detail = ""
+        if status == ERR_CUDA and _lib is not None:
+            detail = " [" + (_lib.hpvcd_last_error_string() or b"").decode(errors="replace") + "]"
+        raise HpvcdError(status, what + detail)

@@ -37,8 +37,10 @@ struct DevPic {
     int16_t* res[3];        // int16 residual planes of intra TBs (k_residual -> k_recon)
     int32_t res_stride[3];  // row stride of res[c] in samples (multiple of 16)
     uint32_t* ready;  // per-CTU ready flags (wavefront)
-    // output placement on the RGB canvas
+    // output placement on its RGB canvas
     int32_t dst_x, dst_y, crop_w, crop_h;
+    uint64_t canvas_off;  // byte offset of the picture's canvas in the output
+    int32_t canvas_w, canvas_h, matrix, full_range;
     int32_t needs_wavefront;
 };
 

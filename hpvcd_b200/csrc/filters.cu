@@ -261,8 +261,10 @@ struct RgbParams {
     int matrix, full_range, canvas_w, canvas_h;
 };
 
-__global__ void k_rgb(const DevPic* __restrict__ pics, RgbParams rp, uint8_t* __restrict__ canvas) {
+__global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out) {
     const DevPic& P = pics[blockIdx.y];
+    const RgbParams rp{P.matrix, P.full_range, P.canvas_w, P.canvas_h};
+    uint8_t* canvas = out + P.canvas_off;
     const int tw = P.crop_w, th = P.crop_h;
     const int copy_w = min(tw, max(rp.canvas_w - P.dst_x, 0));
     const int copy_h = min(th, max(rp.canvas_h - P.dst_y, 0));
@@ -345,14 +347,12 @@ extern "C" cudaError_t hpvcd_launch_sao(const hpvcd::DevPic* pics, int n_pics, i
     return cudaGetLastError();
 }
 
-extern "C" cudaError_t hpvcd_launch_rgb(const hpvcd::DevPic* pics, int n_pics, int max_pixels, int matrix,
-                                        int full_range, int canvas_w, int canvas_h, uint8_t* canvas,
+extern "C" cudaError_t hpvcd_launch_rgb(const hpvcd::DevPic* pics, int n_pics, int max_pixels, uint8_t* out,
                                         cudaStream_t stream) {
     if (n_pics <= 0 || max_pixels <= 0) return cudaSuccess;
     const int threads = 256;
     dim3 grid((max_pixels + threads - 1) / threads, n_pics, 1);
-    hpvcd::RgbParams rp{matrix, full_range, canvas_w, canvas_h};
-    hpvcd::k_rgb<<<grid, threads, 0, stream>>>(pics, rp, canvas);
+    hpvcd::k_rgb<<<grid, threads, 0, stream>>>(pics, out);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }

@@ -756,11 +756,8 @@ extern "C" size_t hpvcd_recon_smem_bytes(int c444) { return hpvcd::ReconLayout(c
 
 extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const uint32_t* rec_prefix,
                                              uint32_t n_pics, uint32_t total_records, uint32_t* dev_err,
-                                             cudaStream_t stream) {
+                                             int sms, cudaStream_t stream) {
     if (total_records == 0) return cudaSuccess;
-    int sms = 148, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t blocks_needed = (total_records + hpvcd::kResWarps - 1) / hpvcd::kResWarps;
     const uint32_t cap = (uint32_t)sms * 8u;
     const int grid = (int)(blocks_needed < cap ? blocks_needed : cap);
@@ -773,14 +770,10 @@ extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd
                                           uint32_t n_items, uint32_t* work_counter, uint32_t* dev_err,
                                           int c444, int grid, cudaStream_t stream) {
     if (n_items == 0) return cudaSuccess;
+    // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
+    // when the plan was built (no non-stream API call here, so launches can
+    // be captured into CUDA graphs)
     const size_t smem = hpvcd::ReconLayout(c444).total;
-    static bool configured[2] = {false, false};
-    if (!configured[c444 ? 1 : 0]) {
-        cudaError_t e = cudaFuncSetAttribute(hpvcd::k_recon, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        configured[c444 ? 1 : 0] = true;
-    }
     // 2^22 polls of >= 64 ns each bound one neighbour wait to a few hundred ms.
     hpvcd::k_recon<<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
                                                                  dev_err, c444, 1u << 22);
@@ -790,8 +783,10 @@ extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd
 
 extern "C" int hpvcd_recon_occupancy(int c444) {
     int blocks = 0;
+    // raise the limit for the larger layout, which covers both
     const size_t smem = hpvcd::ReconLayout(c444).total;
-    cudaFuncSetAttribute(hpvcd::k_recon, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(hpvcd::k_recon, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)hpvcd::ReconLayout(1).total);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon, hpvcd::kReconThreads, smem);
     return blocks;
 }

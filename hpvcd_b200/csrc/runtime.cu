@@ -18,14 +18,14 @@
 using hpvcd::CtuItem;
 using hpvcd::DevPic;
 
-extern "C" cudaError_t hpvcd_launch_residual(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*,
+extern "C" cudaError_t hpvcd_launch_residual(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int,
                                              cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int,
                                           int, cudaStream_t);
 extern "C" int hpvcd_recon_occupancy(int c444);
 extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, cudaStream_t);
-extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, int, int, int, int, uint8_t*, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, uint8_t*, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_mc(const DevPic*, int, int, int, cudaStream_t);
 
 static std::atomic<uint64_t> g_launches{0};
@@ -107,27 +107,69 @@ struct hpvcd_plan {
     size_t canvas_bytes = 0;
     hpvcd_output out{};
     std::vector<hpvcd_tile_place> places;
+    std::vector<hpvcd_canvas> canvases;   // resolved canvas list (>= 1 for RGB8)
+    std::vector<uint64_t> canvas_offs;
     hpvcd_sched sched{};
     int c444 = 0;
     int recon_grid = 0;
+    int sms = 148;
     int max_rgb = 0;
     uint32_t launches_per_run = 0;
+    // Plans owned by a context allocate from the stream-ordered pool of the
+    // ticket's stream (no device-wide synchronisation when the layout of a
+    // serving batch changes); public plans use plain cudaMalloc.
+    cudaStream_t alloc_stream = nullptr;
+    bool pooled = false;
+    cudaGraphExec_t graphs[16] = {};  // captured launch sequences by stage mask
 
+    uint32_t launches_for(uint32_t stages) const {
+        uint32_t L = 0;
+        for (const auto& s : segs) {
+            if (stages & HPVCD_STAGE_RECON) {
+                for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
+                    if ((src[i].flags & HPVCD_PIC_INTER) && src[i].n_pus) ++L;
+                if (rec_prefix[s.first_pic + s.n_pics] > rec_prefix[s.first_pic]) ++L;
+                if (s.n_items) ++L;
+            }
+            if (stages & HPVCD_STAGE_DEBLOCK) L += (s.max_dbk_v > 0) + (s.max_dbk_h > 0);
+            if ((stages & HPVCD_STAGE_SAO) && s.max_sao > 0) ++L;
+        }
+        if ((stages & HPVCD_STAGE_OUTPUT) && out.kind == HPVCD_OUT_RGB8 && max_rgb > 0) ++L;
+        return L;
+    }
+
+    template <typename T>
+    cudaError_t dmalloc(T** p, size_t bytes) {
+        bytes = bytes ? bytes : 256;
+        return pooled ? cudaMallocAsync((void**)p, bytes, alloc_stream) : cudaMalloc((void**)p, bytes);
+    }
+    void dfree(void* p) {
+        if (!p) return;
+        if (pooled)
+            cudaFreeAsync(p, alloc_stream);
+        else
+            cudaFree(p);
+    }
     ~hpvcd_plan() {
-        cudaFree(d_pics);
-        cudaFree(d_items);
-        cudaFree(d_scratch);
-        cudaFree(d_prefix);
-        cudaFree(d_res);
-        cudaFree(d_planes);
-        cudaFree(d_canvas);
+        for (cudaGraphExec_t& gx : graphs)
+            if (gx) cudaGraphExecDestroy(gx);
+        dfree(d_pics);
+        dfree(d_items);
+        dfree(d_scratch);
+        dfree(d_prefix);
+        dfree(d_res);
+        dfree(d_planes);
+        dfree(d_canvas);
     }
 };
 
 namespace {
 
+thread_local char t_last_error[256] = "";
+
 hpvcd_status cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return HPVCD_OK;
+    std::snprintf(t_last_error, sizeof(t_last_error), "%s: %s", cudaGetErrorName(e), cudaGetErrorString(e));
     if (e == cudaErrorMemoryAllocation) return HPVCD_ERR_ALLOC;
     return HPVCD_ERR_CUDA;
 }
@@ -137,6 +179,25 @@ inline int res_stride_of(int w) { return (w + 15) & ~15; }
 size_t res_plane_bytes(const Geo& g) {
     return align_up((size_t)res_stride_of(g.w) * g.h * 2, 256) +
            2 * align_up((size_t)res_stride_of(g.cw) * g.ch * 2, 256);
+}
+
+// Bytes of the output of a batch: all RGB8 canvases, or all YUV planes.
+size_t output_bytes(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out) {
+    size_t b = 0;
+    if (out && out->kind == HPVCD_OUT_RGB8) {
+        if (out->n_canvases) {
+            for (uint32_t k = 0; k < out->n_canvases; ++k)
+                b += (size_t)out->canvases[k].width * out->canvases[k].height * 3;
+        } else {
+            b = (size_t)out->canvas_w * out->canvas_h * 3;
+        }
+        return b;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const Geo geo = geo_of(pics[i]);
+        b += geo.luma_bytes + 2 * geo.chroma_bytes;
+    }
+    return b;
 }
 
 // Device bytes a plan for these pictures needs (planes, scratch, canvas).
@@ -150,7 +211,7 @@ size_t plan_footprint(const hpvcd_picture* pics, uint32_t n, const hpvcd_output*
         bytes += (size_t)g.ctb_cols * g.ctb_rows * (4 + sizeof(CtuItem));
     }
     bytes += n * sizeof(DevPic);
-    if (out && out->kind == HPVCD_OUT_RGB8) bytes += (size_t)out->canvas_w * out->canvas_h * 3;
+    bytes += output_bytes(pics, n, out);
     return bytes;
 }
 
@@ -168,16 +229,20 @@ void fill_inputs(DevPic& d, const hpvcd_picture& p) {
 }
 
 hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out,
-                        const hpvcd_sched* sched, const hpvcd_wp_table* host_wp, hpvcd_plan** result) {
+                        const hpvcd_sched* sched, const hpvcd_wp_table* host_wp, hpvcd_plan** result,
+                        cudaStream_t pool_stream = nullptr, bool pooled = false) {
     if (!pics || n == 0 || !result) return HPVCD_ERR_INVALID_ARG;
     for (uint32_t i = 0; i < n; ++i) {
         const hpvcd_status s = validate(pics[i]);
         if (s != HPVCD_OK) return s;
     }
-    if (out && out->kind == HPVCD_OUT_RGB8 && (!out->place || out->canvas_w == 0 || out->canvas_h == 0))
+    if (out && out->kind == HPVCD_OUT_RGB8 &&
+        (!out->place || (out->n_canvases ? !out->canvases : (out->canvas_w == 0 || out->canvas_h == 0))))
         return HPVCD_ERR_INVALID_ARG;
     hpvcd_plan* P = new (std::nothrow) hpvcd_plan();
     if (!P) return HPVCD_ERR_ALLOC;
+    P->alloc_stream = pool_stream;
+    P->pooled = pooled;
     cudaGetDevice(&P->device);
     P->src.assign(pics, pics + n);
     if (out) {
@@ -185,6 +250,22 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         if (out->kind == HPVCD_OUT_RGB8) {
             P->places.assign(out->place, out->place + n);
             P->out.place = nullptr;
+            if (out->n_canvases) {
+                P->canvases.assign(out->canvases, out->canvases + out->n_canvases);
+            } else {
+                P->canvases.push_back(hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix, out->full_range});
+            }
+            P->out.canvases = nullptr;
+            uint64_t off = 0;
+            for (const hpvcd_canvas& cv : P->canvases) {
+                P->canvas_offs.push_back(off);
+                off += (uint64_t)cv.width * cv.height * 3;
+            }
+            for (uint32_t i = 0; i < n; ++i)
+                if (P->places[i].canvas >= P->canvases.size()) {
+                    delete P;
+                    return HPVCD_ERR_INVALID_ARG;
+                }
         }
     } else {
         P->out.kind = HPVCD_OUT_YUV;
@@ -231,16 +312,18 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     }
     P->rec_prefix.assign(n + 1, 0);
     for (uint32_t i = 0; i < n; ++i) P->rec_prefix[i + 1] = P->rec_prefix[i] + pics[i].n_tus;
-    cudaError_t e = cudaMalloc(&P->d_planes, std::max<size_t>(plane_bytes, 256));
-    if (e == cudaSuccess) e = cudaMalloc(&P->d_res, std::max<size_t>(res_bytes, 256));
-    if (e == cudaSuccess) e = cudaMalloc(&P->d_prefix, sizeof(uint32_t) * (n + 1));
+    cudaError_t e = P->dmalloc(&P->d_planes, plane_bytes);
+    if (e == cudaSuccess) e = P->dmalloc(&P->d_res, res_bytes);
+    if (e == cudaSuccess) e = P->dmalloc(&P->d_prefix, sizeof(uint32_t) * (n + 1));
     if (e == cudaSuccess)
-        e = cudaMemcpy(P->d_prefix, P->rec_prefix.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc(&P->d_scratch, P->scratch_words * sizeof(uint32_t));
+        e = cudaMemcpyAsync(P->d_prefix, P->rec_prefix.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice,
+                            pool_stream);
+    if (e == cudaSuccess) e = P->dmalloc(&P->d_scratch, P->scratch_words * sizeof(uint32_t));
     if (e == cudaSuccess && P->out.kind == HPVCD_OUT_RGB8) {
-        P->canvas_bytes = (size_t)P->out.canvas_w * P->out.canvas_h * 3;
-        e = cudaMalloc(&P->d_canvas, P->canvas_bytes);
-        if (e == cudaSuccess) e = cudaMemset(P->d_canvas, 0, P->canvas_bytes);
+        P->canvas_bytes = 0;
+        for (const hpvcd_canvas& cv : P->canvases) P->canvas_bytes += (size_t)cv.width * cv.height * 3;
+        e = P->dmalloc(&P->d_canvas, P->canvas_bytes);
+        if (e == cudaSuccess) e = cudaMemsetAsync(P->d_canvas, 0, P->canvas_bytes, pool_stream);
     }
     if (e != cudaSuccess) {
         delete P;
@@ -297,6 +380,10 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         d.needs_wavefront = (p.flags & HPVCD_PIC_PRED_IN_PLANE) ? 0 : 1;
         if (P->out.kind == HPVCD_OUT_RGB8) {
             const hpvcd_tile_place& tp = P->places[i];
+            const hpvcd_canvas& cv = P->canvases[tp.canvas];
+            d.canvas_off = P->canvas_offs[tp.canvas];
+            d.canvas_w = (int)cv.width; d.canvas_h = (int)cv.height;
+            d.matrix = (int)cv.matrix; d.full_range = (int)cv.full_range;
             d.dst_x = (int)tp.dst_x; d.dst_y = (int)tp.dst_y;
             d.crop_w = (int)std::min<uint32_t>(tp.crop_w, p.width);
             d.crop_h = (int)std::min<uint32_t>(tp.crop_h, p.height);
@@ -330,11 +417,16 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             if (d.rec[0] != d.fin[0]) s.max_sao = std::max(s.max_sao, d.w * d.h);
         }
     }
-    e = cudaMalloc(&P->d_pics, sizeof(DevPic) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&P->d_items, sizeof(CtuItem) * std::max<size_t>(P->items.size(), 1));
-    if (e == cudaSuccess) e = cudaMemcpy(P->d_pics, P->pics.data(), sizeof(DevPic) * n, cudaMemcpyHostToDevice);
+    e = P->dmalloc(&P->d_pics, sizeof(DevPic) * n);
+    if (e == cudaSuccess) e = P->dmalloc(&P->d_items, sizeof(CtuItem) * std::max<size_t>(P->items.size(), 1));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(P->d_pics, P->pics.data(), sizeof(DevPic) * n, cudaMemcpyHostToDevice, pool_stream);
     if (e == cudaSuccess && !P->items.empty())
-        e = cudaMemcpy(P->d_items, P->items.data(), sizeof(CtuItem) * P->items.size(), cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(P->d_items, P->items.data(), sizeof(CtuItem) * P->items.size(), cudaMemcpyHostToDevice,
+                            pool_stream);
+    // host vectors are pageable: the copies above are staged before returning,
+    // but make the plan's first use ordered after them for plain plans too
+    if (e == cudaSuccess && !pooled) e = cudaStreamSynchronize(pool_stream);
     if (e != cudaSuccess) {
         delete P;
         cudaGetLastError();
@@ -342,23 +434,12 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
+    P->sms = sms;
     int occ = hpvcd_recon_occupancy(P->c444);
     if (occ <= 0) occ = 1;
     if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
     P->recon_grid = sms * occ;
-    // launches per full run
-    uint32_t L = 0;
-    for (const Segment& s : P->segs) {
-        for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
-            if ((P->src[i].flags & HPVCD_PIC_INTER) && P->src[i].n_pus) ++L;
-        if (P->rec_prefix[s.first_pic + s.n_pics] > P->rec_prefix[s.first_pic]) L += 1;  // residual
-        if (s.n_items) L += 1;                                                           // recon
-        if (s.max_dbk_v > 0) L += 1;
-        if (s.max_dbk_h > 0) L += 1;
-        if (s.max_sao > 0) L += 1;
-    }
-    if (P->out.kind == HPVCD_OUT_RGB8 && P->max_rgb > 0) L += 1;
-    P->launches_per_run = L;
+    P->launches_per_run = P->launches_for(HPVCD_STAGE_ALL);
     *result = P;
     return HPVCD_OK;
 }
@@ -397,7 +478,8 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
                     if (e != cudaSuccess) return cuda_status(e);
                 }
             const uint32_t nrec = P->rec_prefix[s.first_pic + s.n_pics] - P->rec_prefix[s.first_pic];
-            e = hpvcd_launch_residual(P->d_pics + s.first_pic, P->d_prefix + s.first_pic, s.n_pics, nrec, d_err, st);
+            e = hpvcd_launch_residual(P->d_pics + s.first_pic, P->d_prefix + s.first_pic, s.n_pics, nrec, d_err,
+                                      P->sms, st);
             if (e != cudaSuccess) return cuda_status(e);
             const int grid = std::max(1, std::min<int>(P->recon_grid, (int)s.n_items));
             e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
@@ -415,9 +497,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
         }
     }
     if ((stages & HPVCD_STAGE_OUTPUT) && P->out.kind == HPVCD_OUT_RGB8) {
-        e = hpvcd_launch_rgb(P->d_pics, (int)P->pics.size(), P->max_rgb, (int)P->out.matrix,
-                             (int)P->out.full_range, (int)P->out.canvas_w, (int)P->out.canvas_h, P->d_canvas,
-                             st);
+        e = hpvcd_launch_rgb(P->d_pics, (int)P->pics.size(), P->max_rgb, P->d_canvas, st);
         if (e != cudaSuccess) return cuda_status(e);
     }
     return HPVCD_OK;
@@ -462,9 +542,14 @@ bool same_layout(const hpvcd_plan* P, const hpvcd_picture* pics, uint32_t n, con
     const uint32_t kind = out ? out->kind : HPVCD_OUT_YUV;
     if (kind != P->out.kind) return false;
     if (kind == HPVCD_OUT_RGB8) {
-        if (out->matrix != P->out.matrix || out->full_range != P->out.full_range ||
-            out->canvas_w != P->out.canvas_w || out->canvas_h != P->out.canvas_h)
-            return false;
+        const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
+        if (nc != P->canvases.size()) return false;
+        for (uint32_t k = 0; k < nc; ++k) {
+            const hpvcd_canvas c = out->n_canvases ? out->canvases[k]
+                                                   : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix,
+                                                                  out->full_range};
+            if (std::memcmp(&c, &P->canvases[k], sizeof(c)) != 0) return false;
+        }
         for (uint32_t i = 0; i < n; ++i)
             if (std::memcmp(&out->place[i], &P->places[i], sizeof(hpvcd_tile_place)) != 0) return false;
     }
@@ -506,6 +591,7 @@ struct hpvcd_gpu {
         for (Slot& s : slots) {
             if (s.stream) cudaStreamSynchronize(s.stream);
             delete s.plan;
+            if (s.stream) cudaStreamSynchronize(s.stream);
             cudaFreeHost(s.h_in);
             cudaFreeHost(s.h_out);
             cudaFree(s.d_in);
@@ -642,6 +728,8 @@ HPVCD_API const char* hpvcd_status_string(int s) {
 
 HPVCD_API uint64_t hpvcd_kernel_launch_count(void) { return g_launches.load(); }
 
+HPVCD_API const char* hpvcd_last_error_string(void) { return t_last_error; }
+
 HPVCD_API hpvcd_status hpvcd_copy(void* dst, const void* src, uint64_t bytes, void* stream) {
     if ((!dst || !src) && bytes) return HPVCD_ERR_INVALID_ARG;
     if (!bytes) return HPVCD_OK;
@@ -661,6 +749,8 @@ HPVCD_API uint64_t hpvcd_abi_sizeof(const char* name) {
              {"hpvcd_pu", sizeof(hpvcd_pu)},           {"hpvcd_wp_entry", sizeof(hpvcd_wp_entry)},
              {"hpvcd_wp_table", sizeof(hpvcd_wp_table)}, {"hpvcd_picture", sizeof(hpvcd_picture)},
              {"hpvcd_tile_place", sizeof(hpvcd_tile_place)}, {"hpvcd_output", sizeof(hpvcd_output)},
+             {"hpvcd_canvas", sizeof(hpvcd_canvas)}, {"hpvcd_server_cfg", sizeof(hpvcd_server_cfg)},
+             {"hpvcd_request", sizeof(hpvcd_request)}, {"hpvcd_completion", sizeof(hpvcd_completion)},
              {"hpvcd_gpu_cfg", sizeof(hpvcd_gpu_cfg)}, {"hpvcd_sched", sizeof(hpvcd_sched)}};
     for (const auto& e : t)
         if (std::strcmp(e.n, name) == 0) return e.s;
@@ -694,7 +784,35 @@ HPVCD_API hpvcd_status hpvcd_plan_destroy(hpvcd_plan* plan) {
 
 HPVCD_API hpvcd_status hpvcd_plan_launch(hpvcd_plan* plan, uint32_t stages, void* stream) {
     if (!plan) return HPVCD_ERR_INVALID_ARG;
-    return plan_launch(plan, stages, (cudaStream_t)stream);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!(stages & HPVCD_STAGE_GRAPH)) return plan_launch(plan, stages, st);
+    if (st == nullptr || st == cudaStreamLegacy) return HPVCD_ERR_INVALID_ARG;
+    const uint32_t key = stages & HPVCD_STAGE_ALL;
+    cudaGraphExec_t& gx = plan->graphs[key];
+    if (!gx) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_status(e);
+        const uint64_t before = g_launches.load();
+        const hpvcd_status ls = plan_launch(plan, key, st);
+        e = cudaStreamEndCapture(st, &g);
+        // captured launches did not run: do not count them
+        g_launches.store(before);
+        if (ls != HPVCD_OK) {
+            if (g) cudaGraphDestroy(g);
+            return ls;
+        }
+        if (e != cudaSuccess) return cuda_status(e);
+        e = cudaGraphInstantiate(&gx, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            gx = nullptr;
+            return cuda_status(e);
+        }
+    }
+    const cudaError_t e = cudaGraphLaunch(gx, st);
+    if (e == cudaSuccess) hpvcd_note_launches(plan->launches_for(key));
+    return cuda_status(e);
 }
 
 HPVCD_API hpvcd_status hpvcd_plan_planes(hpvcd_plan* plan, uint32_t i, void** y, void** cb, void** cr) {
@@ -741,6 +859,15 @@ HPVCD_API hpvcd_status hpvcd_gpu_create(const hpvcd_gpu_cfg* cfg, hpvcd_gpu** ou
     g->budget = c.hbm_budget ? c.hbm_budget : (uint64_t)(free_b * 0.8);
     const uint32_t inflight = c.max_inflight ? std::min<uint32_t>(c.max_inflight, 64) : 4;
     g->slots.resize(inflight);
+    {
+        // keep freed plan memory in the device pool for the next batch
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, c.device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+        cudaGetLastError();
+    }
     for (Slot& s : g->slots) {
         if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) {
@@ -767,7 +894,8 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         const hpvcd_status s = validate(pics[i]);
         if (s != HPVCD_OK) return s;
     }
-    if (out && out->kind == HPVCD_OUT_RGB8 && (!out->place || !out->canvas_w || !out->canvas_h))
+    if (out && out->kind == HPVCD_OUT_RGB8 &&
+        (!out->place || (out->n_canvases ? !out->canvases : (!out->canvas_w || !out->canvas_h))))
         return HPVCD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g->mu);
     cudaSetDevice(g->device);
@@ -786,28 +914,33 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         d.tus = nullptr; d.ctu_tu_start = nullptr; d.coeffs = nullptr; d.cells = nullptr;
         d.sao = nullptr; d.pus = nullptr; d.pred[0] = d.pred[1] = d.pred[2] = nullptr;
     }
-    // A packed batch in page-locked memory goes up in one DMA.
-    const unsigned char* packed_base = nullptr;
-    if (!parts.empty()) {
-        const unsigned char* base = (const unsigned char*)parts[0].src - parts[0].off;
-        bool packed = true;
-        for (const InputPart& pt : parts)
-            if ((const unsigned char*)pt.src - pt.off != base) {
-                packed = false;
-                break;
+    // Runs of parts laid out contiguously (as hpvcd_gpu_pack_inputs lays them
+    // out) in page-locked memory go up by DMA straight from the caller's
+    // memory, one transfer per run; everything else through the staging copy.
+    struct Run {
+        const unsigned char* src;
+        size_t off, bytes;
+        bool pinned;
+    };
+    std::vector<Run> runs;
+    for (const InputPart& pt : parts) {
+        const unsigned char* sp = (const unsigned char*)pt.src;
+        if (!runs.empty()) {
+            Run& r = runs.back();
+            if (sp - pt.off == r.src - r.off && pt.off >= r.off + r.bytes) {
+                r.bytes = pt.off + pt.bytes - r.off;
+                continue;
             }
-        if (packed && is_pinned(base)) packed_base = base;
+        }
+        runs.push_back(Run{sp, pt.off, pt.bytes, false});
+    }
+    bool all_pinned = !runs.empty();
+    for (Run& r : runs) {
+        r.pinned = is_pinned(r.src);
+        all_pinned &= r.pinned;
     }
     // ---- HBM admission ----
-    const size_t out_bytes = [&]() -> size_t {
-        if (out && out->kind == HPVCD_OUT_RGB8) return (size_t)out->canvas_w * out->canvas_h * 3;
-        size_t b = 0;
-        for (uint32_t i = 0; i < n; ++i) {
-            const Geo geo = geo_of(pics[i]);
-            b += geo.luma_bytes + 2 * geo.chroma_bytes;
-        }
-        return b;
-    }();
+    const size_t out_bytes = output_bytes(pics, n, out);
     const bool reuse = slot->plan && same_layout(slot->plan, pics, n, out);
     // HBM admission: what this slot would hold after the call (input arena +
     // plan) against what it holds now; refuse when the context budget would
@@ -816,17 +949,22 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     const uint64_t plan_bytes = reuse ? slot->plan_bytes : plan_footprint(pics, n, out);
     const uint64_t need = std::max<uint64_t>(slot->d_in_cap, align_up(total + total / 4, 1 << 20)) + plan_bytes;
     if (g->in_use - held + need > g->budget) return HPVCD_ERR_ALLOC;
-    const bool direct_out = out && out->host_dst && out->host_dst_bytes >= out_bytes && is_pinned(out->host_dst);
-    hpvcd_status st = packed_base ? HPVCD_OK : grow_pinned(&slot->h_in, &slot->h_in_cap, total);
+    const bool per_canvas_out = out && out->kind == HPVCD_OUT_RGB8 && out->n_canvases && out->canvas_dst;
+    const bool direct_out = per_canvas_out ||
+                            (out && out->host_dst && out->host_dst_bytes >= out_bytes && is_pinned(out->host_dst));
+    hpvcd_status st = all_pinned ? HPVCD_OK : grow_pinned(&slot->h_in, &slot->h_in_cap, total);
     if (st == HPVCD_OK) st = grow_device(&slot->d_in, &slot->d_in_cap, std::max<size_t>(total, 256));
     if (st == HPVCD_OK && !direct_out) st = grow_pinned(&slot->h_out, &slot->h_out_cap, out_bytes);
     if (st != HPVCD_OK) return st;
-    cudaError_t e;
-    if (packed_base) {
-        e = cudaMemcpyAsync(slot->d_in, packed_base, total, cudaMemcpyHostToDevice, slot->stream);
+    cudaError_t e = cudaSuccess;
+    if (all_pinned) {
+        for (const Run& r : runs) {
+            e = cudaMemcpyAsync(slot->d_in + r.off, r.src, r.bytes, cudaMemcpyHostToDevice, slot->stream);
+            if (e != cudaSuccess) break;
+        }
     } else {
         for (const InputPart& pt : parts) std::memcpy(slot->h_in + pt.off, pt.src, pt.bytes);
-        e = cudaMemcpyAsync(slot->d_in, slot->h_in, total, cudaMemcpyHostToDevice, slot->stream);
+        if (total) e = cudaMemcpyAsync(slot->d_in, slot->h_in, total, cudaMemcpyHostToDevice, slot->stream);
     }
     if (e != cudaSuccess) return cuda_status(e);
     for (const InputPart& pt : parts) point_at(dev[pt.pic], pt.kind, slot->d_in + pt.off);
@@ -843,12 +981,12 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         st = plan_rebind(slot->plan, dev.data(), any_wp ? slot->wp.data() : nullptr, slot->stream);
     } else {
         if (slot->plan) {
-            cudaStreamSynchronize(slot->stream);
-            delete slot->plan;
+            delete slot->plan;  // stream-ordered frees on slot->stream
             slot->plan = nullptr;
             slot->plan_bytes = 0;
         }
-        st = plan_build(dev.data(), n, out, nullptr, any_wp ? slot->wp.data() : nullptr, &slot->plan);
+        st = plan_build(dev.data(), n, out, nullptr, any_wp ? slot->wp.data() : nullptr, &slot->plan,
+                        slot->stream, true);
         slot->plan_bytes = st == HPVCD_OK ? plan_bytes : 0;
     }
     g->in_use = g->in_use - held + slot->d_in_cap + slot->plan_bytes;
@@ -858,9 +996,14 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     if (st != HPVCD_OK) return st;
     // ---- output copy back ----
     hpvcd_plan* P = slot->plan;
-    unsigned char* host_out = direct_out ? (unsigned char*)out->host_dst : slot->h_out;
-    slot->direct_out = direct_out ? out->host_dst : nullptr;
-    if (P->out.kind == HPVCD_OUT_RGB8) {
+    unsigned char* host_out = direct_out && !per_canvas_out ? (unsigned char*)out->host_dst : slot->h_out;
+    slot->direct_out = direct_out ? (per_canvas_out ? (void*)1 : out->host_dst) : nullptr;
+    if (per_canvas_out) {  // each canvas straight into its own buffer
+        for (size_t k = 0; k < P->canvases.size() && e == cudaSuccess; ++k)
+            e = cudaMemcpyAsync(out->canvas_dst[k], P->d_canvas + P->canvas_offs[k],
+                                (size_t)P->canvases[k].width * P->canvases[k].height * 3, cudaMemcpyDeviceToHost,
+                                slot->stream);
+    } else if (P->out.kind == HPVCD_OUT_RGB8) {
         e = cudaMemcpyAsync(host_out, P->d_canvas, P->canvas_bytes, cudaMemcpyDeviceToHost, slot->stream);
     } else {
         size_t o = 0;
@@ -935,16 +1078,17 @@ HPVCD_API hpvcd_status hpvcd_gpu_output_size(hpvcd_gpu* g, hpvcd_ticket t, uint6
 }
 
 HPVCD_API hpvcd_status hpvcd_gpu_read(hpvcd_gpu* g, hpvcd_ticket t, void* dst, uint64_t bytes) {
-    if (!g || !dst) return HPVCD_ERR_INVALID_ARG;
+    if (!g) return HPVCD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g->mu);
     Slot* s = find_ticket(g, t);
     if (!s) return HPVCD_ERR_INVALID_ARG;
-    if (bytes < s->out_bytes) return HPVCD_ERR_INVALID_ARG;
+    // outputs DMA'd to per-canvas destinations need no buffer here
+    if (s->direct_out != (void*)1 && (!dst || bytes < s->out_bytes)) return HPVCD_ERR_INVALID_ARG;
     cudaSetDevice(g->device);
     cudaError_t e = cudaEventSynchronize(s->done);
     hpvcd_status st = cuda_status(e);
     if (st == HPVCD_OK) st = device_status(s->plan, s->stream);
-    if (st == HPVCD_OK && dst != s->direct_out)
+    if (st == HPVCD_OK && s->direct_out != (void*)1 && dst != s->direct_out)
         std::memcpy(dst, s->direct_out ? (const unsigned char*)s->direct_out : s->h_out, s->out_bytes);
     s->busy = false;
     s->ticket = 0;

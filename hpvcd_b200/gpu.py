@@ -252,3 +252,78 @@ class DevicePlan:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# Serving loop (hpvcd_server_*): continuous batching of decode requests.
+# ---------------------------------------------------------------------------
+
+class Server:
+    """Requests (one image each: its grid tiles + an RGB8 destination) are
+    queued; a native worker fuses everything queued into one launch whenever
+    a GPU slot frees.  `batching=False` gives the plain one-image-per-launch
+    path with the same machinery."""
+
+    def __init__(self, device: int = 0, max_inflight: int = 2, batching: bool = True,
+                 max_batch_pictures: int = 0, max_batch_bytes: int = 0, hbm_budget: int = 0,
+                 batch_window_us: int = 0):
+        self._L = abi.lib()
+        cfg = abi.ServerCfg(device, max_inflight, max_batch_pictures, max_batch_bytes, hbm_budget,
+                            int(batching), batch_window_us)
+        h = C.c_void_p()
+        _check(self._L.hpvcd_server_create(C.byref(cfg), C.byref(h)), "hpvcd_server_create")
+        self._h = h
+        self._dst = {}
+        self._keep = {}
+
+    def submit(self, pics, places, width: int, height: int, user: int,
+               matrix: int = abi.MATRIX_SMPTE170M, full_range: bool = True,
+               dst: np.ndarray | None = None, zero_copy_keep=None) -> np.ndarray:
+        """Queue one image.  `zero_copy_keep`: keep-alive of inputs packed by
+        pack_pinned() and a page-locked `dst` (pinned_empty()); the server
+        then copies nothing on the host."""
+        arr = _pic_array(pics)
+        pl = (abi.TilePlace * len(places))(*[abi.TilePlace(*t) for t in places])
+        if dst is None:
+            dst = np.empty((height, width, 3), np.uint8)
+        req = abi.Request(C.cast(arr, C.c_void_p), len(pics), C.cast(pl, C.c_void_p),
+                          abi.Canvas(width, height, matrix, int(full_range)),
+                          dst.ctypes.data_as(C.c_void_p), dst.nbytes, user,
+                          abi.REQ_ZERO_COPY if zero_copy_keep is not None else 0)
+        self._dst[user] = dst
+        if zero_copy_keep is not None:
+            self._keep[user] = zero_copy_keep
+        _check(self._L.hpvcd_server_submit(self._h, C.byref(req)), "hpvcd_server_submit")
+        return dst
+
+    def poll(self, max_n: int = 64, timeout_ms: int = -1):
+        buf = (abi.Completion * max_n)()
+        k = self._L.hpvcd_server_poll(self._h, buf, max_n, timeout_ms)
+        out = []
+        for i in range(k):
+            c = buf[i]
+            self._keep.pop(c.user, None)
+            out.append(dict(user=c.user, status=c.status, batch_pictures=c.batch_pictures,
+                            latency_ms=c.latency_ms, queue_ms=c.queue_ms,
+                            image=self._dst.pop(c.user, None)))
+        return out
+
+    def pending(self) -> int:
+        return self._L.hpvcd_server_pending(self._h)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.hpvcd_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

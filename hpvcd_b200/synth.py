@@ -164,7 +164,7 @@ class Grid:
 
 def make_grid(out_w: int, out_h: int, seed: int, bit_depth=10, chroma_idc=1, tile=512,
               synth: SynthSet | None = None, **kw) -> Grid:
-    g = Grid(out_w, out_h, tile, synth or SynthSet())
+    g = Grid(out_w, out_h, tile, synth if synth is not None else SynthSet())
     for r in range(g.rows):
         for col in range(g.cols):
             cfg = intra_cfg(seed * 100003 + r * g.cols + col, tile, tile, bit_depth, chroma_idc, **kw)

@@ -211,18 +211,37 @@ typedef struct hpvcd_picture {
 typedef struct hpvcd_tile_place {
     uint32_t dst_x, dst_y;   /* top-left on the canvas                         */
     uint32_t crop_w, crop_h; /* visible tile size (SPS conformance window size) */
-} hpvcd_tile_place;
+    uint32_t canvas;         /* canvas index (0 when the output has one)       */
+} hpvcd_tile_place; /* 20 bytes */
+
+/* One output image of a batch: its size and colour description (the SPS VUI
+ * of its tiles, lib.rs:1801-1815). */
+typedef struct hpvcd_canvas {
+    uint32_t width, height;
+    uint32_t matrix;         /* HPVCD_MATRIX_*                                 */
+    uint32_t full_range;
+} hpvcd_canvas;
 
 typedef struct hpvcd_output {
     uint32_t kind;           /* HPVCD_OUT_*                                    */
-    uint32_t matrix;         /* HPVCD_MATRIX_*                                 */
-    uint32_t full_range;     /* video_full_range_flag                          */
-    uint32_t canvas_w, canvas_h;
+    uint32_t matrix;         /* HPVCD_MATRIX_* (single canvas)                 */
+    uint32_t full_range;     /* video_full_range_flag (single canvas)          */
+    uint32_t canvas_w, canvas_h; /* single canvas                              */
     const hpvcd_tile_place* place; /* one per picture (RGB8 only)              */
     void* host_dst;          /* optional: page-locked caller buffer that       */
                              /* receives the output directly (then             */
                              /* hpvcd_gpu_read copies nothing)                 */
     uint64_t host_dst_bytes;
+    /* Several canvases (n_canvases > 0): the output is canvases[0], then
+     * canvases[1], ... each packed RGB8 width*height*3 bytes, and
+     * place[i].canvas selects the canvas of picture i.  canvas_w / canvas_h /
+     * matrix / full_range are then ignored. */
+    uint32_t n_canvases;
+    const hpvcd_canvas* canvases;
+    /* Optional per-canvas destinations (n_canvases entries, page-locked):
+     * each canvas is DMA'd straight into its own buffer; host_dst is then
+     * unused and hpvcd_gpu_read copies nothing. */
+    void* const* canvas_dst;
 } hpvcd_output;
 
 /* ------------------------------------------------------------------------ */
@@ -232,6 +251,8 @@ uint32_t hpvcd_abi_version(void);
 const char* hpvcd_status_string(int status);
 /* Number of kernel launches issued by this process so far (all entry points). */
 uint64_t hpvcd_kernel_launch_count(void);
+/* Text of the last CUDA runtime error this thread turned into a status. */
+const char* hpvcd_last_error_string(void);
 
 /* ------------------------------------------------------------------------ */
 /* Host-buffer API: the drop-in under `decode_heic` / `VideoDecoder`.        */
@@ -252,11 +273,11 @@ typedef struct hpvcd_gpu_cfg {
 hpvcd_status hpvcd_gpu_create(const hpvcd_gpu_cfg* cfg, hpvcd_gpu** out);
 hpvcd_status hpvcd_gpu_destroy(hpvcd_gpu* ctx);
 /* Copy the host buffers of `n` pictures to the device, reconstruct them and
- * start the copy of the requested output back.  Host buffers are only read
- * during the call.  Buffers in page-locked memory are copied by DMA straight
- * from where they are (and in one transfer when they are laid out as
- * hpvcd_gpu_pack_inputs lays them out); pageable ones go through a staging
- * copy.  Returns HPVCD_ERR_ALLOC when the batch does not fit the HBM budget
+ * start the copy of the requested output back.  Pageable host buffers are
+ * only read during the call (staging copy).  Buffers in page-locked memory
+ * are copied by DMA straight from where they are, one transfer per run of
+ * buffers laid out as hpvcd_gpu_pack_inputs lays them out, and must stay
+ * valid until the ticket completes.  Returns HPVCD_ERR_ALLOC when the batch does not fit the HBM budget
  * (the caller may retry later). */
 hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* ctx, const hpvcd_picture* pics, uint32_t n,
                               const hpvcd_output* out, hpvcd_ticket* ticket);
@@ -290,6 +311,9 @@ typedef struct hpvcd_plan hpvcd_plan;
 #define HPVCD_STAGE_SAO 0x04u     /* sample adaptive offset                     */
 #define HPVCD_STAGE_OUTPUT 0x08u  /* RGB8 canvas conversion                     */
 #define HPVCD_STAGE_ALL 0x0Fu
+#define HPVCD_STAGE_GRAPH 0x100u /* replay the selected stages as a CUDA graph    */
+                                 /* captured on first use (stream must not be   */
+                                 /* the legacy default stream)                   */
 
 /* Variant knobs chosen by the autotuner / schedule selector.  They never
  * change pixels, only speed. */
@@ -315,6 +339,62 @@ hpvcd_status hpvcd_plan_canvas(hpvcd_plan* plan, void** rgb, uint64_t* bytes);
 hpvcd_status hpvcd_plan_device_status(hpvcd_plan* plan, void* stream);
 /* Number of kernel launches one hpvcd_plan_launch(HPVCD_STAGE_ALL) issues. */
 uint32_t hpvcd_plan_launches_per_run(const hpvcd_plan* plan);
+
+/* ------------------------------------------------------------------------ */
+/* Serving loop: continuous batching of decode requests.  No reference      */
+/* counterpart (the reference decodes one `decode_heic` call at a time, or  */
+/* several on caller threads, decoder.rs:224); this is the service a        */
+/* request router puts in front of the drop-in.                             */
+/* ------------------------------------------------------------------------ */
+typedef struct hpvcd_server hpvcd_server;
+
+typedef struct hpvcd_server_cfg {
+    int32_t device;
+    uint32_t max_inflight;       /* batches on the GPU at once, 0 -> 2           */
+    uint32_t max_batch_pictures; /* pictures fused into one launch, 0 -> 4096    */
+    uint64_t max_batch_bytes;    /* input + output bytes of one batch, 0 -> 2 GiB */
+    uint64_t hbm_budget;         /* context HBM budget, 0 -> 80% of free memory  */
+    uint32_t batching;           /* 1: fuse queued requests; 0: one per launch   */
+    uint32_t batch_window_us;    /* a free slot waits until the oldest queued     */
+                                 /* request is this old (or a batch is full)      */
+} hpvcd_server_cfg;
+
+/* One decode request: the tiles of one image and where its RGB8 goes. */
+typedef struct hpvcd_request {
+    const hpvcd_picture* pics;  /* host buffers, copied during submit          */
+    uint32_t n_pics;
+    const hpvcd_tile_place* place; /* per picture (the canvas index is ignored) */
+    hpvcd_canvas canvas;
+    void* dst;                  /* receives width*height*3 bytes on completion */
+    uint64_t dst_bytes;
+    uint64_t user;              /* caller tag returned in the completion       */
+    uint32_t flags;             /* HPVCD_REQ_*                                 */
+} hpvcd_request;
+
+/* hpvcd_request.flags */
+#define HPVCD_REQ_ZERO_COPY 0x1u /* inputs packed by hpvcd_gpu_pack_inputs in  */
+                                 /* page-locked memory and dst page-locked;     */
+                                 /* both must stay valid until completion, and  */
+                                 /* nothing is copied on the host               */
+
+typedef struct hpvcd_completion {
+    uint64_t user;
+    int32_t status;             /* hpvcd_status of the request                 */
+    uint32_t batch_pictures;    /* pictures of the launch that decoded it      */
+    double latency_ms;          /* submit -> output in dst                     */
+    double queue_ms;            /* submit -> batch launch                      */
+} hpvcd_completion;
+
+hpvcd_status hpvcd_server_create(const hpvcd_server_cfg* cfg, hpvcd_server** out);
+/* Enqueue a request (non-blocking; the request's host buffers may be
+ * released when this returns). */
+hpvcd_status hpvcd_server_submit(hpvcd_server* srv, const hpvcd_request* req);
+/* Up to `max` completions, waiting at most timeout_ms for the first one
+ * (negative: forever).  Returns the number written. */
+uint32_t hpvcd_server_poll(hpvcd_server* srv, hpvcd_completion* out, uint32_t max, int32_t timeout_ms);
+/* Requests submitted and not yet returned by hpvcd_server_poll. */
+uint32_t hpvcd_server_pending(hpvcd_server* srv);
+hpvcd_status hpvcd_server_destroy(hpvcd_server* srv);
 
 /* ------------------------------------------------------------------------ */
 /* Utilities (no reference counterpart).                                    */

@@ -1387,6 +1387,22 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
     if (out && out->kind == HPVCD_OUT_RGB8 && rgb && out->place) {
         // lib.rs:1610-1660 per-tile RGB then row copy with cropping;
         // lib.rs:1964-1978 rgb8 narrowing by >> (bit_depth - 8).
+        // canvases: one (canvas_w x canvas_h) or out->canvases[]; lib.rs:1724
+        // decode_grid per output image.
+        std::vector<uint32_t> cwid, chgt, cmat, cfr;
+        std::vector<size_t> coff;
+        size_t acc = 0;
+        const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
+        for (uint32_t k = 0; k < nc; ++k) {
+            const hpvcd_canvas c = out->n_canvases ? out->canvases[k]
+                                                   : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix,
+                                                                  out->full_range};
+            cwid.push_back(c.width); chgt.push_back(c.height); cmat.push_back(c.matrix); cfr.push_back(c.full_range);
+            coff.push_back(acc);
+            acc += (size_t)c.width * c.height * 3;
+        }
+        for (uint32_t i = 0; i < n; ++i)
+            if (out->place[i].canvas >= nc) return HPVCD_ERR_INVALID_ARG;
         std::atomic<uint32_t> next{0};
         auto convert = [&](uint32_t i) {
             const hpvcd_picture* p = &pics[i];
@@ -1396,13 +1412,15 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
             if (tw <= 0 || th <= 0) return;
             std::vector<uint16_t> buf((size_t)tw * th * 3);
             yuv_to_rgb16(pl[i].y, pl[i].cb, pl[i].cr, g.w, g.h, g.idc, g.bd, tw, th, 0, 0,
-                         (int)out->matrix, out->full_range != 0, buf.data());
+                         (int)cmat[tp.canvas], cfr[tp.canvas] != 0, buf.data());
             const int shift = g.bd - 8;
-            const int copy_w = std::min(tw, std::max((int)out->canvas_w - (int)tp.dst_x, 0));
-            const int copy_h = std::min(th, std::max((int)out->canvas_h - (int)tp.dst_y, 0));
+            const int cw = (int)cwid[tp.canvas], chh = (int)chgt[tp.canvas];
+            uint8_t* base = rgb + coff[tp.canvas];
+            const int copy_w = std::min(tw, std::max(cw - (int)tp.dst_x, 0));
+            const int copy_h = std::min(th, std::max(chh - (int)tp.dst_y, 0));
             for (int y = 0; y < copy_h; ++y)
                 for (int x = 0; x < copy_w * 3; ++x)
-                    rgb[((size_t)(tp.dst_y + y) * out->canvas_w + tp.dst_x) * 3 + x] =
+                    base[((size_t)(tp.dst_y + y) * cw + tp.dst_x) * 3 + x] =
                         (uint8_t)(buf[(size_t)y * tw * 3 + x] >> shift);
         };
         if (threads > 1 && n > 1) {

@@ -217,7 +217,11 @@ def decode_batch(pics, out=None, want_planes=True, threads=1):
             pl_arr[i] = Planes(_p(y), _p(cb) if cb.size else None, _p(cr) if cr.size else None)
     rgb = None
     if out is not None and out.kind == abi.OUT_RGB8:
-        rgb = np.zeros((out.canvas_h, out.canvas_w, 3), np.uint8)
+        if out.n_canvases:
+            cv = (abi.Canvas * out.n_canvases).from_address(out.canvases)
+            rgb = np.zeros(sum(c.width * c.height * 3 for c in cv), np.uint8)
+        else:
+            rgb = np.zeros((out.canvas_h, out.canvas_w, 3), np.uint8)
     rc = lib().orc_decode_batch(arr, u32(n), C.byref(out) if out is not None else None,
                                 pl_arr if want_planes else None,
                                 _p(rgb) if rgb is not None else None, i32(threads))

@@ -41,7 +41,9 @@ def test_struct_layouts_match():
         "hpvcd_sao_ctb": abi.SaoCtb, "hpvcd_pu": abi.Pu, "hpvcd_wp_entry": abi.WpEntry,
         "hpvcd_wp_table": abi.WpTable, "hpvcd_picture": abi.Picture,
         "hpvcd_tile_place": abi.TilePlace, "hpvcd_output": abi.Output,
-        "hpvcd_gpu_cfg": abi.GpuCfg, "hpvcd_sched": abi.Sched,
+        "hpvcd_gpu_cfg": abi.GpuCfg, "hpvcd_sched": abi.Sched, "hpvcd_canvas": abi.Canvas,
+        "hpvcd_server_cfg": abi.ServerCfg, "hpvcd_request": abi.Request,
+        "hpvcd_completion": abi.Completion,
     }
     for name, cls in pairs.items():
         assert L.hpvcd_abi_sizeof(name.encode()) == C.sizeof(cls), name

@@ -253,3 +253,107 @@ def test_packed_pinned_inputs_and_direct_output(dec):
     dec.read(t, dst)
     _, ref = O.decode_batch(pics, out, want_planes=False)
     assert np.array_equal(dst.reshape(ref.shape), ref)
+
+
+def _image(seed, w, h, bd, idc, synth_set):
+    """One image as 512x512 grid tiles; returns (pics, places)."""
+    g = synth.make_grid(w, h, seed=seed, bit_depth=bd, chroma_idc=idc, synth=synth_set)
+    first = len(synth_set) - g.cols * g.rows
+    pics = [synth_set.picture(first + i) for i in range(g.cols * g.rows)]
+    return pics, g.places
+
+
+def test_multi_canvas_batch(dec):
+    s = synth.SynthSet()
+    specs = [(1, 700, 500, 8, 1, abi.MATRIX_SMPTE170M, 1), (2, 512, 512, 10, 3, abi.MATRIX_BT709, 0),
+             (3, 300, 900, 8, 1, abi.MATRIX_BT2020NCL, 1)]
+    pics, places, canv = [], [], []
+    for k, (seed, w, h, bd, idc, m, fr) in enumerate(specs):
+        p, pl = _image(seed, w, h, bd, idc, s)
+        pics += p
+        places += [(x, y, cw, ch, k) for (x, y, cw, ch) in pl]
+        canv.append(abi.Canvas(w, h, m, fr))
+    import ctypes as C
+    pl_arr = (abi.TilePlace * len(places))(*[abi.TilePlace(*t) for t in places])
+    cv_arr = (abi.Canvas * len(canv))(*canv)
+    out = abi.Output(abi.OUT_RGB8, 0, 0, 0, 0, C.cast(pl_arr, C.c_void_p), None, 0, len(canv),
+                     C.cast(cv_arr, C.c_void_p))
+    t = dec.submit(pics, out)
+    dec.wait(t)
+    got = dec.read(t)
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    assert got.size == ref.size and np.array_equal(got, ref)
+
+
+def test_server_alone_equals_in_mix():
+    from hpvcd_b200.gpu import Server
+    s = synth.SynthSet()
+    imgs = [(_image(100 + i, w, h, bd, idc, s), w, h) for i, (w, h, bd, idc) in
+            enumerate([(640, 448, 10, 1), (1024, 768, 8, 1), (512, 1100, 8, 3), (256, 256, 10, 1), (900, 600, 8, 1)])]
+    # alone: one request, plain path
+    with Server(0, max_inflight=1, batching=False) as plain:
+        alone = []
+        for k, ((pics, places), w, h) in enumerate(imgs):
+            plain.submit(pics, places, w, h, user=k)
+            (c,) = plain.poll(1, timeout_ms=60000)
+            assert c["status"] == abi.OK
+            alone.append(c["image"].copy())
+    # in the mix: all submitted at once to a batching server
+    with Server(0, max_inflight=2, batching=True, batch_window_us=200000) as srv:
+        for k, ((pics, places), w, h) in enumerate(imgs):
+            srv.submit(pics, places, w, h, user=k)
+        got = {}
+        while len(got) < len(imgs):
+            for c in srv.poll(16, timeout_ms=60000):
+                assert c["status"] == abi.OK
+                got[c["user"]] = c
+    assert max(c["batch_pictures"] for c in got.values()) > max(len(p) for (p, _), _, _ in imgs)
+    for k, ((pics, places), w, h) in enumerate(imgs):
+        assert np.array_equal(got[k]["image"], alone[k]), k
+        # and both equal the oracle's decode of the image
+        out, keep = synth.grid_output(synth.Grid(w, h, 512, s, places))
+        _, ref = O.decode_batch(pics, out, want_planes=False)
+        assert np.array_equal(alone[k], ref), k
+
+
+def test_plan_graph_replay_matches():
+    g = synth.make_grid(1024, 700, seed=13, bit_depth=8)
+    out, keep = synth.grid_output(g)
+    pics = g.synth.pictures()
+    plan = DevicePlan(pics, out)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        before = abi.lib().hpvcd_kernel_launch_count()
+        plan.launch(abi.STAGE_ALL | abi.STAGE_GRAPH, s)
+        plan.launch(abi.STAGE_ALL | abi.STAGE_GRAPH, s)
+        s.synchronize()
+        counted = abi.lib().hpvcd_kernel_launch_count() - before
+    assert counted == 2 * plan.launches_per_run
+    got = plan.canvas()
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    assert np.array_equal(got, ref)
+    plan.close()
+
+
+def test_server_zero_copy_matches_oracle():
+    from hpvcd_b200.gpu import Server, pack_pinned, pinned_empty
+    s = synth.SynthSet()
+    imgs = [(_image(200 + i, w, h, 10 if i % 2 else 8, 1, s), w, h) for i, (w, h) in
+            enumerate([(640, 448), (1100, 700), (300, 300)])]
+    keep = []
+    with Server(0, max_inflight=2, batching=True, batch_window_us=200000) as srv:
+        for k, ((pics, places), w, h) in enumerate(imgs):
+            packed, kp = pack_pinned(pics)
+            dst, kd = pinned_empty(w * h * 3)
+            keep.append((kp, kd))
+            srv.submit(packed, places, w, h, user=k, dst=dst.reshape(h, w, 3), zero_copy_keep=(kp, kd))
+        got = {}
+        while len(got) < len(imgs):
+            for c in srv.poll(16, timeout_ms=60000):
+                assert c["status"] == abi.OK
+                got[c["user"]] = c
+    assert max(c["batch_pictures"] for c in got.values()) > max(len(p) for (p, _), _, _ in imgs)
+    for k, ((pics, places), w, h) in enumerate(imgs):
+        out, kk = synth.grid_output(synth.Grid(w, h, 512, s, places))
+        _, ref = O.decode_batch(pics, out, want_planes=False)
+        assert np.array_equal(got[k]["image"], ref), k
