@@ -61,6 +61,9 @@ STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_OUTPUT = 0x1, 0x2, 0x4, 0x8
 STAGE_ALL = 0xF
 STAGE_GRAPH = 0x100
 
+# Fixed per-device scratch of hpvcd_decode_noalloc (bytes).
+NOALLOC_SCRATCH_BYTES = 12 * 1024 * 1024 + 256 * 1024
+
 SYNTH_RESIDUAL, SYNTH_INTRA, SYNTH_INTER = 0, 1, 2
 
 
@@ -248,6 +251,7 @@ def lib() -> C.CDLL:
             "hpvcd_server_pending": (u32, [vp]),
             "hpvcd_server_destroy": (i32, [vp]),
             "hpvcd_gpu_pack_inputs": (i32, [C.POINTER(Picture), u32, vp, u64, C.POINTER(Picture)]),
+            "hpvcd_decode_noalloc": (i32, [C.POINTER(Picture), C.POINTER(vp), vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -1094,3 +1094,228 @@ HPVCD_API hpvcd_status hpvcd_gpu_read(hpvcd_gpu* g, hpvcd_ticket t, void* dst, u
     s->ticket = 0;
     return st;
 }
+
+// ---------------------------------------------------------------------------
+// Decoding one picture without allocating (hpvcd_decode_noalloc).
+//
+// Some callers cannot allocate at decode time: an application that hands the
+// decoder a fixed share of HBM and keeps every other byte in its own pool, or
+// a frame loop with a latency budget where cudaMalloc/cudaFree would
+// synchronise the device and stall unrelated streams.  For them the scratch of
+// one picture's decode lives in one fixed array of module global memory,
+// reserved when the module loads: work counter, device error word, wavefront
+// ready flags, the device picture record, the CTU work list, the int16
+// residual planes and, when SAO runs, the pre-SAO planes.  The caller owns the
+// inputs (device buffers) and the output planes.
+//
+// The array is reset per call by the first kernel the call enqueues, so calls
+// ordered on one stream are safe; two calls whose work overlaps on a device
+// (two streams, two host threads) use the same array and race.
+// ---------------------------------------------------------------------------
+
+// 12 MiB + 256 KiB: every picture up to 1024x1024 luma samples in any chroma
+// format and bit depth with SAO on (int16 residual planes <= 6 MiB, pre-SAO
+// planes <= 6 MiB, per-CTU records <= 48 KiB for 16x16 CTBs).
+static constexpr size_t kNoAllocScratchBytes = HPVCD_NOALLOC_SCRATCH_BYTES;
+static_assert(kNoAllocScratchBytes % 256 == 0, "scratch size");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+
+struct NoAllocDevice {
+    unsigned char* base = nullptr;  // address of g_noalloc_scratch on this device
+    int sms = 0;
+    int occ[2] = {0, 0};            // k_recon CTAs per SM (4:2:0 layout, 4:4:4 layout)
+    bool ready = false;
+};
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+// Byte offsets inside the scratch array.  Word 0 is the work counter, word 1
+// the device error word; the ready flags follow at byte 256.
+struct NoAllocLayout {
+    uint64_t ready, pic, prefix, items, res, snap, need;
+};
+
+NoAllocLayout noalloc_layout(const hpvcd_picture& p, const Geo& g) {
+    NoAllocLayout L;
+    const uint64_t n_ctu = (uint64_t)g.ctb_cols * g.ctb_rows;
+    L.ready = 256;
+    L.pic = align_up(L.ready + n_ctu * 4, 256);
+    L.prefix = align_up(L.pic + sizeof(DevPic), 256);
+    L.items = L.prefix + 256;
+    L.res = align_up(L.items + n_ctu * sizeof(CtuItem), 256);
+    L.snap = L.res + res_plane_bytes(g);
+    L.need = L.snap + (sao_active(p) ? align_up(g.luma_bytes, 256) + 2 * align_up(g.chroma_bytes, 256) : 0);
+    return L;
+}
+
+// Once per device, with that device current: the array's device address, the
+// SM count and the k_recon shared-memory limit / occupancy.  None of these
+// calls allocates.
+hpvcd_status noalloc_setup(int dev, NoAllocDevice** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e);
+        e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return cuda_status(e);
+        for (int c444 = 0; c444 < 2; ++c444) d.occ[c444] = std::max(1, hpvcd_recon_occupancy(c444));
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_status(e);
+        d.base = (unsigned char*)p;
+        d.ready = true;
+    }
+    *out = &d;
+    return HPVCD_OK;
+}
+
+// Zero the counter, error word and ready flags; store the picture record and
+// the TB-record prefix; write the CTU work list in wavefront order (sorted by
+// t = x + 2y, then y), the order in which every CTU's left, above-left, above
+// and above-right neighbours come earlier.
+__global__ void k_noalloc_setup(DevPic pic, uint32_t n_tus, unsigned char* base, NoAllocLayout L, int list) {
+    const int cols = pic.ctb_cols, rows = pic.ctb_rows;
+    const int n_ctu = cols * rows;
+    uint32_t* words = (uint32_t*)base;
+    uint32_t* ready = (uint32_t*)(base + L.ready);
+    CtuItem* items = (CtuItem*)(base + L.items);
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid < 2) words[tid] = 0u;
+    if (tid == 0) {
+        *(DevPic*)(base + L.pic) = pic;
+        uint32_t* prefix = (uint32_t*)(base + L.prefix);
+        prefix[0] = 0u;
+        prefix[1] = n_tus;
+    }
+    for (int i = tid; i < n_ctu; i += gridDim.x * blockDim.x) {
+        ready[i] = 0u;
+        if (!list) continue;
+        const int x = i % cols, y = i / cols, t = x + 2 * y;
+        uint32_t rank = 0;
+        for (int yy = 0; yy < rows && 2 * yy <= t; ++yy) {
+            const int run = t - 2 * yy;  // cells of row yy with x' + 2yy < t
+            rank += (uint32_t)(run < cols ? run : cols);
+            if (yy < y && run < cols) ++rank;  // row yy holds a cell of this t before row y
+        }
+        items[rank] = CtuItem{0u, (uint16_t)x, (uint16_t)y};
+    }
+}
+
+}  // namespace
+
+HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* const planes[3],
+                                            uint32_t* dev_status, void* stream) {
+    if (!dev_pic || !planes) return HPVCD_ERR_INVALID_ARG;
+    const hpvcd_picture& p = *dev_pic;
+    hpvcd_status s = validate(p);
+    if (s != HPVCD_OK) return s;
+    if (p.flags & HPVCD_PIC_INTER) {
+        std::snprintf(t_last_error, sizeof(t_last_error),
+                      "hpvcd_decode_noalloc: inter pictures predict from other pictures of one launch; "
+                      "decode them with a plan");
+        return HPVCD_ERR_UNSUPPORTED;
+    }
+    const int n_comp = p.chroma_idc ? 3 : 1;
+    for (int c = 0; c < n_comp; ++c)
+        if (!planes[c] || ((uintptr_t)planes[c] & 255)) {
+            std::snprintf(t_last_error, sizeof(t_last_error),
+                          "hpvcd_decode_noalloc: output plane %d is NULL or not 256-byte aligned", c);
+            return HPVCD_ERR_INVALID_ARG;
+        }
+    const Geo g = geo_of(p);
+    const NoAllocLayout L = noalloc_layout(p, g);
+    if (L.need > kNoAllocScratchBytes) {
+        std::snprintf(t_last_error, sizeof(t_last_error),
+                      "hpvcd_decode_noalloc: a %ux%u picture needs %llu bytes of scratch, the fixed array holds "
+                      "%llu (every picture up to 1024x1024 fits)",
+                      p.width, p.height, (unsigned long long)L.need, (unsigned long long)kNoAllocScratchBytes);
+        return HPVCD_ERR_LIMIT;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return HPVCD_ERR_LIMIT;
+    NoAllocDevice* nd = nullptr;
+    s = noalloc_setup(dev, &nd);
+    if (s != HPVCD_OK) return s;
+    unsigned char* base = nd->base;
+
+    // device picture record (the fields plan_build fills for a YUV output)
+    DevPic d;
+    std::memset(&d, 0, sizeof(d));
+    d.w = g.w; d.h = g.h; d.cw = g.cw; d.ch = g.ch; d.gw = g.gw; d.gh = g.gh;
+    d.idc = p.chroma_idc; d.sub_w = g.sub_w; d.sub_h = g.sub_h;
+    d.bd = p.bit_depth_y; d.bd_c = p.bit_depth_c; d.bps = g.bps;
+    d.log2_ctb = p.log2_ctb; d.ctb_cols = g.ctb_cols; d.ctb_rows = g.ctb_rows;
+    d.flags = p.flags;
+    d.beta_offset_div2 = p.beta_offset_div2;
+    d.tc_offset_div2 = p.tc_offset_div2;
+    d.pps_cb_qp_offset = p.pps_cb_qp_offset;
+    d.pps_cr_qp_offset = p.pps_cr_qp_offset;
+    fill_inputs(d, p);
+    for (int l = 0; l < 2; ++l)
+        for (int r = 0; r < HPVCD_MAX_REFS; ++r) d.ref_pic[l][r] = -1;
+    for (int c = 0; c < 3; ++c) d.fin[c] = c < n_comp ? planes[c] : nullptr;
+    if (sao_active(p)) {
+        unsigned char* sb = base + L.snap;
+        d.rec[0] = sb;
+        d.rec[1] = p.chroma_idc ? sb + align_up(g.luma_bytes, 256) : nullptr;
+        d.rec[2] = p.chroma_idc ? sb + align_up(g.luma_bytes, 256) + align_up(g.chroma_bytes, 256) : nullptr;
+    } else {
+        for (int c = 0; c < 3; ++c) d.rec[c] = d.fin[c];
+    }
+    {
+        unsigned char* rb = base + L.res;
+        d.res_stride[0] = res_stride_of(g.w);
+        d.res_stride[1] = d.res_stride[2] = res_stride_of(g.cw);
+        const size_t ly = align_up((size_t)d.res_stride[0] * g.h * 2, 256);
+        const size_t lc = align_up((size_t)d.res_stride[1] * g.ch * 2, 256);
+        d.res[0] = (int16_t*)rb;
+        d.res[1] = p.chroma_idc ? (int16_t*)(rb + ly) : nullptr;
+        d.res[2] = p.chroma_idc ? (int16_t*)(rb + ly + lc) : nullptr;
+    }
+    d.ready = (uint32_t*)(base + L.ready);
+    d.needs_wavefront = (p.flags & HPVCD_PIC_PRED_IN_PLANE) ? 0 : 1;
+
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t n_ctu = (uint32_t)g.ctb_cols * g.ctb_rows;
+    const DevPic* dp = (const DevPic*)(base + L.pic);
+    uint32_t* work_counter = (uint32_t*)base;
+    uint32_t* d_err = work_counter + 1;
+    const int setup_blocks = (int)std::min<uint32_t>((n_ctu + 255) / 256, (uint32_t)nd->sms);
+    k_noalloc_setup<<<std::max(1, setup_blocks), 256, 0, st>>>(d, p.n_tus, base, L, d.needs_wavefront);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+    hpvcd_note_launches(1);
+    if (p.flags & HPVCD_PIC_PRED_IN_PLANE)
+        for (int c = 0; c < n_comp; ++c) {
+            if (!p.pred[c]) continue;
+            e = cudaMemcpyAsync(d.rec[c], p.pred[c], c ? g.chroma_bytes : g.luma_bytes, cudaMemcpyDeviceToDevice,
+                                st);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
+    const uint32_t* prefix = (const uint32_t*)(base + L.prefix);
+    e = hpvcd_launch_residual(dp, prefix, 1, p.n_tus, d_err, nd->sms, st);
+    if (e != cudaSuccess) return cuda_status(e);
+    if (d.needs_wavefront) {
+        const int c444 = p.chroma_idc == 3 ? 1 : 0;
+        const int grid = std::max(1, std::min<int>(nd->sms * nd->occ[c444], (int)n_ctu));
+        e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, c444, grid, st);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    const int lv = (d.w >= 12 ? (d.w - 4) / 8 : 0) * (d.h / 4);
+    const int lh = (d.h >= 12 ? (d.h - 4) / 8 : 0) * (d.w / 4);
+    const int cv = d.idc ? (d.cw >= 10 ? (d.cw - 2) / 8 : 0) * (d.ch / 4) : 0;
+    const int ch = d.idc ? (d.ch >= 10 ? (d.ch - 2) / 8 : 0) * (d.cw / 4) : 0;
+    e = hpvcd_launch_deblock(dp, 1, std::max(lv, cv), 1, st);
+    if (e == cudaSuccess) e = hpvcd_launch_deblock(dp, 1, std::max(lh, ch), 0, st);
+    if (e == cudaSuccess && sao_active(p)) e = hpvcd_launch_sao(dp, 1, d.w * d.h, st);
+    if (e == cudaSuccess && dev_status)
+        e = cudaMemcpyAsync(dev_status, d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+    return cuda_status(e);
+}

@@ -341,6 +341,43 @@ hpvcd_status hpvcd_plan_device_status(hpvcd_plan* plan, void* stream);
 uint32_t hpvcd_plan_launches_per_run(const hpvcd_plan* plan);
 
 /* ------------------------------------------------------------------------ */
+/* Decoding one picture without allocating.  No counterpart in the          */
+/* reference (its decoder allocates every plane it reconstructs).  For       */
+/* callers that may not allocate while decoding: an application that gives  */
+/* the decoder a fixed share of HBM, or a frame loop in which a cudaMalloc / */
+/* cudaFree (which synchronise the device) would stall other streams.       */
+/* ------------------------------------------------------------------------ */
+/* Bytes of the fixed scratch array each device holds for this entry point:
+ * enough for every picture up to 1024x1024 luma samples (any chroma format,
+ * bit depth, deblocking and SAO). */
+#define HPVCD_NOALLOC_SCRATCH_BYTES (12u * 1024u * 1024u + 256u * 1024u)
+/* Reconstruct, deblock and SAO-filter one intra / residual picture whose
+ * descriptor (a host struct) points at device-resident inputs, writing its
+ * planes into caller-owned device memory: planes[0..2] = Y, Cb, Cr (Cb/Cr
+ * unused for 4:0:0), each 256-byte aligned, unpadded (luma stride = width *
+ * bytes per sample, as hpvcd_plan_planes).  Enqueues its kernels on `stream`
+ * and returns; allocates no memory of any kind.  Its scratch (work counter,
+ * error word, wavefront ready flags, picture record, CTU list, residual and
+ * pre-SAO planes) is one fixed array in the library's device memory; the
+ * call itself zeroes the counter, error word and ready flags on `stream`
+ * before use, and nothing else needs to start at zero.
+ *   - The first call on a device does the set-up (looks up the array's
+ *     address, sets the kernel's shared-memory limit) with that device
+ *     current; make it before any stream capture.
+ *   - Calls ordered on one stream are safe.  Two calls whose work overlaps
+ *     on one device (different streams, different host threads) share the
+ *     array and race.
+ *   - dev_status (device memory, may be NULL) receives the device error word
+ *     when the call's work completes: 0 = OK, bit 0 = a wavefront wait gave
+ *     up (HPVCD_ERR_TIMEOUT), bit 1 = malformed TB record (HPVCD_ERR_BITSTREAM).
+ *   - HPVCD_ERR_LIMIT (message in hpvcd_last_error_string) when the picture
+ *     needs more scratch than HPVCD_NOALLOC_SCRATCH_BYTES;
+ *     HPVCD_ERR_UNSUPPORTED for inter pictures (their references belong to
+ *     the same launch: use a plan). */
+hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* const planes[3],
+                                  uint32_t* dev_status, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Serving loop: continuous batching of decode requests.  No reference      */
 /* counterpart (the reference decodes one `decode_heic` call at a time, or  */
 /* several on caller threads, decoder.rs:224); this is the service a        */
