@@ -61,6 +61,11 @@ STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_OUTPUT = 0x1, 0x2, 0x4, 0x8
 STAGE_ALL = 0xF
 STAGE_GRAPH = 0x100
 
+# Schedule selector network (include/hpvcd_gpu.h).
+FEATURES = 16
+MLP_HIDDEN = 64
+MLP_MAX_VARIANTS = 32
+
 # Fixed per-device scratch of hpvcd_decode_noalloc (bytes).
 NOALLOC_SCRATCH_BYTES = 12 * 1024 * 1024 + 256 * 1024
 
@@ -86,6 +91,12 @@ class Tu(C.Structure):
 TU_DTYPE = np.dtype([
     ("x", "<u2"), ("y", "<u2"), ("coeff_off", "<u4"), ("log2n", "u1"), ("comp", "u1"),
     ("flags", "u1"), ("mode", "u1"), ("qp_y", "i1"), ("cqp_off", "i1"), ("nx", "u1"), ("rsvd", "u1"),
+])
+
+
+PU_DTYPE = np.dtype([
+    ("x", "<u2"), ("y", "<u2"), ("w", "<u2"), ("h", "<u2"), ("mv", "<i2", (2, 2)), ("ref_idx", "i1", (2,)),
+    ("flags", "u1"), ("rsvd", "u1"),
 ])
 
 
@@ -186,8 +197,8 @@ class GpuCfg(C.Structure):
 
 
 class Sched(C.Structure):
-    _fields_ = [("recon_threads", C.c_uint32), ("recon_ctas_per_sm", C.c_uint32),
-                ("filter_tile", C.c_uint32), ("fuse_filters", C.c_uint32)]
+    _fields_ = [("idct", C.c_uint32), ("luma_team", C.c_uint32),
+                ("recon_ctas_per_sm", C.c_uint32), ("rsvd", C.c_uint32)]
 
 
 class SynthCfg(C.Structure):
@@ -203,6 +214,7 @@ class SynthCfg(C.Structure):
         ("cb_qp_offset", C.c_int32), ("cr_qp_offset", C.c_int32),
         ("intra_cu_p", C.c_float), ("bi_p", C.c_float), ("mv_sd", C.c_float),
         ("mv_pad", C.c_float), ("weighted", C.c_uint32), ("n_refs", C.c_uint32),
+        ("tu_mix", C.c_float * 4),
     ]
 
 
@@ -252,6 +264,22 @@ def lib() -> C.CDLL:
             "hpvcd_server_destroy": (i32, [vp]),
             "hpvcd_gpu_pack_inputs": (i32, [C.POINTER(Picture), u32, vp, u64, C.POINTER(Picture)]),
             "hpvcd_decode_noalloc": (i32, [C.POINTER(Picture), C.POINTER(vp), vp, vp]),
+            "hpvcd_plan_set_sched": (i32, [vp, C.POINTER(Sched)]),
+            "hpvcd_plan_features": (i32, [vp, u32, u32, vp, vp]),
+            "hpvcd_plan_autotune": (i32, [vp, C.POINTER(Sched), u32, u32, u32, u32, vp, C.POINTER(C.c_float),
+                                          C.POINTER(u32)]),
+            "hpvcd_plan_select": (i32, [vp, vp, C.POINTER(Sched), u32, vp, C.POINTER(u32)]),
+            "hpvcd_mlp_create": (i32, [u32, u64, C.POINTER(vp)]),
+            "hpvcd_mlp_destroy": (i32, [vp]),
+            "hpvcd_mlp_param_count": (u32, [vp]),
+            "hpvcd_mlp_variants": (u32, [vp]),
+            "hpvcd_mlp_get_params": (i32, [vp, vp, C.c_int]),
+            "hpvcd_mlp_set_params": (i32, [vp, vp]),
+            "hpvcd_mlp_forward": (i32, [vp, vp, u32, vp, vp]),
+            "hpvcd_mlp_grad": (i32, [vp, vp, vp, u32, vp, vp, vp]),
+            "hpvcd_mlp_adam_step": (i32, [vp, C.c_float, vp]),
+            "hpvcd_mlp_train": (i32, [vp, vp, vp, u32, u32, u32, C.c_float, u64, vp, C.POINTER(C.c_float)]),
+            "hpvcd_mlp_pick": (i32, [vp, vp, u32, vp, C.POINTER(u32)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

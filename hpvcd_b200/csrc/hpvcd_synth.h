@@ -51,6 +51,10 @@ typedef struct hpvcd_synth_cfg {
     float mv_pad;             /* MVs are clamped to the picture plus this padding   */
     uint32_t weighted;        /* explicit weighted prediction table                 */
     uint32_t n_refs;          /* references: the n_refs previous pictures           */
+    /* TB-size mix: area fractions of 4x4, 8x8, 16x16, 32x32 TBs that the TU
+     * quadtree aims at (per-level split probabilities derived from it); all
+     * zero -> tu_split_p at every level. */
+    float tu_mix[4];
 } hpvcd_synth_cfg;
 
 typedef struct hpvcd_synth hpvcd_synth;

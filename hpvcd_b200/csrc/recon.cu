@@ -42,6 +42,9 @@ __constant__ int8_t c_dct_mag[33] = {64, 90, 90, 90, 89, 88, 87, 85, 83, 82, 80,
                                      61, 57, 54, 50, 46, 43, 38, 36, 31, 25, 22, 18, 13, 9,  4,  0};
 
 constexpr int kScr = 33;  // padded row stride of the transform scratch
+// Inverse-transform variants of k_residual (schedule knob; pixels identical).
+constexpr int kIdctMatrix = 0;     // matrix product, all-zero rows / columns skipped
+constexpr int kIdctButterfly = 1;  // even-odd butterflies for 16x16 and 32x32 TBs
 
 __device__ __forceinline__ int dct_entry(int n, int k, int m) {
     if (k == 0) return 64;
@@ -58,6 +61,74 @@ __device__ __forceinline__ int dct_entry(int n, int k, int m) {
 
 __device__ __forceinline__ int sat16(int v) { return v < -32768 ? -32768 : (v > 32767 ? 32767 : v); }
 
+// The same basis entry as a compile-time constant, for fully unrolled
+// butterflies (the multiplier becomes an immediate operand).
+__host__ __device__ constexpr int dct_c(int n, int k, int m) {
+    constexpr int8_t mag[33] = {64, 90, 90, 90, 89, 88, 87, 85, 83, 82, 80, 78, 75, 73, 70, 67, 64,
+                                61, 57, 54, 50, 46, 43, 38, 36, 31, 25, 22, 18, 13, 9,  4,  0};
+    if (k == 0) return 64;
+    int j = (k * (32 / n) * (2 * m + 1)) & 127;
+    int sign = 1;
+    if (j > 64) j = 128 - j;
+    if (j > 32) {
+        j = 64 - j;
+        sign = -1;
+    }
+    return sign * mag[j];
+}
+
+// Even-odd (partial butterfly) N-point inverse: out[m] = sum_{k < KMAX}
+// T_N[k][m] * in[k * S].  Rows of the basis are symmetric for even k and
+// antisymmetric for odd k, and T_N[2j][m] = T_{N/2}[j][m], so the even
+// coefficients form an N/2-point inverse and out[N-1-m] = E[m] - O[m].
+// Integer sums in any order are identical, so the result equals the matrix
+// product bit for bit (the clip follows the complete sum in both forms).
+template <int N, int S, int KMAX>
+__device__ __forceinline__ void inv_butterfly(const int* in, int* out) {
+    if constexpr (N == 1) {
+        out[0] = KMAX > 0 ? 64 * in[0] : 0;
+    } else {
+        int e[N / 2];
+        inv_butterfly<N / 2, 2 * S, (KMAX + 1) / 2>(in, e);
+#pragma unroll
+        for (int m = 0; m < N / 2; ++m) {
+            int o = 0;
+#pragma unroll
+            for (int k = 1; k < KMAX && k < N; k += 2) o += dct_c(N, k, m) * in[k * S];
+            out[m] = e[m] + o;
+            out[N - 1 - m] = e[m] - o;
+        }
+    }
+}
+
+// One stage of a 16- or 32-point inverse by butterflies, lane = line:
+// line l reads in[k] = src[l * ls + k * ks] for k < KMAX (the rest are zero)
+// and writes dst[l * ld + m * md] = fin(out[m]).
+template <int N, int KMAX, typename Fin>
+__device__ __forceinline__ void bf_stage(const int16_t* src, int ls, int ks, int16_t* dst, int ld, int md, int lane,
+                                         Fin fin) {
+    if (lane >= N) return;
+    int in[KMAX], out[N];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) in[k] = src[lane * ls + k * ks];
+    inv_butterfly<N, 1, KMAX>(in, out);
+#pragma unroll
+    for (int m = 0; m < N; ++m) dst[lane * ld + m * md] = (int16_t)fin(out[m]);
+}
+
+template <int N, typename Fin>
+__device__ __forceinline__ void bf_stage_k(int kcount, const int16_t* src, int ls, int ks, int16_t* dst, int ld,
+                                           int md, int lane, Fin fin) {
+    if (kcount <= 4)
+        bf_stage<N, 4>(src, ls, ks, dst, ld, md, lane, fin);
+    else if (kcount <= 8)
+        bf_stage<N, 8>(src, ls, ks, dst, ld, md, lane, fin);
+    else if (N == 16 || kcount <= 16)
+        bf_stage<N, (N < 16 ? N : 16)>(src, ls, ks, dst, ld, md, lane, fin);
+    else
+        bf_stage<N, N>(src, ls, ks, dst, ld, md, lane, fin);
+}
+
 // ===========================================================================
 // k_residual
 // ===========================================================================
@@ -66,7 +137,7 @@ constexpr int kResWarps = 8;
 // Residual of one coded TB by one warp (transform.rs:489-858, decode.rs
 // :4754-4903 luma, :5313-5417 chroma).  `emit(r, m, v)` receives every
 // residual sample (row r, column m) in the reference's storage semantics.
-template <typename Emit>
+template <int kIdct, typename Emit>
 __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16_t* dct, int16_t* buf,
                                  int16_t* tmp, int lane, Emit emit) {
     const int n = 1 << t.log2n;
@@ -120,6 +191,36 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
     for (int o = 16; o; o >>= 1) rows = max(rows, __shfl_xor_sync(0xffffffffu, rows, o));
     __syncwarp();
     const bool dst = luma && n == 4 && (t.flags & HPVCD_TU_INTRA);
+    if (kIdct == kIdctButterfly && n >= 16) {
+        // stage 1, lane = column: rows >= `rows` are zero
+        auto st1 = [](int acc) { return clamp3i((acc + 64) >> 7, -32768, 32767); };
+        // stage 2, lane = row: columns >= nx are zero.  The output is kept
+        // as int16 in buf: wrapped at 8 bits (the reference's i16 storage),
+        // saturated above 8 bits (exact: a saturated residual clips a
+        // sample to the same bound as the full value).
+        const int shift2 = 20 - bd;
+        const int add2 = 1 << (shift2 - 1);
+        auto st2 = [=](int acc) {
+            const int v = (acc + add2) >> shift2;
+            return i16s ? (int)(int16_t)v : sat16(v);
+        };
+        if (n == 16) {
+            bf_stage_k<16>(rows, buf, 1, kScr, tmp, 1, kScr, lane, st1);
+            __syncwarp();
+            bf_stage_k<16>(nx, tmp, kScr, 1, buf, kScr, 1, lane, st2);
+        } else {
+            bf_stage_k<32>(rows, buf, 1, kScr, tmp, 1, kScr, lane, st1);
+            __syncwarp();
+            bf_stage_k<32>(nx, tmp, kScr, 1, buf, kScr, 1, lane, st2);
+        }
+        __syncwarp();
+        for (int i = lane; i < n * n; i += 32) {
+            const int r = i / n, m = i % n;
+            emit(r, m, (int)buf[r * kScr + m]);
+        }
+        __syncwarp();
+        return;
+    }
     const int step = 32 / n;
     // stage 1 (columns): tmp[m][c] = clip((sum_k T[k][m] * buf[k][c] + 64) >> 7)
     for (int i = lane; i < n * n; i += 32) {
@@ -153,6 +254,7 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
     __syncwarp();
 }
 
+template <int kIdct>
 __global__ void __launch_bounds__(kResWarps * 32)
 k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_prefix, uint32_t n_pics,
            uint32_t* dev_err) {
@@ -186,7 +288,7 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
         if (in_plane) {  // prediction already in the plane: add + clip (reconstruct.rs:214-251)
             void* pl = P.rec[c];
             const int mx = (1 << (c ? P.bd_c : P.bd)) - 1;
-            tb_residual_warp(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
+            tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
                 const int x = x0 + m, y = y0 + r;
                 if (x < pw && y < ph) {
                     const size_t idx = (size_t)y * pw + x;
@@ -196,7 +298,7 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
         } else {
             int16_t* rp = P.res[c];
             const int rs = P.res_stride[c];
-            tb_residual_warp(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
+            tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
                 const int x = x0 + m, y = y0 + r;
                 if (x < pw && y < ph) rp[(size_t)y * rs + x] = (int16_t)sat16(v);
             });
@@ -216,6 +318,7 @@ struct WalkScratch {
     int32_t s[132];   // substituted reference line: s[2n+q] = above[q], s[2n-q] = left[q]
     int32_t f[132];   // filtered line (same layout); also holds available values before substitution
     int32_t refs[100];  // angular projection, refs[n + k] for k in [-n, 2n]
+    int32_t dc;         // DC value of the current TB
     uint4 recs[32];   // staged TB records
 };
 
@@ -363,11 +466,22 @@ __device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y
     __syncwarp();
 }
 
-// Intra TB of size 8..32 by one warp through shared memory: gather,
-// substitution (intra.rs:84-148), filtering (:151-219), prediction
-// (:257-372), add residual + clip (reconstruct.rs:214-251).
-__device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
-                                             uint32_t dec, WalkScratch& ws, int lane) {
+// Whether the reference line of an n x n intra TB is filtered
+// (intra.rs:151-219: luma, or 4:4:4 chroma, with smoothing on and a mode
+// far enough from the horizontal / vertical).
+__device__ __forceinline__ bool ref_filtered(const Comp& k, int n, int mode) {
+    if (!(k.filt && k.smoothing && mode != 1)) return false;
+    const int md = min(abs(mode - 26), abs(mode - 10));
+    const int thresh = n == 8 ? 7 : (n == 16 ? 1 : 0);
+    return mode == 0 || md > thresh;
+}
+
+// Intra TB of size 8..32, first part, by one warp through shared memory:
+// gather, substitution (intra.rs:84-148), filtering (:151-219) and the
+// per-mode set-up of the prediction (the angular projection into ws.refs,
+// the DC value into ws.dc).
+__device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode, int x0, int y0, uint32_t dec,
+                                              WalkScratch& ws, int lane) {
     const int n = 1 << log2n;
     const int total = 4 * n + 1;
     const int n2 = 2 * n;
@@ -419,12 +533,7 @@ __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode,
     }
     __syncwarp();
     // ---- filtering (luma, or 4:4:4 chroma without strong smoothing) ----
-    bool do_filter = false;
-    if (k.filt && k.smoothing && mode != 1) {
-        const int md = min(abs(mode - 26), abs(mode - 10));
-        const int thresh = n == 8 ? 7 : (n == 16 ? 1 : 0);
-        do_filter = mode == 0 || md > thresh;
-    }
+    const bool do_filter = ref_filtered(k, n, mode);
     const int32_t* R = ws.s;
     if (do_filter) {
         bool strong = false;
@@ -456,11 +565,6 @@ __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode,
         R = ws.f;
     }
     // A(q) = R[n2 + q], L(q) = R[n2 - q]
-    const int max_v = k.max_v;
-    const bool edge_filters = k.luma && n < 32;  // is_luma gate of predict_into
-    const int S = k.S;
-    const int16_t* res = k.res;
-    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
     if (mode >= 2) {
         const int angle = c_intra_angle[mode - 2];
         const bool vertical = mode >= 18;
@@ -473,11 +577,35 @@ __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode,
                 ws.refs[q + n] = vertical ? R[n2 - idx] : R[n2 + idx];  // side(idx)
             }
         }
-        __syncwarp();
+    } else if (mode == 1) {
+        int part = lane < n ? R[n2 + 1 + lane] + R[n2 - 1 - lane] : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+        if (lane == 0) ws.dc = (part + n) >> (log2n + 1);
+    }
+    __syncwarp();
+}
+
+// Intra TB of size 8..32, second part: prediction (intra.rs:257-372) and
+// residual add + clip (reconstruct.rs:214-251) of samples tl, tl + ts, ...
+// (one warp: tl = lane, ts = 32; a team of warps splits the block).
+__device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
+                                                 const WalkScratch& ws, int tl, int ts) {
+    const int n = 1 << log2n;
+    const int n2 = 2 * n;
+    const int32_t* R = ref_filtered(k, n, mode) ? ws.f : ws.s;
+    const int max_v = k.max_v;
+    const bool edge_filters = k.luma && n < 32;  // is_luma gate of predict_into
+    const int S = k.S;
+    const int16_t* res = k.res;
+    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    if (mode >= 2) {
+        const int angle = c_intra_angle[mode - 2];
+        const bool vertical = mode >= 18;
         const int a0 = vertical ? R[n2 + 1] : R[n2 - 1];  // above[1] / left[1]
         const int c0 = R[n2];
 #pragma unroll 4
-        for (int i = lane; i < n * n; i += 32) {
+        for (int i = tl; i < n * n; i += ts) {
             const int yy = i >> log2n, xx = i & (n - 1);
             const int a = vertical ? yy : xx;
             const int b = vertical ? xx : yy;
@@ -497,12 +625,9 @@ __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode,
             }
         }
     } else if (mode == 1) {  // DC
-        int part = lane < n ? R[n2 + 1 + lane] + R[n2 - 1 - lane] : 0;
-#pragma unroll
-        for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
-        const int dc = (part + n) >> (log2n + 1);
+        const int dc = ws.dc;
 #pragma unroll 4
-        for (int i = lane; i < n * n; i += 32) {
+        for (int i = tl; i < n * n; i += ts) {
             const int yy = i >> log2n, xx = i & (n - 1);
             int v = dc;
             if (edge_filters) {
@@ -521,7 +646,7 @@ __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode,
     } else {  // planar
         const int tr = R[n2 + n + 1], bl = R[n2 - n - 1];
 #pragma unroll 4
-        for (int i = lane; i < n * n; i += 32) {
+        for (int i = tl; i < n * n; i += ts) {
             const int yy = i >> log2n, xx = i & (n - 1);
             const int hh = (n - 1 - xx) * R[n2 - yy - 1] + (xx + 1) * tr;
             const int vv = (n - 1 - yy) * R[n2 + xx + 1] + (yy + 1) * bl;
@@ -532,6 +657,13 @@ __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode,
             }
         }
     }
+}
+
+// Intra TB of size 8..32 by one warp.
+__device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
+                                             uint32_t dec, WalkScratch& ws, int lane) {
+    intra_tb_prep(k, log2n, mode, x0, y0, dec, ws, lane);
+    intra_tb_predict(k, log2n, mode, x0, y0, coded, ws, lane, 32);
     __syncwarp();
 }
 
@@ -547,9 +679,23 @@ __device__ __forceinline__ uint32_t mark_rows(uint32_t dec, int x0, int y0, int 
     return dec;
 }
 
+// Luma intra TBs of at least 2^kTeamMinLog2 samples square are predicted by
+// a team of warps when the schedule asks for it: warp 0 prepares the
+// reference line, then warp 0 and the CTA's last warp (otherwise idle during
+// the walk) split the prediction.  Both warps walk the same records and take
+// the same decision per record, so every named barrier has both arrivals.
+constexpr int kTeamMinLog2 = 4;
+constexpr int kTeamBarrier = 1;
+
+__device__ __forceinline__ void team_sync(int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(kTeamBarrier), "r"(threads) : "memory");
+}
+
+template <int kTeam>
 __global__ void __launch_bounds__(kReconThreads)
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
         uint32_t* work_counter, uint32_t* dev_err, int c444, uint32_t spin_limit) {
+    static_assert(kTeam == 1 || kTeam == 2, "team of one or two warps");
     extern __shared__ __align__(16) unsigned char smem[];
     const ReconLayout lay(c444);
     uint32_t* s_item = (uint32_t*)(smem + lay.off_misc);
@@ -658,9 +804,11 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         cp_async_wait_all();
         __syncthreads();
         // ---- decode-order walk: warp c reconstructs component c ----
-        if (warp < ncomp) {
-            const int c = warp;
-            WalkScratch& ws = ((WalkScratch*)(smem + lay.off_ws))[c];
+        const bool helper = kTeam > 1 && warp == kReconWarps - 1;
+        if (warp < ncomp || helper) {
+            const int c = helper ? 0 : warp;
+            WalkScratch& ws = ((WalkScratch*)(smem + lay.off_ws))[warp];
+            WalkScratch& team_ws = ((WalkScratch*)(smem + lay.off_ws))[0];
             Comp k;
             k.S = c ? Sc : ctb;
             k.CW = ReconLayout::cw_of(k.S);
@@ -695,20 +843,28 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     const int x = (int)t.x - (tc ? ocx : oxl), y = (int)t.y - (tc ? ocy : oyl);
                     const int St = tc ? Sc : ctb;
                     if (x < 0 || y < 0 || x + n > St || y + n > St) {
-                        if (lane == 0 && c == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+                        if (lane == 0 && c == 0 && !helper) atomicOr(dev_err, DEV_ERR_BITSTREAM);
                         continue;
                     }
                     if (tc == c && (t.flags & HPVCD_TU_INTRA) && intra_pred_ok) {
                         const bool coded = (t.flags & HPVCD_TU_CBF) != 0;
                         if (t.mode > 34 || t.log2n > 5) {
-                            if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+                            if (lane == 0 && !helper) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+                        } else if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
+                            if (!helper) intra_tb_prep(k, t.log2n, t.mode, x, y, dec, team_ws, lane);
+                            team_sync(32 * kTeam);
+                            intra_tb_predict(k, t.log2n, t.mode, x, y, coded, team_ws, (helper ? 32 : 0) + lane,
+                                             32 * kTeam);
+                            team_sync(32 * kTeam);
+                        } else if (helper) {
+                            // smaller TBs are the leader's alone
                         } else if (t.log2n == 2) {
                             intra_tb4(k, t.mode, x, y, coded, dec, lane);
                         } else {
                             intra_tb_big(k, t.log2n, t.mode, x, y, coded, dec, ws, lane);
                         }
                     }
-                    if (tc == 0) dec = mark_rows(dec, x, y, n, lane, vis_w, vis_h);
+                    if (tc == 0 && !helper) dec = mark_rows(dec, x, y, n, lane, vis_w, vis_h);
                 }
                 __syncwarp();
             }
@@ -756,27 +912,36 @@ extern "C" size_t hpvcd_recon_smem_bytes(int c444) { return hpvcd::ReconLayout(c
 
 extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const uint32_t* rec_prefix,
                                              uint32_t n_pics, uint32_t total_records, uint32_t* dev_err,
-                                             int sms, cudaStream_t stream) {
+                                             int sms, int idct, cudaStream_t stream) {
     if (total_records == 0) return cudaSuccess;
     const uint32_t blocks_needed = (total_records + hpvcd::kResWarps - 1) / hpvcd::kResWarps;
     const uint32_t cap = (uint32_t)sms * 8u;
     const int grid = (int)(blocks_needed < cap ? blocks_needed : cap);
-    hpvcd::k_residual<<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix, n_pics, dev_err);
+    if (idct == hpvcd::kIdctButterfly)
+        hpvcd::k_residual<hpvcd::kIdctButterfly><<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix,
+                                                                                          n_pics, dev_err);
+    else
+        hpvcd::k_residual<hpvcd::kIdctMatrix><<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix, n_pics,
+                                                                                       dev_err);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }
 
 extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd::CtuItem* items,
                                           uint32_t n_items, uint32_t* work_counter, uint32_t* dev_err,
-                                          int c444, int grid, cudaStream_t stream) {
+                                          int c444, int grid, int team, cudaStream_t stream) {
     if (n_items == 0) return cudaSuccess;
     // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
     // when the plan was built (no non-stream API call here, so launches can
     // be captured into CUDA graphs)
     const size_t smem = hpvcd::ReconLayout(c444).total;
     // 2^22 polls of >= 64 ns each bound one neighbour wait to a few hundred ms.
-    hpvcd::k_recon<<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                 dev_err, c444, 1u << 22);
+    if (team == 2)
+        hpvcd::k_recon<2><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
+                                                                        dev_err, c444, 1u << 22);
+    else
+        hpvcd::k_recon<1><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
+                                                                        dev_err, c444, 1u << 22);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }
@@ -785,8 +950,10 @@ extern "C" int hpvcd_recon_occupancy(int c444) {
     int blocks = 0;
     // raise the limit for the larger layout, which covers both
     const size_t smem = hpvcd::ReconLayout(c444).total;
-    cudaFuncSetAttribute(hpvcd::k_recon, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(hpvcd::k_recon<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)hpvcd::ReconLayout(1).total);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon, hpvcd::kReconThreads, smem);
+    cudaFuncSetAttribute(hpvcd::k_recon<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)hpvcd::ReconLayout(1).total);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<1>, hpvcd::kReconThreads, smem);
     return blocks;
 }

@@ -19,14 +19,16 @@ using hpvcd::CtuItem;
 using hpvcd::DevPic;
 
 extern "C" cudaError_t hpvcd_launch_residual(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int,
-                                             cudaStream_t);
+                                             int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int,
-                                          int, cudaStream_t);
+                                          int, int, cudaStream_t);
 extern "C" int hpvcd_recon_occupancy(int c444);
 extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, uint8_t*, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_mc(const DevPic*, int, int, int, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_features(const DevPic*, uint32_t, uint32_t, unsigned long long*, float*, int,
+                                             cudaStream_t);
 
 static std::atomic<uint64_t> g_launches{0};
 extern "C" void hpvcd_note_launches(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -105,13 +107,14 @@ struct hpvcd_plan {
     size_t plane_bytes = 0;
     uint8_t* d_canvas = nullptr;
     size_t canvas_bytes = 0;
+    unsigned long long* d_feat = nullptr;  // k_features sums (32) + the feature vector (16 floats)
     hpvcd_output out{};
     std::vector<hpvcd_tile_place> places;
     std::vector<hpvcd_canvas> canvases;   // resolved canvas list (>= 1 for RGB8)
     std::vector<uint64_t> canvas_offs;
     hpvcd_sched sched{};
     int c444 = 0;
-    int recon_grid = 0;
+    int recon_occ = 1;  // k_recon CTAs per SM at full occupancy
     int sms = 148;
     int max_rgb = 0;
     uint32_t launches_per_run = 0;
@@ -160,6 +163,7 @@ struct hpvcd_plan {
         dfree(d_res);
         dfree(d_planes);
         dfree(d_canvas);
+        dfree(d_feat);
     }
 };
 
@@ -173,6 +177,13 @@ hpvcd_status cuda_status(cudaError_t e) {
     if (e == cudaErrorMemoryAllocation) return HPVCD_ERR_ALLOC;
     return HPVCD_ERR_CUDA;
 }
+
+}  // namespace
+
+// Status mapping shared with the other translation units of the library.
+extern "C" hpvcd_status hpvcd_internal_status(cudaError_t e) { return cuda_status(e); }
+
+namespace {
 
 // int16 residual planes of a picture, rows padded to 16 samples.
 inline int res_stride_of(int w) { return (w + 15) & ~15; }
@@ -270,7 +281,13 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     } else {
         P->out.kind = HPVCD_OUT_YUV;
     }
-    if (sched) P->sched = *sched;
+    if (sched) {
+        if (sched->idct > 1 || sched->luma_team > 2) {
+            delete P;
+            return HPVCD_ERR_INVALID_ARG;
+        }
+        P->sched = *sched;
+    }
     bool any_inter = false;
     for (uint32_t i = 0; i < n; ++i) {
         if (pics[i].chroma_idc == 3) P->c444 = 1;
@@ -319,6 +336,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         e = cudaMemcpyAsync(P->d_prefix, P->rec_prefix.data(), sizeof(uint32_t) * (n + 1), cudaMemcpyHostToDevice,
                             pool_stream);
     if (e == cudaSuccess) e = P->dmalloc(&P->d_scratch, P->scratch_words * sizeof(uint32_t));
+    if (e == cudaSuccess) e = P->dmalloc(&P->d_feat, 32 * sizeof(unsigned long long) + 16 * sizeof(float));
     if (e == cudaSuccess && P->out.kind == HPVCD_OUT_RGB8) {
         P->canvas_bytes = 0;
         for (const hpvcd_canvas& cv : P->canvases) P->canvas_bytes += (size_t)cv.width * cv.height * 3;
@@ -435,10 +453,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
     P->sms = sms;
-    int occ = hpvcd_recon_occupancy(P->c444);
-    if (occ <= 0) occ = 1;
-    if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
-    P->recon_grid = sms * occ;
+    P->recon_occ = std::max(1, hpvcd_recon_occupancy(P->c444));
     P->launches_per_run = P->launches_for(HPVCD_STAGE_ALL);
     *result = P;
     return HPVCD_OK;
@@ -479,11 +494,13 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
                 }
             const uint32_t nrec = P->rec_prefix[s.first_pic + s.n_pics] - P->rec_prefix[s.first_pic];
             e = hpvcd_launch_residual(P->d_pics + s.first_pic, P->d_prefix + s.first_pic, s.n_pics, nrec, d_err,
-                                      P->sms, st);
+                                      P->sms, (int)P->sched.idct, st);
             if (e != cudaSuccess) return cuda_status(e);
-            const int grid = std::max(1, std::min<int>(P->recon_grid, (int)s.n_items));
+            int occ = P->recon_occ;
+            if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
+            const int grid = std::max(1, std::min<int>(P->sms * occ, (int)s.n_items));
             e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
-                                   P->c444, grid, st);
+                                   P->c444, grid, (int)P->sched.luma_team, st);
             if (e != cudaSuccess) return cuda_status(e);
         }
         if (stages & HPVCD_STAGE_DEBLOCK) {
@@ -837,6 +854,104 @@ HPVCD_API hpvcd_status hpvcd_plan_device_status(hpvcd_plan* plan, void* stream) 
 
 HPVCD_API uint32_t hpvcd_plan_launches_per_run(const hpvcd_plan* plan) {
     return plan ? plan->launches_per_run : 0;
+}
+
+HPVCD_API hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched);
+
+// Feature vector (16 floats, include/hpvcd_gpu.h) of pictures [first, first +
+// count) of the plan into dev_out (device memory), enqueued on `stream`.
+HPVCD_API hpvcd_status hpvcd_plan_features(hpvcd_plan* plan, uint32_t first, uint32_t count, float* dev_out,
+                                           void* stream) {
+    if (!plan || !dev_out || count == 0 || first + count > plan->src.size() || first + count < first)
+        return HPVCD_ERR_INVALID_ARG;
+    uint32_t max_rec = 1;
+    for (uint32_t i = first; i < first + count; ++i)
+        max_rec = std::max(max_rec, std::max(plan->src[i].n_tus, plan->src[i].n_pus));
+    return cuda_status(hpvcd_launch_features(plan->d_pics + first, count, max_rec, plan->d_feat, dev_out, plan->sms,
+                                             (cudaStream_t)stream));
+}
+
+// Exhaustive autotuning: one untimed launch, then per candidate schedule
+// `warmup` untimed and `reps` timed launches (CUDA events on `stream`);
+// ms[i] = the fastest timed launch.  The fastest candidate stays set.
+HPVCD_API hpvcd_status hpvcd_plan_autotune(hpvcd_plan* plan, const hpvcd_sched* cands, uint32_t n, uint32_t stages,
+                                           uint32_t reps, uint32_t warmup, void* stream, float* ms, uint32_t* best) {
+    if (!plan || !cands || n == 0 || reps == 0 || reps > 64 || warmup > 64) return HPVCD_ERR_INVALID_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t ev[2];
+    cudaError_t e = cudaEventCreate(&ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev[1]);
+    if (e != cudaSuccess) return cuda_status(e);
+    hpvcd_status s = HPVCD_OK;
+    uint32_t arg = 0;
+    float best_ms = 0.f;
+    std::vector<float> t(reps);
+    s = hpvcd_plan_set_sched(plan, &cands[0]);
+    if (s == HPVCD_OK) s = plan_launch(plan, stages & HPVCD_STAGE_ALL, st);
+    for (uint32_t c = 0; c < n && s == HPVCD_OK; ++c) {
+        s = hpvcd_plan_set_sched(plan, &cands[c]);
+        for (uint32_t w = 0; w < warmup && s == HPVCD_OK; ++w) s = plan_launch(plan, stages & HPVCD_STAGE_ALL, st);
+        for (uint32_t r = 0; r < reps && s == HPVCD_OK; ++r) {
+            e = cudaEventRecord(ev[0], st);
+            if (e == cudaSuccess) s = plan_launch(plan, stages & HPVCD_STAGE_ALL, st);
+            if (s == HPVCD_OK && e == cudaSuccess) e = cudaEventRecord(ev[1], st);
+            if (s == HPVCD_OK && e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+            if (s == HPVCD_OK && e == cudaSuccess) e = cudaEventElapsedTime(&t[r], ev[0], ev[1]);
+            if (s == HPVCD_OK && e != cudaSuccess) s = cuda_status(e);
+        }
+        if (s != HPVCD_OK) break;
+        const float fastest = *std::min_element(t.begin(), t.end());
+        if (ms) ms[c] = fastest;
+        if (c == 0 || fastest < best_ms) {
+            best_ms = fastest;
+            arg = c;
+        }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (s != HPVCD_OK) return s;
+    if (best) *best = arg;
+    return hpvcd_plan_set_sched(plan, &cands[arg]);
+}
+
+HPVCD_API hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched) {
+    if (!plan) return HPVCD_ERR_INVALID_ARG;
+    const hpvcd_sched next = sched ? *sched : hpvcd_sched{};
+    if (next.idct > 1 || next.luma_team > 2) return HPVCD_ERR_INVALID_ARG;
+    if (std::memcmp(&next, &plan->sched, sizeof(next)) == 0) return HPVCD_OK;
+    plan->sched = next;
+    // graphs captured with the previous schedule hold its kernels
+    for (cudaGraphExec_t& gx : plan->graphs)
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
+    return HPVCD_OK;
+}
+
+extern "C" hpvcd_status hpvcd_mlp_pick(hpvcd_mlp*, const float*, uint32_t, void*, uint32_t*);
+extern "C" uint32_t hpvcd_mlp_variants(const hpvcd_mlp*);
+
+// Schedule selection for a plan: with a selector network, the features of
+// the whole batch are computed on the device and the network's predicted-
+// fastest candidate is set; without one (or when its candidate count does
+// not match) exhaustive autotuning over the candidates decides.
+HPVCD_API hpvcd_status hpvcd_plan_select(hpvcd_plan* plan, hpvcd_mlp* mlp, const hpvcd_sched* cands, uint32_t n,
+                                         void* stream, uint32_t* chosen) {
+    if (!plan || !cands || n == 0) return HPVCD_ERR_INVALID_ARG;
+    uint32_t pick = 0;
+    hpvcd_status s;
+    if (mlp && hpvcd_mlp_variants(mlp) == n) {
+        float* fv = (float*)(plan->d_feat + 32);
+        s = hpvcd_plan_features(plan, 0, (uint32_t)plan->src.size(), fv, stream);
+        if (s == HPVCD_OK) s = hpvcd_mlp_pick(mlp, fv, 1, stream, &pick);
+        if (s == HPVCD_OK && pick >= n) s = HPVCD_ERR_INVALID_ARG;
+        if (s == HPVCD_OK) s = hpvcd_plan_set_sched(plan, &cands[pick]);
+    } else {
+        s = hpvcd_plan_autotune(plan, cands, n, HPVCD_STAGE_ALL, 2, 1, stream, nullptr, &pick);
+    }
+    if (s == HPVCD_OK && chosen) *chosen = pick;
+    return s;
 }
 
 HPVCD_API hpvcd_status hpvcd_gpu_create(const hpvcd_gpu_cfg* cfg, hpvcd_gpu** out) {
@@ -1300,12 +1415,13 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
             if (e != cudaSuccess) return cuda_status(e);
         }
     const uint32_t* prefix = (const uint32_t*)(base + L.prefix);
-    e = hpvcd_launch_residual(dp, prefix, 1, p.n_tus, d_err, nd->sms, st);
+    e = hpvcd_launch_residual(dp, prefix, 1, p.n_tus, d_err, nd->sms, 0, st);
     if (e != cudaSuccess) return cuda_status(e);
     if (d.needs_wavefront) {
         const int c444 = p.chroma_idc == 3 ? 1 : 0;
         const int grid = std::max(1, std::min<int>(nd->sms * nd->occ[c444], (int)n_ctu));
-        e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, c444, grid, st);
+        e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, c444, grid, 1,
+                               st);
         if (e != cudaSuccess) return cuda_status(e);
     }
     const int lv = (d.w >= 12 ? (d.w - 4) / 8 : 0) * (d.h / 4);

@@ -152,6 +152,18 @@ struct Gen {
             }
     }
 
+    // TU split probability at a level: tu_split_p, or the conditional
+    // probability that a TB of this size splits given the target area mix.
+    float split_p(int log2) const {
+        const float* m = c.tu_mix;
+        const float tot = m[0] + m[1] + m[2] + m[3];
+        if (!(tot > 0.f)) return c.tu_split_p;
+        float below = 0.f;  // mass of the sizes smaller than this level
+        for (int k = 0; k < log2 - 2; ++k) below += m[k];
+        const float here = m[log2 - 2];
+        return below + here > 0.f ? below / (below + here) : 1.f;
+    }
+
     // Transform tree of an intra or inter CU (decode.rs:3315 transform_tree,
     // :3478 transform_unit ordering: luma TB, then Cb TB(s), then Cr TB(s);
     // for 4:2:0 4x4 luma TBs the chroma TB follows the fourth one).
@@ -161,7 +173,7 @@ struct Gen {
         if (x0 >= w || y0 >= h) return;
         const int size = 1 << log2;
         bool split = log2 > 5 || (nxn && depth == 0);
-        if (!split && log2 > 2 && rng.bern(c.tu_split_p)) split = true;
+        if (!split && log2 > 2 && rng.bern(split_p(log2))) split = true;
         if (split) {
             const int half = size / 2;
             for (int b = 0; b < 4; ++b)
@@ -312,7 +324,7 @@ struct Gen {
     void residual_ctu(int x0, int y0, int log2, int xbase, int ybase, int blk) {
         if (x0 >= w || y0 >= h) return;
         const int size = 1 << log2;
-        if (log2 > 5 || (log2 > 2 && rng.bern(c.tu_split_p))) {
+        if (log2 > 5 || (log2 > 2 && rng.bern(split_p(log2)))) {
             for (int b = 0; b < 4; ++b)
                 residual_ctu(x0 + (b & 1) * size / 2, y0 + (b >> 1) * size / 2, log2 - 1, x0, y0, b);
             return;

@@ -160,7 +160,7 @@ class DevicePlan:
     """Upload the flat buffers of `pics` to HBM once and build a plan."""
 
     def __init__(self, pics, output: abi.Output | None = None, sched: abi.Sched | None = None,
-                 device: int = 0):
+                 device: int = 0, resident: dict | None = None):
         torch = _torch()
         self._L = abi.lib()
         self.torch = torch
@@ -169,7 +169,10 @@ class DevicePlan:
         self.host_pics = list(pics)
         dev = []
         self.input_bytes = 0
-        for p in pics:
+        for i, p in enumerate(pics):
+            if resident and i in resident:  # descriptor already pointing at device buffers
+                dev.append(resident[i])
+                continue
             g = geometry(p)
             ctbs = g["ctb_cols"] * g["ctb_rows"]
             d = abi.Picture()
@@ -213,6 +216,10 @@ class DevicePlan:
     def status(self, stream=None) -> int:
         s = stream if stream is not None else self.torch.cuda.current_stream(self.device)
         return self._L.hpvcd_plan_device_status(self._h, C.c_void_p(s.cuda_stream))
+
+    def set_sched(self, sched: abi.Sched | None) -> None:
+        _check(self._L.hpvcd_plan_set_sched(self._h, C.byref(sched) if sched is not None else None),
+               "hpvcd_plan_set_sched")
 
     def canvas(self) -> np.ndarray:
         ptr, nb = C.c_void_p(), C.c_uint64()

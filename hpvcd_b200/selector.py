@@ -1,0 +1,318 @@
+"""Schedule selection: exhaustive autotuning and the learned selector.
+
+The schedule of a batch (include/hpvcd_gpu.h `hpvcd_sched`) picks kernel
+variants that never change pixels: the inverse transform of k_residual
+(matrix product with zero rows / columns skipped, or even-odd butterflies for
+16x16 / 32x32), the team size of the luma intra walk in k_recon (one warp, or
+two for 16x16 / 32x32 TBs) and the persistent k_recon CTAs per SM (occupancy
+maximum, or one).  Which is fastest depends on the batch: its TB-size mix,
+coefficient density, QP, intra share, size and picture count.
+
+* Exhaustive autotuning (`hpvcd_plan_autotune`) times every schedule on the
+  batch itself: always right, but K decodes' worth of time.
+* The selector network (`hpvcd_mlp_*`, 16 -> 64 -> 64 -> K, bf16 weights,
+  fp32 accumulation, forward / backward / Adam as CUDA kernels in
+  csrc/selector.cu) predicts log(t_k / t_best) for every schedule from the
+  batch's 16 features (`hpvcd_plan_features`, computed on the device from the
+  TB / PU records) and picks the argmin.  It is trained on timings that the
+  autotuner measures, and autotuning stays the fallback (no network) and the
+  judge (its timings score the network's picks).
+
+Frames of the selector workload: 3840x2160 10-bit 4:2:0, QP uniform 17-42,
+TB-size area mix Dirichlet(1, 1, 1, 1) over 4/8/16/32, coded-block fraction
+5-60 %, 30 % intra frames and 70 % inter frames (intra-CU share 0-30 %, MV
+standard deviation 1-32 luma samples, 40 % bi-prediction, 10 % explicit
+weighted prediction), all seeded synthetic.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi, synth
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+WEIGHTS_PATH = os.path.join(HERE, "selector_weights.npz")
+
+# The candidate schedules, in output order of the network.
+SCHEDULES = [abi.Sched(idct, team, ctas, 0) for idct in (0, 1) for team in (1, 2) for ctas in (0, 1)]
+DEFAULT = 0  # (matrix transform, one-warp walk, occupancy maximum): the all-zero schedule
+K = len(SCHEDULES)
+
+
+def schedules_array():
+    return (abi.Sched * K)(*SCHEDULES)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _check(rc, what):
+    abi.check(rc, what)
+
+
+class Mlp:
+    """The selector network on the GPU (hpvcd_mlp_*)."""
+
+    def __init__(self, n_variants: int = K, seed: int = 1, device: int = 0):
+        self.torch = _torch()
+        self.dev = self.torch.device("cuda", device)
+        self._L = abi.lib()
+        h = C.c_void_p()
+        _check(self._L.hpvcd_mlp_create(n_variants, seed, C.byref(h)), "hpvcd_mlp_create")
+        self._h = h
+        self.K = n_variants
+        self.P = self._L.hpvcd_mlp_param_count(h)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _stream(self):
+        return C.c_void_p(self.torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def _dev(self, a, width):
+        t = self.torch.as_tensor(np.ascontiguousarray(a, np.float32).reshape(-1, width), device=self.dev)
+        return t.contiguous()
+
+    def params(self, master: bool = False) -> np.ndarray:
+        out = np.empty(self.P, np.float32)
+        _check(self._L.hpvcd_mlp_get_params(self._h, out.ctypes.data_as(C.c_void_p), int(master)),
+               "hpvcd_mlp_get_params")
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.P
+        _check(self._L.hpvcd_mlp_set_params(self._h, p.ctypes.data_as(C.c_void_p)), "hpvcd_mlp_set_params")
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        X = self._dev(x, abi.FEATURES)
+        Y = self.torch.empty((X.shape[0], self.K), dtype=self.torch.float32, device=self.dev)
+        _check(self._L.hpvcd_mlp_forward(self._h, C.c_void_p(X.data_ptr()), X.shape[0], C.c_void_p(Y.data_ptr()),
+                                         self._stream()), "hpvcd_mlp_forward")
+        return Y.cpu().numpy()
+
+    def grad(self, x: np.ndarray, t: np.ndarray):
+        X = self._dev(x, abi.FEATURES)
+        T = self._dev(t, self.K)
+        G = self.torch.empty(self.P, dtype=self.torch.float32, device=self.dev)
+        Lo = self.torch.empty(1, dtype=self.torch.float32, device=self.dev)
+        _check(self._L.hpvcd_mlp_grad(self._h, C.c_void_p(X.data_ptr()), C.c_void_p(T.data_ptr()), X.shape[0],
+                                      C.c_void_p(G.data_ptr()), C.c_void_p(Lo.data_ptr()), self._stream()),
+               "hpvcd_mlp_grad")
+        return float(Lo.item()), G.cpu().numpy()
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int = 200, batch: int = 256, lr: float = 2e-3,
+              seed: int = 7) -> float:
+        X = self._dev(x, abi.FEATURES)
+        T = self._dev(t, self.K)
+        loss = C.c_float()
+        _check(self._L.hpvcd_mlp_train(self._h, C.c_void_p(X.data_ptr()), C.c_void_p(T.data_ptr()), X.shape[0],
+                                       batch, epochs, lr, seed, self._stream(), C.byref(loss)), "hpvcd_mlp_train")
+        return loss.value
+
+    def pick(self, x: np.ndarray) -> np.ndarray:
+        X = self._dev(x, abi.FEATURES)
+        out = np.empty(X.shape[0], np.uint32)
+        _check(self._L.hpvcd_mlp_pick(self._h, C.c_void_p(X.data_ptr()), X.shape[0], self._stream(),
+                                      out.ctypes.data_as(C.POINTER(C.c_uint32))), "hpvcd_mlp_pick")
+        return out
+
+    def save(self, path: str = WEIGHTS_PATH) -> None:
+        np.savez(path, params=self.params(master=True), n_variants=self.K,
+                 schedules=np.array([[s.idct, s.luma_team, s.recon_ctas_per_sm] for s in SCHEDULES], np.int32))
+
+    @classmethod
+    def load(cls, path: str = WEIGHTS_PATH, device: int = 0) -> "Mlp":
+        z = np.load(path)
+        m = cls(int(z["n_variants"]), device=device)
+        m.set_params(z["params"])
+        return m
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.hpvcd_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Targets and scoring
+# ---------------------------------------------------------------------------
+
+def targets(ms: np.ndarray) -> np.ndarray:
+    """Network targets: log(t_k / t_best) per row of measured times."""
+    ms = np.asarray(ms, np.float64)
+    return np.log(ms / ms.min(axis=1, keepdims=True)).astype(np.float32)
+
+
+def score(picks: np.ndarray, ms: np.ndarray) -> dict:
+    """Decode time achieved by a pick per frame against the autotuned optimum
+    and the fixed default schedule (all from measured times)."""
+    ms = np.asarray(ms, np.float64)
+    n = len(ms)
+    best = ms.min(axis=1)
+    chosen = ms[np.arange(n), np.asarray(picks)]
+    default = ms[:, DEFAULT]
+    return {
+        "frames": int(n),
+        "pick_accuracy": float(np.mean(np.asarray(picks) == ms.argmin(axis=1))),
+        "within_1pct": float(np.mean(chosen <= best * 1.01)),
+        "ms_selected": float(chosen.mean()),
+        "ms_exhaustive": float(best.mean()),
+        "ms_default": float(default.mean()),
+        "gain_vs_default": float(default.sum() / chosen.sum() - 1.0),
+        "regret_vs_exhaustive": float(chosen.sum() / best.sum() - 1.0),
+    }
+
+
+def best_fixed(ms: np.ndarray) -> int:
+    """The single schedule with the lowest total time (the best the method
+    without a network can do without timing each batch)."""
+    return int(np.asarray(ms).sum(axis=0).argmin())
+
+
+# ---------------------------------------------------------------------------
+# Selector-workload frames and their measurement
+# ---------------------------------------------------------------------------
+
+@dataclass
+class FrameSpec:
+    seed: int
+    intra: bool
+    qp: int
+    tu_mix: tuple
+    cbf: float
+    intra_cu: float
+    mv_sd: float
+    bi: float
+    weighted: bool
+
+
+def frame_specs(n: int, seed: int = 0) -> list[FrameSpec]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        mix = tuple(float(v) for v in rng.dirichlet([1.0, 1.0, 1.0, 1.0]))
+        out.append(FrameSpec(seed=seed * 1_000_003 + i, intra=bool(rng.random() < 0.3),
+                             qp=int(rng.integers(17, 43)), tu_mix=mix, cbf=float(rng.uniform(0.05, 0.6)),
+                             intra_cu=float(rng.uniform(0.0, 0.3)), mv_sd=float(rng.uniform(1.0, 32.0)),
+                             bi=0.4, weighted=bool(rng.random() < 0.1)))
+    return out
+
+
+W4K, H4K = 3840, 2160
+
+
+def _frame_cfg(sp: FrameSpec, w=W4K, h=H4K) -> abi.SynthCfg:
+    if sp.intra:
+        c = synth.intra_cfg(sp.seed, w, h, bit_depth=10, chroma_idc=1)
+    else:
+        c = synth.inter_cfg(sp.seed, w, h, bit_depth=10, weighted=sp.weighted, n_refs=2,
+                            intra_cu_p=sp.intra_cu, bi_p=sp.bi)
+        c.mv_sd = sp.mv_sd
+    c.qp_min, c.qp_max = sp.qp, min(sp.qp + 2, 51)
+    c.cbf_p = sp.cbf
+    c.cu_split_p = 0.25
+    for k in range(4):
+        c.tu_mix[k] = sp.tu_mix[k]
+    return c
+
+
+class RefPictures:
+    """Two reference pictures for the inter frames: prediction-in-plane
+    pictures with no TB records, so decoding them is only the copy of their
+    planes.  Uploaded once (`resident` maps plan indices 0 and 1 to their
+    device descriptors)."""
+
+    def __init__(self, w=W4K, h=H4K, seed=99, upload: bool = True):
+        self.synth = synth.SynthSet()
+        for r in range(2):
+            c = synth.residual_cfg(seed + r, w, h, bit_depth=10, chroma_idc=1)
+            c.tu_split_p = 0.0
+            self.synth.add(c)
+        self.pics = []
+        for p in self.synth.pictures():
+            q = abi.Picture()
+            C.pointer(q)[0] = p
+            q.n_tus = 0
+            q.n_coeffs = 0
+            self.pics.append(q)
+        self.resident = None
+        self._plan = None
+        if upload:
+            from .gpu import DevicePlan
+            self._plan = DevicePlan(self.pics)  # owns the device copies
+            self.resident = {0: self._plan.dev_pics[0], 1: self._plan.dev_pics[1]}
+
+
+def build_frame(sp: FrameSpec, refs: RefPictures | None, w=W4K, h=H4K):
+    """Returns (keep-alive SynthSet, pictures of the plan, index of the frame)."""
+    s = synth.SynthSet()
+    if sp.intra:
+        s.add(_frame_cfg(sp, w, h))
+        return s, [s.picture(0)], 0
+    for r in range(2):  # placeholders so the frame's reference slots are 1 and 0
+        s.add(synth.residual_cfg(1 + r, 64, 64, bit_depth=10))
+    s.add(_frame_cfg(sp, w, h))
+    return s, [refs.pics[0], refs.pics[1], s.picture(2)], 2
+
+
+def measure(plan, frame_index: int, reps: int = 2, stages: int = abi.STAGE_ALL):
+    """Features of the frame and the autotuner's time of every schedule."""
+    torch = _torch()
+    L = abi.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    f = torch.empty(abi.FEATURES, dtype=torch.float32, device="cuda")
+    _check(L.hpvcd_plan_features(plan._h, frame_index, 1, C.c_void_p(f.data_ptr()), st), "hpvcd_plan_features")
+    ms = (C.c_float * K)()
+    best = C.c_uint32()
+    _check(L.hpvcd_plan_autotune(plan._h, schedules_array(), K, stages, reps, 0, st, ms, C.byref(best)),
+           "hpvcd_plan_autotune")
+    _check(plan.status(), "device status")
+    return f.cpu().numpy(), np.array(ms[:], np.float32)
+
+
+def collect(n_frames: int, seed: int = 0, out_path: str | None = None, threads: int = 8, reps: int = 2,
+            log_every: int = 100, start: int = 0):
+    """Generate, decode and time `n_frames` selector-workload frames; returns
+    (features [n][16], ms [n][K]).  Frames are generated on `threads` host
+    threads while the GPU measures earlier ones."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from .gpu import DevicePlan
+
+    specs = frame_specs(start + n_frames, seed)[start:]
+    refs = RefPictures()
+    X = np.zeros((n_frames, abi.FEATURES), np.float32)
+    T = np.zeros((n_frames, K), np.float32)
+    done = 0
+    with ThreadPoolExecutor(threads) as pool:
+        futs = [pool.submit(build_frame, sp, refs) for sp in specs[:threads * 2]]
+        nxt = len(futs)
+        for i in range(n_frames):
+            keep, pics, fi = futs[i].result()
+            futs[i] = None
+            if nxt < n_frames:
+                futs.append(pool.submit(build_frame, specs[nxt], refs))
+                nxt += 1
+            plan = DevicePlan(pics, resident=refs.resident if fi else None)
+            X[i], T[i] = measure(plan, fi, reps=reps)
+            plan.close()
+            del keep
+            done = i + 1
+            if out_path and (done % log_every == 0 or done == n_frames):
+                np.savez(out_path, features=X[:done], ms=T[:done], seed=seed, start=start)
+                print(f"[selector] {done}/{n_frames} frames", flush=True)
+    return X[:done], T[:done]

@@ -71,6 +71,13 @@ def tus_of(p: abi.Picture) -> np.ndarray:
     return np.frombuffer(buf, dtype=abi.TU_DTYPE)
 
 
+def pus_of(p: abi.Picture) -> np.ndarray:
+    if p.n_pus == 0:
+        return np.zeros(0, abi.PU_DTYPE)
+    buf = (C.c_uint8 * (p.n_pus * abi.PU_DTYPE.itemsize)).from_address(p.pus)
+    return np.frombuffer(buf, dtype=abi.PU_DTYPE)
+
+
 def coeffs_of(p: abi.Picture) -> np.ndarray:
     if p.n_coeffs == 0:
         return np.zeros(0, np.int16)

@@ -315,13 +315,14 @@ typedef struct hpvcd_plan hpvcd_plan;
                                  /* captured on first use (stream must not be   */
                                  /* the legacy default stream)                   */
 
-/* Variant knobs chosen by the autotuner / schedule selector.  They never
- * change pixels, only speed. */
+/* Schedule knobs chosen by the autotuner / schedule selector.  They never
+ * change pixels, only speed.  All zero is the default schedule. */
 typedef struct hpvcd_sched {
-    uint32_t recon_threads; /* threads per CTU worker of the intra wavefront: 32|64|128 */
-    uint32_t recon_ctas_per_sm; /* persistent CTAs per SM (0 -> occupancy max) */
-    uint32_t filter_tile;   /* post-filter tile edge in luma samples: 32|64   */
-    uint32_t fuse_filters;  /* 1: fused deblock+SAO+RGB kernel, 0: separate passes */
+    uint32_t idct;              /* k_residual inverse transform: 0 matrix product with all-zero
+                                   rows / columns skipped, 1 even-odd butterflies for 16x16 / 32x32 */
+    uint32_t luma_team;         /* warps predicting a 16x16 / 32x32 luma intra TB: 0|1 one, 2 two */
+    uint32_t recon_ctas_per_sm; /* persistent wavefront CTAs per SM (0 -> occupancy max) */
+    uint32_t rsvd;              /* zero */
 } hpvcd_sched;
 
 hpvcd_status hpvcd_plan_create(const hpvcd_picture* dev_pics, uint32_t n,
@@ -339,6 +340,78 @@ hpvcd_status hpvcd_plan_canvas(hpvcd_plan* plan, void** rgb, uint64_t* bytes);
 hpvcd_status hpvcd_plan_device_status(hpvcd_plan* plan, void* stream);
 /* Number of kernel launches one hpvcd_plan_launch(HPVCD_STAGE_ALL) issues. */
 uint32_t hpvcd_plan_launches_per_run(const hpvcd_plan* plan);
+/* Schedule of the plan's next launches (NULL = default); drops CUDA graphs
+ * captured with the previous schedule.  Pixels do not depend on it. */
+hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched);
+
+/* ------------------------------------------------------------------------ */
+/* Schedule selection: exhaustive autotuning and a learned selector.  No    */
+/* reference counterpart (the reference picks SIMD kernels by CPU feature  */
+/* only, src/exec.rs).  Pixels never depend on the schedule.               */
+/* ------------------------------------------------------------------------ */
+#define HPVCD_FEATURES 16      /* per-batch statistics the selector reads      */
+#define HPVCD_MLP_HIDDEN 64    /* 16 -> 64 -> 64 -> K                          */
+#define HPVCD_MLP_MAX_VARIANTS 32
+
+/* Features of pictures [first, first + count) of a plan, computed on the
+ * device from the TB / PU records and written to dev_out (16 floats, device
+ * memory) on `stream`:
+ *   0 log2(luma samples) / 24      1 log2(1 + pictures) / 8
+ *   2 max wavefront length (ctb_cols + 2 ctb_rows) / 256
+ *   3 (mean luma bit depth - 8) / 4   4 4:4:4 share of the area
+ *   5-8 luma TB area share of 4x4, 8x8, 16x16, 32x32 TBs
+ *   9 coded luma TB area / luma area  10 intra luma TB area / luma area
+ *   11 mean QpY / 51   12 std QpY / 16
+ *   13 mean (nx / n) over coded luma TBs (coefficient extent)
+ *   14 log2(1 + mean |mv| in luma samples) / 8   15 bi-predicted PU share */
+hpvcd_status hpvcd_plan_features(hpvcd_plan* plan, uint32_t first, uint32_t count, float* dev_out,
+                                 void* stream);
+/* Exhaustive autotuning: one untimed launch, then per candidate `warmup`
+ * untimed and `reps` timed launches (CUDA events on `stream`, selected
+ * stages); ms[i] (host, may be NULL) = the fastest timed launch of
+ * candidate i.  The fastest candidate stays set on the plan, its index in
+ * *best (may be NULL). */
+hpvcd_status hpvcd_plan_autotune(hpvcd_plan* plan, const hpvcd_sched* cands, uint32_t n,
+                                 uint32_t stages, uint32_t reps, uint32_t warmup, void* stream,
+                                 float* ms, uint32_t* best);
+
+/* The selector network: y = W3 relu(W2 relu(W1 x + b1) + b2) + b3, bf16
+ * parameters, fp32 accumulation; y[k] predicts log(time of variant k / time
+ * of the fastest variant) and the pick is argmin y.  Parameters are one flat
+ * vector: W1 [64][16], b1 [64], W2 [64][64], b2 [64], W3 [K][64], b3 [K]
+ * (row-major [out][in]).  Training keeps an fp32 master copy (Adam). */
+typedef struct hpvcd_mlp hpvcd_mlp;
+hpvcd_status hpvcd_mlp_create(uint32_t n_variants, uint64_t seed, hpvcd_mlp** out);
+hpvcd_status hpvcd_mlp_destroy(hpvcd_mlp* mlp);
+uint32_t hpvcd_mlp_param_count(const hpvcd_mlp* mlp);
+uint32_t hpvcd_mlp_variants(const hpvcd_mlp* mlp);
+/* Host copy of the parameters: master != 0 -> fp32 master copy, else the
+ * bf16 values the forward pass uses (widened to fp32). */
+hpvcd_status hpvcd_mlp_get_params(hpvcd_mlp* mlp, float* host, int master);
+/* Set the master copy (and its bf16 rounding) from host fp32; resets Adam. */
+hpvcd_status hpvcd_mlp_set_params(hpvcd_mlp* mlp, const float* host);
+/* y [B][K] = forward(x [B][16]); device pointers. */
+hpvcd_status hpvcd_mlp_forward(hpvcd_mlp* mlp, const float* dev_x, uint32_t B, float* dev_y,
+                               void* stream);
+/* Gradient of L = mean over B*K of (forward(x) - t)^2 with respect to the
+ * parameters (dev_grad, param_count floats, may be NULL) and L (dev_loss,
+ * may be NULL); the gradient is also kept for hpvcd_mlp_adam_step. */
+hpvcd_status hpvcd_mlp_grad(hpvcd_mlp* mlp, const float* dev_x, const float* dev_t, uint32_t B,
+                            float* dev_grad, float* dev_loss, void* stream);
+/* One Adam step (beta 0.9 / 0.999) with the last gradient. */
+hpvcd_status hpvcd_mlp_adam_step(hpvcd_mlp* mlp, float lr, void* stream);
+/* Mini-batch Adam for `epochs` seeded shuffled passes over n rows. */
+hpvcd_status hpvcd_mlp_train(hpvcd_mlp* mlp, const float* dev_x, const float* dev_t, uint32_t n,
+                             uint32_t batch, uint32_t epochs, float lr, uint64_t seed, void* stream,
+                             float* final_loss);
+/* argmin forward(x) of B feature rows (device) into host_variant[B]. */
+hpvcd_status hpvcd_mlp_pick(hpvcd_mlp* mlp, const float* dev_x, uint32_t B, void* stream,
+                            uint32_t* host_variant);
+/* Choose the plan's schedule among n candidates: the network's pick from
+ * the plan's features when mlp has n outputs, else exhaustive autotuning
+ * (the fallback).  *chosen = the candidate index. */
+hpvcd_status hpvcd_plan_select(hpvcd_plan* plan, hpvcd_mlp* mlp, const hpvcd_sched* cands,
+                               uint32_t n, void* stream, uint32_t* chosen);
 
 /* ------------------------------------------------------------------------ */
 /* Decoding one picture without allocating.  No counterpart in the          */

@@ -357,3 +357,48 @@ def test_server_zero_copy_matches_oracle():
         out, kk = synth.grid_output(synth.Grid(w, h, 512, s, places))
         _, ref = O.decode_batch(pics, out, want_planes=False)
         assert np.array_equal(got[k]["image"], ref), k
+
+
+# --- schedule variants: every knob combination gives the same pixels -------
+def _dense_cfg(cfg):
+    cfg.qp_min, cfg.qp_max = 4, 14      # fine quantisation: large dequantised values
+    cfg.zero_frac = 0.2                 # dense blocks (butterfly path without zero rows)
+    cfg.laplace_scale = 60.0
+    cfg.tu_split_p = 0.2                # mostly 16x16 / 32x32 TBs
+    return cfg
+
+
+def test_schedule_variants_bit_exact():
+    s = synth.SynthSet()
+    s.add(_dense_cfg(synth.intra_cfg(80, 320, 256, bit_depth=8, chroma_idc=1)))    # i16 wrap at 8 bits
+    s.add(_dense_cfg(synth.intra_cfg(81, 256, 192, bit_depth=12, chroma_idc=3)))   # 32x32 chroma TBs
+    s.add(synth.intra_cfg(82, 512, 512, bit_depth=10, chroma_idc=1))
+    s.add(_dense_cfg(synth.residual_cfg(83, 256, 256, bit_depth=10)))              # in-plane add path
+    pics = s.pictures()
+    ref, _ = O.decode_batch(pics)
+    plan = DevicePlan(pics)
+    for idct in (0, 1):
+        for team in (1, 2):
+            for ctas in (0, 1):
+                plan.set_sched(abi.Sched(idct, team, ctas, 0))
+                plan.launch()
+                assert plan.status() == abi.OK
+                got = [plan.planes(i) for i in range(len(pics))]
+                assert_planes_equal(got, ref, f"idct={idct} team={team} ctas={ctas}")
+    plan.close()
+
+
+def test_schedule_variants_inter_bit_exact():
+    s = synth.SynthSet()
+    s.add(_dense_cfg(synth.intra_cfg(90, 320, 192, bit_depth=8)))
+    for i in range(1, 4):
+        s.add(_dense_cfg(synth.inter_cfg(90 + i, 320, 192, weighted=(i == 2))))
+    pics = s.pictures()
+    ref, _ = O.decode_batch(pics)
+    plan = DevicePlan(pics)
+    for sched in (abi.Sched(1, 2, 0, 0), abi.Sched(1, 1, 1, 0), abi.Sched(0, 2, 0, 0)):
+        plan.set_sched(sched)
+        plan.launch()
+        assert plan.status() == abi.OK
+        assert_planes_equal([plan.planes(i) for i in range(len(pics))], ref, "inter variants")
+    plan.close()
