@@ -319,19 +319,28 @@ struct WalkScratch {
     int32_t f[132];   // filtered line (same layout); also holds available values before substitution
     int32_t refs[100];  // angular projection, refs[n + k] for k in [-n, 2n]
     int32_t dc;         // DC value of the current TB
-    uint4 recs[32];   // staged TB records
 };
 
 // Shared-memory layout of one CTA.  Each component has one bordered canvas:
 // row 0 is the row above the CTU (x = -1 .. 2S-1), rows 1..S the CTU, column
 // 7 the column left of the CTU; sample (x, y) is at (y + 1) * CW + x + 8, so
 // the interior rows start 16-byte aligned.
+// Records of one CTU staged at once: up to 256 luma TBs, one "mark decoded"
+// record per inter CU (64 at most) and the chroma TBs (64 per component at
+// 4:2:0, 256 at 4:4:4).  A CTU with more records is malformed.
+constexpr int kRecCap420 = 256 + 64 + 2 * 64;
+constexpr int kRecCap444 = 256 + 64 + 2 * 256;
+constexpr int kListCap = 256;  // intra TBs of one component in one CTU
+constexpr uint32_t kNoStamp = 0xffffffffu;
+
 struct ReconLayout {
-    int cs;  // chroma canvas side
-    size_t off_can_y, off_can_c, off_res_y, off_res_c, off_ws, off_misc, total;
+    int cs;       // chroma canvas side
+    int rec_cap;  // staged records
+    size_t off_can_y, off_can_c, off_res_y, off_res_c, off_ws, off_recs, off_stamp, off_lists, off_misc, total;
     static __host__ __device__ int cw_of(int S) { return 2 * S + 8; }
     __host__ __device__ explicit ReconLayout(int c444) {
         cs = c444 ? 64 : 32;
+        rec_cap = c444 ? kRecCap444 : kRecCap420;
         size_t o = 0;
         off_can_y = o; o += (size_t)65 * cw_of(64) * sizeof(uint16_t);
         o = (o + 15) & ~(size_t)15;
@@ -340,6 +349,10 @@ struct ReconLayout {
         off_res_y = o; o += 64 * 64 * sizeof(int16_t);
         off_res_c = o; o += 2 * (size_t)cs * cs * sizeof(int16_t);
         off_ws = o;    o += kReconWarps * sizeof(WalkScratch);
+        o = (o + 15) & ~(size_t)15;
+        off_recs = o;  o += (size_t)rec_cap * sizeof(hpvcd_tu);
+        off_stamp = o; o += 256 * sizeof(uint32_t);
+        off_lists = o; o += 3 * (size_t)kListCap * sizeof(uint16_t);
         o = (o + 15) & ~(size_t)15;
         off_misc = o;  o += 16;
         total = o;
@@ -369,25 +382,24 @@ __device__ __forceinline__ int cidx(const Comp& k, int x, int y) { return (y + 1
 // Reference sample i of the line (i < 2n: left column bottom-up, 2n: the
 // corner, > 2n: above row) with its availability (decode.rs:4651-4690
 // luma_avail / chroma_avail restricted to this CTU and its already
-// reconstructed neighbours; single slice and tile per picture).  `dec` is
-// this lane's row of the CTU's `decoded` map (lane r holds cell row r).
-__device__ __forceinline__ bool gather_ref(const Comp& k, uint32_t dec, uint32_t wabove, int n2, int x0, int y0,
-                                           int i, int* v) {
+// reconstructed neighbours; single slice and tile per picture).  Inside the
+// CTU a sample is available when the luma record that marked its 4x4 cell
+// decoded comes before the current record `jrec` in decode order: `stamp`
+// holds, per cell, the index of the first luma record covering it
+// (decode.rs:3170-3189 marks cells as records complete).
+__device__ __forceinline__ bool gather_ref(const Comp& k, const uint32_t* stamp, uint32_t jrec, int n2, int x0,
+                                           int y0, int i, int* v) {
     const bool left_side = i < n2;
     const int x = left_side ? x0 - 1 : x0 + (i - n2 - 1);
     const int y = left_side ? y0 + (n2 - 1 - i) : y0 - 1;
-    // decoded word of this sample's cell row (left column: differs per lane)
-    const int row = (min(max(y, 0), k.S - 1) * k.sh) >> 2;
-    const uint32_t wl = __shfl_sync(kFull, dec, row);
     const int ax = k.ox + x, ay = k.oy + y;
     bool a = ax >= 0 && ay >= 0 && ax < k.pw && ay < k.ph;
     if (y >= 0) {
         if (x < 0)
             a = a && y < k.S;  // left CTU (below-left CTU is not reconstructed yet)
         else
-            a = a && x < k.S && y < k.S && ((wl >> ((x * k.sw) >> 2)) & 1u);
+            a = a && x < k.S && y < k.S && stamp[((y * k.sh) >> 2) * 16 + ((x * k.sw) >> 2)] < jrec;
     }
-    (void)wabove;
     *v = a ? (int)k.can[cidx(k, x, y)] : 0;
     return a;
 }
@@ -403,13 +415,12 @@ __device__ __forceinline__ int ref_pos(int k, bool vertical, int n2, int inv) {
 // 4x4 intra TB entirely in registers: the 17 reference samples live in
 // lanes 0..16 (intra.rs:84-148 substitution via shuffles; no filtering for
 // n = 4, intra.rs:174), prediction (intra.rs:257-372) by lanes 0..15.
-__device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y0, bool coded, uint32_t dec,
-                                          int lane) {
+__device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y0, bool coded,
+                                          const uint32_t* stamp, uint32_t jrec, int lane) {
     constexpr int n = 4, n2 = 8, total = 17;
     int v = 0;
-    // every lane joins the shuffle inside gather_ref; lanes past the line
-    // repeat the last position and drop it
-    bool a = gather_ref(k, dec, 0u, n2, x0, y0, min(lane, total - 1), &v);
+    // lanes past the line repeat the last position and drop it
+    bool a = gather_ref(k, stamp, jrec, n2, x0, y0, min(lane, total - 1), &v);
     a = a && lane < total;
     const uint32_t mask = __ballot_sync(kFull, a);
     int sv;
@@ -480,8 +491,8 @@ __device__ __forceinline__ bool ref_filtered(const Comp& k, int n, int mode) {
 // gather, substitution (intra.rs:84-148), filtering (:151-219) and the
 // per-mode set-up of the prediction (the angular projection into ws.refs,
 // the DC value into ws.dc).
-__device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode, int x0, int y0, uint32_t dec,
-                                              WalkScratch& ws, int lane) {
+__device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode, int x0, int y0,
+                                              const uint32_t* stamp, uint32_t jrec, WalkScratch& ws, int lane) {
     const int n = 1 << log2n;
     const int total = 4 * n + 1;
     const int n2 = 2 * n;
@@ -493,7 +504,7 @@ __device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode
         int v = 0;
         bool a = false;
         if (wd * 32 < total) {  // warp-uniform: every lane joins the shuffle inside
-            a = gather_ref(k, dec, 0u, n2, x0, y0, min(i, total - 1), &v);
+            a = gather_ref(k, stamp, jrec, n2, x0, y0, min(i, total - 1), &v);
             a = a && i < total;
         }
         val[wd] = v;
@@ -661,22 +672,10 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
 
 // Intra TB of size 8..32 by one warp.
 __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
-                                             uint32_t dec, WalkScratch& ws, int lane) {
-    intra_tb_prep(k, log2n, mode, x0, y0, dec, ws, lane);
+                                             const uint32_t* stamp, uint32_t jrec, WalkScratch& ws, int lane) {
+    intra_tb_prep(k, log2n, mode, x0, y0, stamp, jrec, ws, lane);
     intra_tb_predict(k, log2n, mode, x0, y0, coded, ws, lane, 32);
     __syncwarp();
-}
-
-// Mark a luma square decoded (decode.rs:3170-3189; cells outside the
-// picture stay unmarked).  Lane r holds cell row r; no synchronisation.
-__device__ __forceinline__ uint32_t mark_rows(uint32_t dec, int x0, int y0, int n, int lane, int vis_w, int vis_h) {
-    const int r0 = y0 >> 2, r1 = (min(y0 + n, vis_h) + 3) >> 2;
-    const int x1 = min(x0 + n, vis_w);
-    if (lane >= r0 && lane < r1 && x1 > x0) {
-        const int c0 = x0 >> 2, c1 = (x1 + 3) >> 2;
-        dec |= (c1 - c0 >= 32 ? kFull : ((1u << (c1 - c0)) - 1u)) << c0;
-    }
-    return dec;
 }
 
 // Luma intra TBs of at least 2^kTeamMinLog2 samples square are predicted by
@@ -719,6 +718,15 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             r1 = min(r1, P.n_tus);
             r0 = min(r0, r1);
         }
+        uint32_t nrec = r1 - r0;
+        if (nrec > (uint32_t)lay.rec_cap) {  // more records than a CTU can hold
+            if (tid == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+            nrec = (uint32_t)lay.rec_cap;
+        }
+        uint4* recs = (uint4*)(smem + lay.off_recs);
+        uint32_t* stamp = (uint32_t*)(smem + lay.off_stamp);
+        uint16_t* lists = (uint16_t*)(smem + lay.off_lists);
+        uint32_t* counts = (uint32_t*)(smem + lay.off_misc) + 1;
         auto can_of = [&](int c) -> uint16_t* {
             return c == 0 ? (uint16_t*)(smem + lay.off_can_y)
                           : (uint16_t*)(smem + lay.off_can_c) +
@@ -743,7 +751,10 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 cp_async16(dst + y * S + 8 * q, src + (size_t)y * P.res_stride[c] + 8 * q);
             }
         }
+        // the CTU's records (16 bytes each; the record array is 16-byte aligned)
+        for (uint32_t i = tid; i < nrec; i += kReconThreads) cp_async16(recs + i, P.tus + r0 + i);
         asm volatile("cp.async.commit_group;" ::: "memory");
+        for (int i = tid; i < 256; i += kReconThreads) stamp[i] = kNoStamp;
         // Inter pictures: the plane holds motion-compensated + residual
         // samples; load the CTU interior so intra TBs can predict from it.
         if (P.flags & HPVCD_PIC_INTER) {
@@ -803,6 +814,64 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         }
         cp_async_wait_all();
         __syncthreads();
+        // ---- decode order, in parallel: every luma record stamps the 4x4
+        // cells it marks decoded (decode.rs:3170-3189; cells outside the
+        // picture stay unmarked), and warp c lists the intra TBs of
+        // component c in decode order ----
+        const int vis_w = min(64, P.w - oxl), vis_h = min(64, P.h - oyl);
+        const bool intra_pred_ok = !(P.flags & HPVCD_PIC_PRED_IN_PLANE);
+        // validity of record i for component tc: -1 skip silently, 0 invalid
+        // (reported), 1 usable; (x, y) relative to the CTU
+        auto rec_check = [&](const hpvcd_tu& t, int& x, int& y) -> int {
+            const int tc = t.comp;
+            if (tc >= ncomp || t.log2n < 2 || t.log2n > 6) return -1;
+            const int n = 1 << t.log2n;
+            x = (int)t.x - (tc ? ocx : oxl);
+            y = (int)t.y - (tc ? ocy : oyl);
+            const int St = tc ? Sc : ctb;
+            return (x < 0 || y < 0 || x + n > St || y + n > St) ? 0 : 1;
+        };
+        for (uint32_t i = tid; i < nrec; i += kReconThreads) {
+            hpvcd_tu t;
+            memcpy(&t, &recs[i], sizeof(t));
+            int x, y;
+            const int ok = rec_check(t, x, y);
+            if (ok == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+            if (ok != 1 || t.comp != 0) continue;
+            const int n = 1 << t.log2n;
+            const int x1 = min(x + n, vis_w), y1 = min(y + n, vis_h);
+            for (int cy = y >> 2; cy < (y1 + 3) >> 2; ++cy)
+                for (int cx = x >> 2; cx < (x1 + 3) >> 2; ++cx) atomicMin(&stamp[cy * 16 + cx], i);
+        }
+        if (warp < ncomp) {
+            const int c = warp;
+            uint32_t cnt = 0;
+            for (uint32_t base = 0; base < nrec; base += 32) {
+                const uint32_t i = base + lane;
+                bool mine = false;
+                if (i < nrec) {
+                    hpvcd_tu t;
+                    memcpy(&t, &recs[i], sizeof(t));
+                    int x, y;
+                    if (t.comp == c && (t.flags & HPVCD_TU_INTRA) && intra_pred_ok && rec_check(t, x, y) == 1) {
+                        if (t.mode > 34 || t.log2n > 5)
+                            atomicOr(dev_err, DEV_ERR_BITSTREAM);
+                        else
+                            mine = true;
+                    }
+                }
+                const uint32_t m = __ballot_sync(kFull, mine);
+                const uint32_t pos = cnt + __popc(m & ((1u << lane) - 1u));
+                if (mine && pos < (uint32_t)kListCap) lists[c * kListCap + pos] = (uint16_t)i;
+                cnt += __popc(m);
+            }
+            if (cnt > (uint32_t)kListCap) {
+                if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+                cnt = kListCap;
+            }
+            if (lane == 0) counts[c] = cnt;
+        }
+        __syncthreads();
         // ---- decode-order walk: warp c reconstructs component c ----
         const bool helper = kTeam > 1 && warp == kReconWarps - 1;
         if (warp < ncomp || helper) {
@@ -826,47 +895,26 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             k.strong = (P.flags & HPVCD_PIC_STRONG_SMOOTHING) != 0;
             k.can = can_of(c);
             k.res = res_of(c);
-            const int vis_w = min(64, P.w - oxl), vis_h = min(64, P.h - oyl);
-            const bool intra_pred_ok = !(P.flags & HPVCD_PIC_PRED_IN_PLANE);
-            uint32_t dec = 0;  // lane r: cell row r of the CTU's `decoded` map
-            for (uint32_t base = r0; base < r1; base += 32) {
-                if (base + lane < r1) ws.recs[lane] = *(const uint4*)(P.tus + base + lane);
-                __syncwarp();
-                const int cnt = (int)min(32u, r1 - base);
-                for (int j = 0; j < cnt; ++j) {
-                    const uint4 w = ws.recs[j];
-                    hpvcd_tu t;
-                    memcpy(&t, &w, sizeof(t));
-                    const int tc = t.comp;
-                    if (tc >= ncomp || t.log2n < 2 || t.log2n > 6) continue;
-                    const int n = 1 << t.log2n;
-                    const int x = (int)t.x - (tc ? ocx : oxl), y = (int)t.y - (tc ? ocy : oyl);
-                    const int St = tc ? Sc : ctb;
-                    if (x < 0 || y < 0 || x + n > St || y + n > St) {
-                        if (lane == 0 && c == 0 && !helper) atomicOr(dev_err, DEV_ERR_BITSTREAM);
-                        continue;
-                    }
-                    if (tc == c && (t.flags & HPVCD_TU_INTRA) && intra_pred_ok) {
-                        const bool coded = (t.flags & HPVCD_TU_CBF) != 0;
-                        if (t.mode > 34 || t.log2n > 5) {
-                            if (lane == 0 && !helper) atomicOr(dev_err, DEV_ERR_BITSTREAM);
-                        } else if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
-                            if (!helper) intra_tb_prep(k, t.log2n, t.mode, x, y, dec, team_ws, lane);
-                            team_sync(32 * kTeam);
-                            intra_tb_predict(k, t.log2n, t.mode, x, y, coded, team_ws, (helper ? 32 : 0) + lane,
-                                             32 * kTeam);
-                            team_sync(32 * kTeam);
-                        } else if (helper) {
-                            // smaller TBs are the leader's alone
-                        } else if (t.log2n == 2) {
-                            intra_tb4(k, t.mode, x, y, coded, dec, lane);
-                        } else {
-                            intra_tb_big(k, t.log2n, t.mode, x, y, coded, dec, ws, lane);
-                        }
-                    }
-                    if (tc == 0 && !helper) dec = mark_rows(dec, x, y, n, lane, vis_w, vis_h);
+            const uint32_t cnt = counts[c];
+            const uint16_t* list = lists + c * kListCap;
+            for (uint32_t e = 0; e < cnt; ++e) {
+                const uint32_t j = list[e];
+                hpvcd_tu t;
+                memcpy(&t, &recs[j], sizeof(t));
+                const int x = (int)t.x - (c ? ocx : oxl), y = (int)t.y - (c ? ocy : oyl);
+                const bool coded = (t.flags & HPVCD_TU_CBF) != 0;
+                if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
+                    if (!helper) intra_tb_prep(k, t.log2n, t.mode, x, y, stamp, j, team_ws, lane);
+                    team_sync(32 * kTeam);
+                    intra_tb_predict(k, t.log2n, t.mode, x, y, coded, team_ws, (helper ? 32 : 0) + lane, 32 * kTeam);
+                    team_sync(32 * kTeam);
+                } else if (helper) {
+                    // smaller TBs are the leader's alone
+                } else if (t.log2n == 2) {
+                    intra_tb4(k, t.mode, x, y, coded, stamp, j, lane);
+                } else {
+                    intra_tb_big(k, t.log2n, t.mode, x, y, coded, stamp, j, ws, lane);
                 }
-                __syncwarp();
             }
         }
         __syncthreads();
