@@ -393,14 +393,19 @@ __device__ __forceinline__ bool gather_ref(const Comp& k, const uint32_t* stamp,
     const int x = left_side ? x0 - 1 : x0 + (i - n2 - 1);
     const int y = left_side ? y0 + (n2 - 1 - i) : y0 - 1;
     const int ax = k.ox + x, ay = k.oy + y;
+    // both loads from clamped (always valid) positions, issued together;
+    // the availability test picks the result
+    const int ys = min(max(y, 0), k.S - 1), xs = min(max(x, 0), k.S - 1);
+    const uint32_t st = stamp[((ys * k.sh) >> 2) * 16 + ((xs * k.sw) >> 2)];
+    const int cv = k.can[cidx(k, x, min(y, k.S - 1))];
     bool a = ax >= 0 && ay >= 0 && ax < k.pw && ay < k.ph;
     if (y >= 0) {
         if (x < 0)
             a = a && y < k.S;  // left CTU (below-left CTU is not reconstructed yet)
         else
-            a = a && x < k.S && y < k.S && stamp[((y * k.sh) >> 2) * 16 + ((x * k.sw) >> 2)] < jrec;
+            a = a && x < k.S && y < k.S && st < jrec;
     }
-    *v = a ? (int)k.can[cidx(k, x, y)] : 0;
+    *v = a ? cv : 0;
     return a;
 }
 
@@ -485,6 +490,114 @@ __device__ __forceinline__ bool ref_filtered(const Comp& k, int n, int mode) {
     const int md = min(abs(mode - 26), abs(mode - 10));
     const int thresh = n == 8 ? 7 : (n == 16 ? 1 : 0);
     return mode == 0 || md > thresh;
+}
+
+// 8x8 intra TB in registers: the 33-sample reference line is s[lane] in
+// `lo` and s[32] in `hi` (the same in every lane); substitution
+// (intra.rs:84-148) by ballots, [1 2 1] filtering (intra.rs:151-219; no
+// strong filter below 32x32) and prediction (intra.rs:257-372) by shuffles,
+// two samples per lane.  Same arithmetic as the shared-memory path.
+__device__ __forceinline__ void intra_tb8(const Comp& k, int mode, int x0, int y0, bool coded,
+                                          const uint32_t* stamp, uint32_t jrec, int lane) {
+    constexpr int n = 8, n2 = 16, log2n = 3;
+    int v_lo = 0, v_hi = 0;
+    const bool a_lo = gather_ref(k, stamp, jrec, n2, x0, y0, lane, &v_lo);
+    const bool a_hi = gather_ref(k, stamp, jrec, n2, x0, y0, 2 * n2, &v_hi);  // uniform
+    const uint32_t mask = __ballot_sync(kFull, a_lo);
+    // ---- substitution: an unavailable sample takes the nearest available
+    // one below it in the line, or the first available one ----
+    const int first = mask ? __ffs(mask) - 1 : 0;
+    const int first_lo = __shfl_sync(kFull, v_lo, first);
+    const uint32_t m0 = mask & ((2u << lane) - 1u);
+    const int below = __shfl_sync(kFull, v_lo, m0 ? 31 - __clz(m0) : 0);
+    const int top = __shfl_sync(kFull, v_lo, mask ? 31 - __clz(mask) : 0);
+    int s_lo, s_hi;
+    if (!mask && !a_hi) {
+        s_lo = s_hi = 1 << (k.bd - 1);
+    } else {
+        const int first_val = mask ? first_lo : v_hi;
+        s_lo = a_lo ? v_lo : (m0 ? below : first_val);
+        s_hi = a_hi ? v_hi : (mask ? top : first_val);
+    }
+    // ---- filtering ----
+    int r_lo = s_lo;
+    const int r_hi = s_hi;
+    if (ref_filtered(k, n, mode)) {
+        const int up = __shfl_up_sync(kFull, s_lo, 1);
+        const int dn = __shfl_down_sync(kFull, s_lo, 1);
+        const int nxt = lane == 31 ? s_hi : dn;
+        r_lo = lane == 0 ? s_lo : (up + 2 * s_lo + nxt + 2) >> 2;
+    }
+    // R(idx), idx in [0, 32]; every lane must call it
+    auto R = [&](int idx) {
+        const int t = __shfl_sync(kFull, r_lo, idx & 31);
+        return idx >= 32 ? r_hi : t;
+    };
+    const int max_v = k.max_v;
+    const bool edge = k.luma;  // edge filters of luma TBs below 32x32
+    int out[2];
+    if (mode >= 2) {
+        const int angle = c_intra_angle[mode - 2];
+        const bool vertical = mode >= 18;
+        const int inv = angle < 0 ? c_inv_angle[mode - 11] : 0;
+        const int c0 = R(n2);
+        const int a0 = R(vertical ? n2 + 1 : n2 - 1);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = lane + 32 * h;
+            const int yy = i >> log2n, xx = i & (n - 1);
+            const int a = vertical ? yy : xx, b = vertical ? xx : yy;
+            const int pos = (a + 1) * angle;
+            const int iidx = pos >> 5, frac = pos & 31;
+            const int r0 = R(ref_pos(b + iidx + 1, vertical, n2, inv));
+            const int r1 = R(ref_pos(min(b + iidx + 2, 2 * n), vertical, n2, inv));
+            int v = clamp3i(frac ? ((32 - frac) * r0 + frac * r1 + 16) >> 5 : r0, 0, max_v);
+            const int e = R(mode == 26 ? n2 - (yy + 1) : n2 + xx + 1);
+            if (edge && ((mode == 26 && xx == 0) || (mode == 10 && yy == 0))) v = clamp3i(a0 + ((e - c0) >> 1), 0, max_v);
+            out[h] = v;
+        }
+    } else if (mode == 1) {  // DC
+        int part = ((lane >= n2 - n && lane < n2) || (lane > n2 && lane <= n2 + n)) ? r_lo : 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+        const int dc = (part + n) >> (log2n + 1);
+        const int l1 = R(n2 - 1), a1 = R(n2 + 1);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = lane + 32 * h;
+            const int yy = i >> log2n, xx = i & (n - 1);
+            const int e = R(yy == 0 ? n2 + xx + 1 : n2 - yy - 1);
+            int v = dc;
+            if (edge) {
+                if (xx == 0 && yy == 0)
+                    v = (l1 + 2 * dc + a1 + 2) >> 2;
+                else if (yy == 0 || xx == 0)
+                    v = (e + 3 * dc + 2) >> 2;
+            }
+            out[h] = v;
+        }
+    } else {  // planar
+        const int tr = R(n2 + n + 1), bl = R(n2 - n - 1);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = lane + 32 * h;
+            const int yy = i >> log2n, xx = i & (n - 1);
+            const int lft = R(n2 - yy - 1), abv = R(n2 + xx + 1);
+            out[h] = ((n - 1 - xx) * lft + (xx + 1) * tr + (n - 1 - yy) * abv + (yy + 1) * bl + n) >> (log2n + 1);
+        }
+    }
+    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int i = lane + 32 * h;
+        const int yy = i >> log2n, xx = i & (n - 1);
+        if (xx < vw && yy < vh) {
+            int v = out[h];
+            if (coded) v = clamp3i(v + k.res[(y0 + yy) * k.S + x0 + xx], 0, max_v);
+            k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
+        }
+    }
+    __syncwarp();
 }
 
 // Intra TB of size 8..32, first part, by one warp through shared memory:
@@ -912,6 +1025,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     // smaller TBs are the leader's alone
                 } else if (t.log2n == 2) {
                     intra_tb4(k, t.mode, x, y, coded, stamp, j, lane);
+                } else if (t.log2n == 3) {
+                    intra_tb8(k, t.mode, x, y, coded, stamp, j, lane);
                 } else {
                     intra_tb_big(k, t.log2n, t.mode, x, y, coded, stamp, j, ws, lane);
                 }
