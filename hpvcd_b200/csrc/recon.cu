@@ -804,7 +804,7 @@ __device__ __forceinline__ void team_sync(int threads) {
 }
 
 template <int kTeam>
-__global__ void __launch_bounds__(kReconThreads)
+__global__ void __launch_bounds__(kReconThreads, 4)
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
         uint32_t* work_counter, uint32_t* dev_err, int c444, uint32_t spin_limit) {
     static_assert(kTeam == 1 || kTeam == 2, "team of one or two warps");
@@ -1010,10 +1010,17 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             k.res = res_of(c);
             const uint32_t cnt = counts[c];
             const uint16_t* list = lists + c * kListCap;
+            // the next record is fetched while the current TB is reconstructed
+            uint32_t jn = cnt ? list[0] : 0u;
+            uint4 wn = cnt ? recs[jn] : make_uint4(0u, 0u, 0u, 0u);
             for (uint32_t e = 0; e < cnt; ++e) {
-                const uint32_t j = list[e];
+                const uint32_t j = jn;
                 hpvcd_tu t;
-                memcpy(&t, &recs[j], sizeof(t));
+                memcpy(&t, &wn, sizeof(t));
+                if (e + 1 < cnt) {
+                    jn = list[e + 1];
+                    wn = recs[jn];
+                }
                 const int x = (int)t.x - (c ? ocx : oxl), y = (int)t.y - (c ? ocy : oyl);
                 const bool coded = (t.flags & HPVCD_TU_CBF) != 0;
                 if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
