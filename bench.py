@@ -56,10 +56,8 @@ def parse_args():
 
 
 def dist_info():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
+    from hpvcd_b200 import replicas
+    return replicas.dist_info()
 
 
 def measured_peaks():
@@ -183,6 +181,7 @@ def run_reference(args):
 
 
 def run_e2e(pics, g, K2, warmup, local, world, dev):
+    from hpvcd_b200 import replicas
     """Same decode through hpvcd_gpu_submit / wait / read: inputs packed in
     page-locked host memory (one H2D DMA per step), RGB8 canvas DMA'd back
     to a page-locked caller buffer every step; wall clock per step."""
@@ -213,10 +212,7 @@ def run_e2e(pics, g, K2, warmup, local, world, dev):
             decd.read(t, dst)
             times.append(time.perf_counter() - t0)
         e2e_total = sum(times)
-        if world > 1:
-            tt = torch.tensor([e2e_total], device=dev)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            e2e_total = float(tt.item())
+        e2e_total = replicas.max_over_ranks(e2e_total, dev)
     lat = sorted(t * 1e3 for t in times)
     return {"value": round(world * MPIX * K2 / e2e_total, 2), "unit": "MPix/s",
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": canvas_bytes,
@@ -230,6 +226,7 @@ def run_ours(args):
     import numpy as np
     import torch
 
+    from hpvcd_b200 import replicas
     from hpvcd_b200 import abi, synth
     from hpvcd_b200.gpu import DevicePlan
 
@@ -283,12 +280,8 @@ def run_ours(args):
 
     step_ms = [ev[k][0].elapsed_time(ev[k][-1]) for k in range(K)]
     stage_ms = [sum(ev[k][i].elapsed_time(ev[k][i + 1]) for k in range(K)) / K for i in range(len(stages))]
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * MPIX * K / (total_ms / 1e3)
+    total_ms = replicas.max_over_ranks(sum(step_ms), dev)
+    value = replicas.whole_job_rate(MPIX * K, total_ms / 1e3, dev)
     lat = sorted(step_ms)
 
     # Roofline of the dominant kernel (the reconstruction kernel): algorithmic
