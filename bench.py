@@ -48,8 +48,10 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["grid", "serving"], default="grid",
-                    help="grid: the 4032x3024 still (default); serving: mixed-size batched serving")
+    ap.add_argument("--workload", choices=["grid", "serving", "selector"], default="grid",
+                    help="grid: the 4032x3024 still (default); serving: mixed-size batched serving; "
+                         "selector: learned schedule selection on 3840x2160 frames")
+    ap.add_argument("--frames", type=int, default=60, help="selector: fresh frames to evaluate")
     ap.add_argument("--images", type=int, default=64, help="serving: number of images")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: Poisson arrivals per second")
     return ap.parse_args()
@@ -302,6 +304,15 @@ def run_ours(args):
                 "traffic": traffic.get("dram_bytes_per_launch") if traffic else None}
     # whole-pipeline bytes (reconstruction + filters + RGB), for context
     pipe_bytes = recon_bytes + 2 * written * 2 + written + OUT_W * OUT_H * 3
+    # per-stage algorithmic bytes: deblocking and SAO read + write the planes
+    # once, RGB reads the planes and writes 3 bytes per output pixel
+    stage_bytes = {"recon": recon_bytes, "deblock": 2 * written, "sao": 2 * written,
+                   "rgb": written + OUT_W * OUT_H * 3}
+    stage_roofline = {}
+    for i, name in enumerate(("recon", "deblock", "sao", "rgb")):
+        gbs = stage_bytes[name] / (stage_ms[i] / 1e3) / 1e9 if stage_ms[i] > 0 else 0.0
+        stage_roofline[name] = {"bytes": int(stage_bytes[name]), "ms": round(stage_ms[i], 4),
+                                "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
 
     # ---- end to end through the C ABI (host buffers) ----
     e2e = None
@@ -328,6 +339,7 @@ def run_ours(args):
         "stages_ms": {"recon": round(stage_ms[0], 4), "deblock": round(stage_ms[1], 4),
                       "sao": round(stage_ms[2], 4), "rgb": round(stage_ms[3], 4)},
         "pipeline_gbs": round(pipe_bytes / (total_ms / K / 1e3) / 1e9, 1),
+        "stage_roofline": stage_roofline,
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,
@@ -393,10 +405,66 @@ def device_batched_vs_plain(imgs, local, reps: int = 5):
            "plain_mpix_per_s": round(mpix / (t_plain / 1e3), 1),
            "speedup": round(t_plain / t_fused, 3), "status": st,
            "fused_launches_per_run": fused.launches_per_run}
+    # the fused batch with the learned schedule (features + network pick on
+    # the device), and exhaustive autotuning as the judge
+    mlp = _selector_network()
+    if mlp is not None:
+        from hpvcd_b200 import selector
+        chosen = C.c_uint32()
+        cs = C.c_void_p(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            abi.check(abi.lib().hpvcd_plan_select(fused._h, mlp.handle, selector.schedules_array(), selector.K, cs,
+                                                  C.byref(chosen)), "hpvcd_plan_select")
+        t_learned = timed(lambda: fused.launch(abi.STAGE_ALL | abi.STAGE_GRAPH, stream))
+        ms = (C.c_float * selector.K)()
+        best = C.c_uint32()
+        with torch.cuda.stream(stream):
+            abi.check(abi.lib().hpvcd_plan_autotune(fused._h, selector.schedules_array(), selector.K, abi.STAGE_ALL,
+                                                    3, 1, cs, ms, C.byref(best)), "hpvcd_plan_autotune")
+        res.update({"learned_ms": round(t_learned, 3), "learned_pick": int(chosen.value),
+                    "learned_mpix_per_s": round(mpix / (t_learned / 1e3), 1),
+                    "learned_speedup_vs_plain": round(t_plain / t_learned, 3),
+                    "autotuned_pick": int(best.value), "autotune_ms": [round(v, 3) for v in ms]})
     fused.close()
     for p in singles:
         p.close()
     return res
+
+
+def _selector_network():
+    """The committed selector network, or None when no weights are present."""
+    from hpvcd_b200 import selector
+    if not os.path.exists(selector.WEIGHTS_PATH):
+        return None
+    return selector.Mlp.load()
+
+
+def run_selector(args):
+    """Learned schedule selection on fresh 3840x2160 10-bit frames (a seed the
+    network never saw): decode time with the network's pick against the
+    fixed default schedule and exhaustive autotuning (every schedule timed on
+    the frame itself)."""
+    import torch
+
+    from hpvcd_b200 import selector
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    mlp = _selector_network()
+    metric = "ms per 3840x2160 frame (learned schedule)"
+    if mlp is None:
+        print(json.dumps({"metric": metric, "unavailable": "no selector weights"}))
+        return 0
+    r = selector.evaluate_live(mlp, args.frames, seed=12345 + rank)
+    line = {"metric": metric, "value": round(r["ms_selected"], 4), "unit": "ms", "higher_is_better": False,
+            "n_gpus": world, "data": "synthetic", "dtype": "int32",
+            "config": {"workload": "selector_4k_frames", "frames": args.frames, "size": "3840x2160",
+                       "bit_depth": 10, "chroma": "4:2:0", "qp": "17..42", "tb_mix": "Dirichlet(1,1,1,1)",
+                       "coded_fraction": "5..60%", "intra_frames": "30%", "schedules": selector.K},
+            "selector": r}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
 
 
 def _single_output(im):
@@ -423,6 +491,9 @@ def run_serving(args):
     zc = dict(zero_copy=True)
     plain_sat = serving.run(imgs, batching=False, arrival_rate=None, device=local, **zc)
     batched_sat = serving.run(imgs, batching=True, arrival_rate=None, device=local, **zc)
+    mlp = _selector_network()
+    learned_sat = (serving.run(imgs, batching=True, arrival_rate=None, device=local, selector=mlp, **zc)
+                   if mlp is not None else None)
     batched_poi = serving.run(imgs, batching=True, arrival_rate=args.rate, device=local, **zc)
     plain_poi = serving.run(imgs, batching=False, arrival_rate=args.rate, device=local, **zc)
     copied_sat = serving.run(imgs, batching=True, arrival_rate=None, device=local)
@@ -435,8 +506,11 @@ def run_serving(args):
                    "arrivals": f"Poisson {args.rate}/s",
                    "host_buffers": "inputs packed in page-locked memory, page-locked outputs (zero copy)"},
         "batched_vs_plain_throughput": round(batched_sat["mpix_per_s"] / plain_sat["mpix_per_s"], 3),
+        "batched_learned_vs_plain_throughput": (round(learned_sat["mpix_per_s"] / plain_sat["mpix_per_s"], 3)
+                                                if learned_sat else None),
         "device": dev,
-        "saturation": {"plain": plain_sat, "batched": batched_sat, "batched_host_copies": copied_sat},
+        "saturation": {"plain": plain_sat, "batched": batched_sat, "batched_learned": learned_sat,
+                       "batched_host_copies": copied_sat},
         "poisson": {"plain": plain_poi, "batched": batched_poi},
     }
     if rank == 0:
@@ -450,6 +524,8 @@ def main():
         return run_reference(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "selector":
+        return run_selector(args)
     return run_ours(args)
 
 

@@ -280,6 +280,10 @@ def lib() -> C.CDLL:
             "hpvcd_mlp_adam_step": (i32, [vp, C.c_float, vp]),
             "hpvcd_mlp_train": (i32, [vp, vp, vp, u32, u32, u32, C.c_float, u64, vp, C.POINTER(C.c_float)]),
             "hpvcd_mlp_pick": (i32, [vp, vp, u32, vp, C.POINTER(u32)]),
+            "hpvcd_gpu_set_selector": (i32, [vp, vp, C.POINTER(Sched), u32]),
+            "hpvcd_gpu_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
+            "hpvcd_server_set_selector": (i32, [vp, vp, C.POINTER(Sched), u32]),
+            "hpvcd_server_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

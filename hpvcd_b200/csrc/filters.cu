@@ -8,7 +8,8 @@
 // reference's filter-then-restore (decode.rs:1831-1880).
 //
 // SAO (sao.rs + decode.rs:2258-2493): out-of-place, every sample reads the
-// deblocked picture (the reference's snapshot) and writes the final plane.
+// deblocked picture (the reference's snapshot) and writes the final plane;
+// four samples per thread with vector loads and stores.
 //
 // RGB (yuv.rs:187-393 Q13 matrix, lib.rs:1964-1978 rgb8 narrowing,
 // lib.rs:1610-1660 tile placement and cropping on the canvas).
@@ -204,33 +205,60 @@ __global__ void k_deblock(const DevPic* __restrict__ pics, int vertical) {
     }
 }
 
-// SAO: one thread per sample.  blockIdx.y = picture, blockIdx.z = component.
+// Four horizontally adjacent samples of a plane (x multiple of 4; plane
+// widths are multiples of 4 samples, so the access is aligned and in bounds).
+__device__ __forceinline__ void load4(const void* plane, int bps, size_t idx, int v[4]) {
+    if (bps == 1) {
+        const uint32_t w = *(const uint32_t*)((const uint8_t*)plane + idx);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] = (w >> (8 * i)) & 0xff;
+    } else {
+        const uint2 w = *(const uint2*)((const uint16_t*)plane + idx);
+        v[0] = w.x & 0xffff; v[1] = w.x >> 16; v[2] = w.y & 0xffff; v[3] = w.y >> 16;
+    }
+}
+__device__ __forceinline__ void store4(void* plane, int bps, size_t idx, const int v[4]) {
+    if (bps == 1)
+        *(uint32_t*)((uint8_t*)plane + idx) =
+            (uint32_t)v[0] | ((uint32_t)v[1] << 8) | ((uint32_t)v[2] << 16) | ((uint32_t)v[3] << 24);
+    else
+        *(uint2*)((uint16_t*)plane + idx) =
+            make_uint2((uint32_t)v[0] | ((uint32_t)v[1] << 16), (uint32_t)v[2] | ((uint32_t)v[3] << 16));
+}
+
+// SAO: one thread per 4 horizontally adjacent samples (they share one CTB:
+// CTB widths are multiples of 8 samples).  blockIdx.y = picture,
+// blockIdx.z = component.  Rows y-1, y, y+1 are read over x-1 .. x+4 once.
 __global__ void k_sao(const DevPic* __restrict__ pics) {
     const DevPic& P = pics[blockIdx.y];
     const int c = blockIdx.z;
     if (P.rec[0] == P.fin[0]) return;  // no SAO for this picture
     if (c > 0 && P.idc == 0) return;
     const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+    const int qw = pw >> 2;
     const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= pw * ph) return;
-    const int x = id % pw, y = id / pw;
+    if (id >= qw * ph) return;
+    const int x0 = (id % qw) * 4, y = id / qw;
     const void* src = P.rec[c];
     void* dst = P.fin[c];
     const int bps = P.bps;
-    const int s = load_sample(src, bps, (size_t)y * pw + x);
-    int out = s;
+    const size_t row = (size_t)y * pw;
+    int s[4];
+    load4(src, bps, row + x0, s);
+    int out[4] = {s[0], s[1], s[2], s[3]};
     const bool on = c == 0 ? (P.flags & HPVCD_PIC_SAO_LUMA) != 0 : (P.flags & HPVCD_PIC_SAO_CHROMA) != 0;
     const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
-    const int lx = x * sw, ly = y * sh;
-    const bool exempt = P.cells && exempt_at(P, lx, ly);
-    if (on && P.sao && !exempt) {
-        const int rx = lx >> P.log2_ctb, ry = ly >> P.log2_ctb;
+    if (on && P.sao) {
+        const int rx = (x0 * sw) >> P.log2_ctb, ry = (y * sh) >> P.log2_ctb;
         const hpvcd_sao_comp sc = P.sao[(size_t)ry * P.ctb_cols + rx].comp[c];
         const int bd = c ? P.bd_c : P.bd;
         const int mx = (1 << bd) - 1;
         if (sc.type_idx == 1) {  // sao.rs:205-233
-            const uint8_t rel = (uint8_t)((uint8_t)(s >> (bd - 5)) - sc.band_pos);
-            if (rel < 4) out = clamp3i(s + sc.offsets[rel], 0, mx);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const uint8_t rel = (uint8_t)((uint8_t)(s[i] >> (bd - 5)) - sc.band_pos);
+                if (rel < 4) out[i] = clamp3i(s[i] + sc.offsets[rel], 0, mx);
+            }
         } else if (sc.type_idx == 2) {  // sao.rs:266-330
             int dx, dy;
             switch (sc.eo_class) {
@@ -239,90 +267,169 @@ __global__ void k_sao(const DevPic* __restrict__ pics) {
                 case 2: dx = 1; dy = 1; break;
                 default: dx = 1; dy = -1; break;
             }
-            const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
-            if (x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph) {
-                const int n1 = load_sample(src, bps, (size_t)y1 * pw + x1);
-                const int n2 = load_sample(src, bps, (size_t)y2 * pw + x2);
-                const int e = ((s > n1) - (s < n1)) + ((s > n2) - (s < n2)) + 2;
-                int o = 0;
-                if (e == 0) o = sc.offsets[0];
-                else if (e == 1) o = sc.offsets[1];
-                else if (e == 3) o = sc.offsets[2];
-                else if (e == 4) o = sc.offsets[3];
-                if (o) out = clamp3i(s + o, 0, mx);
+            // window w[r][i] = sample (x0 - 1 + i, y - 1 + r), i = 0..5
+            int w[3][6];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int yy = y - 1 + r;
+                const bool in_row = yy >= 0 && yy < ph;
+                if (r == 1) {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) w[1][i + 1] = s[i];
+                } else if (in_row) {
+                    int t[4];
+                    load4(src, bps, (size_t)yy * pw + x0, t);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) w[r][i + 1] = t[i];
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) w[r][i + 1] = 0;
+                }
+                w[r][0] = in_row && x0 > 0 ? load_sample(src, bps, (size_t)yy * pw + x0 - 1) : 0;
+                w[r][5] = in_row && x0 + 4 < pw ? load_sample(src, bps, (size_t)yy * pw + x0 + 4) : 0;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int x = x0 + i;
+                const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
+                if (x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph) {
+                    // (x + dx, y + dy) and (x - dx, y - dy) with constant window indexes
+                    int n1, n2;
+                    switch (sc.eo_class) {
+                        case 0: n1 = w[1][i + 2]; n2 = w[1][i]; break;
+                        case 1: n1 = w[2][i + 1]; n2 = w[0][i + 1]; break;
+                        case 2: n1 = w[2][i + 2]; n2 = w[0][i]; break;
+                        default: n1 = w[0][i + 2]; n2 = w[2][i]; break;
+                    }
+                    const int e = ((s[i] > n1) - (s[i] < n1)) + ((s[i] > n2) - (s[i] < n2)) + 2;
+                    int o = 0;
+                    if (e == 0) o = sc.offsets[0];
+                    else if (e == 1) o = sc.offsets[1];
+                    else if (e == 3) o = sc.offsets[2];
+                    else if (e == 4) o = sc.offsets[3];
+                    if (o) out[i] = clamp3i(s[i] + o, 0, mx);
+                }
             }
         }
+        if (P.cells) {  // exempt cells keep the deblocked samples
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (exempt_at(P, (x0 + i) * sw, y * sh)) out[i] = s[i];
+        }
     }
-    store_sample(dst, bps, (size_t)y * pw + x, out);
+    store4(dst, bps, row + x0, out);
 }
 
-// Q13 YCbCr -> RGB8 onto the canvas.  blockIdx.y = picture.
-struct RgbParams {
-    int matrix, full_range, canvas_w, canvas_h;
+// Q13 YCbCr -> RGB8 onto the canvas, four pixels per thread.  blockIdx.y =
+// picture.  Every product and sum stays below 2^31 for bit depths up to 12
+// (|k_y (Y - black)| < 2^26, |coefficient x (C - neutral)| < 2^26), so the
+// 32-bit arithmetic equals the reference's 64-bit one.
+struct RgbCoef {
+    int k_y, k_uv, cr_to_r, cb_to_g, cr_to_g, cb_to_b, y_black, c_black, neutral, cmax, sh, matrix, full;
 };
 
-__global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out) {
-    const DevPic& P = pics[blockIdx.y];
-    const RgbParams rp{P.matrix, P.full_range, P.canvas_w, P.canvas_h};
-    uint8_t* canvas = out + P.canvas_off;
-    const int tw = P.crop_w, th = P.crop_h;
-    const int copy_w = min(tw, max(rp.canvas_w - P.dst_x, 0));
-    const int copy_h = min(th, max(rp.canvas_h - P.dst_y, 0));
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= copy_w * copy_h) return;
-    const int xx = id % copy_w, yy = id / copy_w;
+__device__ __forceinline__ RgbCoef rgb_coef(const DevPic& P) {
+    RgbCoef k;
+    const int Q13 = 13, ONE = 1 << 13, ROUND = 1 << 12;
     const int bd = P.bd;
-    const long long Q13 = 13, ONE = 1 << 13, ROUND = 1 << 12;
-    const long long scale = 1ll << (bd - 8);
-    const bool full = rp.full_range != 0;
-    const long long k_y = full ? ONE : 9539, k_uv = full ? ONE : 9326;
-    long long cr_r0, cb_g0, cr_g0, cb_b0;
-    switch (rp.matrix) {
+    const int scale = 1 << (bd - 8);
+    k.full = P.full_range != 0;
+    k.matrix = P.matrix;
+    k.k_y = k.full ? ONE : 9539;
+    k.k_uv = k.full ? ONE : 9326;
+    int cr_r0, cb_g0, cr_g0, cb_b0;
+    switch (P.matrix) {
         case HPVCD_MATRIX_BT470BG:
         case HPVCD_MATRIX_SMPTE170M: cr_r0 = 11485; cb_g0 = -2819; cr_g0 = -5851; cb_b0 = 14516; break;
         case HPVCD_MATRIX_BT2020NCL: cr_r0 = 12080; cb_g0 = -1348; cr_g0 = -4681; cb_b0 = 17546; break;
         case HPVCD_MATRIX_IDENTITY: cr_r0 = cb_g0 = cr_g0 = cb_b0 = 0; break;
         default: cr_r0 = 12901; cb_g0 = -1534; cr_g0 = -3835; cb_b0 = 15201; break;
     }
-    const long long cmax = (1 << bd) - 1;
-    const long long y_black = full ? 0 : 16 * scale, c_black = y_black, neutral = 128 * scale;
-    const int yr = min(yy, P.h - 1), xc = min(xx, P.w - 1);
-    const long long luma = load_sample(P.fin[0], P.bps, (size_t)yr * P.w + xc);
-    long long r, g, b;
-    if (P.idc == 0) {
-        r = g = b = (k_y * (luma - y_black) + ROUND) >> Q13;
-    } else {
-        const int crow = min(yy / P.sub_h, P.ch - 1), ccol = min(xx / P.sub_w, P.cw - 1);
-        const long long cb = load_sample(P.fin[1], P.bps, (size_t)crow * P.cw + ccol);
-        const long long cr = load_sample(P.fin[2], P.bps, (size_t)crow * P.cw + ccol);
-        if (rp.matrix == HPVCD_MATRIX_IDENTITY) {
-            if (full) {
-                r = cr; g = luma; b = cb;
-            } else {
-                r = (k_uv * (cr - c_black) + ROUND) >> Q13;
-                g = (k_y * (luma - y_black) + ROUND) >> Q13;
-                b = (k_uv * (cb - c_black) + ROUND) >> Q13;
-            }
-        } else if (rp.matrix == HPVCD_MATRIX_YCGCO) {
-            const long long cg = cb - neutral, co = cr - neutral, t = luma - cg;
-            r = t + co; g = luma + cg; b = t - co;
+    k.cr_to_r = (cr_r0 * k.k_uv + ROUND) >> Q13;
+    k.cb_to_g = (cb_g0 * k.k_uv + ROUND) >> Q13;
+    k.cr_to_g = (cr_g0 * k.k_uv + ROUND) >> Q13;
+    k.cb_to_b = (cb_b0 * k.k_uv + ROUND) >> Q13;
+    k.cmax = (1 << bd) - 1;
+    k.y_black = k.full ? 0 : 16 * scale;
+    k.c_black = k.y_black;
+    k.neutral = 128 * scale;
+    k.sh = bd - 8;
+    return k;
+}
+
+__device__ __forceinline__ uint32_t rgb_px(const RgbCoef& k, int idc, int luma, int cb, int cr) {
+    const int Q13 = 13, ROUND = 1 << 12;
+    int r, g, b;
+    if (idc == 0) {
+        r = g = b = (k.k_y * (luma - k.y_black) + ROUND) >> Q13;
+    } else if (k.matrix == HPVCD_MATRIX_IDENTITY) {
+        if (k.full) {
+            r = cr; g = luma; b = cb;
         } else {
-            const long long cr_to_r = (cr_r0 * k_uv + ROUND) >> Q13, cb_to_g = (cb_g0 * k_uv + ROUND) >> Q13;
-            const long long cr_to_g = (cr_g0 * k_uv + ROUND) >> Q13, cb_to_b = (cb_b0 * k_uv + ROUND) >> Q13;
-            const long long yv = k_y * (luma - y_black), cbc = cb - neutral, crc = cr - neutral;
-            r = (yv + cr_to_r * crc + ROUND) >> Q13;
-            g = (yv + cb_to_g * cbc + cr_to_g * crc + ROUND) >> Q13;
-            b = (yv + cb_to_b * cbc + ROUND) >> Q13;
+            r = (k.k_uv * (cr - k.c_black) + ROUND) >> Q13;
+            g = (k.k_y * (luma - k.y_black) + ROUND) >> Q13;
+            b = (k.k_uv * (cb - k.c_black) + ROUND) >> Q13;
+        }
+    } else if (k.matrix == HPVCD_MATRIX_YCGCO) {
+        const int cg = cb - k.neutral, co = cr - k.neutral, t = luma - cg;
+        r = t + co; g = luma + cg; b = t - co;
+    } else {
+        const int yv = k.k_y * (luma - k.y_black), cbc = cb - k.neutral, crc = cr - k.neutral;
+        r = (yv + k.cr_to_r * crc + ROUND) >> Q13;
+        g = (yv + k.cb_to_g * cbc + k.cr_to_g * crc + ROUND) >> Q13;
+        b = (yv + k.cb_to_b * cbc + ROUND) >> Q13;
+    }
+    r = clamp3i(r, 0, k.cmax) >> k.sh;
+    g = clamp3i(g, 0, k.cmax) >> k.sh;
+    b = clamp3i(b, 0, k.cmax) >> k.sh;
+    return (uint32_t)r | ((uint32_t)g << 8) | ((uint32_t)b << 16);
+}
+
+__global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out) {
+    const DevPic& P = pics[blockIdx.y];
+    uint8_t* canvas = out + P.canvas_off;
+    const int copy_w = min(P.crop_w, max(P.canvas_w - P.dst_x, 0));
+    const int copy_h = min(P.crop_h, max(P.canvas_h - P.dst_y, 0));
+    const int qw = (copy_w + 3) >> 2;
+    const int id = blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= qw * copy_h) return;
+    const int x0 = (id % qw) * 4, yy = id / qw;
+    const int cnt = min(4, copy_w - x0);
+    const RgbCoef k = rgb_coef(P);
+    // crop_w <= width (a multiple of 8) and copy_h <= height: x0 .. x0 + 3
+    // and yy are inside the planes
+    int luma[4], cb[4] = {0, 0, 0, 0}, cr[4] = {0, 0, 0, 0};
+    load4(P.fin[0], P.bps, (size_t)yy * P.w + x0, luma);
+    if (P.idc) {
+        const int crow = yy / P.sub_h;
+        if (P.sub_w == 2) {
+            const size_t ci = (size_t)crow * P.cw + (x0 >> 1);  // two chroma samples
+            int t = load_sample(P.fin[1], P.bps, ci), u = load_sample(P.fin[1], P.bps, ci + 1);
+            cb[0] = cb[1] = t; cb[2] = cb[3] = u;
+            t = load_sample(P.fin[2], P.bps, ci);
+            u = load_sample(P.fin[2], P.bps, ci + 1);
+            cr[0] = cr[1] = t; cr[2] = cr[3] = u;
+        } else {
+            load4(P.fin[1], P.bps, (size_t)crow * P.cw + x0, cb);
+            load4(P.fin[2], P.bps, (size_t)crow * P.cw + x0, cr);
         }
     }
-    const int sh = bd - 8;
-    r = r < 0 ? 0 : (r > cmax ? cmax : r);
-    g = g < 0 ? 0 : (g > cmax ? cmax : g);
-    b = b < 0 ? 0 : (b > cmax ? cmax : b);
-    uint8_t* o = canvas + ((size_t)(P.dst_y + yy) * rp.canvas_w + P.dst_x + xx) * 3;
-    o[0] = (uint8_t)(r >> sh);
-    o[1] = (uint8_t)(g >> sh);
-    o[2] = (uint8_t)(b >> sh);
+    uint32_t px[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) px[i] = rgb_px(k, P.idc, luma[i], cb[i], cr[i]);
+    uint8_t* o = canvas + ((size_t)(P.dst_y + yy) * P.canvas_w + P.dst_x + x0) * 3;
+    if (cnt == 4 && ((uintptr_t)o & 3) == 0) {
+        uint32_t* o32 = (uint32_t*)o;
+        o32[0] = px[0] | (px[1] << 24);
+        o32[1] = (px[1] >> 8) | (px[2] << 16);
+        o32[2] = (px[2] >> 16) | (px[3] << 8);
+    } else {
+        for (int i = 0; i < cnt; ++i) {
+            o[3 * i] = (uint8_t)px[i];
+            o[3 * i + 1] = (uint8_t)(px[i] >> 8);
+            o[3 * i + 2] = (uint8_t)(px[i] >> 16);
+        }
+    }
 }
 
 }  // namespace hpvcd
@@ -341,17 +448,18 @@ extern "C" cudaError_t hpvcd_launch_sao(const hpvcd::DevPic* pics, int n_pics, i
                                         cudaStream_t stream) {
     if (n_pics <= 0 || max_samples <= 0) return cudaSuccess;
     const int threads = 256;
-    dim3 grid((max_samples + threads - 1) / threads, n_pics, 3);
+    const int quads = (max_samples + 3) / 4;
+    dim3 grid((quads + threads - 1) / threads, n_pics, 3);
     hpvcd::k_sao<<<grid, threads, 0, stream>>>(pics);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }
 
-extern "C" cudaError_t hpvcd_launch_rgb(const hpvcd::DevPic* pics, int n_pics, int max_pixels, uint8_t* out,
+extern "C" cudaError_t hpvcd_launch_rgb(const hpvcd::DevPic* pics, int n_pics, int max_quads, uint8_t* out,
                                         cudaStream_t stream) {
-    if (n_pics <= 0 || max_pixels <= 0) return cudaSuccess;
+    if (n_pics <= 0 || max_quads <= 0) return cudaSuccess;
     const int threads = 256;
-    dim3 grid((max_pixels + threads - 1) / threads, n_pics, 1);
+    dim3 grid((max_quads + threads - 1) / threads, n_pics, 1);
     hpvcd::k_rgb<<<grid, threads, 0, stream>>>(pics, out);
     hpvcd_note_launches(1);
     return cudaGetLastError();

@@ -27,6 +27,8 @@ extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaSt
 extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, uint8_t*, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_mc(const DevPic*, int, int, int, cudaStream_t);
+extern "C" hpvcd_status hpvcd_mlp_pick(hpvcd_mlp*, const float*, uint32_t, void*, uint32_t*);
+extern "C" uint32_t hpvcd_mlp_variants(const hpvcd_mlp*);
 extern "C" cudaError_t hpvcd_launch_features(const DevPic*, uint32_t, uint32_t, unsigned long long*, float*, int,
                                              cudaStream_t);
 
@@ -116,7 +118,7 @@ struct hpvcd_plan {
     int c444 = 0;
     int recon_occ = 1;  // k_recon CTAs per SM at full occupancy
     int sms = 148;
-    int max_rgb = 0;
+    int max_rgb = 0;  // largest RGB job of one picture, in 4-pixel quads
     uint32_t launches_per_run = 0;
     // Plans owned by a context allocate from the stream-ordered pool of the
     // ticket's stream (no device-wide synchronisation when the layout of a
@@ -405,7 +407,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             d.dst_x = (int)tp.dst_x; d.dst_y = (int)tp.dst_y;
             d.crop_w = (int)std::min<uint32_t>(tp.crop_w, p.width);
             d.crop_h = (int)std::min<uint32_t>(tp.crop_h, p.height);
-            P->max_rgb = std::max(P->max_rgb, d.crop_w * d.crop_h);
+            P->max_rgb = std::max(P->max_rgb, (d.crop_w + 3) / 4 * d.crop_h);  // 4-pixel quads
         }
     }
     // ---- wavefront schedule per segment: sort CTUs by (x + 2y, picture, x) ----
@@ -604,6 +606,10 @@ struct hpvcd_gpu {
     uint64_t next_ticket = 1;
     uint64_t budget = 0;
     uint64_t in_use = 0;
+    // schedule selection per submitted batch (hpvcd_gpu_set_selector)
+    hpvcd_mlp* sel = nullptr;
+    std::vector<hpvcd_sched> sel_cands;
+    uint64_t sel_picks[HPVCD_MLP_MAX_VARIANTS] = {};
     ~hpvcd_gpu() {
         for (Slot& s : slots) {
             if (s.stream) cudaStreamSynchronize(s.stream);
@@ -929,9 +935,6 @@ HPVCD_API hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched*
     return HPVCD_OK;
 }
 
-extern "C" hpvcd_status hpvcd_mlp_pick(hpvcd_mlp*, const float*, uint32_t, void*, uint32_t*);
-extern "C" uint32_t hpvcd_mlp_variants(const hpvcd_mlp*);
-
 // Schedule selection for a plan: with a selector network, the features of
 // the whole batch are computed on the device and the network's predicted-
 // fastest candidate is set; without one (or when its candidate count does
@@ -992,6 +995,22 @@ HPVCD_API hpvcd_status hpvcd_gpu_create(const hpvcd_gpu_cfg* cfg, hpvcd_gpu** ou
         }
     }
     *out = g;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* g, hpvcd_mlp* mlp, const hpvcd_sched* cands, uint32_t n) {
+    if (!g || (mlp && (!cands || n == 0 || n != hpvcd_mlp_variants(mlp)))) return HPVCD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g->mu);
+    g->sel = mlp;
+    g->sel_cands.assign(cands, cands + (mlp ? n : 0));
+    std::memset(g->sel_picks, 0, sizeof(g->sel_picks));
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu* g, uint64_t* counts, uint32_t n) {
+    if (!g || !counts) return HPVCD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g->mu);
+    for (uint32_t i = 0; i < n; ++i) counts[i] = i < HPVCD_MLP_MAX_VARIANTS ? g->sel_picks[i] : 0;
     return HPVCD_OK;
 }
 
@@ -1107,6 +1126,13 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     g->in_use = g->in_use - held + slot->d_in_cap + slot->plan_bytes;
     slot->held = slot->d_in_cap + slot->plan_bytes;
     if (st != HPVCD_OK) return st;
+    if (g->sel) {  // the network picks the batch's schedule from its features
+        uint32_t pick = 0;
+        st = hpvcd_plan_select(slot->plan, g->sel, g->sel_cands.data(), (uint32_t)g->sel_cands.size(), slot->stream,
+                               &pick);
+        if (st != HPVCD_OK) return st;
+        ++g->sel_picks[pick];
+    }
     st = plan_launch(slot->plan, HPVCD_STAGE_ALL, slot->stream);
     if (st != HPVCD_OK) return st;
     // ---- output copy back ----

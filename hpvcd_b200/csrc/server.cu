@@ -360,6 +360,22 @@ HPVCD_API uint32_t hpvcd_server_poll(hpvcd_server* s, hpvcd_completion* out, uin
     return k;
 }
 
+extern "C" hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu*, hpvcd_mlp*, const hpvcd_sched*, uint32_t);
+extern "C" hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu*, uint64_t*, uint32_t);
+
+// The batches this server launches get their schedule from the selector
+// network (NULL: the default schedule).
+HPVCD_API hpvcd_status hpvcd_server_set_selector(hpvcd_server* s, hpvcd_mlp* mlp, const hpvcd_sched* cands,
+                                                 uint32_t n) {
+    if (!s) return HPVCD_ERR_INVALID_ARG;
+    return hpvcd_gpu_set_selector(s->gpu, mlp, cands, n);
+}
+
+HPVCD_API hpvcd_status hpvcd_server_selector_picks(hpvcd_server* s, uint64_t* counts, uint32_t n) {
+    if (!s) return HPVCD_ERR_INVALID_ARG;
+    return hpvcd_gpu_selector_picks(s->gpu, counts, n);
+}
+
 HPVCD_API uint32_t hpvcd_server_pending(hpvcd_server* s) {
     if (!s) return 0;
     std::lock_guard<std::mutex> lock(s->mu);

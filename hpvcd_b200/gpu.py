@@ -87,6 +87,13 @@ class GpuDecoder:
         raw = self.read(t)
         return split_planes(pics, raw)
 
+    def set_selector(self, mlp, schedules) -> None:
+        """Per-submit schedule from the selector network (None: default)."""
+        arr = (abi.Sched * len(schedules))(*schedules)
+        self._sel_keep = (mlp, arr)
+        _check(self._L.hpvcd_gpu_set_selector(self._h, mlp.handle if mlp is not None else None, arr,
+                                              len(schedules)), "hpvcd_gpu_set_selector")
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.hpvcd_gpu_destroy(self._h)
@@ -317,6 +324,18 @@ class Server:
 
     def pending(self) -> int:
         return self._L.hpvcd_server_pending(self._h)
+
+    def set_selector(self, mlp, schedules) -> None:
+        """Per-batch schedule from the selector network (None: default)."""
+        arr = (abi.Sched * len(schedules))(*schedules)
+        self._sel_keep = (mlp, arr)
+        _check(self._L.hpvcd_server_set_selector(self._h, mlp.handle if mlp is not None else None, arr,
+                                                 len(schedules)), "hpvcd_server_set_selector")
+
+    def selector_picks(self, n: int) -> list:
+        out = (C.c_uint64 * n)()
+        _check(self._L.hpvcd_server_selector_picks(self._h, out, n), "hpvcd_server_selector_picks")
+        return list(out)
 
     def close(self):
         if getattr(self, "_h", None):

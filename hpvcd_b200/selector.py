@@ -316,3 +316,113 @@ def collect(n_frames: int, seed: int = 0, out_path: str | None = None, threads: 
                 np.savez(out_path, features=X[:done], ms=T[:done], seed=seed, start=start)
                 print(f"[selector] {done}/{n_frames} frames", flush=True)
     return X[:done], T[:done]
+
+
+# ---------------------------------------------------------------------------
+# Training and evaluation
+# ---------------------------------------------------------------------------
+
+def train_network(x: np.ndarray, ms: np.ndarray, epochs: int = 200, batch: int = 256, lr: float = 2e-3,
+                  seed: int = 1) -> Mlp:
+    """Train the selector network on the GPU (hpvcd_mlp_train) on features
+    and autotuner timings."""
+    m = Mlp(K, seed=seed)
+    m.train(x, targets(ms), epochs=epochs, batch=batch, lr=lr, seed=seed + 1)
+    return m
+
+
+def evaluate_live(mlp: Mlp, n_frames: int, seed: int = 12345, reps: int = 2, log=None) -> dict:
+    """Fresh frames (a seed never trained on): the network's pick, the
+    default schedule and exhaustive autotuning, all timed on the GPU.  Also
+    the cost of choosing (features + network forward, including the read of
+    the pick by the host)."""
+    import torch
+
+    from .gpu import DevicePlan
+
+    L = abi.lib()
+    specs = frame_specs(n_frames, seed)
+    refs = RefPictures()
+    times, picks, choose_ms = [], [], []
+    st = torch.cuda.current_stream()
+    for i, sp in enumerate(specs):
+        keep, pics, fi = build_frame(sp, refs)
+        plan = DevicePlan(pics, resident=refs.resident if fi else None)
+        _, ms = measure(plan, fi, reps=reps)
+        fdev = torch.empty(abi.FEATURES, dtype=torch.float32, device="cuda")
+        out = np.empty(1, np.uint32)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        _check(L.hpvcd_plan_features(plan._h, fi, 1, C.c_void_p(fdev.data_ptr()), C.c_void_p(st.cuda_stream)),
+               "hpvcd_plan_features")
+        _check(L.hpvcd_mlp_pick(mlp.handle, C.c_void_p(fdev.data_ptr()), 1, C.c_void_p(st.cuda_stream),
+                                out.ctypes.data_as(C.POINTER(C.c_uint32))), "hpvcd_mlp_pick")
+        t1.record()
+        torch.cuda.synchronize()
+        choose_ms.append(t0.elapsed_time(t1))
+        plan.close()
+        del keep
+        times.append(ms)
+        picks.append(int(out[0]))
+        if log and (i + 1) % 20 == 0:
+            log(f"[selector] evaluated {i + 1}/{n_frames}")
+    ms = np.array(times)
+    r = score(np.array(picks), ms)
+    r["choose_ms_mean"] = float(np.mean(choose_ms))
+    r["seed"] = seed
+    return r
+
+
+def _main(argv=None):
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="selector data collection / training / evaluation")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    c = sub.add_parser("collect")
+    c.add_argument("--frames", type=int, required=True)
+    c.add_argument("--start", type=int, default=0)
+    c.add_argument("--seed", type=int, default=0)
+    c.add_argument("--out", required=True)
+    c.add_argument("--threads", type=int, default=8)
+    t = sub.add_parser("train")
+    t.add_argument("--data", nargs="+", required=True)
+    t.add_argument("--holdout", type=float, default=0.2)
+    t.add_argument("--epochs", type=int, default=200)
+    t.add_argument("--out", default=WEIGHTS_PATH)
+    t.add_argument("--merged", default=None, help="write the merged data set with its train / held-out split")
+    e = sub.add_parser("evaluate")
+    e.add_argument("--frames", type=int, default=100)
+    e.add_argument("--seed", type=int, default=12345)
+    a = ap.parse_args(argv)
+    if a.cmd == "collect":
+        collect(a.frames, seed=a.seed, out_path=a.out, threads=a.threads, start=a.start)
+    elif a.cmd == "train":
+        xs, ts = [], []
+        for path in a.data:
+            z = np.load(path)
+            xs.append(z["features"])
+            ts.append(z["ms"])
+        x = np.concatenate(xs)
+        ms = np.concatenate(ts)
+        keep = np.all(ms > 0, axis=1)
+        x, ms = x[keep], ms[keep]
+        split = int(round(len(x) * (1 - a.holdout)))
+        m = train_network(x[:split], ms[:split], epochs=a.epochs)
+        picks = m.pick(x[split:])
+        fixed = best_fixed(ms[:split])
+        res = {"train_rows": split, "heldout_rows": len(x) - split, "heldout": score(picks, ms[split:]),
+               "best_fixed": fixed, "best_fixed_heldout": score(np.full(len(ms) - split, fixed), ms[split:])}
+        print(json.dumps(res, indent=1))
+        m.save(a.out)
+        if a.merged:
+            np.savez_compressed(a.merged, features=x.astype(np.float32), ms=ms.astype(np.float32),
+                                train_rows=split)
+    elif a.cmd == "evaluate":
+        m = Mlp.load()
+        print(json.dumps(evaluate_live(m, a.frames, a.seed, log=print), indent=1))
+
+
+if __name__ == "__main__":
+    _main()

@@ -66,7 +66,7 @@ def _percentile(v, q):
 
 def run(imgs, batching: bool, arrival_rate: float | None, seed: int = 1, max_inflight: int = 2,
         device: int = 0, timeout_s: float = 600.0, batch_window_us: int = 2000, warmup: int = 8,
-        zero_copy: bool = False) -> dict:
+        zero_copy: bool = False, selector=None) -> dict:
     """Submit every image (Poisson arrivals at `arrival_rate`/s, or all at
     once when None) and collect the completions.  Returns throughput and
     latency percentiles."""
@@ -76,6 +76,9 @@ def run(imgs, batching: bool, arrival_rate: float | None, seed: int = 1, max_inf
     bad = 0
     with Server(device, max_inflight=max_inflight if batching else 1, batching=batching,
                 batch_window_us=batch_window_us if batching else 0) as srv:
+        if selector is not None:  # the network picks every batch's schedule
+            from .selector import SCHEDULES
+            srv.set_selector(selector, SCHEDULES)
         # warm the server (page-locked arenas, device pool, plan code paths)
         def submit(im, user):
             if zero_copy:
@@ -120,4 +123,5 @@ def run(imgs, batching: bool, arrival_rate: float | None, seed: int = 1, max_inf
             "seconds": round(t1 - t0, 4), "mpix_per_s": round(mpix / (t1 - t0), 2),
             "p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99),
             "queue_p50_ms": _percentile(qms, 50), "mean_batch_pictures": float(np.mean(batch)) if batch else 0.0,
-            "arrival_rate": arrival_rate, "batching": batching, "zero_copy": zero_copy}
+            "arrival_rate": arrival_rate, "batching": batching, "zero_copy": zero_copy,
+            "learned_schedule": selector is not None}

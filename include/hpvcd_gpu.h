@@ -263,6 +263,8 @@ const char* hpvcd_last_error_string(void);
 /* ------------------------------------------------------------------------ */
 typedef struct hpvcd_gpu hpvcd_gpu;
 typedef uint64_t hpvcd_ticket;
+struct hpvcd_sched; /* schedule knobs, defined with the plan API below   */
+struct hpvcd_mlp;   /* selector network, declared with schedule selection */
 
 typedef struct hpvcd_gpu_cfg {
     int32_t device;           /* CUDA device ordinal                          */
@@ -295,6 +297,13 @@ hpvcd_status hpvcd_gpu_wait(hpvcd_gpu* ctx, hpvcd_ticket ticket, int32_t timeout
 hpvcd_status hpvcd_gpu_output_size(hpvcd_gpu* ctx, hpvcd_ticket ticket, uint64_t* bytes);
 /* Copy a finished ticket's output into caller memory and release the ticket. */
 hpvcd_status hpvcd_gpu_read(hpvcd_gpu* ctx, hpvcd_ticket ticket, void* dst, uint64_t bytes);
+/* Per-batch schedule selection for this context: every submit computes the
+ * batch's features on the device, runs the selector network (a short host
+ * wait for its pick) and launches the picked candidate; mlp NULL -> default
+ * schedule.  n must equal the network's output count. */
+hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* ctx, struct hpvcd_mlp* mlp, const struct hpvcd_sched* cands,
+                                    uint32_t n);
+hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu* ctx, uint64_t* counts, uint32_t n);
 
 /* ------------------------------------------------------------------------ */
 /* Device-buffer API (plans).  The picture descriptors point at device      */
@@ -505,6 +514,13 @@ uint32_t hpvcd_server_poll(hpvcd_server* srv, hpvcd_completion* out, uint32_t ma
 /* Requests submitted and not yet returned by hpvcd_server_poll. */
 uint32_t hpvcd_server_pending(hpvcd_server* srv);
 hpvcd_status hpvcd_server_destroy(hpvcd_server* srv);
+/* Schedule of the fused batches: the selector network's pick per batch
+ * (hpvcd_plan_select) among n candidates; mlp NULL -> default schedule.  The
+ * network must outlive the server (or be removed first). */
+hpvcd_status hpvcd_server_set_selector(hpvcd_server* srv, struct hpvcd_mlp* mlp, const hpvcd_sched* cands,
+                                       uint32_t n);
+/* How often each candidate was picked since the selector was set. */
+hpvcd_status hpvcd_server_selector_picks(hpvcd_server* srv, uint64_t* counts, uint32_t n);
 
 /* ------------------------------------------------------------------------ */
 /* Utilities (no reference counterpart).                                    */

@@ -317,3 +317,36 @@ def test_trained_selector_gains_over_no_network():
     assert s["ms_selected"] <= s_fixed["ms_selected"]
     assert s["regret_vs_exhaustive"] < 0.02
     m.close()
+
+
+@pytest.mark.gpu
+def test_server_with_selector_keeps_pixels():
+    """Batches launched by the serving loop with the network choosing each
+    batch's schedule decode exactly as the oracle does."""
+    _gpu()
+    from hpvcd_b200.gpu import Server
+    from oracle import oracle as O
+    s = synth.SynthSet()
+    imgs = []
+    for i, (w, h, bd, idc) in enumerate([(640, 448, 10, 1), (1024, 512, 8, 1), (512, 700, 8, 3), (256, 256, 10, 1)]):
+        g = synth.make_grid(w, h, seed=300 + i, bit_depth=bd, chroma_idc=idc, synth=s)
+        first = len(s) - g.cols * g.rows
+        imgs.append(([s.picture(first + j) for j in range(g.cols * g.rows)], g.places, w, h))
+    m = selector.Mlp(selector.K, seed=3)
+    with Server(0, max_inflight=2, batching=True, batch_window_us=100000) as srv:
+        srv.set_selector(m, selector.SCHEDULES)
+        for k, (pics, places, w, h) in enumerate(imgs):
+            srv.submit(pics, places, w, h, user=k)
+        got = {}
+        while len(got) < len(imgs):
+            for c in srv.poll(16, timeout_ms=60000):
+                assert c["status"] == abi.OK
+                got[c["user"]] = c
+        picks = srv.selector_picks(selector.K)
+        srv.set_selector(None, selector.SCHEDULES)
+    assert sum(picks) >= 1
+    for k, (pics, places, w, h) in enumerate(imgs):
+        out, keep = synth.grid_output(synth.Grid(w, h, 512, s, places))
+        _, ref = O.decode_batch(pics, out, want_planes=False)
+        assert np.array_equal(got[k]["image"], ref), k
+    m.close()
