@@ -366,16 +366,10 @@ def device_batched_vs_plain(imgs, local, reps: int = 5):
     from hpvcd_b200 import abi
     from hpvcd_b200.gpu import DevicePlan
 
+    from hpvcd_b200 import serving
+
     stream = torch.cuda.Stream(device=local)
-    pics, places, canv = [], [], []
-    for k, im in enumerate(imgs):
-        pics += im.pics
-        places += [(x, y, w, h, k) for (x, y, w, h) in im.places]
-        canv.append(abi.Canvas(im.width, im.height, im.matrix, int(im.full_range)))
-    pl_arr = (abi.TilePlace * len(places))(*[abi.TilePlace(*t) for t in places])
-    cv_arr = (abi.Canvas * len(canv))(*canv)
-    out = abi.Output(abi.OUT_RGB8, 0, 0, 0, 0, C.cast(pl_arr, C.c_void_p), None, 0, len(canv),
-                     C.cast(cv_arr, C.c_void_p))
+    pics, out, out_keep = serving.fused_output(imgs)
     fused = DevicePlan(pics, out, device=local)
     singles = []
     keep = []

@@ -271,11 +271,17 @@ def build_frame(sp: FrameSpec, refs: RefPictures | None, w=W4K, h=H4K):
 
 def measure(plan, frame_index: int, reps: int = 2, stages: int = abi.STAGE_ALL):
     """Features of the frame and the autotuner's time of every schedule."""
+    return measure_range(plan, frame_index, 1, reps, stages)
+
+
+def measure_range(plan, first: int, count: int, reps: int = 2, stages: int = abi.STAGE_ALL):
+    """Features of pictures [first, first + count) and the autotuner's time of
+    every schedule for the whole plan."""
     torch = _torch()
     L = abi.lib()
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     f = torch.empty(abi.FEATURES, dtype=torch.float32, device="cuda")
-    _check(L.hpvcd_plan_features(plan._h, frame_index, 1, C.c_void_p(f.data_ptr()), st), "hpvcd_plan_features")
+    _check(L.hpvcd_plan_features(plan._h, first, count, C.c_void_p(f.data_ptr()), st), "hpvcd_plan_features")
     ms = (C.c_float * K)()
     best = C.c_uint32()
     _check(L.hpvcd_plan_autotune(plan._h, schedules_array(), K, stages, reps, 0, st, ms, C.byref(best)),
@@ -316,6 +322,47 @@ def collect(n_frames: int, seed: int = 0, out_path: str | None = None, threads: 
                 np.savez(out_path, features=X[:done], ms=T[:done], seed=seed, start=start)
                 print(f"[selector] {done}/{n_frames} frames", flush=True)
     return X[:done], T[:done]
+
+
+def collect_batches(n_batches: int, seed: int = 0, out_path: str | None = None, threads: int = 4,
+                    reps: int = 2, max_images: int = 64, log_every: int = 50, start: int = 0):
+    """Serving batches as the selector sees them: 1..max_images images of
+    the mixed-size serving workload (serving.make_images) fused into one
+    plan with one RGB8 canvas per image; features over all pictures and the
+    autotuner's time of every schedule.  Returns (features, ms)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from . import serving
+    from .gpu import DevicePlan
+
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(1, max_images + 1, size=start + n_batches)[start:]
+
+    def make(i):
+        keep, imgs = serving.make_images(int(counts[i]), seed=seed * 100_003 + start + i)
+        return keep, imgs
+
+    X = np.zeros((n_batches, abi.FEATURES), np.float32)
+    T = np.zeros((n_batches, K), np.float32)
+    with ThreadPoolExecutor(threads) as pool:
+        futs = [pool.submit(make, i) for i in range(min(threads, n_batches))]
+        nxt = len(futs)
+        for i in range(n_batches):
+            keep, imgs = futs[i].result()
+            futs[i] = None
+            if nxt < n_batches:
+                futs.append(pool.submit(make, nxt))
+                nxt += 1
+            pics, out, okeep = serving.fused_output(imgs)
+            plan = DevicePlan(pics, out)
+            f, ms = measure_range(plan, 0, len(pics), reps=reps)
+            X[i], T[i] = f, ms
+            plan.close()
+            del keep, imgs, okeep
+            if out_path and ((i + 1) % log_every == 0 or i + 1 == n_batches):
+                np.savez(out_path, features=X[:i + 1], ms=T[:i + 1], seed=seed, start=start)
+                print(f"[selector] {i + 1}/{n_batches} batches", flush=True)
+    return X, T
 
 
 # ---------------------------------------------------------------------------
@@ -386,6 +433,12 @@ def _main(argv=None):
     c.add_argument("--seed", type=int, default=0)
     c.add_argument("--out", required=True)
     c.add_argument("--threads", type=int, default=8)
+    b = sub.add_parser("collect-batches")
+    b.add_argument("--batches", type=int, required=True)
+    b.add_argument("--start", type=int, default=0)
+    b.add_argument("--seed", type=int, default=1)
+    b.add_argument("--out", required=True)
+    b.add_argument("--threads", type=int, default=4)
     t = sub.add_parser("train")
     t.add_argument("--data", nargs="+", required=True)
     t.add_argument("--holdout", type=float, default=0.2)
@@ -398,6 +451,8 @@ def _main(argv=None):
     a = ap.parse_args(argv)
     if a.cmd == "collect":
         collect(a.frames, seed=a.seed, out_path=a.out, threads=a.threads, start=a.start)
+    elif a.cmd == "collect-batches":
+        collect_batches(a.batches, seed=a.seed, out_path=a.out, threads=a.threads, start=a.start)
     elif a.cmd == "train":
         xs, ts = [], []
         for path in a.data:

@@ -60,6 +60,22 @@ def make_images(n_images: int, seed: int = 0, max_side: int = 4096):
     return s, imgs
 
 
+def fused_output(imgs):
+    """All tiles of all images as one batch: (pictures, hpvcd_output with one
+    RGB8 canvas per image, keep-alive arrays)."""
+    import ctypes as C
+    pics, places, canv = [], [], []
+    for k, im in enumerate(imgs):
+        pics += im.pics
+        places += [(x, y, w, h, k) for (x, y, w, h) in im.places]
+        canv.append(abi.Canvas(im.width, im.height, im.matrix, int(im.full_range)))
+    pl_arr = (abi.TilePlace * len(places))(*[abi.TilePlace(*t) for t in places])
+    cv_arr = (abi.Canvas * len(canv))(*canv)
+    out = abi.Output(abi.OUT_RGB8, 0, 0, 0, 0, C.cast(pl_arr, C.c_void_p), None, 0, len(canv),
+                     C.cast(cv_arr, C.c_void_p))
+    return pics, out, (pl_arr, cv_arr)
+
+
 def _percentile(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 

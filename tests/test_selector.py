@@ -162,6 +162,26 @@ def test_tu_mix_steers_tb_sizes():
             assert f[5] > 0.6
 
 
+def test_trained_selector_gains_on_heldout_frames_cpu():
+    """The committed network, evaluated with the numpy oracle forward pass on
+    its bf16 weights over the held-out measured frames: faster in total
+    than the fixed default schedule and than the best single schedule of the
+    training frames, and within 1 % of exhaustive autotuning."""
+    if not (os.path.exists(TIMINGS) and os.path.exists(selector.WEIGHTS_PATH)):
+        pytest.skip("no committed selector timings / weights")
+    z = np.load(TIMINGS)
+    x, ms, split = z["features"], z["ms"].astype(np.float64), int(z["train_rows"])
+    w = np.load(selector.WEIGHTS_PATH)
+    K = int(w["n_variants"])
+    y, _, _ = mlp_ref.forward(mlp_ref.bf16_round(w["params"]), x[split:], K)
+    s = selector.score(y.argmin(axis=1), ms[split:])
+    fixed = selector.best_fixed(ms[:split])
+    s_fixed = selector.score(np.full(len(ms) - split, fixed), ms[split:])
+    assert s["gain_vs_default"] > 0.03
+    assert s["ms_selected"] <= s_fixed["ms_selected"]
+    assert s["regret_vs_exhaustive"] < 0.01
+
+
 # ---------------------------------------------------------------------------
 # GPU
 # ---------------------------------------------------------------------------
@@ -313,9 +333,12 @@ def test_trained_selector_gains_over_no_network():
     s = selector.score(picks, ms[split:])
     fixed = selector.best_fixed(ms[:split])
     s_fixed = selector.score(np.full(len(ms) - split, fixed), ms[split:])
-    assert s["gain_vs_default"] > 0.0
+    assert s["gain_vs_default"] > 0.03
     assert s["ms_selected"] <= s_fixed["ms_selected"]
-    assert s["regret_vs_exhaustive"] < 0.02
+    assert s["regret_vs_exhaustive"] < 0.01
+    # the device picks are the oracle's argmin on the same bf16 weights
+    y, _, _ = mlp_ref.forward(m.params(), x[split:], selector.K)
+    assert np.mean(y.argmin(axis=1) == picks) > 0.99
     m.close()
 
 
