@@ -65,6 +65,7 @@ STAGE_GRAPH = 0x100
 FEATURES = 16
 MLP_HIDDEN = 64
 MLP_MAX_VARIANTS = 32
+MLP_NO_PICK = 0xFFFFFFFF
 
 # Fixed per-device scratch of hpvcd_decode_noalloc (bytes).
 NOALLOC_SCRATCH_BYTES = 12 * 1024 * 1024 + 256 * 1024
@@ -280,6 +281,7 @@ def lib() -> C.CDLL:
             "hpvcd_mlp_adam_step": (i32, [vp, C.c_float, vp]),
             "hpvcd_mlp_train": (i32, [vp, vp, vp, u32, u32, u32, C.c_float, u64, vp, C.POINTER(C.c_float)]),
             "hpvcd_mlp_pick": (i32, [vp, vp, u32, vp, C.POINTER(u32)]),
+            "hpvcd_mlp_set_domain": (i32, [vp, vp, vp]),
             "hpvcd_gpu_set_selector": (i32, [vp, vp, C.POINTER(Sched), u32]),
             "hpvcd_gpu_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
             "hpvcd_server_set_selector": (i32, [vp, vp, C.POINTER(Sched), u32]),

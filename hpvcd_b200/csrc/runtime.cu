@@ -609,7 +609,7 @@ struct hpvcd_gpu {
     // schedule selection per submitted batch (hpvcd_gpu_set_selector)
     hpvcd_mlp* sel = nullptr;
     std::vector<hpvcd_sched> sel_cands;
-    uint64_t sel_picks[HPVCD_MLP_MAX_VARIANTS] = {};
+    uint64_t sel_picks[HPVCD_MLP_MAX_VARIANTS + 1] = {};  // last entry: batches outside the domain
     ~hpvcd_gpu() {
         for (Slot& s : slots) {
             if (s.stream) cudaStreamSynchronize(s.stream);
@@ -948,8 +948,8 @@ HPVCD_API hpvcd_status hpvcd_plan_select(hpvcd_plan* plan, hpvcd_mlp* mlp, const
         float* fv = (float*)(plan->d_feat + 32);
         s = hpvcd_plan_features(plan, 0, (uint32_t)plan->src.size(), fv, stream);
         if (s == HPVCD_OK) s = hpvcd_mlp_pick(mlp, fv, 1, stream, &pick);
-        if (s == HPVCD_OK && pick >= n) s = HPVCD_ERR_INVALID_ARG;
-        if (s == HPVCD_OK) s = hpvcd_plan_set_sched(plan, &cands[pick]);
+        // outside the network's training domain: the first (default) candidate
+        if (s == HPVCD_OK) s = hpvcd_plan_set_sched(plan, &cands[pick == HPVCD_MLP_NO_PICK ? 0 : pick]);
     } else {
         s = hpvcd_plan_autotune(plan, cands, n, HPVCD_STAGE_ALL, 2, 1, stream, nullptr, &pick);
     }
@@ -1010,7 +1010,11 @@ HPVCD_API hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* g, hpvcd_mlp* mlp, cons
 HPVCD_API hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu* g, uint64_t* counts, uint32_t n) {
     if (!g || !counts) return HPVCD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g->mu);
-    for (uint32_t i = 0; i < n; ++i) counts[i] = i < HPVCD_MLP_MAX_VARIANTS ? g->sel_picks[i] : 0;
+    // counts[0 .. K-1]: picks per candidate; counts[K] (when n > K): batches
+    // outside the network's domain, which ran candidate 0
+    const uint32_t K = (uint32_t)g->sel_cands.size();
+    for (uint32_t i = 0; i < n; ++i)
+        counts[i] = i < K ? g->sel_picks[i] : (i == K ? g->sel_picks[HPVCD_MLP_MAX_VARIANTS] : 0);
     return HPVCD_OK;
 }
 
@@ -1131,7 +1135,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         st = hpvcd_plan_select(slot->plan, g->sel, g->sel_cands.data(), (uint32_t)g->sel_cands.size(), slot->stream,
                                &pick);
         if (st != HPVCD_OK) return st;
-        ++g->sel_picks[pick];
+        ++g->sel_picks[pick == HPVCD_MLP_NO_PICK ? HPVCD_MLP_MAX_VARIANTS : pick];
     }
     st = plan_launch(slot->plan, HPVCD_STAGE_ALL, slot->stream);
     if (st != HPVCD_OK) return st;

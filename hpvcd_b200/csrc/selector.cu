@@ -294,14 +294,21 @@ __global__ void k_from_bf16(const __nv_bfloat16* __restrict__ src, int n, float*
     if (i < n) dst[i] = __bfloat162float(src[i]);
 }
 
-// argmin over the K outputs of each sample.
-__global__ void k_mlp_argmin(const float* __restrict__ y, int B, int K, uint32_t* __restrict__ pick) {
+// argmin over the K outputs of each sample; with a domain (lo[16], hi[16]),
+// a sample with a feature outside it gets HPVCD_MLP_NO_PICK instead.
+__global__ void k_mlp_argmin(const float* __restrict__ y, int B, int K, uint32_t* __restrict__ pick,
+                             const float* __restrict__ x, const float* __restrict__ dom) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= B) return;
     int best = 0;
     for (int k = 1; k < K; ++k)
         if (y[(size_t)s * K + k] < y[(size_t)s * K + best]) best = k;
-    pick[s] = (uint32_t)best;
+    if (dom)
+        for (int i = 0; i < kFeatures; ++i) {
+            const float v = x[(size_t)s * kFeatures + i];
+            if (!(v >= dom[i] && v <= dom[kFeatures + i])) best = -1;
+        }
+    pick[s] = best < 0 ? (uint32_t)HPVCD_MLP_NO_PICK : (uint32_t)best;
 }
 
 }  // namespace hpvcd
@@ -364,8 +371,9 @@ extern "C" cudaError_t hpvcd_launch_bf16_convert(const float* src, int n, void* 
     return cudaGetLastError();
 }
 
-extern "C" cudaError_t hpvcd_launch_mlp_argmin(const float* y, int B, int K, uint32_t* pick, cudaStream_t st) {
-    k_mlp_argmin<<<(B + 127) / 128, 128, 0, st>>>(y, B, K, pick);
+extern "C" cudaError_t hpvcd_launch_mlp_argmin(const float* y, int B, int K, uint32_t* pick, const float* x,
+                                               const float* dom, cudaStream_t st) {
+    k_mlp_argmin<<<(B + 127) / 128, 128, 0, st>>>(y, B, K, pick, x, dom);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }
@@ -416,9 +424,11 @@ struct hpvcd_mlp {
     uint32_t* idx = nullptr;  // batch row indices
     int idx_cap = 0;
     long long step = 0;
+    float* dom = nullptr;     // feature domain lo[16], hi[16] (device)
+    bool has_domain = false;
     ~hpvcd_mlp() {
         cudaFree(w); cudaFree(master); cudaFree(m); cudaFree(v); cudaFree(grad); cudaFree(loss);
-        cudaFree(pick); cudaFree(act); cudaFree(idx);
+        cudaFree(pick); cudaFree(act); cudaFree(idx); cudaFree(dom);
     }
     size_t per_sample() const { return (size_t)2 * K + 4 * kHidden + kFeatures + K; }
     cudaError_t reserve(int B) {
@@ -489,6 +499,7 @@ HPVCD_API hpvcd_status hpvcd_mlp_create(uint32_t n_variants, uint64_t seed, hpvc
     if (e == cudaSuccess) e = cudaMalloc(&M->grad, sizeof(float) * M->P);
     if (e == cudaSuccess) e = cudaMalloc(&M->loss, sizeof(float) * 4);
     if (e == cudaSuccess) e = cudaMalloc(&M->pick, sizeof(uint32_t) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&M->dom, sizeof(float) * 2 * kFeatures);
     if (e != cudaSuccess) {
         delete M;
         return hpvcd_internal_status(e);
@@ -535,6 +546,20 @@ HPVCD_API hpvcd_status hpvcd_mlp_get_params(hpvcd_mlp* M, float* host, int maste
         if (e == cudaSuccess) e = cudaMemcpy(host, tmp, sizeof(float) * M->P, cudaMemcpyDeviceToHost);
         cudaFree(tmp);
     }
+    return hpvcd_internal_status(e);
+}
+
+// Feature domain of the training data: a pick for features outside
+// [lo, hi] is HPVCD_MLP_NO_PICK (callers then keep the default schedule).
+HPVCD_API hpvcd_status hpvcd_mlp_set_domain(hpvcd_mlp* M, const float* lo, const float* hi) {
+    if (!M || (!lo) != (!hi)) return HPVCD_ERR_INVALID_ARG;
+    if (!lo) {
+        M->has_domain = false;
+        return HPVCD_OK;
+    }
+    cudaError_t e = cudaMemcpy(M->dom, lo, sizeof(float) * kFeatures, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(M->dom + kFeatures, hi, sizeof(float) * kFeatures, cudaMemcpyHostToDevice);
+    M->has_domain = e == cudaSuccess;
     return hpvcd_internal_status(e);
 }
 
@@ -634,7 +659,7 @@ HPVCD_API hpvcd_status hpvcd_mlp_pick(hpvcd_mlp* M, const float* dev_x, uint32_t
         if (e != cudaSuccess) return hpvcd_internal_status(e);
         dpick = tmp;
     }
-    e = hpvcd_launch_mlp_argmin(M->y(), (int)B, M->K, dpick, st);
+    e = hpvcd_launch_mlp_argmin(M->y(), (int)B, M->K, dpick, dev_x, M->has_domain ? M->dom : nullptr, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(host_variant, dpick, sizeof(uint32_t) * B, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(tmp);

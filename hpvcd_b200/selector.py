@@ -124,15 +124,32 @@ class Mlp:
                                       out.ctypes.data_as(C.POINTER(C.c_uint32))), "hpvcd_mlp_pick")
         return out
 
+    def set_domain(self, lo: np.ndarray | None, hi: np.ndarray | None) -> None:
+        """Feature range the network was trained on; batches outside it keep
+        the default schedule (HPVCD_MLP_NO_PICK)."""
+        self.domain = None if lo is None else (np.asarray(lo, np.float32), np.asarray(hi, np.float32))
+        if lo is None:
+            _check(self._L.hpvcd_mlp_set_domain(self._h, None, None), "hpvcd_mlp_set_domain")
+        else:
+            lo_, hi_ = (np.ascontiguousarray(a, np.float32) for a in self.domain)
+            _check(self._L.hpvcd_mlp_set_domain(self._h, lo_.ctypes.data_as(C.c_void_p),
+                                                hi_.ctypes.data_as(C.c_void_p)), "hpvcd_mlp_set_domain")
+
     def save(self, path: str = WEIGHTS_PATH) -> None:
+        extra = {}
+        if getattr(self, "domain", None) is not None:
+            extra = {"domain_lo": self.domain[0], "domain_hi": self.domain[1]}
         np.savez(path, params=self.params(master=True), n_variants=self.K,
-                 schedules=np.array([[s.idct, s.luma_team, s.recon_ctas_per_sm] for s in SCHEDULES], np.int32))
+                 schedules=np.array([[s.idct, s.luma_team, s.recon_ctas_per_sm] for s in SCHEDULES], np.int32),
+                 **extra)
 
     @classmethod
     def load(cls, path: str = WEIGHTS_PATH, device: int = 0) -> "Mlp":
         z = np.load(path)
         m = cls(int(z["n_variants"]), device=device)
         m.set_params(z["params"])
+        if "domain_lo" in z:
+            m.set_domain(z["domain_lo"], z["domain_hi"])
         return m
 
     def close(self):
@@ -369,13 +386,30 @@ def collect_batches(n_batches: int, seed: int = 0, out_path: str | None = None, 
 # Training and evaluation
 # ---------------------------------------------------------------------------
 
+def feature_domain(x: np.ndarray, margin: float = 0.05):
+    """Per-feature [lo, hi] of the training rows, widened by `margin` of the
+    range (at least 0.01)."""
+    lo, hi = x.min(axis=0), x.max(axis=0)
+    pad = np.maximum((hi - lo) * margin, 0.01)
+    return (lo - pad).astype(np.float32), (hi + pad).astype(np.float32)
+
+
 def train_network(x: np.ndarray, ms: np.ndarray, epochs: int = 200, batch: int = 256, lr: float = 2e-3,
                   seed: int = 1) -> Mlp:
     """Train the selector network on the GPU (hpvcd_mlp_train) on features
-    and autotuner timings."""
+    and autotuner timings; its domain is the training rows' feature range."""
     m = Mlp(K, seed=seed)
     m.train(x, targets(ms), epochs=epochs, batch=batch, lr=lr, seed=seed + 1)
+    m.set_domain(*feature_domain(x))
     return m
+
+
+def score_with_fallback(picks: np.ndarray, ms: np.ndarray) -> dict:
+    """score() where a pick outside the domain (MLP_NO_PICK) runs the default."""
+    p = np.where(np.asarray(picks) == abi.MLP_NO_PICK, DEFAULT, np.asarray(picks)).astype(np.int64)
+    r = score(p, ms)
+    r["outside_domain"] = int(np.sum(np.asarray(picks) == abi.MLP_NO_PICK))
+    return r
 
 
 def evaluate_live(mlp: Mlp, n_frames: int, seed: int = 12345, reps: int = 2, log=None) -> dict:
@@ -415,7 +449,7 @@ def evaluate_live(mlp: Mlp, n_frames: int, seed: int = 12345, reps: int = 2, log
         if log and (i + 1) % 20 == 0:
             log(f"[selector] evaluated {i + 1}/{n_frames}")
     ms = np.array(times)
-    r = score(np.array(picks), ms)
+    r = score_with_fallback(np.array(picks), ms)
     r["choose_ms_mean"] = float(np.mean(choose_ms))
     r["seed"] = seed
     return r
@@ -463,12 +497,21 @@ def _main(argv=None):
         ms = np.concatenate(ts)
         keep = np.all(ms > 0, axis=1)
         x, ms = x[keep], ms[keep]
+        perm = np.random.default_rng(2024).permutation(len(x))  # frames and batches in both splits
+        x, ms = x[perm], ms[perm]
         split = int(round(len(x) * (1 - a.holdout)))
         m = train_network(x[:split], ms[:split], epochs=a.epochs)
         picks = m.pick(x[split:])
         fixed = best_fixed(ms[:split])
-        res = {"train_rows": split, "heldout_rows": len(x) - split, "heldout": score(picks, ms[split:]),
-               "best_fixed": fixed, "best_fixed_heldout": score(np.full(len(ms) - split, fixed), ms[split:])}
+        hx, hms = x[split:], ms[split:]
+        is_batch = hx[:, 1] > np.log2(3.0) / 8  # more than one picture
+        res = {"train_rows": split, "heldout_rows": len(x) - split,
+               "heldout": score_with_fallback(picks, hms),
+               "heldout_frames": score_with_fallback(picks[~is_batch], hms[~is_batch]),
+               "heldout_batches": score_with_fallback(picks[is_batch], hms[is_batch]) if is_batch.any() else None,
+               "best_fixed": fixed, "best_fixed_heldout": score(np.full(len(hms), fixed), hms),
+               "best_fixed_heldout_batches": (score(np.full(int(is_batch.sum()), fixed), hms[is_batch])
+                                              if is_batch.any() else None)}
         print(json.dumps(res, indent=1))
         m.save(a.out)
         if a.merged:

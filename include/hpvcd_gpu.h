@@ -361,6 +361,7 @@ hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched);
 #define HPVCD_FEATURES 16      /* per-batch statistics the selector reads      */
 #define HPVCD_MLP_HIDDEN 64    /* 16 -> 64 -> 64 -> K                          */
 #define HPVCD_MLP_MAX_VARIANTS 32
+#define HPVCD_MLP_NO_PICK 0xffffffffu /* features outside the network's domain */
 
 /* Features of pictures [first, first + count) of a plan, computed on the
  * device from the TB / PU records and written to dev_out (16 floats, device
@@ -397,6 +398,10 @@ uint32_t hpvcd_mlp_variants(const hpvcd_mlp* mlp);
 /* Host copy of the parameters: master != 0 -> fp32 master copy, else the
  * bf16 values the forward pass uses (widened to fp32). */
 hpvcd_status hpvcd_mlp_get_params(hpvcd_mlp* mlp, float* host, int master);
+/* Feature domain (host lo[16], hi[16]; both NULL clears it): rows whose
+ * features leave it are not picked for (HPVCD_MLP_NO_PICK), and
+ * hpvcd_plan_select then runs the first (default) candidate. */
+hpvcd_status hpvcd_mlp_set_domain(hpvcd_mlp* mlp, const float* lo, const float* hi);
 /* Set the master copy (and its bf16 rounding) from host fp32; resets Adam. */
 hpvcd_status hpvcd_mlp_set_params(hpvcd_mlp* mlp, const float* host);
 /* y [B][K] = forward(x [B][16]); device pointers. */
@@ -413,12 +418,14 @@ hpvcd_status hpvcd_mlp_adam_step(hpvcd_mlp* mlp, float lr, void* stream);
 hpvcd_status hpvcd_mlp_train(hpvcd_mlp* mlp, const float* dev_x, const float* dev_t, uint32_t n,
                              uint32_t batch, uint32_t epochs, float lr, uint64_t seed, void* stream,
                              float* final_loss);
-/* argmin forward(x) of B feature rows (device) into host_variant[B]. */
+/* argmin forward(x) of B feature rows (device) into host_variant[B]
+ * (HPVCD_MLP_NO_PICK for rows outside the domain, when one is set). */
 hpvcd_status hpvcd_mlp_pick(hpvcd_mlp* mlp, const float* dev_x, uint32_t B, void* stream,
                             uint32_t* host_variant);
 /* Choose the plan's schedule among n candidates: the network's pick from
- * the plan's features when mlp has n outputs, else exhaustive autotuning
- * (the fallback).  *chosen = the candidate index. */
+ * the plan's features when mlp has n outputs (candidate 0 when the features
+ * leave the network's domain: *chosen = HPVCD_MLP_NO_PICK), else exhaustive
+ * autotuning (the fallback).  *chosen = the candidate index. */
 hpvcd_status hpvcd_plan_select(hpvcd_plan* plan, hpvcd_mlp* mlp, const hpvcd_sched* cands,
                                uint32_t n, void* stream, uint32_t* chosen);
 
@@ -519,7 +526,8 @@ hpvcd_status hpvcd_server_destroy(hpvcd_server* srv);
  * network must outlive the server (or be removed first). */
 hpvcd_status hpvcd_server_set_selector(hpvcd_server* srv, struct hpvcd_mlp* mlp, const hpvcd_sched* cands,
                                        uint32_t n);
-/* How often each candidate was picked since the selector was set. */
+/* How often each candidate was picked since the selector was set;
+ * counts[K] (n > K) = batches outside the network's domain. */
 hpvcd_status hpvcd_server_selector_picks(hpvcd_server* srv, uint64_t* counts, uint32_t n);
 
 /* ------------------------------------------------------------------------ */

@@ -174,7 +174,11 @@ def test_trained_selector_gains_on_heldout_frames_cpu():
     w = np.load(selector.WEIGHTS_PATH)
     K = int(w["n_variants"])
     y, _, _ = mlp_ref.forward(mlp_ref.bf16_round(w["params"]), x[split:], K)
-    s = selector.score(y.argmin(axis=1), ms[split:])
+    picks = y.argmin(axis=1)
+    if "domain_lo" in w:  # rows outside the training range keep the default schedule
+        inside = np.all((x[split:] >= w["domain_lo"]) & (x[split:] <= w["domain_hi"]), axis=1)
+        picks = np.where(inside, picks, abi.MLP_NO_PICK)
+    s = selector.score_with_fallback(picks, ms[split:])
     fixed = selector.best_fixed(ms[:split])
     s_fixed = selector.score(np.full(len(ms) - split, fixed), ms[split:])
     assert s["gain_vs_default"] > 0.03
@@ -330,7 +334,7 @@ def test_trained_selector_gains_over_no_network():
     x, ms, split = z["features"], z["ms"].astype(np.float64), int(z["train_rows"])
     m = selector.Mlp.load()
     picks = m.pick(x[split:])
-    s = selector.score(picks, ms[split:])
+    s = selector.score_with_fallback(picks, ms[split:])
     fixed = selector.best_fixed(ms[:split])
     s_fixed = selector.score(np.full(len(ms) - split, fixed), ms[split:])
     assert s["gain_vs_default"] > 0.03
@@ -338,7 +342,8 @@ def test_trained_selector_gains_over_no_network():
     assert s["regret_vs_exhaustive"] < 0.01
     # the device picks are the oracle's argmin on the same bf16 weights
     y, _, _ = mlp_ref.forward(m.params(), x[split:], selector.K)
-    assert np.mean(y.argmin(axis=1) == picks) > 0.99
+    inside = picks != abi.MLP_NO_PICK
+    assert np.mean(y.argmin(axis=1)[inside] == picks[inside]) > 0.99
     m.close()
 
 
@@ -372,4 +377,22 @@ def test_server_with_selector_keeps_pixels():
         out, keep = synth.grid_output(synth.Grid(w, h, 512, s, places))
         _, ref = O.decode_batch(pics, out, want_planes=False)
         assert np.array_equal(got[k]["image"], ref), k
+    m.close()
+
+
+@pytest.mark.gpu
+def test_domain_guard_falls_back_to_default():
+    _gpu()
+    m = selector.Mlp(selector.K, seed=4)
+    x = np.random.default_rng(8).random((6, 16)).astype(np.float32)
+    lo = np.zeros(16, np.float32)
+    hi = np.ones(16, np.float32)
+    m.set_domain(lo, hi)
+    x[2, 5] = 1.5   # outside
+    x[4, 0] = -0.2  # outside
+    picks = m.pick(x)
+    assert picks[2] == abi.MLP_NO_PICK and picks[4] == abi.MLP_NO_PICK
+    assert all(p < selector.K for i, p in enumerate(picks) if i not in (2, 4))
+    m.set_domain(None, None)
+    assert np.all(m.pick(x) < selector.K)
     m.close()
