@@ -236,88 +236,89 @@ __global__ void k_sao(const DevPic* __restrict__ pics) {
     if (c > 0 && P.idc == 0) return;
     const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
     const int qw = pw >> 2;
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= qw * ph) return;
-    const int x0 = (id % qw) * 4, y = id / qw;
-    const void* src = P.rec[c];
-    void* dst = P.fin[c];
-    const int bps = P.bps;
-    const size_t row = (size_t)y * pw;
-    int s[4];
-    load4(src, bps, row + x0, s);
-    int out[4] = {s[0], s[1], s[2], s[3]};
-    const bool on = c == 0 ? (P.flags & HPVCD_PIC_SAO_LUMA) != 0 : (P.flags & HPVCD_PIC_SAO_CHROMA) != 0;
-    const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
-    if (on && P.sao) {
-        const int rx = (x0 * sw) >> P.log2_ctb, ry = (y * sh) >> P.log2_ctb;
-        const hpvcd_sao_comp sc = P.sao[(size_t)ry * P.ctb_cols + rx].comp[c];
-        const int bd = c ? P.bd_c : P.bd;
-        const int mx = (1 << bd) - 1;
-        if (sc.type_idx == 1) {  // sao.rs:205-233
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const uint8_t rel = (uint8_t)((uint8_t)(s[i] >> (bd - 5)) - sc.band_pos);
-                if (rel < 4) out[i] = clamp3i(s[i] + sc.offsets[rel], 0, mx);
-            }
-        } else if (sc.type_idx == 2) {  // sao.rs:266-330
-            int dx, dy;
-            switch (sc.eo_class) {
-                case 0: dx = 1; dy = 0; break;
-                case 1: dx = 0; dy = 1; break;
-                case 2: dx = 1; dy = 1; break;
-                default: dx = 1; dy = -1; break;
-            }
-            // window w[r][i] = sample (x0 - 1 + i, y - 1 + r), i = 0..5
-            int w[3][6];
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                const int yy = y - 1 + r;
-                const bool in_row = yy >= 0 && yy < ph;
-                if (r == 1) {
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) w[1][i + 1] = s[i];
-                } else if (in_row) {
-                    int t[4];
-                    load4(src, bps, (size_t)yy * pw + x0, t);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) w[r][i + 1] = t[i];
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) w[r][i + 1] = 0;
+    // grid-stride over the quads of this picture and component
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < qw * ph; id += gridDim.x * blockDim.x) {
+        const int x0 = (id % qw) * 4, y = id / qw;
+        const void* src = P.rec[c];
+        void* dst = P.fin[c];
+        const int bps = P.bps;
+        const size_t row = (size_t)y * pw;
+        int s[4];
+        load4(src, bps, row + x0, s);
+        int out[4] = {s[0], s[1], s[2], s[3]};
+        const bool on = c == 0 ? (P.flags & HPVCD_PIC_SAO_LUMA) != 0 : (P.flags & HPVCD_PIC_SAO_CHROMA) != 0;
+        const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
+        if (on && P.sao) {
+            const int rx = (x0 * sw) >> P.log2_ctb, ry = (y * sh) >> P.log2_ctb;
+            const hpvcd_sao_comp sc = P.sao[(size_t)ry * P.ctb_cols + rx].comp[c];
+            const int bd = c ? P.bd_c : P.bd;
+            const int mx = (1 << bd) - 1;
+            if (sc.type_idx == 1) {  // sao.rs:205-233
+    #pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const uint8_t rel = (uint8_t)((uint8_t)(s[i] >> (bd - 5)) - sc.band_pos);
+                    if (rel < 4) out[i] = clamp3i(s[i] + sc.offsets[rel], 0, mx);
                 }
-                w[r][0] = in_row && x0 > 0 ? load_sample(src, bps, (size_t)yy * pw + x0 - 1) : 0;
-                w[r][5] = in_row && x0 + 4 < pw ? load_sample(src, bps, (size_t)yy * pw + x0 + 4) : 0;
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int x = x0 + i;
-                const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
-                if (x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph) {
-                    // (x + dx, y + dy) and (x - dx, y - dy) with constant window indexes
-                    int n1, n2;
-                    switch (sc.eo_class) {
-                        case 0: n1 = w[1][i + 2]; n2 = w[1][i]; break;
-                        case 1: n1 = w[2][i + 1]; n2 = w[0][i + 1]; break;
-                        case 2: n1 = w[2][i + 2]; n2 = w[0][i]; break;
-                        default: n1 = w[0][i + 2]; n2 = w[2][i]; break;
+            } else if (sc.type_idx == 2) {  // sao.rs:266-330
+                int dx, dy;
+                switch (sc.eo_class) {
+                    case 0: dx = 1; dy = 0; break;
+                    case 1: dx = 0; dy = 1; break;
+                    case 2: dx = 1; dy = 1; break;
+                    default: dx = 1; dy = -1; break;
+                }
+                // window w[r][i] = sample (x0 - 1 + i, y - 1 + r), i = 0..5
+                int w[3][6];
+    #pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const int yy = y - 1 + r;
+                    const bool in_row = yy >= 0 && yy < ph;
+                    if (r == 1) {
+    #pragma unroll
+                        for (int i = 0; i < 4; ++i) w[1][i + 1] = s[i];
+                    } else if (in_row) {
+                        int t[4];
+                        load4(src, bps, (size_t)yy * pw + x0, t);
+    #pragma unroll
+                        for (int i = 0; i < 4; ++i) w[r][i + 1] = t[i];
+                    } else {
+    #pragma unroll
+                        for (int i = 0; i < 4; ++i) w[r][i + 1] = 0;
                     }
-                    const int e = ((s[i] > n1) - (s[i] < n1)) + ((s[i] > n2) - (s[i] < n2)) + 2;
-                    int o = 0;
-                    if (e == 0) o = sc.offsets[0];
-                    else if (e == 1) o = sc.offsets[1];
-                    else if (e == 3) o = sc.offsets[2];
-                    else if (e == 4) o = sc.offsets[3];
-                    if (o) out[i] = clamp3i(s[i] + o, 0, mx);
+                    w[r][0] = in_row && x0 > 0 ? load_sample(src, bps, (size_t)yy * pw + x0 - 1) : 0;
+                    w[r][5] = in_row && x0 + 4 < pw ? load_sample(src, bps, (size_t)yy * pw + x0 + 4) : 0;
+                }
+    #pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int x = x0 + i;
+                    const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
+                    if (x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph) {
+                        // (x + dx, y + dy) and (x - dx, y - dy) with constant window indexes
+                        int n1, n2;
+                        switch (sc.eo_class) {
+                            case 0: n1 = w[1][i + 2]; n2 = w[1][i]; break;
+                            case 1: n1 = w[2][i + 1]; n2 = w[0][i + 1]; break;
+                            case 2: n1 = w[2][i + 2]; n2 = w[0][i]; break;
+                            default: n1 = w[0][i + 2]; n2 = w[2][i]; break;
+                        }
+                        const int e = ((s[i] > n1) - (s[i] < n1)) + ((s[i] > n2) - (s[i] < n2)) + 2;
+                        int o = 0;
+                        if (e == 0) o = sc.offsets[0];
+                        else if (e == 1) o = sc.offsets[1];
+                        else if (e == 3) o = sc.offsets[2];
+                        else if (e == 4) o = sc.offsets[3];
+                        if (o) out[i] = clamp3i(s[i] + o, 0, mx);
+                    }
                 }
             }
+            if (P.cells) {  // exempt cells keep the deblocked samples
+    #pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (exempt_at(P, (x0 + i) * sw, y * sh)) out[i] = s[i];
+            }
         }
-        if (P.cells) {  // exempt cells keep the deblocked samples
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                if (exempt_at(P, (x0 + i) * sw, y * sh)) out[i] = s[i];
-        }
+        store4(dst, bps, row + x0, out);
     }
-    store4(dst, bps, row + x0, out);
 }
 
 // Q13 YCbCr -> RGB8 onto the canvas, four pixels per thread.  blockIdx.y =
@@ -391,43 +392,44 @@ __global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out
     const int copy_w = min(P.crop_w, max(P.canvas_w - P.dst_x, 0));
     const int copy_h = min(P.crop_h, max(P.canvas_h - P.dst_y, 0));
     const int qw = (copy_w + 3) >> 2;
-    const int id = blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= qw * copy_h) return;
-    const int x0 = (id % qw) * 4, yy = id / qw;
-    const int cnt = min(4, copy_w - x0);
     const RgbCoef k = rgb_coef(P);
-    // crop_w <= width (a multiple of 8) and copy_h <= height: x0 .. x0 + 3
-    // and yy are inside the planes
-    int luma[4], cb[4] = {0, 0, 0, 0}, cr[4] = {0, 0, 0, 0};
-    load4(P.fin[0], P.bps, (size_t)yy * P.w + x0, luma);
-    if (P.idc) {
-        const int crow = yy / P.sub_h;
-        if (P.sub_w == 2) {
-            const size_t ci = (size_t)crow * P.cw + (x0 >> 1);  // two chroma samples
-            int t = load_sample(P.fin[1], P.bps, ci), u = load_sample(P.fin[1], P.bps, ci + 1);
-            cb[0] = cb[1] = t; cb[2] = cb[3] = u;
-            t = load_sample(P.fin[2], P.bps, ci);
-            u = load_sample(P.fin[2], P.bps, ci + 1);
-            cr[0] = cr[1] = t; cr[2] = cr[3] = u;
-        } else {
-            load4(P.fin[1], P.bps, (size_t)crow * P.cw + x0, cb);
-            load4(P.fin[2], P.bps, (size_t)crow * P.cw + x0, cr);
+    // grid-stride over the quads of this picture
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < qw * copy_h; id += gridDim.x * blockDim.x) {
+        const int x0 = (id % qw) * 4, yy = id / qw;
+        const int cnt = min(4, copy_w - x0);
+        // crop_w <= width (a multiple of 8) and copy_h <= height: x0 .. x0 + 3
+        // and yy are inside the planes
+        int luma[4], cb[4] = {0, 0, 0, 0}, cr[4] = {0, 0, 0, 0};
+        load4(P.fin[0], P.bps, (size_t)yy * P.w + x0, luma);
+        if (P.idc) {
+            const int crow = yy / P.sub_h;
+            if (P.sub_w == 2) {
+                const size_t ci = (size_t)crow * P.cw + (x0 >> 1);  // two chroma samples
+                int t = load_sample(P.fin[1], P.bps, ci), u = load_sample(P.fin[1], P.bps, ci + 1);
+                cb[0] = cb[1] = t; cb[2] = cb[3] = u;
+                t = load_sample(P.fin[2], P.bps, ci);
+                u = load_sample(P.fin[2], P.bps, ci + 1);
+                cr[0] = cr[1] = t; cr[2] = cr[3] = u;
+            } else {
+                load4(P.fin[1], P.bps, (size_t)crow * P.cw + x0, cb);
+                load4(P.fin[2], P.bps, (size_t)crow * P.cw + x0, cr);
+            }
         }
-    }
-    uint32_t px[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) px[i] = rgb_px(k, P.idc, luma[i], cb[i], cr[i]);
-    uint8_t* o = canvas + ((size_t)(P.dst_y + yy) * P.canvas_w + P.dst_x + x0) * 3;
-    if (cnt == 4 && ((uintptr_t)o & 3) == 0) {
-        uint32_t* o32 = (uint32_t*)o;
-        o32[0] = px[0] | (px[1] << 24);
-        o32[1] = (px[1] >> 8) | (px[2] << 16);
-        o32[2] = (px[2] >> 16) | (px[3] << 8);
-    } else {
-        for (int i = 0; i < cnt; ++i) {
-            o[3 * i] = (uint8_t)px[i];
-            o[3 * i + 1] = (uint8_t)(px[i] >> 8);
-            o[3 * i + 2] = (uint8_t)(px[i] >> 16);
+        uint32_t px[4];
+    #pragma unroll
+        for (int i = 0; i < 4; ++i) px[i] = rgb_px(k, P.idc, luma[i], cb[i], cr[i]);
+        uint8_t* o = canvas + ((size_t)(P.dst_y + yy) * P.canvas_w + P.dst_x + x0) * 3;
+        if (cnt == 4 && ((uintptr_t)o & 3) == 0) {
+            uint32_t* o32 = (uint32_t*)o;
+            o32[0] = px[0] | (px[1] << 24);
+            o32[1] = (px[1] >> 8) | (px[2] << 16);
+            o32[2] = (px[2] >> 16) | (px[3] << 8);
+        } else {
+            for (int i = 0; i < cnt; ++i) {
+                o[3 * i] = (uint8_t)px[i];
+                o[3 * i + 1] = (uint8_t)(px[i] >> 8);
+                o[3 * i + 2] = (uint8_t)(px[i] >> 16);
+            }
         }
     }
 }
@@ -444,12 +446,22 @@ extern "C" cudaError_t hpvcd_launch_deblock(const hpvcd::DevPic* pics, int n_pic
     return cudaGetLastError();
 }
 
+// Blocks per grid-stride filter launch: 16 per SM of a B200 (148 SMs), split
+// over the (picture, component) slices, so a batch of many small pictures
+// is not thousands of tiny blocks.
+static int filter_blocks_x(int quads, int slices, int threads) {
+    const int target = 148 * 16;
+    const int need = (quads + threads - 1) / threads;
+    const int share = (target + slices - 1) / slices;
+    return need < share ? (need > 0 ? need : 1) : (share > 0 ? share : 1);
+}
+
 extern "C" cudaError_t hpvcd_launch_sao(const hpvcd::DevPic* pics, int n_pics, int max_samples,
                                         cudaStream_t stream) {
     if (n_pics <= 0 || max_samples <= 0) return cudaSuccess;
     const int threads = 256;
     const int quads = (max_samples + 3) / 4;
-    dim3 grid((quads + threads - 1) / threads, n_pics, 3);
+    dim3 grid(filter_blocks_x(quads, n_pics * 3, threads), n_pics, 3);
     hpvcd::k_sao<<<grid, threads, 0, stream>>>(pics);
     hpvcd_note_launches(1);
     return cudaGetLastError();
@@ -459,7 +471,7 @@ extern "C" cudaError_t hpvcd_launch_rgb(const hpvcd::DevPic* pics, int n_pics, i
                                         cudaStream_t stream) {
     if (n_pics <= 0 || max_quads <= 0) return cudaSuccess;
     const int threads = 256;
-    dim3 grid((max_quads + threads - 1) / threads, n_pics, 1);
+    dim3 grid(filter_blocks_x(max_quads, n_pics, threads), n_pics, 1);
     hpvcd::k_rgb<<<grid, threads, 0, stream>>>(pics, out);
     hpvcd_note_launches(1);
     return cudaGetLastError();
