@@ -48,9 +48,9 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["grid", "serving", "selector"], default="grid",
+    ap.add_argument("--workload", choices=["grid", "serving", "selector", "inter"], default="grid",
                     help="grid: the 4032x3024 still (default); serving: mixed-size batched serving; "
-                         "selector: learned schedule selection on 3840x2160 frames")
+                         "selector: learned schedule selection on 3840x2160 frames; inter: 1080p GOP")
     ap.add_argument("--frames", type=int, default=60, help="selector: fresh frames to evaluate")
     ap.add_argument("--images", type=int, default=64, help="serving: number of images")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: Poisson arrivals per second")
@@ -461,6 +461,63 @@ def run_selector(args):
     return 0
 
 
+def run_inter(args):
+    """Inter video: a 32-frame 1920x1080 8-bit 4:2:0 sequence in decode order
+    (an intra frame, then frames predicting from up to 4 earlier frames held
+    on the device: 40 % bi-predicted PUs, MVs N(0, 16 px) within the picture
+    plus 80 px, one frame in ten with explicit weighted prediction), all of it
+    one plan: motion compensation, residuals, intra CUs, deblocking and SAO
+    on the GPU; decoded frames stay in HBM as references."""
+    import torch
+
+    from hpvcd_b200 import abi, synth
+    from hpvcd_b200.gpu import DevicePlan
+
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n_frames, w, h = 32, 1920, 1080
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(1000 + rank, w, h, bit_depth=8, chroma_idc=1))
+    for i in range(1, n_frames):
+        s.add(synth.inter_cfg(1000 + 97 * rank + i, w, h, bit_depth=8, weighted=(i % 10 == 5), n_refs=4))
+    pics = s.pictures()
+    plan = DevicePlan(pics, device=local)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(max(3, args.warmup)):
+        plan.launch(abi.STAGE_ALL, stream)
+    torch.cuda.synchronize(dev)
+    if plan.status(stream) != abi.OK:
+        raise abi.HpvcdError(plan.status(stream), "device status")
+    K = max(1, min(args.steps, 50))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    clocks = Clocks(local)
+    for k in range(K):
+        flush.zero_()
+        ev[k][0].record(stream)
+        plan.launch(abi.STAGE_ALL, stream)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    clock_rec = clocks.stop()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    from hpvcd_b200 import replicas
+    total = replicas.max_over_ranks(sum(ms), dev)
+    mpix = n_frames * w * h / 1e6
+    line = {"metric": "decoded MPix/s (inter video)", "value": round(replicas.whole_job_rate(mpix * K, total / 1e3, dev), 2),
+            "unit": "MPix/s", "n_gpus": world, "steps": K, "ms_per_step": round(total / K, 4),
+            "fps": round(n_frames * K / (total / 1e3), 1), "higher_is_better": True, "scaling": "weak",
+            "data": "synthetic", "dtype": "int32",
+            "config": {"workload": "inter_1080p_gop32", "frames": n_frames, "size": f"{w}x{h}", "bit_depth": 8,
+                       "chroma": "4:2:0", "refs": 4, "bi_pu": "40%", "weighted_frames": "10%",
+                       "l2": "flushed between steps"},
+            "launches_per_step": plan.launches_per_run, "clocks": clock_rec}
+    plan.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def _single_output(im):
     import ctypes as C
 
@@ -526,6 +583,8 @@ def main():
         return run_serving(args)
     if args.workload == "selector":
         return run_selector(args)
+    if args.workload == "inter":
+        return run_inter(args)
     return run_ours(args)
 
 

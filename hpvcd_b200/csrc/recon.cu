@@ -173,6 +173,43 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         return;
     }
     const int nx = (t.nx == 0 || t.nx > n) ? n : t.nx;
+    if (n == 4) {
+        // 4x4 in registers: lane l < 16 holds coefficient (l / 4, l % 4); both
+        // stages gather their four inputs by shuffles.  The same integer sums
+        // as the shared-memory path, clipped after the complete sum.
+        const bool dst = luma && (t.flags & HPVCD_TU_INTRA);
+        const int l = lane & 15, r = l >> 2, c = l & 3;
+        int d = 0;
+        if (lane < 16 && c < nx) {
+            const long long v = ((long long)lv[l] * factor + add) >> bd_shift;
+            d = (int)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v));
+        }
+        // basis entry T[k][m] of the 4-point DCT (rows 64 / 83,36 / 64 / 36,83
+        // with the H.265 signs) or of the DST
+        auto basis = [dst](int k, int m) -> int {
+            if (dst) return c_dst4[k][m];
+            switch (k) {  // dct_c(4, k, m) without a lookup table
+                case 0: return 64;
+                case 1: return m == 0 ? 83 : (m == 1 ? 36 : (m == 2 ? -36 : -83));
+                case 2: return (m == 0 || m == 3) ? 64 : -64;
+                default: return m == 0 ? 36 : (m == 1 ? -83 : (m == 2 ? 83 : -36));
+            }
+        };
+        // stage 1: tmp[r][c] = clip((sum_k T[k][r] d[k][c] + 64) >> 7)
+        int acc = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc += basis(k, r) * __shfl_sync(0xffffffffu, d, k * 4 + c);
+        const int tmp = clamp3i((acc + 64) >> 7, -32768, 32767);
+        // stage 2: out[r][c] = (sum_k T[k][c] tmp[r][k] + add2) >> shift2
+        const int shift2 = 20 - bd;
+        int acc2 = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc2 += basis(k, c) * __shfl_sync(0xffffffffu, tmp, r * 4 + k);
+        const int v = (acc2 + (1 << (shift2 - 1))) >> shift2;
+        if (lane < 16) emit(r, c, i16s ? (int)(int16_t)v : v);
+        __syncwarp();
+        return;
+    }
     // dequantise into buf; columns >= nx are zero (transform.rs:510-511);
     // track the last non-zero row so stage 1 skips all-zero rows.
     int my_rows = 0;
@@ -885,46 +922,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 }
             }
         }
-        // ---- wait for the neighbours (bounded) and load their edges ----
-        if (tid == 0) {
-            const int cx = it.cx, cy = it.cy;
-            const int nb[4][2] = {{cx - 1, cy}, {cx - 1, cy - 1}, {cx, cy - 1}, {cx + 1, cy - 1}};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int nx = nb[q][0], ny = nb[q][1];
-                if (nx < 0 || ny < 0 || nx >= P.ctb_cols) continue;
-                const uint32_t* f = P.ready + (size_t)ny * P.ctb_cols + nx;
-                uint32_t spins = 0;
-                while (ld_acquire(f) == 0u) {
-                    if (++spins > spin_limit) {
-                        atomicOr(dev_err, DEV_ERR_TIMEOUT);
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-            }
-        }
-        __syncthreads();
-        for (int c = 0; c < ncomp; ++c) {
-            const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
-            const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
-            uint16_t* can = can_of(c);
-            const int CW = ReconLayout::cw_of(S);
-            for (int i = tid; i < 3 * S + 1; i += kReconThreads) {
-                if (i < 2 * S + 1) {  // row above: x = i - 1
-                    const int ax = ox + i - 1, ay = oy - 1;
-                    int v = 0;
-                    if (ay >= 0 && ax >= 0 && ax < pw) v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * pw + ax);
-                    can[i + 7] = (uint16_t)v;
-                } else {  // column left: y = i - (2S + 1)
-                    const int y = i - (2 * S + 1);
-                    const int ax = ox - 1, ay = oy + y;
-                    int v = 0;
-                    if (ax >= 0 && ay < ph) v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * pw + ax);
-                    can[(y + 1) * CW + 7] = (uint16_t)v;
-                }
-            }
-        }
+        // the CTU's own records and residuals have arrived: the decode-order
+        // build below runs before the neighbour wait, off the critical path
         cp_async_wait_all();
         __syncthreads();
         // ---- decode order, in parallel: every luma record stamps the 4x4
@@ -983,6 +982,46 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 cnt = kListCap;
             }
             if (lane == 0) counts[c] = cnt;
+        }
+        // ---- wait for the neighbours (bounded), then load their edges ----
+        if (tid == 0) {
+            const int cx = it.cx, cy = it.cy;
+            const int nb[4][2] = {{cx - 1, cy}, {cx - 1, cy - 1}, {cx, cy - 1}, {cx + 1, cy - 1}};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int nx = nb[q][0], ny = nb[q][1];
+                if (nx < 0 || ny < 0 || nx >= P.ctb_cols) continue;
+                const uint32_t* f = P.ready + (size_t)ny * P.ctb_cols + nx;
+                uint32_t spins = 0;
+                while (ld_acquire(f) == 0u) {
+                    if (++spins > spin_limit) {
+                        atomicOr(dev_err, DEV_ERR_TIMEOUT);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __syncthreads();
+        for (int c = 0; c < ncomp; ++c) {
+            const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+            const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+            uint16_t* can = can_of(c);
+            const int CW = ReconLayout::cw_of(S);
+            for (int i = tid; i < 3 * S + 1; i += kReconThreads) {
+                if (i < 2 * S + 1) {  // row above: x = i - 1
+                    const int ax = ox + i - 1, ay = oy - 1;
+                    int v = 0;
+                    if (ay >= 0 && ax >= 0 && ax < pw) v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * pw + ax);
+                    can[i + 7] = (uint16_t)v;
+                } else {  // column left: y = i - (2S + 1)
+                    const int y = i - (2 * S + 1);
+                    const int ax = ox - 1, ay = oy + y;
+                    int v = 0;
+                    if (ax >= 0 && ay < ph) v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * pw + ax);
+                    can[(y + 1) * CW + 7] = (uint16_t)v;
+                }
+            }
         }
         __syncthreads();
         // ---- decode-order walk: warp c reconstructs component c ----
