@@ -905,23 +905,6 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         for (uint32_t i = tid; i < nrec; i += kReconThreads) cp_async16(recs + i, P.tus + r0 + i);
         asm volatile("cp.async.commit_group;" ::: "memory");
         for (int i = tid; i < 256; i += kReconThreads) stamp[i] = kNoStamp;
-        // Inter pictures: the plane holds motion-compensated + residual
-        // samples; load the CTU interior so intra TBs can predict from it.
-        if (P.flags & HPVCD_PIC_INTER) {
-            for (int c = 0; c < ncomp; ++c) {
-                const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
-                const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
-                uint16_t* can = can_of(c);
-                const int CW = ReconLayout::cw_of(S);
-                for (int i = tid; i < S * S; i += kReconThreads) {
-                    const int y = i / S, x = i % S;
-                    const int ax = ox + x, ay = oy + y;
-                    int v = 0;
-                    if (ax < pw && ay < ph) v = load_sample(P.rec[c], P.bps, (size_t)ay * pw + ax);
-                    can[(y + 1) * CW + x + 8] = (uint16_t)v;
-                }
-            }
-        }
         // the CTU's own records and residuals have arrived: the decode-order
         // build below runs before the neighbour wait, off the critical path
         cp_async_wait_all();
@@ -982,6 +965,32 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 cnt = kListCap;
             }
             if (lane == 0) counts[c] = cnt;
+        }
+        __syncthreads();
+        // A CTU without intra TBs (inter pictures) has its final samples in the
+        // plane already: it neither waits for its neighbours nor rewrites
+        // anything, it only releases its flag for the CTUs that predict from it.
+        const bool any_intra = counts[0] + (ncomp > 1 ? counts[1] + counts[2] : 0u) > 0u;
+        if (!any_intra) {
+            if (tid == 0) st_release(P.ready + ci, 1u);
+            continue;
+        }
+        // Inter pictures: the plane holds motion-compensated + residual
+        // samples; load the CTU interior so intra TBs can predict from it.
+        if (P.flags & HPVCD_PIC_INTER) {
+            for (int c = 0; c < ncomp; ++c) {
+                const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+                const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+                uint16_t* can = can_of(c);
+                const int CW = ReconLayout::cw_of(S);
+                for (int i = tid; i < S * S; i += kReconThreads) {
+                    const int y = i / S, x = i % S;
+                    const int ax = ox + x, ay = oy + y;
+                    int v = 0;
+                    if (ax < pw && ay < ph) v = load_sample(P.rec[c], P.bps, (size_t)ay * pw + ax);
+                    can[(y + 1) * CW + x + 8] = (uint16_t)v;
+                }
+            }
         }
         // ---- wait for the neighbours (bounded), then load their edges ----
         if (tid == 0) {
