@@ -88,7 +88,14 @@ struct Segment {
     uint32_t first_pic, n_pics;
     uint32_t item_off, n_items;
     int max_dbk_v, max_dbk_h, max_sao;
+    int max_rgb;  // RGB quads of the segment's largest picture
 };
+
+// Independent pictures (no inter prediction) of a larger batch run as this
+// many segments, each with its whole pipeline on its own stream, so that the
+// streaming passes of one group overlap the latency-bound wavefront of another.
+constexpr int kMaxGroups = 4;
+constexpr uint32_t kMinPicturesPerGroup = 4;
 
 }  // namespace
 
@@ -126,6 +133,12 @@ struct hpvcd_plan {
     cudaStream_t alloc_stream = nullptr;
     bool pooled = false;
     cudaGraphExec_t graphs[16] = {};  // captured launch sequences by stage mask
+    // concurrent segments (independent pictures): one stream per segment,
+    // forked from and joined back into the launching stream
+    bool concurrent = false;
+    cudaStream_t aux[kMaxGroups] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[kMaxGroups] = {};
 
     uint32_t launches_for(uint32_t stages) const {
         uint32_t L = 0;
@@ -138,8 +151,9 @@ struct hpvcd_plan {
             }
             if (stages & HPVCD_STAGE_DEBLOCK) L += (s.max_dbk_v > 0) + (s.max_dbk_h > 0);
             if ((stages & HPVCD_STAGE_SAO) && s.max_sao > 0) ++L;
+            if (concurrent && (stages & HPVCD_STAGE_OUTPUT) && out.kind == HPVCD_OUT_RGB8 && s.max_rgb > 0) ++L;
         }
-        if ((stages & HPVCD_STAGE_OUTPUT) && out.kind == HPVCD_OUT_RGB8 && max_rgb > 0) ++L;
+        if (!concurrent && (stages & HPVCD_STAGE_OUTPUT) && out.kind == HPVCD_OUT_RGB8 && max_rgb > 0) ++L;
         return L;
     }
 
@@ -158,6 +172,11 @@ struct hpvcd_plan {
     ~hpvcd_plan() {
         for (cudaGraphExec_t& gx : graphs)
             if (gx) cudaGraphExecDestroy(gx);
+        for (int g = 0; g < kMaxGroups; ++g) {
+            if (ev_join[g]) cudaEventDestroy(ev_join[g]);
+            if (aux[g]) cudaStreamDestroy(aux[g]);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
         dfree(d_pics);
         dfree(d_items);
         dfree(d_scratch);
@@ -317,9 +336,29 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     // segments: all pictures at once, or one per picture when any picture
     // predicts from another (its references must be final first).
     if (any_inter) {
-        for (uint32_t i = 0; i < n; ++i) P->segs.push_back(Segment{i, 1, 0, 0, 0, 0, 0});
+        for (uint32_t i = 0; i < n; ++i) P->segs.push_back(Segment{i, 1, 0, 0, 0, 0, 0, 0});
     } else {
-        P->segs.push_back(Segment{0, n, 0, 0, 0, 0, 0});
+        // independent pictures: up to kMaxGroups contiguous groups of about
+        // equal luma area, run concurrently
+        const int groups = (int)std::min<uint32_t>((uint32_t)kMaxGroups, n / kMinPicturesPerGroup);
+        if (groups <= 1) {
+            P->segs.push_back(Segment{0, n, 0, 0, 0, 0, 0, 0});
+        } else {
+            double total = 0;
+            for (uint32_t i = 0; i < n; ++i) total += (double)pics[i].width * pics[i].height;
+            double acc = 0;
+            uint32_t first = 0;
+            for (uint32_t i = 0; i < n; ++i) {
+                acc += (double)pics[i].width * pics[i].height;
+                const int done = (int)P->segs.size();
+                const bool last = i + 1 == n;
+                if (last || (done < groups - 1 && acc >= total * (done + 1) / groups)) {
+                    P->segs.push_back(Segment{first, i + 1 - first, 0, 0, 0, 0, 0, 0});
+                    first = i + 1;
+                }
+            }
+            P->concurrent = P->segs.size() > 1;
+        }
     }
     const size_t n_seg = P->segs.size();
     P->scratch_words = n_seg + 1 + ready_words;
@@ -435,6 +474,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             s.max_dbk_v = std::max(s.max_dbk_v, std::max(lv, cv));
             s.max_dbk_h = std::max(s.max_dbk_h, std::max(lh, ch));
             if (d.rec[0] != d.fin[0]) s.max_sao = std::max(s.max_sao, d.w * d.h);
+            if (P->out.kind == HPVCD_OUT_RGB8) s.max_rgb = std::max(s.max_rgb, (d.crop_w + 3) / 4 * d.crop_h);
         }
     }
     e = P->dmalloc(&P->d_pics, sizeof(DevPic) * n);
@@ -456,6 +496,18 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
     P->sms = sms;
     P->recon_occ = std::max(1, hpvcd_recon_occupancy(P->c444));
+    if (P->concurrent) {
+        cudaError_t ce = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
+        for (size_t g = 0; g < P->segs.size() && ce == cudaSuccess; ++g) {
+            ce = cudaStreamCreateWithFlags(&P->aux[g], cudaStreamNonBlocking);
+            if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&P->ev_join[g], cudaEventDisableTiming);
+        }
+        if (ce != cudaSuccess) {
+            delete P;
+            cudaGetLastError();
+            return cuda_status(ce);
+        }
+    }
     P->launches_per_run = P->launches_for(HPVCD_STAGE_ALL);
     *result = P;
     return HPVCD_OK;
@@ -485,9 +537,16 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             }
         }
     }
+    const cudaStream_t origin = st;
+    if (P->concurrent) {  // fork: every segment's stream starts after the work above
+        e = cudaEventRecord(P->ev_fork, origin);
+        for (uint32_t si = 0; si < n_seg && e == cudaSuccess; ++si) e = cudaStreamWaitEvent(P->aux[si], P->ev_fork, 0);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
     for (uint32_t si = 0; si < n_seg; ++si) {
         const Segment& s = P->segs[si];
         const DevPic* dp = P->d_pics + s.first_pic;
+        if (P->concurrent) st = P->aux[si];
         if (stages & HPVCD_STAGE_RECON) {
             for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
                 if ((P->src[i].flags & HPVCD_PIC_INTER) && P->src[i].n_pus) {
@@ -500,7 +559,9 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             if (e != cudaSuccess) return cuda_status(e);
             int occ = P->recon_occ;
             if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
-            const int grid = std::max(1, std::min<int>(P->sms * occ, (int)s.n_items));
+            // concurrent segments share the SMs: each gets its share of the CTAs
+            const int share = P->concurrent ? std::max(1, P->sms * occ / (int)n_seg) : P->sms * occ;
+            const int grid = std::max(1, std::min<int>(share, (int)s.n_items));
             e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
                                    P->c444, grid, (int)P->sched.luma_team, st);
             if (e != cudaSuccess) return cuda_status(e);
@@ -514,8 +575,18 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             e = hpvcd_launch_sao(dp, (int)s.n_pics, s.max_sao, st);
             if (e != cudaSuccess) return cuda_status(e);
         }
+        if (P->concurrent) {
+            if ((stages & HPVCD_STAGE_OUTPUT) && P->out.kind == HPVCD_OUT_RGB8) {
+                e = hpvcd_launch_rgb(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
+            e = cudaEventRecord(P->ev_join[si], st);  // join back into the launching stream
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(origin, P->ev_join[si], 0);
+            if (e != cudaSuccess) return cuda_status(e);
+        }
     }
-    if ((stages & HPVCD_STAGE_OUTPUT) && P->out.kind == HPVCD_OUT_RGB8) {
+    st = origin;
+    if (!P->concurrent && (stages & HPVCD_STAGE_OUTPUT) && P->out.kind == HPVCD_OUT_RGB8) {
         e = hpvcd_launch_rgb(P->d_pics, (int)P->pics.size(), P->max_rgb, P->d_canvas, st);
         if (e != cudaSuccess) return cuda_status(e);
     }

@@ -402,3 +402,34 @@ def test_schedule_variants_inter_bit_exact():
         assert plan.status() == abi.OK
         assert_planes_equal([plan.planes(i) for i in range(len(pics))], ref, "inter variants")
     plan.close()
+
+
+def test_concurrent_groups_direct_and_graph():
+    """A batch of 20 independent tiles runs as concurrent groups (one stream
+    each, forked from and joined into the launching stream), launched
+    directly and replayed as a CUDA graph: both equal the oracle."""
+    g = synth.make_grid(2560, 2048, seed=17, bit_depth=10)   # 5 x 4 tiles of 512
+    out, keep = synth.grid_output(g)
+    pics = g.synth.pictures()
+    assert len(pics) == 20
+    _, ref = O.decode_batch(pics, out, want_planes=False, threads=8)
+    plan = DevicePlan(pics, out)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        plan.launch(abi.STAGE_ALL, s)
+        s.synchronize()
+        assert plan.status(s) == abi.OK
+        assert np.array_equal(plan.canvas(), ref)
+        before = abi.lib().hpvcd_kernel_launch_count()
+        plan.launch(abi.STAGE_ALL | abi.STAGE_GRAPH, s)
+        plan.launch(abi.STAGE_ALL | abi.STAGE_GRAPH, s)
+        s.synchronize()
+        assert abi.lib().hpvcd_kernel_launch_count() - before == 2 * plan.launches_per_run
+        assert plan.status(s) == abi.OK
+    assert np.array_equal(plan.canvas(), ref)
+    # stages launched one at a time give the same picture
+    for st_ in (abi.STAGE_RECON, abi.STAGE_DEBLOCK, abi.STAGE_SAO, abi.STAGE_OUTPUT):
+        plan.launch(st_)
+    torch.cuda.synchronize()
+    assert np.array_equal(plan.canvas(), ref)
+    plan.close()
