@@ -97,6 +97,37 @@ struct Segment {
 constexpr int kMaxGroups = 4;
 constexpr uint32_t kMinPicturesPerGroup = 4;
 
+// Streams and events of the concurrent groups.  A context slot creates one
+// set and lends it to every plan it builds (no stream churn per batch
+// layout); public plans own theirs.
+struct GroupStreams {
+    cudaStream_t aux[kMaxGroups] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[kMaxGroups] = {};
+    bool ready = false;
+    cudaError_t create() {
+        if (ready) return cudaSuccess;
+        cudaError_t e = cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming);
+        for (int g = 0; g < kMaxGroups && e == cudaSuccess; ++g) {
+            e = cudaStreamCreateWithFlags(&aux[g], cudaStreamNonBlocking);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_join[g], cudaEventDisableTiming);
+        }
+        ready = e == cudaSuccess;
+        return e;
+    }
+    void destroy() {
+        for (int g = 0; g < kMaxGroups; ++g) {
+            if (ev_join[g]) cudaEventDestroy(ev_join[g]);
+            if (aux[g]) cudaStreamDestroy(aux[g]);
+            ev_join[g] = nullptr;
+            aux[g] = nullptr;
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        ev_fork = nullptr;
+        ready = false;
+    }
+};
+
 }  // namespace
 
 struct hpvcd_plan {
@@ -136,9 +167,8 @@ struct hpvcd_plan {
     // concurrent segments (independent pictures): one stream per segment,
     // forked from and joined back into the launching stream
     bool concurrent = false;
-    cudaStream_t aux[kMaxGroups] = {};
-    cudaEvent_t ev_fork = nullptr;
-    cudaEvent_t ev_join[kMaxGroups] = {};
+    GroupStreams own;                  // used when the plan is not lent a set
+    const GroupStreams* gs = nullptr;  // the set the launches use
 
     uint32_t launches_for(uint32_t stages) const {
         uint32_t L = 0;
@@ -172,11 +202,7 @@ struct hpvcd_plan {
     ~hpvcd_plan() {
         for (cudaGraphExec_t& gx : graphs)
             if (gx) cudaGraphExecDestroy(gx);
-        for (int g = 0; g < kMaxGroups; ++g) {
-            if (ev_join[g]) cudaEventDestroy(ev_join[g]);
-            if (aux[g]) cudaStreamDestroy(aux[g]);
-        }
-        if (ev_fork) cudaEventDestroy(ev_fork);
+        own.destroy();
         dfree(d_pics);
         dfree(d_items);
         dfree(d_scratch);
@@ -262,7 +288,8 @@ void fill_inputs(DevPic& d, const hpvcd_picture& p) {
 
 hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out,
                         const hpvcd_sched* sched, const hpvcd_wp_table* host_wp, hpvcd_plan** result,
-                        cudaStream_t pool_stream = nullptr, bool pooled = false) {
+                        cudaStream_t pool_stream = nullptr, bool pooled = false,
+                        GroupStreams* lend = nullptr) {
     if (!pics || n == 0 || !result) return HPVCD_ERR_INVALID_ARG;
     for (uint32_t i = 0; i < n; ++i) {
         const hpvcd_status s = validate(pics[i]);
@@ -497,16 +524,14 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     P->sms = sms;
     P->recon_occ = std::max(1, hpvcd_recon_occupancy(P->c444));
     if (P->concurrent) {
-        cudaError_t ce = cudaEventCreateWithFlags(&P->ev_fork, cudaEventDisableTiming);
-        for (size_t g = 0; g < P->segs.size() && ce == cudaSuccess; ++g) {
-            ce = cudaStreamCreateWithFlags(&P->aux[g], cudaStreamNonBlocking);
-            if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&P->ev_join[g], cudaEventDisableTiming);
-        }
+        GroupStreams* set = lend ? lend : &P->own;
+        const cudaError_t ce = set->create();
         if (ce != cudaSuccess) {
             delete P;
             cudaGetLastError();
             return cuda_status(ce);
         }
+        P->gs = set;
     }
     P->launches_per_run = P->launches_for(HPVCD_STAGE_ALL);
     *result = P;
@@ -539,14 +564,15 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
     }
     const cudaStream_t origin = st;
     if (P->concurrent) {  // fork: every segment's stream starts after the work above
-        e = cudaEventRecord(P->ev_fork, origin);
-        for (uint32_t si = 0; si < n_seg && e == cudaSuccess; ++si) e = cudaStreamWaitEvent(P->aux[si], P->ev_fork, 0);
+        e = cudaEventRecord(P->gs->ev_fork, origin);
+        for (uint32_t si = 0; si < n_seg && e == cudaSuccess; ++si)
+            e = cudaStreamWaitEvent(P->gs->aux[si], P->gs->ev_fork, 0);
         if (e != cudaSuccess) return cuda_status(e);
     }
     for (uint32_t si = 0; si < n_seg; ++si) {
         const Segment& s = P->segs[si];
         const DevPic* dp = P->d_pics + s.first_pic;
-        if (P->concurrent) st = P->aux[si];
+        if (P->concurrent) st = P->gs->aux[si];
         if (stages & HPVCD_STAGE_RECON) {
             for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
                 if ((P->src[i].flags & HPVCD_PIC_INTER) && P->src[i].n_pus) {
@@ -580,8 +606,8 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
                 e = hpvcd_launch_rgb(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st);
                 if (e != cudaSuccess) return cuda_status(e);
             }
-            e = cudaEventRecord(P->ev_join[si], st);  // join back into the launching stream
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(origin, P->ev_join[si], 0);
+            e = cudaEventRecord(P->gs->ev_join[si], st);  // join back into the launching stream
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(origin, P->gs->ev_join[si], 0);
             if (e != cudaSuccess) return cuda_status(e);
         }
     }
@@ -666,6 +692,7 @@ struct Slot {
     void* direct_out = nullptr;  // caller's pinned output buffer of the ticket, if any
     bool busy = false;
     std::vector<hpvcd_wp_table> wp;
+    GroupStreams groups;  // lent to the slot's plans
 };
 
 }  // namespace
@@ -686,6 +713,7 @@ struct hpvcd_gpu {
             if (s.stream) cudaStreamSynchronize(s.stream);
             delete s.plan;
             if (s.stream) cudaStreamSynchronize(s.stream);
+            s.groups.destroy();
             cudaFreeHost(s.h_in);
             cudaFreeHost(s.h_out);
             cudaFree(s.d_in);
@@ -1195,7 +1223,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
             slot->plan_bytes = 0;
         }
         st = plan_build(dev.data(), n, out, nullptr, any_wp ? slot->wp.data() : nullptr, &slot->plan,
-                        slot->stream, true);
+                        slot->stream, true, &slot->groups);
         slot->plan_bytes = st == HPVCD_OK ? plan_bytes : 0;
     }
     g->in_use = g->in_use - held + slot->d_in_cap + slot->plan_bytes;
