@@ -81,7 +81,9 @@ struct hpvcd_server {
     std::thread worker;
 
     uint32_t max_pics() const { return cfg.max_batch_pictures ? cfg.max_batch_pictures : 4096; }
-    uint64_t max_bytes() const { return cfg.max_batch_bytes ? cfg.max_batch_bytes : (512ull << 20); }
+    // 128 MiB of inputs per batch by default: several batches in flight
+    // overlap one batch's host <-> device copies with another's decode
+    uint64_t max_bytes() const { return cfg.max_batch_bytes ? cfg.max_batch_bytes : (128ull << 20); }
 
     // Give `a` at least `need` bytes: the smallest recycled arena that fits,
     // else a new page-locked allocation.  Only called on empty arenas (open
@@ -222,7 +224,7 @@ HPVCD_API hpvcd_status hpvcd_server_create(const hpvcd_server_cfg* cfg, hpvcd_se
     hpvcd_server* s = new (std::nothrow) hpvcd_server();
     if (!s) return HPVCD_ERR_ALLOC;
     s->cfg = *cfg;
-    const uint32_t inflight = cfg->max_inflight ? std::min<uint32_t>(cfg->max_inflight, 16) : 2;
+    const uint32_t inflight = cfg->max_inflight ? std::min<uint32_t>(cfg->max_inflight, 16) : 3;
     hpvcd_gpu_cfg gc{cfg->device, inflight, cfg->hbm_budget};
     const hpvcd_status st = hpvcd_gpu_create(&gc, &s->gpu);
     if (st != HPVCD_OK) {

@@ -80,9 +80,9 @@ def _percentile(v, q):
     return float(np.percentile(np.asarray(v), q)) if len(v) else None
 
 
-def run(imgs, batching: bool, arrival_rate: float | None, seed: int = 1, max_inflight: int = 2,
+def run(imgs, batching: bool, arrival_rate: float | None, seed: int = 1, max_inflight: int = 3,
         device: int = 0, timeout_s: float = 600.0, batch_window_us: int = 2000, warmup: int = 8,
-        zero_copy: bool = False, selector=None) -> dict:
+        zero_copy: bool = False, selector=None, max_batch_bytes: int = 0) -> dict:
     """Submit every image (Poisson arrivals at `arrival_rate`/s, or all at
     once when None) and collect the completions.  Returns throughput and
     latency percentiles."""
@@ -91,6 +91,7 @@ def run(imgs, batching: bool, arrival_rate: float | None, seed: int = 1, max_inf
     lat, qms, batch = [], [], []
     bad = 0
     with Server(device, max_inflight=max_inflight if batching else 1, batching=batching,
+                max_batch_bytes=max_batch_bytes if batching else 0,
                 batch_window_us=batch_window_us if batching else 0) as srv:
         if selector is not None:  # the network picks every batch's schedule
             from .selector import SCHEDULES

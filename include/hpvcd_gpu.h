@@ -476,9 +476,10 @@ typedef struct hpvcd_server hpvcd_server;
 
 typedef struct hpvcd_server_cfg {
     int32_t device;
-    uint32_t max_inflight;       /* batches on the GPU at once, 0 -> 2           */
+    uint32_t max_inflight;       /* batches on the GPU at once, 0 -> 3           */
     uint32_t max_batch_pictures; /* pictures fused into one launch, 0 -> 4096    */
-    uint64_t max_batch_bytes;    /* input + output bytes of one batch, 0 -> 2 GiB */
+    uint64_t max_batch_bytes;    /* bytes of one batch, 0 -> 128 MiB (smaller     */
+                                 /* batches pipeline copies with decoding)      */
     uint64_t hbm_budget;         /* context HBM budget, 0 -> 80% of free memory  */
     uint32_t batching;           /* 1: fuse queued requests; 0: one per launch   */
     uint32_t batch_window_us;    /* a free slot waits until the oldest queued     */
