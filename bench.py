@@ -447,7 +447,7 @@ def device_batched_vs_plain(imgs, local, reps: int = 5):
            "speedup": round(t_plain / t_fused, 3), "status": st,
            "fused_launches_per_run": fused.launches_per_run}
     # the fused batch with the learned schedule (features + network pick on
-    # the device), and exhaustive autotuning as the judge
+    # the device), and exhaustive autotuning as the yardstick
     mlp = _selector_network()
     if mlp is not None:
         from hpvcd_b200 import selector

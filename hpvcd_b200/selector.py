@@ -16,7 +16,7 @@ coefficient density, QP, intra share, size and picture count.
   batch's 16 features (`hpvcd_plan_features`, computed on the device from the
   TB / PU records) and picks the argmin.  It is trained on timings that the
   autotuner measures, and autotuning stays the fallback (no network) and the
-  judge (its timings score the network's picks).
+  yardstick (its timings score the network's picks).
 
 Frames of the selector workload: 3840x2160 10-bit 4:2:0, QP uniform 17-42,
 TB-size area mix Dirichlet(1, 1, 1, 1) over 4/8/16/32, coded-block fraction
