@@ -433,3 +433,63 @@ def test_concurrent_groups_direct_and_graph():
     torch.cuda.synchronize()
     assert np.array_equal(plan.canvas(), ref)
     plan.close()
+
+
+# --- edge cases: empty residuals, no records, minimum and ragged sizes ----
+def test_intra_without_coded_residual(dec):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(110, 512, 256, bit_depth=10)
+    c.cbf_p = 0.0          # prediction only: every TB uncoded
+    s.add(c)
+    run_yuv(dec, s.pictures(), "no coded residual")
+
+
+def test_picture_without_records(dec):
+    import ctypes as C
+    s = synth.SynthSet()
+    c = synth.residual_cfg(111, 256, 128, bit_depth=8)
+    s.add(c)
+    p = s.picture(0)
+    q = abi.Picture()
+    C.pointer(q)[0] = p
+    q.n_tus = 0            # prediction in the plane, nothing to add
+    q.n_coeffs = 0
+    run_yuv(dec, [q], "no records")
+
+
+@pytest.mark.parametrize("w,h,log2_ctb", [(8, 8, 4), (8, 8, 6), (4096, 16, 4), (16, 2048, 5), (1032, 24, 6)])
+def test_minimum_and_ragged_sizes(dec, w, h, log2_ctb):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(112 + w + h, w, h, bit_depth=10, chroma_idc=1)
+    c.log2_ctb = log2_ctb
+    s.add(c)
+    run_yuv(dec, s.pictures(), f"{w}x{h} ctb{1 << log2_ctb}")
+
+
+def test_many_ctus_ctb16(dec):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(113, 1024, 1024, bit_depth=8, chroma_idc=1)
+    c.log2_ctb = 4         # 4096 CTUs, a 191-step wavefront
+    s.add(c)
+    run_yuv(dec, s.pictures(), "ctb16 1024x1024")
+
+
+def test_mixed_edge_batch(dec):
+    import ctypes as C
+    s = synth.SynthSet()
+    for i, (w, h, bd, idc, ctb) in enumerate([(8, 8, 8, 1, 4), (520, 264, 10, 3, 5), (64, 1024, 12, 0, 6),
+                                              (1024, 8, 8, 1, 4), (256, 256, 10, 1, 6)]):
+        c = synth.intra_cfg(120 + i, w, h, bit_depth=bd, chroma_idc=idc)
+        c.log2_ctb = ctb
+        if i == 4:
+            c.cbf_p = 0.0
+        s.add(c)
+    r = synth.residual_cfg(130, 128, 64, bit_depth=8)
+    s.add(r)
+    pics = s.pictures()
+    q = abi.Picture()
+    C.pointer(q)[0] = pics[-1]
+    q.n_tus = 0
+    q.n_coeffs = 0
+    pics[-1] = q
+    run_yuv(dec, pics, "mixed edge batch")
