@@ -52,6 +52,20 @@ PIC_SAO_LUMA = 0x0008
 PIC_SAO_CHROMA = 0x0010
 PIC_PRED_IN_PLANE = 0x0020
 PIC_INTER = 0x0040
+PIC_STORE_MASK = 0x00FF0000
+
+
+def PIC_STORE_DPB(e: int) -> int:
+    """hpvcd_picture.flags bits storing the decoded picture into DPB entry e."""
+    return (e + 1) << 16
+
+
+def REF_DPB(e: int) -> int:
+    """hpvcd_picture.ref_slot value naming DPB entry e."""
+    return -2 - e
+
+
+DPB_MAX_READERS = 64
 
 OUT_YUV, OUT_RGB8 = 0, 1
 MATRIX_IDENTITY, MATRIX_BT709, MATRIX_BT470BG = 0, 1, 5
@@ -286,6 +300,9 @@ def lib() -> C.CDLL:
             "hpvcd_gpu_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
             "hpvcd_server_set_selector": (i32, [vp, vp, C.POINTER(Sched), u32]),
             "hpvcd_server_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
+            "hpvcd_dpb_create": (i32, [i32, u32, C.POINTER(vp)]),
+            "hpvcd_dpb_destroy": (i32, [vp]),
+            "hpvcd_gpu_set_dpb": (i32, [vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

@@ -85,7 +85,9 @@ __global__ void k_mc(const DevPic* __restrict__ pics, int pic_index) {
         const int ri = u.ref_idx[l];
         if (ri < 0 || ri >= HPVCD_MAX_REFS) continue;
         const int rp = P.ref_pic[l][ri];
-        if (rp < 0 || rp >= pic_index) continue;
+        // the host maps references to earlier pictures of the batch (< pic_index)
+        // or to DPB pictures appended after the batch's own; -1 is none
+        if (rp < 0 || rp == pic_index) continue;
         const DevPic& R = pics[rp];
         rv[l] = RefView{R.fin[c], R.bps, pw, ph};
         have[l] = true;

@@ -130,6 +130,37 @@ struct GroupStreams {
 
 }  // namespace
 
+// Decoded-picture buffer kept in HBM across submits (dpb.rs:79-454 keeps
+// reference pictures for later frames; here they never leave the device).
+// Entry planes: Y, Cb, Cr at 256-byte aligned offsets, unpadded rows.
+struct hpvcd_dpb {
+    struct Entry {
+        unsigned char* planes = nullptr;
+        size_t bytes = 0;
+        size_t luma_bytes = 0, chroma_bytes = 0;
+        int w = 0, h = 0, idc = 0, bd = 0, bd_c = 0;
+        bool valid = false;
+        cudaEvent_t ev_write = nullptr;  // after the copy that stored the picture
+        bool written = false;
+        cudaEvent_t ev_read[HPVCD_DPB_MAX_READERS] = {};  // per context slot: the last batch reading it
+        bool read[HPVCD_DPB_MAX_READERS] = {};
+    };
+    int device = 0;
+    std::vector<Entry> entries;
+    ~hpvcd_dpb() {
+        for (Entry& e : entries) {
+            if (e.ev_write) cudaEventSynchronize(e.ev_write);
+            for (int k = 0; k < HPVCD_DPB_MAX_READERS; ++k)
+                if (e.ev_read[k]) {
+                    cudaEventSynchronize(e.ev_read[k]);
+                    cudaEventDestroy(e.ev_read[k]);
+                }
+            if (e.ev_write) cudaEventDestroy(e.ev_write);
+            cudaFree(e.planes);
+        }
+    }
+};
+
 struct hpvcd_plan {
     int device = 0;
     std::vector<hpvcd_picture> src;
@@ -164,6 +195,7 @@ struct hpvcd_plan {
     cudaStream_t alloc_stream = nullptr;
     bool pooled = false;
     cudaGraphExec_t graphs[16] = {};  // captured launch sequences by stage mask
+    std::vector<int> dpb_refs;        // DPB entries the pictures predict from
     // concurrent segments (independent pictures): one stream per segment,
     // forked from and joined back into the launching stream
     bool concurrent = false;
@@ -289,7 +321,7 @@ void fill_inputs(DevPic& d, const hpvcd_picture& p) {
 hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out,
                         const hpvcd_sched* sched, const hpvcd_wp_table* host_wp, hpvcd_plan** result,
                         cudaStream_t pool_stream = nullptr, bool pooled = false,
-                        GroupStreams* lend = nullptr) {
+                        GroupStreams* lend = nullptr, const hpvcd_dpb* dpb = nullptr) {
     if (!pics || n == 0 || !result) return HPVCD_ERR_INVALID_ARG;
     for (uint32_t i = 0; i < n; ++i) {
         const hpvcd_status s = validate(pics[i]);
@@ -476,6 +508,57 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             P->max_rgb = std::max(P->max_rgb, (d.crop_w + 3) / 4 * d.crop_h);  // 4-pixel quads
         }
     }
+    // ---- DPB references: every entry a picture predicts from becomes one
+    // more device-table picture, read by motion compensation, never decoded ----
+    {
+        std::vector<int> ext_of(dpb ? dpb->entries.size() : 0, -1);
+        for (uint32_t i = 0; i < n; ++i)
+            for (int l = 0; l < 2; ++l)
+                for (int r = 0; r < HPVCD_MAX_REFS; ++r) {
+                    const int sv = pics[i].ref_slot[l][r];
+                    if (sv > HPVCD_REF_DPB(0)) continue;
+                    const int en = -2 - sv;
+                    const hpvcd_dpb::Entry* E =
+                        dpb && en < (int)dpb->entries.size() ? &dpb->entries[(size_t)en] : nullptr;
+                    if (!E || !E->valid || E->w != (int)pics[i].width || E->h != (int)pics[i].height ||
+                        E->idc != pics[i].chroma_idc || E->bd != pics[i].bit_depth_y ||
+                        E->bd_c != pics[i].bit_depth_c) {
+                        std::snprintf(t_last_error, sizeof(t_last_error),
+                                      "picture %u references DPB entry %d, which is empty or of another format", i,
+                                      en);
+                        delete P;
+                        return HPVCD_ERR_INVALID_ARG;
+                    }
+                    if (ext_of[(size_t)en] < 0) {
+                        ext_of[(size_t)en] = (int)P->pics.size();
+                        P->dpb_refs.push_back(en);
+                        hpvcd_picture q{};
+                        q.width = (uint32_t)E->w;
+                        q.height = (uint32_t)E->h;
+                        q.chroma_idc = (uint8_t)E->idc;
+                        q.bit_depth_y = (uint8_t)E->bd;
+                        q.bit_depth_c = (uint8_t)E->bd_c;
+                        q.log2_ctb = 6;
+                        const Geo gq = geo_of(q);
+                        DevPic d{};
+                        d.w = gq.w; d.h = gq.h; d.cw = gq.cw; d.ch = gq.ch; d.gw = gq.gw; d.gh = gq.gh;
+                        d.idc = E->idc; d.sub_w = gq.sub_w; d.sub_h = gq.sub_h;
+                        d.bd = E->bd; d.bd_c = E->bd_c; d.bps = gq.bps;
+                        d.log2_ctb = 6; d.ctb_cols = gq.ctb_cols; d.ctb_rows = gq.ctb_rows;
+                        for (int ll = 0; ll < 2; ++ll)
+                            for (int rr = 0; rr < HPVCD_MAX_REFS; ++rr) d.ref_pic[ll][rr] = -1;
+                        d.rec[0] = d.fin[0] = E->planes;
+                        if (E->idc) {
+                            d.rec[1] = d.fin[1] = E->planes + align_up(E->luma_bytes, 256);
+                            d.rec[2] = d.fin[2] = E->planes + align_up(E->luma_bytes, 256) +
+                                                  align_up(E->chroma_bytes, 256);
+                        }
+                        d.needs_wavefront = 0;
+                        P->pics.push_back(d);
+                    }
+                    P->pics[i].ref_pic[l][r] = ext_of[(size_t)en];
+                }
+    }
     // ---- wavefront schedule per segment: sort CTUs by (x + 2y, picture, x) ----
     for (Segment& s : P->segs) {
         s.item_off = (uint32_t)P->items.size();
@@ -504,10 +587,11 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             if (P->out.kind == HPVCD_OUT_RGB8) s.max_rgb = std::max(s.max_rgb, (d.crop_w + 3) / 4 * d.crop_h);
         }
     }
-    e = P->dmalloc(&P->d_pics, sizeof(DevPic) * n);
+    e = P->dmalloc(&P->d_pics, sizeof(DevPic) * P->pics.size());
     if (e == cudaSuccess) e = P->dmalloc(&P->d_items, sizeof(CtuItem) * std::max<size_t>(P->items.size(), 1));
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(P->d_pics, P->pics.data(), sizeof(DevPic) * n, cudaMemcpyHostToDevice, pool_stream);
+        e = cudaMemcpyAsync(P->d_pics, P->pics.data(), sizeof(DevPic) * P->pics.size(), cudaMemcpyHostToDevice,
+                            pool_stream);
     if (e == cudaSuccess && !P->items.empty())
         e = cudaMemcpyAsync(P->d_items, P->items.data(), sizeof(CtuItem) * P->items.size(), cudaMemcpyHostToDevice,
                             pool_stream);
@@ -613,7 +697,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
     }
     st = origin;
     if (!P->concurrent && (stages & HPVCD_STAGE_OUTPUT) && P->out.kind == HPVCD_OUT_RGB8) {
-        e = hpvcd_launch_rgb(P->d_pics, (int)P->pics.size(), P->max_rgb, P->d_canvas, st);
+        e = hpvcd_launch_rgb(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
         if (e != cudaSuccess) return cuda_status(e);
     }
     return HPVCD_OK;
@@ -623,7 +707,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
 // batch with identical geometry (same layout key).
 hpvcd_status plan_rebind(hpvcd_plan* P, const hpvcd_picture* pics, const hpvcd_wp_table* host_wp,
                          cudaStream_t st) {
-    for (size_t i = 0; i < P->pics.size(); ++i) {
+    for (size_t i = 0; i < P->src.size(); ++i) {
         P->src[i] = pics[i];
         P->rec_prefix[i + 1] = P->rec_prefix[i] + pics[i].n_tus;
         fill_inputs(P->pics[i], pics[i]);
@@ -642,7 +726,7 @@ hpvcd_status plan_rebind(hpvcd_plan* P, const hpvcd_picture* pics, const hpvcd_w
 }
 
 bool same_layout(const hpvcd_plan* P, const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out) {
-    if (P->src.size() != n) return false;
+    if (P->src.size() != n || !P->dpb_refs.empty()) return false;  // DPB entries may have moved
     for (uint32_t i = 0; i < n; ++i) {
         const hpvcd_picture& a = P->src[i];
         const hpvcd_picture& b = pics[i];
@@ -704,6 +788,7 @@ struct hpvcd_gpu {
     uint64_t next_ticket = 1;
     uint64_t budget = 0;
     uint64_t in_use = 0;
+    hpvcd_dpb* dpb = nullptr;  // hpvcd_gpu_set_dpb
     // schedule selection per submitted batch (hpvcd_gpu_set_selector)
     hpvcd_mlp* sel = nullptr;
     std::vector<hpvcd_sched> sel_cands;
@@ -938,7 +1023,7 @@ HPVCD_API hpvcd_status hpvcd_plan_launch(hpvcd_plan* plan, uint32_t stages, void
 }
 
 HPVCD_API hpvcd_status hpvcd_plan_planes(hpvcd_plan* plan, uint32_t i, void** y, void** cb, void** cr) {
-    if (!plan || i >= plan->pics.size()) return HPVCD_ERR_INVALID_ARG;
+    if (!plan || i >= plan->src.size()) return HPVCD_ERR_INVALID_ARG;
     if (y) *y = plan->pics[i].fin[0];
     if (cb) *cb = plan->pics[i].fin[1];
     if (cr) *cr = plan->pics[i].fin[2];
@@ -1097,6 +1182,92 @@ HPVCD_API hpvcd_status hpvcd_gpu_create(const hpvcd_gpu_cfg* cfg, hpvcd_gpu** ou
     return HPVCD_OK;
 }
 
+namespace {
+
+// After a batch's launch on its slot stream: mark the DPB entries it read,
+// then store the pictures flagged HPVCD_PIC_STORE_DPB into their entries
+// (each store waits for the batches of other slots still reading the entry).
+hpvcd_status dpb_after_launch(hpvcd_gpu* g, Slot* slot, int slot_idx, const hpvcd_picture* pics, uint32_t n) {
+    hpvcd_plan* P = slot->plan;
+    cudaError_t e = cudaSuccess;
+    for (const int en : P->dpb_refs) {
+        hpvcd_dpb::Entry& E = g->dpb->entries[(size_t)en];
+        if (!E.ev_read[slot_idx]) e = cudaEventCreateWithFlags(&E.ev_read[slot_idx], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(E.ev_read[slot_idx], slot->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+        E.read[slot_idx] = true;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t tag = (pics[i].flags & HPVCD_PIC_STORE_MASK) >> 16;
+        if (!tag) continue;
+        if (!g->dpb || tag - 1 >= g->dpb->entries.size()) return HPVCD_ERR_INVALID_ARG;
+        hpvcd_dpb::Entry& E = g->dpb->entries[tag - 1];
+        for (int k = 0; k < HPVCD_DPB_MAX_READERS && e == cudaSuccess; ++k)
+            if (E.read[k] && k != slot_idx) e = cudaStreamWaitEvent(slot->stream, E.ev_read[k], 0);
+        const Geo geo = geo_of(pics[i]);
+        const size_t need = align_up(geo.luma_bytes, 256) + 2 * align_up(geo.chroma_bytes, 256);
+        if (e == cudaSuccess && E.bytes != need) {
+            // a new size: the old storage is released once nothing uses it
+            if (E.written) e = cudaEventSynchronize(E.ev_write);
+            for (int k = 0; k < HPVCD_DPB_MAX_READERS && e == cudaSuccess; ++k)
+                if (E.read[k] && k != slot_idx) e = cudaEventSynchronize(E.ev_read[k]);
+            if (e == cudaSuccess && E.planes) e = cudaStreamSynchronize(slot->stream);
+            if (e == cudaSuccess) {
+                cudaFree(E.planes);
+                E.planes = nullptr;
+                E.bytes = 0;
+                e = cudaMalloc((void**)&E.planes, need);
+                if (e == cudaSuccess) E.bytes = need;
+            }
+        }
+        const DevPic& d = P->pics[i];
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(E.planes, d.fin[0], geo.luma_bytes, cudaMemcpyDeviceToDevice, slot->stream);
+        for (int c = 1; c < (pics[i].chroma_idc ? 3 : 1) && e == cudaSuccess; ++c)
+            e = cudaMemcpyAsync(E.planes + align_up(geo.luma_bytes, 256) + (c - 1) * align_up(geo.chroma_bytes, 256),
+                                d.fin[c], geo.chroma_bytes, cudaMemcpyDeviceToDevice, slot->stream);
+        if (e == cudaSuccess && !E.ev_write) e = cudaEventCreateWithFlags(&E.ev_write, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(E.ev_write, slot->stream);
+        if (e != cudaSuccess) return cuda_status(e);
+        E.written = true;
+        E.valid = true;
+        E.w = (int)pics[i].width;
+        E.h = (int)pics[i].height;
+        E.idc = pics[i].chroma_idc;
+        E.bd = pics[i].bit_depth_y;
+        E.bd_c = pics[i].bit_depth_c;
+        E.luma_bytes = geo.luma_bytes;
+        E.chroma_bytes = geo.chroma_bytes;
+    }
+    return HPVCD_OK;
+}
+
+}  // namespace
+
+HPVCD_API hpvcd_status hpvcd_dpb_create(int32_t device, uint32_t entries, hpvcd_dpb** out) {
+    if (!out || entries == 0 || entries > 254) return HPVCD_ERR_INVALID_ARG;
+    hpvcd_dpb* D = new (std::nothrow) hpvcd_dpb();
+    if (!D) return HPVCD_ERR_ALLOC;
+    D->device = device;
+    D->entries.resize(entries);
+    *out = D;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_dpb_destroy(hpvcd_dpb* D) {
+    if (!D) return HPVCD_ERR_INVALID_ARG;
+    cudaSetDevice(D->device);
+    delete D;
+    return HPVCD_OK;
+}
+
+HPVCD_API hpvcd_status hpvcd_gpu_set_dpb(hpvcd_gpu* g, hpvcd_dpb* dpb) {
+    if (!g || (dpb && dpb->device != g->device)) return HPVCD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g->mu);
+    g->dpb = dpb;
+    return HPVCD_OK;
+}
+
 HPVCD_API hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* g, hpvcd_mlp* mlp, const hpvcd_sched* cands, uint32_t n) {
     if (!g || (mlp && (!cands || n == 0 || n != hpvcd_mlp_variants(mlp)))) return HPVCD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g->mu);
@@ -1135,6 +1306,14 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         (!out->place || (out->n_canvases ? !out->canvases : (!out->canvas_w || !out->canvas_h))))
         return HPVCD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g->mu);
+    for (uint32_t i = 0; i < n; ++i) {  // DPB stores need an attached DPB with that entry
+        const uint32_t tag = (pics[i].flags & HPVCD_PIC_STORE_MASK) >> 16;
+        if (tag && (!g->dpb || tag - 1 >= g->dpb->entries.size())) {
+            std::snprintf(t_last_error, sizeof(t_last_error), "picture %u stores into DPB entry %u, which does not exist",
+                          i, tag - 1);
+            return HPVCD_ERR_INVALID_ARG;
+        }
+    }
     cudaSetDevice(g->device);
     Slot* slot = nullptr;
     for (Slot& s : g->slots)
@@ -1223,7 +1402,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
             slot->plan_bytes = 0;
         }
         st = plan_build(dev.data(), n, out, nullptr, any_wp ? slot->wp.data() : nullptr, &slot->plan,
-                        slot->stream, true, &slot->groups);
+                        slot->stream, true, &slot->groups, g->dpb);
         slot->plan_bytes = st == HPVCD_OK ? plan_bytes : 0;
     }
     g->in_use = g->in_use - held + slot->d_in_cap + slot->plan_bytes;
@@ -1236,7 +1415,18 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         if (st != HPVCD_OK) return st;
         ++g->sel_picks[pick == HPVCD_MLP_NO_PICK ? HPVCD_MLP_MAX_VARIANTS : pick];
     }
+    const int slot_idx = (int)(slot - g->slots.data());
+    // DPB entries this batch predicts from: wait for the stores that filled them
+    for (const int en : slot->plan->dpb_refs) {
+        hpvcd_dpb::Entry& E = g->dpb->entries[(size_t)en];
+        if (E.written) {
+            const cudaError_t we = cudaStreamWaitEvent(slot->stream, E.ev_write, 0);
+            if (we != cudaSuccess) return cuda_status(we);
+        }
+    }
     st = plan_launch(slot->plan, HPVCD_STAGE_ALL, slot->stream);
+    if (st != HPVCD_OK) return st;
+    st = dpb_after_launch(g, slot, slot_idx, pics, n);
     if (st != HPVCD_OK) return st;
     // ---- output copy back ----
     hpvcd_plan* P = slot->plan;

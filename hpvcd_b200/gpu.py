@@ -94,9 +94,48 @@ class GpuDecoder:
         _check(self._L.hpvcd_gpu_set_selector(self._h, mlp.handle if mlp is not None else None, arr,
                                               len(schedules)), "hpvcd_gpu_set_selector")
 
+    def set_dpb(self, dpb: "Dpb | None") -> None:
+        """Decoded-picture buffer the submits store into (flags
+        abi.PIC_STORE_DPB(e)) and predict from (ref_slot abi.REF_DPB(e))."""
+        self._dpb_keep = dpb
+        _check(self._L.hpvcd_gpu_set_dpb(self._h, dpb.handle if dpb is not None else None), "hpvcd_gpu_set_dpb")
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.hpvcd_gpu_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Dpb:
+    """Device-resident decoded-picture buffer (hpvcd_dpb_*): `entries`
+    reference pictures kept in HBM across submits of one context."""
+
+    def __init__(self, device: int = 0, entries: int = 16):
+        self._L = abi.lib()
+        h = C.c_void_p()
+        _check(self._L.hpvcd_dpb_create(device, entries, C.byref(h)), "hpvcd_dpb_create")
+        self._h = h
+        self.entries = entries
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.hpvcd_dpb_destroy(self._h)
             self._h = None
 
     def __enter__(self):

@@ -160,6 +160,13 @@ typedef struct hpvcd_wp_table {
 #define HPVCD_PIC_PRED_IN_PLANE 0x0020u      /* planes hold the prediction on entry:   */
                                              /* every TB only adds its residual        */
 #define HPVCD_PIC_INTER 0x0040u              /* picture has motion-compensated PUs     */
+/* Store the decoded picture into entry e of the context's DPB (hpvcd_dpb)
+ * after it is reconstructed; bits 16..23 of flags, 0 = no store. */
+#define HPVCD_PIC_STORE_DPB(e) ((uint32_t)((e) + 1) << 16)
+#define HPVCD_PIC_STORE_MASK 0x00ff0000u
+/* hpvcd_picture.ref_slot value naming DPB entry e (a picture decoded by an
+ * earlier submit); values >= 0 name pictures of the same batch, -1 none. */
+#define HPVCD_REF_DPB(e) (-2 - (int32_t)(e))
 
 /*
  * One coded picture (one HEIC grid tile, one still image, or one video frame).
@@ -189,7 +196,8 @@ typedef struct hpvcd_picture {
     const hpvcd_sao_ctb* sao;      /* ctb_cols * ctb_rows, NULL -> no SAO     */
     const hpvcd_pu* pus;           /* n_pus, inter pictures only              */
     const hpvcd_wp_table* wp;      /* NULL -> default weighted prediction     */
-    int32_t ref_slot[2][HPVCD_MAX_REFS]; /* reference list -> DPB slot         */
+    int32_t ref_slot[2][HPVCD_MAX_REFS]; /* reference: batch index (< this one), */
+                                         /* HPVCD_REF_DPB(e), or -1               */
     const void* pred[3];           /* PRED_IN_PLANE: initial Y/Cb/Cr planes   */
 } hpvcd_picture;
 
@@ -304,6 +312,25 @@ hpvcd_status hpvcd_gpu_read(hpvcd_gpu* ctx, hpvcd_ticket ticket, void* dst, uint
 hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* ctx, struct hpvcd_mlp* mlp, const struct hpvcd_sched* cands,
                                     uint32_t n);
 hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu* ctx, uint64_t* counts, uint32_t n);
+
+/* Decoded-picture buffer in HBM across submits, for video decoded frame by
+ * frame (dpb.rs:79-454 and video.rs:1045-1379 keep reference pictures on the
+ * host and clone planes per slice; here they never leave the device).  A
+ * submit stores pictures flagged HPVCD_PIC_STORE_DPB(e) into entry e after
+ * decoding them, and pictures of later submits predict from entry e through
+ * ref_slot = HPVCD_REF_DPB(e).  Ordering across the context's tickets is
+ * kept on the device (a store waits for earlier batches reading the entry;
+ * a batch waits for the store that filled an entry it reads).  Within one
+ * submit, references to pictures of the same batch use batch indices.  One
+ * DPB serves one context. */
+#define HPVCD_DPB_MAX_READERS 64
+typedef struct hpvcd_dpb hpvcd_dpb;
+hpvcd_status hpvcd_dpb_create(int32_t device, uint32_t entries, hpvcd_dpb** out);
+/* Waits for the entries' pending copies, then frees them. */
+hpvcd_status hpvcd_dpb_destroy(hpvcd_dpb* dpb);
+/* The DPB this context's submits store into and predict from (NULL: none);
+ * it must outlive the context's tickets. */
+hpvcd_status hpvcd_gpu_set_dpb(hpvcd_gpu* ctx, hpvcd_dpb* dpb);
 
 /* ------------------------------------------------------------------------ */
 /* Device-buffer API (plans).  The picture descriptors point at device      */

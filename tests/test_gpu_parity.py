@@ -16,7 +16,7 @@ torch = pytest.importorskip("torch")
 if not torch.cuda.is_available():  # pragma: no cover
     pytest.skip("needs a CUDA GPU", allow_module_level=True)
 
-from hpvcd_b200.gpu import DevicePlan, GpuDecoder  # noqa: E402
+from hpvcd_b200.gpu import DevicePlan, GpuDecoder, split_planes  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
 
@@ -493,3 +493,64 @@ def test_mixed_edge_batch(dec):
     q.n_coeffs = 0
     pics[-1] = q
     run_yuv(dec, pics, "mixed edge batch")
+
+
+# --- decoded-picture buffer: frame-by-frame submits predict from HBM ------
+def _frame_by_frame(pics, in_flight):
+    """Submit each picture alone; reference pictures come from the DPB
+    (picture k is stored into entry k, batch index j becomes REF_DPB(j))."""
+    import ctypes as C
+    from hpvcd_b200.gpu import Dpb
+    with GpuDecoder(0, max_inflight=in_flight) as d, Dpb(0, entries=len(pics)) as dpb:
+        d.set_dpb(dpb)
+        tickets, out = [], []
+        for k, p in enumerate(pics):
+            q = abi.Picture()
+            C.pointer(q)[0] = p
+            q.flags = p.flags | abi.PIC_STORE_DPB(k)
+            for l in range(2):
+                for r in range(abi.MAX_REFS):
+                    s = p.ref_slot[l][r]
+                    q.ref_slot[l][r] = abi.REF_DPB(s) if s >= 0 else -1
+            tickets.append((d.submit([q]), q))
+            if len(tickets) >= in_flight:
+                t, qq = tickets.pop(0)
+                d.wait(t)
+                out += split_planes([qq], d.read(t))
+        for t, qq in tickets:
+            d.wait(t)
+            out += split_planes([qq], d.read(t))
+        d.set_dpb(None)
+    return out
+
+
+@pytest.mark.parametrize("in_flight", [1, 2])
+def test_dpb_frame_by_frame_matches_batch(in_flight):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(140, 320, 192, bit_depth=8))
+    for i in range(1, 6):
+        s.add(synth.inter_cfg(140 + i, 320, 192, weighted=(i == 3)))
+    pics = s.pictures()
+    ref, _ = O.decode_batch(pics)
+    assert_planes_equal(_frame_by_frame(pics, in_flight), ref, f"dpb in_flight={in_flight}")
+
+
+def test_dpb_rejects_empty_entry(dec):
+    import ctypes as C
+    from hpvcd_b200.gpu import Dpb
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(150, 128, 64, bit_depth=8))
+    s.add(synth.inter_cfg(151, 128, 64))
+    pics = s.pictures()
+    q = abi.Picture()
+    C.pointer(q)[0] = pics[1]
+    q.ref_slot[0][0] = abi.REF_DPB(3)  # never stored
+    with GpuDecoder(0) as d, Dpb(0, entries=4) as dpb:
+        with pytest.raises(abi.HpvcdError) as ei:
+            d.submit([q])          # no DPB attached
+        assert ei.value.status == abi.ERR_INVALID_ARG
+        d.set_dpb(dpb)
+        with pytest.raises(abi.HpvcdError) as ei:
+            d.submit([q])          # entry 3 empty
+        assert ei.value.status == abi.ERR_INVALID_ARG
+        d.set_dpb(None)
