@@ -167,7 +167,12 @@ class Picture(C.Structure):
         ("cells", C.c_void_p), ("sao", C.c_void_p), ("pus", C.c_void_p), ("wp", C.c_void_p),
         ("ref_slot", (C.c_int32 * MAX_REFS) * 2),
         ("pred", C.c_void_p * 3),
+        ("scaling", C.c_void_p),
     ]
+
+
+class Scaling(C.Structure):
+    _fields_ = [("m", ((C.c_uint8 * 64) * 6) * 4), ("dc", (C.c_uint8 * 6) * 4)]
 
 
 class TilePlace(C.Structure):
@@ -230,6 +235,7 @@ class SynthCfg(C.Structure):
         ("intra_cu_p", C.c_float), ("bi_p", C.c_float), ("mv_sd", C.c_float),
         ("mv_pad", C.c_float), ("weighted", C.c_uint32), ("n_refs", C.c_uint32),
         ("tu_mix", C.c_float * 4),
+        ("scaling", C.c_uint32),
     ]
 
 

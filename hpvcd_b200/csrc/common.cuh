@@ -25,6 +25,7 @@ struct DevPic {
     const hpvcd_cell* cells;
     const hpvcd_sao_ctb* sao;
     const hpvcd_pu* pus;
+    const hpvcd_scaling* scaling;  // NULL: flat scale
     uint32_t n_tus, n_pus;
     uint64_t n_coeffs;
     hpvcd_wp_table wp;

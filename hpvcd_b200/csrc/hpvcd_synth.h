@@ -55,6 +55,10 @@ typedef struct hpvcd_synth_cfg {
      * quadtree aims at (per-level split probabilities derived from it); all
      * zero -> tu_split_p at every level. */
     float tu_mix[4];
+    /* 1: random scaling lists (hpvcd_scaling, entries 1..255 rising with
+     * frequency, DC 1..255), drawn from their own seeded stream so the rest
+     * of the picture is the same as without them. */
+    uint32_t scaling;
 } hpvcd_synth_cfg;
 
 typedef struct hpvcd_synth hpvcd_synth;

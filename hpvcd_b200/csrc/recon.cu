@@ -159,13 +159,33 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
     // transform.rs:701-725 dequant_params (non-extended precision: range 15)
     const int bd_shift = bd + t.log2n + 10 - 15;
     const int qs = clamp3i(qpp, 0, 51 + 6 * (bd - 8));
-    const long long factor = (long long)c_dequant_scale[qs % 6] * (1ll << (qs / 6)) * 16;
+    const long long base = (long long)c_dequant_scale[qs % 6] * (1ll << (qs / 6));
     const long long add = 1ll << (bd_shift - 1);
+    // Scaling lists (decode.rs:5874-5899, transform.rs:668-683): the factor
+    // of coefficient (r, c) is base * m(r, c) instead of base * 16; 4x4
+    // lists index the 4x4 raster, larger TBs the 8x8 list upsampled, with
+    // the DC entry for 16x16 and 32x32.  Transform-skip TBs above 4x4 stay
+    // flat.
+    const uint8_t* sm = nullptr;
+    int sdc = 16;
+    if (P.scaling && (!(t.flags & HPVCD_TU_TSKIP) || n == 4)) {
+        const int size_id = t.log2n - 2;
+        const int matrix_id = min((int)t.comp, 2) + ((t.flags & HPVCD_TU_INTRA) ? 0 : 3);
+        sm = P.scaling->m[size_id][matrix_id];
+        sdc = P.scaling->dc[size_id][matrix_id];
+    }
+    const int down = t.log2n > 3 ? t.log2n - 3 : 0;
+    auto factor_at = [&](int r, int c) -> long long {
+        if (!sm) return base * 16;
+        if (n == 4) return base * sm[r * 4 + c];
+        if (n >= 16 && r == 0 && c == 0) return base * sdc;
+        return base * sm[(r >> down) * 8 + (c >> down)];
+    };
     if (t.flags & HPVCD_TU_TSKIP) {  // transform.rs:728-792
         const int tr_shift = 15 - bd - t.log2n;
         const int tr_add = tr_shift > 0 ? 1 << (tr_shift - 1) : 0;
         for (int i = lane; i < n * n; i += 32) {
-            long long v = ((long long)lv[i] * factor + add) >> bd_shift;
+            long long v = ((long long)lv[i] * factor_at(i / n, i % n) + add) >> bd_shift;
             v = v < -32768 ? -32768 : (v > 32767 ? 32767 : v);
             const int r = tr_shift >= 0 ? ((int)v + tr_add) >> tr_shift : (int)((unsigned)v << (-tr_shift));
             emit(i / n, i % n, i16s ? (int)(int16_t)r : r);
@@ -181,7 +201,7 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         const int l = lane & 15, r = l >> 2, c = l & 3;
         int d = 0;
         if (lane < 16 && c < nx) {
-            const long long v = ((long long)lv[l] * factor + add) >> bd_shift;
+            const long long v = ((long long)lv[l] * factor_at(r, c) + add) >> bd_shift;
             d = (int)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v));
         }
         // basis entry T[k][m] of the 4-point DCT (rows 64 / 83,36 / 64 / 36,83
@@ -217,7 +237,7 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         const int r = i / n, c = i % n;
         int v = 0;
         if (c < nx) {
-            const long long d = ((long long)lv[i] * factor + add) >> bd_shift;
+            const long long d = ((long long)lv[i] * factor_at(r, c) + add) >> bd_shift;
             v = (int)(d < -32768 ? -32768 : (d > 32767 ? 32767 : d));
         }
         buf[r * kScr + c] = (int16_t)v;

@@ -52,6 +52,8 @@ struct Picture {
     std::vector<hpvcd_pu> pus;
     hpvcd_wp_table wp{};
     bool has_wp = false;
+    hpvcd_scaling scaling{};
+    bool has_scaling = false;
     std::vector<uint8_t> pred8[3];
     std::vector<uint16_t> pred16[3];
 };
@@ -452,6 +454,21 @@ struct Gen {
         for (int l = 0; l < 2; ++l)
             for (int r = 0; r < HPVCD_MAX_REFS; ++r)
                 d.ref_slot[l][r] = r < pic_index ? pic_index - 1 - r : -1;
+        if (c.scaling) {
+            P.has_scaling = true;
+            Rng sr(c.seed ^ 0x5CA1E5ull);
+            for (int s = 0; s < 4; ++s)
+                for (int m = 0; m < 6; ++m) {
+                    const int used = s ? 8 : 4;
+                    const int slope = sr.range(0, 12);
+                    for (int y = 0; y < used; ++y)
+                        for (int x = 0; x < used; ++x) {
+                            const int v = 16 + slope * (x + y) + (int)std::lround(sr.gauss() * 6.0);
+                            P.scaling.m[s][m][y * used + x] = (uint8_t)std::clamp(v, 1, 255);
+                        }
+                    P.scaling.dc[s][m] = (uint8_t)sr.range(1, 255);
+                }
+        }
         P.cells.assign((size_t)gw * gh, hpvcd_cell{});
         const int ctb = 1 << log2_ctb;
         const int cols = (w + ctb - 1) / ctb, rows = (h + ctb - 1) / ctb;
@@ -565,6 +582,7 @@ int32_t hpvcd_synth_add(hpvcd_synth* s, const hpvcd_synth_cfg* cfg) {
     d.n_pus = (uint32_t)pic->pus.size();
     d.pus = pic->pus.empty() ? nullptr : pic->pus.data();
     d.wp = pic->has_wp ? &pic->wp : nullptr;
+    d.scaling = pic->has_scaling ? &pic->scaling : nullptr;
     for (int c = 0; c < 3; ++c)
         d.pred[c] = !pic->pred8[c].empty() ? (const void*)pic->pred8[c].data()
                     : !pic->pred16[c].empty() ? (const void*)pic->pred16[c].data()

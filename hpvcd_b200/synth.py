@@ -114,7 +114,7 @@ def residual_cfg(seed: int, width=512, height=512, bit_depth=8, chroma_idc=1) ->
 
 
 def intra_cfg(seed: int, width=512, height=512, bit_depth=10, chroma_idc=1, sao=True,
-              deblock=True, tskip_p=0.0, tqb_p=0.0, cbf_p=0.9) -> abi.SynthCfg:
+              deblock=True, tskip_p=0.0, tqb_p=0.0, cbf_p=0.9, scaling=False) -> abi.SynthCfg:
     """Intra still tile: random CU (64..8) and TU (32..4) quadtrees, modes
     uniform over 35, coefficients as the residual case, deblocking on, SAO
     with random band/edge types and offsets in [-7, 7]."""
@@ -125,6 +125,7 @@ def intra_cfg(seed: int, width=512, height=512, bit_depth=10, chroma_idc=1, sao=
     c.bit_depth = bit_depth
     c.chroma_idc = chroma_idc
     c.cbf_p = cbf_p
+    c.scaling = int(scaling)
     c.tskip_p = tskip_p
     c.tqb_p = tqb_p
     c.sao_p = 0.7 if sao else 0.0
@@ -138,8 +139,8 @@ def intra_cfg(seed: int, width=512, height=512, bit_depth=10, chroma_idc=1, sao=
 
 
 def inter_cfg(seed: int, width=1920, height=1080, bit_depth=8, weighted=False, n_refs=4,
-              intra_cu_p=0.1, bi_p=0.4) -> abi.SynthCfg:
-    c = intra_cfg(seed, width, height, bit_depth=bit_depth, chroma_idc=1)
+              intra_cu_p=0.1, bi_p=0.4, scaling=False) -> abi.SynthCfg:
+    c = intra_cfg(seed, width, height, bit_depth=bit_depth, chroma_idc=1, scaling=scaling)
     c.kind = abi.SYNTH_INTER
     c.weighted = int(weighted)
     c.n_refs = n_refs

@@ -151,6 +151,18 @@ typedef struct hpvcd_wp_table {
     hpvcd_wp_entry e[2][HPVCD_MAX_REFS];
 } hpvcd_wp_table;
 
+/* Scaling lists of a picture (config.rs:373 `ScalingList`, the PPS list when
+ * present, else the SPS list; decode.rs:5874-5899), resolved by the host:
+ * m[size_id][matrix_id] is what `ScalingList::matrix` returns (8x8 raster;
+ * the 4x4 lists use the first 16 entries, 4x4 raster), dc[size_id][matrix_id]
+ * the DC value of the 16x16 / 32x32 lists.  size_id = log2(TB size) - 2;
+ * matrix_id = component + 3 for TBs of inter CUs.  Transform-skip TBs larger
+ * than 4x4 use the flat scale, as the reference does. */
+typedef struct hpvcd_scaling {
+    uint8_t m[4][6][64];
+    uint8_t dc[4][6];
+} hpvcd_scaling; /* 1560 bytes */
+
 /* hpvcd_picture.flags */
 #define HPVCD_PIC_STRONG_SMOOTHING 0x0001u   /* strong_intra_smoothing_enabled_flag   */
 #define HPVCD_PIC_SMOOTHING_DISABLED 0x0002u /* RExt intra_smoothing_disabled_flag     */
@@ -199,6 +211,7 @@ typedef struct hpvcd_picture {
     int32_t ref_slot[2][HPVCD_MAX_REFS]; /* reference: batch index (< this one), */
                                          /* HPVCD_REF_DPB(e), or -1               */
     const void* pred[3];           /* PRED_IN_PLANE: initial Y/Cb/Cr planes   */
+    const hpvcd_scaling* scaling;  /* NULL -> flat (scaling_list_enabled = 0) */
 } hpvcd_picture;
 
 /* Output of a batch.  RGB8 is the `decode_heic_rgb8` path (lib.rs:1964):

@@ -826,6 +826,19 @@ void load_block_clipped(const uint16_t* plane, int stride, int width, int height
         for (int x = 0; x < vw; ++x) pred[y * n + x] = plane[(size_t)(y0 + y) * stride + x0 + x];
 }
 
+// decode.rs:5874-5899 scaling_matrix_from_lists: the list of this size,
+// component and prediction mode ([intra Y, Cb, Cr, inter Y, Cb, Cr]); none
+// (flat) without lists and for transform skip above 4x4.
+const uint8_t* scaling_select(const hpvcd_scaling* s, int comp, int n, bool inter, bool tskip, int* dc) {
+    if (!s || (tskip && n != 4)) return nullptr;
+    int size_id = 0;
+    while ((4 << size_id) < n) ++size_id;
+    size_id = std::min(size_id, 3);
+    const int matrix_id = std::min(comp, 2) + (inter ? 3 : 0);
+    *dc = s->dc[size_id][matrix_id];
+    return s->m[size_id][matrix_id];
+}
+
 // Residual of one TB: decode.rs:4754-4802 (8-bit i16 path) and :4835-4903
 // (i32 path) for luma, :5313-5417 for chroma.
 void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_t* res) {
@@ -846,13 +859,16 @@ void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_
         const int pps_off = t.comp == 1 ? p->pps_cb_qp_offset : p->pps_cr_qp_offset;
         qpp = qp_prime(qpc(t.qp_y + pps_off + t.cqp_off, g.idc, bd), bd);
     }
+    int sc_dc = 16;
+    const uint8_t* sc = scaling_select(p->scaling, t.comp, n, !(t.flags & HPVCD_TU_INTRA),
+                                       (t.flags & HPVCD_TU_TSKIP) != 0, &sc_dc);
     if (t.flags & HPVCD_TU_TSKIP) {
         const orc_ts_params tp = ts_params(n, qpp, bd, false);
-        dequant_ts(lv, n, tp, nullptr, 16, i16s, res);
+        dequant_ts(lv, n, tp, sc, sc_dc, i16s, res);
         return;
     }
     int32_t deq[32 * 32];
-    dequant(lv, n, dequant_params(n, qpp, bd, false), nullptr, 16, i16s, deq);
+    dequant(lv, n, dequant_params(n, qpp, bd, false), sc, sc_dc, i16s, deq);
     if (luma && n == 4 && (t.flags & HPVCD_TU_INTRA))
         inv_dst4(deq, bd, 15, i16s, res);
     else
@@ -1187,6 +1203,16 @@ void orc_dequant(const int32_t* levels, int32_t n, const orc_dequant_params* p,
                  const uint8_t* scaling, int32_t dc, int32_t i16s, int32_t* out) {
     dequant(levels, n, *p, scaling, dc, i16s != 0, out);
 }
+int32_t orc_scaling_select(const hpvcd_scaling* s, int32_t comp, int32_t n, int32_t inter, int32_t tskip,
+                           int32_t* first, int32_t* dc) {
+    int d = 16;
+    const uint8_t* m = scaling_select(s, comp, n, inter != 0, tskip != 0, &d);
+    if (!m) return 0;
+    *first = m[0];
+    *dc = d;
+    return 1;
+}
+
 void orc_dequant_ts(const int32_t* levels, int32_t n, const orc_ts_params* p,
                     const uint8_t* scaling, int32_t dc, int32_t i16s, int32_t* out) {
     dequant_ts(levels, n, *p, scaling, dc, i16s != 0, out);

@@ -44,6 +44,10 @@ void orc_ts_params_get(int32_t n, int32_t qp_prime, int32_t bd, int32_t ext, orc
 void orc_dequant(const int32_t* levels, int32_t n, const orc_dequant_params* p,
                  const uint8_t* scaling /* NULL = flat */, int32_t scaling_dc, int32_t i16_store,
                  int32_t* out);
+/* decode.rs:5874-5899: 1 and the selected list's first entry and DC when a
+ * list applies, 0 for the flat scale. */
+int32_t orc_scaling_select(const hpvcd_scaling* s, int32_t comp, int32_t n, int32_t inter, int32_t tskip,
+                           int32_t* first, int32_t* dc);
 void orc_dequant_ts(const int32_t* levels, int32_t n, const orc_ts_params* p,
                     const uint8_t* scaling, int32_t scaling_dc, int32_t i16_store, int32_t* out);
 void orc_inv_dct(const int32_t* coeff, int32_t n, int32_t bd, int32_t max_range, int32_t nx,

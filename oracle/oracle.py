@@ -88,6 +88,15 @@ def dequant(levels, n, params, scaling=None, dc=16, i16=False, ts=False) -> np.n
     return out
 
 
+def scaling_select(scaling, comp, n, inter, tskip):
+    """decode.rs:5874-5899: (first entry, DC) of the list a TB uses, or None
+    for the flat scale.  `scaling` is an abi.Scaling."""
+    first, dc = C.c_int32(), C.c_int32()
+    ok = lib().orc_scaling_select(C.byref(scaling), i32(comp), i32(n), i32(int(inter)), i32(int(tskip)),
+                                  C.byref(first), C.byref(dc))
+    return (first.value, dc.value) if ok else None
+
+
 def inv_dct(coeff, n, bd, max_range=15, nx=None, i16=False) -> np.ndarray:
     c = np.ascontiguousarray(coeff, dtype=np.int32).reshape(-1)
     out = np.zeros(n * n, np.int32)

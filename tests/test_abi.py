@@ -43,7 +43,7 @@ def test_struct_layouts_match():
         "hpvcd_tile_place": abi.TilePlace, "hpvcd_output": abi.Output,
         "hpvcd_gpu_cfg": abi.GpuCfg, "hpvcd_sched": abi.Sched, "hpvcd_canvas": abi.Canvas,
         "hpvcd_server_cfg": abi.ServerCfg, "hpvcd_request": abi.Request,
-        "hpvcd_completion": abi.Completion,
+        "hpvcd_completion": abi.Completion, "hpvcd_scaling": abi.Scaling,
     }
     for name, cls in pairs.items():
         assert L.hpvcd_abi_sizeof(name.encode()) == C.sizeof(cls), name

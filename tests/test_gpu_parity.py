@@ -554,3 +554,71 @@ def test_dpb_rejects_empty_entry(dec):
             d.submit([q])          # entry 3 empty
         assert ei.value.status == abi.ERR_INVALID_ARG
         d.set_dpb(None)
+
+
+# --- scaling lists (scaling_list_enabled_flag with signalled matrices) -----
+@pytest.mark.parametrize("bd,idc", [(8, 1), (10, 3), (12, 0)])
+def test_scaling_lists_intra(dec, bd, idc):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(160 + bd, 384, 256, bit_depth=bd, chroma_idc=idc, tskip_p=0.3, tqb_p=0.05,
+                          scaling=True))
+    run_yuv(dec, s.pictures(), f"scaling lists {bd}-bit idc {idc}")
+
+
+def test_scaling_lists_residual_and_inter(dec):
+    s = synth.SynthSet()
+    r = synth.residual_cfg(170, 256, 128, bit_depth=10)
+    r.scaling = 1
+    s.add(r)
+    run_yuv(dec, s.pictures(), "scaling lists residual")
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(171, 320, 192, bit_depth=8, scaling=True))
+    for i in range(1, 4):
+        s.add(synth.inter_cfg(171 + i, 320, 192, weighted=(i == 2), scaling=True))
+    run_yuv(dec, s.pictures(), "scaling lists inter")
+
+
+def test_scaling_lists_large_transform_skip(dec):
+    """RExt transform skip above 4x4 keeps the flat scale (decode.rs:5882-5888)."""
+    import ctypes as C
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(175, 256, 256, bit_depth=10, scaling=True))
+    p = s.picture(0)
+    tus = np.ctypeslib.as_array((C.c_uint8 * (p.n_tus * 16)).from_address(p.tus)).view(abi.TU_DTYPE).copy()
+    coded = (tus["flags"] & abi.TU_CBF) != 0
+    big = coded & (tus["log2n"] >= 3) & ((tus["flags"] & abi.TU_TQB) == 0)
+    pick = np.flatnonzero(big)[::3]
+    assert pick.size > 10
+    tus["flags"][pick] |= abi.TU_TSKIP
+    q = abi.Picture()
+    C.pointer(q)[0] = p
+    q.tus = tus.ctypes.data
+    run_yuv(dec, [q], "transform skip 8x8..32x32 with scaling lists")
+
+
+def test_scaling_lists_plan_and_server():
+    from hpvcd_b200.gpu import Server, pack_pinned, pinned_empty
+    g = synth.make_grid(1024, 512, seed=177, bit_depth=10, scaling=True)
+    out, keep = synth.grid_output(g)
+    pics = g.synth.pictures()
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    plan = DevicePlan(pics, out)
+    plan.launch()
+    torch.cuda.synchronize()
+    assert np.array_equal(plan.canvas(), ref)
+    plan.close()
+    kp_all = []
+    with Server(0, max_inflight=2, batching=True, batch_window_us=100000) as srv:
+        srv.submit(pics, g.places, g.out_w, g.out_h, user=0)
+        packed, kp = pack_pinned(pics)
+        dst, kd = pinned_empty(g.out_w * g.out_h * 3)
+        kp_all.append((kp, kd))
+        srv.submit(packed, g.places, g.out_w, g.out_h, user=1, dst=dst.reshape(g.out_h, g.out_w, 3),
+                   zero_copy_keep=(kp, kd))
+        got = {}
+        while len(got) < 2:
+            for c in srv.poll(4, timeout_ms=60000):
+                assert c["status"] == abi.OK
+                got[c["user"]] = c
+    for k in (0, 1):
+        assert np.array_equal(got[k]["image"], ref), k

@@ -319,3 +319,45 @@ def test_luma_deblock_step_edges(tc, maxv):
                         gq = [int(pl[8 + k, line]) for k in range(4)]
                     P, Q = _py_apply(p, q, dec, tc, maxv)
                     assert gp == P and gq == Q, (pv, qv, dec, vertical, line)
+
+
+def _constant_lists(values):
+    """ScalingList::test_constant_lists (config.rs): every size's matrix
+    `matrix_id` filled with values[matrix_id], DC the same."""
+    s = O.abi.Scaling()
+    for size_id in range(4):
+        for mid, v in enumerate(values):
+            for i in range(64):
+                s.m[size_id][mid][i] = v
+            s.dc[size_id][mid] = v
+    return s
+
+
+def test_scaling_list_selection_uses_prediction_mode_and_ts_size():
+    # decode.rs scaling_list_selection_uses_prediction_mode_and_ts_size
+    lists = _constant_lists([10, 20, 30, 40, 50, 60])
+    assert O.scaling_select(lists, 1, 8, inter=False, tskip=False) == (20, 20)
+    assert O.scaling_select(lists, 1, 8, inter=True, tskip=False) == (50, 50)
+    assert O.scaling_select(lists, 0, 4, inter=False, tskip=True) is not None
+    assert O.scaling_select(lists, 0, 8, inter=False, tskip=True) is None
+    assert O.scaling_select(lists, 0, 32, inter=True, tskip=True) is None
+    assert O.scaling_select(lists, 2, 32, inter=True, tskip=False) == (60, 60)
+
+
+@pytest.mark.parametrize("n", [8, 16, 32])
+def test_scaled_dequant_upsamples_the_8x8_list(n):
+    # transform.rs:668-683: 8x8 list replicated over n/8 x n/8 blocks, DC
+    # entry at (0, 0) from 16x16 up; factor = factor/16 * m.
+    rng = np.random.default_rng(n)
+    m8 = rng.integers(1, 256, 64).astype(np.uint8)
+    dc = 77
+    levels = rng.integers(-300, 300, n * n).astype(np.int32)
+    p = O.dequant_params(n, 33, 10)
+    got = O.dequant(levels, n, p, m8, dc=dc)
+    rep = n // 8
+    m = np.repeat(np.repeat(m8.reshape(8, 8), rep, 0), rep, 1).astype(np.int64).reshape(-1)
+    if n >= 16:
+        m[0] = dc
+    f = (p.factor // 16) * m
+    want = np.clip((levels.astype(np.int64) * f + p.add) >> p.shift, p.clip_min, p.clip_max)
+    assert np.array_equal(got, want)
