@@ -41,6 +41,7 @@ STATUS_NAMES = {
 }
 
 TU_CBF, TU_TSKIP, TU_INTRA, TU_TQB = 0x01, 0x02, 0x04, 0x08
+TU_ROTATE, TU_RDPCM_H, TU_RDPCM_V = 0x10, 0x20, 0x40
 CELL_EXEMPT = 0x01
 PU_L0, PU_L1 = 0x01, 0x02
 MAX_REFS = 16
@@ -235,7 +236,7 @@ class SynthCfg(C.Structure):
         ("intra_cu_p", C.c_float), ("bi_p", C.c_float), ("mv_sd", C.c_float),
         ("mv_pad", C.c_float), ("weighted", C.c_uint32), ("n_refs", C.c_uint32),
         ("tu_mix", C.c_float * 4),
-        ("scaling", C.c_uint32),
+        ("scaling", C.c_uint32), ("rext", C.c_uint32), ("tskip_log2_max", C.c_uint32),
     ]
 
 

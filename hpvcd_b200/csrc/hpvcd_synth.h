@@ -59,6 +59,13 @@ typedef struct hpvcd_synth_cfg {
      * frequency, DC 1..255), drawn from their own seeded stream so the rest
      * of the picture is the same as without them. */
     uint32_t scaling;
+    /* RExt residual tools (bit mask): 1 transform_skip_rotation_enabled,
+     * 2 implicit_rdpcm_enabled, 4 explicit_rdpcm_enabled (inter CUs draw
+     * none / horizontal / vertical per transform-skip or bypass TB). */
+    uint32_t rext;
+    /* log2_max_transform_skip_block_size (2..5; 0 -> 2): transform skip is
+     * drawn for coded TBs up to this size. */
+    uint32_t tskip_log2_max;
 } hpvcd_synth_cfg;
 
 typedef struct hpvcd_synth hpvcd_synth;

@@ -145,7 +145,8 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
     const int bd = luma ? P.bd : P.bd_c;
     const bool i16s = bd <= 8;
     const int16_t* lv = P.coeffs + t.coeff_off;
-    if (t.flags & HPVCD_TU_TQB) {  // decode.rs:4754-4757 / :4830-4834: residual = levels
+    const uint32_t rext = t.flags & (HPVCD_TU_ROTATE | HPVCD_TU_RDPCM_H | HPVCD_TU_RDPCM_V);
+    if ((t.flags & HPVCD_TU_TQB) && !rext) {  // decode.rs:4754-4757 / :4830-4834: residual = levels
         for (int i = lane; i < n * n; i += 32) emit(i / n, i % n, (int)lv[i]);
         return;
     }
@@ -181,6 +182,45 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         if (n >= 16 && r == 0 && c == 0) return base * sdc;
         return base * sm[(r >> down) * 8 + (c >> down)];
     };
+    if (rext && (t.flags & (HPVCD_TU_TSKIP | HPVCD_TU_TQB))) {
+        // RExt residual modification (decode.rs:8418-8446): the TS / TQB
+        // residual goes to int32 scratch (rotated: sample i from n*n-1-i),
+        // then one lane per column (vertical RDPCM) or row (horizontal)
+        // accumulates it.  At 8 bits the reference adds in wrapping i16;
+        // the int32 sums wrapped once at the end are the same values.
+        int32_t* r32 = reinterpret_cast<int32_t*>(buf);  // buf + tmp: 32 * kScr int32
+        const int tr_shift = 15 - bd - t.log2n;
+        const int tr_add = tr_shift > 0 ? 1 << (tr_shift - 1) : 0;
+        const bool rot = (rext & HPVCD_TU_ROTATE) != 0;
+        for (int i = lane; i < n * n; i += 32) {
+            int r;
+            if (t.flags & HPVCD_TU_TQB) {
+                r = lv[i];
+            } else {
+                long long v = ((long long)lv[i] * factor_at(i / n, i % n) + add) >> bd_shift;
+                v = v < -32768 ? -32768 : (v > 32767 ? 32767 : v);
+                r = tr_shift >= 0 ? ((int)v + tr_add) >> tr_shift : (int)((unsigned)v << (-tr_shift));
+            }
+            r32[rot ? n * n - 1 - i : i] = r;
+        }
+        __syncwarp();
+        if (lane < n) {
+            if (rext & HPVCD_TU_RDPCM_V) {
+                int acc = 0;
+                for (int y = 0; y < n; ++y) r32[y * n + lane] = acc += r32[y * n + lane];
+            } else if (rext & HPVCD_TU_RDPCM_H) {
+                int acc = 0;
+                for (int x = 0; x < n; ++x) r32[lane * n + x] = acc += r32[lane * n + x];
+            }
+        }
+        __syncwarp();
+        for (int i = lane; i < n * n; i += 32) {
+            const int r = r32[i];
+            emit(i / n, i % n, i16s ? (int)(int16_t)r : r);
+        }
+        __syncwarp();
+        return;
+    }
     if (t.flags & HPVCD_TU_TSKIP) {  // transform.rs:728-792
         const int tr_shift = 15 - bd - t.log2n;
         const int tr_add = tr_shift > 0 ? 1 << (tr_shift - 1) : 0;
@@ -316,7 +356,7 @@ __global__ void __launch_bounds__(kResWarps * 32)
 k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_prefix, uint32_t n_pics,
            uint32_t* dev_err) {
     __shared__ int16_t dct[32 * 32];
-    __shared__ int16_t scr[kResWarps][2][32 * kScr];
+    __shared__ __align__(16) int16_t scr[kResWarps][2][32 * kScr];  // per warp: buf, tmp (contiguous)
     for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) dct[i] = (int16_t)dct_entry(32, i / 32, i % 32);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -120,8 +120,23 @@ struct Gen {
         t.qp_y = (int8_t)qp;
         t.cqp_off = (int8_t)cqp_off;
         const int n = 1 << log2n;
-        if ((flags & HPVCD_TU_CBF) && log2n == 2 && !(flags & HPVCD_TU_TQB) && rng.bern(c.tskip_p))
+        const int ts_max = c.tskip_log2_max > 2 ? (int)c.tskip_log2_max : 2;
+        if ((flags & HPVCD_TU_CBF) && log2n <= ts_max && !(flags & HPVCD_TU_TQB) && rng.bern(c.tskip_p))
             flags |= HPVCD_TU_TSKIP;
+        // decode.rs:4356-4374 rext_post_ops, resolved here as the host does
+        if (c.rext && (flags & HPVCD_TU_CBF) && (flags & (HPVCD_TU_TSKIP | HPVCD_TU_TQB))) {
+            const bool inter = !(flags & HPVCD_TU_INTRA);
+            if ((c.rext & 1) && (flags & HPVCD_TU_TSKIP) && !(flags & HPVCD_TU_TQB) && log2n == 2 && !inter)
+                flags |= HPVCD_TU_ROTATE;
+            if (inter) {
+                if (c.rext & 4) {
+                    const int d = rng.range(0, 2);
+                    if (d) flags |= d == 1 ? HPVCD_TU_RDPCM_H : HPVCD_TU_RDPCM_V;
+                }
+            } else if ((c.rext & 2) && (mode == 10 || mode == 26)) {
+                flags |= mode == 26 ? HPVCD_TU_RDPCM_V : HPVCD_TU_RDPCM_H;
+            }
+        }
         t.flags = flags;
         if (flags & HPVCD_TU_CBF) {
             t.nx = make_levels(n, &t.coeff_off);

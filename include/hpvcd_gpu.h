@@ -61,6 +61,15 @@ typedef enum hpvcd_status {
 #define HPVCD_TU_TSKIP 0x02u /* transform_skip_flag                                  */
 #define HPVCD_TU_INTRA 0x04u /* block of an intra CU (prediction from neighbours)    */
 #define HPVCD_TU_TQB 0x08u   /* cu_transquant_bypass: residual = levels verbatim     */
+/* RExt residual modification of a transform-skip or transquant-bypass TB, as
+ * the host resolved it (decode.rs:4356-4374 rext_post_ops, applied by
+ * apply_rext_residual_ops, decode.rs:8418-8446): ROTATE reverses the 4x4
+ * residual (transform_skip_rotation_enabled, intra); RDPCM_V / RDPCM_H
+ * accumulate it down the columns / along the rows (implicit for intra modes
+ * 26 / 10, explicit_rdpcm_dir for inter CUs).  Ignored on other TBs. */
+#define HPVCD_TU_ROTATE 0x10u
+#define HPVCD_TU_RDPCM_H 0x20u
+#define HPVCD_TU_RDPCM_V 0x40u
 
 /*
  * One transform block, or one "mark decoded" record.  Records of a picture are

@@ -839,6 +839,28 @@ const uint8_t* scaling_select(const hpvcd_scaling* s, int comp, int n, bool inte
     return s->m[size_id][matrix_id];
 }
 
+// decode.rs:8418-8446 apply_rext_residual_ops: reverse the block, then
+// accumulate down the columns (dir 1) or along the rows (dir 0).  With i16
+// storage the reference adds in i16, wrapping (release arithmetic).
+void rext_residual_ops(int32_t* res, int n, bool rotate, int dir, bool i16s) {
+    if (rotate)
+        for (int i = 0; i < n * n / 2; ++i) std::swap(res[i], res[n * n - 1 - i]);
+    auto add = [i16s](int32_t a, int32_t b) -> int32_t {
+        return i16s ? (int32_t)(int16_t)(uint16_t)((uint32_t)a + (uint32_t)b) : a + b;
+    };
+    if (dir == 1) {
+        for (int y = 1; y < n; ++y)
+            for (int x = 0; x < n; ++x) res[y * n + x] = add(res[y * n + x], res[(y - 1) * n + x]);
+    } else if (dir == 0) {
+        for (int y = 0; y < n; ++y)
+            for (int x = 1; x < n; ++x) res[y * n + x] = add(res[y * n + x], res[y * n + x - 1]);
+    }
+}
+
+int rdpcm_dir(const hpvcd_tu& t) {
+    return (t.flags & HPVCD_TU_RDPCM_V) ? 1 : ((t.flags & HPVCD_TU_RDPCM_H) ? 0 : -1);
+}
+
 // Residual of one TB: decode.rs:4754-4802 (8-bit i16 path) and :4835-4903
 // (i32 path) for luma, :5313-5417 for chroma.
 void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_t* res) {
@@ -850,6 +872,7 @@ void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_
     for (int i = 0; i < n * n; ++i) lv[i] = p->coeffs[(size_t)t.coeff_off + i];
     if (t.flags & HPVCD_TU_TQB) {  // lossless: levels verbatim (saturated for i16 storage)
         for (int i = 0; i < n * n; ++i) res[i] = i16s ? clamp3(lv[i], -32768, 32767) : lv[i];
+        rext_residual_ops(res, n, (t.flags & HPVCD_TU_ROTATE) != 0, rdpcm_dir(t), i16s);
         return;
     }
     int qpp;
@@ -865,6 +888,7 @@ void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_
     if (t.flags & HPVCD_TU_TSKIP) {
         const orc_ts_params tp = ts_params(n, qpp, bd, false);
         dequant_ts(lv, n, tp, sc, sc_dc, i16s, res);
+        rext_residual_ops(res, n, (t.flags & HPVCD_TU_ROTATE) != 0, rdpcm_dir(t), i16s);
         return;
     }
     int32_t deq[32 * 32];
@@ -1203,6 +1227,10 @@ void orc_dequant(const int32_t* levels, int32_t n, const orc_dequant_params* p,
                  const uint8_t* scaling, int32_t dc, int32_t i16s, int32_t* out) {
     dequant(levels, n, *p, scaling, dc, i16s != 0, out);
 }
+void orc_rext_residual_ops(int32_t* res, int32_t n, int32_t rotate, int32_t dir, int32_t i16s) {
+    rext_residual_ops(res, n, rotate != 0, dir, i16s != 0);
+}
+
 int32_t orc_scaling_select(const hpvcd_scaling* s, int32_t comp, int32_t n, int32_t inter, int32_t tskip,
                            int32_t* first, int32_t* dc) {
     int d = 16;

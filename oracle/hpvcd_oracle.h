@@ -44,6 +44,9 @@ void orc_ts_params_get(int32_t n, int32_t qp_prime, int32_t bd, int32_t ext, orc
 void orc_dequant(const int32_t* levels, int32_t n, const orc_dequant_params* p,
                  const uint8_t* scaling /* NULL = flat */, int32_t scaling_dc, int32_t i16_store,
                  int32_t* out);
+/* decode.rs:8418-8446: rotate, then RDPCM (dir 1 vertical, 0 horizontal,
+ * -1 none), in place on an n*n residual. */
+void orc_rext_residual_ops(int32_t* res, int32_t n, int32_t rotate, int32_t dir, int32_t i16s);
 /* decode.rs:5874-5899: 1 and the selected list's first entry and DC when a
  * list applies, 0 for the flat scale. */
 int32_t orc_scaling_select(const hpvcd_scaling* s, int32_t comp, int32_t n, int32_t inter, int32_t tskip,

@@ -88,6 +88,14 @@ def dequant(levels, n, params, scaling=None, dc=16, i16=False, ts=False) -> np.n
     return out
 
 
+def rext_residual_ops(res, n, rotate=False, rdpcm=None, i16=False) -> np.ndarray:
+    """decode.rs:8418-8446 on a copy of `res` (rdpcm: None, 0 horizontal, 1 vertical)."""
+    r = np.ascontiguousarray(res, dtype=np.int32).reshape(-1).copy()
+    lib().orc_rext_residual_ops(_p(r), i32(n), i32(int(rotate)), i32(-1 if rdpcm is None else rdpcm),
+                                i32(int(i16)))
+    return r
+
+
 def scaling_select(scaling, comp, n, inter, tskip):
     """decode.rs:5874-5899: (first entry, DC) of the list a TB uses, or None
     for the flat scale.  `scaling` is an abi.Scaling."""

@@ -5,6 +5,7 @@ flat buffers and compares plane for plane (and the RGB8 canvas) with the
 oracle restatement of the reference's scalar decode.  Integer work: the
 tolerance is zero.
 """
+import ctypes
 import numpy as np
 import pytest
 
@@ -18,6 +19,8 @@ if not torch.cuda.is_available():  # pragma: no cover
 
 from hpvcd_b200.gpu import DevicePlan, GpuDecoder, split_planes  # noqa: E402
 from oracle import oracle as O  # noqa: E402
+
+C_u8 = ctypes.c_uint8
 
 
 @pytest.fixture(scope="module")
@@ -622,3 +625,30 @@ def test_scaling_lists_plan_and_server():
                 got[c["user"]] = c
     for k in (0, 1):
         assert np.array_equal(got[k]["image"], ref), k
+
+
+# --- RExt residual tools: rotation, implicit / explicit RDPCM, large TS -----
+@pytest.mark.parametrize("bd,idc", [(8, 1), (10, 3), (12, 1)])
+def test_rext_rotation_rdpcm_intra(dec, bd, idc):
+    s = synth.SynthSet()
+    for k in range(2):
+        c = synth.intra_cfg(180 + bd + k, 384, 256, bit_depth=bd, chroma_idc=idc, tskip_p=0.5, tqb_p=0.1,
+                            scaling=(k == 1))
+        c.rext = 7
+        c.tskip_log2_max = 5
+        s.add(c)
+    pics = s.pictures()
+    tus = np.concatenate([np.ctypeslib.as_array((C_u8 * (p.n_tus * 16)).from_address(p.tus))
+                          .view(abi.TU_DTYPE) for p in pics])
+    assert (tus["flags"] & abi.TU_ROTATE).any() and (tus["flags"] & (abi.TU_RDPCM_H | abi.TU_RDPCM_V)).any()
+    run_yuv(dec, pics, f"rext intra {bd}-bit idc {idc}")
+
+
+def test_rext_explicit_rdpcm_inter(dec):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(190, 320, 192, bit_depth=10))
+    for i in range(1, 4):
+        c = synth.inter_cfg(190 + i, 320, 192, bit_depth=10, weighted=(i == 2))
+        c.tskip_p, c.tqb_p, c.rext, c.tskip_log2_max = 0.5, 0.1, 7, 4
+        s.add(c)
+    run_yuv(dec, s.pictures(), "rext inter explicit rdpcm")

@@ -361,3 +361,21 @@ def test_scaled_dequant_upsamples_the_8x8_list(n):
     f = (p.factor // 16) * m
     want = np.clip((levels.astype(np.int64) * f + p.add) >> p.shift, p.clip_min, p.clip_max)
     assert np.array_equal(got, want)
+
+
+def test_rext_residual_ops():
+    # decode.rs:8418-8446: rotation reverses the block; vertical RDPCM adds
+    # the row above, horizontal the sample to the left; i16 storage wraps.
+    r = np.arange(16, dtype=np.int32)
+    assert np.array_equal(O.rext_residual_ops(r, 4, rotate=True), r[::-1])
+    v = O.rext_residual_ops(r, 4, rdpcm=1).reshape(4, 4)
+    assert np.array_equal(v, np.cumsum(r.reshape(4, 4), axis=0))
+    h = O.rext_residual_ops(r, 4, rdpcm=0).reshape(4, 4)
+    assert np.array_equal(h, np.cumsum(r.reshape(4, 4), axis=1))
+    both = O.rext_residual_ops(r, 4, rotate=True, rdpcm=0).reshape(4, 4)
+    assert np.array_equal(both, np.cumsum(r[::-1].reshape(4, 4), axis=1))
+    big = np.full(64, 30000, np.int32)
+    w = O.rext_residual_ops(big, 8, rdpcm=1, i16=True).reshape(8, 8)
+    want = (np.cumsum(big.reshape(8, 8).astype(np.int64), axis=0) + 32768) % 65536 - 32768
+    assert np.array_equal(w, want)
+    assert np.array_equal(O.rext_residual_ops(big, 8, rdpcm=1).reshape(8, 8), np.cumsum(big.reshape(8, 8), axis=0))
