@@ -53,6 +53,7 @@ PIC_SAO_LUMA = 0x0008
 PIC_SAO_CHROMA = 0x0010
 PIC_PRED_IN_PLANE = 0x0020
 PIC_INTER = 0x0040
+PIC_CROSS_COMPONENT = 0x0080
 PIC_STORE_MASK = 0x00FF0000
 
 
@@ -100,13 +101,13 @@ class Tu(C.Structure):
     _fields_ = [
         ("x", C.c_uint16), ("y", C.c_uint16), ("coeff_off", C.c_uint32),
         ("log2n", C.c_uint8), ("comp", C.c_uint8), ("flags", C.c_uint8), ("mode", C.c_uint8),
-        ("qp_y", C.c_int8), ("cqp_off", C.c_int8), ("nx", C.c_uint8), ("rsvd", C.c_uint8),
+        ("qp_y", C.c_int8), ("cqp_off", C.c_int8), ("nx", C.c_uint8), ("res_scale", C.c_int8),
     ]
 
 
 TU_DTYPE = np.dtype([
     ("x", "<u2"), ("y", "<u2"), ("coeff_off", "<u4"), ("log2n", "u1"), ("comp", "u1"),
-    ("flags", "u1"), ("mode", "u1"), ("qp_y", "i1"), ("cqp_off", "i1"), ("nx", "u1"), ("rsvd", "u1"),
+    ("flags", "u1"), ("mode", "u1"), ("qp_y", "i1"), ("cqp_off", "i1"), ("nx", "u1"), ("res_scale", "i1"),
 ])
 
 
@@ -237,6 +238,7 @@ class SynthCfg(C.Structure):
         ("mv_pad", C.c_float), ("weighted", C.c_uint32), ("n_refs", C.c_uint32),
         ("tu_mix", C.c_float * 4),
         ("scaling", C.c_uint32), ("rext", C.c_uint32), ("tskip_log2_max", C.c_uint32),
+        ("ccp_p", C.c_float),
     ]
 
 

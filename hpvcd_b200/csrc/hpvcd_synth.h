@@ -66,6 +66,9 @@ typedef struct hpvcd_synth_cfg {
     /* log2_max_transform_skip_block_size (2..5; 0 -> 2): transform skip is
      * drawn for coded TBs up to this size. */
     uint32_t tskip_log2_max;
+    /* 4:4:4 only: cross_component_prediction_enabled; probability that a
+     * chroma TB of a TU with coded luma gets a non-zero res_scale. */
+    float ccp_p;
 } hpvcd_synth_cfg;
 
 typedef struct hpvcd_synth hpvcd_synth;

@@ -23,6 +23,8 @@
 //     (chroma availability only depends on the luma `decoded` map, which
 //     each warp replays from the records), all in shared memory; finally
 //     the CTU is written out and its ready flag released.
+#include <climits>
+
 #include "common.cuh"
 
 namespace hpvcd {
@@ -137,13 +139,15 @@ constexpr int kResWarps = 8;
 // Residual of one coded TB by one warp (transform.rs:489-858, decode.rs
 // :4754-4903 luma, :5313-5417 chroma).  `emit(r, m, v)` receives every
 // residual sample (row r, column m) in the reference's storage semantics.
+// `allow16` false keeps 8-bit residuals in i32 storage (the reference's
+// path for chroma TBs with cross-component prediction, decode.rs:5313-5316).
 template <int kIdct, typename Emit>
 __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16_t* dct, int16_t* buf,
-                                 int16_t* tmp, int lane, Emit emit) {
+                                 int16_t* tmp, int lane, Emit emit, bool allow16 = true) {
     const int n = 1 << t.log2n;
     const bool luma = t.comp == 0;
     const int bd = luma ? P.bd : P.bd_c;
-    const bool i16s = bd <= 8;
+    const bool i16s = bd <= 8 && allow16;
     const int16_t* lv = P.coeffs + t.coeff_off;
     const uint32_t rext = t.flags & (HPVCD_TU_ROTATE | HPVCD_TU_RDPCM_H | HPVCD_TU_RDPCM_V);
     if ((t.flags & HPVCD_TU_TQB) && !rext) {  // decode.rs:4754-4757 / :4830-4834: residual = levels
@@ -371,6 +375,7 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
         const DevPic& P = pics[lo];
         const hpvcd_tu t = P.tus[g - rec_prefix[lo]];
         if (!(t.flags & HPVCD_TU_CBF)) continue;
+        if ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && t.comp && t.res_scale) continue;  // k_ccp's
         const int c = t.comp;
         const int ncomp = P.idc ? 3 : 1;
         const int n = 1 << t.log2n;
@@ -400,6 +405,86 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
                 if (x < pw && y < ph) rp[(size_t)y * rs + x] = (int16_t)sat16(v);
             });
         }
+    }
+}
+
+// ===========================================================================
+// k_ccp -- chroma TBs with cross-component prediction (RExt 4:4:4)
+// ===========================================================================
+// One warp per chroma TB with res_scale != 0 of a HPVCD_PIC_CROSS_COMPONENT
+// picture: it recomputes its TU's luma residual rY (the matrix inverse
+// transform, which keeps i32 values above 8 bits), then the chroma residual
+// in i32 storage (decode.rs:5286-5426; zero without coded residual,
+// :5428-5466), adds (res_scale * ((rY << BitDepthC) >> BitDepthY)) >> 3
+// (decode.rs:5488-5504) and writes it where k_residual would.
+constexpr int kCcpWarps = 4;
+
+__global__ void __launch_bounds__(kCcpWarps * 32)
+k_ccp(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_prefix, uint32_t n_pics,
+      uint32_t* dev_err) {
+    __shared__ int16_t dct[32 * 32];
+    __shared__ __align__(16) int16_t scr[kCcpWarps][2][32 * kScr];
+    __shared__ int32_t ry_all[kCcpWarps][32 * 32];
+    for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) dct[i] = (int16_t)dct_entry(32, i / 32, i % 32);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t* ry = ry_all[warp];
+    const uint32_t total = rec_prefix[n_pics];
+    for (uint32_t g = rec_prefix[0] + blockIdx.x * kCcpWarps + warp; g < total; g += gridDim.x * kCcpWarps) {
+        uint32_t lo = 0, hi = n_pics;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (rec_prefix[mid] <= g) lo = mid; else hi = mid;
+        }
+        const DevPic& P = pics[lo];
+        if (!(P.flags & HPVCD_PIC_CROSS_COMPONENT)) continue;
+        const uint32_t gl = g - rec_prefix[lo];
+        const hpvcd_tu t = P.tus[gl];
+        if (t.comp == 0 || t.res_scale == 0) continue;
+        const int n = 1 << t.log2n;
+        bool bad = P.idc != 3 || t.comp > 2 || t.log2n < 2 || t.log2n > 5 || (int)t.x >= P.cw ||
+                   (int)t.y >= P.ch ||
+                   ((t.flags & HPVCD_TU_CBF) && (uint64_t)t.coeff_off + (uint64_t)n * n > P.n_coeffs);
+        // the TU's luma TB: same place and size, among the three records before
+        hpvcd_tu lt{};
+        bool found = false;
+        for (uint32_t k = 1; k <= 3 && k <= gl && !found; ++k) {
+            lt = P.tus[gl - k];
+            found = lt.comp == 0 && lt.x == t.x && lt.y == t.y && lt.log2n == t.log2n;
+        }
+        bad = bad || !found || !(lt.flags & HPVCD_TU_CBF) ||
+              (uint64_t)lt.coeff_off + (uint64_t)n * n > P.n_coeffs;
+        if (bad) {
+            if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+            continue;
+        }
+        tb_residual_warp<kIdctMatrix>(P, lt, dct, scr[warp][0], scr[warp][1], lane,
+                                      [&](int r, int m, int v) { ry[r * n + m] = v; });
+        __syncwarp();
+        const int c = t.comp, x0 = t.x, y0 = t.y, pw = P.cw, ph = P.ch;
+        const int bdy = P.bd, bdc = P.bd_c, rs = t.res_scale;
+        const bool in_plane = (P.flags & HPVCD_PIC_PRED_IN_PLANE) || !(t.flags & HPVCD_TU_INTRA);
+        const int mx = (1 << bdc) - 1;
+        auto out = [&](int r, int m, long long v) {
+            const long long sy = ((long long)ry[r * n + m] << bdc) >> bdy;
+            v += (rs * sy) >> 3;
+            const int vv = (int)(v < INT_MIN ? INT_MIN : (v > INT_MAX ? INT_MAX : v));
+            const int x = x0 + m, y = y0 + r;
+            if (x >= pw || y >= ph) return;
+            if (in_plane) {
+                const size_t idx = (size_t)y * pw + x;
+                const long long s = (long long)load_sample(P.rec[c], P.bps, idx) + vv;
+                store_sample(P.rec[c], P.bps, idx, (int)(s < 0 ? 0 : (s > mx ? mx : s)));
+            } else {
+                P.res[c][(size_t)y * P.res_stride[c] + x] = (int16_t)sat16(vv);
+            }
+        };
+        if (t.flags & HPVCD_TU_CBF)
+            tb_residual_warp<kIdctMatrix>(P, t, dct, scr[warp][0], scr[warp][1], lane,
+                                          [&](int r, int m, int v) { out(r, m, v); }, false);
+        else
+            for (int i = lane; i < n * n; i += 32) out(i / n, i % n, 0);
+        __syncwarp();
     }
 }
 
@@ -1130,7 +1215,10 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     wn = recs[jn];
                 }
                 const int x = (int)t.x - (c ? ocx : oxl), y = (int)t.y - (c ? ocy : oyl);
-                const bool coded = (t.flags & HPVCD_TU_CBF) != 0;
+                // a chroma TB with cross-component prediction has a residual
+                // (written by k_ccp) even without coded coefficients
+                const bool coded = (t.flags & HPVCD_TU_CBF) != 0 ||
+                                   ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && c && t.res_scale);
                 if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
                     if (!helper) intra_tb_prep(k, t.log2n, t.mode, x, y, stamp, j, team_ws, lane);
                     team_sync(32 * kTeam);
@@ -1201,6 +1289,17 @@ extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const ui
     else
         hpvcd::k_residual<hpvcd::kIdctMatrix><<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix, n_pics,
                                                                                        dev_err);
+    hpvcd_note_launches(1);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t hpvcd_launch_ccp(const hpvcd::DevPic* pics, const uint32_t* rec_prefix, uint32_t n_pics,
+                                        uint32_t total_records, uint32_t* dev_err, int sms, cudaStream_t stream) {
+    if (total_records == 0) return cudaSuccess;
+    const uint32_t blocks_needed = (total_records + hpvcd::kCcpWarps - 1) / hpvcd::kCcpWarps;
+    const uint32_t cap = (uint32_t)sms * 8u;
+    const int grid = (int)(blocks_needed < cap ? blocks_needed : cap);
+    hpvcd::k_ccp<<<grid, hpvcd::kCcpWarps * 32, 0, stream>>>(pics, rec_prefix, n_pics, dev_err);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }

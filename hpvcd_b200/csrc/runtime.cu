@@ -20,6 +20,8 @@ using hpvcd::DevPic;
 
 extern "C" cudaError_t hpvcd_launch_residual(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int,
                                              int, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_ccp(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int,
+                                        cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int,
                                           int, int, cudaStream_t);
 extern "C" int hpvcd_recon_occupancy(int c444);
@@ -202,13 +204,19 @@ struct hpvcd_plan {
     GroupStreams own;                  // used when the plan is not lent a set
     const GroupStreams* gs = nullptr;  // the set the launches use
 
+    // whether a segment has cross-component pictures (k_ccp runs for it)
+    bool seg_ccp(const Segment& s) const {
+        for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
+            if ((src[i].flags & HPVCD_PIC_CROSS_COMPONENT) && src[i].n_tus) return true;
+        return false;
+    }
     uint32_t launches_for(uint32_t stages) const {
         uint32_t L = 0;
         for (const auto& s : segs) {
             if (stages & HPVCD_STAGE_RECON) {
                 for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
                     if ((src[i].flags & HPVCD_PIC_INTER) && src[i].n_pus) ++L;
-                if (rec_prefix[s.first_pic + s.n_pics] > rec_prefix[s.first_pic]) ++L;
+                if (rec_prefix[s.first_pic + s.n_pics] > rec_prefix[s.first_pic]) L += 1 + seg_ccp(s);
                 if (s.n_items) ++L;
             }
             if (stages & HPVCD_STAGE_DEBLOCK) L += (s.max_dbk_v > 0) + (s.max_dbk_h > 0);
@@ -667,6 +675,9 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             const uint32_t nrec = P->rec_prefix[s.first_pic + s.n_pics] - P->rec_prefix[s.first_pic];
             e = hpvcd_launch_residual(P->d_pics + s.first_pic, P->d_prefix + s.first_pic, s.n_pics, nrec, d_err,
                                       P->sms, (int)P->sched.idct, st);
+            if (e == cudaSuccess && nrec && P->seg_ccp(s))
+                e = hpvcd_launch_ccp(P->d_pics + s.first_pic, P->d_prefix + s.first_pic, s.n_pics, nrec, d_err,
+                                     P->sms, st);
             if (e != cudaSuccess) return cuda_status(e);
             int occ = P->recon_occ;
             if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
@@ -1740,6 +1751,8 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
         }
     const uint32_t* prefix = (const uint32_t*)(base + L.prefix);
     e = hpvcd_launch_residual(dp, prefix, 1, p.n_tus, d_err, nd->sms, 0, st);
+    if (e == cudaSuccess && (p.flags & HPVCD_PIC_CROSS_COMPONENT) && p.n_tus)
+        e = hpvcd_launch_ccp(dp, prefix, 1, p.n_tus, d_err, nd->sms, st);
     if (e != cudaSuccess) return cuda_status(e);
     if (d.needs_wavefront) {
         const int c444 = p.chroma_idc == 3 ? 1 : 0;

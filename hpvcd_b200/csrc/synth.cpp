@@ -110,8 +110,10 @@ struct Gen {
         return (uint8_t)(max_x + 1);
     }
 
-    void push_tb(int comp, int x, int y, int log2n, uint8_t flags, int mode, int qp, int cqp_off) {
+    void push_tb(int comp, int x, int y, int log2n, uint8_t flags, int mode, int qp, int cqp_off,
+                 int res_scale = 0) {
         hpvcd_tu t{};
+        t.res_scale = (int8_t)res_scale;
         t.x = (uint16_t)x;
         t.y = (uint16_t)y;
         t.log2n = (uint8_t)log2n;
@@ -222,10 +224,13 @@ struct Gen {
             return;
         }
         const int cmode = idc == 3 ? cmodes[q] : cmodes[0];
+        const bool ccp_on = c.ccp_p > 0.f && idc == 3 && cbf_l;
         for (int comp = 1; comp <= 2; ++comp) {
             const bool cbf = rng.bern(c.cbf_p);
-            if (!intra && !cbf) continue;
-            push_tb(comp, cx, cy, clog2, base | (cbf ? HPVCD_TU_CBF : 0), cmode, qp, 0);
+            int rs = 0;  // cross_comp_pred ResScaleVal
+            if (ccp_on && rng.bern(c.ccp_p)) rs = (rng.bern(0.5) ? -1 : 1) * (1 << rng.range(0, 3));
+            if (!intra && !cbf && !rs) continue;
+            push_tb(comp, cx, cy, clog2, base | (cbf ? HPVCD_TU_CBF : 0), cmode, qp, 0, rs);
         }
     }
 
@@ -462,6 +467,7 @@ struct Gen {
         d.bit_depth_y = d.bit_depth_c = (uint8_t)bd;
         d.log2_ctb = (uint8_t)log2_ctb;
         d.flags = c.pic_flags;
+        if (c.ccp_p > 0.f && idc == 3) d.flags |= HPVCD_PIC_CROSS_COMPONENT;
         d.beta_offset_div2 = (int8_t)c.beta_offset_div2;
         d.tc_offset_div2 = (int8_t)c.tc_offset_div2;
         d.pps_cb_qp_offset = (int8_t)c.cb_qp_offset;

@@ -98,7 +98,8 @@ typedef struct hpvcd_tu {
     int8_t qp_y;        /* QpY of the coding unit (may be negative, bd > 8)    */
     int8_t cqp_off;     /* chroma TBs: slice + CU chroma QP offset             */
     uint8_t nx;         /* max_x + 1 from residual_coding (columns >= nx zero) */
-    uint8_t rsvd;
+    int8_t res_scale;   /* chroma TBs of HPVCD_PIC_CROSS_COMPONENT pictures:   */
+                        /* ResScaleVal of cross_comp_pred (0, +-1, 2, 4, 8)    */
 } hpvcd_tu; /* 16 bytes */
 
 /* hpvcd_cell.flags */
@@ -181,6 +182,12 @@ typedef struct hpvcd_scaling {
 #define HPVCD_PIC_PRED_IN_PLANE 0x0020u      /* planes hold the prediction on entry:   */
                                              /* every TB only adds its residual        */
 #define HPVCD_PIC_INTER 0x0040u              /* picture has motion-compensated PUs     */
+/* cross_component_prediction_enabled_flag (4:4:4): a chroma TB with
+ * res_scale != 0 adds (res_scale * ((rY << BitDepthC) >> BitDepthY)) >> 3 of
+ * its TU's luma residual rY (decode.rs:5488-5504), also when it has no coded
+ * residual of its own (decode.rs:5428).  The TU's luma TB is one of the three
+ * records before the chroma record. */
+#define HPVCD_PIC_CROSS_COMPONENT 0x0080u
 /* Store the decoded picture into entry e of the context's DPB (hpvcd_dpb)
  * after it is reconstructed; bits 16..23 of flags, 0 = no store. */
 #define HPVCD_PIC_STORE_DPB(e) ((uint32_t)((e) + 1) << 16)

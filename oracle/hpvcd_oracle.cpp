@@ -863,11 +863,13 @@ int rdpcm_dir(const hpvcd_tu& t) {
 
 // Residual of one TB: decode.rs:4754-4802 (8-bit i16 path) and :4835-4903
 // (i32 path) for luma, :5313-5417 for chroma.
-void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_t* res) {
+// `allow16` false: i32 storage at 8 bits (chroma TBs with cross-component
+// prediction, decode.rs:5313-5316).
+void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_t* res, bool allow16 = true) {
     const int n = 1 << t.log2n;
     const bool luma = t.comp == 0;
     const int bd = luma ? g.bd : g.bd_c;
-    const bool i16s = bd <= 8;
+    const bool i16s = bd <= 8 && allow16;
     int32_t lv[32 * 32];
     for (int i = 0; i < n * n; ++i) lv[i] = p->coeffs[(size_t)t.coeff_off + i];
     if (t.flags & HPVCD_TU_TQB) {  // lossless: levels verbatim (saturated for i16 storage)
@@ -911,19 +913,31 @@ int recon_picture(const hpvcd_picture* p, orc_planes* pl) {
     const bool pred_in_plane = (p->flags & HPVCD_PIC_PRED_IN_PLANE) != 0;
     uint16_t pred[64 * 64];
     int32_t res[32 * 32];
+    int32_t cc_luma[32 * 32];  // decode.rs:279 cross_comp_luma: the last coded luma residual
+    const bool ccp_pic = (p->flags & HPVCD_PIC_CROSS_COMPONENT) != 0;
     for (uint32_t i = 0; i < p->n_tus; ++i) {
         const hpvcd_tu& t = p->tus[i];
         const int n = 1 << t.log2n;
         if (t.comp > 2 || (t.comp > 0 && g.idc == 0)) return HPVCD_ERR_BITSTREAM;
+        const bool ccp = ccp_pic && t.comp > 0 && t.res_scale != 0;
         const bool coded = (t.flags & HPVCD_TU_CBF) != 0;
         const bool intra = (t.flags & HPVCD_TU_INTRA) != 0;
-        if (t.log2n < 2 || t.log2n > 6 || (coded && t.log2n > 5)) return HPVCD_ERR_BITSTREAM;
+        if (t.log2n < 2 || t.log2n > 6 || ((coded || ccp) && t.log2n > 5)) return HPVCD_ERR_BITSTREAM;
         if (coded && (uint64_t)t.coeff_off + (uint64_t)n * n > p->n_coeffs) return HPVCD_ERR_BITSTREAM;
+        if (ccp) {  // the TU's coded luma TB is among the three records before
+            bool found = false;
+            for (uint32_t k = 1; k <= 3 && k <= i && !found; ++k) {
+                const hpvcd_tu& l = p->tus[i - k];
+                found = l.comp == 0 && l.x == t.x && l.y == t.y && l.log2n == t.log2n &&
+                        (l.flags & HPVCD_TU_CBF);
+            }
+            if (!found || g.idc != 3) return HPVCD_ERR_BITSTREAM;
+        }
         const bool luma = t.comp == 0;
         uint16_t* plane = luma ? pl->y : (t.comp == 1 ? pl->cb : pl->cr);
         const int pw = luma ? g.w : g.cw, ph = luma ? g.h : g.ch;
         const int bd = luma ? g.bd : g.bd_c;
-        if (!coded && !intra) {  // end of an inter CU / residual-free inter TB
+        if (!coded && !intra && !ccp) {  // end of an inter CU / residual-free inter TB
             if (luma) st.mark_decoded(t.x, t.y, n);
             continue;
         }
@@ -934,9 +948,18 @@ int recon_picture(const hpvcd_picture* p, orc_planes* pl) {
         const int vw = std::min(std::max(pw - (int)t.x, 0), n);
         const int vh = std::min(std::max(ph - (int)t.y, 0), n);
         if (coded) {
-            tb_residual(p, g, t, res);
+            tb_residual(p, g, t, res, !ccp);
         } else {
             for (int k = 0; k < n * n; ++k) res[k] = 0;  // predict_only: copy (add zero)
+        }
+        if (ccp_pic && t.comp == 0 && coded)
+            for (int k = 0; k < n * n; ++k) cc_luma[k] = res[k];
+        if (ccp) {  // decode.rs:5488-5504 apply_cross_comp_residual
+            for (int k = 0; k < n * n; ++k) {
+                const int64_t sy = ((int64_t)cc_luma[k] << g.bd_c) >> g.bd;
+                const int64_t v = (int64_t)res[k] + ((t.res_scale * sy) >> 3);
+                res[k] = (int32_t)clamp3<int64_t>(v, INT32_MIN, INT32_MAX);
+            }
         }
         if (vw > 0 && vh > 0)
             add_residual(plane + (size_t)t.y * pw + t.x, pw, pred, res, n, vw, vh, bd);

@@ -652,3 +652,43 @@ def test_rext_explicit_rdpcm_inter(dec):
         c.tskip_p, c.tqb_p, c.rext, c.tskip_log2_max = 0.5, 0.1, 7, 4
         s.add(c)
     run_yuv(dec, s.pictures(), "rext inter explicit rdpcm")
+
+
+# --- cross-component prediction (4:4:4 RExt) -------------------------------
+@pytest.mark.parametrize("bd", [8, 10, 12])
+def test_cross_component_intra(dec, bd):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(200 + bd, 384, 256, bit_depth=bd, chroma_idc=3, tskip_p=0.2, tqb_p=0.05)
+    c.ccp_p = 0.6
+    s.add(c)
+    c2 = synth.intra_cfg(210 + bd, 256, 256, bit_depth=bd, chroma_idc=3, tskip_p=0.3, tqb_p=0.05, scaling=True,
+                         cbf_p=0.5)
+    c2.ccp_p, c2.rext, c2.tskip_log2_max = 0.6, 7, 5
+    s.add(c2)
+    pics = s.pictures()
+    assert all(p.flags & abi.PIC_CROSS_COMPONENT for p in pics)
+    tus = np.ctypeslib.as_array((C_u8 * (pics[1].n_tus * 16)).from_address(pics[1].tus)).view(abi.TU_DTYPE)
+    ccp_only = (tus["res_scale"] != 0) & ((tus["flags"] & abi.TU_CBF) == 0)
+    assert ccp_only.any()           # chroma residual from luma alone
+    run_yuv(dec, pics, f"cross-component {bd}-bit")
+
+
+def test_cross_component_inter_and_plan(dec):
+    s = synth.SynthSet()
+    c0 = synth.intra_cfg(220, 320, 192, bit_depth=10, chroma_idc=3)
+    c0.ccp_p = 0.5
+    s.add(c0)
+    for i in range(1, 4):
+        c = synth.inter_cfg(220 + i, 320, 192, bit_depth=10, weighted=(i == 2))
+        c.chroma_idc = 3
+        c.ccp_p, c.tskip_p, c.rext = 0.5, 0.3, 7
+        s.add(c)
+    pics = s.pictures()
+    run_yuv(dec, pics, "cross-component inter")
+    ref, _ = O.decode_batch(pics)
+    plan = DevicePlan(pics)
+    plan.launch()
+    torch.cuda.synchronize()
+    assert plan.status() == abi.OK
+    assert_planes_equal([plan.planes(i) for i in range(len(pics))], ref, "cross-component plan")
+    plan.close()

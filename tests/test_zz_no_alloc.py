@@ -68,6 +68,10 @@ def _pictures():
         synth.intra_cfg(9104, 384, 256, bit_depth=12, chroma_idc=0),            # 4:0:0
     ]
     cfgs[3].log2_ctb = 4
+    # 4:4:4 with cross-component prediction, RExt rotation / RDPCM and scaling lists
+    rx = synth.intra_cfg(9105, 256, 192, bit_depth=10, chroma_idc=3, tskip_p=0.3, tqb_p=0.05, scaling=True)
+    rx.ccp_p, rx.rext, rx.tskip_log2_max = 0.5, 7, 5
+    cfgs.append(rx)
     for c in cfgs:
         s.add(c)
     return s, s.pictures()
@@ -93,7 +97,7 @@ def test_noalloc_matches_plan_entry_point_on_consecutive_calls():
 
     # consecutive calls on one stream, no synchronisation between them; the
     # first picture twice to show the scratch is reset per call
-    order = [0, 1, 2, 3, 0]
+    order = [0, 1, 2, 3, 4, 0]
     outs = [NoAllocOut(torch, pics[i]) for i in order]
     torch.cuda.synchronize()
     free1 = torch.cuda.mem_get_info()[0]
