@@ -504,32 +504,37 @@ struct WalkScratch {
 };
 
 // Shared-memory layout of one CTA.  Each component has one bordered canvas:
-// row 0 is the row above the CTU (x = -1 .. 2S-1), rows 1..S the CTU, column
-// 7 the column left of the CTU; sample (x, y) is at (y + 1) * CW + x + 8, so
-// the interior rows start 16-byte aligned.
+// row 0 is the row above the CTU (x = -1 .. 2S-1 for a CTU S wide), rows
+// 1..Sh the CTU, column 7 the column left of the CTU; sample (x, y) is at
+// (y + 1) * CW + x + 8, so the interior rows start 16-byte aligned.
 // Records of one CTU staged at once: up to 256 luma TBs, one "mark decoded"
 // record per inter CU (64 at most) and the chroma TBs (64 per component at
-// 4:2:0, 256 at 4:4:4).  A CTU with more records is malformed.
+// 4:2:0, 128 at 4:2:2, 256 at 4:4:4).  A CTU with more records is malformed.
+// Chroma formats of a layout: kFmt420 (also 4:0:0), kFmt444, kFmt422; the
+// 4:4:4 layout holds every format, the 4:2:2 one also 4:2:0.
+constexpr int kFmt420 = 0, kFmt444 = 1, kFmt422 = 2;
 constexpr int kRecCap420 = 256 + 64 + 2 * 64;
+constexpr int kRecCap422 = 256 + 64 + 2 * 128;
 constexpr int kRecCap444 = 256 + 64 + 2 * 256;
 constexpr int kListCap = 256;  // intra TBs of one component in one CTU
 constexpr uint32_t kNoStamp = 0xffffffffu;
 
 struct ReconLayout {
-    int cs;       // chroma canvas side
-    int rec_cap;  // staged records
+    int cs_w, cs_h;  // chroma canvas width and height (CTU interior)
+    int rec_cap;     // staged records
     size_t off_can_y, off_can_c, off_res_y, off_res_c, off_ws, off_recs, off_stamp, off_lists, off_misc, total;
     static __host__ __device__ int cw_of(int S) { return 2 * S + 8; }
-    __host__ __device__ explicit ReconLayout(int c444) {
-        cs = c444 ? 64 : 32;
-        rec_cap = c444 ? kRecCap444 : kRecCap420;
+    __host__ __device__ explicit ReconLayout(int cfmt) {
+        cs_w = cfmt == kFmt444 ? 64 : 32;
+        cs_h = cfmt == kFmt420 ? 32 : 64;
+        rec_cap = cfmt == kFmt444 ? kRecCap444 : (cfmt == kFmt422 ? kRecCap422 : kRecCap420);
         size_t o = 0;
         off_can_y = o; o += (size_t)65 * cw_of(64) * sizeof(uint16_t);
         o = (o + 15) & ~(size_t)15;
-        off_can_c = o; o += 2 * (size_t)(cs + 1) * cw_of(cs) * sizeof(uint16_t);
+        off_can_c = o; o += 2 * (size_t)(cs_h + 1) * cw_of(cs_w) * sizeof(uint16_t);
         o = (o + 15) & ~(size_t)15;
         off_res_y = o; o += 64 * 64 * sizeof(int16_t);
-        off_res_c = o; o += 2 * (size_t)cs * cs * sizeof(int16_t);
+        off_res_c = o; o += 2 * (size_t)cs_w * cs_h * sizeof(int16_t);
         off_ws = o;    o += kReconWarps * sizeof(WalkScratch);
         o = (o + 15) & ~(size_t)15;
         off_recs = o;  o += (size_t)rec_cap * sizeof(hpvcd_tu);
@@ -551,7 +556,8 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 struct Comp {
     int ox, oy;   // CTU origin in component samples
     int pw, ph;   // plane size
-    int S, CW;    // CTU side in component samples, canvas row stride
+    int S, Sh;    // CTU width (also the residual canvas stride) and height in component samples
+    int CW;       // canvas row stride
     int sw, sh;   // luma samples per component sample (1 or 2)
     int bd, max_v;
     bool luma, filt, smoothing, strong;
@@ -577,15 +583,15 @@ __device__ __forceinline__ bool gather_ref(const Comp& k, const uint32_t* stamp,
     const int ax = k.ox + x, ay = k.oy + y;
     // both loads from clamped (always valid) positions, issued together;
     // the availability test picks the result
-    const int ys = min(max(y, 0), k.S - 1), xs = min(max(x, 0), k.S - 1);
+    const int ys = min(max(y, 0), k.Sh - 1), xs = min(max(x, 0), k.S - 1);
     const uint32_t st = stamp[((ys * k.sh) >> 2) * 16 + ((xs * k.sw) >> 2)];
-    const int cv = k.can[cidx(k, x, min(y, k.S - 1))];
+    const int cv = k.can[cidx(k, x, min(y, k.Sh - 1))];
     bool a = ax >= 0 && ay >= 0 && ax < k.pw && ay < k.ph;
     if (y >= 0) {
         if (x < 0)
-            a = a && y < k.S;  // left CTU (below-left CTU is not reconstructed yet)
+            a = a && y < k.Sh;  // left CTU (below-left CTU is not reconstructed yet)
         else
-            a = a && x < k.S && y < k.S && st < jrec;
+            a = a && x < k.S && y < k.Sh && st < jrec;
     }
     *v = a ? cv : 0;
     return a;
@@ -988,10 +994,10 @@ __device__ __forceinline__ void team_sync(int threads) {
 template <int kTeam>
 __global__ void __launch_bounds__(kReconThreads, 4)
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
-        uint32_t* work_counter, uint32_t* dev_err, int c444, uint32_t spin_limit) {
+        uint32_t* work_counter, uint32_t* dev_err, int cfmt, uint32_t spin_limit) {
     static_assert(kTeam == 1 || kTeam == 2, "team of one or two warps");
     extern __shared__ __align__(16) unsigned char smem[];
-    const ReconLayout lay(c444);
+    const ReconLayout lay(cfmt);
     uint32_t* s_item = (uint32_t*)(smem + lay.off_misc);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (;;) {
@@ -1005,7 +1011,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         const int ctb = 1 << P.log2_ctb;
         const int ncomp = P.idc ? 3 : 1;
         const int oxl = it.cx * ctb, oyl = it.cy * ctb;
-        const int ocx = oxl / P.sub_w, ocy = oyl / P.sub_h, Sc = ctb / P.sub_w;
+        // chroma CTU: Scw x Sch samples (4:2:2: half as wide as tall)
+        const int ocx = oxl / P.sub_w, ocy = oyl / P.sub_h, Scw = ctb / P.sub_w, Sch = ctb / P.sub_h;
         const uint32_t ci = (uint32_t)it.cy * P.ctb_cols + it.cx;
         uint32_t r0 = P.ctu_start[ci], r1 = P.ctu_start[ci + 1];
         if (r1 > P.n_tus || r0 > r1) {  // malformed CTU range: report, reconstruct nothing
@@ -1025,17 +1032,17 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         auto can_of = [&](int c) -> uint16_t* {
             return c == 0 ? (uint16_t*)(smem + lay.off_can_y)
                           : (uint16_t*)(smem + lay.off_can_c) +
-                                (size_t)(c - 1) * (lay.cs + 1) * ReconLayout::cw_of(lay.cs);
+                                (size_t)(c - 1) * (lay.cs_h + 1) * ReconLayout::cw_of(lay.cs_w);
         };
         auto res_of = [&](int c) -> int16_t* {
             return c == 0 ? (int16_t*)(smem + lay.off_res_y)
-                          : (int16_t*)(smem + lay.off_res_c) + (size_t)(c - 1) * lay.cs * lay.cs;
+                          : (int16_t*)(smem + lay.off_res_c) + (size_t)(c - 1) * lay.cs_w * lay.cs_h;
         };
         // ---- prefetch the residual canvases (cp.async, 8 samples per copy) ----
         for (int c = 0; c < ncomp; ++c) {
-            const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+            const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
             const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
-            const int rows = min(S, ph - oy), cols = min(S, pw - ox);
+            const int rows = min(Sh, ph - oy), cols = min(S, pw - ox);
             const int chunks = (cols + 7) >> 3;
             const int16_t* src = P.res[c] + (size_t)oy * P.res_stride[c] + ox;
             int16_t* dst = res_of(c);
@@ -1068,8 +1075,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             const int n = 1 << t.log2n;
             x = (int)t.x - (tc ? ocx : oxl);
             y = (int)t.y - (tc ? ocy : oyl);
-            const int St = tc ? Sc : ctb;
-            return (x < 0 || y < 0 || x + n > St || y + n > St) ? 0 : 1;
+            const int Sw = tc ? Scw : ctb, Sh = tc ? Sch : ctb;
+            return (x < 0 || y < 0 || x + n > Sw || y + n > Sh) ? 0 : 1;
         };
         for (uint32_t i = tid; i < nrec; i += kReconThreads) {
             hpvcd_tu t;
@@ -1124,11 +1131,11 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         // samples; load the CTU interior so intra TBs can predict from it.
         if (P.flags & HPVCD_PIC_INTER) {
             for (int c = 0; c < ncomp; ++c) {
-                const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+                const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
                 const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
                 uint16_t* can = can_of(c);
                 const int CW = ReconLayout::cw_of(S);
-                for (int i = tid; i < S * S; i += kReconThreads) {
+                for (int i = tid; i < S * Sh; i += kReconThreads) {
                     const int y = i / S, x = i % S;
                     const int ax = ox + x, ay = oy + y;
                     int v = 0;
@@ -1158,11 +1165,11 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         }
         __syncthreads();
         for (int c = 0; c < ncomp; ++c) {
-            const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+            const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
             const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
             uint16_t* can = can_of(c);
             const int CW = ReconLayout::cw_of(S);
-            for (int i = tid; i < 3 * S + 1; i += kReconThreads) {
+            for (int i = tid; i < 2 * S + 1 + Sh; i += kReconThreads) {
                 if (i < 2 * S + 1) {  // row above: x = i - 1
                     const int ax = ox + i - 1, ay = oy - 1;
                     int v = 0;
@@ -1185,7 +1192,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             WalkScratch& ws = ((WalkScratch*)(smem + lay.off_ws))[warp];
             WalkScratch& team_ws = ((WalkScratch*)(smem + lay.off_ws))[0];
             Comp k;
-            k.S = c ? Sc : ctb;
+            k.S = c ? Scw : ctb;
+            k.Sh = c ? Sch : ctb;
             k.CW = ReconLayout::cw_of(k.S);
             k.ox = c ? ocx : oxl;
             k.oy = c ? ocy : oyl;
@@ -1238,11 +1246,11 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         __syncthreads();
         // ---- publish the CTU (8 samples per store when rows allow) ----
         for (int c = 0; c < ncomp; ++c) {
-            const int S = c ? Sc : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+            const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
             const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
             const uint16_t* can = can_of(c);
             const int CW = ReconLayout::cw_of(S);
-            const int rows = min(S, ph - oy), cols = min(S, pw - ox);
+            const int rows = min(Sh, ph - oy), cols = min(S, pw - ox);
             if ((pw & 7) == 0 && (cols & 7) == 0) {
                 const int chunks = cols >> 3;
                 for (int i = tid; i < rows * chunks; i += kReconThreads) {
@@ -1274,7 +1282,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
 
 }  // namespace hpvcd
 
-extern "C" size_t hpvcd_recon_smem_bytes(int c444) { return hpvcd::ReconLayout(c444).total; }
+extern "C" size_t hpvcd_recon_smem_bytes(int cfmt) { return hpvcd::ReconLayout(cfmt).total; }
 
 extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const uint32_t* rec_prefix,
                                              uint32_t n_pics, uint32_t total_records, uint32_t* dev_err,
@@ -1306,31 +1314,31 @@ extern "C" cudaError_t hpvcd_launch_ccp(const hpvcd::DevPic* pics, const uint32_
 
 extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd::CtuItem* items,
                                           uint32_t n_items, uint32_t* work_counter, uint32_t* dev_err,
-                                          int c444, int grid, int team, cudaStream_t stream) {
+                                          int cfmt, int grid, int team, cudaStream_t stream) {
     if (n_items == 0) return cudaSuccess;
     // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
     // when the plan was built (no non-stream API call here, so launches can
     // be captured into CUDA graphs)
-    const size_t smem = hpvcd::ReconLayout(c444).total;
+    const size_t smem = hpvcd::ReconLayout(cfmt).total;
     // 2^22 polls of >= 64 ns each bound one neighbour wait to a few hundred ms.
     if (team == 2)
         hpvcd::k_recon<2><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                        dev_err, c444, 1u << 22);
+                                                                        dev_err, cfmt, 1u << 22);
     else
         hpvcd::k_recon<1><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                        dev_err, c444, 1u << 22);
+                                                                        dev_err, cfmt, 1u << 22);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }
 
-extern "C" int hpvcd_recon_occupancy(int c444) {
+extern "C" int hpvcd_recon_occupancy(int cfmt) {
     int blocks = 0;
-    // raise the limit for the larger layout, which covers both
-    const size_t smem = hpvcd::ReconLayout(c444).total;
+    // raise the limit for the 4:4:4 layout, which covers every format
+    const size_t smem = hpvcd::ReconLayout(cfmt).total;
     cudaFuncSetAttribute(hpvcd::k_recon<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)hpvcd::ReconLayout(1).total);
+                         (int)hpvcd::ReconLayout(hpvcd::kFmt444).total);
     cudaFuncSetAttribute(hpvcd::k_recon<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)hpvcd::ReconLayout(1).total);
+                         (int)hpvcd::ReconLayout(hpvcd::kFmt444).total);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<1>, hpvcd::kReconThreads, smem);
     return blocks;
 }

@@ -24,7 +24,7 @@ extern "C" cudaError_t hpvcd_launch_ccp(const DevPic*, const uint32_t*, uint32_t
                                         cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int,
                                           int, int, cudaStream_t);
-extern "C" int hpvcd_recon_occupancy(int c444);
+extern "C" int hpvcd_recon_occupancy(int cfmt);
 extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, uint8_t*, cudaStream_t);
@@ -50,8 +50,8 @@ Geo geo_of(const hpvcd_picture& p) {
     Geo g;
     g.w = (int)p.width;
     g.h = (int)p.height;
-    g.sub_w = p.chroma_idc == 1 ? 2 : 1;
-    g.sub_h = p.chroma_idc == 1 ? 2 : 1;
+    g.sub_w = p.chroma_idc == 1 || p.chroma_idc == 2 ? 2 : 1;  // SubWidthC
+    g.sub_h = p.chroma_idc == 1 ? 2 : 1;                        // SubHeightC
     g.cw = p.chroma_idc ? (g.w + g.sub_w - 1) / g.sub_w : 0;
     g.ch = p.chroma_idc ? (g.h + g.sub_h - 1) / g.sub_h : 0;
     g.gw = (g.w + 3) / 4;
@@ -68,7 +68,7 @@ Geo geo_of(const hpvcd_picture& p) {
 hpvcd_status validate(const hpvcd_picture& p) {
     if (p.width == 0 || p.height == 0 || p.width > 16384 || p.height > 16384) return HPVCD_ERR_LIMIT;
     if ((p.width & 7) || (p.height & 7)) return HPVCD_ERR_BITSTREAM;
-    if (p.chroma_idc == 2 || p.chroma_idc > 3) return HPVCD_ERR_UNSUPPORTED;
+    if (p.chroma_idc > 3) return HPVCD_ERR_UNSUPPORTED;
     if (p.bit_depth_y < 8 || p.bit_depth_y > 12 || p.bit_depth_c < 8 || p.bit_depth_c > 12)
         return HPVCD_ERR_UNSUPPORTED;
     if ((p.bit_depth_y == 8) != (p.bit_depth_c == 8)) return HPVCD_ERR_UNSUPPORTED;
@@ -186,7 +186,7 @@ struct hpvcd_plan {
     std::vector<hpvcd_canvas> canvases;   // resolved canvas list (>= 1 for RGB8)
     std::vector<uint64_t> canvas_offs;
     hpvcd_sched sched{};
-    int c444 = 0;
+    int cfmt = 0;  // k_recon shared-memory layout: 0 4:2:0 / 4:0:0, 1 4:4:4 (fits all), 2 4:2:2
     int recon_occ = 1;  // k_recon CTAs per SM at full occupancy
     int sms = 148;
     int max_rgb = 0;  // largest RGB job of one picture, in 4-pixel quads
@@ -336,6 +336,25 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         const hpvcd_status s = validate(pics[i]);
         if (s != HPVCD_OK) return s;
     }
+    // Motion compensation reads a reference with the current picture's
+    // geometry, so every reference of a picture with PUs has its size and
+    // sample format (as in any conforming stream).
+    for (uint32_t i = 0; i < n; ++i) {
+        const hpvcd_picture& p = pics[i];
+        if (!(p.flags & HPVCD_PIC_INTER) || !p.n_pus) continue;
+        for (int l = 0; l < 2; ++l)
+            for (int r = 0; r < HPVCD_MAX_REFS; ++r) {
+                const int sv = p.ref_slot[l][r];
+                if (sv < 0 || (uint32_t)sv >= i) continue;
+                const hpvcd_picture& q = pics[sv];
+                if (q.width != p.width || q.height != p.height || q.chroma_idc != p.chroma_idc ||
+                    q.bit_depth_y != p.bit_depth_y || q.bit_depth_c != p.bit_depth_c) {
+                    std::snprintf(t_last_error, sizeof(t_last_error),
+                                  "picture %u references picture %d of another size or format", i, sv);
+                    return HPVCD_ERR_BITSTREAM;
+                }
+            }
+    }
     if (out && out->kind == HPVCD_OUT_RGB8 &&
         (!out->place || (out->n_canvases ? !out->canvases : (out->canvas_w == 0 || out->canvas_h == 0))))
         return HPVCD_ERR_INVALID_ARG;
@@ -379,7 +398,8 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     }
     bool any_inter = false;
     for (uint32_t i = 0; i < n; ++i) {
-        if (pics[i].chroma_idc == 3) P->c444 = 1;
+        if (pics[i].chroma_idc == 3) P->cfmt = 1;
+        if (pics[i].chroma_idc == 2 && P->cfmt == 0) P->cfmt = 2;
         if (pics[i].flags & HPVCD_PIC_INTER) any_inter = true;
     }
     // ---- planes + scratch layout ----
@@ -615,7 +635,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
     P->sms = sms;
-    P->recon_occ = std::max(1, hpvcd_recon_occupancy(P->c444));
+    P->recon_occ = std::max(1, hpvcd_recon_occupancy(P->cfmt));
     if (P->concurrent) {
         GroupStreams* set = lend ? lend : &P->own;
         const cudaError_t ce = set->create();
@@ -685,7 +705,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             const int share = P->concurrent ? std::max(1, P->sms * occ / (int)n_seg) : P->sms * occ;
             const int grid = std::max(1, std::min<int>(share, (int)s.n_items));
             e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
-                                   P->c444, grid, (int)P->sched.luma_team, st);
+                                   P->cfmt, grid, (int)P->sched.luma_team, st);
             if (e != cudaSuccess) return cuda_status(e);
         }
         if (stages & HPVCD_STAGE_DEBLOCK) {
@@ -1577,7 +1597,7 @@ constexpr int kNoAllocMaxDevices = 64;
 struct NoAllocDevice {
     unsigned char* base = nullptr;  // address of g_noalloc_scratch on this device
     int sms = 0;
-    int occ[2] = {0, 0};            // k_recon CTAs per SM (4:2:0 layout, 4:4:4 layout)
+    int occ[3] = {0, 0, 0};         // k_recon CTAs per SM (4:2:0, 4:4:4, 4:2:2 layouts)
     bool ready = false;
 };
 std::mutex g_noalloc_mu;
@@ -1614,7 +1634,7 @@ hpvcd_status noalloc_setup(int dev, NoAllocDevice** out) {
         if (e != cudaSuccess) return cuda_status(e);
         e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return cuda_status(e);
-        for (int c444 = 0; c444 < 2; ++c444) d.occ[c444] = std::max(1, hpvcd_recon_occupancy(c444));
+        for (int f = 0; f < 3; ++f) d.occ[f] = std::max(1, hpvcd_recon_occupancy(f));
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_status(e);
         d.base = (unsigned char*)p;
@@ -1755,9 +1775,9 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
         e = hpvcd_launch_ccp(dp, prefix, 1, p.n_tus, d_err, nd->sms, st);
     if (e != cudaSuccess) return cuda_status(e);
     if (d.needs_wavefront) {
-        const int c444 = p.chroma_idc == 3 ? 1 : 0;
-        const int grid = std::max(1, std::min<int>(nd->sms * nd->occ[c444], (int)n_ctu));
-        e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, c444, grid, 1,
+        const int cfmt = p.chroma_idc == 3 ? 1 : (p.chroma_idc == 2 ? 2 : 0);
+        const int grid = std::max(1, std::min<int>(nd->sms * nd->occ[cfmt], (int)n_ctu));
+        e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, cfmt, grid, 1,
                                st);
         if (e != cudaSuccess) return cuda_status(e);
     }

@@ -71,8 +71,8 @@ struct Gen {
         w = (int)c.width;
         h = (int)c.height;
         idc = (int)c.chroma_idc;
-        sub_w = idc == 1 ? 2 : 1;
-        sub_h = idc == 1 ? 2 : 1;
+        sub_w = idc == 1 || idc == 2 ? 2 : 1;  // SubWidthC
+        sub_h = idc == 1 ? 2 : 1;              // SubHeightC
         gw = (w + 3) / 4;
         gh = (h + 3) / 4;
         bd = (int)c.bit_depth;
@@ -225,13 +225,17 @@ struct Gen {
         }
         const int cmode = idc == 3 ? cmodes[q] : cmodes[0];
         const bool ccp_on = c.ccp_p > 0.f && idc == 3 && cbf_l;
-        for (int comp = 1; comp <= 2; ++comp) {
-            const bool cbf = rng.bern(c.cbf_p);
-            int rs = 0;  // cross_comp_pred ResScaleVal
-            if (ccp_on && rng.bern(c.ccp_p)) rs = (rng.bern(0.5) ? -1 : 1) * (1 << rng.range(0, 3));
-            if (!intra && !cbf && !rs) continue;
-            push_tb(comp, cx, cy, clog2, base | (cbf ? HPVCD_TU_CBF : 0), cmode, qp, 0, rs);
-        }
+        // 4:2:2: two square chroma TBs stacked per component, all Cb then all
+        // Cr (decode.rs:5034-5060), each with its own cbf
+        const int n_tb = idc == 2 ? 2 : 1;
+        for (int comp = 1; comp <= 2; ++comp)
+            for (int t = 0; t < n_tb; ++t) {
+                const bool cbf = rng.bern(c.cbf_p);
+                int rs = 0;  // cross_comp_pred ResScaleVal
+                if (ccp_on && rng.bern(c.ccp_p)) rs = (rng.bern(0.5) ? -1 : 1) * (1 << rng.range(0, 3));
+                if (!intra && !cbf && !rs) continue;
+                push_tb(comp, cx, cy + (t << clog2), clog2, base | (cbf ? HPVCD_TU_CBF : 0), cmode, qp, 0, rs);
+            }
     }
 
     int chroma_mode_for(int lmode) {  // H.265 Table 8-2 (intra_chroma_pred_mode 0..4)
@@ -368,8 +372,11 @@ struct Gen {
         } else {
             return;
         }
+        // 4:2:2: two square chroma TBs stacked per component (decode.rs:5034)
+        const int n_tb = idc == 2 ? 2 : 1;
         for (int comp = 1; comp <= 2; ++comp)
-            push_tb(comp, cx, cy, clog2, HPVCD_TU_CBF | HPVCD_TU_INTRA, 0, qp, 0);
+            for (int t = 0; t < n_tb; ++t)
+                push_tb(comp, cx, cy + (t << clog2), clog2, HPVCD_TU_CBF | HPVCD_TU_INTRA, 0, qp, 0);
     }
 
     static bool motion_differs(const CellMeta& a, const CellMeta& b) {
@@ -585,7 +592,7 @@ int32_t hpvcd_synth_add(hpvcd_synth* s, const hpvcd_synth_cfg* cfg) {
     if (cfg->width == 0 || cfg->height == 0 || (cfg->width & 7) || (cfg->height & 7) ||
         cfg->width > 16384 || cfg->height > 16384)
         return -HPVCD_ERR_INVALID_ARG;
-    if (cfg->chroma_idc == 2 || cfg->chroma_idc > 3 || cfg->bit_depth < 8 || cfg->bit_depth > 12 ||
+    if (cfg->chroma_idc > 3 || cfg->bit_depth < 8 || cfg->bit_depth > 12 ||
         cfg->log2_ctb < 4 || cfg->log2_ctb > 6 || cfg->qp_min > cfg->qp_max)
         return -HPVCD_ERR_INVALID_ARG;
     auto pic = std::make_unique<Picture>();

@@ -87,9 +87,10 @@ def coeffs_of(p: abi.Picture) -> np.ndarray:
 
 def geometry(p: abi.Picture) -> dict:
     ctb = 1 << p.log2_ctb
-    sw = 2 if p.chroma_idc == 1 else 1
-    cw, ch = ((p.width + sw - 1) // sw, (p.height + sw - 1) // sw) if p.chroma_idc else (0, 0)
-    return dict(w=p.width, h=p.height, cw=cw, ch=ch, sub=sw,
+    sw = 2 if p.chroma_idc in (1, 2) else 1   # SubWidthC
+    sh = 2 if p.chroma_idc == 1 else 1        # SubHeightC
+    cw, ch = ((p.width + sw - 1) // sw, (p.height + sh - 1) // sh) if p.chroma_idc else (0, 0)
+    return dict(w=p.width, h=p.height, cw=cw, ch=ch, sub=sw, sub_w=sw, sub_h=sh,
                 ctb_cols=(p.width + ctb - 1) // ctb, ctb_rows=(p.height + ctb - 1) // ctb,
                 gw=(p.width + 3) // 4, gh=(p.height + 3) // 4,
                 bytes_per_sample=1 if p.bit_depth_y <= 8 else 2)

@@ -86,7 +86,10 @@ typedef enum hpvcd_status {
  *
  * x, y are in samples of the component plane.  For 4:2:0, a group of four 4x4
  * luma TBs is followed by one 4x4 chroma TB per chroma component at the
- * parent's position (decode.rs:3601-3609).
+ * parent's position (decode.rs:3601-3609).  For 4:2:2 every chroma TB of the
+ * 4:2:0 layout is two square TBs stacked vertically, the upper one first,
+ * all Cb TBs before the Cr TBs (decode.rs:5030-5060), with the intra mode
+ * already mapped by the 4:2:2 table (decode.rs:3265-3280).
  */
 typedef struct hpvcd_tu {
     uint16_t x, y;
@@ -205,7 +208,7 @@ typedef struct hpvcd_scaling {
  */
 typedef struct hpvcd_picture {
     uint32_t width, height; /* coded luma size (multiple of the minimum CB)   */
-    uint8_t chroma_idc;     /* 0 mono, 1 4:2:0, 3 4:4:4 (2 -> UNSUPPORTED)     */
+    uint8_t chroma_idc;     /* 0 mono, 1 4:2:0, 2 4:2:2, 3 4:4:4               */
     uint8_t bit_depth_y;    /* 8..12                                           */
     uint8_t bit_depth_c;
     uint8_t log2_ctb; /* 4..6                                              */

@@ -678,7 +678,7 @@ void yuv_to_rgb16(const uint16_t* Y, const uint16_t* Cb, const uint16_t* Cr, int
     const int64_t cb_to_g = (cb_g0 * k_uv + ROUND) >> Q13;
     const int64_t cr_to_g = (cr_g0 * k_uv + ROUND) >> Q13;
     const int64_t cb_to_b = (cb_b0 * k_uv + ROUND) >> Q13;
-    const int sub_w = idc == 1 ? 2 : 1, sub_h = idc == 1 ? 2 : 1;
+    const int sub_w = idc == 1 || idc == 2 ? 2 : 1, sub_h = idc == 1 ? 2 : 1;
     const int cw = (width + sub_w - 1) / sub_w, ch = (height + sub_h - 1) / sub_h;
     crop_left = std::min(crop_left, width - 1);
     crop_top = std::min(crop_top, height - 1);
@@ -735,8 +735,8 @@ Geo geo_of(const hpvcd_picture* p) {
     g.w = (int)p->width;
     g.h = (int)p->height;
     g.idc = p->chroma_idc;
-    g.sub_w = g.idc == 1 ? 2 : 1;
-    g.sub_h = g.idc == 1 ? 2 : 1;
+    g.sub_w = g.idc == 1 || g.idc == 2 ? 2 : 1;  // SubWidthC
+    g.sub_h = g.idc == 1 ? 2 : 1;                  // SubHeightC
     g.cw = g.idc == 0 ? 0 : (g.w + g.sub_w - 1) / g.sub_w;
     g.ch = g.idc == 0 ? 0 : (g.h + g.sub_h - 1) / g.sub_h;
     g.gw = (g.w + 3) / 4;
@@ -754,7 +754,7 @@ int validate(const hpvcd_picture* p) {
     if (!p) return HPVCD_ERR_INVALID_ARG;
     if (p->width == 0 || p->height == 0 || p->width > 16384 || p->height > 16384)
         return HPVCD_ERR_LIMIT;
-    if (p->chroma_idc == 2 || p->chroma_idc > 3) return HPVCD_ERR_UNSUPPORTED;
+    if (p->chroma_idc > 3) return HPVCD_ERR_UNSUPPORTED;
     if (p->bit_depth_y < 8 || p->bit_depth_y > 12 || p->bit_depth_c < 8 || p->bit_depth_c > 12)
         return HPVCD_ERR_UNSUPPORTED;
     if (p->log2_ctb < 4 || p->log2_ctb > 6) return HPVCD_ERR_BITSTREAM;

@@ -224,8 +224,9 @@ def decode_batch(pics, out=None, want_planes=True, threads=1):
     pl_arr = (Planes * n)()
     for i, p in enumerate(pics):
         w, h = p.width, p.height
-        sw = 2 if p.chroma_idc == 1 else 1
-        cw, ch = ((w + sw - 1) // sw, (h + sw - 1) // sw) if p.chroma_idc else (0, 0)
+        sw = 2 if p.chroma_idc in (1, 2) else 1   # SubWidthC
+        sh = 2 if p.chroma_idc == 1 else 1        # SubHeightC
+        cw, ch = ((w + sw - 1) // sw, (h + sh - 1) // sh) if p.chroma_idc else (0, 0)
         y = np.zeros((h, w), np.uint16)
         cb = np.zeros((ch, cw), np.uint16)
         cr = np.zeros((ch, cw), np.uint16)

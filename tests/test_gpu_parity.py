@@ -214,10 +214,22 @@ def test_errors_map_to_status(dec):
     s = synth.SynthSet()
     s.add(synth.intra_cfg(80, 64, 64))
     bad = s.picture(0)
-    bad.chroma_idc = 2
+    bad.chroma_idc = 4     # no such chroma format
     with pytest.raises(abi.HpvcdError) as e:
         dec.submit([bad])
     assert e.value.status == abi.ERR_UNSUPPORTED
+    bad = s.picture(0)
+    bad.bit_depth_y = bad.bit_depth_c = 14   # above the supported 12 bits
+    with pytest.raises(abi.HpvcdError) as e:
+        dec.submit([bad])
+    assert e.value.status == abi.ERR_UNSUPPORTED
+    # a reference of another size (motion compensation would read outside it)
+    s2 = synth.SynthSet()
+    s2.add(synth.intra_cfg(81, 128, 64, bit_depth=8))
+    s2.add(synth.inter_cfg(82, 128, 128))
+    with pytest.raises(abi.HpvcdError) as e:
+        dec.submit(s2.pictures())
+    assert e.value.status == abi.ERR_BITSTREAM
     p2 = s.picture(0)
     p2.width = 0
     with pytest.raises(abi.HpvcdError) as e:
@@ -692,3 +704,49 @@ def test_cross_component_inter_and_plan(dec):
     assert plan.status() == abi.OK
     assert_planes_equal([plan.planes(i) for i in range(len(pics))], ref, "cross-component plan")
     plan.close()
+
+
+# --- 4:2:2: two stacked square chroma TBs, chroma CTU half as wide as tall --
+@pytest.mark.parametrize("bd,log2_ctb", [(8, 6), (10, 5), (12, 4)])
+def test_422_intra(dec, bd, log2_ctb):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(230 + bd, 392, 264, bit_depth=bd, chroma_idc=2, tskip_p=0.2, tqb_p=0.05,
+                        scaling=(bd == 10))
+    c.log2_ctb = log2_ctb
+    c.rext, c.tskip_log2_max = 7, 3
+    s.add(c)
+    run_yuv(dec, s.pictures(), f"4:2:2 {bd}-bit ctb {1 << log2_ctb}")
+
+
+def test_422_residual_inter_and_rgb(dec):
+    s = synth.SynthSet()
+    s.add(synth.residual_cfg(240, 256, 128, bit_depth=8, chroma_idc=2))
+    run_yuv(dec, s.pictures(), "4:2:2 residual")
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(241, 320, 192, bit_depth=8, chroma_idc=2))
+    for i in range(1, 4):
+        c = synth.inter_cfg(241 + i, 320, 192, bit_depth=8, weighted=(i == 2))
+        c.chroma_idc = 2
+        s.add(c)
+    run_yuv(dec, s.pictures(), "4:2:2 inter")
+    g = synth.make_grid(1100, 700, seed=245, bit_depth=10, chroma_idc=2)
+    out, keep = synth.grid_output(g, matrix=abi.MATRIX_BT709, full_range=False)
+    pics = g.synth.pictures()
+    t = dec.submit(pics, out)
+    dec.wait(t)
+    got = dec.read(t)
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    assert np.array_equal(got.reshape(ref.shape), ref)
+
+
+def test_mixed_formats_one_batch(dec):
+    """4:2:0, 4:2:2, 4:4:4 and 4:0:0 pictures share one launch (the 4:4:4
+    shared-memory layout holds every format)."""
+    s = synth.SynthSet()
+    for i, idc in enumerate([1, 2, 3, 0, 2, 1, 2, 3]):
+        s.add(synth.intra_cfg(250 + i, 256, 192, bit_depth=8 if i % 2 else 10, chroma_idc=idc))
+    run_yuv(dec, s.pictures(), "mixed chroma formats")
+    s = synth.SynthSet()
+    for i, idc in enumerate([1, 2, 1, 2]):
+        s.add(synth.intra_cfg(260 + i, 256, 192, bit_depth=8, chroma_idc=idc))
+    run_yuv(dec, s.pictures(), "4:2:0 + 4:2:2")

@@ -275,13 +275,17 @@ def test_plan_features_match_host_restatement():
     for k, v in enumerate((0.1, 0.2, 0.3, 0.4)):
         c.tu_mix[k] = v
     s.add(c)
-    s.add(synth.inter_cfg(33, 256, 256, weighted=True))
+    s.add(synth.intra_cfg(34, 256, 256, bit_depth=8, chroma_idc=1))
+    s.add(synth.inter_cfg(33, 256, 256, weighted=True, n_refs=1))
     pics = s.pictures()
+    for l in range(2):            # the inter picture predicts from the one before only
+        for r in range(1, abi.MAX_REFS):
+            pics[3].ref_slot[l][r] = -1
     plan = DevicePlan(pics)
     L = abi.lib()
     f = torch.empty(16, dtype=torch.float32, device="cuda")
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    for first, count in ((0, 3), (2, 1), (1, 1)):
+    for first, count in ((0, 4), (3, 1), (1, 1)):
         abi.check(L.hpvcd_plan_features(plan._h, first, count, C.c_void_p(f.data_ptr()), st), "features")
         np.testing.assert_allclose(f.cpu().numpy(), features_host(pics[first:first + count]), rtol=1e-5, atol=1e-6)
     plan.close()
