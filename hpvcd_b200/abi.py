@@ -54,6 +54,8 @@ PIC_SAO_CHROMA = 0x0010
 PIC_PRED_IN_PLANE = 0x0020
 PIC_INTER = 0x0040
 PIC_CROSS_COMPONENT = 0x0080
+PIC_SAO_NO_ACROSS_SLICES = 0x0100
+PIC_SAO_NO_ACROSS_TILES = 0x0200
 PIC_STORE_MASK = 0x00FF0000
 
 
@@ -170,6 +172,7 @@ class Picture(C.Structure):
         ("ref_slot", (C.c_int32 * MAX_REFS) * 2),
         ("pred", C.c_void_p * 3),
         ("scaling", C.c_void_p),
+        ("ctb_region", C.c_void_p),
     ]
 
 
@@ -238,7 +241,7 @@ class SynthCfg(C.Structure):
         ("mv_pad", C.c_float), ("weighted", C.c_uint32), ("n_refs", C.c_uint32),
         ("tu_mix", C.c_float * 4),
         ("scaling", C.c_uint32), ("rext", C.c_uint32), ("tskip_log2_max", C.c_uint32),
-        ("ccp_p", C.c_float),
+        ("ccp_p", C.c_float), ("regions", C.c_uint32),
     ]
 
 

@@ -26,6 +26,7 @@ struct DevPic {
     const hpvcd_sao_ctb* sao;
     const hpvcd_pu* pus;
     const hpvcd_scaling* scaling;  // NULL: flat scale
+    const uint16_t* ctb_region;    // slice << 8 | tile per CTB, NULL: one region
     uint32_t n_tus, n_pus;
     uint64_t n_coeffs;
     hpvcd_wp_table wp;

@@ -288,11 +288,24 @@ __global__ void k_sao(const DevPic* __restrict__ pics) {
                     w[r][0] = in_row && x0 > 0 ? load_sample(src, bps, (size_t)yy * pw + x0 - 1) : 0;
                     w[r][5] = in_row && x0 + 4 < pw ? load_sample(src, bps, (size_t)yy * pw + x0 + 4) : 0;
                 }
-    #pragma unroll
+                    // slice / tile boundaries SAO may not cross (sao.rs:380-414):
+                // bits of the CTB regions that must agree
+                const uint32_t rmask = P.ctb_region ? (((P.flags & HPVCD_PIC_SAO_NO_ACROSS_SLICES) ? 0xff00u : 0u) |
+                                                       ((P.flags & HPVCD_PIC_SAO_NO_ACROSS_TILES) ? 0x00ffu : 0u))
+                                                    : 0u;
+                auto region_ok = [&](int ax, int ay, int bx, int by) {
+                    if (!rmask) return true;
+                    const int s = P.log2_ctb;
+                    const uint32_t ra = P.ctb_region[(size_t)((ay * sh) >> s) * P.ctb_cols + ((ax * sw) >> s)];
+                    const uint32_t rb = P.ctb_region[(size_t)((by * sh) >> s) * P.ctb_cols + ((bx * sw) >> s)];
+                    return ((ra ^ rb) & rmask) == 0u;
+                };
+#pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     const int x = x0 + i;
                     const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
-                    if (x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph) {
+                    if (x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph &&
+                        region_ok(x, y, x1, y1) && region_ok(x, y, x2, y2)) {
                         // (x + dx, y + dy) and (x - dx, y - dy) with constant window indexes
                         int n1, n2;
                         switch (sc.eo_class) {

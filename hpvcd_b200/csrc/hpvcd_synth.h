@@ -69,6 +69,10 @@ typedef struct hpvcd_synth_cfg {
     /* 4:4:4 only: cross_component_prediction_enabled; probability that a
      * chroma TB of a TU with coded luma gets a non-zero res_scale. */
     float ccp_p;
+    /* Slices and tiles (hpvcd_picture.ctb_region): 1 = three slices split at
+     * random CTB addresses in raster order, 2 = a uniform 2x2 tile grid with
+     * one slice per tile.  0 = one slice and tile. */
+    uint32_t regions;
 } hpvcd_synth_cfg;
 
 typedef struct hpvcd_synth hpvcd_synth;

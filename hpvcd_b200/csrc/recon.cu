@@ -559,6 +559,7 @@ struct Comp {
     int S, Sh;    // CTU width (also the residual canvas stride) and height in component samples
     int CW;       // canvas row stride
     int sw, sh;   // luma samples per component sample (1 or 2)
+    uint32_t nb_ok;  // neighbour CTUs of the same slice and tile: 1 left, 2 above-left, 4 above, 8 above-right
     int bd, max_v;
     bool luma, filt, smoothing, strong;
     uint16_t* can;       // bordered canvas
@@ -570,7 +571,7 @@ __device__ __forceinline__ int cidx(const Comp& k, int x, int y) { return (y + 1
 // Reference sample i of the line (i < 2n: left column bottom-up, 2n: the
 // corner, > 2n: above row) with its availability (decode.rs:4651-4690
 // luma_avail / chroma_avail restricted to this CTU and its already
-// reconstructed neighbours; single slice and tile per picture).  Inside the
+// reconstructed neighbours of the same slice and tile).  Inside the
 // CTU a sample is available when the luma record that marked its 4x4 cell
 // decoded comes before the current record `jrec` in decode order: `stamp`
 // holds, per cell, the index of the first luma record covering it
@@ -589,9 +590,11 @@ __device__ __forceinline__ bool gather_ref(const Comp& k, const uint32_t* stamp,
     bool a = ax >= 0 && ay >= 0 && ax < k.pw && ay < k.ph;
     if (y >= 0) {
         if (x < 0)
-            a = a && y < k.Sh;  // left CTU (below-left CTU is not reconstructed yet)
+            a = a && y < k.Sh && (k.nb_ok & 1u);  // left CTU (below-left CTU is not reconstructed yet)
         else
             a = a && x < k.S && y < k.Sh && st < jrec;
+    } else {  // row above: above-left, above or above-right CTU
+        a = a && (k.nb_ok & (x < 0 ? 2u : (x < k.S ? 4u : 8u)));
     }
     *v = a ? cv : 0;
     return a;
@@ -1144,6 +1147,18 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 }
             }
         }
+        // neighbour CTUs that intra prediction may read: same slice and tile
+        // (decode.rs:4651-4690)
+        uint32_t nb_ok = 0xfu;
+        if (P.ctb_region) {
+            const uint16_t me = P.ctb_region[ci];
+            const int cx = it.cx, cy = it.cy;
+            auto same = [&](int nx, int ny) {
+                return nx >= 0 && ny >= 0 && nx < P.ctb_cols && P.ctb_region[(size_t)ny * P.ctb_cols + nx] == me;
+            };
+            nb_ok = (same(cx - 1, cy) ? 1u : 0u) | (same(cx - 1, cy - 1) ? 2u : 0u) | (same(cx, cy - 1) ? 4u : 0u) |
+                    (same(cx + 1, cy - 1) ? 8u : 0u);
+        }
         // ---- wait for the neighbours (bounded), then load their edges ----
         if (tid == 0) {
             const int cx = it.cx, cy = it.cy;
@@ -1201,6 +1216,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             k.ph = c ? P.ch : P.h;
             k.sw = c ? P.sub_w : 1;
             k.sh = c ? P.sub_h : 1;
+            k.nb_ok = nb_ok;
             k.bd = c ? P.bd_c : P.bd;
             k.max_v = (1 << k.bd) - 1;
             k.luma = c == 0;

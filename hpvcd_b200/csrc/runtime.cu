@@ -322,6 +322,7 @@ void fill_inputs(DevPic& d, const hpvcd_picture& p) {
     d.sao = p.sao;
     d.pus = p.pus;
     d.scaling = p.scaling;
+    d.ctb_region = p.ctb_region;
     d.n_tus = p.n_tus;
     d.n_pus = p.n_pus;
     d.n_coeffs = p.n_coeffs;
@@ -889,13 +890,13 @@ hpvcd_status device_status(hpvcd_plan* P, cudaStream_t st) {
 
 // Layout of the inputs of a batch in one arena (256-byte aligned parts in a
 // fixed order per picture: tus, ctu starts, coefficients, cells, SAO, PUs,
-// scaling lists, prediction planes).  Shared by hpvcd_gpu_pack_inputs and submit.
+// scaling lists, CTB regions, prediction planes).  Shared by hpvcd_gpu_pack_inputs and submit.
 struct InputPart {
     const void* src;
     size_t bytes;
     size_t off;
     uint32_t pic;
-    int kind;  // 0..5 as above, 6..8 = prediction planes Y/Cb/Cr, 9 = scaling lists
+    int kind;  // 0..5 as above, 6..8 = prediction planes Y/Cb/Cr, 9 = scaling lists, 10 = CTB regions
 };
 
 size_t input_layout(const hpvcd_picture* pics, uint32_t n, std::vector<InputPart>* parts) {
@@ -916,6 +917,7 @@ size_t input_layout(const hpvcd_picture* pics, uint32_t n, std::vector<InputPart
         add(i, 4, p.sao, ctbs * sizeof(hpvcd_sao_ctb));
         add(i, 5, p.pus, (size_t)p.n_pus * sizeof(hpvcd_pu));
         add(i, 9, p.scaling, sizeof(hpvcd_scaling));
+        add(i, 10, p.ctb_region, ctbs * sizeof(uint16_t));
         if (p.flags & HPVCD_PIC_PRED_IN_PLANE)
             for (int c = 0; c < (p.chroma_idc ? 3 : 1); ++c)
                 add(i, 6 + c, p.pred[c], c ? geo.chroma_bytes : geo.luma_bytes);
@@ -932,6 +934,7 @@ void point_at(hpvcd_picture& d, int kind, const void* ptr) {
         case 4: d.sao = (const hpvcd_sao_ctb*)ptr; break;
         case 5: d.pus = (const hpvcd_pu*)ptr; break;
         case 9: d.scaling = (const hpvcd_scaling*)ptr; break;
+        case 10: d.ctb_region = (const uint16_t*)ptr; break;
         default: d.pred[kind - 6] = ptr; break;
     }
 }
@@ -1365,6 +1368,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         d.tus = nullptr; d.ctu_tu_start = nullptr; d.coeffs = nullptr; d.cells = nullptr;
         d.sao = nullptr; d.pus = nullptr; d.pred[0] = d.pred[1] = d.pred[2] = nullptr;
         d.scaling = nullptr;
+        d.ctb_region = nullptr;
     }
     // Runs of parts laid out contiguously (as hpvcd_gpu_pack_inputs lays them
     // out) in page-locked memory go up by DMA straight from the caller's

@@ -159,6 +159,7 @@ struct hpvcd_server {
             p.sao = (const hpvcd_sao_ctb*)fix(p.sao);
             p.pus = (const hpvcd_pu*)fix(p.pus);
             p.scaling = (const hpvcd_scaling*)fix(p.scaling);
+            p.ctb_region = (const uint16_t*)fix(p.ctb_region);
             for (int c = 0; c < 3; ++c) p.pred[c] = fix(p.pred[c]);
             if (p.wp) p.wp = &b.wp[i];
         }
@@ -333,6 +334,7 @@ HPVCD_API hpvcd_status hpvcd_server_submit(hpvcd_server* s, const hpvcd_request*
             p.sao = (const hpvcd_sao_ctb*)off(p.sao);
             p.pus = (const hpvcd_pu*)off(p.pus);
             p.scaling = (const hpvcd_scaling*)off(p.scaling);
+            p.ctb_region = (const uint16_t*)off(p.ctb_region);
             for (int c = 0; c < 3; ++c) p.pred[c] = off(p.pred[c]);
             bp->wp[first + i] = req->pics[i].wp ? *req->pics[i].wp : hpvcd_wp_table{};
             p.wp = req->pics[i].wp ? (const hpvcd_wp_table*)1 : nullptr;  // resolved at launch

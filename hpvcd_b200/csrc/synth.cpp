@@ -54,6 +54,7 @@ struct Picture {
     bool has_wp = false;
     hpvcd_scaling scaling{};
     bool has_scaling = false;
+    std::vector<uint16_t> ctb_region;
     std::vector<uint8_t> pred8[3];
     std::vector<uint16_t> pred16[3];
 };
@@ -497,6 +498,24 @@ struct Gen {
                     P.scaling.dc[s][m] = (uint8_t)sr.range(1, 255);
                 }
         }
+        if (c.regions) {  // own seeded stream: the rest of the picture is unchanged
+            Rng rr(c.seed ^ 0x7E61045ull);
+            const int ctbz = 1 << log2_ctb;
+            const int cols = (w + ctbz - 1) / ctbz, rows = (h + ctbz - 1) / ctbz, n = cols * rows;
+            P.ctb_region.assign((size_t)n, 0);
+            if (c.regions == 1 && n >= 3) {
+                int a = rr.range(1, n - 2), b = rr.range(1, n - 1);
+                if (a > b) std::swap(a, b);
+                if (a == b) b = std::min(n - 1, b + 1);
+                for (int i = 0; i < n; ++i) P.ctb_region[(size_t)i] = (uint16_t)((i >= a) + (i >= b)) << 8;
+            } else if (c.regions == 2) {
+                for (int y = 0; y < rows; ++y)
+                    for (int x = 0; x < cols; ++x) {
+                        const int tile = (x >= (cols + 1) / 2) + 2 * (y >= (rows + 1) / 2);
+                        P.ctb_region[(size_t)y * cols + x] = (uint16_t)(tile << 8 | tile);
+                    }
+            }
+        }
         P.cells.assign((size_t)gw * gh, hpvcd_cell{});
         const int ctb = 1 << log2_ctb;
         const int cols = (w + ctb - 1) / ctb, rows = (h + ctb - 1) / ctb;
@@ -611,6 +630,7 @@ int32_t hpvcd_synth_add(hpvcd_synth* s, const hpvcd_synth_cfg* cfg) {
     d.pus = pic->pus.empty() ? nullptr : pic->pus.data();
     d.wp = pic->has_wp ? &pic->wp : nullptr;
     d.scaling = pic->has_scaling ? &pic->scaling : nullptr;
+    d.ctb_region = pic->ctb_region.empty() ? nullptr : pic->ctb_region.data();
     for (int c = 0; c < 3; ++c)
         d.pred[c] = !pic->pred8[c].empty() ? (const void*)pic->pred8[c].data()
                     : !pic->pred16[c].empty() ? (const void*)pic->pred16[c].data()

@@ -191,6 +191,12 @@ typedef struct hpvcd_scaling {
  * residual of its own (decode.rs:5428).  The TU's luma TB is one of the three
  * records before the chroma record. */
 #define HPVCD_PIC_CROSS_COMPONENT 0x0080u
+/* SAO edge offset does not use neighbours across a slice / tile boundary
+ * (slice_loop_filter_across_slices_enabled_flag = 0 /
+ * loop_filter_across_tiles_enabled_flag = 0; sao.rs:380-414); needs
+ * hpvcd_picture.ctb_region. */
+#define HPVCD_PIC_SAO_NO_ACROSS_SLICES 0x0100u
+#define HPVCD_PIC_SAO_NO_ACROSS_TILES 0x0200u
 /* Store the decoded picture into entry e of the context's DPB (hpvcd_dpb)
  * after it is reconstructed; bits 16..23 of flags, 0 = no store. */
 #define HPVCD_PIC_STORE_DPB(e) ((uint32_t)((e) + 1) << 16)
@@ -231,6 +237,12 @@ typedef struct hpvcd_picture {
                                          /* HPVCD_REF_DPB(e), or -1               */
     const void* pred[3];           /* PRED_IN_PLANE: initial Y/Cb/Cr planes   */
     const hpvcd_scaling* scaling;  /* NULL -> flat (scaling_list_enabled = 0) */
+    /* Slices and tiles: per CTB in raster order, slice_idx << 8 | tile_id.
+     * Intra prediction never reads a CTB of another slice or tile
+     * (decode.rs:4651-4690 same_slice / same_tile); SAO follows the
+     * HPVCD_PIC_SAO_NO_ACROSS_* flags; deblocking gating is folded into the
+     * cells' boundary strengths by the host.  NULL -> one slice, one tile. */
+    const uint16_t* ctb_region;
 } hpvcd_picture;
 
 /* Output of a batch.  RGB8 is the `decode_heic_rgb8` path (lib.rs:1964):

@@ -621,8 +621,12 @@ void sao_band(uint16_t* dst, const uint16_t* src, int w, int x0, int y0, int x_e
 }
 
 // sao.rs:266-330 (edge offset, picture-border samples untouched)
+// `nb_ok(x, y, nx, ny)`: neighbour (nx, ny) may be used for the sample at
+// (x, y) (sao.rs:433-497 apply_sao_edge_offset_gated; always true without
+// restricted boundaries).
+template <typename NbOk>
 void sao_edge(uint16_t* dst, const uint16_t* src, int w, int h, int x0, int y0, int x_end,
-              int y_end, const int32_t* off, int eo_class, int bd) {
+              int y_end, const int32_t* off, int eo_class, int bd, NbOk nb_ok) {
     const int mx = (1 << bd) - 1;
     int dx, dy;
     switch (eo_class) {
@@ -637,6 +641,7 @@ void sao_edge(uint16_t* dst, const uint16_t* src, int w, int h, int x0, int y0, 
             const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
             if (x1 < 0 || y1 < 0 || x1 >= w || y1 >= h) continue;
             if (x2 < 0 || y2 < 0 || x2 >= w || y2 >= h) continue;
+            if (!nb_ok(x, y, x1, y1) || !nb_ok(x, y, x2, y2)) continue;
             const int n1 = src[(size_t)y1 * w + x1], n2 = src[(size_t)y2 * w + x2];
             const int e = ((s > n1) - (s < n1)) + ((s > n2) - (s < n2)) + 2;
             int o = 0;
@@ -766,15 +771,23 @@ struct PicState {
     Geo g;
     orc_planes pl;
     std::vector<uint8_t> decoded;  // decode.rs `decoded` map, per 4x4 luma cell
+    int cur_region = 0;            // slice / tile of the TB being predicted
 
-    bool luma_avail(int x, int y) const {  // decode.rs:4651-4668 (single slice / tile)
+    int region_at(int x, int y) const {  // luma position -> slice << 8 | tile
+        const hpvcd_picture* p = pic;
+        if (!p->ctb_region) return 0;
+        return p->ctb_region[(size_t)(y >> g.log2_ctb) * g.ctb_cols + (x >> g.log2_ctb)];
+    }
+    bool luma_avail(int x, int y) const {  // decode.rs:4651-4668 (same tile, same slice, decoded)
         if (x < 0 || y < 0 || x >= g.w || y >= g.h) return false;
+        if (region_at(x, y) != cur_region) return false;
         return decoded[(size_t)(y / 4) * g.gw + x / 4] != 0;
     }
     bool chroma_avail(int cx, int cy) const {  // decode.rs:4669-4690
         if (cx < 0 || cy < 0 || cx >= g.cw || cy >= g.ch) return false;
         const int lx = cx * g.sub_w, ly = cy * g.sub_h;
         if (lx >= g.w || ly >= g.h) return false;
+        if (region_at(lx, ly) != cur_region) return false;
         return decoded[(size_t)(ly / 4) * g.gw + lx / 4] != 0;
     }
     void mark_decoded(int x0, int y0, int n) {  // decode.rs:3170-3189
@@ -941,8 +954,10 @@ int recon_picture(const hpvcd_picture* p, orc_planes* pl) {
             if (luma) st.mark_decoded(t.x, t.y, n);
             continue;
         }
-        if (intra && !pred_in_plane)
+        if (intra && !pred_in_plane) {
+            st.cur_region = luma ? st.region_at(t.x, t.y) : st.region_at(t.x * g.sub_w, t.y * g.sub_h);
             predict_block(st, t.comp, t.x, t.y, n, t.mode, pred);
+        }
         else
             load_block_clipped(plane, pw, pw, ph, t.x, t.y, n, pred);
         const int vw = std::min(std::max(pw - (int)t.x, 0), n);
@@ -1184,6 +1199,11 @@ int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
     if (!sao_luma && !sao_chroma) return HPVCD_OK;
     const Geo g = geo_of(p);
     const int ctb = 1 << g.log2_ctb;
+    const bool no_slices = (p->flags & HPVCD_PIC_SAO_NO_ACROSS_SLICES) != 0;
+    const bool no_tiles = (p->flags & HPVCD_PIC_SAO_NO_ACROSS_TILES) != 0;
+    auto region_of = [&](int lx, int ly) -> int {
+        return p->ctb_region[(size_t)(ly >> g.log2_ctb) * g.ctb_cols + (lx >> g.log2_ctb)];
+    };
     const std::vector<uint16_t> oy(pl->y, pl->y + (size_t)g.w * g.h);
     std::vector<uint16_t> ocb, ocr;
     if (g.idc) {
@@ -1211,7 +1231,14 @@ int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
                 if (sc.type_idx == 1)
                     sao_band(dst, src, pw, cx0, cy0, cx1, cy1, off, sc.band_pos, bd);
                 else
-                    sao_edge(dst, src, pw, ph, cx0, cy0, cx1, cy1, off, sc.eo_class, bd);
+                    sao_edge(dst, src, pw, ph, cx0, cy0, cx1, cy1, off, sc.eo_class, bd,
+                             [&](int x, int y, int nx, int ny) {  // sao.rs:380-425 (slice / tile part)
+                                 if (!p->ctb_region) return true;
+                                 const int ra = region_of(x * sw, y * sh), rb = region_of(nx * sw, ny * sh);
+                                 if (no_slices && (ra >> 8) != (rb >> 8)) return false;
+                                 if (no_tiles && (ra & 0xff) != (rb & 0xff)) return false;
+                                 return true;
+                             });
             }
         }
     // decode.rs:2444-2485: exempt samples keep their pre-SAO value.
@@ -1365,7 +1392,7 @@ void orc_apply_luma_decision(uint16_t* plane, int32_t stride, int32_t vertical, 
 }
 void orc_sao_edge(uint16_t* dst, const uint16_t* src, int32_t w, int32_t h, int32_t x0, int32_t y0,
                   int32_t x_end, int32_t y_end, const int32_t* off, int32_t eo, int32_t bd) {
-    sao_edge(dst, src, w, h, x0, y0, x_end, y_end, off, eo, bd);
+    sao_edge(dst, src, w, h, x0, y0, x_end, y_end, off, eo, bd, [](int, int, int, int) { return true; });
 }
 void orc_sao_band(uint16_t* dst, const uint16_t* src, int32_t w, int32_t x0, int32_t y0,
                   int32_t x_end, int32_t y_end, const int32_t* off, int32_t bp, int32_t bd) {

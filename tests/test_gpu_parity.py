@@ -750,3 +750,55 @@ def test_mixed_formats_one_batch(dec):
     for i, idc in enumerate([1, 2, 1, 2]):
         s.add(synth.intra_cfg(260 + i, 256, 192, bit_depth=8, chroma_idc=idc))
     run_yuv(dec, s.pictures(), "4:2:0 + 4:2:2")
+
+
+# --- slices and tiles: intra availability and SAO across their boundaries --
+@pytest.mark.parametrize("regions,idc,no_across", [(1, 1, 0), (1, 2, abi.PIC_SAO_NO_ACROSS_SLICES),
+                                                  (2, 3, abi.PIC_SAO_NO_ACROSS_TILES),
+                                                  (2, 1, abi.PIC_SAO_NO_ACROSS_SLICES | abi.PIC_SAO_NO_ACROSS_TILES)])
+def test_slices_and_tiles(dec, regions, idc, no_across):
+    s = synth.SynthSet()
+    for k, (w, h, ctb) in enumerate([(384, 320, 6), (264, 200, 5)]):
+        c = synth.intra_cfg(410 + 7 * regions + idc + k, w, h, bit_depth=10 if k else 8, chroma_idc=idc)
+        c.log2_ctb = ctb
+        c.regions = regions
+        c.pic_flags |= no_across
+        s.add(c)
+    pics = s.pictures()
+    assert all(p.ctb_region for p in pics)
+    run_yuv(dec, pics, f"regions {regions} idc {idc} flags {no_across:#x}")
+    ref, _ = O.decode_batch(pics)
+    plan = DevicePlan(pics)
+    plan.launch()
+    torch.cuda.synchronize()
+    assert_planes_equal([plan.planes(i) for i in range(len(pics))], ref, "regions plan")
+    plan.close()
+
+
+def test_tiles_through_the_server():
+    from hpvcd_b200.gpu import Server, pack_pinned, pinned_empty
+    s = synth.SynthSet()
+    places = []
+    for k, (x, y) in enumerate([(0, 0), (512, 0), (0, 256), (512, 256)]):
+        c = synth.intra_cfg(421 + k, 512, 256, bit_depth=10)
+        c.regions = 2 if k % 2 else 1
+        c.pic_flags |= abi.PIC_SAO_NO_ACROSS_TILES | abi.PIC_SAO_NO_ACROSS_SLICES
+        s.add(c)
+        places.append((x, y, 512, 256))
+    pics = s.pictures()
+    out, keep = synth.grid_output(synth.Grid(1024, 512, 512, s, places))
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    kp_all = []
+    with Server(0, max_inflight=2, batching=True, batch_window_us=100000) as srv:
+        srv.submit(pics, places, 1024, 512, user=0)
+        packed, kp = pack_pinned(pics)
+        dst, kd = pinned_empty(1024 * 512 * 3)
+        kp_all.append((kp, kd))
+        srv.submit(packed, places, 1024, 512, user=1, dst=dst.reshape(512, 1024, 3), zero_copy_keep=(kp, kd))
+        got = {}
+        while len(got) < 2:
+            for c in srv.poll(4, timeout_ms=60000):
+                assert c["status"] == abi.OK
+                got[c["user"]] = c
+    for k in (0, 1):
+        assert np.array_equal(got[k]["image"], ref), k
