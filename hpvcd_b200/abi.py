@@ -43,6 +43,7 @@ STATUS_NAMES = {
 TU_CBF, TU_TSKIP, TU_INTRA, TU_TQB = 0x01, 0x02, 0x04, 0x08
 TU_ROTATE, TU_RDPCM_H, TU_RDPCM_V = 0x10, 0x20, 0x40
 CELL_EXEMPT = 0x01
+CELL_INTER = 0x02
 PU_L0, PU_L1 = 0x01, 0x02
 MAX_REFS = 16
 
@@ -56,6 +57,7 @@ PIC_INTER = 0x0040
 PIC_CROSS_COMPONENT = 0x0080
 PIC_SAO_NO_ACROSS_SLICES = 0x0100
 PIC_SAO_NO_ACROSS_TILES = 0x0200
+PIC_CONSTRAINED_INTRA = 0x0400
 PIC_STORE_MASK = 0x00FF0000
 
 

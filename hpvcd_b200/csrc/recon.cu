@@ -560,6 +560,8 @@ struct Comp {
     int CW;       // canvas row stride
     int sw, sh;   // luma samples per component sample (1 or 2)
     uint32_t nb_ok;  // neighbour CTUs of the same slice and tile: 1 left, 2 above-left, 4 above, 8 above-right
+    const hpvcd_cell* ci_cells;  // constrained intra prediction: cells whose INTER samples are unusable
+    int gw;                      // cells per row
     int bd, max_v;
     bool luma, filt, smoothing, strong;
     uint16_t* can;       // bordered canvas
@@ -596,6 +598,8 @@ __device__ __forceinline__ bool gather_ref(const Comp& k, const uint32_t* stamp,
     } else {  // row above: above-left, above or above-right CTU
         a = a && (k.nb_ok & (x < 0 ? 2u : (x < k.S ? 4u : 8u)));
     }
+    if (a && k.ci_cells)  // decode.rs:4641-4649 constrained_intra_ok
+        a = !(k.ci_cells[(size_t)((ay * k.sh) >> 2) * k.gw + ((ax * k.sw) >> 2)].flags & HPVCD_CELL_INTER);
     *v = a ? cv : 0;
     return a;
 }
@@ -1217,6 +1221,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             k.sw = c ? P.sub_w : 1;
             k.sh = c ? P.sub_h : 1;
             k.nb_ok = nb_ok;
+            k.ci_cells = (P.flags & HPVCD_PIC_CONSTRAINED_INTRA) ? P.cells : nullptr;
+            k.gw = P.gw;
             k.bd = c ? P.bd_c : P.bd;
             k.max_v = (1 << k.bd) - 1;
             k.luma = c == 0;

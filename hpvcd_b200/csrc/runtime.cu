@@ -77,7 +77,7 @@ hpvcd_status validate(const hpvcd_picture& p) {
     if (p.n_coeffs && !p.coeffs) return HPVCD_ERR_INVALID_ARG;
     if (p.n_pus && !p.pus) return HPVCD_ERR_INVALID_ARG;
     if (!p.ctu_tu_start) return HPVCD_ERR_INVALID_ARG;
-    if ((p.flags & HPVCD_PIC_DEBLOCK) && !p.cells) return HPVCD_ERR_INVALID_ARG;
+    if ((p.flags & (HPVCD_PIC_DEBLOCK | HPVCD_PIC_CONSTRAINED_INTRA)) && !p.cells) return HPVCD_ERR_INVALID_ARG;
     if ((p.flags & HPVCD_PIC_PRED_IN_PLANE) && !p.pred[0]) return HPVCD_ERR_INVALID_ARG;
     return HPVCD_OK;
 }

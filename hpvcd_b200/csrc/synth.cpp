@@ -167,7 +167,7 @@ struct Gen {
             for (int x = x0; x < std::min(x0 + size, w); x += 4) {
                 hpvcd_cell& cl = P.cells[(size_t)(y / 4) * gw + x / 4];
                 cl.qp_y = (int8_t)qp;
-                cl.flags = exempt ? HPVCD_CELL_EXEMPT : 0;
+                cl.flags = (exempt ? HPVCD_CELL_EXEMPT : 0) | (intra ? 0 : HPVCD_CELL_INTER);
                 cell(x, y).intra = intra;
             }
     }

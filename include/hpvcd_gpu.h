@@ -107,6 +107,7 @@ typedef struct hpvcd_tu {
 
 /* hpvcd_cell.flags */
 #define HPVCD_CELL_EXEMPT 0x01u /* tqb CU, or I_PCM CU with pcm_loop_filter_disabled */
+#define HPVCD_CELL_INTER 0x02u  /* cell of an inter CU (motion map !is_intra)          */
 
 /*
  * Per 4x4 luma cell deblocking metadata (decode.rs:101-335 maps qp_y_map,
@@ -197,6 +198,10 @@ typedef struct hpvcd_scaling {
  * hpvcd_picture.ctb_region. */
 #define HPVCD_PIC_SAO_NO_ACROSS_SLICES 0x0100u
 #define HPVCD_PIC_SAO_NO_ACROSS_TILES 0x0200u
+/* constrained_intra_pred_flag: intra prediction treats samples of cells
+ * flagged HPVCD_CELL_INTER as unavailable (decode.rs:4641-4649); needs
+ * cells. */
+#define HPVCD_PIC_CONSTRAINED_INTRA 0x0400u
 /* Store the decoded picture into entry e of the context's DPB (hpvcd_dpb)
  * after it is reconstructed; bits 16..23 of flags, 0 = no store. */
 #define HPVCD_PIC_STORE_DPB(e) ((uint32_t)((e) + 1) << 16)

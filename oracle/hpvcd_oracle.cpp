@@ -763,6 +763,7 @@ int validate(const hpvcd_picture* p) {
     if (p->bit_depth_y < 8 || p->bit_depth_y > 12 || p->bit_depth_c < 8 || p->bit_depth_c > 12)
         return HPVCD_ERR_UNSUPPORTED;
     if (p->log2_ctb < 4 || p->log2_ctb > 6) return HPVCD_ERR_BITSTREAM;
+    if ((p->flags & HPVCD_PIC_CONSTRAINED_INTRA) && !p->cells) return HPVCD_ERR_INVALID_ARG;
     return HPVCD_OK;
 }
 
@@ -778,9 +779,14 @@ struct PicState {
         if (!p->ctb_region) return 0;
         return p->ctb_region[(size_t)(y >> g.log2_ctb) * g.ctb_cols + (x >> g.log2_ctb)];
     }
+    bool constrained_ok(int x, int y) const {  // decode.rs:4641-4649
+        if (!(pic->flags & HPVCD_PIC_CONSTRAINED_INTRA)) return true;
+        return !(pic->cells[(size_t)(y / 4) * g.gw + x / 4].flags & HPVCD_CELL_INTER);
+    }
     bool luma_avail(int x, int y) const {  // decode.rs:4651-4668 (same tile, same slice, decoded)
         if (x < 0 || y < 0 || x >= g.w || y >= g.h) return false;
         if (region_at(x, y) != cur_region) return false;
+        if (!constrained_ok(x, y)) return false;
         return decoded[(size_t)(y / 4) * g.gw + x / 4] != 0;
     }
     bool chroma_avail(int cx, int cy) const {  // decode.rs:4669-4690
@@ -788,6 +794,7 @@ struct PicState {
         const int lx = cx * g.sub_w, ly = cy * g.sub_h;
         if (lx >= g.w || ly >= g.h) return false;
         if (region_at(lx, ly) != cur_region) return false;
+        if (!constrained_ok(lx, ly)) return false;
         return decoded[(size_t)(ly / 4) * g.gw + lx / 4] != 0;
     }
     void mark_decoded(int x0, int y0, int n) {  // decode.rs:3170-3189

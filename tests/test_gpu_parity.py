@@ -802,3 +802,20 @@ def test_tiles_through_the_server():
                 got[c["user"]] = c
     for k in (0, 1):
         assert np.array_equal(got[k]["image"], ref), k
+
+
+# --- constrained intra prediction -------------------------------------------
+@pytest.mark.parametrize("bd,idc", [(8, 1), (10, 2), (10, 3)])
+def test_constrained_intra(dec, bd, idc):
+    s = synth.SynthSet()
+    c0 = synth.intra_cfg(510 + bd + idc, 320, 192, bit_depth=bd, chroma_idc=idc)
+    c0.pic_flags |= abi.PIC_CONSTRAINED_INTRA
+    s.add(c0)
+    for i in range(1, 4):
+        c = synth.inter_cfg(510 + bd + idc + i, 320, 192, bit_depth=bd, intra_cu_p=0.4, weighted=(i == 2))
+        c.chroma_idc = idc
+        c.pic_flags |= abi.PIC_CONSTRAINED_INTRA
+        if i == 3:
+            c.regions = 1
+        s.add(c)
+    run_yuv(dec, s.pictures(), f"constrained intra {bd}-bit idc {idc}")
