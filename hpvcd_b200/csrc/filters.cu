@@ -13,6 +13,8 @@
 //
 // RGB (yuv.rs:187-393 Q13 matrix, lib.rs:1964-1978 rgb8 narrowing,
 // lib.rs:1610-1660 tile placement and cropping on the canvas).
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace hpvcd {
@@ -229,6 +231,9 @@ __device__ __forceinline__ void store4(void* plane, int bps, size_t idx, const i
 // SAO: one thread per 4 horizontally adjacent samples (they share one CTB:
 // CTB widths are multiples of 8 samples).  blockIdx.y = picture,
 // blockIdx.z = component.  Rows y-1, y, y+1 are read over x-1 .. x+4 once.
+// kGated: some picture of the launch has SAO boundaries it may not cross
+// (slices / tiles); the other instantiation carries no region test.
+template <bool kGated>
 __global__ void k_sao(const DevPic* __restrict__ pics) {
     const DevPic& P = pics[blockIdx.y];
     const int c = blockIdx.z;
@@ -288,40 +293,52 @@ __global__ void k_sao(const DevPic* __restrict__ pics) {
                     w[r][0] = in_row && x0 > 0 ? load_sample(src, bps, (size_t)yy * pw + x0 - 1) : 0;
                     w[r][5] = in_row && x0 + 4 < pw ? load_sample(src, bps, (size_t)yy * pw + x0 + 4) : 0;
                 }
-                    // slice / tile boundaries SAO may not cross (sao.rs:380-414):
+                // slice / tile boundaries SAO may not cross (sao.rs:380-414):
                 // bits of the CTB regions that must agree
                 const uint32_t rmask = P.ctb_region ? (((P.flags & HPVCD_PIC_SAO_NO_ACROSS_SLICES) ? 0xff00u : 0u) |
                                                        ((P.flags & HPVCD_PIC_SAO_NO_ACROSS_TILES) ? 0x00ffu : 0u))
                                                     : 0u;
                 auto region_ok = [&](int ax, int ay, int bx, int by) {
-                    if (!rmask) return true;
                     const int s = P.log2_ctb;
                     const uint32_t ra = P.ctb_region[(size_t)((ay * sh) >> s) * P.ctb_cols + ((ax * sw) >> s)];
                     const uint32_t rb = P.ctb_region[(size_t)((by * sh) >> s) * P.ctb_cols + ((bx * sw) >> s)];
                     return ((ra ^ rb) & rmask) == 0u;
                 };
+                // the sample loop, compiled with and without the region test
+                auto eo_quad = [&](auto gated) {
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int x = x0 + i;
-                    const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
-                    if (x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph &&
-                        region_ok(x, y, x1, y1) && region_ok(x, y, x2, y2)) {
-                        // (x + dx, y + dy) and (x - dx, y - dy) with constant window indexes
-                        int n1, n2;
-                        switch (sc.eo_class) {
-                            case 0: n1 = w[1][i + 2]; n2 = w[1][i]; break;
-                            case 1: n1 = w[2][i + 1]; n2 = w[0][i + 1]; break;
-                            case 2: n1 = w[2][i + 2]; n2 = w[0][i]; break;
-                            default: n1 = w[0][i + 2]; n2 = w[2][i]; break;
+                    for (int i = 0; i < 4; ++i) {
+                        const int x = x0 + i;
+                        const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
+                        bool ok = x1 >= 0 && y1 >= 0 && x1 < pw && y1 < ph && x2 >= 0 && y2 >= 0 && x2 < pw && y2 < ph;
+                        if constexpr (decltype(gated)::value) ok = ok && region_ok(x, y, x1, y1) && region_ok(x, y, x2, y2);
+                        if (ok) {
+                            // (x + dx, y + dy) and (x - dx, y - dy) with constant window indexes
+                            int n1, n2;
+                            switch (sc.eo_class) {
+                                case 0: n1 = w[1][i + 2]; n2 = w[1][i]; break;
+                                case 1: n1 = w[2][i + 1]; n2 = w[0][i + 1]; break;
+                                case 2: n1 = w[2][i + 2]; n2 = w[0][i]; break;
+                                default: n1 = w[0][i + 2]; n2 = w[2][i]; break;
+                            }
+                            const int e = ((s[i] > n1) - (s[i] < n1)) + ((s[i] > n2) - (s[i] < n2)) + 2;
+                            int o = 0;
+                            if (e == 0) o = sc.offsets[0];
+                            else if (e == 1) o = sc.offsets[1];
+                            else if (e == 3) o = sc.offsets[2];
+                            else if (e == 4) o = sc.offsets[3];
+                            if (o) out[i] = clamp3i(s[i] + o, 0, mx);
                         }
-                        const int e = ((s[i] > n1) - (s[i] < n1)) + ((s[i] > n2) - (s[i] < n2)) + 2;
-                        int o = 0;
-                        if (e == 0) o = sc.offsets[0];
-                        else if (e == 1) o = sc.offsets[1];
-                        else if (e == 3) o = sc.offsets[2];
-                        else if (e == 4) o = sc.offsets[3];
-                        if (o) out[i] = clamp3i(s[i] + o, 0, mx);
                     }
+                };
+                if constexpr (kGated) {
+                    if (rmask)
+                        eo_quad(std::true_type{});
+                    else
+                        eo_quad(std::false_type{});
+                } else {
+                    (void)rmask;
+                    eo_quad(std::false_type{});
                 }
             }
             if (P.cells) {  // exempt cells keep the deblocked samples
@@ -469,13 +486,16 @@ static int filter_blocks_x(int quads, int slices, int threads) {
     return need < share ? (need > 0 ? need : 1) : (share > 0 ? share : 1);
 }
 
-extern "C" cudaError_t hpvcd_launch_sao(const hpvcd::DevPic* pics, int n_pics, int max_samples,
+extern "C" cudaError_t hpvcd_launch_sao(const hpvcd::DevPic* pics, int n_pics, int max_samples, int gated,
                                         cudaStream_t stream) {
     if (n_pics <= 0 || max_samples <= 0) return cudaSuccess;
     const int threads = 256;
     const int quads = (max_samples + 3) / 4;
     dim3 grid(filter_blocks_x(quads, n_pics * 3, threads), n_pics, 3);
-    hpvcd::k_sao<<<grid, threads, 0, stream>>>(pics);
+    if (gated)
+        hpvcd::k_sao<true><<<grid, threads, 0, stream>>>(pics);
+    else
+        hpvcd::k_sao<false><<<grid, threads, 0, stream>>>(pics);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }

@@ -562,6 +562,8 @@ struct Comp {
     uint32_t nb_ok;  // neighbour CTUs of the same slice and tile: 1 left, 2 above-left, 4 above, 8 above-right
     const hpvcd_cell* ci_cells;  // constrained intra prediction: cells whose INTER samples are unusable
     int gw;                      // cells per row
+    bool restricted;             // nb_ok != 0xf or ci_cells: gather_ref runs restricted_ok
+    bool ccp;                    // chroma of a cross-component picture: res_scale gives a residual
     int bd, max_v;
     bool luma, filt, smoothing, strong;
     uint16_t* can;       // bordered canvas
@@ -578,6 +580,22 @@ __device__ __forceinline__ int cidx(const Comp& k, int x, int y) { return (y + 1
 // decoded comes before the current record `jrec` in decode order: `stamp`
 // holds, per cell, the index of the first luma record covering it
 // (decode.rs:3170-3189 marks cells as records complete).
+// Slices, tiles and constrained intra prediction: a sample of a neighbour CTU
+// of another slice or tile (decode.rs:4651-4690 same_slice / same_tile) or
+// of an inter cell under constrained_intra_pred (decode.rs:4641-4649) is not
+// available.  (x, y) relative to the CTU, (ax, ay) in the plane.
+__device__ __forceinline__ bool restricted_ok(const Comp& k, int x, int y, int ax, int ay) {
+    uint32_t bit = 0;  // 1 left, 2 above-left, 4 above, 8 above-right, 0 this CTU
+    if (x < 0)
+        bit = y < 0 ? 2u : 1u;
+    else if (y < 0)
+        bit = x < k.S ? 4u : 8u;
+    if (bit && !(k.nb_ok & bit)) return false;
+    if (k.ci_cells && (k.ci_cells[(size_t)((ay * k.sh) >> 2) * k.gw + ((ax * k.sw) >> 2)].flags & HPVCD_CELL_INTER))
+        return false;
+    return true;
+}
+
 __device__ __forceinline__ bool gather_ref(const Comp& k, const uint32_t* stamp, uint32_t jrec, int n2, int x0,
                                            int y0, int i, int* v) {
     const bool left_side = i < n2;
@@ -592,14 +610,11 @@ __device__ __forceinline__ bool gather_ref(const Comp& k, const uint32_t* stamp,
     bool a = ax >= 0 && ay >= 0 && ax < k.pw && ay < k.ph;
     if (y >= 0) {
         if (x < 0)
-            a = a && y < k.Sh && (k.nb_ok & 1u);  // left CTU (below-left CTU is not reconstructed yet)
+            a = a && y < k.Sh;  // left CTU (below-left CTU is not reconstructed yet)
         else
             a = a && x < k.S && y < k.Sh && st < jrec;
-    } else {  // row above: above-left, above or above-right CTU
-        a = a && (k.nb_ok & (x < 0 ? 2u : (x < k.S ? 4u : 8u)));
     }
-    if (a && k.ci_cells)  // decode.rs:4641-4649 constrained_intra_ok
-        a = !(k.ci_cells[(size_t)((ay * k.sh) >> 2) * k.gw + ((ax * k.sw) >> 2)].flags & HPVCD_CELL_INTER);
+    if (k.restricted && a) a = restricted_ok(k, x, y, ax, ay);  // warp-uniform branch
     *v = a ? cv : 0;
     return a;
 }
@@ -998,7 +1013,10 @@ __device__ __forceinline__ void team_sync(int threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(kTeamBarrier), "r"(threads) : "memory");
 }
 
-template <int kTeam>
+// kFeat: some picture of the launch has slices / tiles, constrained intra
+// prediction or cross-component prediction; without them the availability
+// and coded tests compile to the plain single-region form.
+template <int kTeam, bool kFeat>
 __global__ void __launch_bounds__(kReconThreads, 4)
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
         uint32_t* work_counter, uint32_t* dev_err, int cfmt, uint32_t spin_limit) {
@@ -1154,7 +1172,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         // neighbour CTUs that intra prediction may read: same slice and tile
         // (decode.rs:4651-4690)
         uint32_t nb_ok = 0xfu;
-        if (P.ctb_region) {
+        if (kFeat && P.ctb_region) {
             const uint16_t me = P.ctb_region[ci];
             const int cx = it.cx, cy = it.cy;
             auto same = [&](int nx, int ny) {
@@ -1221,8 +1239,10 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             k.sw = c ? P.sub_w : 1;
             k.sh = c ? P.sub_h : 1;
             k.nb_ok = nb_ok;
-            k.ci_cells = (P.flags & HPVCD_PIC_CONSTRAINED_INTRA) ? P.cells : nullptr;
+            k.ci_cells = kFeat && (P.flags & HPVCD_PIC_CONSTRAINED_INTRA) ? P.cells : nullptr;
             k.gw = P.gw;
+            k.restricted = kFeat && (nb_ok != 0xfu || k.ci_cells != nullptr);
+            k.ccp = kFeat && c && (P.flags & HPVCD_PIC_CROSS_COMPONENT);
             k.bd = c ? P.bd_c : P.bd;
             k.max_v = (1 << k.bd) - 1;
             k.luma = c == 0;
@@ -1247,8 +1267,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 const int x = (int)t.x - (c ? ocx : oxl), y = (int)t.y - (c ? ocy : oyl);
                 // a chroma TB with cross-component prediction has a residual
                 // (written by k_ccp) even without coded coefficients
-                const bool coded = (t.flags & HPVCD_TU_CBF) != 0 ||
-                                   ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && c && t.res_scale);
+                const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
                 if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
                     if (!helper) intra_tb_prep(k, t.log2n, t.mode, x, y, stamp, j, team_ws, lane);
                     team_sync(32 * kTeam);
@@ -1336,19 +1355,26 @@ extern "C" cudaError_t hpvcd_launch_ccp(const hpvcd::DevPic* pics, const uint32_
 
 extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd::CtuItem* items,
                                           uint32_t n_items, uint32_t* work_counter, uint32_t* dev_err,
-                                          int cfmt, int grid, int team, cudaStream_t stream) {
+                                          int cfmt, int grid, int team, int feat, cudaStream_t stream) {
     if (n_items == 0) return cudaSuccess;
     // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
     // when the plan was built (no non-stream API call here, so launches can
     // be captured into CUDA graphs)
     const size_t smem = hpvcd::ReconLayout(cfmt).total;
     // 2^22 polls of >= 64 ns each bound one neighbour wait to a few hundred ms.
-    if (team == 2)
-        hpvcd::k_recon<2><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                        dev_err, cfmt, 1u << 22);
+    const uint32_t spin = 1u << 22;
+    if (team == 2 && feat)
+        hpvcd::k_recon<2, true><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
+                                                                              dev_err, cfmt, spin);
+    else if (team == 2)
+        hpvcd::k_recon<2, false><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
+                                                                               dev_err, cfmt, spin);
+    else if (feat)
+        hpvcd::k_recon<1, true><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
+                                                                              dev_err, cfmt, spin);
     else
-        hpvcd::k_recon<1><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                        dev_err, cfmt, 1u << 22);
+        hpvcd::k_recon<1, false><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
+                                                                               dev_err, cfmt, spin);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }
@@ -1357,10 +1383,11 @@ extern "C" int hpvcd_recon_occupancy(int cfmt) {
     int blocks = 0;
     // raise the limit for the 4:4:4 layout, which covers every format
     const size_t smem = hpvcd::ReconLayout(cfmt).total;
-    cudaFuncSetAttribute(hpvcd::k_recon<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)hpvcd::ReconLayout(hpvcd::kFmt444).total);
-    cudaFuncSetAttribute(hpvcd::k_recon<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)hpvcd::ReconLayout(hpvcd::kFmt444).total);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<1>, hpvcd::kReconThreads, smem);
+    const int lim = (int)hpvcd::ReconLayout(hpvcd::kFmt444).total;
+    cudaFuncSetAttribute(hpvcd::k_recon<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(hpvcd::k_recon<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(hpvcd::k_recon<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(hpvcd::k_recon<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<1, false>, hpvcd::kReconThreads, smem);
     return blocks;
 }

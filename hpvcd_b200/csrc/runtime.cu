@@ -22,11 +22,11 @@ extern "C" cudaError_t hpvcd_launch_residual(const DevPic*, const uint32_t*, uin
                                              int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_ccp(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int,
                                         cudaStream_t);
-extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int,
+extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int, int,
                                           int, int, cudaStream_t);
 extern "C" int hpvcd_recon_occupancy(int cfmt);
 extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaStream_t);
-extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, uint8_t*, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_mc(const DevPic*, int, int, int, cudaStream_t);
 extern "C" hpvcd_status hpvcd_mlp_pick(hpvcd_mlp*, const float*, uint32_t, void*, uint32_t*);
@@ -186,6 +186,7 @@ struct hpvcd_plan {
     std::vector<hpvcd_canvas> canvases;   // resolved canvas list (>= 1 for RGB8)
     std::vector<uint64_t> canvas_offs;
     hpvcd_sched sched{};
+    bool recon_feat = false;  // k_recon with slices / tiles, constrained intra or cross-component tests
     int cfmt = 0;  // k_recon shared-memory layout: 0 4:2:0 / 4:0:0, 1 4:4:4 (fits all), 2 4:2:2
     int recon_occ = 1;  // k_recon CTAs per SM at full occupancy
     int sms = 148;
@@ -204,6 +205,13 @@ struct hpvcd_plan {
     GroupStreams own;                  // used when the plan is not lent a set
     const GroupStreams* gs = nullptr;  // the set the launches use
 
+    // whether SAO of a segment must respect slice / tile boundaries
+    bool seg_sao_gated(const Segment& s) const {
+        for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
+            if (src[i].ctb_region && (src[i].flags & (HPVCD_PIC_SAO_NO_ACROSS_SLICES | HPVCD_PIC_SAO_NO_ACROSS_TILES)))
+                return true;
+        return false;
+    }
     // whether a segment has cross-component pictures (k_ccp runs for it)
     bool seg_ccp(const Segment& s) const {
         for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
@@ -399,6 +407,9 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     }
     bool any_inter = false;
     for (uint32_t i = 0; i < n; ++i) {
+        if (pics[i].ctb_region ||
+            (pics[i].flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT)))
+            P->recon_feat = true;
         if (pics[i].chroma_idc == 3) P->cfmt = 1;
         if (pics[i].chroma_idc == 2 && P->cfmt == 0) P->cfmt = 2;
         if (pics[i].flags & HPVCD_PIC_INTER) any_inter = true;
@@ -706,7 +717,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             const int share = P->concurrent ? std::max(1, P->sms * occ / (int)n_seg) : P->sms * occ;
             const int grid = std::max(1, std::min<int>(share, (int)s.n_items));
             e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
-                                   P->cfmt, grid, (int)P->sched.luma_team, st);
+                                   P->cfmt, grid, (int)P->sched.luma_team, P->recon_feat ? 1 : 0, st);
             if (e != cudaSuccess) return cuda_status(e);
         }
         if (stages & HPVCD_STAGE_DEBLOCK) {
@@ -715,7 +726,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             if (e != cudaSuccess) return cuda_status(e);
         }
         if (stages & HPVCD_STAGE_SAO) {
-            e = hpvcd_launch_sao(dp, (int)s.n_pics, s.max_sao, st);
+            e = hpvcd_launch_sao(dp, (int)s.n_pics, s.max_sao, P->seg_sao_gated(s) ? 1 : 0, st);
             if (e != cudaSuccess) return cuda_status(e);
         }
         if (P->concurrent) {
@@ -1782,6 +1793,7 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
         const int cfmt = p.chroma_idc == 3 ? 1 : (p.chroma_idc == 2 ? 2 : 0);
         const int grid = std::max(1, std::min<int>(nd->sms * nd->occ[cfmt], (int)n_ctu));
         e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, cfmt, grid, 1,
+                               (p.ctb_region || (p.flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT))) ? 1 : 0,
                                st);
         if (e != cudaSuccess) return cuda_status(e);
     }
@@ -1791,7 +1803,10 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
     const int ch = d.idc ? (d.ch >= 10 ? (d.ch - 2) / 8 : 0) * (d.cw / 4) : 0;
     e = hpvcd_launch_deblock(dp, 1, std::max(lv, cv), 1, st);
     if (e == cudaSuccess) e = hpvcd_launch_deblock(dp, 1, std::max(lh, ch), 0, st);
-    if (e == cudaSuccess && sao_active(p)) e = hpvcd_launch_sao(dp, 1, d.w * d.h, st);
+    if (e == cudaSuccess && sao_active(p))
+        e = hpvcd_launch_sao(dp, 1, d.w * d.h,
+                             p.ctb_region && (p.flags & (HPVCD_PIC_SAO_NO_ACROSS_SLICES | HPVCD_PIC_SAO_NO_ACROSS_TILES)),
+                             st);
     if (e == cudaSuccess && dev_status)
         e = cudaMemcpyAsync(dev_status, d_err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
     return cuda_status(e);
