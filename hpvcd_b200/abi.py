@@ -73,7 +73,7 @@ def REF_DPB(e: int) -> int:
 
 DPB_MAX_READERS = 64
 
-OUT_YUV, OUT_RGB8 = 0, 1
+OUT_YUV, OUT_RGB8, OUT_YUV_CANVAS = 0, 1, 2
 MATRIX_IDENTITY, MATRIX_BT709, MATRIX_BT470BG = 0, 1, 5
 MATRIX_SMPTE170M, MATRIX_YCGCO, MATRIX_BT2020NCL = 6, 8, 9
 

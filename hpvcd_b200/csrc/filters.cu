@@ -464,6 +464,37 @@ __global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out
     }
 }
 
+// Native YCbCr canvas (lib.rs:871-991 stitch_native_yuv_band): component
+// blockIdx.z of picture blockIdx.y copied onto its canvas plane at (dst_x,
+// dst_y) / subsampling, rows and columns past the picture repeating its last
+// one, four samples per thread.  The canvas holds Y, then Cb, then Cr, in
+// the picture's sample size.
+__global__ void k_yuv_canvas(const DevPic* __restrict__ pics, uint8_t* __restrict__ out) {
+    const DevPic& P = pics[blockIdx.y];
+    const int c = blockIdx.z;
+    if (c > 0 && P.idc == 0) return;
+    const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
+    const int CW = (P.canvas_w + sw - 1) / sw, CH = (P.canvas_h + sh - 1) / sh;
+    const int dx = P.dst_x / sw, dy = P.dst_y / sh;
+    const int copy_w = min((P.crop_w + sw - 1) / sw, max(CW - dx, 0));
+    const int copy_h = min((P.crop_h + sh - 1) / sh, max(CH - dy, 0));
+    const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+    const size_t luma_bytes = (size_t)P.canvas_w * P.canvas_h * P.bps;
+    const size_t chroma_bytes = (size_t)CW * CH * P.bps;
+    uint8_t* plane = out + P.canvas_off + (c == 0 ? 0 : luma_bytes + (c - 1) * chroma_bytes);
+    const int qw = (copy_w + 3) >> 2;
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < qw * copy_h; id += gridDim.x * blockDim.x) {
+        const int x0 = (id % qw) * 4, y = id / qw;
+        const size_t srow = (size_t)min(y, ph - 1) * pw;
+        const size_t drow = (size_t)(dy + y) * CW + dx;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int x = x0 + i;
+            if (x < copy_w) store_sample(plane, P.bps, drow + x, load_sample(P.fin[c], P.bps, srow + min(x, pw - 1)));
+        }
+    }
+}
+
 }  // namespace hpvcd
 
 extern "C" cudaError_t hpvcd_launch_deblock(const hpvcd::DevPic* pics, int n_pics, int max_segments,
@@ -506,6 +537,16 @@ extern "C" cudaError_t hpvcd_launch_rgb(const hpvcd::DevPic* pics, int n_pics, i
     const int threads = 256;
     dim3 grid(filter_blocks_x(max_quads, n_pics, threads), n_pics, 1);
     hpvcd::k_rgb<<<grid, threads, 0, stream>>>(pics, out);
+    hpvcd_note_launches(1);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t hpvcd_launch_yuv_canvas(const hpvcd::DevPic* pics, int n_pics, int max_quads, uint8_t* out,
+                                               cudaStream_t stream) {
+    if (n_pics <= 0 || max_quads <= 0) return cudaSuccess;
+    const int threads = 256;
+    dim3 grid(filter_blocks_x(max_quads, n_pics * 3, threads), n_pics, 3);
+    hpvcd::k_yuv_canvas<<<grid, threads, 0, stream>>>(pics, out);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }

@@ -28,6 +28,7 @@ extern "C" int hpvcd_recon_occupancy(int cfmt);
 extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, uint8_t*, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_yuv_canvas(const DevPic*, int, int, uint8_t*, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_mc(const DevPic*, int, int, int, cudaStream_t);
 extern "C" hpvcd_status hpvcd_mlp_pick(hpvcd_mlp*, const float*, uint32_t, void*, uint32_t*);
 extern "C" uint32_t hpvcd_mlp_variants(const hpvcd_mlp*);
@@ -81,6 +82,9 @@ hpvcd_status validate(const hpvcd_picture& p) {
     if ((p.flags & HPVCD_PIC_PRED_IN_PLANE) && !p.pred[0]) return HPVCD_ERR_INVALID_ARG;
     return HPVCD_OK;
 }
+
+// Outputs written onto canvases (pictures placed by out->place).
+bool canvas_kind(uint32_t kind) { return kind == HPVCD_OUT_RGB8 || kind == HPVCD_OUT_YUV_CANVAS; }
 
 bool sao_active(const hpvcd_picture& p) {
     return p.sao && (p.flags & (HPVCD_PIC_SAO_LUMA | HPVCD_PIC_SAO_CHROMA));
@@ -185,6 +189,7 @@ struct hpvcd_plan {
     std::vector<hpvcd_tile_place> places;
     std::vector<hpvcd_canvas> canvases;   // resolved canvas list (>= 1 for RGB8)
     std::vector<uint64_t> canvas_offs;
+    std::vector<size_t> canvas_sizes;  // bytes of each canvas
     hpvcd_sched sched{};
     bool recon_feat = false;  // k_recon with slices / tiles, constrained intra or cross-component tests
     int cfmt = 0;  // k_recon shared-memory layout: 0 4:2:0 / 4:0:0, 1 4:4:4 (fits all), 2 4:2:2
@@ -229,9 +234,9 @@ struct hpvcd_plan {
             }
             if (stages & HPVCD_STAGE_DEBLOCK) L += (s.max_dbk_v > 0) + (s.max_dbk_h > 0);
             if ((stages & HPVCD_STAGE_SAO) && s.max_sao > 0) ++L;
-            if (concurrent && (stages & HPVCD_STAGE_OUTPUT) && out.kind == HPVCD_OUT_RGB8 && s.max_rgb > 0) ++L;
+            if (concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(out.kind) && s.max_rgb > 0) ++L;
         }
-        if (!concurrent && (stages & HPVCD_STAGE_OUTPUT) && out.kind == HPVCD_OUT_RGB8 && max_rgb > 0) ++L;
+        if (!concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(out.kind) && max_rgb > 0) ++L;
         return L;
     }
 
@@ -287,16 +292,38 @@ size_t res_plane_bytes(const Geo& g) {
            2 * align_up((size_t)res_stride_of(g.cw) * g.ch * 2, 256);
 }
 
-// Bytes of the output of a batch: all RGB8 canvases, or all YUV planes.
+uint32_t n_canvases_of(const hpvcd_output* out) { return out->n_canvases ? out->n_canvases : 1; }
+
+hpvcd_canvas canvas_of(const hpvcd_output* out, uint32_t k) {
+    return out->n_canvases ? out->canvases[k]
+                           : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix, out->full_range};
+}
+
+// Sample format of a YUV canvas: that of the first picture placed on it
+// (8-bit 4:0:0 when none is).
+struct CanvasFmt {
+    int idc, bps;
+};
+CanvasFmt canvas_fmt(const hpvcd_picture* pics, uint32_t n, const hpvcd_tile_place* place, uint32_t k) {
+    for (uint32_t i = 0; i < n; ++i)
+        if (place[i].canvas == k) return CanvasFmt{pics[i].chroma_idc, geo_of(pics[i]).bps};
+    return CanvasFmt{0, 1};
+}
+
+size_t canvas_bytes_of(uint32_t kind, const hpvcd_canvas& cv, CanvasFmt f) {
+    const size_t w = cv.width, h = cv.height;
+    if (kind == HPVCD_OUT_RGB8) return w * h * 3;
+    const size_t sw = f.idc == 1 || f.idc == 2 ? 2 : 1, sh = f.idc == 1 ? 2 : 1;
+    const size_t cw = f.idc ? (w + sw - 1) / sw : 0, ch = f.idc ? (h + sh - 1) / sh : 0;
+    return (w * h + 2 * cw * ch) * (size_t)f.bps;
+}
+
+// Bytes of the output of a batch: all canvases, or all YUV planes.
 size_t output_bytes(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out) {
     size_t b = 0;
-    if (out && out->kind == HPVCD_OUT_RGB8) {
-        if (out->n_canvases) {
-            for (uint32_t k = 0; k < out->n_canvases; ++k)
-                b += (size_t)out->canvases[k].width * out->canvases[k].height * 3;
-        } else {
-            b = (size_t)out->canvas_w * out->canvas_h * 3;
-        }
+    if (out && canvas_kind(out->kind)) {
+        for (uint32_t k = 0; k < n_canvases_of(out); ++k)
+            b += canvas_bytes_of(out->kind, canvas_of(out, k), canvas_fmt(pics, n, out->place, k));
         return b;
     }
     for (uint32_t i = 0; i < n; ++i) {
@@ -364,9 +391,20 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
                 }
             }
     }
-    if (out && out->kind == HPVCD_OUT_RGB8 &&
+    if (out && canvas_kind(out->kind) &&
         (!out->place || (out->n_canvases ? !out->canvases : (out->canvas_w == 0 || out->canvas_h == 0))))
         return HPVCD_ERR_INVALID_ARG;
+    if (out && out->kind > HPVCD_OUT_YUV_CANVAS) return HPVCD_ERR_INVALID_ARG;
+    if (out && out->kind == HPVCD_OUT_YUV_CANVAS)  // every picture of a canvas in its format
+        for (uint32_t i = 0; i < n; ++i) {
+            if (out->place[i].canvas >= n_canvases_of(out)) return HPVCD_ERR_INVALID_ARG;
+            const CanvasFmt f = canvas_fmt(pics, n, out->place, out->place[i].canvas);
+            if (f.idc != pics[i].chroma_idc || f.bps != geo_of(pics[i]).bps) {
+                std::snprintf(t_last_error, sizeof(t_last_error),
+                              "picture %u differs in chroma format or sample size from its YUV canvas", i);
+                return HPVCD_ERR_INVALID_ARG;
+            }
+        }
     hpvcd_plan* P = new (std::nothrow) hpvcd_plan();
     if (!P) return HPVCD_ERR_ALLOC;
     P->alloc_stream = pool_stream;
@@ -375,19 +413,17 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     P->src.assign(pics, pics + n);
     if (out) {
         P->out = *out;
-        if (out->kind == HPVCD_OUT_RGB8) {
+        if (canvas_kind(out->kind)) {
             P->places.assign(out->place, out->place + n);
             P->out.place = nullptr;
-            if (out->n_canvases) {
-                P->canvases.assign(out->canvases, out->canvases + out->n_canvases);
-            } else {
-                P->canvases.push_back(hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix, out->full_range});
-            }
+            for (uint32_t k = 0; k < n_canvases_of(out); ++k) P->canvases.push_back(canvas_of(out, k));
             P->out.canvases = nullptr;
             uint64_t off = 0;
-            for (const hpvcd_canvas& cv : P->canvases) {
+            for (uint32_t k = 0; k < P->canvases.size(); ++k) {
                 P->canvas_offs.push_back(off);
-                off += (uint64_t)cv.width * cv.height * 3;
+                P->canvas_sizes.push_back(
+                    canvas_bytes_of(out->kind, P->canvases[k], canvas_fmt(pics, n, out->place, k)));
+                off += P->canvas_sizes.back();
             }
             for (uint32_t i = 0; i < n; ++i)
                 if (P->places[i].canvas >= P->canvases.size()) {
@@ -478,9 +514,9 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
                             pool_stream);
     if (e == cudaSuccess) e = P->dmalloc(&P->d_scratch, P->scratch_words * sizeof(uint32_t));
     if (e == cudaSuccess) e = P->dmalloc(&P->d_feat, 32 * sizeof(unsigned long long) + 16 * sizeof(float));
-    if (e == cudaSuccess && P->out.kind == HPVCD_OUT_RGB8) {
+    if (e == cudaSuccess && canvas_kind(P->out.kind)) {
         P->canvas_bytes = 0;
-        for (const hpvcd_canvas& cv : P->canvases) P->canvas_bytes += (size_t)cv.width * cv.height * 3;
+        for (const size_t b : P->canvas_sizes) P->canvas_bytes += b;
         e = P->dmalloc(&P->d_canvas, P->canvas_bytes);
         if (e == cudaSuccess) e = cudaMemsetAsync(P->d_canvas, 0, P->canvas_bytes, pool_stream);
     }
@@ -537,15 +573,17 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             d.res[2] = p.chroma_idc ? (int16_t*)(rb + ly + lc) : nullptr;
         }
         d.needs_wavefront = (p.flags & HPVCD_PIC_PRED_IN_PLANE) ? 0 : 1;
-        if (P->out.kind == HPVCD_OUT_RGB8) {
+        if (canvas_kind(P->out.kind)) {
             const hpvcd_tile_place& tp = P->places[i];
             const hpvcd_canvas& cv = P->canvases[tp.canvas];
             d.canvas_off = P->canvas_offs[tp.canvas];
             d.canvas_w = (int)cv.width; d.canvas_h = (int)cv.height;
             d.matrix = (int)cv.matrix; d.full_range = (int)cv.full_range;
             d.dst_x = (int)tp.dst_x; d.dst_y = (int)tp.dst_y;
-            d.crop_w = (int)std::min<uint32_t>(tp.crop_w, p.width);
-            d.crop_h = (int)std::min<uint32_t>(tp.crop_h, p.height);
+            // RGB8 crops at the picture; the YUV canvas repeats its last row / column
+            const bool rgb = P->out.kind == HPVCD_OUT_RGB8;
+            d.crop_w = (int)(rgb ? std::min<uint32_t>(tp.crop_w, p.width) : std::min<uint32_t>(tp.crop_w, 65536));
+            d.crop_h = (int)(rgb ? std::min<uint32_t>(tp.crop_h, p.height) : std::min<uint32_t>(tp.crop_h, 65536));
             P->max_rgb = std::max(P->max_rgb, (d.crop_w + 3) / 4 * d.crop_h);  // 4-pixel quads
         }
     }
@@ -625,7 +663,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             s.max_dbk_v = std::max(s.max_dbk_v, std::max(lv, cv));
             s.max_dbk_h = std::max(s.max_dbk_h, std::max(lh, ch));
             if (d.rec[0] != d.fin[0]) s.max_sao = std::max(s.max_sao, d.w * d.h);
-            if (P->out.kind == HPVCD_OUT_RGB8) s.max_rgb = std::max(s.max_rgb, (d.crop_w + 3) / 4 * d.crop_h);
+            if (canvas_kind(P->out.kind)) s.max_rgb = std::max(s.max_rgb, (d.crop_w + 3) / 4 * d.crop_h);
         }
     }
     e = P->dmalloc(&P->d_pics, sizeof(DevPic) * P->pics.size());
@@ -730,8 +768,10 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             if (e != cudaSuccess) return cuda_status(e);
         }
         if (P->concurrent) {
-            if ((stages & HPVCD_STAGE_OUTPUT) && P->out.kind == HPVCD_OUT_RGB8) {
-                e = hpvcd_launch_rgb(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st);
+            if ((stages & HPVCD_STAGE_OUTPUT) && canvas_kind(P->out.kind)) {
+                e = P->out.kind == HPVCD_OUT_RGB8 ? hpvcd_launch_rgb(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st)
+                                                  : hpvcd_launch_yuv_canvas(dp, (int)s.n_pics, s.max_rgb,
+                                                                            P->d_canvas, st);
                 if (e != cudaSuccess) return cuda_status(e);
             }
             e = cudaEventRecord(P->gs->ev_join[si], st);  // join back into the launching stream
@@ -740,8 +780,10 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
         }
     }
     st = origin;
-    if (!P->concurrent && (stages & HPVCD_STAGE_OUTPUT) && P->out.kind == HPVCD_OUT_RGB8) {
-        e = hpvcd_launch_rgb(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
+    if (!P->concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(P->out.kind)) {
+        e = P->out.kind == HPVCD_OUT_RGB8
+                ? hpvcd_launch_rgb(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st)
+                : hpvcd_launch_yuv_canvas(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
         if (e != cudaSuccess) return cuda_status(e);
     }
     return HPVCD_OK;
@@ -785,7 +827,7 @@ bool same_layout(const hpvcd_plan* P, const hpvcd_picture* pics, uint32_t n, con
     }
     const uint32_t kind = out ? out->kind : HPVCD_OUT_YUV;
     if (kind != P->out.kind) return false;
-    if (kind == HPVCD_OUT_RGB8) {
+    if (canvas_kind(kind)) {
         const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
         if (nc != P->canvases.size()) return false;
         for (uint32_t k = 0; k < nc; ++k) {
@@ -1351,7 +1393,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         const hpvcd_status s = validate(pics[i]);
         if (s != HPVCD_OK) return s;
     }
-    if (out && out->kind == HPVCD_OUT_RGB8 &&
+    if (out && canvas_kind(out->kind) &&
         (!out->place || (out->n_canvases ? !out->canvases : (!out->canvas_w || !out->canvas_h))))
         return HPVCD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g->mu);
@@ -1416,7 +1458,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     const uint64_t plan_bytes = reuse ? slot->plan_bytes : plan_footprint(pics, n, out);
     const uint64_t need = std::max<uint64_t>(slot->d_in_cap, align_up(total + total / 4, 1 << 20)) + plan_bytes;
     if (g->in_use - held + need > g->budget) return HPVCD_ERR_ALLOC;
-    const bool per_canvas_out = out && out->kind == HPVCD_OUT_RGB8 && out->n_canvases && out->canvas_dst;
+    const bool per_canvas_out = out && canvas_kind(out->kind) && out->n_canvases && out->canvas_dst;
     const bool direct_out = per_canvas_out ||
                             (out && out->host_dst && out->host_dst_bytes >= out_bytes && is_pinned(out->host_dst));
     hpvcd_status st = all_pinned ? HPVCD_OK : grow_pinned(&slot->h_in, &slot->h_in_cap, total);
@@ -1485,10 +1527,9 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     slot->direct_out = direct_out ? (per_canvas_out ? (void*)1 : out->host_dst) : nullptr;
     if (per_canvas_out) {  // each canvas straight into its own buffer
         for (size_t k = 0; k < P->canvases.size() && e == cudaSuccess; ++k)
-            e = cudaMemcpyAsync(out->canvas_dst[k], P->d_canvas + P->canvas_offs[k],
-                                (size_t)P->canvases[k].width * P->canvases[k].height * 3, cudaMemcpyDeviceToHost,
-                                slot->stream);
-    } else if (P->out.kind == HPVCD_OUT_RGB8) {
+            e = cudaMemcpyAsync(out->canvas_dst[k], P->d_canvas + P->canvas_offs[k], P->canvas_sizes[k],
+                                cudaMemcpyDeviceToHost, slot->stream);
+    } else if (canvas_kind(P->out.kind)) {
         e = cudaMemcpyAsync(host_out, P->d_canvas, P->canvas_bytes, cudaMemcpyDeviceToHost, slot->stream);
     } else {
         size_t o = 0;

@@ -173,6 +173,31 @@ def pack_pinned(pics):
     return list(out), (keep, buf, nb)
 
 
+def yuv_canvas_planes(pics, out: abi.Output, raw: np.ndarray):
+    """Split an HPVCD_OUT_YUV_CANVAS output into (Y, Cb, Cr) arrays per
+    canvas (native sample type; Cb / Cr empty for 4:0:0).  A canvas has the
+    chroma format and sample size of the first picture placed on it."""
+    n_c = out.n_canvases or 1
+    cv = (abi.Canvas * out.n_canvases).from_address(out.canvases) if out.n_canvases else None
+    place = (abi.TilePlace * len(pics)).from_address(out.place)
+    res, off = [], 0
+    for k in range(n_c):
+        w, h = (cv[k].width, cv[k].height) if cv is not None else (out.canvas_w, out.canvas_h)
+        first = next((p for i, p in enumerate(pics) if place[i].canvas == k), None)
+        idc = first.chroma_idc if first is not None else 0
+        bps = 1 if first is None or (first.bit_depth_y <= 8 and first.bit_depth_c <= 8) else 2
+        sw, sh = (2 if idc in (1, 2) else 1), (2 if idc == 1 else 1)
+        cw, ch = ((w + sw - 1) // sw, (h + sh - 1) // sh) if idc else (0, 0)
+        dt = np.uint8 if bps == 1 else np.uint16
+        planes = []
+        for (pw, ph) in [(w, h), (cw, ch), (cw, ch)]:
+            nb = pw * ph * bps
+            planes.append(raw[off:off + nb].view(dt).reshape(ph, pw))
+            off += nb
+        res.append(tuple(planes))
+    return res
+
+
 def split_planes(pics, raw: np.ndarray):
     out = []
     o = 0

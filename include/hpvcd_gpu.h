@@ -256,6 +256,16 @@ typedef struct hpvcd_picture {
  * the part of a tile outside the canvas is cropped. */
 #define HPVCD_OUT_YUV 0u  /* per-picture planes                              */
 #define HPVCD_OUT_RGB8 1u /* packed RGB8 canvas                               */
+/* Native YCbCr canvas, the `decode_heic_yuv` grid path (lib.rs:993-1091
+ * fill_native_grid_yuv / stitch_native_yuv_band): per canvas its Y plane
+ * (width x height), then Cb and Cr (ceil(width / SubWidthC) x
+ * ceil(height / SubHeightC)), one byte per sample at 8 bits, two otherwise.
+ * A canvas takes the chroma format and bit depth of its pictures (all equal;
+ * 8-bit 4:0:0 when none is placed on it).  Picture i fills
+ * ceil(crop_w / SubWidthC) x ceil(crop_h / SubHeightC) chroma samples from
+ * (dst_x / SubWidthC, dst_y / SubHeightC), rows and columns past the picture
+ * repeating its last one; matrix and range are not used. */
+#define HPVCD_OUT_YUV_CANVAS 2u
 
 /* Matrix coefficients as in src/color.rs `MatrixCoefficients` (H.273 values). */
 #define HPVCD_MATRIX_IDENTITY 0u

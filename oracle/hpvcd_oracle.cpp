@@ -1495,6 +1495,66 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
             if (g.idc && planes_out[i].cr) std::memcpy(planes_out[i].cr, pl[i].cr, (size_t)g.cw * g.ch * 2);
         }
     }
+    if (out && out->kind == HPVCD_OUT_YUV_CANVAS && rgb && out->place) {
+        // lib.rs:993-1091 fill_native_grid_yuv and :871-991
+        // stitch_native_yuv_band: each tile's visible part copied onto the
+        // image planes at its grid position (chroma at position / subsampling),
+        // rows past the tile repeating its last row, columns its last sample.
+        const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
+        for (uint32_t i = 0; i < n; ++i)
+            if (out->place[i].canvas >= nc) return HPVCD_ERR_INVALID_ARG;
+        struct Cv { int w, h, idc, bps, sw, sh, cw, ch; size_t off; };
+        std::vector<Cv> cvs;
+        size_t acc = 0;
+        for (uint32_t k = 0; k < nc; ++k) {
+            Cv c{};
+            c.w = (int)(out->n_canvases ? out->canvases[k].width : out->canvas_w);
+            c.h = (int)(out->n_canvases ? out->canvases[k].height : out->canvas_h);
+            c.idc = 0;
+            c.bps = 1;
+            for (uint32_t i = 0; i < n; ++i)
+                if (out->place[i].canvas == k) {
+                    c.idc = pics[i].chroma_idc;
+                    c.bps = geo_of(&pics[i]).bd > 8 || geo_of(&pics[i]).bd_c > 8 ? 2 : 1;
+                    break;
+                }
+            c.sw = c.idc == 1 || c.idc == 2 ? 2 : 1;
+            c.sh = c.idc == 1 ? 2 : 1;
+            c.cw = c.idc ? (c.w + c.sw - 1) / c.sw : 0;
+            c.ch = c.idc ? (c.h + c.sh - 1) / c.sh : 0;
+            c.off = acc;
+            acc += ((size_t)c.w * c.h + 2 * (size_t)c.cw * c.ch) * c.bps;
+            cvs.push_back(c);
+        }
+        for (uint32_t i = 0; i < n; ++i) {
+            const Geo g = geo_of(&pics[i]);
+            const hpvcd_tile_place& tp = out->place[i];
+            const Cv& c = cvs[tp.canvas];
+            if (c.idc != g.idc || c.bps != (g.bd > 8 || g.bd_c > 8 ? 2 : 1)) return HPVCD_ERR_INVALID_ARG;
+            for (int comp = 0; comp < (g.idc ? 3 : 1); ++comp) {
+                const int sw = comp ? c.sw : 1, sh = comp ? c.sh : 1;
+                const int CW = comp ? c.cw : c.w, CH = comp ? c.ch : c.h;
+                const int pw = comp ? g.cw : g.w, ph = comp ? g.ch : g.h;
+                const int dx = (int)tp.dst_x / sw, dy = (int)tp.dst_y / sh;
+                const int copy_w = std::min(((int)tp.crop_w + sw - 1) / sw, std::max(CW - dx, 0));
+                const int copy_h = std::min(((int)tp.crop_h + sh - 1) / sh, std::max(CH - dy, 0));
+                const uint16_t* src = comp == 0 ? pl[i].y : (comp == 1 ? pl[i].cb : pl[i].cr);
+                uint8_t* base = rgb + c.off +
+                                (comp == 0 ? 0 : ((size_t)c.w * c.h + (size_t)(comp - 1) * c.cw * c.ch) * c.bps);
+                for (int y = 0; y < copy_h; ++y)
+                    for (int x = 0; x < copy_w; ++x) {
+                        const uint16_t v = src[(size_t)std::min(y, ph - 1) * pw + std::min(x, pw - 1)];
+                        const size_t o = (size_t)(dy + y) * CW + dx + x;
+                        if (c.bps == 1) {
+                            base[o] = (uint8_t)v;
+                        } else {
+                            base[2 * o] = (uint8_t)v;
+                            base[2 * o + 1] = (uint8_t)(v >> 8);
+                        }
+                    }
+            }
+        }
+    }
     if (out && out->kind == HPVCD_OUT_RGB8 && rgb && out->place) {
         // lib.rs:1610-1660 per-tile RGB then row copy with cropping;
         // lib.rs:1964-1978 rgb8 narrowing by >> (bit_depth - 8).

@@ -216,6 +216,32 @@ def yuv_to_rgb16(y, cb, cr, width, height, chroma_idc, bd, dw, dh, matrix, full_
     return out
 
 
+def yuv_canvas_layout(pics, out):
+    """Per canvas of an OUT_YUV_CANVAS output: (offset, width, height,
+    chroma_idc, bytes per sample); a canvas takes its first picture's format."""
+    n_c = out.n_canvases or 1
+    cv = (abi.Canvas * out.n_canvases).from_address(out.canvases) if out.n_canvases else None
+    place = (abi.TilePlace * len(pics)).from_address(out.place)
+    res, off = [], 0
+    for k in range(n_c):
+        w, h = (cv[k].width, cv[k].height) if cv is not None else (out.canvas_w, out.canvas_h)
+        idc, bps = 0, 1
+        for i, p in enumerate(pics):
+            if place[i].canvas == k:
+                idc, bps = p.chroma_idc, 1 if p.bit_depth_y <= 8 and p.bit_depth_c <= 8 else 2
+                break
+        sw = 2 if idc in (1, 2) else 1
+        sh = 2 if idc == 1 else 1
+        cw, ch = ((w + sw - 1) // sw, (h + sh - 1) // sh) if idc else (0, 0)
+        res.append((off, w, h, idc, bps))
+        off += (w * h + 2 * cw * ch) * bps
+    return res, off
+
+
+def yuv_canvas_bytes(pics, out) -> int:
+    return yuv_canvas_layout(pics, out)[1]
+
+
 def decode_batch(pics, out=None, want_planes=True, threads=1):
     """Oracle decode of a list of abi.Picture; returns (planes list, rgb canvas or None)."""
     n = len(pics)
@@ -240,6 +266,8 @@ def decode_batch(pics, out=None, want_planes=True, threads=1):
             rgb = np.zeros(sum(c.width * c.height * 3 for c in cv), np.uint8)
         else:
             rgb = np.zeros((out.canvas_h, out.canvas_w, 3), np.uint8)
+    elif out is not None and out.kind == abi.OUT_YUV_CANVAS:
+        rgb = np.zeros(yuv_canvas_bytes(pics, out), np.uint8)
     rc = lib().orc_decode_batch(arr, u32(n), C.byref(out) if out is not None else None,
                                 pl_arr if want_planes else None,
                                 _p(rgb) if rgb is not None else None, i32(threads))

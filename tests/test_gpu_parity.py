@@ -819,3 +819,59 @@ def test_constrained_intra(dec, bd, idc):
             c.regions = 1
         s.add(c)
     run_yuv(dec, s.pictures(), f"constrained intra {bd}-bit idc {idc}")
+
+
+# --- native YCbCr canvas output (decode_heic_yuv of a grid) -----------------
+@pytest.mark.parametrize("bd,idc", [(10, 1), (8, 1), (8, 2), (12, 3), (10, 0)])
+def test_yuv_canvas_grid(dec, bd, idc):
+    from hpvcd_b200.gpu import yuv_canvas_planes
+    g = synth.make_grid(1100, 700, seed=600 + bd + idc, bit_depth=bd, chroma_idc=idc)
+    pics = g.synth.pictures()
+    out, keep = synth.grid_output(g)
+    out.kind = abi.OUT_YUV_CANVAS
+    t = dec.submit(pics, out)
+    dec.wait(t)
+    got = dec.read(t)
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    assert got.size == ref.size and np.array_equal(got, ref)
+    (Y, Cb, Cr), = yuv_canvas_planes(pics, out, got)
+    assert Y.shape == (700, 1100)
+
+
+def test_yuv_canvas_multi_and_plan():
+    import ctypes as C
+    from hpvcd_b200.gpu import yuv_canvas_planes
+    s = synth.SynthSet()
+    pics, places, canv = [], [], []
+    for k, (seed, w, h, bd, idc) in enumerate([(1, 700, 500, 8, 1), (2, 512, 512, 10, 3), (3, 300, 900, 8, 2)]):
+        p, pl = _image(620 + seed, w, h, bd, idc, s)
+        pics += p
+        places += [(x, y, cw, ch, k) for (x, y, cw, ch) in pl]
+        canv.append(abi.Canvas(w, h, 0, 0))
+    pl_arr = (abi.TilePlace * len(places))(*[abi.TilePlace(*t) for t in places])
+    cv_arr = (abi.Canvas * len(canv))(*canv)
+    out = abi.Output(abi.OUT_YUV_CANVAS, 0, 0, 0, 0, C.cast(pl_arr, C.c_void_p), None, 0, len(canv),
+                     C.cast(cv_arr, C.c_void_p))
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    plan = DevicePlan(pics, out)
+    plan.launch(abi.STAGE_ALL | abi.STAGE_GRAPH)
+    torch.cuda.synchronize()
+    ptr, nb = plan.canvas_ptr()
+    got = np.empty(nb, np.uint8)
+    abi.check(abi.lib().hpvcd_copy(got.ctypes.data_as(C.c_void_p), C.c_void_p(ptr), nb, None), "copy")
+    assert nb == ref.size and np.array_equal(got, ref)
+    assert [y.shape for y, _, _ in yuv_canvas_planes(pics, out, got)] == [(500, 700), (512, 512), (900, 300)]
+    plan.close()
+
+
+def test_yuv_canvas_rejects_mixed_formats(dec):
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(630, 256, 256, bit_depth=8, chroma_idc=1))
+    s.add(synth.intra_cfg(631, 256, 256, bit_depth=10, chroma_idc=1))
+    pics = s.pictures()
+    g = synth.Grid(512, 256, 256, s, [(0, 0, 256, 256), (256, 0, 256, 256)])
+    out, keep = synth.grid_output(g)
+    out.kind = abi.OUT_YUV_CANVAS
+    with pytest.raises(abi.HpvcdError) as e:
+        dec.submit(pics, out)
+    assert e.value.status == abi.ERR_INVALID_ARG

@@ -379,3 +379,31 @@ def test_rext_residual_ops():
     want = (np.cumsum(big.reshape(8, 8).astype(np.int64), axis=0) + 32768) % 65536 - 32768
     assert np.array_equal(w, want)
     assert np.array_equal(O.rext_residual_ops(big, 8, rdpcm=1).reshape(8, 8), np.cumsum(big.reshape(8, 8), axis=0))
+
+
+@pytest.mark.parametrize("bd,idc", [(8, 1), (10, 2), (12, 3), (8, 0)])
+def test_yuv_canvas_stitch_matches_planes(bd, idc):
+    """lib.rs:871-991: the oracle's native YUV canvas is the tiles' planes
+    copied to their grid positions (checked here against numpy slicing of
+    the same decode, crops at the canvas edge included)."""
+    import ctypes as C
+    from hpvcd_b200 import synth
+    from hpvcd_b200.gpu import yuv_canvas_planes
+    g = synth.make_grid(200, 136, seed=7 + bd + idc, bit_depth=bd, chroma_idc=idc, tile=64, sao=False)
+    pics = g.synth.pictures()
+    out, keep = synth.grid_output(g)
+    out.kind = O.abi.OUT_YUV_CANVAS
+    planes, raw = O.decode_batch(pics, out)
+    (Y, Cb, Cr), = yuv_canvas_planes(pics, out, raw)
+    sw, sh = (2 if idc in (1, 2) else 1), (2 if idc == 1 else 1)
+    want = [np.zeros(Y.shape, np.uint16), np.zeros(Cb.shape, np.uint16), np.zeros(Cr.shape, np.uint16)]
+    for pl, (x, y, cw, ch) in zip(planes, g.places):
+        for c in range(3 if idc else 1):
+            s_w, s_h = (sw, sh) if c else (1, 1)
+            W = want[c]
+            dx, dy = x // s_w, y // s_h
+            tw, th = -(-cw // s_w), -(-ch // s_h)
+            tw, th = min(tw, W.shape[1] - dx), min(th, W.shape[0] - dy)
+            W[dy:dy + th, dx:dx + tw] = pl[c][:th, :tw]
+    for c, got in enumerate((Y, Cb, Cr)):
+        assert np.array_equal(got.astype(np.uint16), want[c]), c
