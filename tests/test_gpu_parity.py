@@ -854,7 +854,10 @@ def test_yuv_canvas_multi_and_plan():
                      C.cast(cv_arr, C.c_void_p))
     _, ref = O.decode_batch(pics, out, want_planes=False)
     plan = DevicePlan(pics, out)
-    plan.launch(abi.STAGE_ALL | abi.STAGE_GRAPH)
+    st = torch.cuda.Stream()          # graph capture needs a non-default stream
+    with torch.cuda.stream(st):
+        plan.launch(abi.STAGE_ALL | abi.STAGE_GRAPH, st)
+        plan.launch(abi.STAGE_ALL | abi.STAGE_GRAPH, st)
     torch.cuda.synchronize()
     ptr, nb = plan.canvas_ptr()
     got = np.empty(nb, np.uint8)
