@@ -76,6 +76,7 @@ DPB_MAX_READERS = 64
 OUT_YUV, OUT_RGB8, OUT_YUV_CANVAS = 0, 1, 2
 MATRIX_IDENTITY, MATRIX_BT709, MATRIX_BT470BG = 0, 1, 5
 MATRIX_SMPTE170M, MATRIX_YCGCO, MATRIX_BT2020NCL = 6, 8, 9
+CANVAS_NATIVE = 0x100  # hpvcd_canvas.matrix: native YCbCr planes on an RGB8 output
 
 STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_OUTPUT = 0x1, 0x2, 0x4, 0x8
 STAGE_ALL = 0xF

@@ -418,6 +418,7 @@ __device__ __forceinline__ uint32_t rgb_px(const RgbCoef& k, int idc, int luma, 
 
 __global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out) {
     const DevPic& P = pics[blockIdx.y];
+    if (P.matrix == (int)HPVCD_CANVAS_NATIVE) return;  // k_yuv_canvas's picture
     uint8_t* canvas = out + P.canvas_off;
     const int copy_w = min(P.crop_w, max(P.canvas_w - P.dst_x, 0));
     const int copy_h = min(P.crop_h, max(P.canvas_h - P.dst_y, 0));
@@ -472,6 +473,7 @@ __global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out
 __global__ void k_yuv_canvas(const DevPic* __restrict__ pics, uint8_t* __restrict__ out) {
     const DevPic& P = pics[blockIdx.y];
     const int c = blockIdx.z;
+    if (P.matrix != (int)HPVCD_CANVAS_NATIVE) return;  // k_rgb's picture
     if (c > 0 && P.idc == 0) return;
     const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
     const int CW = (P.canvas_w + sw - 1) / sw, CH = (P.canvas_h + sh - 1) / sh;

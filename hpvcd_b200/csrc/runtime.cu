@@ -190,6 +190,7 @@ struct hpvcd_plan {
     std::vector<hpvcd_canvas> canvases;   // resolved canvas list (>= 1 for RGB8)
     std::vector<uint64_t> canvas_offs;
     std::vector<size_t> canvas_sizes;  // bytes of each canvas
+    bool any_rgb_canvas = false, any_native_canvas = false;  // which output kernels run
     hpvcd_sched sched{};
     bool recon_feat = false;  // k_recon with slices / tiles, constrained intra or cross-component tests
     int cfmt = 0;  // k_recon shared-memory layout: 0 4:2:0 / 4:0:0, 1 4:4:4 (fits all), 2 4:2:2
@@ -234,9 +235,11 @@ struct hpvcd_plan {
             }
             if (stages & HPVCD_STAGE_DEBLOCK) L += (s.max_dbk_v > 0) + (s.max_dbk_h > 0);
             if ((stages & HPVCD_STAGE_SAO) && s.max_sao > 0) ++L;
-            if (concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(out.kind) && s.max_rgb > 0) ++L;
+            if (concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(out.kind) && s.max_rgb > 0)
+                L += (uint32_t)any_rgb_canvas + (uint32_t)any_native_canvas;
         }
-        if (!concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(out.kind) && max_rgb > 0) ++L;
+        if (!concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(out.kind) && max_rgb > 0)
+            L += (uint32_t)any_rgb_canvas + (uint32_t)any_native_canvas;
         return L;
     }
 
@@ -310,9 +313,15 @@ CanvasFmt canvas_fmt(const hpvcd_picture* pics, uint32_t n, const hpvcd_tile_pla
     return CanvasFmt{0, 1};
 }
 
+// Canvas receiving native YCbCr planes (every canvas of a YUV canvas output,
+// HPVCD_CANVAS_NATIVE ones of an RGB8 output).
+bool native_canvas(uint32_t kind, const hpvcd_canvas& cv) {
+    return kind == HPVCD_OUT_YUV_CANVAS || cv.matrix == HPVCD_CANVAS_NATIVE;
+}
+
 size_t canvas_bytes_of(uint32_t kind, const hpvcd_canvas& cv, CanvasFmt f) {
     const size_t w = cv.width, h = cv.height;
-    if (kind == HPVCD_OUT_RGB8) return w * h * 3;
+    if (!native_canvas(kind, cv)) return w * h * 3;
     const size_t sw = f.idc == 1 || f.idc == 2 ? 2 : 1, sh = f.idc == 1 ? 2 : 1;
     const size_t cw = f.idc ? (w + sw - 1) / sw : 0, ch = f.idc ? (h + sh - 1) / sh : 0;
     return (w * h + 2 * cw * ch) * (size_t)f.bps;
@@ -395,9 +404,10 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         (!out->place || (out->n_canvases ? !out->canvases : (out->canvas_w == 0 || out->canvas_h == 0))))
         return HPVCD_ERR_INVALID_ARG;
     if (out && out->kind > HPVCD_OUT_YUV_CANVAS) return HPVCD_ERR_INVALID_ARG;
-    if (out && out->kind == HPVCD_OUT_YUV_CANVAS)  // every picture of a canvas in its format
+    if (out && canvas_kind(out->kind))  // every picture of a native canvas in its format
         for (uint32_t i = 0; i < n; ++i) {
             if (out->place[i].canvas >= n_canvases_of(out)) return HPVCD_ERR_INVALID_ARG;
+            if (!native_canvas(out->kind, canvas_of(out, out->place[i].canvas))) continue;
             const CanvasFmt f = canvas_fmt(pics, n, out->place, out->place[i].canvas);
             if (f.idc != pics[i].chroma_idc || f.bps != geo_of(pics[i]).bps) {
                 std::snprintf(t_last_error, sizeof(t_last_error),
@@ -578,10 +588,12 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             const hpvcd_canvas& cv = P->canvases[tp.canvas];
             d.canvas_off = P->canvas_offs[tp.canvas];
             d.canvas_w = (int)cv.width; d.canvas_h = (int)cv.height;
-            d.matrix = (int)cv.matrix; d.full_range = (int)cv.full_range;
+            const bool rgb = !native_canvas(P->out.kind, cv);
+            d.matrix = rgb ? (int)cv.matrix : (int)HPVCD_CANVAS_NATIVE;  // selects k_rgb or k_yuv_canvas
+            d.full_range = (int)cv.full_range;
+            (rgb ? P->any_rgb_canvas : P->any_native_canvas) = true;
             d.dst_x = (int)tp.dst_x; d.dst_y = (int)tp.dst_y;
-            // RGB8 crops at the picture; the YUV canvas repeats its last row / column
-            const bool rgb = P->out.kind == HPVCD_OUT_RGB8;
+            // RGB8 crops at the picture; a native canvas repeats its last row / column
             d.crop_w = (int)(rgb ? std::min<uint32_t>(tp.crop_w, p.width) : std::min<uint32_t>(tp.crop_w, 65536));
             d.crop_h = (int)(rgb ? std::min<uint32_t>(tp.crop_h, p.height) : std::min<uint32_t>(tp.crop_h, 65536));
             P->max_rgb = std::max(P->max_rgb, (d.crop_w + 3) / 4 * d.crop_h);  // 4-pixel quads
@@ -769,9 +781,9 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
         }
         if (P->concurrent) {
             if ((stages & HPVCD_STAGE_OUTPUT) && canvas_kind(P->out.kind)) {
-                e = P->out.kind == HPVCD_OUT_RGB8 ? hpvcd_launch_rgb(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st)
-                                                  : hpvcd_launch_yuv_canvas(dp, (int)s.n_pics, s.max_rgb,
-                                                                            P->d_canvas, st);
+                if (P->any_rgb_canvas) e = hpvcd_launch_rgb(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st);
+                if (e == cudaSuccess && P->any_native_canvas)
+                    e = hpvcd_launch_yuv_canvas(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st);
                 if (e != cudaSuccess) return cuda_status(e);
             }
             e = cudaEventRecord(P->gs->ev_join[si], st);  // join back into the launching stream
@@ -781,9 +793,9 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
     }
     st = origin;
     if (!P->concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(P->out.kind)) {
-        e = P->out.kind == HPVCD_OUT_RGB8
-                ? hpvcd_launch_rgb(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st)
-                : hpvcd_launch_yuv_canvas(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
+        if (P->any_rgb_canvas) e = hpvcd_launch_rgb(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
+        if (e == cudaSuccess && P->any_native_canvas)
+            e = hpvcd_launch_yuv_canvas(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
         if (e != cudaSuccess) return cuda_status(e);
     }
     return HPVCD_OK;

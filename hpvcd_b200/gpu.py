@@ -173,16 +173,24 @@ def pack_pinned(pics):
     return list(out), (keep, buf, nb)
 
 
-def yuv_canvas_planes(pics, out: abi.Output, raw: np.ndarray):
-    """Split an HPVCD_OUT_YUV_CANVAS output into (Y, Cb, Cr) arrays per
-    canvas (native sample type; Cb / Cr empty for 4:0:0).  A canvas has the
-    chroma format and sample size of the first picture placed on it."""
+def canvas_views(pics, out: abi.Output, raw: np.ndarray):
+    """Split the output of a canvas batch (RGB8 or YUV canvas) into one view
+    per canvas: an (h, w, 3) uint8 array for an RGB8 canvas, a (Y, Cb, Cr)
+    tuple in native sample type for a native one (every canvas of an
+    OUT_YUV_CANVAS output, CANVAS_NATIVE ones of an RGB8 output; Cb / Cr
+    empty for 4:0:0).  A native canvas has the chroma format and sample size
+    of the first picture placed on it."""
     n_c = out.n_canvases or 1
     cv = (abi.Canvas * out.n_canvases).from_address(out.canvases) if out.n_canvases else None
     place = (abi.TilePlace * len(pics)).from_address(out.place)
     res, off = [], 0
     for k in range(n_c):
         w, h = (cv[k].width, cv[k].height) if cv is not None else (out.canvas_w, out.canvas_h)
+        matrix = cv[k].matrix if cv is not None else out.matrix
+        if out.kind == abi.OUT_RGB8 and matrix != abi.CANVAS_NATIVE:
+            res.append(raw[off:off + w * h * 3].reshape(h, w, 3))
+            off += w * h * 3
+            continue
         first = next((p for i, p in enumerate(pics) if place[i].canvas == k), None)
         idc = first.chroma_idc if first is not None else 0
         bps = 1 if first is None or (first.bit_depth_y <= 8 and first.bit_depth_c <= 8) else 2
@@ -196,6 +204,9 @@ def yuv_canvas_planes(pics, out: abi.Output, raw: np.ndarray):
             off += nb
         res.append(tuple(planes))
     return res
+
+
+yuv_canvas_planes = canvas_views
 
 
 def split_planes(pics, raw: np.ndarray):

@@ -285,9 +285,17 @@ typedef struct hpvcd_tile_place {
  * of its tiles, lib.rs:1801-1815). */
 typedef struct hpvcd_canvas {
     uint32_t width, height;
-    uint32_t matrix;         /* HPVCD_MATRIX_*                                 */
+    uint32_t matrix;         /* HPVCD_MATRIX_*, or HPVCD_CANVAS_NATIVE         */
     uint32_t full_range;
 } hpvcd_canvas;
+
+/* hpvcd_canvas.matrix of an RGB8 output: this canvas receives its pictures'
+ * native YCbCr planes, laid out as an HPVCD_OUT_YUV_CANVAS canvas, instead
+ * of RGB8.  One submit then returns an image in RGB8 together with its
+ * auxiliary images at native depth: the alpha plane (a 4:0:0 picture, Y
+ * only; lib.rs:470-527 decode_alpha_plane_native) and the gain map
+ * (lib.rs:555 DecodedGainMapImage planes). */
+#define HPVCD_CANVAS_NATIVE 0x100u
 
 typedef struct hpvcd_output {
     uint32_t kind;           /* HPVCD_OUT_*                                    */

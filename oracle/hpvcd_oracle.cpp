@@ -1495,21 +1495,33 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
             if (g.idc && planes_out[i].cr) std::memcpy(planes_out[i].cr, pl[i].cr, (size_t)g.cw * g.ch * 2);
         }
     }
-    if (out && out->kind == HPVCD_OUT_YUV_CANVAS && rgb && out->place) {
-        // lib.rs:993-1091 fill_native_grid_yuv and :871-991
-        // stitch_native_yuv_band: each tile's visible part copied onto the
-        // image planes at its grid position (chroma at position / subsampling),
-        // rows past the tile repeating its last row, columns its last sample.
+    if (out && (out->kind == HPVCD_OUT_RGB8 || out->kind == HPVCD_OUT_YUV_CANVAS) && rgb && out->place) {
+        // Canvases: one (canvas_w x canvas_h) or out->canvases[] (lib.rs:1724
+        // decode_grid per output image).  An RGB8 canvas holds packed RGB8; a
+        // native one (every canvas of a YUV canvas output, HPVCD_CANVAS_NATIVE
+        // ones of an RGB8 output) Y then Cb then Cr in the format of its
+        // pictures (8-bit 4:0:0 without pictures).
         const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
         for (uint32_t i = 0; i < n; ++i)
             if (out->place[i].canvas >= nc) return HPVCD_ERR_INVALID_ARG;
-        struct Cv { int w, h, idc, bps, sw, sh, cw, ch; size_t off; };
+        struct Cv {
+            bool native;
+            int w, h, idc, bps, sw, sh, cw, ch;
+            uint32_t matrix, full_range;
+            size_t off;
+        };
         std::vector<Cv> cvs;
         size_t acc = 0;
         for (uint32_t k = 0; k < nc; ++k) {
+            const hpvcd_canvas cv = out->n_canvases ? out->canvases[k]
+                                                    : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix,
+                                                                   out->full_range};
             Cv c{};
-            c.w = (int)(out->n_canvases ? out->canvases[k].width : out->canvas_w);
-            c.h = (int)(out->n_canvases ? out->canvases[k].height : out->canvas_h);
+            c.native = out->kind == HPVCD_OUT_YUV_CANVAS || cv.matrix == HPVCD_CANVAS_NATIVE;
+            c.w = (int)cv.width;
+            c.h = (int)cv.height;
+            c.matrix = cv.matrix;
+            c.full_range = cv.full_range;
             c.idc = 0;
             c.bps = 1;
             for (uint32_t i = 0; i < n; ++i)
@@ -1523,13 +1535,18 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
             c.cw = c.idc ? (c.w + c.sw - 1) / c.sw : 0;
             c.ch = c.idc ? (c.h + c.sh - 1) / c.sh : 0;
             c.off = acc;
-            acc += ((size_t)c.w * c.h + 2 * (size_t)c.cw * c.ch) * c.bps;
+            acc += c.native ? ((size_t)c.w * c.h + 2 * (size_t)c.cw * c.ch) * c.bps : (size_t)c.w * c.h * 3;
             cvs.push_back(c);
         }
+        // native canvases: lib.rs:993-1091 fill_native_grid_yuv and :871-991
+        // stitch_native_yuv_band: each tile's visible part copied onto the
+        // image planes at its grid position (chroma at position / subsampling),
+        // rows past the tile repeating its last row, columns its last sample.
         for (uint32_t i = 0; i < n; ++i) {
             const Geo g = geo_of(&pics[i]);
             const hpvcd_tile_place& tp = out->place[i];
             const Cv& c = cvs[tp.canvas];
+            if (!c.native) continue;
             if (c.idc != g.idc || c.bps != (g.bd > 8 || g.bd_c > 8 ? 2 : 1)) return HPVCD_ERR_INVALID_ARG;
             for (int comp = 0; comp < (g.idc ? 3 : 1); ++comp) {
                 const int sw = comp ? c.sw : 1, sh = comp ? c.sh : 1;
@@ -1554,44 +1571,27 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
                     }
             }
         }
-    }
-    if (out && out->kind == HPVCD_OUT_RGB8 && rgb && out->place) {
-        // lib.rs:1610-1660 per-tile RGB then row copy with cropping;
-        // lib.rs:1964-1978 rgb8 narrowing by >> (bit_depth - 8).
-        // canvases: one (canvas_w x canvas_h) or out->canvases[]; lib.rs:1724
-        // decode_grid per output image.
-        std::vector<uint32_t> cwid, chgt, cmat, cfr;
-        std::vector<size_t> coff;
-        size_t acc = 0;
-        const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
-        for (uint32_t k = 0; k < nc; ++k) {
-            const hpvcd_canvas c = out->n_canvases ? out->canvases[k]
-                                                   : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix,
-                                                                  out->full_range};
-            cwid.push_back(c.width); chgt.push_back(c.height); cmat.push_back(c.matrix); cfr.push_back(c.full_range);
-            coff.push_back(acc);
-            acc += (size_t)c.width * c.height * 3;
-        }
-        for (uint32_t i = 0; i < n; ++i)
-            if (out->place[i].canvas >= nc) return HPVCD_ERR_INVALID_ARG;
+        // RGB8 canvases: lib.rs:1610-1660 per-tile RGB then row copy with
+        // cropping; lib.rs:1964-1978 rgb8 narrowing by >> (bit_depth - 8).
         std::atomic<uint32_t> next{0};
         auto convert = [&](uint32_t i) {
             const hpvcd_picture* p = &pics[i];
             const Geo g = geo_of(p);
             const hpvcd_tile_place& tp = out->place[i];
+            const Cv& c = cvs[tp.canvas];
+            if (c.native) return;
             const int tw = (int)tp.crop_w, th = (int)tp.crop_h;
             if (tw <= 0 || th <= 0) return;
             std::vector<uint16_t> buf((size_t)tw * th * 3);
-            yuv_to_rgb16(pl[i].y, pl[i].cb, pl[i].cr, g.w, g.h, g.idc, g.bd, tw, th, 0, 0,
-                         (int)cmat[tp.canvas], cfr[tp.canvas] != 0, buf.data());
+            yuv_to_rgb16(pl[i].y, pl[i].cb, pl[i].cr, g.w, g.h, g.idc, g.bd, tw, th, 0, 0, (int)c.matrix,
+                         c.full_range != 0, buf.data());
             const int shift = g.bd - 8;
-            const int cw = (int)cwid[tp.canvas], chh = (int)chgt[tp.canvas];
-            uint8_t* base = rgb + coff[tp.canvas];
-            const int copy_w = std::min(tw, std::max(cw - (int)tp.dst_x, 0));
-            const int copy_h = std::min(th, std::max(chh - (int)tp.dst_y, 0));
+            uint8_t* base = rgb + c.off;
+            const int copy_w = std::min(tw, std::max(c.w - (int)tp.dst_x, 0));
+            const int copy_h = std::min(th, std::max(c.h - (int)tp.dst_y, 0));
             for (int y = 0; y < copy_h; ++y)
                 for (int x = 0; x < copy_w * 3; ++x)
-                    base[((size_t)(tp.dst_y + y) * cw + tp.dst_x) * 3 + x] =
+                    base[((size_t)(tp.dst_y + y) * c.w + tp.dst_x) * 3 + x] =
                         (uint8_t)(buf[(size_t)y * tw * 3 + x] >> shift);
         };
         if (threads > 1 && n > 1) {

@@ -217,14 +217,20 @@ def yuv_to_rgb16(y, cb, cr, width, height, chroma_idc, bd, dw, dh, matrix, full_
 
 
 def yuv_canvas_layout(pics, out):
-    """Per canvas of an OUT_YUV_CANVAS output: (offset, width, height,
-    chroma_idc, bytes per sample); a canvas takes its first picture's format."""
+    """Per canvas of a canvas output: (offset, width, height, chroma_idc,
+    bytes per sample); RGB8 canvases have chroma_idc None and 3 bytes per
+    pixel, native ones the format of their first picture."""
     n_c = out.n_canvases or 1
     cv = (abi.Canvas * out.n_canvases).from_address(out.canvases) if out.n_canvases else None
     place = (abi.TilePlace * len(pics)).from_address(out.place)
     res, off = [], 0
     for k in range(n_c):
         w, h = (cv[k].width, cv[k].height) if cv is not None else (out.canvas_w, out.canvas_h)
+        matrix = cv[k].matrix if cv is not None else out.matrix
+        if out.kind == abi.OUT_RGB8 and matrix != abi.CANVAS_NATIVE:
+            res.append((off, w, h, None, 3))
+            off += w * h * 3
+            continue
         idc, bps = 0, 1
         for i, p in enumerate(pics):
             if place[i].canvas == k:
@@ -260,13 +266,9 @@ def decode_batch(pics, out=None, want_planes=True, threads=1):
         if want_planes:
             pl_arr[i] = Planes(_p(y), _p(cb) if cb.size else None, _p(cr) if cr.size else None)
     rgb = None
-    if out is not None and out.kind == abi.OUT_RGB8:
-        if out.n_canvases:
-            cv = (abi.Canvas * out.n_canvases).from_address(out.canvases)
-            rgb = np.zeros(sum(c.width * c.height * 3 for c in cv), np.uint8)
-        else:
-            rgb = np.zeros((out.canvas_h, out.canvas_w, 3), np.uint8)
-    elif out is not None and out.kind == abi.OUT_YUV_CANVAS:
+    if out is not None and out.kind == abi.OUT_RGB8 and not out.n_canvases and out.matrix != abi.CANVAS_NATIVE:
+        rgb = np.zeros((out.canvas_h, out.canvas_w, 3), np.uint8)
+    elif out is not None and out.kind in (abi.OUT_RGB8, abi.OUT_YUV_CANVAS):
         rgb = np.zeros(yuv_canvas_bytes(pics, out), np.uint8)
     rc = lib().orc_decode_batch(arr, u32(n), C.byref(out) if out is not None else None,
                                 pl_arr if want_planes else None,

@@ -878,3 +878,42 @@ def test_yuv_canvas_rejects_mixed_formats(dec):
     with pytest.raises(abi.HpvcdError) as e:
         dec.submit(pics, out)
     assert e.value.status == abi.ERR_INVALID_ARG
+
+
+def test_rgb_with_alpha_and_gain_map_canvases(dec):
+    """One submit: a 10-bit grid image to RGB8, its 8-bit 4:0:0 alpha plane
+    and a half-size 4:2:0 gain map at native depth (CANVAS_NATIVE canvases),
+    also DMA'd straight into per-canvas page-locked buffers."""
+    import ctypes as C
+    from hpvcd_b200.gpu import canvas_views, pinned_empty
+    s = synth.SynthSet()
+    W, H = 1100, 700
+    img, img_pl = _image(640, W, H, 10, 1, s)
+    alpha, alpha_pl = _image(641, W, H, 8, 0, s)
+    gm, gm_pl = _image(642, W // 2, H // 2, 10, 1, s)
+    pics = img + alpha + gm
+    places = ([(x, y, cw, ch, 0) for (x, y, cw, ch) in img_pl] + [(x, y, cw, ch, 1) for (x, y, cw, ch) in alpha_pl]
+              + [(x, y, cw, ch, 2) for (x, y, cw, ch) in gm_pl])
+    canv = [abi.Canvas(W, H, abi.MATRIX_SMPTE170M, 1), abi.Canvas(W, H, abi.CANVAS_NATIVE, 0),
+            abi.Canvas(W // 2, H // 2, abi.CANVAS_NATIVE, 0)]
+    pl_arr = (abi.TilePlace * len(places))(*[abi.TilePlace(*t) for t in places])
+    cv_arr = (abi.Canvas * 3)(*canv)
+    out = abi.Output(abi.OUT_RGB8, 0, 0, 0, 0, C.cast(pl_arr, C.c_void_p), None, 0, 3, C.cast(cv_arr, C.c_void_p))
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    t = dec.submit(pics, out)
+    dec.wait(t)
+    got = dec.read(t)
+    assert got.size == ref.size and np.array_equal(got, ref)
+    rgb, (a, acb, acr), (gy, gcb, gcr) = canvas_views(pics, out, got)
+    assert rgb.shape == (H, W, 3) and a.shape == (H, W) and a.dtype == np.uint8 and acb.size == 0
+    assert gy.shape == (H // 2, W // 2) and gy.dtype == np.uint16 and gcb.shape == (H // 4, W // 4)
+    # the same into one page-locked buffer per canvas
+    sizes = [v.nbytes if isinstance(v, np.ndarray) else sum(x.nbytes for x in v) for v in (rgb, (a, acb, acr),
+                                                                                           (gy, gcb, gcr))]
+    bufs = [pinned_empty(nb) for nb in sizes]
+    dsts = (C.c_void_p * 3)(*[b.ctypes.data for b, _ in bufs])
+    out.canvas_dst = C.cast(dsts, C.c_void_p)
+    t = dec.submit(pics, out)
+    dec.wait(t)
+    assert abi.lib().hpvcd_gpu_read(dec._h, t, None, 0) == abi.OK  # nothing to copy: already in place
+    assert np.array_equal(np.concatenate([b for b, _ in bufs]), ref)
