@@ -188,16 +188,21 @@ class TilePlace(C.Structure):
                 ("crop_h", C.c_uint32), ("canvas", C.c_uint32)]
 
 
+ORIENT_NORMAL, ORIENT_FLIP_H, ORIENT_ROTATE180, ORIENT_FLIP_V = 1, 2, 3, 4
+ORIENT_TRANSPOSE, ORIENT_ROTATE90, ORIENT_TRANSVERSE, ORIENT_ROTATE270 = 5, 6, 7, 8
+
+
 class Canvas(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("matrix", C.c_uint32),
-                ("full_range", C.c_uint32)]
+                ("full_range", C.c_uint32), ("orientation", C.c_uint32)]
 
 
 class Output(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("matrix", C.c_uint32), ("full_range", C.c_uint32),
                 ("canvas_w", C.c_uint32), ("canvas_h", C.c_uint32), ("place", C.c_void_p),
                 ("host_dst", C.c_void_p), ("host_dst_bytes", C.c_uint64),
-                ("n_canvases", C.c_uint32), ("canvases", C.c_void_p), ("canvas_dst", C.c_void_p)]
+                ("n_canvases", C.c_uint32), ("canvases", C.c_void_p), ("canvas_dst", C.c_void_p),
+                ("orientation", C.c_uint32)]
 
 
 class ServerCfg(C.Structure):

@@ -43,6 +43,7 @@ struct DevPic {
     int32_t dst_x, dst_y, crop_w, crop_h;
     uint64_t canvas_off;  // byte offset of the picture's canvas in the output
     int32_t canvas_w, canvas_h, matrix, full_range;
+    int32_t orientation;  // HPVCD_ORIENT_* of the canvas (0 normal)
     int32_t needs_wavefront;
 };
 

@@ -416,6 +416,25 @@ __device__ __forceinline__ uint32_t rgb_px(const RgbCoef& k, int idc, int luma, 
     return (uint32_t)r | ((uint32_t)g << 8) | ((uint32_t)b << 16);
 }
 
+// Index in the oriented W x H image (stored layout) of stored sample (x, y)
+// (lib.rs:2065-2110 rotate_luma, :2112-2200 rotate_buf; TRANSPOSE /
+// TRANSVERSE keep their place there).
+__device__ __forceinline__ size_t oriented_index(int x, int y, int W, int H, int o) {
+    switch (o) {
+        case HPVCD_ORIENT_FLIP_H: return (size_t)y * W + (W - 1 - x);
+        case HPVCD_ORIENT_ROTATE180: return (size_t)(H - 1 - y) * W + (W - 1 - x);
+        case HPVCD_ORIENT_FLIP_V: return (size_t)(H - 1 - y) * W + x;
+        case HPVCD_ORIENT_ROTATE90: return (size_t)x * H + (H - 1 - y);
+        case HPVCD_ORIENT_ROTATE270: return (size_t)(W - 1 - x) * H + y;
+        default: return (size_t)y * W + x;
+    }
+}
+
+__device__ __forceinline__ bool moves_samples(int o) {
+    return o == HPVCD_ORIENT_FLIP_H || o == HPVCD_ORIENT_ROTATE180 || o == HPVCD_ORIENT_FLIP_V ||
+           o == HPVCD_ORIENT_ROTATE90 || o == HPVCD_ORIENT_ROTATE270;
+}
+
 __global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out) {
     const DevPic& P = pics[blockIdx.y];
     if (P.matrix == (int)HPVCD_CANVAS_NATIVE) return;  // k_yuv_canvas's picture
@@ -449,6 +468,16 @@ __global__ void k_rgb(const DevPic* __restrict__ pics, uint8_t* __restrict__ out
         uint32_t px[4];
     #pragma unroll
         for (int i = 0; i < 4; ++i) px[i] = rgb_px(k, P.idc, luma[i], cb[i], cr[i]);
+        if (moves_samples(P.orientation)) {  // each pixel to its oriented place
+            for (int i = 0; i < cnt; ++i) {
+                uint8_t* q = canvas + oriented_index(P.dst_x + x0 + i, P.dst_y + yy, P.canvas_w, P.canvas_h,
+                                                     P.orientation) * 3;
+                q[0] = (uint8_t)px[i];
+                q[1] = (uint8_t)(px[i] >> 8);
+                q[2] = (uint8_t)(px[i] >> 16);
+            }
+            continue;
+        }
         uint8_t* o = canvas + ((size_t)(P.dst_y + yy) * P.canvas_w + P.dst_x + x0) * 3;
         if (cnt == 4 && ((uintptr_t)o & 3) == 0) {
             uint32_t* o32 = (uint32_t*)o;
@@ -485,14 +514,16 @@ __global__ void k_yuv_canvas(const DevPic* __restrict__ pics, uint8_t* __restric
     const size_t chroma_bytes = (size_t)CW * CH * P.bps;
     uint8_t* plane = out + P.canvas_off + (c == 0 ? 0 : luma_bytes + (c - 1) * chroma_bytes);
     const int qw = (copy_w + 3) >> 2;
+    const int o = P.orientation;
     for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < qw * copy_h; id += gridDim.x * blockDim.x) {
         const int x0 = (id % qw) * 4, y = id / qw;
         const size_t srow = (size_t)min(y, ph - 1) * pw;
-        const size_t drow = (size_t)(dy + y) * CW + dx;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const int x = x0 + i;
-            if (x < copy_w) store_sample(plane, P.bps, drow + x, load_sample(P.fin[c], P.bps, srow + min(x, pw - 1)));
+            if (x < copy_w)
+                store_sample(plane, P.bps, oriented_index(dx + x, dy + y, CW, CH, o),
+                             load_sample(P.fin[c], P.bps, srow + min(x, pw - 1)));
         }
     }
 }

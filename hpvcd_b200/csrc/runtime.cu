@@ -299,7 +299,7 @@ uint32_t n_canvases_of(const hpvcd_output* out) { return out->n_canvases ? out->
 
 hpvcd_canvas canvas_of(const hpvcd_output* out, uint32_t k) {
     return out->n_canvases ? out->canvases[k]
-                           : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix, out->full_range};
+                           : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix, out->full_range, out->orientation};
 }
 
 // Sample format of a YUV canvas: that of the first picture placed on it
@@ -591,6 +591,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             const bool rgb = !native_canvas(P->out.kind, cv);
             d.matrix = rgb ? (int)cv.matrix : (int)HPVCD_CANVAS_NATIVE;  // selects k_rgb or k_yuv_canvas
             d.full_range = (int)cv.full_range;
+            d.orientation = (int)cv.orientation;
             (rgb ? P->any_rgb_canvas : P->any_native_canvas) = true;
             d.dst_x = (int)tp.dst_x; d.dst_y = (int)tp.dst_y;
             // RGB8 crops at the picture; a native canvas repeats its last row / column
@@ -843,9 +844,7 @@ bool same_layout(const hpvcd_plan* P, const hpvcd_picture* pics, uint32_t n, con
         const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
         if (nc != P->canvases.size()) return false;
         for (uint32_t k = 0; k < nc; ++k) {
-            const hpvcd_canvas c = out->n_canvases ? out->canvases[k]
-                                                   : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix,
-                                                                  out->full_range};
+            const hpvcd_canvas c = canvas_of(out, k);
             if (std::memcmp(&c, &P->canvases[k], sizeof(c)) != 0) return false;
         }
         for (uint32_t i = 0; i < n; ++i)

@@ -184,11 +184,15 @@ def canvas_views(pics, out: abi.Output, raw: np.ndarray):
     cv = (abi.Canvas * out.n_canvases).from_address(out.canvases) if out.n_canvases else None
     place = (abi.TilePlace * len(pics)).from_address(out.place)
     res, off = [], 0
+    def shape(w, h):  # rows, columns of the oriented image
+        return (w, h) if orient in (abi.ORIENT_ROTATE90, abi.ORIENT_ROTATE270) else (h, w)
+
     for k in range(n_c):
         w, h = (cv[k].width, cv[k].height) if cv is not None else (out.canvas_w, out.canvas_h)
         matrix = cv[k].matrix if cv is not None else out.matrix
+        orient = cv[k].orientation if cv is not None else out.orientation
         if out.kind == abi.OUT_RGB8 and matrix != abi.CANVAS_NATIVE:
-            res.append(raw[off:off + w * h * 3].reshape(h, w, 3))
+            res.append(raw[off:off + w * h * 3].reshape(*shape(w, h), 3))
             off += w * h * 3
             continue
         first = next((p for i, p in enumerate(pics) if place[i].canvas == k), None)
@@ -200,7 +204,7 @@ def canvas_views(pics, out: abi.Output, raw: np.ndarray):
         planes = []
         for (pw, ph) in [(w, h), (cw, ch), (cw, ch)]:
             nb = pw * ph * bps
-            planes.append(raw[off:off + nb].view(dt).reshape(ph, pw))
+            planes.append(raw[off:off + nb].view(dt).reshape(*shape(pw, ph)))
             off += nb
         res.append(tuple(planes))
     return res

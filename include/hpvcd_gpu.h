@@ -284,10 +284,26 @@ typedef struct hpvcd_tile_place {
 /* One output image of a batch: its size and colour description (the SPS VUI
  * of its tiles, lib.rs:1801-1815). */
 typedef struct hpvcd_canvas {
-    uint32_t width, height;
+    uint32_t width, height;  /* the image as stored (before orientation)      */
     uint32_t matrix;         /* HPVCD_MATRIX_*, or HPVCD_CANVAS_NATIVE         */
     uint32_t full_range;
+    uint32_t orientation;    /* HPVCD_ORIENT_* (0 = normal)                    */
 } hpvcd_canvas;
+
+/* Orientation of a canvas (metadata.rs:31 `Orientation`, EXIF numbering,
+ * from the HEIF irot / imir boxes), applied to the finished canvas as
+ * lib.rs:2017-2110 apply_orientation does: the output holds the oriented
+ * image, height x width for ROTATE90 / ROTATE270.  TRANSPOSE and TRANSVERSE
+ * leave the samples in their stored places (the reference's rotate_luma /
+ * rotate_buf treat them so); a native canvas rotates each plane. */
+#define HPVCD_ORIENT_NORMAL 1u
+#define HPVCD_ORIENT_FLIP_H 2u
+#define HPVCD_ORIENT_ROTATE180 3u
+#define HPVCD_ORIENT_FLIP_V 4u
+#define HPVCD_ORIENT_TRANSPOSE 5u
+#define HPVCD_ORIENT_ROTATE90 6u
+#define HPVCD_ORIENT_TRANSVERSE 7u
+#define HPVCD_ORIENT_ROTATE270 8u
 
 /* hpvcd_canvas.matrix of an RGB8 output: this canvas receives its pictures'
  * native YCbCr planes, laid out as an HPVCD_OUT_YUV_CANVAS canvas, instead
@@ -317,6 +333,7 @@ typedef struct hpvcd_output {
      * each canvas is DMA'd straight into its own buffer; host_dst is then
      * unused and hpvcd_gpu_read copies nothing. */
     void* const* canvas_dst;
+    uint32_t orientation;     /* single canvas: HPVCD_ORIENT_* (0 = normal)    */
 } hpvcd_output;
 
 /* ------------------------------------------------------------------------ */

@@ -1431,6 +1431,30 @@ int32_t orc_sao_picture(const hpvcd_picture* pic, orc_planes* planes) {
     return sao_picture(pic, planes);
 }
 
+// lib.rs:2065-2110 rotate_luma and :2112-2200 rotate_buf on a w x h image of
+// `esz`-byte elements: FlipH / Rotate180 / FlipV / Rotate90 / Rotate270 move
+// the elements (Rotate90: row r, column c -> row c, column h - 1 - r of the
+// h-wide result; Rotate270: -> row w - 1 - c, column r); Normal, Transpose
+// and Transverse leave them in place.
+static void orient_samples(uint8_t* img, int w, int h, int esz, uint32_t o) {
+    if (o != HPVCD_ORIENT_FLIP_H && o != HPVCD_ORIENT_ROTATE180 && o != HPVCD_ORIENT_FLIP_V &&
+        o != HPVCD_ORIENT_ROTATE90 && o != HPVCD_ORIENT_ROTATE270)
+        return;
+    const std::vector<uint8_t> src(img, img + (size_t)w * h * esz);
+    for (int r = 0; r < h; ++r)
+        for (int c = 0; c < w; ++c) {
+            size_t d;
+            switch (o) {
+                case HPVCD_ORIENT_FLIP_H: d = (size_t)r * w + (w - 1 - c); break;
+                case HPVCD_ORIENT_ROTATE180: d = (size_t)(h - 1 - r) * w + (w - 1 - c); break;
+                case HPVCD_ORIENT_FLIP_V: d = (size_t)(h - 1 - r) * w + c; break;
+                case HPVCD_ORIENT_ROTATE90: d = (size_t)c * h + (h - 1 - r); break;
+                default: d = (size_t)(w - 1 - c) * h + r; break;  // Rotate270
+            }
+            std::memcpy(img + d * esz, &src[((size_t)r * w + c) * esz], (size_t)esz);
+        }
+}
+
 int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out,
                          orc_planes* planes_out, uint8_t* rgb, int32_t threads) {
     if (!pics && n) return HPVCD_ERR_INVALID_ARG;
@@ -1507,7 +1531,7 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
         struct Cv {
             bool native;
             int w, h, idc, bps, sw, sh, cw, ch;
-            uint32_t matrix, full_range;
+            uint32_t matrix, full_range, orientation;
             size_t off;
         };
         std::vector<Cv> cvs;
@@ -1515,8 +1539,9 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
         for (uint32_t k = 0; k < nc; ++k) {
             const hpvcd_canvas cv = out->n_canvases ? out->canvases[k]
                                                     : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix,
-                                                                   out->full_range};
+                                                                   out->full_range, out->orientation};
             Cv c{};
+            c.orientation = cv.orientation;
             c.native = out->kind == HPVCD_OUT_YUV_CANVAS || cv.matrix == HPVCD_CANVAS_NATIVE;
             c.w = (int)cv.width;
             c.h = (int)cv.height;
@@ -1603,6 +1628,20 @@ int32_t orc_decode_batch(const hpvcd_picture* pics, uint32_t n, const hpvcd_outp
             for (auto& th : pool) th.join();
         } else {
             for (uint32_t i = 0; i < n; ++i) convert(i);
+        }
+        // lib.rs:2017-2110 apply_orientation on each finished canvas
+        for (const Cv& c : cvs) {
+            if (c.native) {
+                uint8_t* p0 = rgb + c.off;
+                orient_samples(p0, c.w, c.h, c.bps, c.orientation);
+                if (c.idc) {
+                    uint8_t* p1 = p0 + (size_t)c.w * c.h * c.bps;
+                    orient_samples(p1, c.cw, c.ch, c.bps, c.orientation);
+                    orient_samples(p1 + (size_t)c.cw * c.ch * c.bps, c.cw, c.ch, c.bps, c.orientation);
+                }
+            } else {
+                orient_samples(rgb + c.off, c.w, c.h, 3, c.orientation);
+            }
         }
     }
     return HPVCD_OK;

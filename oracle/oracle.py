@@ -267,7 +267,8 @@ def decode_batch(pics, out=None, want_planes=True, threads=1):
             pl_arr[i] = Planes(_p(y), _p(cb) if cb.size else None, _p(cr) if cr.size else None)
     rgb = None
     if out is not None and out.kind == abi.OUT_RGB8 and not out.n_canvases and out.matrix != abi.CANVAS_NATIVE:
-        rgb = np.zeros((out.canvas_h, out.canvas_w, 3), np.uint8)
+        rot = out.orientation in (abi.ORIENT_ROTATE90, abi.ORIENT_ROTATE270)
+        rgb = np.zeros((out.canvas_w, out.canvas_h, 3) if rot else (out.canvas_h, out.canvas_w, 3), np.uint8)
     elif out is not None and out.kind in (abi.OUT_RGB8, abi.OUT_YUV_CANVAS):
         rgb = np.zeros(yuv_canvas_bytes(pics, out), np.uint8)
     rc = lib().orc_decode_batch(arr, u32(n), C.byref(out) if out is not None else None,

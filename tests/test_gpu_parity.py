@@ -917,3 +917,33 @@ def test_rgb_with_alpha_and_gain_map_canvases(dec):
     dec.wait(t)
     assert abi.lib().hpvcd_gpu_read(dec._h, t, None, 0) == abi.OK  # nothing to copy: already in place
     assert np.array_equal(np.concatenate([b for b, _ in bufs]), ref)
+
+
+# --- orientation (irot / imir) of the output canvases ------------------------
+@pytest.mark.parametrize("orient", [2, 3, 4, 5, 6, 8])
+def test_oriented_canvases(dec, orient):
+    import ctypes as C
+    s = synth.SynthSet()
+    W, H = 1100, 700
+    img, img_pl = _image(650 + orient, W, H, 10, 1, s)
+    alpha, alpha_pl = _image(660 + orient, W, H, 8, 0, s)
+    pics = img + alpha
+    places = [(x, y, cw, ch, 0) for (x, y, cw, ch) in img_pl] + [(x, y, cw, ch, 1) for (x, y, cw, ch) in alpha_pl]
+    canv = [abi.Canvas(W, H, abi.MATRIX_BT709, 0, orient), abi.Canvas(W, H, abi.CANVAS_NATIVE, 0, orient)]
+    pl_arr = (abi.TilePlace * len(places))(*[abi.TilePlace(*t) for t in places])
+    cv_arr = (abi.Canvas * 2)(*canv)
+    out = abi.Output(abi.OUT_RGB8, 0, 0, 0, 0, C.cast(pl_arr, C.c_void_p), None, 0, 2, C.cast(cv_arr, C.c_void_p))
+    _, ref = O.decode_batch(pics, out, want_planes=False)
+    t = dec.submit(pics, out)
+    dec.wait(t)
+    got = dec.read(t)
+    assert got.size == ref.size and np.array_equal(got, ref)
+    g = synth.make_grid(1100, 700, seed=670 + orient, bit_depth=8, chroma_idc=2)
+    out2, keep = synth.grid_output(g)
+    out2.kind = abi.OUT_YUV_CANVAS
+    out2.orientation = orient
+    p2 = g.synth.pictures()
+    _, ref2 = O.decode_batch(p2, out2, want_planes=False)
+    t = dec.submit(p2, out2)
+    dec.wait(t)
+    assert np.array_equal(dec.read(t), ref2)

@@ -407,3 +407,31 @@ def test_yuv_canvas_stitch_matches_planes(bd, idc):
             W[dy:dy + th, dx:dx + tw] = pl[c][:th, :tw]
     for c, got in enumerate((Y, Cb, Cr)):
         assert np.array_equal(got.astype(np.uint16), want[c]), c
+
+
+@pytest.mark.parametrize("orient", range(0, 9))
+def test_orientation_of_the_oracle_canvas(orient):
+    """lib.rs:2065-2200: FlipH / Rotate180 / FlipV / Rotate90 (clockwise) /
+    Rotate270 move the pixels; Normal, Transpose and Transverse leave them
+    (the reference's rotate_luma / rotate_buf).  Checked on RGB8 and on a
+    native 4:2:0 canvas against numpy flips and rotations of the normal one."""
+    from hpvcd_b200 import synth
+    from hpvcd_b200.gpu import canvas_views
+    g = synth.make_grid(136, 72, seed=31, bit_depth=8, chroma_idc=1, tile=64, sao=False)
+    pics = g.synth.pictures()
+    turn = {2: np.fliplr, 3: lambda a: np.rot90(a, 2), 4: np.flipud, 6: lambda a: np.rot90(a, -1),
+            8: lambda a: np.rot90(a, 1)}.get(orient, lambda a: a)
+
+    def planes(out, raw):
+        views = canvas_views(pics, out, raw.reshape(-1))
+        return [p.copy() for v in views for p in (v if isinstance(v, tuple) else (v,))]
+
+    for kind in (O.abi.OUT_RGB8, O.abi.OUT_YUV_CANVAS):
+        out, keep = synth.grid_output(g)
+        out.kind = kind
+        _, base = O.decode_batch(pics, out, want_planes=False)
+        normal = planes(out, base)
+        out.orientation = orient
+        _, got = O.decode_batch(pics, out, want_planes=False)
+        for p0, p1 in zip(normal, planes(out, got)):
+            assert np.array_equal(turn(p0), p1)
