@@ -47,6 +47,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--e2e-inflight", type=int, default=3, help="steps in flight in the end-to-end measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["grid", "serving", "selector", "inter"], default="grid",
                     help="grid: the 4032x3024 still (default); serving: mixed-size batched serving; "
@@ -182,12 +183,12 @@ def run_reference(args):
     return 0
 
 
-def run_e2e(pics, g, K2, warmup, local, world, dev):
+def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2):
     """Same decode through hpvcd_gpu_submit / wait / read: inputs packed in
     page-locked host memory (one H2D DMA per step), the RGB8 canvas DMA'd
-    back to a page-locked caller buffer every step.  Two steps are in flight
-    (each with its own output buffer), so one step's copies overlap the
-    other's decoding; throughput = steps / wall time from the first submit
+    back to a page-locked caller buffer every step.  `in_flight` steps are
+    queued (each with its own output buffer), so one step's copies overlap
+    another's decoding; throughput = steps / wall time from the first submit
     to the last read, latency = submit -> read per step."""
     import torch
 
@@ -198,19 +199,19 @@ def run_e2e(pics, g, K2, warmup, local, world, dev):
     h2d = pkeep[2]
     canvas_bytes = OUT_W * OUT_H * 3
     outs = []
-    for _ in range(2):
+    for _ in range(in_flight):
         dst, dkeep = pinned_empty(canvas_bytes)
         o, okeep = synth.grid_output(g)
         o.host_dst = dst.ctypes.data
         o.host_dst_bytes = canvas_bytes
         outs.append((o, dst, dkeep, okeep))
     mlp = _selector_network()
-    with GpuDecoder(local, max_inflight=2) as decd:
+    with GpuDecoder(local, max_inflight=in_flight) as decd:
         if mlp is not None:  # every submit picks its schedule from the batch's features
             from hpvcd_b200 import selector
             decd.set_selector(mlp, selector.SCHEDULES)
         for k in range(max(3, warmup // 2)):
-            o, dst = outs[k % 2][:2]
+            o, dst = outs[k % in_flight][:2]
             t = decd.submit(packed, o)
             decd.wait(t)
             decd.read(t, dst)
@@ -220,8 +221,8 @@ def run_e2e(pics, g, K2, warmup, local, world, dev):
         pending = []  # (ticket, dst, submit time)
         t_start = time.perf_counter()
         for k in range(K2):
-            o, dst = outs[k % 2][:2]
-            if len(pending) == 2:  # the buffer of step k - 2 is read before it is reused
+            o, dst = outs[k % in_flight][:2]
+            if len(pending) == in_flight:  # the buffer of step k - in_flight is read before it is reused
                 t, d, ts = pending.pop(0)
                 decd.wait(t)
                 decd.read(t, d)
@@ -238,7 +239,7 @@ def run_e2e(pics, g, K2, warmup, local, world, dev):
             "steps": K2, "ms_per_step": round(e2e_total / K2 * 1e3, 3),
             "p50_ms": round(lat[len(lat) // 2], 3),
             "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3),
-            "in_flight": 2,
+            "in_flight": in_flight,
             "api": "hpvcd_gpu_submit/wait/read, pinned packed inputs, pinned RGB8 output",
             "schedule": "network pick per submit" if mlp is not None else "default"}
 
@@ -376,7 +377,7 @@ def run_ours(args):
     e2e = None
     K2 = args.e2e_steps if args.e2e_steps is not None else max(5, min(K, 50))
     if K2 > 0:
-        e2e = run_e2e(pics, g, K2, args.warmup, local, world, dev)
+        e2e = run_e2e(pics, g, K2, args.warmup, local, world, dev, max(1, args.e2e_inflight))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
