@@ -41,7 +41,7 @@ STATUS_NAMES = {
 }
 
 TU_CBF, TU_TSKIP, TU_INTRA, TU_TQB = 0x01, 0x02, 0x04, 0x08
-TU_ROTATE, TU_RDPCM_H, TU_RDPCM_V = 0x10, 0x20, 0x40
+TU_ROTATE, TU_RDPCM_H, TU_RDPCM_V, TU_PCM = 0x10, 0x20, 0x40, 0x80
 CELL_EXEMPT = 0x01
 CELL_INTER = 0x02
 PU_L0, PU_L1 = 0x01, 0x02
@@ -58,6 +58,7 @@ PIC_CROSS_COMPONENT = 0x0080
 PIC_SAO_NO_ACROSS_SLICES = 0x0100
 PIC_SAO_NO_ACROSS_TILES = 0x0200
 PIC_CONSTRAINED_INTRA = 0x0400
+PIC_PCM = 0x0800
 PIC_STORE_MASK = 0x00FF0000
 
 
@@ -249,7 +250,7 @@ class SynthCfg(C.Structure):
         ("mv_pad", C.c_float), ("weighted", C.c_uint32), ("n_refs", C.c_uint32),
         ("tu_mix", C.c_float * 4),
         ("scaling", C.c_uint32), ("rext", C.c_uint32), ("tskip_log2_max", C.c_uint32),
-        ("ccp_p", C.c_float), ("regions", C.c_uint32),
+        ("ccp_p", C.c_float), ("regions", C.c_uint32), ("pcm_p", C.c_float),
     ]
 
 

@@ -73,6 +73,9 @@ typedef struct hpvcd_synth_cfg {
      * random CTB addresses in raster order, 2 = a uniform 2x2 tile grid with
      * one slice per tile.  0 = one slice and tile. */
     uint32_t regions;
+    /* Probability that an 8x8..32x32 intra CU is I_PCM (random samples at a
+     * random PCM bit depth, pcm_loop_filter_disabled drawn per CU). */
+    float pcm_p;
 } hpvcd_synth_cfg;
 
 typedef struct hpvcd_synth hpvcd_synth;

@@ -150,7 +150,9 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
     const bool i16s = bd <= 8 && allow16;
     const int16_t* lv = P.coeffs + t.coeff_off;
     const uint32_t rext = t.flags & (HPVCD_TU_ROTATE | HPVCD_TU_RDPCM_H | HPVCD_TU_RDPCM_V);
-    if ((t.flags & HPVCD_TU_TQB) && !rext) {  // decode.rs:4754-4757 / :4830-4834: residual = levels
+    // decode.rs:4754-4757 / :4830-4834: residual = levels (transquant bypass);
+    // an I_PCM record's levels are its samples (decode.rs:2768-2839)
+    if ((t.flags & (HPVCD_TU_TQB | HPVCD_TU_PCM)) && !rext) {
         for (int i = lane; i < n * n; i += 32) emit(i / n, i % n, (int)lv[i]);
         return;
     }
@@ -390,11 +392,12 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
         if (in_plane) {  // prediction already in the plane: add + clip (reconstruct.rs:214-251)
             void* pl = P.rec[c];
             const int mx = (1 << (c ? P.bd_c : P.bd)) - 1;
+            const int keep = (t.flags & HPVCD_TU_PCM) ? 0 : 1;  // I_PCM samples replace the plane's
             tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
                 const int x = x0 + m, y = y0 + r;
                 if (x < pw && y < ph) {
                     const size_t idx = (size_t)y * pw + x;
-                    store_sample(pl, P.bps, idx, clamp3i(load_sample(pl, P.bps, idx) + v, 0, mx));
+                    store_sample(pl, P.bps, idx, clamp3i(keep * load_sample(pl, P.bps, idx) + v, 0, mx));
                 }
             });
         } else {
@@ -630,6 +633,17 @@ __device__ __forceinline__ int ref_pos(int k, bool vertical, int n2, int inv) {
 // 4x4 intra TB entirely in registers: the 17 reference samples live in
 // lanes 0..16 (intra.rs:84-148 substitution via shuffles; no filtering for
 // n = 4, intra.rs:174), prediction (intra.rs:257-372) by lanes 0..15.
+// I_PCM block (decode.rs:2768-2839): its samples, staged in the residual
+// canvas by k_residual, go to the canvas unchanged.
+__device__ __forceinline__ void pcm_tb(const Comp& k, int log2n, int x0, int y0, int lane) {
+    const int n = 1 << log2n;
+    for (int i = lane; i < n * n; i += 32) {
+        const int yy = i >> log2n, xx = i & (n - 1);
+        k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)clamp3i(k.res[(y0 + yy) * k.S + x0 + xx], 0, k.max_v);
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y0, bool coded,
                                           const uint32_t* stamp, uint32_t jrec, int lane) {
     constexpr int n = 4, n2 = 8, total = 17;
@@ -1014,8 +1028,8 @@ __device__ __forceinline__ void team_sync(int threads) {
 }
 
 // kFeat: some picture of the launch has slices / tiles, constrained intra
-// prediction or cross-component prediction; without them the availability
-// and coded tests compile to the plain single-region form.
+// prediction, cross-component prediction or I_PCM blocks; without them the
+// availability, coded and PCM tests compile to the plain form.
 template <int kTeam, bool kFeat>
 __global__ void __launch_bounds__(kReconThreads, 4)
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
@@ -1268,7 +1282,9 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 // a chroma TB with cross-component prediction has a residual
                 // (written by k_ccp) even without coded coefficients
                 const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
-                if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
+                if (kFeat && (t.flags & HPVCD_TU_PCM)) {  // leader alone, no team step
+                    if (!helper) pcm_tb(k, t.log2n, x, y, lane);
+                } else if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
                     if (!helper) intra_tb_prep(k, t.log2n, t.mode, x, y, stamp, j, team_ws, lane);
                     team_sync(32 * kTeam);
                     intra_tb_predict(k, t.log2n, t.mode, x, y, coded, team_ws, (helper ? 32 : 0) + lane, 32 * kTeam);

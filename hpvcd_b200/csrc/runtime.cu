@@ -454,7 +454,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     bool any_inter = false;
     for (uint32_t i = 0; i < n; ++i) {
         if (pics[i].ctb_region ||
-            (pics[i].flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT)))
+            (pics[i].flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT | HPVCD_PIC_PCM)))
             P->recon_feat = true;
         if (pics[i].chroma_idc == 3) P->cfmt = 1;
         if (pics[i].chroma_idc == 2 && P->cfmt == 0) P->cfmt = 2;
@@ -1845,7 +1845,8 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
         const int cfmt = p.chroma_idc == 3 ? 1 : (p.chroma_idc == 2 ? 2 : 0);
         const int grid = std::max(1, std::min<int>(nd->sms * nd->occ[cfmt], (int)n_ctu));
         e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, cfmt, grid, 1,
-                               (p.ctb_region || (p.flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT))) ? 1 : 0,
+                               (p.ctb_region || (p.flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT |
+                                                           HPVCD_PIC_PCM))) ? 1 : 0,
                                st);
         if (e != cudaSuccess) return cuda_status(e);
     }

@@ -342,8 +342,39 @@ struct Gen {
         const bool inter = c.kind == HPVCD_SYNTH_INTER && !rng.bern(c.intra_cu_p);
         if (inter)
             inter_cu(x0, y0, log2, qp, tqb);
+        else if (c.pcm_p > 0.f && log2 >= 3 && log2 <= 5 && rng.bern(c.pcm_p))
+            pcm_cu(x0, y0, log2, qp);
         else
             intra_cu(x0, y0, log2, qp, tqb);
+    }
+
+    // I_PCM CU (decode.rs:2768-2839): one record per component whose levels
+    // are the samples, pcm_sample << (BitDepth - PcmBitDepth).
+    void pcm_cu(int x0, int y0, int log2, int qp) {
+        const int size = 1 << log2;
+        fill_cells(x0, y0, size, qp, rng.bern(0.5), true);  // exempt: pcm_loop_filter_disabled
+        mark_tu_edges(x0, y0, size);
+        const int pbd = rng.range(std::max(1, bd - 4), bd);
+        auto push_pcm = [&](int comp, int x, int y, int lg) {
+            hpvcd_tu t{};
+            t.x = (uint16_t)x;
+            t.y = (uint16_t)y;
+            t.log2n = (uint8_t)lg;
+            t.comp = (uint8_t)comp;
+            t.flags = HPVCD_TU_CBF | HPVCD_TU_INTRA | HPVCD_TU_PCM;
+            t.mode = 1;
+            t.qp_y = (int8_t)qp;
+            const int n = 1 << lg;
+            t.nx = (uint8_t)n;
+            t.coeff_off = (uint32_t)P.coeffs.size();
+            for (int i = 0; i < n * n; ++i) P.coeffs.push_back((int16_t)(rng.range(0, (1 << pbd) - 1) << (bd - pbd)));
+            P.tus.push_back(t);
+        };
+        push_pcm(0, x0, y0, log2);
+        if (idc == 0) return;
+        const int clog2 = idc == 3 ? log2 : log2 - 1, n_tb = idc == 2 ? 2 : 1;
+        for (int comp = 1; comp <= 2; ++comp)
+            for (int t = 0; t < n_tb; ++t) push_pcm(comp, x0 / sub_w, y0 / sub_h + (t << clog2), clog2);
     }
 
     // Residual-only picture: quadtree of TBs from 32x32 down to 4x4, each
@@ -476,6 +507,7 @@ struct Gen {
         d.log2_ctb = (uint8_t)log2_ctb;
         d.flags = c.pic_flags;
         if (c.ccp_p > 0.f && idc == 3) d.flags |= HPVCD_PIC_CROSS_COMPONENT;
+        if (c.pcm_p > 0.f) d.flags |= HPVCD_PIC_PCM;
         d.beta_offset_div2 = (int8_t)c.beta_offset_div2;
         d.tc_offset_div2 = (int8_t)c.tc_offset_div2;
         d.pps_cb_qp_offset = (int8_t)c.cb_qp_offset;

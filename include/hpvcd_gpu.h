@@ -70,6 +70,12 @@ typedef enum hpvcd_status {
 #define HPVCD_TU_ROTATE 0x10u
 #define HPVCD_TU_RDPCM_H 0x20u
 #define HPVCD_TU_RDPCM_V 0x40u
+/* I_PCM coding unit (decode.rs:2768-2839 decode_pcm_cu): the record's n*n
+ * levels are the reconstructed samples (pcm_sample << (BitDepth -
+ * PcmBitDepth)); no prediction, no transform.  One record per component
+ * (4:2:2 chroma: two stacked), flagged CBF | INTRA | PCM, on pictures flagged
+ * HPVCD_PIC_PCM. */
+#define HPVCD_TU_PCM 0x80u
 
 /*
  * One transform block, or one "mark decoded" record.  Records of a picture are
@@ -202,6 +208,8 @@ typedef struct hpvcd_scaling {
  * flagged HPVCD_CELL_INTER as unavailable (decode.rs:4641-4649); needs
  * cells. */
 #define HPVCD_PIC_CONSTRAINED_INTRA 0x0400u
+/* pcm_enabled_flag: records may carry HPVCD_TU_PCM. */
+#define HPVCD_PIC_PCM 0x0800u
 /* Store the decoded picture into entry e of the context's DPB (hpvcd_dpb)
  * after it is reconstructed; bits 16..23 of flags, 0 = no store. */
 #define HPVCD_PIC_STORE_DPB(e) ((uint32_t)((e) + 1) << 16)

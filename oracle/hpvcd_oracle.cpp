@@ -892,7 +892,7 @@ void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_
     const bool i16s = bd <= 8 && allow16;
     int32_t lv[32 * 32];
     for (int i = 0; i < n * n; ++i) lv[i] = p->coeffs[(size_t)t.coeff_off + i];
-    if (t.flags & HPVCD_TU_TQB) {  // lossless: levels verbatim (saturated for i16 storage)
+    if (t.flags & (HPVCD_TU_TQB | HPVCD_TU_PCM)) {  // lossless / I_PCM: levels verbatim (saturated for i16 storage)
         for (int i = 0; i < n * n; ++i) res[i] = i16s ? clamp3(lv[i], -32768, 32767) : lv[i];
         rext_residual_ops(res, n, (t.flags & HPVCD_TU_ROTATE) != 0, rdpcm_dir(t), i16s);
         return;
@@ -961,7 +961,9 @@ int recon_picture(const hpvcd_picture* p, orc_planes* pl) {
             if (luma) st.mark_decoded(t.x, t.y, n);
             continue;
         }
-        if (intra && !pred_in_plane) {
+        if (t.flags & HPVCD_TU_PCM) {  // decode.rs:2768-2839: the samples replace the block
+            for (int k = 0; k < n * n; ++k) pred[k] = 0;
+        } else if (intra && !pred_in_plane) {
             st.cur_region = luma ? st.region_at(t.x, t.y) : st.region_at(t.x * g.sub_w, t.y * g.sub_h);
             predict_block(st, t.comp, t.x, t.y, n, t.mode, pred);
         }

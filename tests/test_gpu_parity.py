@@ -947,3 +947,28 @@ def test_oriented_canvases(dec, orient):
     t = dec.submit(p2, out2)
     dec.wait(t)
     assert np.array_equal(dec.read(t), ref2)
+
+
+# --- I_PCM coding units ------------------------------------------------------
+@pytest.mark.parametrize("bd,idc", [(8, 1), (10, 2), (12, 3), (10, 0)])
+def test_pcm_cus(dec, bd, idc):
+    s = synth.SynthSet()
+    c = synth.intra_cfg(710 + bd + idc, 320, 256, bit_depth=bd, chroma_idc=idc)
+    c.pcm_p = 0.3
+    s.add(c)
+    pics = s.pictures()
+    tus = np.ctypeslib.as_array((C_u8 * (pics[0].n_tus * 16)).from_address(pics[0].tus)).view(abi.TU_DTYPE)
+    assert (tus["flags"] & abi.TU_PCM).any()
+    run_yuv(dec, pics, f"I_PCM {bd}-bit idc {idc}")
+
+
+def test_pcm_in_inter_pictures(dec):
+    s = synth.SynthSet()
+    c0 = synth.intra_cfg(720, 320, 192, bit_depth=8)
+    c0.pcm_p = 0.2
+    s.add(c0)
+    for i in range(1, 4):
+        c = synth.inter_cfg(720 + i, 320, 192, intra_cu_p=0.4, weighted=(i == 2))
+        c.pcm_p = 0.3
+        s.add(c)
+    run_yuv(dec, s.pictures(), "I_PCM in inter pictures")
