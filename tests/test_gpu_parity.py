@@ -972,3 +972,55 @@ def test_pcm_in_inter_pictures(dec):
         c.pcm_p = 0.3
         s.add(c)
     run_yuv(dec, s.pictures(), "I_PCM in inter pictures")
+
+
+# --- error paths of the added tools ------------------------------------------
+def test_added_tools_reject_malformed_inputs(dec):
+    import ctypes as C
+    from hpvcd_b200.gpu import Dpb
+    # cross-component chroma TB whose TU has no matching luma record: the
+    # kernel's own check reports it, nothing is written out of place
+    s = synth.SynthSet()
+    c = synth.intra_cfg(730, 128, 128, bit_depth=10, chroma_idc=3)
+    c.ccp_p = 0.9
+    s.add(c)
+    p = s.picture(0)
+    tus = np.ctypeslib.as_array((C_u8 * (p.n_tus * 16)).from_address(p.tus)).view(abi.TU_DTYPE).copy()
+    k = int(np.flatnonzero((tus["comp"] > 0) & (tus["res_scale"] != 0))[0])
+    for back in (1, 2, 3):
+        if k - back >= 0 and tus["comp"][k - back] == 0:
+            tus["x"][k - back] += 4          # the luma record moves away
+    q = abi.Picture()
+    C.pointer(q)[0] = p
+    q.tus = tus.ctypes.data
+    with pytest.raises(abi.HpvcdError) as e:
+        t = dec.submit([q])
+        dec.wait(t)
+        dec.read(t)
+    assert e.value.status == abi.ERR_BITSTREAM
+    # constrained intra prediction needs the cells
+    q2 = abi.Picture()
+    C.pointer(q2)[0] = p
+    q2.flags |= abi.PIC_CONSTRAINED_INTRA
+    q2.flags &= ~abi.PIC_DEBLOCK
+    q2.cells = None
+    with pytest.raises(abi.HpvcdError) as e:
+        dec.submit([q2])
+    assert e.value.status == abi.ERR_INVALID_ARG
+    # a DPB store into an entry the DPB does not have
+    q3 = abi.Picture()
+    C.pointer(q3)[0] = p
+    q3.flags = (p.flags & ~abi.PIC_CROSS_COMPONENT) | abi.PIC_STORE_DPB(5)
+    with GpuDecoder(0) as d2, Dpb(0, entries=2) as dpb:
+        d2.set_dpb(dpb)
+        with pytest.raises(abi.HpvcdError) as e:
+            d2.submit([q3])
+        assert e.value.status == abi.ERR_INVALID_ARG
+        d2.set_dpb(None)
+    # an output kind that does not exist
+    g = synth.make_grid(256, 256, seed=731, bit_depth=8, tile=256)
+    out, keep = synth.grid_output(g)
+    out.kind = 7
+    with pytest.raises(abi.HpvcdError) as e:
+        dec.submit(g.synth.pictures(), out)
+    assert e.value.status == abi.ERR_INVALID_ARG
