@@ -177,6 +177,7 @@ class Picture(C.Structure):
         ("pred", C.c_void_p * 3),
         ("scaling", C.c_void_p),
         ("ctb_region", C.c_void_p),
+        ("slice_deblock", C.c_void_p),
     ]
 
 

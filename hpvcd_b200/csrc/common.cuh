@@ -27,6 +27,7 @@ struct DevPic {
     const hpvcd_pu* pus;
     const hpvcd_scaling* scaling;  // NULL: flat scale
     const uint16_t* ctb_region;    // slice << 8 | tile per CTB, NULL: one region
+    const int8_t* slice_deblock;   // 256 x {beta, tc} offsets (div2) per slice, NULL: picture values
     uint32_t n_tus, n_pus;
     uint64_t n_coeffs;
     hpvcd_wp_table wp;

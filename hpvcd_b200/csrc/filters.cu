@@ -38,6 +38,18 @@ __device__ __forceinline__ bool exempt_at(const DevPic& P, int lx, int ly) {
     return (cell_at(P, lx, ly).flags & HPVCD_CELL_EXEMPT) != 0;
 }
 
+// Deblocking offsets (div2) of the slice holding luma sample (qx, qy)
+// (decode.rs:1762 slice_deblock_at: the q sample's slice).
+__device__ __forceinline__ void slice_offsets(const DevPic& P, int qx, int qy, int* beta_div2, int* tc_div2) {
+    *beta_div2 = P.beta_offset_div2;
+    *tc_div2 = P.tc_offset_div2;
+    if (P.slice_deblock && P.ctb_region) {
+        const int s = P.ctb_region[(size_t)(qy >> P.log2_ctb) * P.ctb_cols + (qx >> P.log2_ctb)] >> 8;
+        *beta_div2 = P.slice_deblock[2 * s];
+        *tc_div2 = P.slice_deblock[2 * s + 1];
+    }
+}
+
 // Luma segment: 8 taps x 4 lines around the edge, in registers.
 // v[line][tap+4] with tap -4..3 (p3..p0, q0..q3).
 __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan) {
@@ -49,8 +61,10 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan)
     const int qp_q = q.qp_y;
     const int avg = (qp_p + qp_q + 1) >> 1;
     const int sh = P.bd - 8;
-    const int beta = c_beta[clamp3i(avg + 2 * P.beta_offset_div2, 0, 51)] << sh;
-    const int tc = c_tc[clamp3i(avg + 2 * (bs - 1) + 2 * P.tc_offset_div2, 0, 53)] << sh;
+    int bo, to;
+    slice_offsets(P, vertical ? edge : mid, vertical ? mid : edge, &bo, &to);
+    const int beta = c_beta[clamp3i(avg + 2 * bo, 0, 51)] << sh;
+    const int tc = c_tc[clamp3i(avg + 2 * (bs - 1) + 2 * to, 0, 53)] << sh;
     if (tc == 0) return;
     const int w = P.w;
     void* pl = P.rec[0];
@@ -140,6 +154,9 @@ __device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int sca
         ppy = min(max(ley - 1, 0), P.h - 1);
     }
     const int avg = (qp_at(P, ppx, ppy) + qp_at(P, lqx, lqy) + 1) >> 1;
+    int bo, to;
+    slice_offsets(P, lqx, lqy, &bo, &to);
+    (void)bo;
     const int sh = P.bd_c - 8;
     const int maxv = (1 << P.bd_c) - 1;
     const int cw = P.cw;
@@ -147,7 +164,7 @@ __device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int sca
     for (int plane = 0; plane < 2; ++plane) {
         const int off = plane == 0 ? P.pps_cb_qp_offset : P.pps_cr_qp_offset;
         const int qc = qpc_map(avg + off, P.idc, P.bd_c);
-        const int tc = c_tc[clamp3i(qc + 2 + 2 * P.tc_offset_div2, 0, 53)] << sh;
+        const int tc = c_tc[clamp3i(qc + 2 + 2 * to, 0, 53)] << sh;
         if (tc == 0) continue;
         void* pl = P.rec[1 + plane];
         for (int s = scan; s < scan + 4; ++s) {

@@ -367,6 +367,7 @@ void fill_inputs(DevPic& d, const hpvcd_picture& p) {
     d.pus = p.pus;
     d.scaling = p.scaling;
     d.ctb_region = p.ctb_region;
+    d.slice_deblock = p.slice_deblock;
     d.n_tus = p.n_tus;
     d.n_pus = p.n_pus;
     d.n_coeffs = p.n_coeffs;
@@ -954,13 +955,14 @@ hpvcd_status device_status(hpvcd_plan* P, cudaStream_t st) {
 
 // Layout of the inputs of a batch in one arena (256-byte aligned parts in a
 // fixed order per picture: tus, ctu starts, coefficients, cells, SAO, PUs,
-// scaling lists, CTB regions, prediction planes).  Shared by hpvcd_gpu_pack_inputs and submit.
+// scaling lists, CTB regions, slice deblocking offsets, prediction planes).  Shared by hpvcd_gpu_pack_inputs and submit.
 struct InputPart {
     const void* src;
     size_t bytes;
     size_t off;
     uint32_t pic;
-    int kind;  // 0..5 as above, 6..8 = prediction planes Y/Cb/Cr, 9 = scaling lists, 10 = CTB regions
+    int kind;  // 0..5 as above, 6..8 = prediction planes Y/Cb/Cr, 9 = scaling lists, 10 = CTB regions,
+               // 11 = per-slice deblocking offsets
 };
 
 size_t input_layout(const hpvcd_picture* pics, uint32_t n, std::vector<InputPart>* parts) {
@@ -982,6 +984,7 @@ size_t input_layout(const hpvcd_picture* pics, uint32_t n, std::vector<InputPart
         add(i, 5, p.pus, (size_t)p.n_pus * sizeof(hpvcd_pu));
         add(i, 9, p.scaling, sizeof(hpvcd_scaling));
         add(i, 10, p.ctb_region, ctbs * sizeof(uint16_t));
+        add(i, 11, p.slice_deblock, 512);
         if (p.flags & HPVCD_PIC_PRED_IN_PLANE)
             for (int c = 0; c < (p.chroma_idc ? 3 : 1); ++c)
                 add(i, 6 + c, p.pred[c], c ? geo.chroma_bytes : geo.luma_bytes);
@@ -999,6 +1002,7 @@ void point_at(hpvcd_picture& d, int kind, const void* ptr) {
         case 5: d.pus = (const hpvcd_pu*)ptr; break;
         case 9: d.scaling = (const hpvcd_scaling*)ptr; break;
         case 10: d.ctb_region = (const uint16_t*)ptr; break;
+        case 11: d.slice_deblock = (const int8_t*)ptr; break;
         default: d.pred[kind - 6] = ptr; break;
     }
 }
@@ -1433,6 +1437,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         d.sao = nullptr; d.pus = nullptr; d.pred[0] = d.pred[1] = d.pred[2] = nullptr;
         d.scaling = nullptr;
         d.ctb_region = nullptr;
+        d.slice_deblock = nullptr;
     }
     // Runs of parts laid out contiguously (as hpvcd_gpu_pack_inputs lays them
     // out) in page-locked memory go up by DMA straight from the caller's

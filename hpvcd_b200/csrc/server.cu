@@ -160,6 +160,7 @@ struct hpvcd_server {
             p.pus = (const hpvcd_pu*)fix(p.pus);
             p.scaling = (const hpvcd_scaling*)fix(p.scaling);
             p.ctb_region = (const uint16_t*)fix(p.ctb_region);
+            p.slice_deblock = (const int8_t*)fix(p.slice_deblock);
             for (int c = 0; c < 3; ++c) p.pred[c] = fix(p.pred[c]);
             if (p.wp) p.wp = &b.wp[i];
         }
@@ -335,6 +336,7 @@ HPVCD_API hpvcd_status hpvcd_server_submit(hpvcd_server* s, const hpvcd_request*
             p.pus = (const hpvcd_pu*)off(p.pus);
             p.scaling = (const hpvcd_scaling*)off(p.scaling);
             p.ctb_region = (const uint16_t*)off(p.ctb_region);
+            p.slice_deblock = (const int8_t*)off(p.slice_deblock);
             for (int c = 0; c < 3; ++c) p.pred[c] = off(p.pred[c]);
             bp->wp[first + i] = req->pics[i].wp ? *req->pics[i].wp : hpvcd_wp_table{};
             p.wp = req->pics[i].wp ? (const hpvcd_wp_table*)1 : nullptr;  // resolved at launch

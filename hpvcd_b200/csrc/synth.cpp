@@ -55,6 +55,7 @@ struct Picture {
     hpvcd_scaling scaling{};
     bool has_scaling = false;
     std::vector<uint16_t> ctb_region;
+    std::vector<int8_t> slice_deblock;  // 256 x {beta, tc} div2
     std::vector<uint8_t> pred8[3];
     std::vector<uint16_t> pred16[3];
 };
@@ -540,6 +541,11 @@ struct Gen {
                 if (a > b) std::swap(a, b);
                 if (a == b) b = std::min(n - 1, b + 1);
                 for (int i = 0; i < n; ++i) P.ctb_region[(size_t)i] = (uint16_t)((i >= a) + (i >= b)) << 8;
+                P.slice_deblock.assign(512, 0);
+                for (int k = 0; k < 3; ++k) {  // each slice its own offsets
+                    P.slice_deblock[(size_t)2 * k] = (int8_t)rr.range(-6, 6);
+                    P.slice_deblock[(size_t)2 * k + 1] = (int8_t)rr.range(-6, 6);
+                }
             } else if (c.regions == 2) {
                 for (int y = 0; y < rows; ++y)
                     for (int x = 0; x < cols; ++x) {
@@ -663,6 +669,7 @@ int32_t hpvcd_synth_add(hpvcd_synth* s, const hpvcd_synth_cfg* cfg) {
     d.wp = pic->has_wp ? &pic->wp : nullptr;
     d.scaling = pic->has_scaling ? &pic->scaling : nullptr;
     d.ctb_region = pic->ctb_region.empty() ? nullptr : pic->ctb_region.data();
+    d.slice_deblock = pic->slice_deblock.empty() ? nullptr : pic->slice_deblock.data();
     for (int c = 0; c < 3; ++c)
         d.pred[c] = !pic->pred8[c].empty() ? (const void*)pic->pred8[c].data()
                     : !pic->pred16[c].empty() ? (const void*)pic->pred16[c].data()

@@ -272,6 +272,7 @@ class DevicePlan:
             d.wp = self._upload(p.wp, C.sizeof(abi.WpTable))
             d.scaling = self._upload(p.scaling, C.sizeof(abi.Scaling))
             d.ctb_region = self._upload(p.ctb_region, ctbs * 2)
+            d.slice_deblock = self._upload(p.slice_deblock, 512)
             for c in range(3):
                 if p.pred[c]:
                     nb = (g["w"] * g["h"] if c == 0 else g["cw"] * g["ch"]) * g["bytes_per_sample"]

@@ -256,6 +256,11 @@ typedef struct hpvcd_picture {
      * HPVCD_PIC_SAO_NO_ACROSS_* flags; deblocking gating is folded into the
      * cells' boundary strengths by the host.  NULL -> one slice, one tile. */
     const uint16_t* ctb_region;
+    /* Per-slice deblocking offsets (decode.rs:1762 slice_deblock_at): 256
+     * pairs {slice_beta_offset_div2, slice_tc_offset_div2} indexed by the
+     * slice of ctb_region; an edge uses the pair of the slice holding its q
+     * sample.  NULL (or no ctb_region) -> beta/tc_offset_div2 above. */
+    const int8_t* slice_deblock;
 } hpvcd_picture;
 
 /* Output of a batch.  RGB8 is the `decode_heic_rgb8` path (lib.rs:1964):

@@ -1083,7 +1083,18 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
     const Geo g = geo_of(p);
     const hpvcd_cell* cells = p->cells;
     const int bd_shift = g.bd - 8, bd_shift_c = g.bd_c - 8;
-    const int beta_offset = p->beta_offset_div2 * 2, tc_offset = p->tc_offset_div2 * 2;
+    // decode.rs:1762 slice_deblock_at: the offsets of the slice holding the
+    // q sample, else the picture's
+    auto offsets_at = [&](int qx, int qy, int* beta_offset, int* tc_offset) {
+        int b = p->beta_offset_div2, t = p->tc_offset_div2;
+        if (p->slice_deblock && p->ctb_region) {
+            const int s = p->ctb_region[(size_t)(qy >> g.log2_ctb) * g.ctb_cols + (qx >> g.log2_ctb)] >> 8;
+            b = p->slice_deblock[2 * s];
+            t = p->slice_deblock[2 * s + 1];
+        }
+        *beta_offset = 2 * b;
+        *tc_offset = 2 * t;
+    };
     auto qp_at = [&](int px, int py) {
         const int gx = std::min(px / 4, g.gw - 1), gy = std::min(py / 4, g.gh - 1);
         return (int)cells[(size_t)gy * g.gw + gx].qp_y;
@@ -1133,6 +1144,8 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
                 const int qp_p = pass == 0 ? qp_at(edge - 1, mid) : qp_at(mid, edge - 1);
                 const int qp_q = pass == 0 ? qp_at(edge, mid) : qp_at(mid, edge);
                 const int avg = (qp_p + qp_q + 1) >> 1;
+                int beta_offset, tc_offset;
+                offsets_at(pass == 0 ? edge : mid, pass == 0 ? mid : edge, &beta_offset, &tc_offset);
                 const int beta = kBeta[clamp3(avg + beta_offset, 0, 51)] << bd_shift;
                 const int tc = kTc[clamp3(avg + 2 * (bs - 1) + tc_offset, 0, 53)] << bd_shift;
                 if (tc == 0) continue;
@@ -1167,6 +1180,9 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
                     ppy = std::min(std::max(ley - 1, 0), g.h - 1);
                 }
                 const int avg = (qp_at(ppx, ppy) + qp_at(lqx, lqy) + 1) >> 1;
+                int beta_offset, tc_offset;
+                offsets_at(lqx, lqy, &beta_offset, &tc_offset);
+                (void)beta_offset;
                 for (int plane = 0; plane < 2; ++plane) {
                     const int coff = plane == 0 ? p->pps_cb_qp_offset : p->pps_cr_qp_offset;
                     const int qpcv = qpc(avg + coff, g.idc, g.bd_c);
