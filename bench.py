@@ -48,6 +48,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--e2e-inflight", type=int, default=3, help="steps in flight in the end-to-end measurement")
+    ap.add_argument("--e2e-schedule", choices=("network", "default"), default="network",
+                    help="end-to-end: schedule picked per submit by the selector network, or the default one")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["grid", "serving", "selector", "inter"], default="grid",
                     help="grid: the 4032x3024 still (default); serving: mixed-size batched serving; "
@@ -183,7 +185,7 @@ def run_reference(args):
     return 0
 
 
-def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2):
+def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="network"):
     """Same decode through hpvcd_gpu_submit / wait / read: inputs packed in
     page-locked host memory (one H2D DMA per step), the RGB8 canvas DMA'd
     back to a page-locked caller buffer every step.  `in_flight` steps are
@@ -205,7 +207,7 @@ def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2):
         o.host_dst = dst.ctypes.data
         o.host_dst_bytes = canvas_bytes
         outs.append((o, dst, dkeep, okeep))
-    mlp = _selector_network()
+    mlp = _selector_network() if schedule == "network" else None
     with GpuDecoder(local, max_inflight=in_flight) as decd:
         if mlp is not None:  # every submit picks its schedule from the batch's features
             from hpvcd_b200 import selector
@@ -377,7 +379,7 @@ def run_ours(args):
     e2e = None
     K2 = args.e2e_steps if args.e2e_steps is not None else max(5, min(K, 50))
     if K2 > 0:
-        e2e = run_e2e(pics, g, K2, args.warmup, local, world, dev, max(1, args.e2e_inflight))
+        e2e = run_e2e(pics, g, K2, args.warmup, local, world, dev, max(1, args.e2e_inflight), args.e2e_schedule)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

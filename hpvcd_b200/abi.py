@@ -322,6 +322,7 @@ def lib() -> C.CDLL:
             "hpvcd_gpu_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
             "hpvcd_server_set_selector": (i32, [vp, vp, C.POINTER(Sched), u32]),
             "hpvcd_server_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
+            "hpvcd_batch_features": (i32, [C.POINTER(Picture), u32, C.POINTER(C.c_float)]),
             "hpvcd_dpb_create": (i32, [i32, u32, C.POINTER(vp)]),
             "hpvcd_dpb_destroy": (i32, [vp]),
             "hpvcd_gpu_set_dpb": (i32, [vp, vp]),

@@ -25,6 +25,9 @@ extern "C" cudaError_t hpvcd_launch_ccp(const DevPic*, const uint32_t*, uint32_t
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int, int,
                                           int, int, cudaStream_t);
 extern "C" int hpvcd_recon_occupancy(int cfmt);
+extern "C" hpvcd_status hpvcd_mlp_host_copy(hpvcd_mlp* M, float* params, float* lohi, int* has_domain);
+extern "C" uint32_t hpvcd_mlp_pick_host(const float* w, uint32_t K, const float* x, const float* lohi,
+                                        int has_domain);
 extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, uint8_t*, cudaStream_t);
@@ -890,6 +893,10 @@ struct hpvcd_gpu {
     // schedule selection per submitted batch (hpvcd_gpu_set_selector)
     hpvcd_mlp* sel = nullptr;
     std::vector<hpvcd_sched> sel_cands;
+    // host copy of the network, read by the submit path's host-side pick
+    std::vector<float> sel_w;
+    float sel_lohi[2 * HPVCD_FEATURES] = {};
+    int sel_has_domain = 0;
     uint64_t sel_picks[HPVCD_MLP_MAX_VARIANTS + 1] = {};  // last entry: batches outside the domain
     ~hpvcd_gpu() {
         for (Slot& s : slots) {
@@ -1380,6 +1387,17 @@ HPVCD_API hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* g, hpvcd_mlp* mlp, cons
     g->sel = mlp;
     g->sel_cands.assign(cands, cands + (mlp ? n : 0));
     std::memset(g->sel_picks, 0, sizeof(g->sel_picks));
+    g->sel_w.clear();
+    if (mlp) {  // the network as it is now: later training needs another set_selector
+        cudaSetDevice(g->device);
+        g->sel_w.resize(hpvcd_mlp_param_count(mlp));
+        const hpvcd_status s = hpvcd_mlp_host_copy(mlp, g->sel_w.data(), g->sel_lohi, &g->sel_has_domain);
+        if (s != HPVCD_OK) {
+            g->sel = nullptr;
+            g->sel_cands.clear();
+            return s;
+        }
+    }
     return HPVCD_OK;
 }
 
@@ -1517,10 +1535,13 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     g->in_use = g->in_use - held + slot->d_in_cap + slot->plan_bytes;
     slot->held = slot->d_in_cap + slot->plan_bytes;
     if (st != HPVCD_OK) return st;
-    if (g->sel) {  // the network picks the batch's schedule from its features
-        uint32_t pick = 0;
-        st = hpvcd_plan_select(slot->plan, g->sel, g->sel_cands.data(), (uint32_t)g->sel_cands.size(), slot->stream,
-                               &pick);
+    if (g->sel) {  // the network picks the batch's schedule from its features, on the host
+        float fv[HPVCD_FEATURES];
+        st = hpvcd_batch_features(pics, n, fv);
+        if (st != HPVCD_OK) return st;
+        const uint32_t pick = hpvcd_mlp_pick_host(g->sel_w.data(), (uint32_t)g->sel_cands.size(), fv,
+                                                  g->sel_lohi, g->sel_has_domain);
+        st = hpvcd_plan_set_sched(slot->plan, &g->sel_cands[pick == HPVCD_MLP_NO_PICK ? 0 : pick]);
         if (st != HPVCD_OK) return st;
         ++g->sel_picks[pick == HPVCD_MLP_NO_PICK ? HPVCD_MLP_MAX_VARIANTS : pick];
     }

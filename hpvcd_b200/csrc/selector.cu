@@ -533,6 +533,118 @@ HPVCD_API hpvcd_status hpvcd_mlp_destroy(hpvcd_mlp* M) {
 HPVCD_API uint32_t hpvcd_mlp_param_count(const hpvcd_mlp* M) { return M ? (uint32_t)M->P : 0; }
 HPVCD_API uint32_t hpvcd_mlp_variants(const hpvcd_mlp* M) { return M ? (uint32_t)M->K : 0; }
 
+// ---------------------------------------------------------------------------
+// Host-side selection for batches whose records are in host memory (the
+// hpvcd_gpu_submit path): the features from the host records and the
+// network's forward pass on the host, so a submit picks its schedule without
+// a device round trip.  The sums are the integer sums of k_features and the
+// forward uses the bf16-rounded weights with fused multiply-adds in the
+// kernel's order, so the outputs are those of k_mlp_forward.
+// ---------------------------------------------------------------------------
+HPVCD_API hpvcd_status hpvcd_batch_features(const hpvcd_picture* pics, uint32_t n, float* out) {
+    if (!pics || !out) return HPVCD_ERR_INVALID_ARG;
+    unsigned long long acc[FA_COUNT] = {};
+    double area = 0, bdsum = 0, a444 = 0;
+    int wave = 0;
+    for (uint32_t p = 0; p < n; ++p) {
+        const hpvcd_picture& P = pics[p];
+        const double a = (double)P.width * P.height;
+        area += a;
+        bdsum += a * P.bit_depth_y;
+        if (P.chroma_idc == 3) a444 += a;
+        const int ctb = 1 << P.log2_ctb;
+        wave = std::max(wave, (int)((P.width + ctb - 1) / ctb + 2 * ((P.height + ctb - 1) / ctb)));
+        for (uint32_t r = 0; r < P.n_tus && P.tus; ++r) {
+            const hpvcd_tu& t = P.tus[r];
+            if (t.comp != 0 || t.log2n < 2 || t.log2n > 5) continue;
+            const bool coded = (t.flags & HPVCD_TU_CBF) != 0, intra = (t.flags & HPVCD_TU_INTRA) != 0;
+            if (!coded && !intra) continue;
+            const unsigned long long ar = 1ull << (2 * t.log2n);
+            acc[FA_TB4 + (t.log2n - 2)] += ar;
+            if (coded) {
+                acc[FA_CODED] += ar;
+                const int nn = 1 << t.log2n;
+                const int nx = (t.nx == 0 || t.nx > nn) ? nn : t.nx;
+                acc[FA_NX] += (unsigned long long)(64 * nx / nn);
+                acc[FA_NCODED] += 1;
+            }
+            if (intra) acc[FA_INTRA] += ar;
+            const int qp = t.qp_y + 64;
+            acc[FA_QP] += (unsigned long long)qp;
+            acc[FA_QP2] += (unsigned long long)(qp * qp);
+            acc[FA_NTB] += 1;
+        }
+        for (uint32_t u = 0; u < P.n_pus && P.pus; ++u) {
+            const hpvcd_pu& pu = P.pus[u];
+            acc[FA_NPU] += 1;
+            int lists = 0;
+            for (int l = 0; l < 2; ++l)
+                if (pu.flags & (1u << l)) {
+                    acc[FA_MV] += (unsigned long long)(std::abs((int)pu.mv[l][0]) + std::abs((int)pu.mv[l][1]));
+                    ++lists;
+                }
+            acc[FA_NMV] += (unsigned long long)lists;
+            if (lists == 2) acc[FA_BI] += 1;
+        }
+    }
+    // k_features_finish
+    area = std::max(area, 1.0);
+    const double tb = std::max((double)(acc[FA_TB4] + acc[FA_TB8] + acc[FA_TB16] + acc[FA_TB32]), 1.0);
+    const double ntb = std::max((double)acc[FA_NTB], 1.0);
+    const double qp_mean = (double)acc[FA_QP] / ntb;
+    const double qp_var = std::max((double)acc[FA_QP2] / ntb - qp_mean * qp_mean, 0.0);
+    const double nmv = std::max((double)acc[FA_NMV], 1.0);
+    out[0] = (float)(std::log2(area) / 24.0);
+    out[1] = (float)(std::log2(1.0 + n) / 8.0);
+    out[2] = (float)(wave / 256.0);
+    out[3] = (float)((bdsum / area - 8.0) / 4.0);
+    out[4] = (float)(a444 / area);
+    for (int k = 0; k < 4; ++k) out[5 + k] = (float)(acc[FA_TB4 + k] / tb);
+    out[9] = (float)(acc[FA_CODED] / area);
+    out[10] = (float)(acc[FA_INTRA] / area);
+    out[11] = (float)((qp_mean - 64.0) / 51.0);
+    out[12] = (float)(std::sqrt(qp_var) / 16.0);
+    out[13] = (float)((double)acc[FA_NX] / std::max((double)acc[FA_NCODED], 1.0) / 64.0);
+    out[14] = (float)(std::log2(1.0 + (double)acc[FA_MV] / nmv / 4.0) / 8.0);
+    out[15] = (float)((double)acc[FA_BI] / std::max((double)acc[FA_NPU], 1.0));
+    return HPVCD_OK;
+}
+
+// Host copy of a network: its bf16-rounded parameters as fp32 and, when it
+// has one, its feature domain (lo[16], hi[16]).
+extern "C" hpvcd_status hpvcd_mlp_host_copy(hpvcd_mlp* M, float* params, float* lohi, int* has_domain);
+
+// k_mlp_forward + k_mlp_argmin for one sample on the host.
+extern "C" uint32_t hpvcd_mlp_pick_host(const float* w, uint32_t K, const float* x, const float* lohi,
+                                        int has_domain) {
+    const MlpLayout L((int)K);
+    float h1[kHidden], h2[kHidden];
+    for (int j = 0; j < kHidden; ++j) {
+        float a = w[L.b1 + j];
+        for (int i = 0; i < kFeatures; ++i) a = std::fma(w[L.w1 + j * kFeatures + i], x[i], a);
+        h1[j] = std::max(a, 0.f);
+    }
+    for (int j = 0; j < kHidden; ++j) {
+        float a = w[L.b2 + j];
+        for (int i = 0; i < kHidden; ++i) a = std::fma(w[L.w2 + j * kHidden + i], h1[i], a);
+        h2[j] = std::max(a, 0.f);
+    }
+    int best = 0;
+    float best_y = 0.f;
+    for (int k = 0; k < (int)K; ++k) {
+        float a = w[L.b3 + k];
+        for (int i = 0; i < kHidden; ++i) a = std::fma(w[L.w3 + k * kHidden + i], h2[i], a);
+        if (k == 0 || a < best_y) {
+            best = k;
+            best_y = a;
+        }
+    }
+    if (has_domain)
+        for (int i = 0; i < kFeatures; ++i)
+            if (!(x[i] >= lohi[i] && x[i] <= lohi[kFeatures + i])) return HPVCD_MLP_NO_PICK;
+    return (uint32_t)best;
+}
+
 HPVCD_API hpvcd_status hpvcd_mlp_get_params(hpvcd_mlp* M, float* host, int master) {
     if (!M || !host) return HPVCD_ERR_INVALID_ARG;
     cudaError_t e;
@@ -547,6 +659,15 @@ HPVCD_API hpvcd_status hpvcd_mlp_get_params(hpvcd_mlp* M, float* host, int maste
         cudaFree(tmp);
     }
     return hpvcd_internal_status(e);
+}
+
+extern "C" hpvcd_status hpvcd_mlp_host_copy(hpvcd_mlp* M, float* params, float* lohi, int* has_domain) {
+    if (!M || !params || !lohi || !has_domain) return HPVCD_ERR_INVALID_ARG;
+    const hpvcd_status s = hpvcd_mlp_get_params(M, params, 0);
+    if (s != HPVCD_OK) return s;
+    *has_domain = M->has_domain ? 1 : 0;
+    if (!M->has_domain) return HPVCD_OK;
+    return hpvcd_internal_status(cudaMemcpy(lohi, M->dom, sizeof(float) * 2 * kFeatures, cudaMemcpyDeviceToHost));
 }
 
 // Feature domain of the training data: a pick for features outside

@@ -94,6 +94,12 @@ class GpuDecoder:
         _check(self._L.hpvcd_gpu_set_selector(self._h, mlp.handle if mlp is not None else None, arr,
                                               len(schedules)), "hpvcd_gpu_set_selector")
 
+    def selector_picks(self, n: int) -> list:
+        """Picks per candidate schedule so far ([K]: batches outside the domain)."""
+        out = (C.c_uint64 * n)()
+        _check(self._L.hpvcd_gpu_selector_picks(self._h, out, n), "hpvcd_gpu_selector_picks")
+        return list(out)
+
     def set_dpb(self, dpb: "Dpb | None") -> None:
         """Decoded-picture buffer the submits store into (flags
         abi.PIC_STORE_DPB(e)) and predict from (ref_slot abi.REF_DPB(e))."""

@@ -500,6 +500,9 @@ hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched);
  *   14 log2(1 + mean |mv| in luma samples) / 8   15 bi-predicted PU share */
 hpvcd_status hpvcd_plan_features(hpvcd_plan* plan, uint32_t first, uint32_t count, float* dev_out,
                                  void* stream);
+/* The same 16 features on the host from host-memory pictures (the same
+ * integer sums, the same formulas), written to out[16]. */
+hpvcd_status hpvcd_batch_features(const hpvcd_picture* host_pics, uint32_t n, float* out);
 /* Exhaustive autotuning: one untimed launch, then per candidate `warmup`
  * untimed and `reps` timed launches (CUDA events on `stream`, selected
  * stages); ms[i] (host, may be NULL) = the fastest timed launch of

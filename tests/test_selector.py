@@ -162,6 +162,28 @@ def test_tu_mix_steers_tb_sizes():
             assert f[5] > 0.6
 
 
+def test_host_batch_features_match_the_restatement():
+    """hpvcd_batch_features (the submit path's host-side features) equals the
+    restatement of k_features / k_features_finish on intra, inter and 4:4:4
+    batches (no GPU needed)."""
+    import ctypes as C
+    L = abi.lib()
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(31, 512, 384, bit_depth=10, chroma_idc=1))
+    c = synth.intra_cfg(32, 256, 256, bit_depth=8, chroma_idc=3, tskip_p=0.1)
+    for k, v in enumerate((0.1, 0.2, 0.3, 0.4)):
+        c.tu_mix[k] = v
+    s.add(c)
+    s.add(synth.intra_cfg(34, 256, 256, bit_depth=8, chroma_idc=1))
+    s.add(synth.inter_cfg(33, 256, 256, weighted=True))
+    pics = s.pictures()
+    for first, count in ((0, 4), (3, 1), (1, 1), (0, 2)):
+        arr = (abi.Picture * count)(*pics[first:first + count])
+        f = (C.c_float * 16)()
+        assert L.hpvcd_batch_features(arr, count, f) == abi.OK
+        np.testing.assert_allclose(np.array(f), features_host(pics[first:first + count]), rtol=1e-6, atol=1e-7)
+
+
 def test_trained_selector_gains_on_heldout_frames_cpu():
     """The committed network, evaluated with the numpy oracle forward pass on
     its bf16 weights over the held-out measured frames: faster in total
@@ -381,6 +403,43 @@ def test_server_with_selector_keeps_pixels():
         out, keep = synth.grid_output(synth.Grid(w, h, 512, s, places))
         _, ref = O.decode_batch(pics, out, want_planes=False)
         assert np.array_equal(got[k]["image"], ref), k
+    m.close()
+
+
+@pytest.mark.gpu
+def test_submit_path_host_pick_equals_device_pick():
+    """A context's submit picks on the host (host features, host forward of
+    the bf16 weights); the pick equals the device path's (k_features + the
+    network kernels, hpvcd_plan_select) on the same batches."""
+    torch = _gpu()
+    import ctypes as C
+    from hpvcd_b200.gpu import DevicePlan, GpuDecoder
+    m = selector.Mlp.load() if os.path.exists(selector.WEIGHTS_PATH) else selector.Mlp(selector.K, seed=5)
+    L = abi.lib()
+    cands = (abi.Sched * selector.K)(*selector.SCHEDULES)
+    batches = []
+    for i in range(4):
+        s = synth.SynthSet()
+        g = synth.make_grid(1024 + 256 * i, 768, seed=40 + i, bit_depth=10 if i % 2 else 8, synth=s)
+        batches.append((s, s.pictures()))
+    with GpuDecoder(0) as d:
+        d.set_selector(m, selector.SCHEDULES)
+        for s, pics in batches:
+            before = d.selector_picks(selector.K + 1)
+            t = d.submit(pics)
+            d.wait(t)
+            d.read(t)
+            after = d.selector_picks(selector.K + 1)
+            host_pick = int(np.flatnonzero(np.array(after) - np.array(before))[0])
+            plan = DevicePlan(pics)
+            dev_pick = C.c_uint32()
+            st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+            assert L.hpvcd_plan_select(plan._h, m.handle, cands, selector.K, st, C.byref(dev_pick)) == abi.OK
+            torch.cuda.synchronize()
+            dp = selector.K if dev_pick.value == abi.MLP_NO_PICK else dev_pick.value
+            assert host_pick == dp
+            plan.close()
+        d.set_selector(None, selector.SCHEDULES)
     m.close()
 
 
