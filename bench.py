@@ -49,7 +49,8 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--e2e-inflight", type=int, default=3, help="steps in flight in the end-to-end measurement")
     ap.add_argument("--e2e-schedule", choices=("network", "default"), default="network",
-                    help="end-to-end: schedule picked per submit by the selector network, or the default one")
+                    help="end-to-end: the selector network's pick per submit (the headline), or the default "
+                         "schedule; the other one is reported beside it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["grid", "serving", "selector", "inter"], default="grid",
                     help="grid: the 4032x3024 still (default); serving: mixed-size batched serving; "
@@ -377,9 +378,12 @@ def run_ours(args):
 
     # ---- end to end through the C ABI (host buffers) ----
     e2e = None
-    K2 = args.e2e_steps if args.e2e_steps is not None else max(5, min(K, 50))
+    K2 = args.e2e_steps if args.e2e_steps is not None else max(5, min(K, 200))
     if K2 > 0:
         e2e = run_e2e(pics, g, K2, args.warmup, local, world, dev, max(1, args.e2e_inflight), args.e2e_schedule)
+        other = "network" if args.e2e_schedule == "default" else "default"
+        alt = run_e2e(pics, g, K2, args.warmup, local, world, dev, max(1, args.e2e_inflight), other)
+        e2e["other_schedule"] = {k: alt[k] for k in ("value", "ms_per_step", "p50_ms", "p99_ms", "schedule")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
