@@ -1535,13 +1535,26 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     g->in_use = g->in_use - held + slot->d_in_cap + slot->plan_bytes;
     slot->held = slot->d_in_cap + slot->plan_bytes;
     if (st != HPVCD_OK) return st;
-    if (g->sel) {  // the network picks the batch's schedule from its features, on the host
-        float fv[HPVCD_FEATURES];
-        st = hpvcd_batch_features(pics, n, fv);
-        if (st != HPVCD_OK) return st;
-        const uint32_t pick = hpvcd_mlp_pick_host(g->sel_w.data(), (uint32_t)g->sel_cands.size(), fv,
-                                                  g->sel_lohi, g->sel_has_domain);
-        st = hpvcd_plan_set_sched(slot->plan, &g->sel_cands[pick == HPVCD_MLP_NO_PICK ? 0 : pick]);
+    if (g->sel) {  // the network picks the batch's schedule from its features
+        // Up to kHostPickRecords records (a few ms of host work at most) the
+        // features and the network run on the host, with no device round
+        // trip; larger batches use the kernels and wait for their pick.  Both
+        // give the same pick.
+        constexpr uint64_t kHostPickRecords = 1u << 19;
+        uint64_t records = 0;
+        for (uint32_t i = 0; i < n; ++i) records += pics[i].n_tus + pics[i].n_pus;
+        uint32_t pick = 0;
+        if (records <= kHostPickRecords) {
+            float fv[HPVCD_FEATURES];
+            st = hpvcd_batch_features(pics, n, fv);
+            if (st != HPVCD_OK) return st;
+            pick = hpvcd_mlp_pick_host(g->sel_w.data(), (uint32_t)g->sel_cands.size(), fv, g->sel_lohi,
+                                       g->sel_has_domain);
+            st = hpvcd_plan_set_sched(slot->plan, &g->sel_cands[pick == HPVCD_MLP_NO_PICK ? 0 : pick]);
+        } else {
+            st = hpvcd_plan_select(slot->plan, g->sel, g->sel_cands.data(), (uint32_t)g->sel_cands.size(),
+                                   slot->stream, &pick);
+        }
         if (st != HPVCD_OK) return st;
         ++g->sel_picks[pick == HPVCD_MLP_NO_PICK ? HPVCD_MLP_MAX_VARIANTS : pick];
     }
