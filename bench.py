@@ -48,9 +48,10 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--e2e-inflight", type=int, default=3, help="steps in flight in the end-to-end measurement")
-    ap.add_argument("--e2e-schedule", choices=("network", "default"), default="network",
-                    help="end-to-end: the selector network's pick per submit (the headline), or the default "
-                         "schedule; the other one is reported beside it")
+    ap.add_argument("--e2e-schedule", default="network",
+                    help="end-to-end: 'network' (the selector's pick per submit, the headline), 'default', "
+                         "or 'fixed:K' (candidate K of the selector's list); the network and the default "
+                         "schedule are reported beside each other")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["grid", "serving", "selector", "inter"], default="grid",
                     help="grid: the 4032x3024 still (default); serving: mixed-size batched serving; "
@@ -210,6 +211,9 @@ def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="netwo
         outs.append((o, dst, dkeep, okeep))
     mlp = _selector_network() if schedule == "network" else None
     with GpuDecoder(local, max_inflight=in_flight) as decd:
+        if schedule.startswith("fixed:"):
+            from hpvcd_b200 import selector
+            decd.set_sched(selector.SCHEDULES[int(schedule.split(":")[1])])
         if mlp is not None:  # every submit picks its schedule from the batch's features
             from hpvcd_b200 import selector
             decd.set_selector(mlp, selector.SCHEDULES)
@@ -244,7 +248,7 @@ def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="netwo
             "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3),
             "in_flight": in_flight,
             "api": "hpvcd_gpu_submit/wait/read, pinned packed inputs, pinned RGB8 output",
-            "schedule": "network pick per submit" if mlp is not None else "default"}
+            "schedule": "network pick per submit" if mlp is not None else schedule}
 
 
 def run_ours(args):

@@ -320,6 +320,7 @@ def lib() -> C.CDLL:
             "hpvcd_mlp_set_domain": (i32, [vp, vp, vp]),
             "hpvcd_gpu_set_selector": (i32, [vp, vp, C.POINTER(Sched), u32]),
             "hpvcd_gpu_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
+            "hpvcd_gpu_set_sched": (i32, [vp, C.POINTER(Sched)]),
             "hpvcd_server_set_selector": (i32, [vp, vp, C.POINTER(Sched), u32]),
             "hpvcd_server_selector_picks": (i32, [vp, C.POINTER(u64), u32]),
             "hpvcd_batch_features": (i32, [C.POINTER(Picture), u32, C.POINTER(C.c_float)]),

@@ -893,6 +893,7 @@ struct hpvcd_gpu {
     // schedule selection per submitted batch (hpvcd_gpu_set_selector)
     hpvcd_mlp* sel = nullptr;
     std::vector<hpvcd_sched> sel_cands;
+    hpvcd_sched fixed{};  // hpvcd_gpu_set_sched: the schedule without a selector
     // host copy of the network, read by the submit path's host-side pick
     std::vector<float> sel_w;
     float sel_lohi[2 * HPVCD_FEATURES] = {};
@@ -1401,6 +1402,13 @@ HPVCD_API hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* g, hpvcd_mlp* mlp, cons
     return HPVCD_OK;
 }
 
+HPVCD_API hpvcd_status hpvcd_gpu_set_sched(hpvcd_gpu* g, const hpvcd_sched* sched) {
+    if (!g) return HPVCD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(g->mu);
+    g->fixed = sched ? *sched : hpvcd_sched{};
+    return HPVCD_OK;
+}
+
 HPVCD_API hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu* g, uint64_t* counts, uint32_t n) {
     if (!g || !counts) return HPVCD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g->mu);
@@ -1557,6 +1565,29 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
         }
         if (st != HPVCD_OK) return st;
         ++g->sel_picks[pick == HPVCD_MLP_NO_PICK ? HPVCD_MLP_MAX_VARIANTS : pick];
+    } else {
+        st = hpvcd_plan_set_sched(slot->plan, &g->fixed);
+        if (st != HPVCD_OK) return st;
+    }
+    // Tickets already in flight share the SMs with this one: the wavefront
+    // kernel's persistent grid keeps to its share of the CTA slots (its CTAs
+    // wait for their neighbour CTUs in place, holding slots the other
+    // tickets' kernels need).  At three tickets in flight on the 4032x3024
+    // grid this is worth about 15 % of throughput; a ticket alone keeps the
+    // full grid.
+    {
+        int others = 0;
+        for (const Slot& s : g->slots)
+            if (s.busy && &s != slot) ++others;
+        if (others > 0) {
+            hpvcd_sched s2 = slot->plan->sched;
+            const int occ = std::max(1, slot->plan->recon_occ);
+            const int share = std::max(1, occ / (others + 1));
+            const int cur = s2.recon_ctas_per_sm ? (int)s2.recon_ctas_per_sm : occ;
+            s2.recon_ctas_per_sm = (uint32_t)std::min(cur, share);
+            st = hpvcd_plan_set_sched(slot->plan, &s2);
+            if (st != HPVCD_OK) return st;
+        }
     }
     const int slot_idx = (int)(slot - g->slots.data());
     // DPB entries this batch predicts from: wait for the stores that filled them

@@ -94,6 +94,11 @@ class GpuDecoder:
         _check(self._L.hpvcd_gpu_set_selector(self._h, mlp.handle if mlp is not None else None, arr,
                                               len(schedules)), "hpvcd_gpu_set_selector")
 
+    def set_sched(self, sched: abi.Sched | None) -> None:
+        """Schedule of the submits while no selector is set (None: the default)."""
+        _check(self._L.hpvcd_gpu_set_sched(self._h, C.byref(sched) if sched is not None else None),
+               "hpvcd_gpu_set_sched")
+
     def selector_picks(self, n: int) -> list:
         """Picks per candidate schedule so far ([K]: batches outside the domain)."""
         out = (C.c_uint64 * n)()

@@ -409,6 +409,9 @@ hpvcd_status hpvcd_gpu_read(hpvcd_gpu* ctx, hpvcd_ticket ticket, void* dst, uint
 hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* ctx, struct hpvcd_mlp* mlp, const struct hpvcd_sched* cands,
                                     uint32_t n);
 hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu* ctx, uint64_t* counts, uint32_t n);
+/* The schedule of this context's submits while no selector is set (NULL:
+ * the default, all-zero schedule). */
+hpvcd_status hpvcd_gpu_set_sched(hpvcd_gpu* ctx, const struct hpvcd_sched* sched);
 
 /* Decoded-picture buffer in HBM across submits, for video decoded frame by
  * frame (dpb.rs:79-454 and video.rs:1045-1379 keep reference pictures on the
