@@ -1413,7 +1413,8 @@ HPVCD_API hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu* g, uint64_t* counts, 
     if (!g || !counts) return HPVCD_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(g->mu);
     // counts[0 .. K-1]: picks per candidate; counts[K] (when n > K): batches
-    // outside the network's domain, which ran candidate 0
+    // outside the network's domain (features out of range, or submitted
+    // while other tickets ran), which ran the fixed schedule
     const uint32_t K = (uint32_t)g->sel_cands.size();
     for (uint32_t i = 0; i < n; ++i)
         counts[i] = i < K ? g->sel_picks[i] : (i == K ? g->sel_picks[HPVCD_MLP_MAX_VARIANTS] : 0);
@@ -1543,7 +1544,17 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     g->in_use = g->in_use - held + slot->d_in_cap + slot->plan_bytes;
     slot->held = slot->d_in_cap + slot->plan_bytes;
     if (st != HPVCD_OK) return st;
-    if (g->sel) {  // the network picks the batch's schedule from its features
+    int others = 0;  // tickets of this context already in flight
+    for (const Slot& s : g->slots)
+        if (s.busy && &s != slot) ++others;
+    // The network was trained on batches decoded alone; with other tickets in
+    // flight the batch runs the context's fixed schedule (counted with the
+    // batches outside the network's domain).
+    if (g->sel && others > 0) {
+        st = hpvcd_plan_set_sched(slot->plan, &g->fixed);
+        if (st != HPVCD_OK) return st;
+        ++g->sel_picks[HPVCD_MLP_MAX_VARIANTS];
+    } else if (g->sel) {  // the network picks the batch's schedule from its features
         // Up to kHostPickRecords records (a few ms of host work at most) the
         // features and the network run on the host, with no device round
         // trip; larger batches use the kernels and wait for their pick.  Both
@@ -1558,10 +1569,11 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
             if (st != HPVCD_OK) return st;
             pick = hpvcd_mlp_pick_host(g->sel_w.data(), (uint32_t)g->sel_cands.size(), fv, g->sel_lohi,
                                        g->sel_has_domain);
-            st = hpvcd_plan_set_sched(slot->plan, &g->sel_cands[pick == HPVCD_MLP_NO_PICK ? 0 : pick]);
+            st = hpvcd_plan_set_sched(slot->plan, pick == HPVCD_MLP_NO_PICK ? &g->fixed : &g->sel_cands[pick]);
         } else {
             st = hpvcd_plan_select(slot->plan, g->sel, g->sel_cands.data(), (uint32_t)g->sel_cands.size(),
                                    slot->stream, &pick);
+            if (st == HPVCD_OK && pick == HPVCD_MLP_NO_PICK) st = hpvcd_plan_set_sched(slot->plan, &g->fixed);
         }
         if (st != HPVCD_OK) return st;
         ++g->sel_picks[pick == HPVCD_MLP_NO_PICK ? HPVCD_MLP_MAX_VARIANTS : pick];
@@ -1576,9 +1588,6 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     // grid this is worth about 15 % of throughput; a ticket alone keeps the
     // full grid.
     {
-        int others = 0;
-        for (const Slot& s : g->slots)
-            if (s.busy && &s != slot) ++others;
         if (others > 0) {
             hpvcd_sched s2 = slot->plan->sched;
             const int occ = std::max(1, slot->plan->recon_occ);

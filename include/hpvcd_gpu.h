@@ -408,6 +408,10 @@ hpvcd_status hpvcd_gpu_read(hpvcd_gpu* ctx, hpvcd_ticket ticket, void* dst, uint
  * schedule.  n must equal the network's output count. */
 hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* ctx, struct hpvcd_mlp* mlp, const struct hpvcd_sched* cands,
                                     uint32_t n);
+/* counts[k]: batches that ran candidate k; counts[K] (n > K): batches
+ * outside the network's domain -- features out of its range, or submitted
+ * while other tickets of the context ran (it was trained on batches decoded
+ * alone) -- which ran the context's fixed schedule (hpvcd_gpu_set_sched). */
 hpvcd_status hpvcd_gpu_selector_picks(hpvcd_gpu* ctx, uint64_t* counts, uint32_t n);
 /* The schedule of this context's submits while no selector is set (NULL:
  * the default, all-zero schedule). */
