@@ -381,8 +381,11 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
         }
         return lo;
     };
-    // Residual of record t of picture P; `pair`: this lane's half of two 4x4 TBs.
-    auto one = [&](const DevPic& P, const hpvcd_tu t, bool pair) {
+    // Residual of record g; `pair`: this lane's half of two 4x4 TBs.
+    auto one = [&](uint32_t g, bool pair) {
+        const uint32_t lo = pic_of(g);
+        const DevPic& P = pics[lo];
+        const hpvcd_tu t = P.tus[g - rec_prefix[lo]];
         if (!(t.flags & HPVCD_TU_CBF)) return;
         if ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && t.comp && t.res_scale) return;  // k_ccp's
         const int c = t.comp;
@@ -421,17 +424,12 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
     // records one after the other.
     for (uint32_t g0 = rec_prefix[0] + 2 * (blockIdx.x * kResWarps + warp); g0 < total;
          g0 += 2 * gridDim.x * kResWarps) {
-        // each half reads its record once
         const uint32_t gh = g0 + (lane >> 4);
-        uint32_t lo = 0;
-        uint4 raw = make_uint4(0u, 0u, 0u, 0u);
         bool plain4 = false;
         if (gh < total) {
-            lo = pic_of(gh);
+            const uint32_t lo = pic_of(gh);
             const DevPic& P = pics[lo];
-            raw = reinterpret_cast<const uint4*>(P.tus)[gh - rec_prefix[lo]];
-            hpvcd_tu t;
-            memcpy(&t, &raw, sizeof(t));
+            const hpvcd_tu t = P.tus[gh - rec_prefix[lo]];
             const int c = t.comp;
             const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
             plain4 = (t.flags & HPVCD_TU_CBF) && t.log2n == 2 && c < (P.idc ? 3 : 1) &&
@@ -442,22 +440,9 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
         }
         const bool pair = __all_sync(0xffffffffu, plain4);
         for (int h = 0; h < (pair ? 1 : 2); ++h) {  // one call site: `one` inlines
-            // pair: every lane its own half's record; else record g0 + h for all,
-            // from the first lane of half h
-            const int src = (h << 4);
-            uint4 w = raw;
-            uint32_t l2 = lo;
-            if (!pair) {
-                w.x = __shfl_sync(0xffffffffu, raw.x, src);
-                w.y = __shfl_sync(0xffffffffu, raw.y, src);
-                w.z = __shfl_sync(0xffffffffu, raw.z, src);
-                w.w = __shfl_sync(0xffffffffu, raw.w, src);
-                l2 = __shfl_sync(0xffffffffu, lo, src);
-            }
-            if (!pair && g0 + h >= total) break;
-            hpvcd_tu t;
-            memcpy(&t, &w, sizeof(t));
-            one(pics[l2], t, pair);
+            const uint32_t g = pair ? gh : g0 + h;
+            if (g >= total) break;
+            one(g, pair);
         }
     }
 }
