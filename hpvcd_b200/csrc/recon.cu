@@ -141,12 +141,9 @@ constexpr int kResWarps = 8;
 // residual sample (row r, column m) in the reference's storage semantics.
 // `allow16` false keeps 8-bit residuals in i32 storage (the reference's
 // path for chroma TBs with cross-component prediction, decode.rs:5313-5316).
-// `pair`: two plain coded 4x4 TBs at once, lanes 0-15 one (P, t) and lanes
-// 16-31 the other (the caller passes each half its own; no transform skip,
-// bypass, I_PCM or RExt flags), every lane emitting its sample.
 template <int kIdct, typename Emit>
 __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16_t* dct, int16_t* buf,
-                                 int16_t* tmp, int lane, Emit emit, bool allow16 = true, bool pair = false) {
+                                 int16_t* tmp, int lane, Emit emit, bool allow16 = true) {
     const int n = 1 << t.log2n;
     const bool luma = t.comp == 0;
     const int bd = luma ? P.bd : P.bd_c;
@@ -248,10 +245,8 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         // as the shared-memory path, clipped after the complete sum.
         const bool dst = luma && (t.flags & HPVCD_TU_INTRA);
         const int l = lane & 15, r = l >> 2, c = l & 3;
-        const int h = lane & 16;  // first lane of this half
-        const bool mine = pair || lane < 16;
         int d = 0;
-        if (mine && c < nx) {
+        if (lane < 16 && c < nx) {
             const long long v = ((long long)lv[l] * factor_at(r, c) + add) >> bd_shift;
             d = (int)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v));
         }
@@ -269,15 +264,15 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         // stage 1: tmp[r][c] = clip((sum_k T[k][r] d[k][c] + 64) >> 7)
         int acc = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) acc += basis(k, r) * __shfl_sync(0xffffffffu, d, h + k * 4 + c);
+        for (int k = 0; k < 4; ++k) acc += basis(k, r) * __shfl_sync(0xffffffffu, d, k * 4 + c);
         const int tmp = clamp3i((acc + 64) >> 7, -32768, 32767);
         // stage 2: out[r][c] = (sum_k T[k][c] tmp[r][k] + add2) >> shift2
         const int shift2 = 20 - bd;
         int acc2 = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) acc2 += basis(k, c) * __shfl_sync(0xffffffffu, tmp, h + r * 4 + k);
+        for (int k = 0; k < 4; ++k) acc2 += basis(k, c) * __shfl_sync(0xffffffffu, tmp, r * 4 + k);
         const int v = (acc2 + (1 << (shift2 - 1))) >> shift2;
-        if (mine) emit(r, c, i16s ? (int)(int16_t)v : v);
+        if (lane < 16) emit(r, c, i16s ? (int)(int16_t)v : v);
         __syncwarp();
         return;
     }
@@ -372,30 +367,25 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t total = rec_prefix[n_pics];
-    // picture of global record g (binary search in the prefix)
-    auto pic_of = [&](uint32_t g) -> uint32_t {
+    for (uint32_t g = rec_prefix[0] + blockIdx.x * kResWarps + warp; g < total; g += gridDim.x * kResWarps) {
+        // picture of global record g (binary search in the prefix)
         uint32_t lo = 0, hi = n_pics;
         while (hi - lo > 1) {
             const uint32_t mid = (lo + hi) >> 1;
             if (rec_prefix[mid] <= g) lo = mid; else hi = mid;
         }
-        return lo;
-    };
-    // Residual of record g; `pair`: this lane's half of two 4x4 TBs.
-    auto one = [&](uint32_t g, bool pair) {
-        const uint32_t lo = pic_of(g);
         const DevPic& P = pics[lo];
         const hpvcd_tu t = P.tus[g - rec_prefix[lo]];
-        if (!(t.flags & HPVCD_TU_CBF)) return;
-        if ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && t.comp && t.res_scale) return;  // k_ccp's
+        if (!(t.flags & HPVCD_TU_CBF)) continue;
+        if ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && t.comp && t.res_scale) continue;  // k_ccp's
         const int c = t.comp;
         const int ncomp = P.idc ? 3 : 1;
         const int n = 1 << t.log2n;
         const int pw = c < 3 && c ? P.cw : P.w, ph = c < 3 && c ? P.ch : P.h;
         if (c >= ncomp || t.log2n < 2 || t.log2n > 5 || (int)t.x >= pw || (int)t.y >= ph ||
             (uint64_t)t.coeff_off + (uint64_t)n * n > P.n_coeffs) {
-            if ((lane & 15) == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
-            return;
+            if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+            continue;
         }
         const int x0 = t.x, y0 = t.y;
         const bool in_plane = (P.flags & HPVCD_PIC_PRED_IN_PLANE) || !(t.flags & HPVCD_TU_INTRA);
@@ -409,40 +399,14 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
                     const size_t idx = (size_t)y * pw + x;
                     store_sample(pl, P.bps, idx, clamp3i(keep * load_sample(pl, P.bps, idx) + v, 0, mx));
                 }
-            }, true, pair);
+            });
         } else {
             int16_t* rp = P.res[c];
             const int rs = P.res_stride[c];
             tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
                 const int x = x0 + m, y = y0 + r;
                 if (x < pw && y < ph) rp[(size_t)y * rs + x] = (int16_t)sat16(v);
-            }, true, pair);
-        }
-    };
-    // Records in pairs: two plain coded 4x4 TBs (most TBs) share one warp,
-    // half each (their transforms are independent); any other pair runs its
-    // records one after the other.
-    for (uint32_t g0 = rec_prefix[0] + 2 * (blockIdx.x * kResWarps + warp); g0 < total;
-         g0 += 2 * gridDim.x * kResWarps) {
-        const uint32_t gh = g0 + (lane >> 4);
-        bool plain4 = false;
-        if (gh < total) {
-            const uint32_t lo = pic_of(gh);
-            const DevPic& P = pics[lo];
-            const hpvcd_tu t = P.tus[gh - rec_prefix[lo]];
-            const int c = t.comp;
-            const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
-            plain4 = (t.flags & HPVCD_TU_CBF) && t.log2n == 2 && c < (P.idc ? 3 : 1) &&
-                     !(t.flags & (HPVCD_TU_TSKIP | HPVCD_TU_TQB | HPVCD_TU_PCM | HPVCD_TU_ROTATE | HPVCD_TU_RDPCM_H |
-                                  HPVCD_TU_RDPCM_V)) &&
-                     !((P.flags & HPVCD_PIC_CROSS_COMPONENT) && c && t.res_scale) && (int)t.x < pw &&
-                     (int)t.y < ph && (uint64_t)t.coeff_off + 16 <= P.n_coeffs;
-        }
-        const bool pair = __all_sync(0xffffffffu, plain4);
-        for (int h = 0; h < (pair ? 1 : 2); ++h) {  // one call site: `one` inlines
-            const uint32_t g = pair ? gh : g0 + h;
-            if (g >= total) break;
-            one(g, pair);
+            });
         }
     }
 }
