@@ -1196,13 +1196,12 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     (same(cx + 1, cy - 1) ? 8u : 0u);
         }
         // ---- wait for the neighbours (bounded), then load their edges ----
-        if (tid == 0) {
-            const int cx = it.cx, cy = it.cy;
-            const int nb[4][2] = {{cx - 1, cy}, {cx - 1, cy - 1}, {cx, cy - 1}, {cx + 1, cy - 1}};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int nx = nb[q][0], ny = nb[q][1];
-                if (nx < 0 || ny < 0 || nx >= P.ctb_cols) continue;
+        // threads 0..3 poll one neighbour each (left, above-left, above,
+        // above-right), so the four flag round trips overlap
+        if (tid < 4) {
+            const int nx = it.cx + (tid == 3 ? 1 : (tid == 2 ? 0 : -1));
+            const int ny = it.cy - (tid == 0 ? 0 : 1);
+            if (nx >= 0 && ny >= 0 && nx < P.ctb_cols) {
                 const uint32_t* f = P.ready + (size_t)ny * P.ctb_cols + nx;
                 uint32_t spins = 0;
                 while (ld_acquire(f) == 0u) {
