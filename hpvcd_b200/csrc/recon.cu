@@ -1301,32 +1301,6 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         }
         __syncthreads();
         // ---- publish the CTU (8 samples per store when rows allow) ----
-        // An inter picture's plane already holds every sample of the CTU but
-        // those of its intra TBs: only their blocks go out, a warp per TB.
-        if (P.flags & HPVCD_PIC_INTER) {
-            for (int c = 0; c < ncomp; ++c) {
-                const int S = c ? Scw : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
-                const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
-                const uint16_t* can = can_of(c);
-                const int CW = ReconLayout::cw_of(S);
-                const uint16_t* list = lists + c * kListCap;
-                for (uint32_t e = warp; e < counts[c]; e += kReconWarps) {
-                    hpvcd_tu t;
-                    memcpy(&t, &recs[list[e]], sizeof(t));
-                    const int n = 1 << t.log2n, x = (int)t.x - ox, y = (int)t.y - oy;
-                    for (int i = lane; i < n * n; i += 32) {
-                        const int yy = i >> t.log2n, xx = i & (n - 1);
-                        if (ox + x + xx < pw && oy + y + yy < ph)
-                            store_sample(P.rec[c], P.bps, (size_t)(oy + y + yy) * pw + ox + x + xx,
-                                         can[(y + yy + 1) * CW + 8 + x + xx]);
-                    }
-                }
-            }
-            __threadfence();
-            __syncthreads();
-            if (tid == 0) st_release(P.ready + ci, 1u);
-            continue;
-        }
         for (int c = 0; c < ncomp; ++c) {
             const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
             const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
