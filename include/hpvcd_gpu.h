@@ -402,10 +402,15 @@ hpvcd_status hpvcd_gpu_wait(hpvcd_gpu* ctx, hpvcd_ticket ticket, int32_t timeout
 hpvcd_status hpvcd_gpu_output_size(hpvcd_gpu* ctx, hpvcd_ticket ticket, uint64_t* bytes);
 /* Copy a finished ticket's output into caller memory and release the ticket. */
 hpvcd_status hpvcd_gpu_read(hpvcd_gpu* ctx, hpvcd_ticket ticket, void* dst, uint64_t bytes);
-/* Per-batch schedule selection for this context: every submit computes the
- * batch's features on the device, runs the selector network (a short host
- * wait for its pick) and launches the picked candidate; mlp NULL -> default
- * schedule.  n must equal the network's output count. */
+/* Per-batch schedule selection for this context: a submit that finds no
+ * other ticket in flight computes the batch's features, runs the selector
+ * network and launches the picked candidate -- on the host (hpvcd_batch_
+ * features and a host copy of the bf16 weights, no device round trip) for
+ * batches of up to 512k records, else on the device with a short host wait
+ * for the pick; the same pick either way.  Submits made while other tickets
+ * run take the fixed schedule (hpvcd_gpu_set_sched).  The weights are copied
+ * here: a network trained further needs another call.  mlp NULL -> no
+ * selection.  n must equal the network's output count. */
 hpvcd_status hpvcd_gpu_set_selector(hpvcd_gpu* ctx, struct hpvcd_mlp* mlp, const struct hpvcd_sched* cands,
                                     uint32_t n);
 /* counts[k]: batches that ran candidate k; counts[K] (n > K): batches
