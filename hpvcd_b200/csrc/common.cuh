@@ -39,7 +39,7 @@ struct DevPic {
     void* fin[3];
     int16_t* res[3];        // int16 residual planes of intra TBs (k_residual -> k_recon)
     int32_t res_stride[3];  // row stride of res[c] in samples (multiple of 16)
-    uint32_t* ready;  // per-CTU ready flags (wavefront)
+    uint32_t* ready;  // wavefront progress: 4 words per CTU, one level (0..4) per component
     // output placement on its RGB canvas
     int32_t dst_x, dst_y, crop_w, crop_h;
     uint64_t canvas_off;  // byte offset of the picture's canvas in the output

@@ -17,12 +17,17 @@
 //     CTUs are claimed from a global queue sorted by wavefront index
 //     (x + 2y) across all pictures, so a CTU is only claimed after every CTU
 //     it depends on (left, above-left, above, above-right) was claimed by a
-//     running CTA: no deadlock for any grid size.  Per CTU the residuals are
-//     prefetched with cp.async while thread 0 waits (bounded) for the
-//     neighbours; then luma, Cb and Cr are walked by three warps in parallel
-//     (chroma availability only depends on the luma `decoded` map, which
-//     each warp replays from the records), all in shared memory; finally
-//     the CTU is written out and its ready flag released.
+//     running CTA: no deadlock for any grid size.  Per CTU the residuals and
+//     records are staged with cp.async, then luma, Cb and Cr are walked by
+//     three warps in parallel (chroma availability only depends on the luma
+//     `decoded` map, which each warp replays from the records), all in
+//     shared memory.  Neighbours synchronise per component and quadrant:
+//     each walking warp releases how many quadrants of its CTU are done once
+//     their right-column / bottom-row samples are in the plane, and reads a
+//     neighbour's edge segment only when a TB on its own top or left edge
+//     needs it (waits bounded), so a CTU starts while its left and
+//     above-right neighbours are still being walked.  Finally the whole CTU
+//     is written out for the filters.
 #include <climits>
 
 #include "common.cuh"
@@ -544,7 +549,7 @@ struct ReconLayout {
         off_stamp = o; o += 256 * sizeof(uint32_t);
         off_lists = o; o += 3 * (size_t)kListCap * sizeof(uint16_t);
         o = (o + 15) & ~(size_t)15;
-        off_misc = o;  o += 16;
+        off_misc = o;  o += 128;  // claimed item, list counts, edge masks, neighbour levels
         total = o;
     }
 };
@@ -1027,13 +1032,147 @@ __device__ __forceinline__ void team_sync(int threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(kTeamBarrier), "r"(threads) : "memory");
 }
 
+// ---- wavefront progress between neighbouring CTUs ----
+// Every CTU publishes, per component, a level: how many of its quadrants
+// (z-order: top-left, top-right, bottom-left, bottom-right) are
+// reconstructed with their edge samples in the plane.  Other CTUs only read
+// a CTU's right column and bottom row, so the levels that matter are 2 (top
+// half of the right column), 3 (left half of the bottom row) and 4 (all).
+// A CTU reads seven edge segments of its neighbours, each needing one level
+// of one neighbour (0 left, 1 above-left, 2 above, 3 above-right):
+//   bit 0 above-left corner        above-left  >= 4
+//   bit 1 above row, left half      above       >= 3
+//   bit 2 above row, right half     above       >= 4
+//   bit 3 above-right, left half    above-right >= 3
+//   bit 4 above-right, right half   above-right >= 4
+//   bit 5 left column, top half     left        >= 2
+//   bit 6 left column, bottom half  left        >= 4
+constexpr int kSegs = 7;
+
+__device__ __forceinline__ int seg_nb(int s) { return s == 0 ? 1 : (s <= 2 ? 2 : (s <= 4 ? 3 : 0)); }
+__device__ __forceinline__ uint32_t seg_level(int s) { return s == 5 ? 2u : ((s == 1 || s == 3) ? 3u : 4u); }
+__device__ __forceinline__ int seg_len(int s, int S, int Sh) { return s == 0 ? 1 : (s <= 4 ? S >> 1 : Sh >> 1); }
+
+// Segments of neighbour nb readable once it has reached level v.
+__device__ __forceinline__ uint32_t segs_at(int nb, uint32_t v) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int s = 0; s < kSegs; ++s)
+        if (seg_nb(s) == nb && seg_level(s) <= v) m |= 1u << s;
+    return m;
+}
+
+// Edge segments an n x n TB at (x, y) of a component CTU S x Sh reads from
+// its neighbours: the row above spans x - 1 .. x + 2n - 1 (intra.rs:84-148),
+// the left column y - 1 .. y + 2n - 1, below-left never past the CTU.
+__device__ __forceinline__ uint32_t segs_needed(int x, int y, int n, int S, int Sh) {
+    uint32_t m = 0;
+    const int hs = S >> 1, hh = Sh >> 1;
+    if (y == 0) {
+        if (x == 0) m |= 1u;
+        const int lo = max(x - 1, 0), hi = min(x + 2 * n, S);
+        if (lo < hs) m |= 2u;
+        if (hi > hs) m |= 4u;
+        if (x + 2 * n > S) m |= 8u;
+        if (x + 2 * n > S + hs) m |= 16u;
+    }
+    if (x == 0) {
+        const int lo = max(y - 1, 0), hi = min(y + 2 * n, Sh);
+        if (lo < hh) m |= 32u;
+        if (hi > hh) m |= 64u;
+    }
+    return m;
+}
+
+// One component's neighbour edges as the canvas holds them: row 0 is the
+// row above (x = -1 at index 7, x at 8 + x), column 7 the left column.
+struct EdgeGeo {
+    void* plane;
+    uint16_t* can;
+    int ox, oy, S, Sh, pw, ph, CW;
+};
+
+// Loads the segments m[c] of components 0..ncomp-1 into their canvases,
+// thread t of nt; every load of a thread is issued before its first store.
+// Samples outside the picture read as 0 (they are never available).
+template <int kPer>
+__device__ __forceinline__ void fetch_edges(const EdgeGeo* g, const uint32_t* m, int ncomp, int bps, int t, int nt) {
+    int tot[3] = {0, 0, 0};
+    for (int c = 0; c < ncomp; ++c)
+        for (int s = 0; s < kSegs; ++s)
+            if (m[c] >> s & 1u) tot[c] += seg_len(s, g[c].S, g[c].Sh);
+    const int total = tot[0] + tot[1] + tot[2];
+    int v[kPer];
+    uint16_t* dst[kPer];
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+        const int i = t + r * nt;
+        dst[r] = nullptr;
+        v[r] = 0;
+        if (i >= total) continue;
+        int c = 0, j = i;
+        while (c < 2 && j >= tot[c]) j -= tot[c++];
+        const EdgeGeo& e = g[c];
+        int s = 0;
+        for (; s < kSegs; ++s) {
+            if (!(m[c] >> s & 1u)) continue;
+            const int L = seg_len(s, e.S, e.Sh);
+            if (j < L) break;
+            j -= L;
+        }
+        if (s >= kSegs) continue;  // unreachable: i < total
+        int dx, dy, idx;
+        if (s == 0) {
+            dx = -1, dy = -1, idx = 7;
+        } else if (s <= 4) {
+            dx = (s - 1) * (e.S >> 1) + j, dy = -1, idx = 8 + dx;
+        } else {
+            dx = -1, dy = (s - 5) * (e.Sh >> 1) + j, idx = (dy + 1) * e.CW + 7;
+        }
+        const int ax = e.ox + dx, ay = e.oy + dy;
+        if (ax >= 0 && ay >= 0 && ax < e.pw && ay < e.ph) v[r] = load_sample_cg(e.plane, bps, (size_t)ay * e.pw + ax);
+        dst[r] = e.can + idx;
+    }
+#pragma unroll
+    for (int r = 0; r < kPer; ++r)
+        if (dst[r]) *dst[r] = (uint16_t)v[r];
+}
+
+// Writes the edge samples of quadrants [from, to) of one component to the
+// plane (lanes of one warp) and releases level `to`: the warp barrier orders
+// every lane's stores before lane 0's release store, which is cumulative.
+__device__ __forceinline__ void publish_level(const EdgeGeo& e, int bps, int from, int to, uint32_t* level,
+                                              int lane) {
+    const int rows = min(e.Sh, e.ph - e.oy), cols = min(e.S, e.pw - e.ox);
+    const int hs = e.S >> 1, hh = e.Sh >> 1;
+    const bool right = cols == e.S, bottom = rows == e.Sh;  // a neighbour exists on that side
+    // right column rows [r0, r1), bottom row cols [b0, b1)
+    const int r0 = from < 2 ? 0 : hh, r1 = to >= 4 ? e.Sh : (to >= 2 ? hh : 0);
+    const int b0 = from < 3 ? 0 : hs, b1 = to >= 4 ? e.S : (to >= 3 ? hs : 0);
+    const int nr = right ? max(0, min(r1, rows) - r0) : 0;
+    const int nb = bottom ? max(0, min(b1, cols) - b0) : 0;
+    __syncwarp();
+    for (int i = lane; i < nr + nb; i += 32) {
+        int x, y;
+        if (i < nr)
+            x = e.S - 1, y = r0 + i;
+        else
+            x = b0 + i - nr, y = e.Sh - 1;
+        store_sample(e.plane, bps, (size_t)(e.oy + y) * e.pw + e.ox + x, e.can[(y + 1) * e.CW + 8 + x]);
+    }
+    __syncwarp();
+    if (lane == 0) st_release(level, (uint32_t)to);
+}
+
 // kFeat: some picture of the launch has slices / tiles, constrained intra
 // prediction, cross-component prediction or I_PCM blocks; without them the
-// availability, coded and PCM tests compile to the plain form.
+// availability, coded and PCM tests compile to the plain form.  fine: the
+// quadrant-level wavefront; otherwise a CTU waits for its neighbours' last
+// level before its walk and releases only its last level.
 template <int kTeam, bool kFeat>
 __global__ void __launch_bounds__(kReconThreads, 4)
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
-        uint32_t* work_counter, uint32_t* dev_err, int cfmt, uint32_t spin_limit) {
+        uint32_t* work_counter, uint32_t* dev_err, int cfmt, uint32_t spin_limit, int fine) {
     static_assert(kTeam == 1 || kTeam == 2, "team of one or two warps");
     extern __shared__ __align__(16) unsigned char smem[];
     const ReconLayout lay(cfmt);
@@ -1160,10 +1299,12 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         __syncthreads();
         // A CTU without intra TBs (inter pictures) has its final samples in the
         // plane already: it neither waits for its neighbours nor rewrites
-        // anything, it only releases its flag for the CTUs that predict from it.
+        // anything, it only releases every component for the CTUs that
+        // predict from it.
         const bool any_intra = counts[0] + (ncomp > 1 ? counts[1] + counts[2] : 0u) > 0u;
+        uint32_t* level = P.ready + (size_t)ci * 4;  // per-component progress of this CTU
         if (!any_intra) {
-            if (tid == 0) st_release(P.ready + ci, 1u);
+            if (tid < ncomp) st_release(level + tid, 4u);
             continue;
         }
         // Inter pictures: the plane holds motion-compensated + residual
@@ -1195,44 +1336,57 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             nb_ok = (same(cx - 1, cy) ? 1u : 0u) | (same(cx - 1, cy - 1) ? 2u : 0u) | (same(cx, cy - 1) ? 4u : 0u) |
                     (same(cx + 1, cy - 1) ? 8u : 0u);
         }
-        // ---- wait for the neighbours (bounded), then load their edges ----
-        // threads 0..3 poll one neighbour each (left, above-left, above,
-        // above-right), so the four flag round trips overlap
-        if (tid < 4) {
-            const int nx = it.cx + (tid == 3 ? 1 : (tid == 2 ? 0 : -1));
-            const int ny = it.cy - (tid == 0 ? 0 : 1);
-            if (nx >= 0 && ny >= 0 && nx < P.ctb_cols) {
-                const uint32_t* f = P.ready + (size_t)ny * P.ctb_cols + nx;
+        // ---- neighbour edges available now: one level read per neighbour
+        // and component, then every segment already released is loaded ----
+        EdgeGeo eg[3];
+        for (int c = 0; c < ncomp; ++c) {
+            eg[c].plane = P.rec[c];
+            eg[c].can = can_of(c);
+            eg[c].S = c ? Scw : ctb;
+            eg[c].Sh = c ? Sch : ctb;
+            eg[c].ox = c ? ocx : oxl;
+            eg[c].oy = c ? ocy : oyl;
+            eg[c].pw = c ? P.cw : P.w;
+            eg[c].ph = c ? P.ch : P.h;
+            eg[c].CW = ReconLayout::cw_of(eg[c].S);
+        }
+        uint32_t* s_have = (uint32_t*)(smem + lay.off_misc) + 4;
+        uint32_t* s_lvl = (uint32_t*)(smem + lay.off_misc) + 8;
+        // neighbour nb of this CTU: its level words, or null outside the picture
+        auto nb_level = [&](int nb) -> const uint32_t* {
+            const int nx = it.cx + (nb == 3 ? 1 : (nb == 2 ? 0 : -1));
+            const int ny = it.cy - (nb == 0 ? 0 : 1);
+            if (nx < 0 || ny < 0 || nx >= P.ctb_cols) return nullptr;
+            return P.ready + ((size_t)ny * P.ctb_cols + nx) * 4;
+        };
+        if (tid < 4 * ncomp) {
+            const uint32_t* f = nb_level(tid & 3);
+            uint32_t v = 4u;
+            if (f) {
+                v = ld_acquire(f + (tid >> 2));
                 uint32_t spins = 0;
-                while (ld_acquire(f) == 0u) {
+                while (!fine && v < 4u) {  // whole-CTU wavefront: wait (bounded) for the last level
                     if (++spins > spin_limit) {
                         atomicOr(dev_err, DEV_ERR_TIMEOUT);
+                        v = 4u;
                         break;
                     }
                     __nanosleep(64);
+                    v = ld_acquire(f + (tid >> 2));
                 }
             }
+            s_lvl[tid] = v;
         }
         __syncthreads();
-        for (int c = 0; c < ncomp; ++c) {
-            const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
-            const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
-            uint16_t* can = can_of(c);
-            const int CW = ReconLayout::cw_of(S);
-            for (int i = tid; i < 2 * S + 1 + Sh; i += kReconThreads) {
-                if (i < 2 * S + 1) {  // row above: x = i - 1
-                    const int ax = ox + i - 1, ay = oy - 1;
-                    int v = 0;
-                    if (ay >= 0 && ax >= 0 && ax < pw) v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * pw + ax);
-                    can[i + 7] = (uint16_t)v;
-                } else {  // column left: y = i - (2S + 1)
-                    const int y = i - (2 * S + 1);
-                    const int ax = ox - 1, ay = oy + y;
-                    int v = 0;
-                    if (ax >= 0 && ay < ph) v = load_sample_cg(P.rec[c], P.bps, (size_t)ay * pw + ax);
-                    can[(y + 1) * CW + 7] = (uint16_t)v;
-                }
-            }
+        if (tid < ncomp) {
+            uint32_t h = 0;
+            for (int nb = 0; nb < 4; ++nb) h |= segs_at(nb, s_lvl[tid * 4 + nb]);
+            s_have[tid] = h;
+        }
+        __syncthreads();
+        {
+            const uint32_t m[3] = {s_have[0], ncomp > 1 ? s_have[1] : 0u, ncomp > 1 ? s_have[2] : 0u};
+            fetch_edges<5>(eg, m, ncomp, P.bps, tid, kReconThreads);
         }
         __syncthreads();
         // ---- decode-order walk: warp c reconstructs component c ----
@@ -1266,6 +1420,9 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             k.res = res_of(c);
             const uint32_t cnt = counts[c];
             const uint16_t* list = lists + c * kListCap;
+            // edge segments in the canvas, quadrants released (the leader's)
+            uint32_t have = s_have[c];
+            int prog = 0;
             // the next record is fetched while the current TB is reconstructed
             uint32_t jn = cnt ? list[0] : 0u;
             uint4 wn = cnt ? recs[jn] : make_uint4(0u, 0u, 0u, 0u);
@@ -1278,6 +1435,49 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     wn = recs[jn];
                 }
                 const int x = (int)t.x - (c ? ocx : oxl), y = (int)t.y - (c ? ocy : oyl);
+                if (!helper) {
+                    // decode order is z-order: every quadrant before this TB's
+                    // is done, so its edge samples go out and its level is released
+                    const int q = (x >= (k.S >> 1) ? 1 : 0) + (y >= (k.Sh >> 1) ? 2 : 0);
+                    if (fine && q > prog) {
+                        if (q >= 2) publish_level(eg[c], P.bps, prog, q, level + c, lane);
+                        prog = q;
+                    }
+                    // a TB on the CTU's top or left edge reads neighbour segments
+                    const uint32_t miss = (x == 0 || y == 0) ? segs_needed(x, y, 1 << t.log2n, k.S, k.Sh) & ~have : 0u;
+                    if (miss) {
+                        // lanes 0..3 wait (bounded) for one neighbour each, then
+                        // every segment the levels seen release is loaded
+                        uint32_t lv = 0u;  // level seen (0: not polled)
+                        if (lane < 4) {
+                            uint32_t need = 0;
+                            for (int s = 0; s < kSegs; ++s)
+                                if ((miss >> s & 1u) && seg_nb(s) == lane) need = max(need, seg_level(s));
+                            const uint32_t* f = nb_level(lane);
+                            if (!f) {
+                                lv = 4u;  // outside the picture: nothing to wait for
+                            } else if (need) {
+                                uint32_t spins = 0;
+                                while ((lv = ld_acquire(f + c)) < need) {
+                                    if (++spins > spin_limit) {
+                                        atomicOr(dev_err, DEV_ERR_TIMEOUT);
+                                        lv = need;
+                                        break;
+                                    }
+                                    __nanosleep(64);
+                                }
+                            }
+                        }
+                        __syncwarp();  // orders the acquires before every lane's loads
+                        uint32_t got = 0;
+#pragma unroll
+                        for (int nb = 0; nb < 4; ++nb) got |= segs_at(nb, __shfl_sync(kFull, lv, nb));
+                        got = (got | miss) & ~have;
+                        fetch_edges<7>(&eg[c], &got, 1, P.bps, lane, 32);
+                        have |= got;
+                        __syncwarp();
+                    }
+                }
                 // a chroma TB with cross-component prediction has a residual
                 // (written by k_ccp) even without coded coefficients
                 const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
@@ -1298,9 +1498,11 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     intra_tb_big(k, t.log2n, t.mode, x, y, coded, stamp, j, ws, lane);
                 }
             }
+            if (!helper && warp < ncomp) publish_level(eg[c], P.bps, prog, 4, level + c, lane);
         }
         __syncthreads();
-        // ---- publish the CTU (8 samples per store when rows allow) ----
+        // ---- write the CTU out for the filters (8 samples per store when
+        // rows allow); the kernel boundary orders it before them ----
         for (int c = 0; c < ncomp; ++c) {
             const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
             const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
@@ -1330,9 +1532,6 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 }
             }
         }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) st_release(P.ready + ci, 1u);
     }
 }
 
@@ -1370,7 +1569,7 @@ extern "C" cudaError_t hpvcd_launch_ccp(const hpvcd::DevPic* pics, const uint32_
 
 extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd::CtuItem* items,
                                           uint32_t n_items, uint32_t* work_counter, uint32_t* dev_err,
-                                          int cfmt, int grid, int team, int feat, cudaStream_t stream) {
+                                          int cfmt, int grid, int team, int feat, int fine, cudaStream_t stream) {
     if (n_items == 0) return cudaSuccess;
     // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
     // when the plan was built (no non-stream API call here, so launches can
@@ -1380,16 +1579,16 @@ extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd
     const uint32_t spin = 1u << 22;
     if (team == 2 && feat)
         hpvcd::k_recon<2, true><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                              dev_err, cfmt, spin);
+                                                                              dev_err, cfmt, spin, fine);
     else if (team == 2)
         hpvcd::k_recon<2, false><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                               dev_err, cfmt, spin);
+                                                                               dev_err, cfmt, spin, fine);
     else if (feat)
         hpvcd::k_recon<1, true><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                              dev_err, cfmt, spin);
+                                                                              dev_err, cfmt, spin, fine);
     else
         hpvcd::k_recon<1, false><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                               dev_err, cfmt, spin);
+                                                                               dev_err, cfmt, spin, fine);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }

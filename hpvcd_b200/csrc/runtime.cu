@@ -23,7 +23,7 @@ extern "C" cudaError_t hpvcd_launch_residual(const DevPic*, const uint32_t*, uin
 extern "C" cudaError_t hpvcd_launch_ccp(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int,
                                         cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int, int,
-                                          int, int, cudaStream_t);
+                                          int, int, int, cudaStream_t);
 extern "C" int hpvcd_recon_occupancy(int cfmt);
 extern "C" hpvcd_status hpvcd_mlp_host_copy(hpvcd_mlp* M, float* params, float* lohi, int* has_domain);
 extern "C" uint32_t hpvcd_mlp_pick_host(const float* w, uint32_t K, const float* x, const float* lohi,
@@ -181,7 +181,7 @@ struct hpvcd_plan {
     std::vector<uint32_t> rec_prefix;  // TB records of pictures [0, i)
     uint32_t* d_prefix = nullptr;
     unsigned char* d_res = nullptr;    // int16 residual planes
-    uint32_t* d_scratch = nullptr;  // [seg counters][err][ready flags...]
+    uint32_t* d_scratch = nullptr;  // [seg counters][err][progress words...]
     size_t scratch_words = 0;
     unsigned char* d_planes = nullptr;
     size_t plane_bytes = 0;
@@ -481,7 +481,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             fin_off[i] = rec_off[i];
         }
         ready_off[i] = ready_words;
-        ready_words += (size_t)g.ctb_cols * g.ctb_rows;
+        ready_words += (size_t)4 * g.ctb_cols * g.ctb_rows;  // one progress word per component
     }
     // segments: all pictures at once, or one per picture when any picture
     // predicts from another (its references must be final first).
@@ -720,7 +720,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
 
 hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
     cudaError_t e = cudaSuccess;
-    // Work counters, the device error word and the wavefront ready flags are
+    // Work counters, the device error word and the wavefront progress words are
     // reset by every launch that reconstructs.
     if (stages & HPVCD_STAGE_RECON) {
         e = cudaMemsetAsync(P->d_scratch, 0, P->scratch_words * sizeof(uint32_t), st);
@@ -772,7 +772,8 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             const int share = P->concurrent ? std::max(1, P->sms * occ / (int)n_seg) : P->sms * occ;
             const int grid = std::max(1, std::min<int>(share, (int)s.n_items));
             e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
-                                   P->cfmt, grid, (int)P->sched.luma_team, P->recon_feat ? 1 : 0, st);
+                                   P->cfmt, grid, (int)P->sched.luma_team, P->recon_feat ? 1 : 0,
+                                   P->sched.wave ? 0 : 1, st);
             if (e != cudaSuccess) return cuda_status(e);
         }
         if (stages & HPVCD_STAGE_DEBLOCK) {
@@ -1221,7 +1222,7 @@ HPVCD_API hpvcd_status hpvcd_plan_autotune(hpvcd_plan* plan, const hpvcd_sched* 
 HPVCD_API hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched) {
     if (!plan) return HPVCD_ERR_INVALID_ARG;
     const hpvcd_sched next = sched ? *sched : hpvcd_sched{};
-    if (next.idct > 1 || next.luma_team > 2) return HPVCD_ERR_INVALID_ARG;
+    if (next.idct > 1 || next.luma_team > 2 || next.wave > 1) return HPVCD_ERR_INVALID_ARG;
     if (std::memcmp(&next, &plan->sched, sizeof(next)) == 0) return HPVCD_OK;
     plan->sched = next;
     // graphs captured with the previous schedule hold its kernels
@@ -1584,9 +1585,11 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     // Tickets already in flight share the SMs with this one: the wavefront
     // kernel's persistent grid keeps to its share of the CTA slots (its CTAs
     // wait for their neighbour CTUs in place, holding slots the other
-    // tickets' kernels need).  At three tickets in flight on the 4032x3024
-    // grid this is worth about 15 % of throughput; a ticket alone keeps the
-    // full grid.
+    // tickets' kernels need), and it waits for whole neighbour CTUs: with the
+    // SMs busy, starting a CTU early only trades its slot for mid-walk polls.
+    // At three tickets in flight on the 4032x3024 grid the share is worth
+    // about 15 % of throughput; a ticket alone keeps the full grid and the
+    // quadrant-level wavefront, which shortens its critical path.
     {
         if (others > 0) {
             hpvcd_sched s2 = slot->plan->sched;
@@ -1594,6 +1597,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
             const int share = std::max(1, occ / (others + 1));
             const int cur = s2.recon_ctas_per_sm ? (int)s2.recon_ctas_per_sm : occ;
             s2.recon_ctas_per_sm = (uint32_t)std::min(cur, share);
+            s2.wave = 1;
             st = hpvcd_plan_set_sched(slot->plan, &s2);
             if (st != HPVCD_OK) return st;
         }
@@ -1720,7 +1724,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_read(hpvcd_gpu* g, hpvcd_ticket t, void* dst, u
 // synchronise the device and stall unrelated streams.  For them the scratch of
 // one picture's decode lives in one fixed array of module global memory,
 // reserved when the module loads: work counter, device error word, wavefront
-// ready flags, the device picture record, the CTU work list, the int16
+// wavefront progress words, the device picture record, the CTU work list, the int16
 // residual planes and, when SAO runs, the pre-SAO planes.  The caller owns the
 // inputs (device buffers) and the output planes.
 //
@@ -1750,7 +1754,7 @@ std::mutex g_noalloc_mu;
 NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
 
 // Byte offsets inside the scratch array.  Word 0 is the work counter, word 1
-// the device error word; the ready flags follow at byte 256.
+// the device error word; the progress words follow at byte 256.
 struct NoAllocLayout {
     uint64_t ready, pic, prefix, items, res, snap, need;
 };
@@ -1759,7 +1763,7 @@ NoAllocLayout noalloc_layout(const hpvcd_picture& p, const Geo& g) {
     NoAllocLayout L;
     const uint64_t n_ctu = (uint64_t)g.ctb_cols * g.ctb_rows;
     L.ready = 256;
-    L.pic = align_up(L.ready + n_ctu * 4, 256);
+    L.pic = align_up(L.ready + n_ctu * 16, 256);  // four progress words per CTU
     L.prefix = align_up(L.pic + sizeof(DevPic), 256);
     L.items = L.prefix + 256;
     L.res = align_up(L.items + n_ctu * sizeof(CtuItem), 256);
@@ -1790,7 +1794,7 @@ hpvcd_status noalloc_setup(int dev, NoAllocDevice** out) {
     return HPVCD_OK;
 }
 
-// Zero the counter, error word and ready flags; store the picture record and
+// Zero the counter, error word and progress words; store the picture record and
 // the TB-record prefix; write the CTU work list in wavefront order (sorted by
 // t = x + 2y, then y), the order in which every CTU's left, above-left, above
 // and above-right neighbours come earlier.
@@ -1809,7 +1813,7 @@ __global__ void k_noalloc_setup(DevPic pic, uint32_t n_tus, unsigned char* base,
         prefix[1] = n_tus;
     }
     for (int i = tid; i < n_ctu; i += gridDim.x * blockDim.x) {
-        ready[i] = 0u;
+        for (int c = 0; c < 4; ++c) ready[(size_t)i * 4 + c] = 0u;
         if (!list) continue;
         const int x = i % cols, y = i / cols, t = x + 2 * y;
         uint32_t rank = 0;
@@ -1926,7 +1930,7 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
         e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, cfmt, grid, 1,
                                (p.ctb_region || (p.flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT |
                                                            HPVCD_PIC_PCM))) ? 1 : 0,
-                               st);
+                               1, st);
         if (e != cudaSuccess) return cuda_status(e);
     }
     const int lv = (d.w >= 12 ? (d.w - 4) / 8 : 0) * (d.h / 4);

@@ -467,7 +467,9 @@ typedef struct hpvcd_sched {
                                    rows / columns skipped, 1 even-odd butterflies for 16x16 / 32x32 */
     uint32_t luma_team;         /* warps predicting a 16x16 / 32x32 luma intra TB: 0|1 one, 2 two */
     uint32_t recon_ctas_per_sm; /* persistent wavefront CTAs per SM (0 -> occupancy max) */
-    uint32_t rsvd;              /* zero */
+    uint32_t wave;              /* wavefront synchronisation: 0 per quadrant (a CTU is walked while
+                                   its left / above-right neighbours still are), 1 whole CTUs (one
+                                   wait per CTU: fewer polls when tickets share the SMs) */
 } hpvcd_sched;
 
 hpvcd_status hpvcd_plan_create(const hpvcd_picture* dev_pics, uint32_t n,

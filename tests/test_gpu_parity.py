@@ -395,11 +395,14 @@ def test_schedule_variants_bit_exact():
     for idct in (0, 1):
         for team in (1, 2):
             for ctas in (0, 1):
-                plan.set_sched(abi.Sched(idct, team, ctas, 0))
-                plan.launch()
-                assert plan.status() == abi.OK
-                got = [plan.planes(i) for i in range(len(pics))]
-                assert_planes_equal(got, ref, f"idct={idct} team={team} ctas={ctas}")
+                for wave in (0, 1):   # quadrant-level / whole-CTU wavefront
+                    plan.set_sched(abi.Sched(idct, team, ctas, wave))
+                    plan.launch()
+                    assert plan.status() == abi.OK
+                    got = [plan.planes(i) for i in range(len(pics))]
+                    assert_planes_equal(got, ref, f"idct={idct} team={team} ctas={ctas} wave={wave}")
+    with pytest.raises(abi.HpvcdError):
+        plan.set_sched(abi.Sched(0, 1, 0, 2))
     plan.close()
 
 
@@ -411,7 +414,7 @@ def test_schedule_variants_inter_bit_exact():
     pics = s.pictures()
     ref, _ = O.decode_batch(pics)
     plan = DevicePlan(pics)
-    for sched in (abi.Sched(1, 2, 0, 0), abi.Sched(1, 1, 1, 0), abi.Sched(0, 2, 0, 0)):
+    for sched in (abi.Sched(1, 2, 0, 0), abi.Sched(1, 1, 1, 0), abi.Sched(0, 2, 0, 0), abi.Sched(1, 2, 0, 1)):
         plan.set_sched(sched)
         plan.launch()
         assert plan.status() == abi.OK
