@@ -525,6 +525,8 @@ constexpr int kRecCap420 = 256 + 64 + 2 * 64;
 constexpr int kRecCap422 = 256 + 64 + 2 * 128;
 constexpr int kRecCap444 = 256 + 64 + 2 * 256;
 constexpr int kListCap = 256;  // intra TBs of one component in one CTU
+// list entry: record index (< 1024) | kListEvent for a wavefront event
+constexpr uint32_t kListRec = 0x3ffu, kListEvent = 0x8000u;
 constexpr uint32_t kNoStamp = 0xffffffffu;
 
 struct ReconLayout {
@@ -1048,6 +1050,7 @@ __device__ __forceinline__ void team_sync(int threads) {
 //   bit 5 left column, top half     left        >= 2
 //   bit 6 left column, bottom half  left        >= 4
 constexpr int kSegs = 7;
+constexpr uint32_t kSegMask = (1u << kSegs) - 1u;
 
 __device__ __forceinline__ int seg_nb(int s) { return s == 0 ? 1 : (s <= 2 ? 2 : (s <= 4 ? 3 : 0)); }
 __device__ __forceinline__ uint32_t seg_level(int s) { return s == 5 ? 2u : ((s == 1 || s == 3) ? 3u : 4u); }
@@ -1092,50 +1095,43 @@ struct EdgeGeo {
     int ox, oy, S, Sh, pw, ph, CW;
 };
 
-// Loads the segments m[c] of components 0..ncomp-1 into their canvases,
-// thread t of nt; every load of a thread is issued before its first store.
-// Samples outside the picture read as 0 (they are never available).
+// Loads the segments m of one component into its canvas, thread t of nt;
+// every load of a thread is issued before its first store.  Samples outside
+// the picture read as 0 (they are never available).
 template <int kPer>
-__device__ __forceinline__ void fetch_edges(const EdgeGeo* g, const uint32_t* m, int ncomp, int bps, int t, int nt) {
-    int tot[3] = {0, 0, 0};
-    for (int c = 0; c < ncomp; ++c)
-        for (int s = 0; s < kSegs; ++s)
-            if (m[c] >> s & 1u) tot[c] += seg_len(s, g[c].S, g[c].Sh);
-    const int total = tot[0] + tot[1] + tot[2];
-    int v[kPer];
-    uint16_t* dst[kPer];
+__device__ __forceinline__ void fetch_edges(const EdgeGeo& e, uint32_t m, int bps, int t, int nt) {
+    int total = 0;
+    for (int s = 0; s < kSegs; ++s)
+        if (m >> s & 1u) total += seg_len(s, e.S, e.Sh);
+    int v[kPer], dst[kPer];
 #pragma unroll
     for (int r = 0; r < kPer; ++r) {
         const int i = t + r * nt;
-        dst[r] = nullptr;
+        dst[r] = -1;
         v[r] = 0;
         if (i >= total) continue;
-        int c = 0, j = i;
-        while (c < 2 && j >= tot[c]) j -= tot[c++];
-        const EdgeGeo& e = g[c];
-        int s = 0;
+        int j = i, s = 0;
         for (; s < kSegs; ++s) {
-            if (!(m[c] >> s & 1u)) continue;
+            if (!(m >> s & 1u)) continue;
             const int L = seg_len(s, e.S, e.Sh);
             if (j < L) break;
             j -= L;
         }
         if (s >= kSegs) continue;  // unreachable: i < total
-        int dx, dy, idx;
+        int dx, dy;
         if (s == 0) {
-            dx = -1, dy = -1, idx = 7;
+            dx = -1, dy = -1, dst[r] = 7;
         } else if (s <= 4) {
-            dx = (s - 1) * (e.S >> 1) + j, dy = -1, idx = 8 + dx;
+            dx = (s - 1) * (e.S >> 1) + j, dy = -1, dst[r] = 8 + dx;
         } else {
-            dx = -1, dy = (s - 5) * (e.Sh >> 1) + j, idx = (dy + 1) * e.CW + 7;
+            dx = -1, dy = (s - 5) * (e.Sh >> 1) + j, dst[r] = (dy + 1) * e.CW + 7;
         }
         const int ax = e.ox + dx, ay = e.oy + dy;
         if (ax >= 0 && ay >= 0 && ax < e.pw && ay < e.ph) v[r] = load_sample_cg(e.plane, bps, (size_t)ay * e.pw + ax);
-        dst[r] = e.can + idx;
     }
 #pragma unroll
     for (int r = 0; r < kPer; ++r)
-        if (dst[r]) *dst[r] = (uint16_t)v[r];
+        if (dst[r] >= 0) e.can[dst[r]] = (uint16_t)v[r];
 }
 
 // Writes the edge samples of quadrants [from, to) of one component to the
@@ -1162,6 +1158,75 @@ __device__ __forceinline__ void publish_level(const EdgeGeo& e, int bps, int fro
     }
     __syncwarp();
     if (lane == 0) st_release(level, (uint32_t)to);
+}
+
+// Edge geometry of component c of CTU (cx, cy) of picture P.
+__device__ __forceinline__ EdgeGeo edge_geo(const DevPic& P, uint16_t* can, int c, int cx, int cy) {
+    const int ctb = 1 << P.log2_ctb;
+    EdgeGeo e;
+    e.plane = P.rec[c];
+    e.can = can;
+    e.S = c ? ctb / P.sub_w : ctb;
+    e.Sh = c ? ctb / P.sub_h : ctb;
+    e.ox = cx * e.S;
+    e.oy = cy * e.Sh;
+    e.pw = c ? P.cw : P.w;
+    e.ph = c ? P.ch : P.h;
+    e.CW = ReconLayout::cw_of(e.S);
+    return e;
+}
+
+// The walk's rare step, taken only by TBs flagged when the lists were built
+// (a per-TB test in the loop itself costs the walk about 10 %): release the
+// quadrants before this TB's (edge samples of quadrants from `prog` on go to
+// the plane), then make sure the canvas holds every neighbour segment the
+// n x n TB at (x, y) reads: with a courier warp (s_have_c) by waiting for its
+// bits, else lanes 0..3 wait (bounded) for one neighbour each and the warp
+// loads every segment the levels seen release.  Returns segments held |
+// (quadrants done << 8).
+__device__ __forceinline__ uint32_t walk_event(const DevPic& P, uint16_t* can, int c, int cx, int cy, int x, int y,
+                                            int n, int prog, uint32_t have, uint32_t spin_limit, uint32_t* dev_err,
+                                            int lane) {
+    const EdgeGeo e = edge_geo(P, can, c, cx, cy);
+    const int q = (x >= (e.S >> 1) ? 1 : 0) + (y >= (e.Sh >> 1) ? 2 : 0);
+    if (q > prog) {
+        if (q >= 2) publish_level(e, P.bps, prog, q, P.ready + ((size_t)cy * P.ctb_cols + cx) * 4 + c, lane);
+        prog = q;
+    }
+    const uint32_t miss = (x == 0 || y == 0) ? segs_needed(x, y, n, e.S, e.Sh) & ~have : 0u;
+    if (miss) {
+        uint32_t lv = 0u;  // level seen (0: not polled)
+        if (lane < 4) {
+            uint32_t need = 0;
+            for (int s = 0; s < kSegs; ++s)
+                if ((miss >> s & 1u) && seg_nb(s) == lane) need = max(need, seg_level(s));
+            const int nx = cx + (lane == 3 ? 1 : (lane == 2 ? 0 : -1));
+            const int ny = cy - (lane == 0 ? 0 : 1);
+            if (nx < 0 || ny < 0 || nx >= P.ctb_cols) {
+                lv = 4u;  // outside the picture: nothing to wait for
+            } else if (need) {
+                const uint32_t* f = P.ready + ((size_t)ny * P.ctb_cols + nx) * 4 + c;
+                uint32_t spins = 0;
+                while ((lv = ld_acquire(f)) < need) {
+                    if (++spins > spin_limit) {
+                        atomicOr(dev_err, DEV_ERR_TIMEOUT);
+                        lv = need;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __syncwarp();  // orders the acquires before every lane's loads
+        uint32_t got = 0;
+#pragma unroll
+        for (int nb = 0; nb < 4; ++nb) got |= segs_at(nb, __shfl_sync(kFull, lv, nb));
+        got = (got | miss) & ~have;
+        fetch_edges<7>(e, got, P.bps, lane, 32);
+        have |= got;
+        __syncwarp();
+    }
+    return have | ((uint32_t)prog << 8);
 }
 
 // kFeat: some picture of the launch has slices / tiles, constrained intra
@@ -1270,24 +1335,45 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         }
         if (warp < ncomp) {
             const int c = warp;
+            const int hs = (c ? Scw : ctb) >> 1, hh = (c ? Sch : ctb) >> 1;
             uint32_t cnt = 0;
+            int qmax = 0;  // quadrant of the entries listed so far (z-order: never decreases)
             for (uint32_t base = 0; base < nrec; base += 32) {
                 const uint32_t i = base + lane;
                 bool mine = false;
+                int q = -1;
+                bool edge = false;
                 if (i < nrec) {
                     hpvcd_tu t;
                     memcpy(&t, &recs[i], sizeof(t));
                     int x, y;
                     if (t.comp == c && (t.flags & HPVCD_TU_INTRA) && intra_pred_ok && rec_check(t, x, y) == 1) {
-                        if (t.mode > 34 || t.log2n > 5)
+                        if (t.mode > 34 || t.log2n > 5) {
                             atomicOr(dev_err, DEV_ERR_BITSTREAM);
-                        else
+                        } else {
                             mine = true;
+                            q = (x >= hs ? 1 : 0) + (y >= hh ? 2 : 0);
+                            edge = x == 0 || y == 0;
+                        }
                     }
                 }
+                // running maximum of q over the list order: an entry that opens
+                // a later quadrant, or sits on the CTU's top / left edge, is an
+                // event of the quadrant-level wavefront
+                int run = q;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int o = __shfl_up_sync(kFull, run, d);
+                    if (lane >= d) run = max(run, o);
+                }
+                int before = __shfl_up_sync(kFull, run, 1);
+                before = max(lane ? before : -1, qmax);
+                qmax = max(qmax, __shfl_sync(kFull, run, 31));
+                const bool event = fine && (q > before || edge);
                 const uint32_t m = __ballot_sync(kFull, mine);
                 const uint32_t pos = cnt + __popc(m & ((1u << lane) - 1u));
-                if (mine && pos < (uint32_t)kListCap) lists[c * kListCap + pos] = (uint16_t)i;
+                if (mine && pos < (uint32_t)kListCap)
+                    lists[c * kListCap + pos] = (uint16_t)(i | (event ? kListEvent : 0u));
                 cnt += __popc(m);
             }
             if (cnt > (uint32_t)kListCap) {
@@ -1338,18 +1424,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         }
         // ---- neighbour edges available now: one level read per neighbour
         // and component, then every segment already released is loaded ----
-        EdgeGeo eg[3];
-        for (int c = 0; c < ncomp; ++c) {
-            eg[c].plane = P.rec[c];
-            eg[c].can = can_of(c);
-            eg[c].S = c ? Scw : ctb;
-            eg[c].Sh = c ? Sch : ctb;
-            eg[c].ox = c ? ocx : oxl;
-            eg[c].oy = c ? ocy : oyl;
-            eg[c].pw = c ? P.cw : P.w;
-            eg[c].ph = c ? P.ch : P.h;
-            eg[c].CW = ReconLayout::cw_of(eg[c].S);
-        }
+        auto geo = [&](int c) { return edge_geo(P, can_of(c), c, it.cx, it.cy); };
         uint32_t* s_have = (uint32_t*)(smem + lay.off_misc) + 4;
         uint32_t* s_lvl = (uint32_t*)(smem + lay.off_misc) + 8;
         // neighbour nb of this CTU: its level words, or null outside the picture
@@ -1384,10 +1459,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             s_have[tid] = h;
         }
         __syncthreads();
-        {
-            const uint32_t m[3] = {s_have[0], ncomp > 1 ? s_have[1] : 0u, ncomp > 1 ? s_have[2] : 0u};
-            fetch_edges<5>(eg, m, ncomp, P.bps, tid, kReconThreads);
-        }
+        for (int c = 0; c < ncomp; ++c) fetch_edges<2>(geo(c), s_have[c], P.bps, tid, kReconThreads);
         __syncthreads();
         // ---- decode-order walk: warp c reconstructs component c ----
         const bool helper = kTeam > 1 && warp == kReconWarps - 1;
@@ -1425,58 +1497,22 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             int prog = 0;
             // the next record is fetched while the current TB is reconstructed
             uint32_t jn = cnt ? list[0] : 0u;
-            uint4 wn = cnt ? recs[jn] : make_uint4(0u, 0u, 0u, 0u);
+            uint4 wn = cnt ? recs[jn & kListRec] : make_uint4(0u, 0u, 0u, 0u);
             for (uint32_t e = 0; e < cnt; ++e) {
-                const uint32_t j = jn;
+                const uint32_t j = jn & kListRec;
+                const bool event = (jn & kListEvent) != 0u;
                 hpvcd_tu t;
                 memcpy(&t, &wn, sizeof(t));
                 if (e + 1 < cnt) {
                     jn = list[e + 1];
-                    wn = recs[jn];
+                    wn = recs[jn & kListRec];
                 }
                 const int x = (int)t.x - (c ? ocx : oxl), y = (int)t.y - (c ? ocy : oyl);
-                if (!helper) {
-                    // decode order is z-order: every quadrant before this TB's
-                    // is done, so its edge samples go out and its level is released
-                    const int q = (x >= (k.S >> 1) ? 1 : 0) + (y >= (k.Sh >> 1) ? 2 : 0);
-                    if (fine && q > prog) {
-                        if (q >= 2) publish_level(eg[c], P.bps, prog, q, level + c, lane);
-                        prog = q;
-                    }
-                    // a TB on the CTU's top or left edge reads neighbour segments
-                    const uint32_t miss = (x == 0 || y == 0) ? segs_needed(x, y, 1 << t.log2n, k.S, k.Sh) & ~have : 0u;
-                    if (miss) {
-                        // lanes 0..3 wait (bounded) for one neighbour each, then
-                        // every segment the levels seen release is loaded
-                        uint32_t lv = 0u;  // level seen (0: not polled)
-                        if (lane < 4) {
-                            uint32_t need = 0;
-                            for (int s = 0; s < kSegs; ++s)
-                                if ((miss >> s & 1u) && seg_nb(s) == lane) need = max(need, seg_level(s));
-                            const uint32_t* f = nb_level(lane);
-                            if (!f) {
-                                lv = 4u;  // outside the picture: nothing to wait for
-                            } else if (need) {
-                                uint32_t spins = 0;
-                                while ((lv = ld_acquire(f + c)) < need) {
-                                    if (++spins > spin_limit) {
-                                        atomicOr(dev_err, DEV_ERR_TIMEOUT);
-                                        lv = need;
-                                        break;
-                                    }
-                                    __nanosleep(64);
-                                }
-                            }
-                        }
-                        __syncwarp();  // orders the acquires before every lane's loads
-                        uint32_t got = 0;
-#pragma unroll
-                        for (int nb = 0; nb < 4; ++nb) got |= segs_at(nb, __shfl_sync(kFull, lv, nb));
-                        got = (got | miss) & ~have;
-                        fetch_edges<7>(&eg[c], &got, 1, P.bps, lane, 32);
-                        have |= got;
-                        __syncwarp();
-                    }
+                if (event && !helper) {
+                    const uint32_t r = walk_event(P, k.can, c, it.cx, it.cy, x, y, 1 << t.log2n, prog, have, spin_limit,
+                                                  dev_err, lane);
+                    have = r & kSegMask;
+                    prog = (int)(r >> 8);
                 }
                 // a chroma TB with cross-component prediction has a residual
                 // (written by k_ccp) even without coded coefficients
@@ -1498,7 +1534,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     intra_tb_big(k, t.log2n, t.mode, x, y, coded, stamp, j, ws, lane);
                 }
             }
-            if (!helper && warp < ncomp) publish_level(eg[c], P.bps, prog, 4, level + c, lane);
+            if (!helper && warp < ncomp) publish_level(geo(c), P.bps, prog, 4, level + c, lane);
         }
         __syncthreads();
         // ---- write the CTU out for the filters (8 samples per store when
