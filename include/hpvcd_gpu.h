@@ -444,7 +444,8 @@ hpvcd_status hpvcd_gpu_set_dpb(hpvcd_gpu* ctx, hpvcd_dpb* dpb);
 /* ------------------------------------------------------------------------ */
 /* Device-buffer API (plans).  The picture descriptors point at device      */
 /* memory that stays valid while the plan lives.  A plan owns its own        */
-/* device scratch (work queues, ready flags, ping-pong planes) and output.   */
+/* device scratch (work queues, wavefront progress words, ping-pong        */
+/* planes) and output.                                                     */
 /* hpvcd_plan_launch only enqueues kernels on `stream` (no allocation, no    */
 /* synchronisation), so it can be captured into a CUDA graph.               */
 /* ------------------------------------------------------------------------ */
@@ -587,9 +588,9 @@ hpvcd_status hpvcd_plan_select(hpvcd_plan* plan, hpvcd_mlp* mlp, const hpvcd_sch
  * unused for 4:0:0), each 256-byte aligned, unpadded (luma stride = width *
  * bytes per sample, as hpvcd_plan_planes).  Enqueues its kernels on `stream`
  * and returns; allocates no memory of any kind.  Its scratch (work counter,
- * error word, wavefront ready flags, picture record, CTU list, residual and
+ * error word, wavefront progress words, picture record, CTU list, residual and
  * pre-SAO planes) is one fixed array in the library's device memory; the
- * call itself zeroes the counter, error word and ready flags on `stream`
+ * call itself zeroes the counter, error word and progress words on `stream`
  * before use, and nothing else needs to start at zero.
  *   - The first call on a device does the set-up (looks up the array's
  *     address, sets the kernel's shared-memory limit) with that device
