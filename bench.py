@@ -53,6 +53,8 @@ def parse_args():
                          "submits that find no other ticket in flight), or 'fixed:K' (candidate K of the "
                          "selector's list); the network and the default schedule are reported beside each other")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--coeff16", action="store_true",
+                    help="keep every tile's int16 level pool (default: int8 pools where every level fits)")
     ap.add_argument("--workload", choices=["grid", "serving", "selector", "inter"], default="grid",
                     help="grid: the 4032x3024 still (default); serving: mixed-size batched serving; "
                          "selector: learned schedule selection on 3840x2160 frames; inter: 1080p GOP")
@@ -280,6 +282,9 @@ def run_ours(args):
     g = synth.config1_grid(seed=rank)
     out, keep = synth.grid_output(g)
     pics = g.synth.pictures()
+    # host transport choice: tiles whose levels all fit in int8 ship an int8
+    # pool (half the bytes over PCIe); the pixels are the same
+    c8keep = [] if args.coeff16 else synth.narrow_coeffs(pics)
     plan = DevicePlan(pics, out, device=local)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
@@ -361,13 +366,14 @@ def run_ours(args):
     lat = sorted(step_ms)
 
     # Roofline of the dominant kernel (the reconstruction kernel): algorithmic
-    # bytes per launch = dense int16 levels of the coded TBs + TB records +
-    # CTU index + the reconstructed samples written once.
-    n_coeffs = sum(p.n_coeffs for p in pics)
+    # bytes per launch = dense levels of the coded TBs (int16, or int8 in a
+    # narrowed pool) + TB records + CTU index + the reconstructed samples
+    # written once.
+    coeff_bytes = sum(p.n_coeffs * (1 if p.flags & abi.PIC_COEFF8 else 2) for p in pics)
     n_tus = sum(p.n_tus for p in pics)
     ctus = sum(synth.geometry(p)["ctb_cols"] * synth.geometry(p)["ctb_rows"] + 1 for p in pics)
     written = sum(p.width * p.height * 3 // 2 * synth.geometry(p)["bytes_per_sample"] for p in pics)
-    recon_bytes = n_coeffs * 2 + n_tus * 16 + ctus * 4 + written
+    recon_bytes = coeff_bytes + n_tus * 16 + ctus * 4 + written
     peak, peak_kind = measured_peaks()
     recon_s = stage_ms[0] / 1e3
     achieved = recon_bytes / recon_s / 1e9
@@ -409,6 +415,7 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "tiles": 48, "tile": "512x512 (edge tiles cropped)",
                    "out": f"{OUT_W}x{OUT_H} RGB8 BT.601 full range", "bit_depth": 10, "chroma": "4:2:0",
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
+                   "levels": f"int8 pools for {len(c8keep)} of {len(pics)} tiles (every level fits), else int16",
                    "inputs": "seeded synthetic flat buffers (CU/TU quadtrees, modes, QP 22-37, "
                              "85% zero levels, Laplacian(8), deblock on, random SAO)"},
         "latency_ms": {"p50": round(lat[len(lat) // 2], 4),

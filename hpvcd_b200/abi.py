@@ -59,6 +59,7 @@ PIC_SAO_NO_ACROSS_SLICES = 0x0100
 PIC_SAO_NO_ACROSS_TILES = 0x0200
 PIC_CONSTRAINED_INTRA = 0x0400
 PIC_PCM = 0x0800
+PIC_COEFF8 = 0x1000
 PIC_STORE_MASK = 0x00FF0000
 
 

@@ -153,12 +153,16 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
     const bool luma = t.comp == 0;
     const int bd = luma ? P.bd : P.bd_c;
     const bool i16s = bd <= 8 && allow16;
-    const int16_t* lv = P.coeffs + t.coeff_off;
+    // levels: int16, or int8 when the host narrowed the picture's pool
+    const bool c8 = (P.flags & HPVCD_PIC_COEFF8) != 0;
+    const int16_t* lv16 = P.coeffs + t.coeff_off;
+    const int8_t* lv8 = (const int8_t*)P.coeffs + t.coeff_off;
+    auto lv = [&](int i) -> int { return c8 ? (int)lv8[i] : (int)lv16[i]; };
     const uint32_t rext = t.flags & (HPVCD_TU_ROTATE | HPVCD_TU_RDPCM_H | HPVCD_TU_RDPCM_V);
     // decode.rs:4754-4757 / :4830-4834: residual = levels (transquant bypass);
     // an I_PCM record's levels are its samples (decode.rs:2768-2839)
     if ((t.flags & (HPVCD_TU_TQB | HPVCD_TU_PCM)) && !rext) {
-        for (int i = lane; i < n * n; i += 32) emit(i / n, i % n, (int)lv[i]);
+        for (int i = lane; i < n * n; i += 32) emit(i / n, i % n, (int)lv(i));
         return;
     }
     int qpp;
@@ -206,9 +210,9 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         for (int i = lane; i < n * n; i += 32) {
             int r;
             if (t.flags & HPVCD_TU_TQB) {
-                r = lv[i];
+                r = lv(i);
             } else {
-                long long v = ((long long)lv[i] * factor_at(i / n, i % n) + add) >> bd_shift;
+                long long v = ((long long)lv(i) * factor_at(i / n, i % n) + add) >> bd_shift;
                 v = v < -32768 ? -32768 : (v > 32767 ? 32767 : v);
                 r = tr_shift >= 0 ? ((int)v + tr_add) >> tr_shift : (int)((unsigned)v << (-tr_shift));
             }
@@ -236,7 +240,7 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         const int tr_shift = 15 - bd - t.log2n;
         const int tr_add = tr_shift > 0 ? 1 << (tr_shift - 1) : 0;
         for (int i = lane; i < n * n; i += 32) {
-            long long v = ((long long)lv[i] * factor_at(i / n, i % n) + add) >> bd_shift;
+            long long v = ((long long)lv(i) * factor_at(i / n, i % n) + add) >> bd_shift;
             v = v < -32768 ? -32768 : (v > 32767 ? 32767 : v);
             const int r = tr_shift >= 0 ? ((int)v + tr_add) >> tr_shift : (int)((unsigned)v << (-tr_shift));
             emit(i / n, i % n, i16s ? (int)(int16_t)r : r);
@@ -252,7 +256,7 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         const int l = lane & 15, r = l >> 2, c = l & 3;
         int d = 0;
         if (lane < 16 && c < nx) {
-            const long long v = ((long long)lv[l] * factor_at(r, c) + add) >> bd_shift;
+            const long long v = ((long long)lv(l) * factor_at(r, c) + add) >> bd_shift;
             d = (int)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v));
         }
         // basis entry T[k][m] of the 4-point DCT (rows 64 / 83,36 / 64 / 36,83
@@ -288,7 +292,7 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
         const int r = i / n, c = i % n;
         int v = 0;
         if (c < nx) {
-            const long long d = ((long long)lv[i] * factor_at(r, c) + add) >> bd_shift;
+            const long long d = ((long long)lv(i) * factor_at(r, c) + add) >> bd_shift;
             v = (int)(d < -32768 ? -32768 : (d > 32767 ? 32767 : d));
         }
         buf[r * kScr + c] = (int16_t)v;

@@ -987,7 +987,7 @@ size_t input_layout(const hpvcd_picture* pics, uint32_t n, std::vector<InputPart
         const size_t ctbs = (size_t)geo.ctb_cols * geo.ctb_rows;
         add(i, 0, p.tus, (size_t)p.n_tus * sizeof(hpvcd_tu));
         add(i, 1, p.ctu_tu_start, (ctbs + 1) * sizeof(uint32_t));
-        add(i, 2, p.coeffs, (size_t)p.n_coeffs * sizeof(int16_t));
+        add(i, 2, p.coeffs, (size_t)p.n_coeffs * ((p.flags & HPVCD_PIC_COEFF8) ? 1 : sizeof(int16_t)));
         add(i, 3, p.cells, (size_t)geo.gw * geo.gh * sizeof(hpvcd_cell));
         add(i, 4, p.sao, ctbs * sizeof(hpvcd_sao_ctb));
         add(i, 5, p.pus, (size_t)p.n_pus * sizeof(hpvcd_pu));

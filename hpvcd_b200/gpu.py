@@ -276,7 +276,7 @@ class DevicePlan:
             C.pointer(d)[0] = p
             d.tus = self._upload(p.tus, p.n_tus * 16)
             d.ctu_tu_start = self._upload(p.ctu_tu_start, (ctbs + 1) * 4)
-            d.coeffs = self._upload(p.coeffs, p.n_coeffs * 2)
+            d.coeffs = self._upload(p.coeffs, p.n_coeffs * (1 if p.flags & abi.PIC_COEFF8 else 2))
             d.cells = self._upload(p.cells, g["gw"] * g["gh"] * 4)
             d.sao = self._upload(p.sao, ctbs * 36)
             d.pus = self._upload(p.pus, p.n_pus * 20)

@@ -79,10 +79,31 @@ def pus_of(p: abi.Picture) -> np.ndarray:
 
 
 def coeffs_of(p: abi.Picture) -> np.ndarray:
+    """The picture's level pool (int16, or int8 with PIC_COEFF8)."""
     if p.n_coeffs == 0:
         return np.zeros(0, np.int16)
+    if p.flags & abi.PIC_COEFF8:
+        return np.frombuffer((C.c_int8 * p.n_coeffs).from_address(p.coeffs), dtype=np.int8)
     buf = (C.c_int16 * p.n_coeffs).from_address(p.coeffs)
     return np.frombuffer(buf, dtype=np.int16)
+
+
+def narrow_coeffs(pics) -> list:
+    """Host transport choice: every picture whose levels all lie in
+    [-128, 127] gets an int8 copy of its pool (PIC_COEFF8), half the bytes
+    to copy.  Returns the new pools, which must outlive the pictures' use."""
+    keep = []
+    for p in pics:
+        if p.n_coeffs == 0 or p.flags & abi.PIC_COEFF8:
+            continue
+        lv = coeffs_of(p)
+        if lv.min() < -128 or lv.max() > 127:
+            continue
+        c8 = np.ascontiguousarray(lv.astype(np.int8))
+        keep.append(c8)
+        p.coeffs = c8.ctypes.data
+        p.flags |= abi.PIC_COEFF8
+    return keep
 
 
 def geometry(p: abi.Picture) -> dict:

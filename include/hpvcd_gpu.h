@@ -210,6 +210,10 @@ typedef struct hpvcd_scaling {
 #define HPVCD_PIC_CONSTRAINED_INTRA 0x0400u
 /* pcm_enabled_flag: records may carry HPVCD_TU_PCM. */
 #define HPVCD_PIC_PCM 0x0800u
+/* coeffs holds int8 levels: the host narrows a picture whose every level
+ * lies in [-128, 127] and so copies half the pool; n_coeffs and
+ * hpvcd_tu.coeff_off still count levels. */
+#define HPVCD_PIC_COEFF8 0x1000u
 /* Store the decoded picture into entry e of the context's DPB (hpvcd_dpb)
  * after it is reconstructed; bits 16..23 of flags, 0 = no store. */
 #define HPVCD_PIC_STORE_DPB(e) ((uint32_t)((e) + 1) << 16)
@@ -241,7 +245,7 @@ typedef struct hpvcd_picture {
     uint64_t n_coeffs;
     const hpvcd_tu* tus;           /* n_tus                                  */
     const uint32_t* ctu_tu_start;  /* ctb_cols * ctb_rows + 1 prefix offsets  */
-    const int16_t* coeffs;         /* n_coeffs                               */
+    const int16_t* coeffs;         /* n_coeffs (int8 with HPVCD_PIC_COEFF8)  */
     const hpvcd_cell* cells;       /* ceil(w/4) * ceil(h/4), NULL -> no deblock */
     const hpvcd_sao_ctb* sao;      /* ctb_cols * ctb_rows, NULL -> no SAO     */
     const hpvcd_pu* pus;           /* n_pus, inter pictures only              */

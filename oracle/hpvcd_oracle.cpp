@@ -891,7 +891,11 @@ void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_
     const int bd = luma ? g.bd : g.bd_c;
     const bool i16s = bd <= 8 && allow16;
     int32_t lv[32 * 32];
-    for (int i = 0; i < n * n; ++i) lv[i] = p->coeffs[(size_t)t.coeff_off + i];
+    // the pool holds int16 levels, or int8 ones when the host narrowed it
+    // (HPVCD_PIC_COEFF8: a transport format only, the levels are the same)
+    const bool c8 = (p->flags & HPVCD_PIC_COEFF8) != 0;
+    for (int i = 0; i < n * n; ++i)
+        lv[i] = c8 ? ((const int8_t*)p->coeffs)[(size_t)t.coeff_off + i] : p->coeffs[(size_t)t.coeff_off + i];
     if (t.flags & (HPVCD_TU_TQB | HPVCD_TU_PCM)) {  // lossless / I_PCM: levels verbatim (saturated for i16 storage)
         for (int i = 0; i < n * n; ++i) res[i] = i16s ? clamp3(lv[i], -32768, 32767) : lv[i];
         rext_residual_ops(res, n, (t.flags & HPVCD_TU_ROTATE) != 0, rdpcm_dir(t), i16s);

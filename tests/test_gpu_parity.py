@@ -65,6 +65,32 @@ def test_residual_picture_10bit_444(dec):
     run_yuv(dec, s.pictures(), "residual 10-bit 4:4:4")
 
 
+# --- int8 level pools (HPVCD_PIC_COEFF8), host buffers and device plans ----
+def test_int8_level_pool(dec):
+    """Narrowed pools decode bit-exactly through hpvcd_gpu_submit (the packed
+    input sized by the flag) and through a device plan, mixed in one batch
+    with pictures that keep their int16 pool."""
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(404, 320, 192, bit_depth=8))      # the inter pictures predict from it
+    for i in range(1, 3):
+        s.add(synth.inter_cfg(404 + i, 320, 192, bit_depth=8, weighted=(i == 2), n_refs=1))
+    s.add(synth.intra_cfg(401, 320, 192, bit_depth=10, chroma_idc=1))
+    s.add(synth.intra_cfg(402, 192, 128, bit_depth=8, chroma_idc=3))
+    s.add(synth.residual_cfg(403, 256, 128, bit_depth=8))
+    pics = s.pictures()
+    lv = synth.coeffs_of(pics[4])
+    lv[np.argmax(np.abs(lv))] = 300            # this one keeps int16
+    ref, _ = O.decode_batch(pics)
+    keep = synth.narrow_coeffs(pics)
+    assert len(keep) >= 4 and not pics[4].flags & abi.PIC_COEFF8
+    assert_planes_equal(dec.decode_yuv(pics), ref, "int8 pools, host submit")
+    plan = DevicePlan(pics)
+    plan.launch()
+    assert plan.status() == abi.OK
+    assert_planes_equal([plan.planes(i) for i in range(len(pics))], ref, "int8 pools, device plan")
+    plan.close()
+
+
 # --- intra pictures: prediction + residual + deblock + SAO -----------------
 @pytest.mark.parametrize("bd,idc", [(8, 1), (10, 1), (8, 3), (10, 3), (8, 0)])
 def test_intra_tile(dec, bd, idc):

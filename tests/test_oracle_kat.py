@@ -435,3 +435,34 @@ def test_orientation_of_the_oracle_canvas(orient):
         _, got = O.decode_batch(pics, out, want_planes=False)
         for p0, p1 in zip(normal, planes(out, got)):
             assert np.array_equal(turn(p0), p1)
+
+
+def test_int8_level_pool_decodes_the_same():
+    """HPVCD_PIC_COEFF8 is a transport format: a picture whose levels all
+    fit in int8 decodes identically from the narrowed pool (intra, residual-
+    only and inter pictures, 8 and 10 bit, 4:2:0 and 4:4:4), and a picture
+    with a level outside [-128, 127] keeps its int16 pool."""
+    from hpvcd_b200 import abi, synth
+    s = synth.SynthSet()
+    s.add(synth.intra_cfg(304, 160, 96, bit_depth=8))       # the inter pictures predict from it
+    for i in range(1, 3):
+        s.add(synth.inter_cfg(304 + i, 160, 96, bit_depth=8, weighted=(i == 2), n_refs=1))
+    s.add(synth.intra_cfg(301, 192, 128, bit_depth=10, chroma_idc=1))
+    s.add(synth.intra_cfg(302, 128, 128, bit_depth=8, chroma_idc=3))
+    s.add(synth.residual_cfg(303, 128, 96, bit_depth=8))
+    pics = s.pictures()
+    want, _ = O.decode_batch(pics)
+    keep = synth.narrow_coeffs(pics)
+    assert len(keep) >= 4 and sum(1 for p in pics if p.flags & abi.PIC_COEFF8) == len(keep)
+    got, _ = O.decode_batch(pics)
+    for a, b in zip(want, got):
+        for pa, pb in zip(a, b):
+            assert np.array_equal(pa, pb)
+    # a level beyond int8 keeps the int16 pool
+    s2 = synth.SynthSet()
+    s2.add(synth.intra_cfg(311, 64, 64, bit_depth=10))
+    p2 = s2.pictures()
+    lv = synth.coeffs_of(p2[0])
+    if lv.size:
+        lv[np.argmax(np.abs(lv))] = 200
+        assert synth.narrow_coeffs(p2) == [] and not p2[0].flags & abi.PIC_COEFF8
