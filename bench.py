@@ -79,8 +79,8 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """Per-launch DRAM traffic of the dominant kernel from the committed ncu
-    summary (profiles/recon_traffic.json), or None."""
+    """DRAM traffic of the reconstruction stage per step from the committed
+    ncu summaries (profiles/recon_traffic.json), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "recon_traffic.json")) as f:
             return json.load(f)
@@ -378,7 +378,10 @@ def run_ours(args):
     recon_s = stage_ms[0] / 1e3
     achieved = recon_bytes / recon_s / 1e9
     traffic = profile_traffic()
-    roofline = {"kernel": "k_recon", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+    # achieved, algorithmic bytes and traffic all cover the reconstruction
+    # stage: k_residual + k_recon of every group of one step
+    roofline = {"kernel": "k_recon", "scope": "reconstruction stage (k_residual + k_recon, one step)",
+                "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": recon_bytes,
                 "traffic": traffic.get("dram_bytes_per_launch") if traffic else None}
