@@ -303,6 +303,7 @@ def lib() -> C.CDLL:
             "hpvcd_gpu_pack_inputs": (i32, [C.POINTER(Picture), u32, vp, u64, C.POINTER(Picture)]),
             "hpvcd_decode_noalloc": (i32, [C.POINTER(Picture), C.POINTER(vp), vp, vp]),
             "hpvcd_plan_set_sched": (i32, [vp, C.POINTER(Sched)]),
+            "hpvcd_plan_set_wait_test": (i32, [vp, u32, i32]),
             "hpvcd_plan_features": (i32, [vp, u32, u32, vp, vp]),
             "hpvcd_plan_autotune": (i32, [vp, C.POINTER(Sched), u32, u32, u32, u32, vp, C.POINTER(C.c_float),
                                           C.POINTER(u32)]),

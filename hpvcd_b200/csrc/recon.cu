@@ -1609,14 +1609,16 @@ extern "C" cudaError_t hpvcd_launch_ccp(const hpvcd::DevPic* pics, const uint32_
 
 extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd::CtuItem* items,
                                           uint32_t n_items, uint32_t* work_counter, uint32_t* dev_err,
-                                          int cfmt, int grid, int team, int feat, int fine, cudaStream_t stream) {
+                                          int cfmt, int grid, int team, int feat, int fine, uint32_t spin,
+                                          cudaStream_t stream) {
     if (n_items == 0) return cudaSuccess;
     // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
     // when the plan was built (no non-stream API call here, so launches can
     // be captured into CUDA graphs)
     const size_t smem = hpvcd::ReconLayout(cfmt).total;
-    // 2^22 polls of >= 64 ns each bound one neighbour wait to a few hundred ms.
-    const uint32_t spin = 1u << 22;
+    // default: 2^22 polls of >= 64 ns each bound one neighbour wait to a few
+    // hundred ms
+    if (spin == 0) spin = 1u << 22;
     if (team == 2 && feat)
         hpvcd::k_recon<2, true><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
                                                                               dev_err, cfmt, spin, fine);

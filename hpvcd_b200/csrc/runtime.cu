@@ -23,7 +23,7 @@ extern "C" cudaError_t hpvcd_launch_residual(const DevPic*, const uint32_t*, uin
 extern "C" cudaError_t hpvcd_launch_ccp(const DevPic*, const uint32_t*, uint32_t, uint32_t, uint32_t*, int,
                                         cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int, int,
-                                          int, int, int, cudaStream_t);
+                                          int, int, int, uint32_t, cudaStream_t);
 extern "C" int hpvcd_recon_occupancy(int cfmt);
 extern "C" hpvcd_status hpvcd_mlp_host_copy(hpvcd_mlp* M, float* params, float* lohi, int* has_domain);
 extern "C" uint32_t hpvcd_mlp_pick_host(const float* w, uint32_t K, const float* x, const float* lohi,
@@ -95,7 +95,7 @@ bool sao_active(const hpvcd_picture& p) {
 
 struct Segment {
     uint32_t first_pic, n_pics;
-    uint32_t item_off, n_items;
+    uint32_t item_off, n_items;  // n_items: entries launched (one fewer while a test drops a CTU)
     int max_dbk_v, max_dbk_h, max_sao;
     int max_rgb;  // RGB quads of the segment's largest picture
 };
@@ -207,6 +207,10 @@ struct hpvcd_plan {
     cudaStream_t alloc_stream = nullptr;
     bool pooled = false;
     cudaGraphExec_t graphs[16] = {};  // captured launch sequences by stage mask
+    // test hook of the bounded wavefront waits (hpvcd_plan_set_wait_test):
+    // polls per wait (0 = default) and the work-list entry left out (-1 none)
+    uint32_t spin_limit = 0;
+    int32_t drop_item = -1;
     std::vector<int> dpb_refs;        // DPB entries the pictures predict from
     // concurrent segments (independent pictures): one stream per segment,
     // forked from and joined back into the launching stream
@@ -773,7 +777,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             const int grid = std::max(1, std::min<int>(share, (int)s.n_items));
             e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
                                    P->cfmt, grid, (int)P->sched.luma_team, P->recon_feat ? 1 : 0,
-                                   P->sched.wave ? 0 : 1, st);
+                                   P->sched.wave ? 0 : 1, P->spin_limit, st);
             if (e != cudaSuccess) return cuda_status(e);
         }
         if (stages & HPVCD_STAGE_DEBLOCK) {
@@ -1226,6 +1230,41 @@ HPVCD_API hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched*
     if (std::memcmp(&next, &plan->sched, sizeof(next)) == 0) return HPVCD_OK;
     plan->sched = next;
     // graphs captured with the previous schedule hold its kernels
+    for (cudaGraphExec_t& gx : plan->graphs)
+        if (gx) {
+            cudaGraphExecDestroy(gx);
+            gx = nullptr;
+        }
+    return HPVCD_OK;
+}
+
+// Test hook of the bounded wavefront waits: every wait of the plan's
+// reconstruction kernel gives up after `spin_limit` polls (0 = the default),
+// and entry `drop_ctu` of the CTU work list is left out of the launches
+// (-1 restores it): that CTU is never reconstructed, so the waits of the CTUs
+// predicting from it run out, set the device error word and return.
+HPVCD_API hpvcd_status hpvcd_plan_set_wait_test(hpvcd_plan* plan, uint32_t spin_limit, int32_t drop_ctu) {
+    if (!plan || drop_ctu < -1 || (drop_ctu >= 0 && (size_t)drop_ctu >= plan->items.size()))
+        return HPVCD_ERR_INVALID_ARG;
+    std::vector<CtuItem> list = plan->items;
+    for (size_t si = 0; si < plan->segs.size(); ++si) {
+        Segment& sg = plan->segs[si];
+        const uint32_t end = si + 1 < plan->segs.size() ? plan->segs[si + 1].item_off : (uint32_t)plan->items.size();
+        sg.n_items = end - sg.item_off;
+        if (drop_ctu >= 0 && (uint32_t)drop_ctu >= sg.item_off && (uint32_t)drop_ctu < end) {
+            // the segment's later entries move up by one; its last slot is not launched
+            list.erase(list.begin() + drop_ctu);
+            list.insert(list.begin() + (end - 1), plan->items[(size_t)drop_ctu]);
+            sg.n_items -= 1;
+        }
+    }
+    if (!list.empty()) {
+        const cudaError_t e =
+            cudaMemcpy(plan->d_items, list.data(), sizeof(CtuItem) * list.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    plan->spin_limit = spin_limit;
+    plan->drop_item = drop_ctu;
     for (cudaGraphExec_t& gx : plan->graphs)
         if (gx) {
             cudaGraphExecDestroy(gx);
@@ -1840,6 +1879,12 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
                       "decode them with a plan");
         return HPVCD_ERR_UNSUPPORTED;
     }
+    if (p.flags & HPVCD_PIC_STORE_MASK) {
+        std::snprintf(t_last_error, sizeof(t_last_error),
+                      "hpvcd_decode_noalloc: decoded-picture buffer stores belong to a context's submits; the "
+                      "picture's planes are the caller's here");
+        return HPVCD_ERR_UNSUPPORTED;
+    }
     const int n_comp = p.chroma_idc ? 3 : 1;
     for (int c = 0; c < n_comp; ++c)
         if (!planes[c] || ((uintptr_t)planes[c] & 255)) {
@@ -1859,7 +1904,12 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_status(e);
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return HPVCD_ERR_LIMIT;
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        std::snprintf(t_last_error, sizeof(t_last_error),
+                      "hpvcd_decode_noalloc: device %d is beyond the %d devices this entry point serves", dev,
+                      kNoAllocMaxDevices);
+        return HPVCD_ERR_LIMIT;
+    }
     NoAllocDevice* nd = nullptr;
     s = noalloc_setup(dev, &nd);
     if (s != HPVCD_OK) return s;
@@ -1930,7 +1980,7 @@ HPVCD_API hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* 
         e = hpvcd_launch_recon(dp, (const CtuItem*)(base + L.items), n_ctu, work_counter, d_err, cfmt, grid, 1,
                                (p.ctb_region || (p.flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT |
                                                            HPVCD_PIC_PCM))) ? 1 : 0,
-                               1, st);
+                               1, 0, st);
         if (e != cudaSuccess) return cuda_status(e);
     }
     const int lv = (d.w >= 12 ? (d.w - 4) / 8 : 0) * (d.h / 4);

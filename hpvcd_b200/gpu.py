@@ -321,6 +321,11 @@ class DevicePlan:
         _check(self._L.hpvcd_plan_set_sched(self._h, C.byref(sched) if sched is not None else None),
                "hpvcd_plan_set_sched")
 
+    def set_wait_test(self, spin_limit: int = 0, drop_ctu: int = -1) -> None:
+        """Bound every wavefront wait to `spin_limit` polls (0: default) and
+        leave work-list entry `drop_ctu` out of the launches (-1: none)."""
+        _check(self._L.hpvcd_plan_set_wait_test(self._h, spin_limit, drop_ctu), "hpvcd_plan_set_wait_test")
+
     def canvas(self) -> np.ndarray:
         ptr, nb = C.c_void_p(), C.c_uint64()
         _check(self._L.hpvcd_plan_canvas(self._h, C.byref(ptr), C.byref(nb)), "hpvcd_plan_canvas")

@@ -495,6 +495,15 @@ uint32_t hpvcd_plan_launches_per_run(const hpvcd_plan* plan);
 /* Schedule of the plan's next launches (NULL = default); drops CUDA graphs
  * captured with the previous schedule.  Pixels do not depend on it. */
 hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched);
+/* Test hook of the bounded device waits.  No reference counterpart (the
+ * reference's WPP rows always publish, wpp.rs:168-172).  Every wavefront
+ * wait of the plan's later launches gives up after spin_limit polls (0 = the
+ * default, 2^22 polls of >= 64 ns each); drop_ctu >= 0 leaves that entry of
+ * the plan's CTU work list (wavefront order) out of the launches, -1 restores
+ * it.  A dropped CTU is never reconstructed, so the waits of the CTUs that
+ * predict from it run out and the launch completes with HPVCD_ERR_TIMEOUT in
+ * hpvcd_plan_device_status.  Synchronous; drops captured CUDA graphs. */
+hpvcd_status hpvcd_plan_set_wait_test(hpvcd_plan* plan, uint32_t spin_limit, int32_t drop_ctu);
 
 /* ------------------------------------------------------------------------ */
 /* Schedule selection: exhaustive autotuning and a learned selector.  No    */
@@ -608,7 +617,9 @@ hpvcd_status hpvcd_plan_select(hpvcd_plan* plan, hpvcd_mlp* mlp, const hpvcd_sch
  *   - HPVCD_ERR_LIMIT (message in hpvcd_last_error_string) when the picture
  *     needs more scratch than HPVCD_NOALLOC_SCRATCH_BYTES;
  *     HPVCD_ERR_UNSUPPORTED for inter pictures (their references belong to
- *     the same launch: use a plan). */
+ *     the same launch: use a plan) and for pictures flagged
+ *     HPVCD_PIC_STORE_DPB(e) (stores into a decoded-picture buffer belong to
+ *     a context's submits). */
 hpvcd_status hpvcd_decode_noalloc(const hpvcd_picture* dev_pic, void* const planes[3],
                                   uint32_t* dev_status, void* stream);
 

@@ -1079,6 +1079,14 @@ int mc_picture(const hpvcd_picture* p, const orc_planes* refs, int n_refs, orc_p
     return HPVCD_OK;
 }
 
+// slice_deblocking_filter_disabled_flag per slice index (decode.rs:1762
+// SliceDeblock.disabled; slice 0 stands for the picture when it has no
+// slice map).  The flat buffers carry no such flag: a host folds it into the
+// boundary strengths.  The oracle keeps the reference's own test so that the
+// fold can be checked against it; orc_set_disabled_slices sets it.
+static uint8_t g_slice_disabled[256];
+static bool g_any_slice_disabled = false;
+
 // decode.rs:1774-2146 apply_deblocking (single slice, PPS-level parameters).
 int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
     int rc = validate(p);
@@ -1098,6 +1106,13 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
         }
         *beta_offset = 2 * b;
         *tc_offset = 2 * t;
+    };
+    // decode.rs:1934, :1979, :2060: a segment whose q sample lies in a slice
+    // with deblocking disabled is skipped
+    auto disabled_at = [&](int qx, int qy) {
+        if (!g_any_slice_disabled) return false;
+        const int s = p->ctb_region ? p->ctb_region[(size_t)(qy >> g.log2_ctb) * g.ctb_cols + (qx >> g.log2_ctb)] >> 8 : 0;
+        return g_slice_disabled[s] != 0;
     };
     auto qp_at = [&](int px, int py) {
         const int gx = std::min(px / 4, g.gw - 1), gy = std::min(py / 4, g.gh - 1);
@@ -1145,6 +1160,7 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
                 const int mid = scan + 1;
                 const int bs = pass == 0 ? bs_v(edge, mid) : bs_h(mid, edge);
                 if (bs == 0) continue;
+                if (pass == 0 ? disabled_at(edge, mid) : disabled_at(mid, edge)) continue;
                 const int qp_p = pass == 0 ? qp_at(edge - 1, mid) : qp_at(mid, edge - 1);
                 const int qp_q = pass == 0 ? qp_at(edge, mid) : qp_at(mid, edge);
                 const int avg = (qp_p + qp_q + 1) >> 1;
@@ -1175,6 +1191,7 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
                 const int bs = pass == 0 ? bs_v(lex, ley) : bs_h(lex, ley);
                 if (bs < 2) continue;
                 const int lqx = std::min(lex, g.w - 1), lqy = std::min(ley, g.h - 1);
+                if (disabled_at(lqx, lqy)) continue;
                 int ppx, ppy;
                 if (pass == 0) {
                     ppx = std::min(std::max(lex - 1, 0), g.w - 1);
@@ -1294,6 +1311,17 @@ int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
 // C exports
 // ---------------------------------------------------------------------------
 extern "C" {
+
+// Slices whose deblocking is disabled (flags[256], one per slice index;
+// NULL clears them all).  Test input of the oracle only.
+void orc_set_disabled_slices(const uint8_t* flags) {
+    g_any_slice_disabled = false;
+    for (int i = 0; i < 256; ++i) {
+        g_slice_disabled[i] = flags ? flags[i] : 0;
+        g_any_slice_disabled = g_any_slice_disabled || g_slice_disabled[i];
+    }
+}
+
 
 int32_t orc_max_log2_tr_range(int32_t bd, int32_t ext) { return max_tr_range(bd, ext != 0); }
 void orc_dequant_params_get(int32_t n, int32_t qp, int32_t bd, int32_t ext, orc_dequant_params* o) {

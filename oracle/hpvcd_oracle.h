@@ -37,6 +37,9 @@ typedef struct orc_ts_params {
 } orc_ts_params;
 
 /* transform.rs */
+/* Slices whose deblocking is disabled (flags[256] by slice index, NULL
+ * clears): the reference's SliceDeblock.disabled, a test input. */
+void orc_set_disabled_slices(const uint8_t* flags);
 int32_t orc_max_log2_tr_range(int32_t bd, int32_t ext);
 void orc_dequant_params_get(int32_t n, int32_t qp_prime, int32_t bd, int32_t ext,
                             orc_dequant_params* out);

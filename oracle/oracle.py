@@ -59,8 +59,19 @@ def lib() -> C.CDLL:
         L.orc_deblock_picture.argtypes = [C.POINTER(abi.Picture), C.POINTER(Planes)]
         L.orc_sao_picture.argtypes = [C.POINTER(abi.Picture), C.POINTER(Planes)]
         L.orc_mc_picture.argtypes = [C.POINTER(abi.Picture), C.POINTER(Planes), i32, C.POINTER(Planes)]
+        L.orc_set_disabled_slices.argtypes = [vp]
+        L.orc_set_disabled_slices.restype = None
         _lib = L
     return _lib
+
+
+def set_disabled_slices(slices) -> None:
+    """Slice indexes whose deblocking is disabled in later oracle decodes
+    (decode.rs:1934 / :1979 / :2060 `sd.disabled`); None or [] clears."""
+    flags = np.zeros(256, np.uint8)
+    for s in slices or ():
+        flags[s] = 1
+    lib().orc_set_disabled_slices(_p(flags) if flags.any() else None)
 
 
 def _p(a: np.ndarray):

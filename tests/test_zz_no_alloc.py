@@ -116,6 +116,29 @@ def test_noalloc_matches_plan_entry_point_on_consecutive_calls():
             assert diff.max(initial=0) <= TOLERANCE, f"picture {i} component {c}"
 
 
+def test_noalloc_matches_the_oracle():
+    """The no-allocation planes of two pictures (one with deblocking and SAO,
+    one 4:4:4 with cross-component prediction and RExt tools) against the
+    CPU oracle directly, not only against the plan entry point."""
+    torch = _torch()
+    from hpvcd_b200.gpu import DevicePlan
+    from oracle import oracle as O
+    L = abi.lib()
+    keep, pics = _pictures()
+    plan = DevicePlan(pics)  # uploads the inputs; its own launches are not used here
+    ref, _ = O.decode_batch(pics)
+    stream = torch.cuda.current_stream()
+    for i in (0, 4):
+        for _ in range(2):  # two calls in a row on the shared scratch
+            o = NoAllocOut(torch, pics[i])
+            assert _call(L, plan.dev_pics[i], o, stream) == abi.OK, L.hpvcd_last_error_string()
+            torch.cuda.synchronize()
+            assert int(o.status.item()) == 0
+            for c, g in enumerate(o.host()):
+                diff = np.abs(g.astype(np.int32) - ref[i][c].astype(np.int32))
+                assert diff.max(initial=0) <= TOLERANCE, f"picture {i} component {c}"
+
+
 def test_noalloc_largest_stated_picture_fits():
     torch = _torch()
     from hpvcd_b200.gpu import DevicePlan
@@ -157,6 +180,11 @@ def test_noalloc_rejects_what_it_cannot_hold():
 
     s.add(synth.intra_cfg(9303, 256, 128))
     ok = s.picture(2)
+    stored = abi.Picture()
+    C.pointer(stored)[0] = ok
+    stored.flags |= abi.PIC_STORE_DPB(0)  # DPB stores belong to a context's submits
+    assert L.hpvcd_decode_noalloc(C.byref(stored), dummy, None, None) == abi.ERR_UNSUPPORTED
+    assert b"decoded-picture buffer" in L.hpvcd_last_error_string()
     bad = (C.c_void_p * 3)(256 + 16, 512, 768)  # misaligned luma plane
     assert L.hpvcd_decode_noalloc(C.byref(ok), bad, None, None) == abi.ERR_INVALID_ARG
     assert L.hpvcd_decode_noalloc(None, dummy, None, None) == abi.ERR_INVALID_ARG
