@@ -57,9 +57,10 @@ def inter_gop(seed=1000, n_frames=32, w=1920, h=1080):
     return s, s.pictures()
 
 
-def frame_by_frame(pics, in_flight=2, entries=5):
+def frame_by_frame(pics, in_flight=2, entries=32):
     """One frame per submit; frame k is stored in DPB entry k % entries and
-    reads its references (at most 4 frames back) from theirs."""
+    reads its references from theirs (the sequence's references reach back
+    up to the intra frame, so every frame keeps its own entry)."""
     out = []
     with GpuDecoder(0, max_inflight=in_flight) as d, Dpb(0, entries) as dpb:
         d.set_dpb(dpb)
