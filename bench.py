@@ -302,7 +302,7 @@ def run_ours(args):
         pick = int(chosen.value)
         sc = selector.SCHEDULES[pick] if pick < selector.K else None
         schedule = {"selected_by": "network", "pick": pick,
-                    "sched": [sc.idct, sc.luma_team, sc.recon_ctas_per_sm] if sc is not None else None}
+                    "sched": [sc.idct, sc.chroma_warps, sc.recon_ctas_per_sm] if sc is not None else None}
     for _ in range(args.warmup):
         flush.zero_()
         plan.launch(abi.STAGE_ALL, stream)

@@ -233,7 +233,7 @@ class GpuCfg(C.Structure):
 
 
 class Sched(C.Structure):
-    _fields_ = [("idct", C.c_uint32), ("luma_team", C.c_uint32),
+    _fields_ = [("idct", C.c_uint32), ("chroma_warps", C.c_uint32),
                 ("recon_ctas_per_sm", C.c_uint32), ("wave", C.c_uint32)]
 
 

@@ -503,22 +503,31 @@ k_ccp(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_prefix, 
 // ===========================================================================
 // k_recon
 // ===========================================================================
-constexpr int kReconWarps = 4;
-constexpr int kReconThreads = kReconWarps * 32;
 constexpr unsigned kFull = 0xffffffffu;
 
-// Per-warp scratch of the decode-order walk.
+// Per-warp scratch of the decode-order walk (reference samples fit in 16 bits).
 struct WalkScratch {
-    int32_t s[132];   // substituted reference line: s[2n+q] = above[q], s[2n-q] = left[q]
-    int32_t f[132];   // filtered line (same layout); also holds available values before substitution
-    int32_t refs[100];  // angular projection, refs[n + k] for k in [-n, 2n]
+    int16_t s[132];     // substituted reference line: s[2n+q] = above[q], s[2n-q] = left[q]
+    int16_t f[132];     // filtered line (same layout); also holds available values before substitution
+    int16_t refs[100];  // angular projection, refs[n + k] for k in [-n, 2n]
     int32_t dc;         // DC value of the current TB
 };
+constexpr size_t kWsBytes = (sizeof(WalkScratch) + 15) & ~(size_t)15;
 
-// Shared-memory layout of one CTA.  Each component has one bordered canvas:
-// row 0 is the row above the CTU (x = -1 .. 2S-1 for a CTU S wide), rows
-// 1..Sh the CTU, column 7 the column left of the CTU; sample (x, y) is at
-// (y + 1) * CW + x + 8, so the interior rows start 16-byte aligned.
+// One bordered canvas per component of a CTU S x Sh: the row above the CTU
+// first (x = -1 .. 2S-1 at index x + 8), then the CTU's Sh rows of S + 8
+// entries (index 7 = the column left of the CTU, x at x + 8).  Both row
+// lengths are multiples of 8 entries, so every interior row starts 16-byte
+// aligned.
+__host__ __device__ __forceinline__ int can_top(int S) { return 2 * S + 8; }
+__host__ __device__ __forceinline__ int can_row(int S) { return S + 8; }
+__host__ __device__ __forceinline__ int can_size(int S, int Sh) { return can_top(S) + Sh * can_row(S); }
+__device__ __forceinline__ int can_at(int S, int x, int y) {
+    return y < 0 ? x + 8 : can_top(S) + y * can_row(S) + x + 8;
+}
+
+// Shared-memory layout of one CTA: the canvases, one walk scratch per warp,
+// the CTU's staged records, the 16x16 stamp map, the three TB lists.
 // Records of one CTU staged at once: up to 256 luma TBs, one "mark decoded"
 // record per inter CU (64 at most) and the chroma TBs (64 per component at
 // 4:2:0, 128 at 4:2:2, 256 at 4:4:4).  A CTU with more records is malformed.
@@ -528,7 +537,7 @@ constexpr int kFmt420 = 0, kFmt444 = 1, kFmt422 = 2;
 constexpr int kRecCap420 = 256 + 64 + 2 * 64;
 constexpr int kRecCap422 = 256 + 64 + 2 * 128;
 constexpr int kRecCap444 = 256 + 64 + 2 * 256;
-constexpr int kListCap = 256;  // intra TBs of one component in one CTU
+constexpr int kListCap = 256;  // intra TBs of luma in one CTU (all 4x4)
 // list entry: record index (< 1024) | kListEvent for a wavefront event
 constexpr uint32_t kListRec = 0x3ffu, kListEvent = 0x8000u;
 constexpr uint32_t kNoStamp = 0xffffffffu;
@@ -536,28 +545,28 @@ constexpr uint32_t kNoStamp = 0xffffffffu;
 struct ReconLayout {
     int cs_w, cs_h;  // chroma canvas width and height (CTU interior)
     int rec_cap;     // staged records
-    size_t off_can_y, off_can_c, off_res_y, off_res_c, off_ws, off_recs, off_stamp, off_lists, off_misc, total;
-    static __host__ __device__ int cw_of(int S) { return 2 * S + 8; }
-    __host__ __device__ explicit ReconLayout(int cfmt) {
+    int list_c;      // list entries per chroma component
+    size_t off_can_y, off_can_c, off_ws, off_recs, off_stamp, off_lists, off_misc, total;
+    __host__ __device__ ReconLayout(int cfmt, int warps) {
         cs_w = cfmt == kFmt444 ? 64 : 32;
         cs_h = cfmt == kFmt420 ? 32 : 64;
         rec_cap = cfmt == kFmt444 ? kRecCap444 : (cfmt == kFmt422 ? kRecCap422 : kRecCap420);
+        list_c = cfmt == kFmt444 ? 256 : (cfmt == kFmt422 ? 128 : 64);
         size_t o = 0;
-        off_can_y = o; o += (size_t)65 * cw_of(64) * sizeof(uint16_t);
+        off_can_y = o; o += (size_t)can_size(64, 64) * sizeof(uint16_t);
         o = (o + 15) & ~(size_t)15;
-        off_can_c = o; o += 2 * (size_t)(cs_h + 1) * cw_of(cs_w) * sizeof(uint16_t);
+        off_can_c = o; o += 2 * (size_t)can_size(cs_w, cs_h) * sizeof(uint16_t);
         o = (o + 15) & ~(size_t)15;
-        off_res_y = o; o += 64 * 64 * sizeof(int16_t);
-        off_res_c = o; o += 2 * (size_t)cs_w * cs_h * sizeof(int16_t);
-        off_ws = o;    o += kReconWarps * sizeof(WalkScratch);
-        o = (o + 15) & ~(size_t)15;
+        off_ws = o;    o += (size_t)warps * kWsBytes;
         off_recs = o;  o += (size_t)rec_cap * sizeof(hpvcd_tu);
         off_stamp = o; o += 256 * sizeof(uint32_t);
-        off_lists = o; o += 3 * (size_t)kListCap * sizeof(uint16_t);
+        off_lists = o; o += (size_t)(kListCap + 2 * list_c) * sizeof(uint16_t);
         o = (o + 15) & ~(size_t)15;
         off_misc = o;  o += 128;  // claimed item, list counts, edge masks, neighbour levels
         total = o;
     }
+    __host__ __device__ int list_off(int c) const { return c == 0 ? 0 : kListCap + (c - 1) * list_c; }
+    __host__ __device__ int list_cap(int c) const { return c == 0 ? kListCap : list_c; }
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -570,8 +579,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 struct Comp {
     int ox, oy;   // CTU origin in component samples
     int pw, ph;   // plane size
-    int S, Sh;    // CTU width (also the residual canvas stride) and height in component samples
-    int CW;       // canvas row stride
+    int S, Sh;    // CTU width and height in component samples
     int sw, sh;   // luma samples per component sample (1 or 2)
     uint32_t nb_ok;  // neighbour CTUs of the same slice and tile: 1 left, 2 above-left, 4 above, 8 above-right
     const hpvcd_cell* ci_cells;  // constrained intra prediction: cells whose INTER samples are unusable
@@ -581,10 +589,11 @@ struct Comp {
     int bd, max_v;
     bool luma, filt, smoothing, strong;
     uint16_t* can;       // bordered canvas
-    const int16_t* res;  // S x S residual canvas
+    const int16_t* res;  // int16 residual plane (k_residual) at the CTU origin
+    int rs;              // its row stride in samples (a multiple of 16)
 };
 
-__device__ __forceinline__ int cidx(const Comp& k, int x, int y) { return (y + 1) * k.CW + x + 8; }
+__device__ __forceinline__ int cidx(const Comp& k, int x, int y) { return can_at(k.S, x, y); }
 
 // Reference sample i of the line (i < 2n: left column bottom-up, 2n: the
 // corner, > 2n: above row) with its availability (decode.rs:4651-4690
@@ -620,7 +629,7 @@ __device__ __forceinline__ bool gather_ref(const Comp& k, const uint32_t* stamp,
     // the availability test picks the result
     const int ys = min(max(y, 0), k.Sh - 1), xs = min(max(x, 0), k.S - 1);
     const uint32_t st = stamp[((ys * k.sh) >> 2) * 16 + ((xs * k.sw) >> 2)];
-    const int cv = k.can[cidx(k, x, min(y, k.Sh - 1))];
+    const int cv = k.can[cidx(k, y < 0 ? x : min(x, k.S - 1), min(y, k.Sh - 1))];
     bool a = ax >= 0 && ay >= 0 && ax < k.pw && ay < k.ph;
     if (y >= 0) {
         if (x < 0)
@@ -644,13 +653,16 @@ __device__ __forceinline__ int ref_pos(int k, bool vertical, int n2, int inv) {
 // 4x4 intra TB entirely in registers: the 17 reference samples live in
 // lanes 0..16 (intra.rs:84-148 substitution via shuffles; no filtering for
 // n = 4, intra.rs:174), prediction (intra.rs:257-372) by lanes 0..15.
-// I_PCM block (decode.rs:2768-2839): its samples, staged in the residual
-// canvas by k_residual, go to the canvas unchanged.
+// I_PCM block (decode.rs:2768-2839): its samples, written to the residual
+// plane by k_residual, go to the canvas unchanged.
 __device__ __forceinline__ void pcm_tb(const Comp& k, int log2n, int x0, int y0, int lane) {
     const int n = 1 << log2n;
+    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
     for (int i = lane; i < n * n; i += 32) {
         const int yy = i >> log2n, xx = i & (n - 1);
-        k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)clamp3i(k.res[(y0 + yy) * k.S + x0 + xx], 0, k.max_v);
+        if (xx < vw && yy < vh)
+            k.can[cidx(k, x0 + xx, y0 + yy)] =
+                (uint16_t)clamp3i(k.res[(size_t)(y0 + yy) * k.rs + x0 + xx], 0, k.max_v);
     }
     __syncwarp();
 }
@@ -658,6 +670,11 @@ __device__ __forceinline__ void pcm_tb(const Comp& k, int log2n, int x0, int y0,
 __device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y0, bool coded,
                                           const uint32_t* stamp, uint32_t jrec, int lane) {
     constexpr int n = 4, n2 = 8, total = 17;
+    const int yy = lane >> 2, xx = lane & 3;
+    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    const bool mine = lane < 16 && xx < vw && yy < vh;
+    // the residual is loaded first: its latency overlaps the prediction
+    const int rv = coded && mine ? (int)k.res[(size_t)(y0 + yy) * k.rs + x0 + xx] : 0;
     int v = 0;
     // lanes past the line repeat the last position and drop it
     bool a = gather_ref(k, stamp, jrec, n2, x0, y0, min(lane, total - 1), &v);
@@ -672,7 +689,6 @@ __device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y
         sv = __shfl_sync(kFull, v, j);
     }
     // sv in lane i = s[i]
-    const int yy = lane >> 2, xx = lane & 3;
     int pred;
     if (mode >= 2) {
         const int angle = c_intra_angle[mode - 2];
@@ -709,9 +725,8 @@ __device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y
         const int tr = __shfl_sync(kFull, sv, n2 + n + 1), bl = __shfl_sync(kFull, sv, n2 - n - 1);
         pred = ((n - 1 - xx) * lft + (xx + 1) * tr + (n - 1 - yy) * abv + (yy + 1) * bl + n) >> 3;
     }
-    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
-    if (lane < 16 && xx < vw && yy < vh) {
-        if (coded) pred = clamp3i(pred + k.res[(y0 + yy) * k.S + x0 + xx], 0, k.max_v);
+    if (mine) {
+        if (coded) pred = clamp3i(pred + rv, 0, k.max_v);
         k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)pred;
     }
     __syncwarp();
@@ -735,6 +750,14 @@ __device__ __forceinline__ bool ref_filtered(const Comp& k, int n, int mode) {
 __device__ __forceinline__ void intra_tb8(const Comp& k, int mode, int x0, int y0, bool coded,
                                           const uint32_t* stamp, uint32_t jrec, int lane) {
     constexpr int n = 8, n2 = 16, log2n = 3;
+    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    int rv[2];  // residuals of this lane's two samples, loaded first
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int i = lane + 32 * h;
+        const int yy = i >> log2n, xx = i & (n - 1);
+        rv[h] = coded && xx < vw && yy < vh ? (int)k.res[(size_t)(y0 + yy) * k.rs + x0 + xx] : 0;
+    }
     int v_lo = 0, v_hi = 0;
     const bool a_lo = gather_ref(k, stamp, jrec, n2, x0, y0, lane, &v_lo);
     const bool a_hi = gather_ref(k, stamp, jrec, n2, x0, y0, 2 * n2, &v_hi);  // uniform
@@ -821,27 +844,44 @@ __device__ __forceinline__ void intra_tb8(const Comp& k, int mode, int x0, int y
             out[h] = ((n - 1 - xx) * lft + (xx + 1) * tr + (n - 1 - yy) * abv + (yy + 1) * bl + n) >> (log2n + 1);
         }
     }
-    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const int i = lane + 32 * h;
         const int yy = i >> log2n, xx = i & (n - 1);
         if (xx < vw && yy < vh) {
             int v = out[h];
-            if (coded) v = clamp3i(v + k.res[(y0 + yy) * k.S + x0 + xx], 0, max_v);
+            if (coded) v = clamp3i(v + rv[h], 0, max_v);
             k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
         }
     }
     __syncwarp();
 }
 
+// Stages the visible part of a coded n x n TB's residual (n >= 8) into the
+// TB's own canvas area with 16-byte asynchronous copies (the prediction
+// only reads samples outside the TB; each predicting lane then reads its
+// sample's residual in place).
+__device__ __forceinline__ void stage_residual(const Comp& k, int log2n, int x0, int y0, int lane) {
+    const int n = 1 << log2n;
+    const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    const int lc = log2n - 3;  // 8-sample chunks per row: log2
+    const int chunks = ((vw + 7) >> 3);
+    for (int i = lane; i < (vh << lc); i += 32) {
+        const int r = i >> lc, q = i & ((1 << lc) - 1);
+        if (q < chunks)
+            cp_async16(k.can + cidx(k, x0 + 8 * q, y0 + r), k.res + (size_t)(y0 + r) * k.rs + x0 + 8 * q);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
 // Intra TB of size 8..32, first part, by one warp through shared memory:
 // gather, substitution (intra.rs:84-148), filtering (:151-219) and the
 // per-mode set-up of the prediction (the angular projection into ws.refs,
-// the DC value into ws.dc).
-__device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode, int x0, int y0,
+// the DC value into ws.dc).  A coded TB's residual is staged meanwhile.
+__device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
                                               const uint32_t* stamp, uint32_t jrec, WalkScratch& ws, int lane) {
     const int n = 1 << log2n;
+    if (coded) stage_residual(k, log2n, x0, y0, lane);
     const int total = 4 * n + 1;
     const int n2 = 2 * n;
     uint32_t mask[5];
@@ -893,7 +933,7 @@ __device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode
     __syncwarp();
     // ---- filtering (luma, or 4:4:4 chroma without strong smoothing) ----
     const bool do_filter = ref_filtered(k, n, mode);
-    const int32_t* R = ws.s;
+    const int16_t* R = ws.s;
     if (do_filter) {
         bool strong = false;
         const int tl = ws.s[n2], tr = ws.s[2 * n2], bl = ws.s[0];
@@ -947,17 +987,21 @@ __device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode
 
 // Intra TB of size 8..32, second part: prediction (intra.rs:257-372) and
 // residual add + clip (reconstruct.rs:214-251) of samples tl, tl + ts, ...
-// (one warp: tl = lane, ts = 32; a team of warps splits the block).
+// (one warp: tl = lane, ts = 32).  A coded TB's residual is in its canvas
+// area (stage_residual).
 __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
                                                  const WalkScratch& ws, int tl, int ts) {
     const int n = 1 << log2n;
     const int n2 = 2 * n;
-    const int32_t* R = ref_filtered(k, n, mode) ? ws.f : ws.s;
+    const int16_t* R = ref_filtered(k, n, mode) ? ws.f : ws.s;
     const int max_v = k.max_v;
     const bool edge_filters = k.luma && n < 32;  // is_luma gate of predict_into
-    const int S = k.S;
-    const int16_t* res = k.res;
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    if (coded) {  // the staged residual has arrived for every lane
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+    }
+    auto res_at = [&](int xx, int yy) { return (int)(int16_t)k.can[cidx(k, x0 + xx, y0 + yy)]; };
     if (mode >= 2) {
         const int angle = c_intra_angle[mode - 2];
         const bool vertical = mode >= 18;
@@ -979,7 +1023,7 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
                 if (mode == 10 && yy == 0) v = clamp3i(a0 + ((R[n2 + xx + 1] - c0) >> 1), 0, max_v);
             }
             if (xx < vw && yy < vh) {
-                if (coded) v = clamp3i(v + res[(y0 + yy) * S + x0 + xx], 0, max_v);
+                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
                 k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
@@ -998,7 +1042,7 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
                     v = (R[n2 - yy - 1] + 3 * dc + 2) >> 2;
             }
             if (xx < vw && yy < vh) {
-                if (coded) v = clamp3i(v + res[(y0 + yy) * S + x0 + xx], 0, max_v);
+                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
                 k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
@@ -1011,7 +1055,7 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
             const int vv = (n - 1 - yy) * R[n2 + xx + 1] + (yy + 1) * bl;
             int v = (hh + vv + n) >> (log2n + 1);
             if (xx < vw && yy < vh) {
-                if (coded) v = clamp3i(v + res[(y0 + yy) * S + x0 + xx], 0, max_v);
+                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
                 k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
@@ -1021,21 +1065,9 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
 // Intra TB of size 8..32 by one warp.
 __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
                                              const uint32_t* stamp, uint32_t jrec, WalkScratch& ws, int lane) {
-    intra_tb_prep(k, log2n, mode, x0, y0, stamp, jrec, ws, lane);
+    intra_tb_prep(k, log2n, mode, x0, y0, coded, stamp, jrec, ws, lane);
     intra_tb_predict(k, log2n, mode, x0, y0, coded, ws, lane, 32);
     __syncwarp();
-}
-
-// Luma intra TBs of at least 2^kTeamMinLog2 samples square are predicted by
-// a team of warps when the schedule asks for it: warp 0 prepares the
-// reference line, then warp 0 and the CTA's last warp (otherwise idle during
-// the walk) split the prediction.  Both warps walk the same records and take
-// the same decision per record, so every named barrier has both arrivals.
-constexpr int kTeamMinLog2 = 4;
-constexpr int kTeamBarrier = 1;
-
-__device__ __forceinline__ void team_sync(int threads) {
-    asm volatile("bar.sync %0, %1;" ::"r"(kTeamBarrier), "r"(threads) : "memory");
 }
 
 // ---- wavefront progress between neighbouring CTUs ----
@@ -1096,7 +1128,7 @@ __device__ __forceinline__ uint32_t segs_needed(int x, int y, int n, int S, int 
 struct EdgeGeo {
     void* plane;
     uint16_t* can;
-    int ox, oy, S, Sh, pw, ph, CW;
+    int ox, oy, S, Sh, pw, ph;
 };
 
 // Loads the segments m of one component into its canvas, thread t of nt;
@@ -1124,12 +1156,13 @@ __device__ __forceinline__ void fetch_edges(const EdgeGeo& e, uint32_t m, int bp
         if (s >= kSegs) continue;  // unreachable: i < total
         int dx, dy;
         if (s == 0) {
-            dx = -1, dy = -1, dst[r] = 7;
+            dx = -1, dy = -1;
         } else if (s <= 4) {
-            dx = (s - 1) * (e.S >> 1) + j, dy = -1, dst[r] = 8 + dx;
+            dx = (s - 1) * (e.S >> 1) + j, dy = -1;
         } else {
-            dx = -1, dy = (s - 5) * (e.Sh >> 1) + j, dst[r] = (dy + 1) * e.CW + 7;
+            dx = -1, dy = (s - 5) * (e.Sh >> 1) + j;
         }
+        dst[r] = can_at(e.S, dx, dy);
         const int ax = e.ox + dx, ay = e.oy + dy;
         if (ax >= 0 && ay >= 0 && ax < e.pw && ay < e.ph) v[r] = load_sample_cg(e.plane, bps, (size_t)ay * e.pw + ax);
     }
@@ -1158,7 +1191,7 @@ __device__ __forceinline__ void publish_level(const EdgeGeo& e, int bps, int fro
             x = e.S - 1, y = r0 + i;
         else
             x = b0 + i - nr, y = e.Sh - 1;
-        store_sample(e.plane, bps, (size_t)(e.oy + y) * e.pw + e.ox + x, e.can[(y + 1) * e.CW + 8 + x]);
+        store_sample(e.plane, bps, (size_t)(e.oy + y) * e.pw + e.ox + x, e.can[can_at(e.S, x, y)]);
     }
     __syncwarp();
     if (lane == 0) st_release(level, (uint32_t)to);
@@ -1176,7 +1209,6 @@ __device__ __forceinline__ EdgeGeo edge_geo(const DevPic& P, uint16_t* can, int 
     e.oy = cy * e.Sh;
     e.pw = c ? P.cw : P.w;
     e.ph = c ? P.ch : P.h;
-    e.CW = ReconLayout::cw_of(e.S);
     return e;
 }
 
@@ -1233,20 +1265,30 @@ __device__ __forceinline__ uint32_t walk_event(const DevPic& P, uint16_t* can, i
     return have | ((uint32_t)prog << 8);
 }
 
+// Warps of a k_recon CTA: warp 0 walks luma, chroma is walked by warp 1
+// (Cb, then Cr: kCW = 1) or by warps 1 and 2 (one component each: kCW = 2).
+// Two warps keep eight CTU walks resident per SM at 4:2:0 (shared memory
+// and registers both allow it); the third warp shortens a CTU whose chroma
+// walk is as long as its luma walk (4:4:4).
+__host__ __device__ constexpr int recon_warps(int kCW) { return 1 + kCW; }
+
 // kFeat: some picture of the launch has slices / tiles, constrained intra
 // prediction, cross-component prediction or I_PCM blocks; without them the
 // availability, coded and PCM tests compile to the plain form.  fine: the
 // quadrant-level wavefront; otherwise a CTU waits for its neighbours' last
 // level before its walk and releases only its last level.
-template <int kTeam, bool kFeat>
-__global__ void __launch_bounds__(kReconThreads, 4)
+template <int kCW, bool kFeat>
+__global__ void __launch_bounds__(32 * recon_warps(kCW), kCW == 1 ? 8 : 5)
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
         uint32_t* work_counter, uint32_t* dev_err, int cfmt, uint32_t spin_limit, int fine) {
-    static_assert(kTeam == 1 || kTeam == 2, "team of one or two warps");
+    static_assert(kCW == 1 || kCW == 2, "one or two chroma warps");
+    constexpr int kWarps = recon_warps(kCW), kThreads = 32 * kWarps;
     extern __shared__ __align__(16) unsigned char smem[];
-    const ReconLayout lay(cfmt);
+    const ReconLayout lay(cfmt, kWarps);
     uint32_t* s_item = (uint32_t*)(smem + lay.off_misc);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // components walked (and listed) by this warp: [c_lo, c_hi]
+    const int c_lo = warp == 0 ? 0 : (kCW == 1 ? 1 : warp), c_hi = warp == 0 ? 0 : (kCW == 1 ? 2 : warp);
     for (;;) {
         __syncthreads();
         if (tid == 0) *s_item = atomicAdd(work_counter, 1u);
@@ -1278,40 +1320,20 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
         uint32_t* counts = (uint32_t*)(smem + lay.off_misc) + 1;
         auto can_of = [&](int c) -> uint16_t* {
             return c == 0 ? (uint16_t*)(smem + lay.off_can_y)
-                          : (uint16_t*)(smem + lay.off_can_c) +
-                                (size_t)(c - 1) * (lay.cs_h + 1) * ReconLayout::cw_of(lay.cs_w);
+                          : (uint16_t*)(smem + lay.off_can_c) + (size_t)(c - 1) * can_size(lay.cs_w, lay.cs_h);
         };
-        auto res_of = [&](int c) -> int16_t* {
-            return c == 0 ? (int16_t*)(smem + lay.off_res_y)
-                          : (int16_t*)(smem + lay.off_res_c) + (size_t)(c - 1) * lay.cs_w * lay.cs_h;
-        };
-        // ---- prefetch the residual canvases (cp.async, 8 samples per copy) ----
-        for (int c = 0; c < ncomp; ++c) {
-            const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
-            const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
-            const int rows = min(Sh, ph - oy), cols = min(S, pw - ox);
-            const int chunks = (cols + 7) >> 3;
-            const int16_t* src = P.res[c] + (size_t)oy * P.res_stride[c] + ox;
-            int16_t* dst = res_of(c);
-            for (int i = tid; i < rows * chunks; i += kReconThreads) {
-                const int y = i / chunks, q = i % chunks;
-                // residual rows are padded to 16 samples, so a 16-byte copy never
-                // leaves the allocation; samples beyond `cols` are unused
-                cp_async16(dst + y * S + 8 * q, src + (size_t)y * P.res_stride[c] + 8 * q);
-            }
-        }
         // the CTU's records (16 bytes each; the record array is 16-byte aligned)
-        for (uint32_t i = tid; i < nrec; i += kReconThreads) cp_async16(recs + i, P.tus + r0 + i);
+        for (uint32_t i = tid; i < nrec; i += kThreads) cp_async16(recs + i, P.tus + r0 + i);
         asm volatile("cp.async.commit_group;" ::: "memory");
-        for (int i = tid; i < 256; i += kReconThreads) stamp[i] = kNoStamp;
-        // the CTU's own records and residuals have arrived: the decode-order
-        // build below runs before the neighbour wait, off the critical path
+        for (int i = tid; i < 256; i += kThreads) stamp[i] = kNoStamp;
+        // the CTU's own records have arrived: the decode-order build below
+        // runs before the neighbour wait, off the critical path
         cp_async_wait_all();
         __syncthreads();
         // ---- decode order, in parallel: every luma record stamps the 4x4
         // cells it marks decoded (decode.rs:3170-3189; cells outside the
-        // picture stay unmarked), and warp c lists the intra TBs of
-        // component c in decode order ----
+        // picture stay unmarked), and each warp lists the intra TBs of its
+        // components in decode order ----
         const int vis_w = min(64, P.w - oxl), vis_h = min(64, P.h - oyl);
         const bool intra_pred_ok = !(P.flags & HPVCD_PIC_PRED_IN_PLANE);
         // validity of record i for component tc: -1 skip silently, 0 invalid
@@ -1325,7 +1347,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             const int Sw = tc ? Scw : ctb, Sh = tc ? Sch : ctb;
             return (x < 0 || y < 0 || x + n > Sw || y + n > Sh) ? 0 : 1;
         };
-        for (uint32_t i = tid; i < nrec; i += kReconThreads) {
+        for (uint32_t i = tid; i < nrec; i += kThreads) {
             hpvcd_tu t;
             memcpy(&t, &recs[i], sizeof(t));
             int x, y;
@@ -1337,9 +1359,10 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             for (int cy = y >> 2; cy < (y1 + 3) >> 2; ++cy)
                 for (int cx = x >> 2; cx < (x1 + 3) >> 2; ++cx) atomicMin(&stamp[cy * 16 + cx], i);
         }
-        if (warp < ncomp) {
-            const int c = warp;
+        for (int c = c_lo; c <= c_hi && c < ncomp; ++c) {
             const int hs = (c ? Scw : ctb) >> 1, hh = (c ? Sch : ctb) >> 1;
+            const uint32_t cap = (uint32_t)lay.list_cap(c);
+            uint16_t* list = lists + lay.list_off(c);
             uint32_t cnt = 0;
             int qmax = 0;  // quadrant of the entries listed so far (z-order: never decreases)
             for (uint32_t base = 0; base < nrec; base += 32) {
@@ -1376,13 +1399,12 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 const bool event = fine && (q > before || edge);
                 const uint32_t m = __ballot_sync(kFull, mine);
                 const uint32_t pos = cnt + __popc(m & ((1u << lane) - 1u));
-                if (mine && pos < (uint32_t)kListCap)
-                    lists[c * kListCap + pos] = (uint16_t)(i | (event ? kListEvent : 0u));
+                if (mine && pos < cap) list[pos] = (uint16_t)(i | (event ? kListEvent : 0u));
                 cnt += __popc(m);
             }
-            if (cnt > (uint32_t)kListCap) {
+            if (cnt > cap) {
                 if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
-                cnt = kListCap;
+                cnt = cap;
             }
             if (lane == 0) counts[c] = cnt;
         }
@@ -1404,13 +1426,12 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
                 const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
                 uint16_t* can = can_of(c);
-                const int CW = ReconLayout::cw_of(S);
-                for (int i = tid; i < S * Sh; i += kReconThreads) {
+                for (int i = tid; i < S * Sh; i += kThreads) {
                     const int y = i / S, x = i % S;
                     const int ax = ox + x, ay = oy + y;
                     int v = 0;
                     if (ax < pw && ay < ph) v = load_sample(P.rec[c], P.bps, (size_t)ay * pw + ax);
-                    can[(y + 1) * CW + x + 8] = (uint16_t)v;
+                    can[can_at(S, x, y)] = (uint16_t)v;
                 }
             }
         }
@@ -1463,18 +1484,14 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             s_have[tid] = h;
         }
         __syncthreads();
-        for (int c = 0; c < ncomp; ++c) fetch_edges<2>(geo(c), s_have[c], P.bps, tid, kReconThreads);
+        for (int c = 0; c < ncomp; ++c) fetch_edges<(kThreads < 96 ? 4 : 3)>(geo(c), s_have[c], P.bps, tid, kThreads);
         __syncthreads();
-        // ---- decode-order walk: warp c reconstructs component c ----
-        const bool helper = kTeam > 1 && warp == kReconWarps - 1;
-        if (warp < ncomp || helper) {
-            const int c = helper ? 0 : warp;
-            WalkScratch& ws = ((WalkScratch*)(smem + lay.off_ws))[warp];
-            WalkScratch& team_ws = ((WalkScratch*)(smem + lay.off_ws))[0];
+        // ---- decode-order walk: each warp reconstructs its components ----
+        WalkScratch& ws = *(WalkScratch*)(smem + lay.off_ws + (size_t)warp * kWsBytes);
+        for (int c = c_lo; c <= c_hi && c < ncomp; ++c) {
             Comp k;
             k.S = c ? Scw : ctb;
             k.Sh = c ? Sch : ctb;
-            k.CW = ReconLayout::cw_of(k.S);
             k.ox = c ? ocx : oxl;
             k.oy = c ? ocy : oyl;
             k.pw = c ? P.cw : P.w;
@@ -1493,10 +1510,11 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             k.smoothing = !(P.flags & HPVCD_PIC_SMOOTHING_DISABLED);
             k.strong = (P.flags & HPVCD_PIC_STRONG_SMOOTHING) != 0;
             k.can = can_of(c);
-            k.res = res_of(c);
+            k.rs = P.res_stride[c];
+            k.res = P.res[c] + (size_t)k.oy * k.rs + k.ox;
             const uint32_t cnt = counts[c];
-            const uint16_t* list = lists + c * kListCap;
-            // edge segments in the canvas, quadrants released (the leader's)
+            const uint16_t* list = lists + lay.list_off(c);
+            // edge segments in the canvas, quadrants released
             uint32_t have = s_have[c];
             int prog = 0;
             // the next record is fetched while the current TB is reconstructed
@@ -1511,8 +1529,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     jn = list[e + 1];
                     wn = recs[jn & kListRec];
                 }
-                const int x = (int)t.x - (c ? ocx : oxl), y = (int)t.y - (c ? ocy : oyl);
-                if (event && !helper) {
+                const int x = (int)t.x - k.ox, y = (int)t.y - k.oy;
+                if (event) {
                     const uint32_t r = walk_event(P, k.can, c, it.cx, it.cy, x, y, 1 << t.log2n, prog, have, spin_limit,
                                                   dev_err, lane);
                     have = r & kSegMask;
@@ -1521,15 +1539,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 // a chroma TB with cross-component prediction has a residual
                 // (written by k_ccp) even without coded coefficients
                 const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
-                if (kFeat && (t.flags & HPVCD_TU_PCM)) {  // leader alone, no team step
-                    if (!helper) pcm_tb(k, t.log2n, x, y, lane);
-                } else if (kTeam > 1 && c == 0 && t.log2n >= kTeamMinLog2) {
-                    if (!helper) intra_tb_prep(k, t.log2n, t.mode, x, y, stamp, j, team_ws, lane);
-                    team_sync(32 * kTeam);
-                    intra_tb_predict(k, t.log2n, t.mode, x, y, coded, team_ws, (helper ? 32 : 0) + lane, 32 * kTeam);
-                    team_sync(32 * kTeam);
-                } else if (helper) {
-                    // smaller TBs are the leader's alone
+                if (kFeat && (t.flags & HPVCD_TU_PCM)) {
+                    pcm_tb(k, t.log2n, x, y, lane);
                 } else if (t.log2n == 2) {
                     intra_tb4(k, t.mode, x, y, coded, stamp, j, lane);
                 } else if (t.log2n == 3) {
@@ -1538,7 +1549,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     intra_tb_big(k, t.log2n, t.mode, x, y, coded, stamp, j, ws, lane);
                 }
             }
-            if (!helper && warp < ncomp) publish_level(geo(c), P.bps, prog, 4, level + c, lane);
+            publish_level(geo(c), P.bps, prog, 4, level + c, lane);
         }
         __syncthreads();
         // ---- write the CTU out for the filters (8 samples per store when
@@ -1547,13 +1558,12 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
             const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
             const uint16_t* can = can_of(c);
-            const int CW = ReconLayout::cw_of(S);
             const int rows = min(Sh, ph - oy), cols = min(S, pw - ox);
             if ((pw & 7) == 0 && (cols & 7) == 0) {
                 const int chunks = cols >> 3;
-                for (int i = tid; i < rows * chunks; i += kReconThreads) {
+                for (int i = tid; i < rows * chunks; i += kThreads) {
                     const int y = i / chunks, q = i % chunks;
-                    const uint4 v = *(const uint4*)(can + (y + 1) * CW + 8 + 8 * q);
+                    const uint4 v = *(const uint4*)(can + can_at(S, 8 * q, y));
                     const size_t off = (size_t)(oy + y) * pw + ox + 8 * q;
                     if (P.bps == 2) {
                         *(uint4*)((uint16_t*)P.rec[c] + off) = v;
@@ -1566,9 +1576,9 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     }
                 }
             } else {
-                for (int i = tid; i < rows * cols; i += kReconThreads) {
+                for (int i = tid; i < rows * cols; i += kThreads) {
                     const int y = i / cols, x = i % cols;
-                    store_sample(P.rec[c], P.bps, (size_t)(oy + y) * pw + ox + x, can[(y + 1) * CW + 8 + x]);
+                    store_sample(P.rec[c], P.bps, (size_t)(oy + y) * pw + ox + x, can[can_at(S, x, y)]);
                 }
             }
         }
@@ -1577,7 +1587,9 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
 
 }  // namespace hpvcd
 
-extern "C" size_t hpvcd_recon_smem_bytes(int cfmt) { return hpvcd::ReconLayout(cfmt).total; }
+extern "C" size_t hpvcd_recon_smem_bytes(int cfmt, int chroma_warps) {
+    return hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(chroma_warps == 2 ? 2 : 1)).total;
+}
 
 extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const uint32_t* rec_prefix,
                                              uint32_t n_pics, uint32_t total_records, uint32_t* dev_err,
@@ -1609,41 +1621,51 @@ extern "C" cudaError_t hpvcd_launch_ccp(const hpvcd::DevPic* pics, const uint32_
 
 extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd::CtuItem* items,
                                           uint32_t n_items, uint32_t* work_counter, uint32_t* dev_err,
-                                          int cfmt, int grid, int team, int feat, int fine, uint32_t spin,
+                                          int cfmt, int grid, int chroma_warps, int feat, int fine, uint32_t spin,
                                           cudaStream_t stream) {
     if (n_items == 0) return cudaSuccess;
     // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
     // when the plan was built (no non-stream API call here, so launches can
     // be captured into CUDA graphs)
-    const size_t smem = hpvcd::ReconLayout(cfmt).total;
+    const int cw = chroma_warps == 2 ? 2 : 1;
+    const size_t smem = hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(cw)).total;
+    const int threads = 32 * hpvcd::recon_warps(cw);
     // default: 2^22 polls of >= 64 ns each bound one neighbour wait to a few
     // hundred ms
     if (spin == 0) spin = 1u << 22;
-    if (team == 2 && feat)
-        hpvcd::k_recon<2, true><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                              dev_err, cfmt, spin, fine);
-    else if (team == 2)
-        hpvcd::k_recon<2, false><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                               dev_err, cfmt, spin, fine);
+    if (cw == 2 && feat)
+        hpvcd::k_recon<2, true><<<grid, threads, smem, stream>>>(pics, items, n_items, work_counter, dev_err, cfmt,
+                                                                 spin, fine);
+    else if (cw == 2)
+        hpvcd::k_recon<2, false><<<grid, threads, smem, stream>>>(pics, items, n_items, work_counter, dev_err, cfmt,
+                                                                  spin, fine);
     else if (feat)
-        hpvcd::k_recon<1, true><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                              dev_err, cfmt, spin, fine);
+        hpvcd::k_recon<1, true><<<grid, threads, smem, stream>>>(pics, items, n_items, work_counter, dev_err, cfmt,
+                                                                 spin, fine);
     else
-        hpvcd::k_recon<1, false><<<grid, hpvcd::kReconThreads, smem, stream>>>(pics, items, n_items, work_counter,
-                                                                               dev_err, cfmt, spin, fine);
+        hpvcd::k_recon<1, false><<<grid, threads, smem, stream>>>(pics, items, n_items, work_counter, dev_err, cfmt,
+                                                                  spin, fine);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }
 
-extern "C" int hpvcd_recon_occupancy(int cfmt) {
+// CTAs per SM of the wavefront kernel with the layout of `cfmt` and one or
+// two chroma warps (raises the shared-memory limit of every instantiation
+// to the 4:4:4 layout of three warps, the largest).
+extern "C" int hpvcd_recon_occupancy(int cfmt, int chroma_warps) {
     int blocks = 0;
-    // raise the limit for the 4:4:4 layout, which covers every format
-    const size_t smem = hpvcd::ReconLayout(cfmt).total;
-    const int lim = (int)hpvcd::ReconLayout(hpvcd::kFmt444).total;
+    const int cw = chroma_warps == 2 ? 2 : 1;
+    const size_t smem = hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(cw)).total;
+    const int lim = (int)hpvcd::ReconLayout(hpvcd::kFmt444, hpvcd::recon_warps(2)).total;
     cudaFuncSetAttribute(hpvcd::k_recon<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     cudaFuncSetAttribute(hpvcd::k_recon<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     cudaFuncSetAttribute(hpvcd::k_recon<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     cudaFuncSetAttribute(hpvcd::k_recon<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<1, false>, hpvcd::kReconThreads, smem);
+    if (cw == 2)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<2, false>, 32 * hpvcd::recon_warps(2),
+                                                      smem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<1, false>, 32 * hpvcd::recon_warps(1),
+                                                      smem);
     return blocks;
 }

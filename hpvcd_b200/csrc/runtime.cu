@@ -24,7 +24,7 @@ extern "C" cudaError_t hpvcd_launch_ccp(const DevPic*, const uint32_t*, uint32_t
                                         cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_recon(const DevPic*, const CtuItem*, uint32_t, uint32_t*, uint32_t*, int, int,
                                           int, int, int, uint32_t, cudaStream_t);
-extern "C" int hpvcd_recon_occupancy(int cfmt);
+extern "C" int hpvcd_recon_occupancy(int cfmt, int chroma_warps);
 extern "C" hpvcd_status hpvcd_mlp_host_copy(hpvcd_mlp* M, float* params, float* lohi, int* has_domain);
 extern "C" uint32_t hpvcd_mlp_pick_host(const float* w, uint32_t K, const float* x, const float* lohi,
                                         int has_domain);
@@ -87,6 +87,9 @@ hpvcd_status validate(const hpvcd_picture& p) {
 }
 
 // Outputs written onto canvases (pictures placed by out->place).
+// k_recon shared-memory layout class of a picture: 0 4:2:0 / 4:0:0, 1 4:4:4, 2 4:2:2.
+int recon_class(const hpvcd_picture& p) { return p.chroma_idc == 3 ? 1 : (p.chroma_idc == 2 ? 2 : 0); }
+
 bool canvas_kind(uint32_t kind) { return kind == HPVCD_OUT_RGB8 || kind == HPVCD_OUT_YUV_CANVAS; }
 
 bool sao_active(const hpvcd_picture& p) {
@@ -95,7 +98,7 @@ bool sao_active(const hpvcd_picture& p) {
 
 struct Segment {
     uint32_t first_pic, n_pics;
-    uint32_t item_off, n_items;  // n_items: entries launched (one fewer while a test drops a CTU)
+    uint32_t wave_first, n_waves;  // the segment's wavefront launches (hpvcd_plan::waves)
     int max_dbk_v, max_dbk_h, max_sao;
     int max_rgb;  // RGB quads of the segment's largest picture
 };
@@ -196,8 +199,19 @@ struct hpvcd_plan {
     bool any_rgb_canvas = false, any_native_canvas = false;  // which output kernels run
     hpvcd_sched sched{};
     bool recon_feat = false;  // k_recon with slices / tiles, constrained intra or cross-component tests
-    int cfmt = 0;  // k_recon shared-memory layout: 0 4:2:0 / 4:0:0, 1 4:4:4 (fits all), 2 4:2:2
-    int recon_occ = 1;  // k_recon CTAs per SM at full occupancy
+    // Wavefront launches: per segment, one per chroma-format class of its
+    // pictures (k_recon shared-memory layout 0 4:2:0 / 4:0:0, 1 4:4:4, 2
+    // 4:2:2), so the pictures of one class get the CTAs per SM of their own
+    // layout.  item_off / n_full: the wave's range of the CTU work list;
+    // n_items: entries launched (one fewer while a test drops a CTU).
+    struct Wave {
+        uint32_t seg;
+        int cfmt;
+        uint32_t item_off, n_items, n_full;
+    };
+    std::vector<Wave> waves;
+    int occ[3][2] = {{1, 1}, {1, 1}, {1, 1}};  // k_recon CTAs per SM by class and chroma warps (1, 2)
+    int occ_of(int cfmt) const { return occ[cfmt][sched.chroma_warps == 2 ? 1 : 0]; }
     int sms = 148;
     int max_rgb = 0;  // largest RGB job of one picture, in 4-pixel quads
     uint32_t launches_per_run = 0;
@@ -238,7 +252,7 @@ struct hpvcd_plan {
                 for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
                     if ((src[i].flags & HPVCD_PIC_INTER) && src[i].n_pus) ++L;
                 if (rec_prefix[s.first_pic + s.n_pics] > rec_prefix[s.first_pic]) L += 1 + seg_ccp(s);
-                if (s.n_items) ++L;
+                for (uint32_t w = s.wave_first; w < s.wave_first + s.n_waves; ++w) L += waves[w].n_items > 0;
             }
             if (stages & HPVCD_STAGE_DEBLOCK) L += (s.max_dbk_v > 0) + (s.max_dbk_h > 0);
             if ((stages & HPVCD_STAGE_SAO) && s.max_sao > 0) ++L;
@@ -453,7 +467,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         P->out.kind = HPVCD_OUT_YUV;
     }
     if (sched) {
-        if (sched->idct > 1 || sched->luma_team > 2) {
+        if (sched->idct > 1 || sched->chroma_warps > 2) {
             delete P;
             return HPVCD_ERR_INVALID_ARG;
         }
@@ -464,8 +478,6 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         if (pics[i].ctb_region ||
             (pics[i].flags & (HPVCD_PIC_CONSTRAINED_INTRA | HPVCD_PIC_CROSS_COMPONENT | HPVCD_PIC_PCM)))
             P->recon_feat = true;
-        if (pics[i].chroma_idc == 3) P->cfmt = 1;
-        if (pics[i].chroma_idc == 2 && P->cfmt == 0) P->cfmt = 2;
         if (pics[i].flags & HPVCD_PIC_INTER) any_inter = true;
     }
     // ---- planes + scratch layout ----
@@ -514,8 +526,36 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             P->concurrent = P->segs.size() > 1;
         }
     }
-    const size_t n_seg = P->segs.size();
-    P->scratch_words = n_seg + 1 + ready_words;
+    // ---- wavefront schedule per segment and format class: CTUs sorted by
+    // (x + 2y, picture, y) ----
+    for (uint32_t si = 0; si < P->segs.size(); ++si) {
+        Segment& s = P->segs[si];
+        s.wave_first = (uint32_t)P->waves.size();
+        int max_t = 0;
+        for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
+            const Geo g = geo_of(pics[i]);
+            max_t = std::max(max_t, g.ctb_cols + 2 * g.ctb_rows);
+        }
+        for (int cls = 0; cls < 3; ++cls) {
+            const uint32_t off = (uint32_t)P->items.size();
+            for (int t = 0; t <= max_t; ++t)
+                for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
+                    const hpvcd_picture& p = pics[i];
+                    if (p.flags & HPVCD_PIC_PRED_IN_PLANE) continue;  // k_residual did it all
+                    if (recon_class(p) != cls) continue;
+                    const Geo g = geo_of(p);
+                    for (int y = 0; y < g.ctb_rows; ++y) {
+                        const int x = t - 2 * y;
+                        if (x >= 0 && x < g.ctb_cols) P->items.push_back(CtuItem{i, (uint16_t)x, (uint16_t)y});
+                    }
+                }
+            const uint32_t cnt = (uint32_t)P->items.size() - off;
+            if (cnt) P->waves.push_back(hpvcd_plan::Wave{si, cls, off, cnt, cnt});
+        }
+        s.n_waves = (uint32_t)P->waves.size() - s.wave_first;
+    }
+    const size_t n_waves = P->waves.size();
+    P->scratch_words = n_waves + 1 + ready_words;
     size_t res_bytes = 0;
     std::vector<size_t> res_off(n);
     for (uint32_t i = 0; i < n; ++i) {
@@ -579,7 +619,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         d.fin[1] = fb + align_up(g.luma_bytes, 256);
         d.fin[2] = fb + align_up(g.luma_bytes, 256) + align_up(g.chroma_bytes, 256);
         if (!p.chroma_idc) d.rec[1] = d.rec[2] = d.fin[1] = d.fin[2] = nullptr;
-        d.ready = P->d_scratch + n_seg + 1 + ready_off[i];
+        d.ready = P->d_scratch + n_waves + 1 + ready_off[i];
         {
             unsigned char* rb = P->d_res + res_off[i];
             d.res_stride[0] = res_stride_of(g.w);
@@ -659,22 +699,8 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
                     P->pics[i].ref_pic[l][r] = ext_of[(size_t)en];
                 }
     }
-    // ---- wavefront schedule per segment: sort CTUs by (x + 2y, picture, x) ----
+    // ---- filter and output job sizes per segment ----
     for (Segment& s : P->segs) {
-        s.item_off = (uint32_t)P->items.size();
-        int max_t = 0;
-        for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i)
-            max_t = std::max(max_t, P->pics[i].ctb_cols + 2 * P->pics[i].ctb_rows);
-        for (int t = 0; t <= max_t; ++t)
-            for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
-                const DevPic& d = P->pics[i];
-                if (!d.needs_wavefront) continue;  // prediction in plane: k_residual did it all
-                for (int y = 0; y < d.ctb_rows; ++y) {
-                    const int x = t - 2 * y;
-                    if (x >= 0 && x < d.ctb_cols) P->items.push_back(CtuItem{i, (uint16_t)x, (uint16_t)y});
-                }
-            }
-        s.n_items = (uint32_t)P->items.size() - s.item_off;
         for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
             const DevPic& d = P->pics[i];
             const int lv = (d.w >= 12 ? (d.w - 4) / 8 : 0) * (d.h / 4);
@@ -706,7 +732,8 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
     P->sms = sms;
-    P->recon_occ = std::max(1, hpvcd_recon_occupancy(P->cfmt));
+    for (int cls = 0; cls < 3; ++cls)
+        for (int cw = 1; cw <= 2; ++cw) P->occ[cls][cw - 1] = std::max(1, hpvcd_recon_occupancy(cls, cw));
     if (P->concurrent) {
         GroupStreams* set = lend ? lend : &P->own;
         const cudaError_t ce = set->create();
@@ -731,7 +758,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
         if (e != cudaSuccess) return cuda_status(e);
     }
     const uint32_t n_seg = (uint32_t)P->segs.size();
-    uint32_t* d_err = P->d_scratch + n_seg;
+    uint32_t* d_err = P->d_scratch + P->waves.size();
     if (stages & HPVCD_STAGE_RECON) {
         for (size_t i = 0; i < P->src.size(); ++i) {
             const hpvcd_picture& p = P->src[i];
@@ -770,15 +797,20 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
                 e = hpvcd_launch_ccp(P->d_pics + s.first_pic, P->d_prefix + s.first_pic, s.n_pics, nrec, d_err,
                                      P->sms, st);
             if (e != cudaSuccess) return cuda_status(e);
-            int occ = P->recon_occ;
-            if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
-            // concurrent segments share the SMs: each gets its share of the CTAs
-            const int share = P->concurrent ? std::max(1, P->sms * occ / (int)n_seg) : P->sms * occ;
-            const int grid = std::max(1, std::min<int>(share, (int)s.n_items));
-            e = hpvcd_launch_recon(P->d_pics, P->d_items + s.item_off, s.n_items, P->d_scratch + si, d_err,
-                                   P->cfmt, grid, (int)P->sched.luma_team, P->recon_feat ? 1 : 0,
-                                   P->sched.wave ? 0 : 1, P->spin_limit, st);
-            if (e != cudaSuccess) return cuda_status(e);
+            // the segment's format classes one after another, each wave with
+            // its own layout and work counter
+            for (uint32_t w = s.wave_first; w < s.wave_first + s.n_waves; ++w) {
+                const hpvcd_plan::Wave& wv = P->waves[w];
+                int occ = P->occ_of(wv.cfmt);
+                if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
+                // concurrent segments share the SMs: each gets its share of the CTAs
+                const int share = P->concurrent ? std::max(1, P->sms * occ / (int)n_seg) : P->sms * occ;
+                const int grid = std::max(1, std::min<int>(share, (int)wv.n_items));
+                e = hpvcd_launch_recon(P->d_pics, P->d_items + wv.item_off, wv.n_items, P->d_scratch + w, d_err,
+                                       wv.cfmt, grid, (int)P->sched.chroma_warps, P->recon_feat ? 1 : 0,
+                                       P->sched.wave ? 0 : 1, P->spin_limit, st);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
         }
         if (stages & HPVCD_STAGE_DEBLOCK) {
             e = hpvcd_launch_deblock(dp, (int)s.n_pics, s.max_dbk_v, 1, st);
@@ -1226,7 +1258,7 @@ HPVCD_API hpvcd_status hpvcd_plan_autotune(hpvcd_plan* plan, const hpvcd_sched* 
 HPVCD_API hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched) {
     if (!plan) return HPVCD_ERR_INVALID_ARG;
     const hpvcd_sched next = sched ? *sched : hpvcd_sched{};
-    if (next.idct > 1 || next.luma_team > 2 || next.wave > 1) return HPVCD_ERR_INVALID_ARG;
+    if (next.idct > 1 || next.chroma_warps > 2 || next.wave > 1) return HPVCD_ERR_INVALID_ARG;
     if (std::memcmp(&next, &plan->sched, sizeof(next)) == 0) return HPVCD_OK;
     plan->sched = next;
     // graphs captured with the previous schedule hold its kernels
@@ -1247,15 +1279,14 @@ HPVCD_API hpvcd_status hpvcd_plan_set_wait_test(hpvcd_plan* plan, uint32_t spin_
     if (!plan || drop_ctu < -1 || (drop_ctu >= 0 && (size_t)drop_ctu >= plan->items.size()))
         return HPVCD_ERR_INVALID_ARG;
     std::vector<CtuItem> list = plan->items;
-    for (size_t si = 0; si < plan->segs.size(); ++si) {
-        Segment& sg = plan->segs[si];
-        const uint32_t end = si + 1 < plan->segs.size() ? plan->segs[si + 1].item_off : (uint32_t)plan->items.size();
-        sg.n_items = end - sg.item_off;
-        if (drop_ctu >= 0 && (uint32_t)drop_ctu >= sg.item_off && (uint32_t)drop_ctu < end) {
-            // the segment's later entries move up by one; its last slot is not launched
+    for (hpvcd_plan::Wave& wv : plan->waves) {
+        const uint32_t end = wv.item_off + wv.n_full;
+        wv.n_items = wv.n_full;
+        if (drop_ctu >= 0 && (uint32_t)drop_ctu >= wv.item_off && (uint32_t)drop_ctu < end) {
+            // the wave's later entries move up by one; its last slot is not launched
             list.erase(list.begin() + drop_ctu);
             list.insert(list.begin() + (end - 1), plan->items[(size_t)drop_ctu]);
-            sg.n_items -= 1;
+            wv.n_items -= 1;
         }
     }
     if (!list.empty()) {
@@ -1632,7 +1663,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     {
         if (others > 0) {
             hpvcd_sched s2 = slot->plan->sched;
-            const int occ = std::max(1, slot->plan->recon_occ);
+            const int occ = std::max(1, slot->plan->occ_of(0));
             const int share = std::max(1, occ / (others + 1));
             const int cur = s2.recon_ctas_per_sm ? (int)s2.recon_ctas_per_sm : occ;
             s2.recon_ctas_per_sm = (uint32_t)std::min(cur, share);
@@ -1823,7 +1854,7 @@ hpvcd_status noalloc_setup(int dev, NoAllocDevice** out) {
         if (e != cudaSuccess) return cuda_status(e);
         e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return cuda_status(e);
-        for (int f = 0; f < 3; ++f) d.occ[f] = std::max(1, hpvcd_recon_occupancy(f));
+        for (int f = 0; f < 3; ++f) d.occ[f] = std::max(1, hpvcd_recon_occupancy(f, 1));
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_status(e);
         d.base = (unsigned char*)p;

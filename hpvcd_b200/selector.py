@@ -3,9 +3,10 @@
 The schedule of a batch (include/hpvcd_gpu.h `hpvcd_sched`) picks kernel
 variants that never change pixels: the inverse transform of k_residual
 (matrix product with zero rows / columns skipped, or even-odd butterflies for
-16x16 / 32x32), the team size of the luma intra walk in k_recon (one warp, or
-two for 16x16 / 32x32 TBs) and the persistent k_recon CTAs per SM (occupancy
-maximum, or one).  Which is fastest depends on the batch: its TB-size mix,
+16x16 / 32x32), the chroma warps of the wavefront kernel k_recon (one warp
+walking Cb then Cr in a CTA of two warps, or one warp per chroma component in
+a CTA of three) and the persistent k_recon CTAs per SM (occupancy maximum, or
+one).  Which is fastest depends on the batch: its TB-size mix,
 coefficient density, QP, intra share, size and picture count.
 
 * Exhaustive autotuning (`hpvcd_plan_autotune`) times every schedule on the
@@ -38,7 +39,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS_PATH = os.path.join(HERE, "selector_weights.npz")
 
 # The candidate schedules, in output order of the network.
-SCHEDULES = [abi.Sched(idct, team, ctas, 0) for idct in (0, 1) for team in (1, 2) for ctas in (0, 1)]
+SCHEDULES = [abi.Sched(idct, cw, ctas, 0) for idct in (0, 1) for cw in (1, 2) for ctas in (0, 1)]
 DEFAULT = 0  # (matrix transform, one-warp walk, occupancy maximum): the all-zero schedule
 K = len(SCHEDULES)
 
@@ -140,7 +141,7 @@ class Mlp:
         if getattr(self, "domain", None) is not None:
             extra = {"domain_lo": self.domain[0], "domain_hi": self.domain[1]}
         np.savez(path, params=self.params(master=True), n_variants=self.K,
-                 schedules=np.array([[s.idct, s.luma_team, s.recon_ctas_per_sm] for s in SCHEDULES], np.int32),
+                 schedules=np.array([[s.idct, s.chroma_warps, s.recon_ctas_per_sm] for s in SCHEDULES], np.int32),
                  **extra)
 
     @classmethod

@@ -470,7 +470,8 @@ typedef struct hpvcd_plan hpvcd_plan;
 typedef struct hpvcd_sched {
     uint32_t idct;              /* k_residual inverse transform: 0 matrix product with all-zero
                                    rows / columns skipped, 1 even-odd butterflies for 16x16 / 32x32 */
-    uint32_t luma_team;         /* warps predicting a 16x16 / 32x32 luma intra TB: 0|1 one, 2 two */
+    uint32_t chroma_warps;      /* chroma walk of the wavefront kernel: 0|1 one warp (Cb, then Cr;
+                                   two warps per CTA), 2 one warp per component (three per CTA) */
     uint32_t recon_ctas_per_sm; /* persistent wavefront CTAs per SM (0 -> occupancy max) */
     uint32_t wave;              /* wavefront synchronisation: 0 per quadrant (a CTU is walked while
                                    its left / above-right neighbours still are), 1 whole CTUs (one

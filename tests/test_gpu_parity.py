@@ -419,14 +419,14 @@ def test_schedule_variants_bit_exact():
     ref, _ = O.decode_batch(pics)
     plan = DevicePlan(pics)
     for idct in (0, 1):
-        for team in (1, 2):
+        for cw in (1, 2):       # chroma warps of the wavefront kernel
             for ctas in (0, 1):
                 for wave in (0, 1):   # quadrant-level / whole-CTU wavefront
-                    plan.set_sched(abi.Sched(idct, team, ctas, wave))
+                    plan.set_sched(abi.Sched(idct, cw, ctas, wave))
                     plan.launch()
                     assert plan.status() == abi.OK
                     got = [plan.planes(i) for i in range(len(pics))]
-                    assert_planes_equal(got, ref, f"idct={idct} team={team} ctas={ctas} wave={wave}")
+                    assert_planes_equal(got, ref, f"idct={idct} chroma_warps={cw} ctas={ctas} wave={wave}")
     with pytest.raises(abi.HpvcdError):
         plan.set_sched(abi.Sched(0, 1, 0, 2))
     plan.close()
