@@ -79,6 +79,7 @@ OUT_YUV, OUT_RGB8, OUT_YUV_CANVAS = 0, 1, 2
 MATRIX_IDENTITY, MATRIX_BT709, MATRIX_BT470BG = 0, 1, 5
 MATRIX_SMPTE170M, MATRIX_YCGCO, MATRIX_BT2020NCL = 6, 8, 9
 CANVAS_NATIVE = 0x100  # hpvcd_canvas.matrix: native YCbCr planes on an RGB8 output
+OUTPUT_CANVAS_ONLY = 0x1  # hpvcd_output.options: RGB8 canvases only, final planes not kept
 
 STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_OUTPUT = 0x1, 0x2, 0x4, 0x8
 STAGE_ALL = 0xF
@@ -205,7 +206,7 @@ class Output(C.Structure):
                 ("canvas_w", C.c_uint32), ("canvas_h", C.c_uint32), ("place", C.c_void_p),
                 ("host_dst", C.c_void_p), ("host_dst_bytes", C.c_uint64),
                 ("n_canvases", C.c_uint32), ("canvases", C.c_void_p), ("canvas_dst", C.c_void_p),
-                ("orientation", C.c_uint32)]
+                ("orientation", C.c_uint32), ("options", C.c_uint32)]
 
 
 class ServerCfg(C.Structure):

@@ -46,6 +46,7 @@ struct DevPic {
     int32_t canvas_w, canvas_h, matrix, full_range;
     int32_t orientation;  // HPVCD_ORIENT_* of the canvas (0 normal)
     int32_t needs_wavefront;
+    int32_t write_fin;  // the tile filter kernel writes the final planes (else only the canvas)
 };
 
 // Work item of the reconstruction kernel: one CTU of one picture.

@@ -13,6 +13,7 @@
 //
 // RGB (yuv.rs:187-393 Q13 matrix, lib.rs:1964-1978 rgb8 narrowing,
 // lib.rs:1610-1660 tile placement and cropping on the canvas).
+#include <algorithm>
 #include <type_traits>
 
 #include "common.cuh"
@@ -50,9 +51,25 @@ __device__ __forceinline__ void slice_offsets(const DevPic& P, int qx, int qy, i
     }
 }
 
+// Sample accessors of the deblocking segments, in plane coordinates: a
+// plane in global memory, or a region of it staged in shared memory.
+struct GPlane {
+    void* p;
+    int w, bps;
+    __device__ int ld(int x, int y) const { return load_sample(p, bps, (size_t)y * w + x); }
+    __device__ void st(int x, int y, int v) const { store_sample(p, bps, (size_t)y * w + x, v); }
+};
+struct SPlane {
+    uint16_t* s;
+    int x0, y0, rw;  // plane coordinates of region entry 0, region row length
+    __device__ int ld(int x, int y) const { return s[(y - y0) * rw + (x - x0)]; }
+    __device__ void st(int x, int y, int v) const { s[(y - y0) * rw + (x - x0)] = (uint16_t)v; }
+};
+
 // Luma segment: 8 taps x 4 lines around the edge, in registers.
 // v[line][tap+4] with tap -4..3 (p3..p0, q0..q3).
-__device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan) {
+template <class Pl>
+__device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& pl) {
     const int mid = scan + 1;
     const hpvcd_cell& q = vertical ? cell_at(P, edge, mid) : cell_at(P, mid, edge);
     const int bs = vertical ? q.bs_v : q.bs_h;
@@ -66,17 +83,20 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan)
     const int beta = c_beta[clamp3i(avg + 2 * bo, 0, 51)] << sh;
     const int tc = c_tc[clamp3i(avg + 2 * (bs - 1) + 2 * to, 0, 53)] << sh;
     if (tc == 0) return;
-    const int w = P.w;
-    void* pl = P.rec[0];
-    const int bps = P.bps;
     int v[4][8];
-    auto idx = [&](int line, int tap) -> size_t {
-        return vertical ? (size_t)(scan + line) * w + (edge + tap) : (size_t)(edge + tap) * w + (scan + line);
+    auto ld = [&](int line, int tap) {
+        return vertical ? pl.ld(edge + tap, scan + line) : pl.ld(scan + line, edge + tap);
+    };
+    auto st = [&](int line, int tap, int val) {
+        if (vertical)
+            pl.st(edge + tap, scan + line, val);
+        else
+            pl.st(scan + line, edge + tap, val);
     };
 #pragma unroll
     for (int l = 0; l < 4; ++l)
 #pragma unroll
-        for (int t = 0; t < 8; ++t) v[l][t] = load_sample(pl, bps, idx(l, t - 4));
+        for (int t = 0; t < 8; ++t) v[l][t] = ld(l, t - 4);
     // deblock.rs:216-238 luma_decision (lines 0 and 3)
     auto g = [&](int l, int tap) { return v[l][tap + 4]; };
     const int dp0 = abs(g(0, -3) - 2 * g(0, -2) + g(0, -1));
@@ -103,31 +123,31 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan)
         if (strong) {  // deblock.rs:605-616
             auto c = [&](int o, int x) { return clamp3i(clamp3i(x, o - 2 * tc, o + 2 * tc), 0, maxv); };
             if (!ex_p) {
-                store_sample(pl, bps, idx(l, -1), c(p0, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3));
-                store_sample(pl, bps, idx(l, -2), c(p1, (p2 + p1 + p0 + q0 + 2) >> 2));
-                store_sample(pl, bps, idx(l, -3), c(p2, (2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3));
+                st(l, -1, c(p0, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3));
+                st(l, -2, c(p1, (p2 + p1 + p0 + q0 + 2) >> 2));
+                st(l, -3, c(p2, (2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3));
             }
             if (!ex_q) {
-                store_sample(pl, bps, idx(l, 0), c(q0, (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3));
-                store_sample(pl, bps, idx(l, 1), c(q1, (p0 + q0 + q1 + q2 + 2) >> 2));
-                store_sample(pl, bps, idx(l, 2), c(q2, (p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3));
+                st(l, 0, c(q0, (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3));
+                st(l, 1, c(q1, (p0 + q0 + q1 + q2 + 2) >> 2));
+                st(l, 2, c(q2, (p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3));
             }
         } else {  // deblock.rs:617-631
             const int delta0 = (9 * (q0 - p0) - 3 * (q1 - p1) + 8) >> 4;
             if (abs(delta0) < tc * 10) {
                 const int delta = clamp3i(delta0, -tc, tc);
                 if (!ex_p) {
-                    store_sample(pl, bps, idx(l, -1), clamp3i(p0 + delta, 0, maxv));
+                    st(l, -1, clamp3i(p0 + delta, 0, maxv));
                     if (do_p1) {
                         const int dp1 = clamp3i((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -tc2, tc2);
-                        store_sample(pl, bps, idx(l, -2), clamp3i(p1 + dp1, 0, maxv));
+                        st(l, -2, clamp3i(p1 + dp1, 0, maxv));
                     }
                 }
                 if (!ex_q) {
-                    store_sample(pl, bps, idx(l, 0), clamp3i(q0 - delta, 0, maxv));
+                    st(l, 0, clamp3i(q0 - delta, 0, maxv));
                     if (do_q1) {
                         const int dq1 = clamp3i((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -tc2, tc2);
-                        store_sample(pl, bps, idx(l, 1), clamp3i(q1 + dq1, 0, maxv));
+                        st(l, 1, clamp3i(q1 + dq1, 0, maxv));
                     }
                 }
             }
@@ -136,7 +156,8 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan)
 }
 
 // Chroma segment (decode.rs:2036-2137): 4 chroma lines, both Cb and Cr.
-__device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int scan) {
+template <class Pl>
+__device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& cb, const Pl& cr) {
     const int mid = scan + 1;
     const int lex = vertical ? edge * P.sub_w : mid * P.sub_w;
     const int ley = vertical ? mid * P.sub_h : edge * P.sub_h;
@@ -159,39 +180,26 @@ __device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int sca
     (void)bo;
     const int sh = P.bd_c - 8;
     const int maxv = (1 << P.bd_c) - 1;
-    const int cw = P.cw;
     const int scan_max = vertical ? P.ch : P.cw;
     for (int plane = 0; plane < 2; ++plane) {
         const int off = plane == 0 ? P.pps_cb_qp_offset : P.pps_cr_qp_offset;
         const int qc = qpc_map(avg + off, P.idc, P.bd_c);
         const int tc = c_tc[clamp3i(qc + 2 + 2 * to, 0, 53)] << sh;
         if (tc == 0) continue;
-        void* pl = P.rec[1 + plane];
+        const Pl& pl = plane == 0 ? cb : cr;
         for (int s = scan; s < scan + 4; ++s) {
             if (s >= scan_max) continue;
-            size_t ip0, ip1, iq0, iq1;
-            int pxl, pyl, qxl, qyl;  // luma positions of p0 / q0 for exemption
-            if (vertical) {
-                ip0 = (size_t)s * cw + edge - 1;
-                ip1 = ip0 - 1;
-                iq0 = (size_t)s * cw + edge;
-                iq1 = iq0 + 1;
-                pxl = (edge - 1) * P.sub_w; pyl = s * P.sub_h;
-                qxl = edge * P.sub_w; qyl = s * P.sub_h;
-            } else {
-                ip0 = (size_t)(edge - 1) * cw + s;
-                ip1 = (size_t)(edge - 2) * cw + s;
-                iq0 = (size_t)edge * cw + s;
-                iq1 = (size_t)(edge + 1) * cw + s;
-                pxl = s * P.sub_w; pyl = (edge - 1) * P.sub_h;
-                qxl = s * P.sub_w; qyl = edge * P.sub_h;
-            }
-            const int p0 = load_sample(pl, P.bps, ip0), p1 = load_sample(pl, P.bps, ip1);
-            const int q0 = load_sample(pl, P.bps, iq0), q1 = load_sample(pl, P.bps, iq1);
+            // p1, p0 | q0, q1 across the edge, in chroma plane coordinates
+            const int xp0 = vertical ? edge - 1 : s, yp0 = vertical ? s : edge - 1;
+            const int xp1 = vertical ? edge - 2 : s, yp1 = vertical ? s : edge - 2;
+            const int xq0 = vertical ? edge : s, yq0 = vertical ? s : edge;
+            const int xq1 = vertical ? edge + 1 : s, yq1 = vertical ? s : edge + 1;
+            const int p0 = pl.ld(xp0, yp0), p1 = pl.ld(xp1, yp1);
+            const int q0 = pl.ld(xq0, yq0), q1 = pl.ld(xq1, yq1);
             const int delta = clamp3i((((q0 - p0) * 4 + p1 - q1 + 4) >> 3), -tc, tc);
-            if (delta != 0) {
-                if (!exempt_at(P, pxl, pyl)) store_sample(pl, P.bps, ip0, clamp3i(p0 + delta, 0, maxv));
-                if (!exempt_at(P, qxl, qyl)) store_sample(pl, P.bps, iq0, clamp3i(q0 - delta, 0, maxv));
+            if (delta != 0) {  // exemption by the luma positions of p0 / q0
+                if (!exempt_at(P, xp0 * P.sub_w, yp0 * P.sub_h)) pl.st(xp0, yp0, clamp3i(p0 + delta, 0, maxv));
+                if (!exempt_at(P, xq0 * P.sub_w, yq0 * P.sub_h)) pl.st(xq0, yq0, clamp3i(q0 - delta, 0, maxv));
             }
         }
     }
@@ -211,7 +219,7 @@ __global__ void k_deblock(const DevPic* __restrict__ pics, int vertical) {
         // same rows; horizontal edges: neighbouring segments of the same edge
         const int e = vertical ? id % n_edges : id / n_segs;
         const int s = vertical ? id / n_edges : id % n_segs;
-        luma_segment(P, vertical != 0, 8 * (e + 1), 4 * s);
+        luma_segment(P, vertical != 0, 8 * (e + 1), 4 * s, GPlane{P.rec[0], P.w, P.bps});
     } else {
         if (P.idc == 0) return;
         const int edge_max = vertical ? P.cw : P.ch, scan_max = vertical ? P.ch : P.cw;
@@ -220,7 +228,8 @@ __global__ void k_deblock(const DevPic* __restrict__ pics, int vertical) {
         if (id >= n_edges * n_segs) return;
         const int e = vertical ? id % n_edges : id / n_segs;
         const int s = vertical ? id / n_edges : id % n_segs;
-        chroma_segment(P, vertical != 0, 8 * (e + 1), 4 * s);
+        chroma_segment(P, vertical != 0, 8 * (e + 1), 4 * s, GPlane{P.rec[1], P.cw, P.bps},
+                       GPlane{P.rec[2], P.cw, P.bps});
     }
 }
 
@@ -545,6 +554,286 @@ __global__ void k_yuv_canvas(const DevPic* __restrict__ pics, uint8_t* __restric
     }
 }
 
+// ===========================================================================
+// k_filter_tile -- deblocking, SAO and the output of one 64 x 64 luma tile
+// (and its chroma) per CTA, in shared memory.
+//
+// The tile is staged with 8 columns and 4 rows of halo on every side.  The
+// vertical-edge pass runs over every 4-line segment of the staged rows whose
+// edge lies in [X, X + 64], the horizontal-edge pass over every 4-column
+// segment of the staged columns X - 4 .. X + 67 whose edge lies in [Y, Y + 64]:
+// each segment reads and writes only samples of its own lines within 4 of
+// its edge, so the staged samples the SAO of the tile reads (one ring around
+// it) get exactly the values of the reference's whole-picture vertical pass
+// followed by its horizontal pass (decode.rs:1774-2146).  SAO then reads
+// those deblocked samples (the reference's snapshot, decode.rs:2258-2493) and
+// its results replace them in place only after every thread has read its
+// neighbours.  Finally the tile's final samples go to the picture's final
+// planes (unless the caller asked for its canvas only) and, for an RGB8
+// canvas, are converted and stored at their canvas position.  The kernel
+// reads `rec` and writes `fin`, which are always different planes.
+// ===========================================================================
+constexpr int kTile = 64;
+constexpr int kTileThreads = 256;
+
+// Region of one component: the tile (tw x th samples at (tx, ty)) with 8
+// columns and 4 rows of halo; row length tw + 16 (a multiple of 8 entries).
+struct TileComp {
+    int tx, ty, tw, th, pw, ph;
+    SPlane sp;
+    __device__ int rw() const { return tw + 16; }
+    __device__ int rh() const { return th + 8; }
+};
+
+__host__ __device__ inline size_t tile_comp_entries(int tw, int th) { return (size_t)(tw + 16) * (th + 8); }
+// Shared memory of a k_filter_tile CTA for the chroma-format class cfmt
+// (0 4:2:0 / 4:0:0, 1 4:4:4, 2 4:2:2).
+__host__ __device__ inline size_t tile_smem_bytes(int cfmt) {
+    const int tw = cfmt == 1 ? 64 : 32, th = cfmt == 0 ? 32 : 64;
+    return (tile_comp_entries(64, 64) + 2 * tile_comp_entries(tw, th)) * sizeof(uint16_t);
+}
+
+// SAO of sample (x, y) of component c, s0 its deblocked value (sao.rs:179-330,
+// the driver decode.rs:2258-2493): band offset in place, edge offset from
+// the deblocked neighbours, picture-border samples and exempt cells
+// unchanged; rmask: bits of the CTB regions (slice << 8 | tile) that must
+// agree across an edge-offset neighbour (0: no restriction).
+template <bool kGated, class Pl>
+__device__ __forceinline__ int sao_sample(const DevPic& P, int c, int x, int y, int s0, const Pl& src, uint32_t rmask) {
+    const bool on = c == 0 ? (P.flags & HPVCD_PIC_SAO_LUMA) != 0 : (P.flags & HPVCD_PIC_SAO_CHROMA) != 0;
+    if (!on || !P.sao) return s0;
+    const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
+    if (P.cells && exempt_at(P, x * sw, y * sh)) return s0;  // exempt cells keep the deblocked sample
+    const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+    const hpvcd_sao_comp sc = P.sao[(size_t)((y * sh) >> P.log2_ctb) * P.ctb_cols + ((x * sw) >> P.log2_ctb)].comp[c];
+    const int bd = c ? P.bd_c : P.bd;
+    const int mx = (1 << bd) - 1;
+    if (sc.type_idx == 1) {  // sao.rs:205-233
+        const uint8_t rel = (uint8_t)((uint8_t)(s0 >> (bd - 5)) - sc.band_pos);
+        return rel < 4 ? clamp3i(s0 + sc.offsets[rel], 0, mx) : s0;
+    }
+    if (sc.type_idx != 2) return s0;
+    int dx, dy;  // sao.rs:266-330
+    switch (sc.eo_class) {
+        case 0: dx = 1; dy = 0; break;
+        case 1: dx = 0; dy = 1; break;
+        case 2: dx = 1; dy = 1; break;
+        default: dx = 1; dy = -1; break;
+    }
+    const int x1 = x + dx, y1 = y + dy, x2 = x - dx, y2 = y - dy;
+    if (x1 < 0 || y1 < 0 || x1 >= pw || y1 >= ph || x2 < 0 || y2 < 0 || x2 >= pw || y2 >= ph) return s0;
+    if (kGated && rmask) {  // slice / tile boundaries SAO may not cross (sao.rs:380-414)
+        auto region = [&](int ax, int ay) {
+            return (uint32_t)P.ctb_region[(size_t)((ay * sh) >> P.log2_ctb) * P.ctb_cols + ((ax * sw) >> P.log2_ctb)];
+        };
+        const uint32_t r0 = region(x, y);
+        if (((r0 ^ region(x1, y1)) & rmask) || ((r0 ^ region(x2, y2)) & rmask)) return s0;
+    }
+    const int n1 = src.ld(x1, y1), n2 = src.ld(x2, y2);
+    const int e = ((s0 > n1) - (s0 < n1)) + ((s0 > n2) - (s0 < n2)) + 2;
+    const int o = e == 0 ? sc.offsets[0] : (e == 1 ? sc.offsets[1] : (e == 3 ? sc.offsets[2] : (e == 4 ? sc.offsets[3] : 0)));
+    return o ? clamp3i(s0 + o, 0, mx) : s0;
+}
+
+// Eight horizontally adjacent samples of a plane row at (x, y), as uint16,
+// zero outside the plane.  Vector load when the whole group is inside and
+// 16-byte aligned.
+__device__ __forceinline__ uint4 load8(const void* plane, int bps, int pw, int ph, int x, int y) {
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    if (y < 0 || y >= ph || x + 8 <= 0 || x >= pw) return make_uint4(0u, 0u, 0u, 0u);
+    const size_t idx = (size_t)y * pw + x;
+    if (x >= 0 && x + 8 <= pw) {
+        if (bps == 2 && (idx & 7) == 0) return *(const uint4*)((const uint16_t*)plane + idx);
+        if (bps == 1 && (idx & 7) == 0) {
+            const uint2 b = *(const uint2*)((const uint8_t*)plane + idx);
+            w[0] = (b.x & 0xffu) | ((b.x & 0xff00u) << 8);
+            w[1] = ((b.x >> 16) & 0xffu) | ((b.x >> 8) & 0xff0000u);
+            w[2] = (b.y & 0xffu) | ((b.y & 0xff00u) << 8);
+            w[3] = ((b.y >> 16) & 0xffu) | ((b.y >> 8) & 0xff0000u);
+            return make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int xx = x + i;
+        const uint32_t v = (xx >= 0 && xx < pw) ? (uint32_t)load_sample(plane, bps, idx + i) : 0u;
+        w[i >> 1] |= v << (16 * (i & 1));
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+template <bool kGated>
+__global__ void __launch_bounds__(kTileThreads)
+k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rgb) {
+    extern __shared__ __align__(16) uint16_t tsm[];
+    const DevPic& P = pics[blockIdx.y];
+    const int tid = threadIdx.x;
+    const int tiles_x = (P.w + kTile - 1) / kTile, tiles_y = (P.h + kTile - 1) / kTile;
+    const int ncomp = P.idc ? 3 : 1;
+    const bool deblock = (P.flags & HPVCD_PIC_DEBLOCK) && P.cells;
+    const bool do_rgb = rgb && out && P.matrix != (int)HPVCD_CANVAS_NATIVE;
+    const uint32_t rmask = (kGated && P.ctb_region) ? (((P.flags & HPVCD_PIC_SAO_NO_ACROSS_SLICES) ? 0xff00u : 0u) |
+                                                       ((P.flags & HPVCD_PIC_SAO_NO_ACROSS_TILES) ? 0x00ffu : 0u))
+                                                    : 0u;
+    for (int t = blockIdx.x; t < tiles_x * tiles_y; t += gridDim.x) {
+        const int X = (t % tiles_x) * kTile, Y = (t / tiles_x) * kTile;
+        TileComp tc[3];
+        size_t off = 0;
+        for (int c = 0; c < 3; ++c) {
+            const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
+            TileComp& k = tc[c];
+            k.tx = X / sw; k.ty = Y / sh; k.tw = kTile / sw; k.th = kTile / sh;
+            k.pw = c ? P.cw : P.w; k.ph = c ? P.ch : P.h;
+            k.sp = SPlane{tsm + off, k.tx - 8, k.ty - 4, k.tw + 16};
+            off += tile_comp_entries(k.tw, k.th);
+        }
+        // ---- 1. stage the tile and its halo (8 samples per copy) ----
+        __syncthreads();  // the previous tile's readers are done
+        for (int c = 0; c < ncomp; ++c) {
+            const TileComp& k = tc[c];
+            const int chunks = k.rw() >> 3;
+            for (int i = tid; i < k.rh() * chunks; i += kTileThreads) {
+                const int r = i / chunks, q = i - r * chunks;
+                *(uint4*)(k.sp.s + r * k.rw() + 8 * q) =
+                    load8(P.rec[c], P.bps, k.pw, k.ph, k.sp.x0 + 8 * q, k.sp.y0 + r);
+            }
+        }
+        __syncthreads();
+        if (deblock) {
+            // ---- 2. vertical edges, then 3. horizontal edges ----
+            const TileComp& Lc = tc[0];
+            const TileComp& Cb = tc[1];
+            const int nec_v = Cb.tw / 8 + 1, nsc_v = Cb.rh() / 4;        // chroma V: edges, segments
+            const int nec_h = Cb.th / 8 + 1, nsc_h = (Cb.tw + 8) / 4;    // chroma H
+            for (int pass = 0; pass < 2; ++pass) {
+                const bool vertical = pass == 0;
+                const int n_luma = 9 * 18;
+                const int n_chroma = P.idc ? (vertical ? nec_v * nsc_v : nec_h * nsc_h) : 0;
+                for (int j = tid; j < n_luma + n_chroma; j += kTileThreads) {
+                    if (j < n_luma) {
+                        const int e = (vertical ? X : Y) + 8 * (j % 9);
+                        const int scan = (vertical ? Y - 4 : X - 4) + 4 * (j / 9);
+                        const int emax = vertical ? P.w : P.h, smax = vertical ? P.h : P.w;
+                        if (e >= 8 && e <= emax - 4 && scan >= 0 && scan + 4 <= smax)
+                            luma_segment(P, vertical, e, scan, Lc.sp);
+                    } else {
+                        const int jj = j - n_luma;
+                        const int ne = vertical ? nec_v : nec_h;
+                        const int e = (vertical ? Cb.tx : Cb.ty) + 8 * (jj % ne);
+                        const int scan = (vertical ? Cb.ty - 4 : Cb.tx - 4) + 4 * (jj / ne);
+                        const int emax = vertical ? P.cw : P.ch, smax = vertical ? P.ch : P.cw;
+                        if (e >= 8 && e <= emax - 2 && scan >= 0 && scan + 4 <= smax)
+                            chroma_segment(P, vertical, e, scan, Cb.sp, tc[2].sp);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        // ---- 4. SAO: every result computed from the deblocked samples,
+        // then written back ----
+        if (P.sao && (P.flags & (HPVCD_PIC_SAO_LUMA | HPVCD_PIC_SAO_CHROMA))) {
+            for (int c = 0; c < ncomp; ++c) {
+                const TileComp& k = tc[c];
+                constexpr int kMax = kTile * kTile / kTileThreads;  // samples per thread (16)
+                int res[kMax];
+                const int n = k.tw * k.th;
+#pragma unroll
+                for (int r = 0; r < kMax; ++r) {
+                    const int i = tid + r * kTileThreads;
+                    res[r] = -1;
+                    if (i >= n) continue;
+                    const int x = k.tx + i % k.tw, y = k.ty + i / k.tw;
+                    if (x >= k.pw || y >= k.ph) continue;
+                    res[r] = sao_sample<kGated>(P, c, x, y, k.sp.ld(x, y), k.sp, rmask);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int r = 0; r < kMax; ++r) {
+                    const int i = tid + r * kTileThreads;
+                    if (i < n && res[r] >= 0) k.sp.st(k.tx + i % k.tw, k.ty + i / k.tw, res[r]);
+                }
+                __syncthreads();
+            }
+        }
+        // ---- 5. final planes (8 samples per store) ----
+        if (P.write_fin) {
+            for (int c = 0; c < ncomp; ++c) {
+                const TileComp& k = tc[c];
+                const int rows = min(k.th, k.ph - k.ty), cols = min(k.tw, k.pw - k.tx);
+                const int chunks = (cols + 7) >> 3;
+                for (int i = tid; i < rows * chunks; i += kTileThreads) {
+                    const int r = i / chunks, q = i - r * chunks;
+                    const int x = k.tx + 8 * q, y = k.ty + r;
+                    const uint16_t* src = k.sp.s + (r + 4) * k.rw() + 8 + 8 * q;
+                    const size_t idx = (size_t)y * k.pw + x;
+                    if (8 * q + 8 <= cols && (idx & 7) == 0) {
+                        const uint4 v = *(const uint4*)src;
+                        if (P.bps == 2) {
+                            *(uint4*)((uint16_t*)P.fin[c] + idx) = v;
+                        } else {
+                            const uint32_t lo = (v.x & 0xffu) | ((v.x >> 8) & 0xff00u) | ((v.y & 0xffu) << 16) |
+                                                ((v.y & 0xff0000u) << 8);
+                            const uint32_t hi = (v.z & 0xffu) | ((v.z >> 8) & 0xff00u) | ((v.w & 0xffu) << 16) |
+                                                ((v.w & 0xff0000u) << 8);
+                            *(uint2*)((uint8_t*)P.fin[c] + idx) = make_uint2(lo, hi);
+                        }
+                    } else {
+                        for (int u = 0; u < 8 && 8 * q + u < cols; ++u) store_sample(P.fin[c], P.bps, idx + u, src[u]);
+                    }
+                }
+            }
+        }
+        // ---- 6. RGB8 at the canvas position (four pixels per thread) ----
+        if (do_rgb) {
+            uint8_t* canvas = out + P.canvas_off;
+            const int copy_w = min(P.crop_w, max(P.canvas_w - P.dst_x, 0));
+            const int copy_h = min(P.crop_h, max(P.canvas_h - P.dst_y, 0));
+            const RgbCoef kc = rgb_coef(P);
+            const TileComp& L = tc[0];
+            for (int i = tid; i < (kTile / 4) * kTile; i += kTileThreads) {
+                const int x0 = X + 4 * (i % (kTile / 4)), yy = Y + i / (kTile / 4);
+                if (x0 >= copy_w || yy >= copy_h) continue;
+                const int cnt = min(4, copy_w - x0);
+                uint32_t px[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int x = min(x0 + u, L.pw - 1);
+                    const int luma = L.sp.ld(x, yy);
+                    int cb = 0, cr = 0;
+                    if (P.idc) {
+                        cb = tc[1].sp.ld(x / P.sub_w, yy / P.sub_h);
+                        cr = tc[2].sp.ld(x / P.sub_w, yy / P.sub_h);
+                    }
+                    px[u] = rgb_px(kc, P.idc, luma, cb, cr);
+                }
+                if (moves_samples(P.orientation)) {  // each pixel to its oriented place
+                    for (int u = 0; u < cnt; ++u) {
+                        uint8_t* q = canvas + oriented_index(P.dst_x + x0 + u, P.dst_y + yy, P.canvas_w, P.canvas_h,
+                                                             P.orientation) * 3;
+                        q[0] = (uint8_t)px[u];
+                        q[1] = (uint8_t)(px[u] >> 8);
+                        q[2] = (uint8_t)(px[u] >> 16);
+                    }
+                    continue;
+                }
+                uint8_t* o = canvas + ((size_t)(P.dst_y + yy) * P.canvas_w + P.dst_x + x0) * 3;
+                if (cnt == 4 && ((uintptr_t)o & 3) == 0) {
+                    uint32_t* o32 = (uint32_t*)o;
+                    o32[0] = px[0] | (px[1] << 24);
+                    o32[1] = (px[1] >> 8) | (px[2] << 16);
+                    o32[2] = (px[2] >> 16) | (px[3] << 8);
+                } else {
+                    for (int u = 0; u < cnt; ++u) {
+                        o[3 * u] = (uint8_t)px[u];
+                        o[3 * u + 1] = (uint8_t)(px[u] >> 8);
+                        o[3 * u + 2] = (uint8_t)(px[u] >> 16);
+                    }
+                }
+            }
+        }
+    }
+}
+
 }  // namespace hpvcd
 
 extern "C" cudaError_t hpvcd_launch_deblock(const hpvcd::DevPic* pics, int n_pics, int max_segments,
@@ -599,4 +888,32 @@ extern "C" cudaError_t hpvcd_launch_yuv_canvas(const hpvcd::DevPic* pics, int n_
     hpvcd::k_yuv_canvas<<<grid, threads, 0, stream>>>(pics, out);
     hpvcd_note_launches(1);
     return cudaGetLastError();
+}
+
+// One k_filter_tile launch over pictures [0, n_pics) of `pics`: max_tiles =
+// the 64 x 64 tiles of the largest picture, cfmt = the largest chroma
+// layout class among them, out = the plan's canvases when RGB8 canvases are
+// written (else NULL).  The shared-memory limit of the 4:4:4 layout was
+// raised once by hpvcd_filter_tile_setup().
+extern "C" cudaError_t hpvcd_launch_filter_tile(const hpvcd::DevPic* pics, int n_pics, int max_tiles, int cfmt,
+                                                int gated, uint8_t* out, cudaStream_t stream) {
+    if (n_pics <= 0 || max_tiles <= 0) return cudaSuccess;
+    const int target = 148 * 8;  // resident CTAs of 256 threads on a B200
+    const int per_pic = std::max(1, (target + n_pics - 1) / n_pics);
+    dim3 grid(std::min(max_tiles, std::max(per_pic, 1)), n_pics, 1);
+    const size_t smem = hpvcd::tile_smem_bytes(cfmt);
+    if (gated)
+        hpvcd::k_filter_tile<true><<<grid, hpvcd::kTileThreads, smem, stream>>>(pics, out, out ? 1 : 0);
+    else
+        hpvcd::k_filter_tile<false><<<grid, hpvcd::kTileThreads, smem, stream>>>(pics, out, out ? 1 : 0);
+    hpvcd_note_launches(1);
+    return cudaGetLastError();
+}
+
+extern "C" cudaError_t hpvcd_filter_tile_setup() {
+    const int lim = (int)hpvcd::tile_smem_bytes(1);
+    cudaError_t e = cudaFuncSetAttribute(hpvcd::k_filter_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(hpvcd::k_filter_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    return e;
 }

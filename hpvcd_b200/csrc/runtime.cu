@@ -32,6 +32,8 @@ extern "C" cudaError_t hpvcd_launch_deblock(const DevPic*, int, int, int, cudaSt
 extern "C" cudaError_t hpvcd_launch_sao(const DevPic*, int, int, int, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_rgb(const DevPic*, int, int, uint8_t*, cudaStream_t);
 extern "C" cudaError_t hpvcd_launch_yuv_canvas(const DevPic*, int, int, uint8_t*, cudaStream_t);
+extern "C" cudaError_t hpvcd_launch_filter_tile(const DevPic*, int, int, int, int, uint8_t*, cudaStream_t);
+extern "C" cudaError_t hpvcd_filter_tile_setup();
 extern "C" cudaError_t hpvcd_launch_mc(const DevPic*, int, int, int, cudaStream_t);
 extern "C" hpvcd_status hpvcd_mlp_pick(hpvcd_mlp*, const float*, uint32_t, void*, uint32_t*);
 extern "C" uint32_t hpvcd_mlp_variants(const hpvcd_mlp*);
@@ -101,7 +103,12 @@ struct Segment {
     uint32_t wave_first, n_waves;  // the segment's wavefront launches (hpvcd_plan::waves)
     int max_dbk_v, max_dbk_h, max_sao;
     int max_rgb;  // RGB quads of the segment's largest picture
+    int max_tiles = 0;  // 64 x 64 filter tiles of the segment's largest picture
+    int tile_cfmt = 0;  // largest chroma layout class of its pictures (k_filter_tile shared memory)
 };
+
+// Deblocking, SAO and output requested together run as the fused tile kernel.
+constexpr uint32_t kFilterStages = HPVCD_STAGE_DEBLOCK | HPVCD_STAGE_SAO | HPVCD_STAGE_OUTPUT;
 
 // Independent pictures (no inter prediction) of a larger batch run as this
 // many segments, each with its whole pipeline on its own stream, so that the
@@ -254,13 +261,20 @@ struct hpvcd_plan {
                 if (rec_prefix[s.first_pic + s.n_pics] > rec_prefix[s.first_pic]) L += 1 + seg_ccp(s);
                 for (uint32_t w = s.wave_first; w < s.wave_first + s.n_waves; ++w) L += waves[w].n_items > 0;
             }
+            if ((stages & kFilterStages) == kFilterStages) {
+                L += s.max_tiles > 0;
+                if (concurrent && canvas_kind(out.kind) && s.max_rgb > 0) L += (uint32_t)any_native_canvas;
+                continue;
+            }
             if (stages & HPVCD_STAGE_DEBLOCK) L += (s.max_dbk_v > 0) + (s.max_dbk_h > 0);
             if ((stages & HPVCD_STAGE_SAO) && s.max_sao > 0) ++L;
             if (concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(out.kind) && s.max_rgb > 0)
                 L += (uint32_t)any_rgb_canvas + (uint32_t)any_native_canvas;
         }
         if (!concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(out.kind) && max_rgb > 0)
-            L += (uint32_t)any_rgb_canvas + (uint32_t)any_native_canvas;
+            L += (stages & kFilterStages) == kFilterStages
+                     ? (uint32_t)any_native_canvas
+                     : (uint32_t)any_rgb_canvas + (uint32_t)any_native_canvas;
         return L;
     }
 
@@ -480,6 +494,21 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             P->recon_feat = true;
         if (pics[i].flags & HPVCD_PIC_INTER) any_inter = true;
     }
+    // ---- which pictures keep their final planes: all, unless the output is
+    // RGB8 canvases only; then those that a later picture predicts from,
+    // that a DPB stores, or whose canvas is a native one ----
+    std::vector<char> keep_fin(n, 1);
+    if (out && out->kind == HPVCD_OUT_RGB8 && (out->options & HPVCD_OUTPUT_CANVAS_ONLY)) {
+        for (uint32_t i = 0; i < n; ++i)
+            keep_fin[i] = (pics[i].flags & HPVCD_PIC_STORE_MASK) != 0 ||
+                          native_canvas(out->kind, canvas_of(out, out->place[i].canvas));
+        for (uint32_t i = 0; i < n; ++i)
+            for (int l = 0; l < 2; ++l)
+                for (int r = 0; r < HPVCD_MAX_REFS; ++r) {
+                    const int sv = pics[i].ref_slot[l][r];
+                    if (sv >= 0 && (uint32_t)sv < n) keep_fin[(size_t)sv] = 1;
+                }
+    }
     // ---- planes + scratch layout ----
     size_t plane_bytes = 0;
     std::vector<size_t> rec_off(n), fin_off(n);
@@ -490,7 +519,10 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         const size_t one = align_up(g.luma_bytes, 256) + 2 * align_up(g.chroma_bytes, 256);
         rec_off[i] = plane_bytes;
         plane_bytes += one;
-        if (sao_active(pics[i])) {
+        // the final planes are separate when SAO runs (it reads the deblocked
+        // planes) or when they are kept (the tile filter kernel never writes
+        // the planes it reads)
+        if (sao_active(pics[i]) || keep_fin[i]) {
             fin_off[i] = plane_bytes;
             plane_bytes += one;
         } else {
@@ -631,6 +663,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             d.res[2] = p.chroma_idc ? (int16_t*)(rb + ly + lc) : nullptr;
         }
         d.needs_wavefront = (p.flags & HPVCD_PIC_PRED_IN_PLANE) ? 0 : 1;
+        d.write_fin = keep_fin[i];
         if (canvas_kind(P->out.kind)) {
             const hpvcd_tile_place& tp = P->places[i];
             const hpvcd_canvas& cv = P->canvases[tp.canvas];
@@ -710,6 +743,8 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             s.max_dbk_v = std::max(s.max_dbk_v, std::max(lv, cv));
             s.max_dbk_h = std::max(s.max_dbk_h, std::max(lh, ch));
             if (d.rec[0] != d.fin[0]) s.max_sao = std::max(s.max_sao, d.w * d.h);
+            s.max_tiles = std::max(s.max_tiles, ((d.w + 63) / 64) * ((d.h + 63) / 64));
+            s.tile_cfmt = std::max(s.tile_cfmt, d.idc == 3 ? 1 : (d.idc == 2 ? 2 : 0));
             if (canvas_kind(P->out.kind)) s.max_rgb = std::max(s.max_rgb, (d.crop_w + 3) / 4 * d.crop_h);
         }
     }
@@ -734,6 +769,13 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     P->sms = sms;
     for (int cls = 0; cls < 3; ++cls)
         for (int cw = 1; cw <= 2; ++cw) P->occ[cls][cw - 1] = std::max(1, hpvcd_recon_occupancy(cls, cw));
+    {
+        const cudaError_t fe = hpvcd_filter_tile_setup();
+        if (fe != cudaSuccess) {
+            delete P;
+            return cuda_status(fe);
+        }
+    }
     if (P->concurrent) {
         GroupStreams* set = lend ? lend : &P->own;
         const cudaError_t ce = set->create();
@@ -759,6 +801,7 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
     }
     const uint32_t n_seg = (uint32_t)P->segs.size();
     uint32_t* d_err = P->d_scratch + P->waves.size();
+    const bool fused = (stages & kFilterStages) == kFilterStages;
     if (stages & HPVCD_STAGE_RECON) {
         for (size_t i = 0; i < P->src.size(); ++i) {
             const hpvcd_picture& p = P->src[i];
@@ -812,18 +855,24 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
                 if (e != cudaSuccess) return cuda_status(e);
             }
         }
-        if (stages & HPVCD_STAGE_DEBLOCK) {
-            e = hpvcd_launch_deblock(dp, (int)s.n_pics, s.max_dbk_v, 1, st);
-            if (e == cudaSuccess) e = hpvcd_launch_deblock(dp, (int)s.n_pics, s.max_dbk_h, 0, st);
+        if (fused) {  // deblocking, SAO and RGB8 in one pass over 64 x 64 tiles
+            e = hpvcd_launch_filter_tile(dp, (int)s.n_pics, s.max_tiles, s.tile_cfmt, P->seg_sao_gated(s) ? 1 : 0,
+                                         canvas_kind(P->out.kind) && P->any_rgb_canvas ? P->d_canvas : nullptr, st);
             if (e != cudaSuccess) return cuda_status(e);
-        }
-        if (stages & HPVCD_STAGE_SAO) {
-            e = hpvcd_launch_sao(dp, (int)s.n_pics, s.max_sao, P->seg_sao_gated(s) ? 1 : 0, st);
-            if (e != cudaSuccess) return cuda_status(e);
+        } else {
+            if (stages & HPVCD_STAGE_DEBLOCK) {
+                e = hpvcd_launch_deblock(dp, (int)s.n_pics, s.max_dbk_v, 1, st);
+                if (e == cudaSuccess) e = hpvcd_launch_deblock(dp, (int)s.n_pics, s.max_dbk_h, 0, st);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
+            if (stages & HPVCD_STAGE_SAO) {
+                e = hpvcd_launch_sao(dp, (int)s.n_pics, s.max_sao, P->seg_sao_gated(s) ? 1 : 0, st);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
         }
         if (P->concurrent) {
             if ((stages & HPVCD_STAGE_OUTPUT) && canvas_kind(P->out.kind)) {
-                if (P->any_rgb_canvas) e = hpvcd_launch_rgb(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st);
+                if (P->any_rgb_canvas && !fused) e = hpvcd_launch_rgb(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st);
                 if (e == cudaSuccess && P->any_native_canvas)
                     e = hpvcd_launch_yuv_canvas(dp, (int)s.n_pics, s.max_rgb, P->d_canvas, st);
                 if (e != cudaSuccess) return cuda_status(e);
@@ -835,7 +884,8 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
     }
     st = origin;
     if (!P->concurrent && (stages & HPVCD_STAGE_OUTPUT) && canvas_kind(P->out.kind)) {
-        if (P->any_rgb_canvas) e = hpvcd_launch_rgb(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
+        if (P->any_rgb_canvas && !fused)
+            e = hpvcd_launch_rgb(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
         if (e == cudaSuccess && P->any_native_canvas)
             e = hpvcd_launch_yuv_canvas(P->d_pics, (int)P->src.size(), P->max_rgb, P->d_canvas, st);
         if (e != cudaSuccess) return cuda_status(e);
@@ -881,6 +931,7 @@ bool same_layout(const hpvcd_plan* P, const hpvcd_picture* pics, uint32_t n, con
     }
     const uint32_t kind = out ? out->kind : HPVCD_OUT_YUV;
     if (kind != P->out.kind) return false;
+    if ((out ? out->options : 0u) != P->out.options) return false;
     if (canvas_kind(kind)) {
         const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
         if (nc != P->canvases.size()) return false;

@@ -351,7 +351,17 @@ typedef struct hpvcd_output {
      * unused and hpvcd_gpu_read copies nothing. */
     void* const* canvas_dst;
     uint32_t orientation;     /* single canvas: HPVCD_ORIENT_* (0 = normal)    */
+    uint32_t options;         /* HPVCD_OUTPUT_* bits (0 = none)                */
 } hpvcd_output;
+
+/* hpvcd_output.options: an RGB8 output keeps only its canvases.  The final
+ * YCbCr planes of a picture are then not written to device memory when no
+ * later picture of the batch predicts from it, it is not stored into a
+ * decoded-picture buffer and its canvas is an RGB8 one; hpvcd_plan_planes
+ * still returns their addresses, but their contents are undefined.  Saves
+ * the plane write (1.5 samples per pixel) of a decode whose product is the
+ * canvas. */
+#define HPVCD_OUTPUT_CANVAS_ONLY 0x1u
 
 /* ------------------------------------------------------------------------ */
 /* Library information.                                                     */
