@@ -663,7 +663,7 @@ __device__ __forceinline__ uint4 load8(const void* plane, int bps, int pw, int p
 }
 
 template <bool kGated>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, 4)
 k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rgb) {
     extern __shared__ __align__(16) uint16_t tsm[];
     const DevPic& P = pics[blockIdx.y];

@@ -744,7 +744,9 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
             s.max_dbk_h = std::max(s.max_dbk_h, std::max(lh, ch));
             if (d.rec[0] != d.fin[0]) s.max_sao = std::max(s.max_sao, d.w * d.h);
             s.max_tiles = std::max(s.max_tiles, ((d.w + 63) / 64) * ((d.h + 63) / 64));
-            s.tile_cfmt = std::max(s.tile_cfmt, d.idc == 3 ? 1 : (d.idc == 2 ? 2 : 0));
+            // the 4:4:4 layout holds every format, the 4:2:2 one also 4:2:0
+            const int tcls = d.idc == 3 ? 1 : (d.idc == 2 ? 2 : 0);
+            if (tcls == 1 || (tcls == 2 && s.tile_cfmt == 0)) s.tile_cfmt = tcls;
             if (canvas_kind(P->out.kind)) s.max_rgb = std::max(s.max_rgb, (d.crop_w + 3) / 4 * d.crop_h);
         }
     }
