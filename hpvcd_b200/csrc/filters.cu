@@ -51,6 +51,34 @@ __device__ __forceinline__ void slice_offsets(const DevPic& P, int qx, int qy, i
     }
 }
 
+// Cell (4x4 luma block) lookups of the filters, by cell coordinates: the
+// picture's map in global memory, or the cells around a tile staged in
+// shared memory (global memory outside them).
+struct GCells {
+    const hpvcd_cell* g;
+    int gw;
+    __device__ hpvcd_cell at(int gx, int gy) const { return g[(size_t)gy * gw + gx]; }
+};
+struct SCells {
+    const hpvcd_cell* s;
+    int gx0, gy0, sw, sh;  // staged cells [gx0, gx0 + sw) x [gy0, gy0 + sh)
+    const hpvcd_cell* g;
+    int gw;
+    __device__ hpvcd_cell at(int gx, int gy) const {
+        const int lx = gx - gx0, ly = gy - gy0;
+        return (lx >= 0 && ly >= 0 && lx < sw && ly < sh) ? s[ly * sw + lx] : g[(size_t)gy * gw + gx];
+    }
+};
+// QP of luma sample (px, py), positions past the picture clamped to its last cell.
+template <class Cl>
+__device__ __forceinline__ int qp_of(const DevPic& P, const Cl& cl, int px, int py) {
+    return cl.at(min(px >> 2, P.gw - 1), min(py >> 2, P.gh - 1)).qp_y;
+}
+template <class Cl>
+__device__ __forceinline__ bool exempt_of(const Cl& cl, int lx, int ly) {
+    return (cl.at(lx >> 2, ly >> 2).flags & HPVCD_CELL_EXEMPT) != 0;
+}
+
 // Sample accessors of the deblocking segments, in plane coordinates: a
 // plane in global memory, or a region of it staged in shared memory.
 struct GPlane {
@@ -68,13 +96,13 @@ struct SPlane {
 
 // Luma segment: 8 taps x 4 lines around the edge, in registers.
 // v[line][tap+4] with tap -4..3 (p3..p0, q0..q3).
-template <class Pl>
-__device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& pl) {
+template <class Pl, class Cl>
+__device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& pl, const Cl& cl) {
     const int mid = scan + 1;
-    const hpvcd_cell& q = vertical ? cell_at(P, edge, mid) : cell_at(P, mid, edge);
+    const hpvcd_cell q = vertical ? cl.at(edge >> 2, mid >> 2) : cl.at(mid >> 2, edge >> 2);
     const int bs = vertical ? q.bs_v : q.bs_h;
     if (bs == 0) return;
-    const int qp_p = vertical ? qp_at(P, edge - 1, mid) : qp_at(P, mid, edge - 1);
+    const int qp_p = vertical ? qp_of(P, cl, edge - 1, mid) : qp_of(P, cl, mid, edge - 1);
     const int qp_q = q.qp_y;
     const int avg = (qp_p + qp_q + 1) >> 1;
     const int sh = P.bd - 8;
@@ -113,7 +141,7 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan,
     const bool do_p1 = dp0 + dp3 < side_thr, do_q1 = dq0 + dq3 < side_thr;
     const int maxv = (1 << P.bd) - 1;
     // exemption of the P / Q side (whole 4x4 cells)
-    const bool ex_p = vertical ? exempt_at(P, edge - 1, mid) : exempt_at(P, mid, edge - 1);
+    const bool ex_p = vertical ? exempt_of(cl, edge - 1, mid) : exempt_of(cl, mid, edge - 1);
     const bool ex_q = (q.flags & HPVCD_CELL_EXEMPT) != 0;
     const int tc2 = tc >> 1;
 #pragma unroll
@@ -156,13 +184,14 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan,
 }
 
 // Chroma segment (decode.rs:2036-2137): 4 chroma lines, both Cb and Cr.
-template <class Pl>
-__device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& cb, const Pl& cr) {
+template <class Pl, class Cl>
+__device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& cb, const Pl& cr,
+                               const Cl& cl) {
     const int mid = scan + 1;
     const int lex = vertical ? edge * P.sub_w : mid * P.sub_w;
     const int ley = vertical ? mid * P.sub_h : edge * P.sub_h;
     if (lex >= P.w || ley >= P.h) return;
-    const hpvcd_cell& q = cell_at(P, lex, ley);
+    const hpvcd_cell q = cl.at(lex >> 2, ley >> 2);
     const int bs = vertical ? q.bs_v : q.bs_h;
     if (bs < 2) return;
     const int lqx = min(lex, P.w - 1), lqy = min(ley, P.h - 1);
@@ -174,7 +203,7 @@ __device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int sca
         ppx = min(lex, P.w - 1);
         ppy = min(max(ley - 1, 0), P.h - 1);
     }
-    const int avg = (qp_at(P, ppx, ppy) + qp_at(P, lqx, lqy) + 1) >> 1;
+    const int avg = (qp_of(P, cl, ppx, ppy) + qp_of(P, cl, lqx, lqy) + 1) >> 1;
     int bo, to;
     slice_offsets(P, lqx, lqy, &bo, &to);
     (void)bo;
@@ -198,8 +227,8 @@ __device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int sca
             const int q0 = pl.ld(xq0, yq0), q1 = pl.ld(xq1, yq1);
             const int delta = clamp3i((((q0 - p0) * 4 + p1 - q1 + 4) >> 3), -tc, tc);
             if (delta != 0) {  // exemption by the luma positions of p0 / q0
-                if (!exempt_at(P, xp0 * P.sub_w, yp0 * P.sub_h)) pl.st(xp0, yp0, clamp3i(p0 + delta, 0, maxv));
-                if (!exempt_at(P, xq0 * P.sub_w, yq0 * P.sub_h)) pl.st(xq0, yq0, clamp3i(q0 - delta, 0, maxv));
+                if (!exempt_of(cl, xp0 * P.sub_w, yp0 * P.sub_h)) pl.st(xp0, yp0, clamp3i(p0 + delta, 0, maxv));
+                if (!exempt_of(cl, xq0 * P.sub_w, yq0 * P.sub_h)) pl.st(xq0, yq0, clamp3i(q0 - delta, 0, maxv));
             }
         }
     }
@@ -219,7 +248,7 @@ __global__ void k_deblock(const DevPic* __restrict__ pics, int vertical) {
         // same rows; horizontal edges: neighbouring segments of the same edge
         const int e = vertical ? id % n_edges : id / n_segs;
         const int s = vertical ? id / n_edges : id % n_segs;
-        luma_segment(P, vertical != 0, 8 * (e + 1), 4 * s, GPlane{P.rec[0], P.w, P.bps});
+        luma_segment(P, vertical != 0, 8 * (e + 1), 4 * s, GPlane{P.rec[0], P.w, P.bps}, GCells{P.cells, P.gw});
     } else {
         if (P.idc == 0) return;
         const int edge_max = vertical ? P.cw : P.ch, scan_max = vertical ? P.ch : P.cw;
@@ -229,7 +258,7 @@ __global__ void k_deblock(const DevPic* __restrict__ pics, int vertical) {
         const int e = vertical ? id % n_edges : id / n_segs;
         const int s = vertical ? id / n_edges : id % n_segs;
         chroma_segment(P, vertical != 0, 8 * (e + 1), 4 * s, GPlane{P.rec[1], P.cw, P.bps},
-                       GPlane{P.rec[2], P.cw, P.bps});
+                       GPlane{P.rec[2], P.cw, P.bps}, GCells{P.cells, P.gw});
     }
 }
 
@@ -586,26 +615,40 @@ struct TileComp {
 };
 
 __host__ __device__ inline size_t tile_comp_entries(int tw, int th) { return (size_t)(tw + 16) * (th + 8); }
+// Cells staged per tile: luma columns X - 16 .. X + 79 and rows Y - 8 ..
+// Y + 71 (every cell a luma or chroma segment of the tile looks up), and the
+// SAO parameters of the (up to 4 x 4) CTBs covering the tile.
+constexpr int kTileCellsW = 24, kTileCellsH = 20, kTileSaoCtbs = 16;
 // Shared memory of a k_filter_tile CTA for the chroma-format class cfmt
-// (0 4:2:0 / 4:0:0, 1 4:4:4, 2 4:2:2).
-__host__ __device__ inline size_t tile_smem_bytes(int cfmt) {
+// (0 4:2:0 / 4:0:0, 1 4:4:4, 2 4:2:2): samples, then cells, then SAO.
+__host__ __device__ inline size_t tile_sample_bytes(int cfmt) {
     const int tw = cfmt == 1 ? 64 : 32, th = cfmt == 0 ? 32 : 64;
     return (tile_comp_entries(64, 64) + 2 * tile_comp_entries(tw, th)) * sizeof(uint16_t);
 }
+__host__ __device__ inline size_t tile_smem_bytes(int cfmt) {
+    return tile_sample_bytes(cfmt) + kTileCellsW * kTileCellsH * sizeof(hpvcd_cell) +
+           kTileSaoCtbs * sizeof(hpvcd_sao_ctb);
+}
+
+// SAO parameters of the CTBs covering a tile, staged in shared memory.
+struct SSao {
+    const hpvcd_sao_ctb* s;
+    int cx0, cy0, n;  // CTBs [cx0, cx0 + n) x [cy0, cy0 + n)
+    __device__ hpvcd_sao_comp at(int ctbx, int ctby, int c) const { return s[(ctby - cy0) * n + (ctbx - cx0)].comp[c]; }
+};
 
 // SAO of sample (x, y) of component c, s0 its deblocked value (sao.rs:179-330,
 // the driver decode.rs:2258-2493): band offset in place, edge offset from
 // the deblocked neighbours, picture-border samples and exempt cells
 // unchanged; rmask: bits of the CTB regions (slice << 8 | tile) that must
 // agree across an edge-offset neighbour (0: no restriction).
-template <bool kGated, class Pl>
-__device__ __forceinline__ int sao_sample(const DevPic& P, int c, int x, int y, int s0, const Pl& src, uint32_t rmask) {
-    const bool on = c == 0 ? (P.flags & HPVCD_PIC_SAO_LUMA) != 0 : (P.flags & HPVCD_PIC_SAO_CHROMA) != 0;
-    if (!on || !P.sao) return s0;
+template <bool kGated, class Pl, class Cl>
+__device__ __forceinline__ int sao_sample(const DevPic& P, int c, int x, int y, int s0, const Pl& src, const Cl& cl,
+                                          const SSao& sao, uint32_t rmask) {
     const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
-    if (P.cells && exempt_at(P, x * sw, y * sh)) return s0;  // exempt cells keep the deblocked sample
+    if (P.cells && exempt_of(cl, x * sw, y * sh)) return s0;  // exempt cells keep the deblocked sample
     const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
-    const hpvcd_sao_comp sc = P.sao[(size_t)((y * sh) >> P.log2_ctb) * P.ctb_cols + ((x * sw) >> P.log2_ctb)].comp[c];
+    const hpvcd_sao_comp sc = sao.at((x * sw) >> P.log2_ctb, (y * sh) >> P.log2_ctb, c);
     const int bd = c ? P.bd_c : P.bd;
     const int mx = (1 << bd) - 1;
     if (sc.type_idx == 1) {  // sao.rs:205-233
@@ -663,8 +706,8 @@ __device__ __forceinline__ uint4 load8(const void* plane, int bps, int pw, int p
 }
 
 template <bool kGated>
-__global__ void __launch_bounds__(kTileThreads, 4)
-k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rgb) {
+__global__ void __launch_bounds__(kTileThreads, 3)
+k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rgb, int cfmt) {
     extern __shared__ __align__(16) uint16_t tsm[];
     const DevPic& P = pics[blockIdx.y];
     const int tid = threadIdx.x;
@@ -672,6 +715,9 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
     const int ncomp = P.idc ? 3 : 1;
     const bool deblock = (P.flags & HPVCD_PIC_DEBLOCK) && P.cells;
     const bool do_rgb = rgb && out && P.matrix != (int)HPVCD_CANVAS_NATIVE;
+    const bool sao_on = P.sao && (P.flags & (HPVCD_PIC_SAO_LUMA | HPVCD_PIC_SAO_CHROMA));
+    const size_t cells_off = tile_sample_bytes(cfmt);
+    const size_t sao_off = cells_off + kTileCellsW * kTileCellsH * sizeof(hpvcd_cell);
     const uint32_t rmask = (kGated && P.ctb_region) ? (((P.flags & HPVCD_PIC_SAO_NO_ACROSS_SLICES) ? 0xff00u : 0u) |
                                                        ((P.flags & HPVCD_PIC_SAO_NO_ACROSS_TILES) ? 0x00ffu : 0u))
                                                     : 0u;
@@ -687,8 +733,25 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
             k.sp = SPlane{tsm + off, k.tx - 8, k.ty - 4, k.tw + 16};
             off += tile_comp_entries(k.tw, k.th);
         }
-        // ---- 1. stage the tile and its halo (8 samples per copy) ----
+        // ---- 1. stage the tile and its halo (8 samples per copy), the cells
+        // around it and the SAO parameters of its CTBs ----
         __syncthreads();  // the previous tile's readers are done
+        hpvcd_cell* s_cells = (hpvcd_cell*)((unsigned char*)tsm + cells_off);
+        const SCells cl{s_cells, (X - 16) >> 2, (Y - 8) >> 2, kTileCellsW, kTileCellsH, P.cells, P.gw};
+        if (P.cells)
+            for (int i = tid; i < kTileCellsW * kTileCellsH; i += kTileThreads) {
+                const int gx = cl.gx0 + i % kTileCellsW, gy = cl.gy0 + i / kTileCellsW;
+                s_cells[i] = (gx >= 0 && gy >= 0 && gx < P.gw && gy < P.gh) ? P.cells[(size_t)gy * P.gw + gx]
+                                                                            : hpvcd_cell{};
+            }
+        hpvcd_sao_ctb* s_sao = (hpvcd_sao_ctb*)((unsigned char*)tsm + sao_off);
+        const int nsc = max(1, kTile >> P.log2_ctb);
+        const SSao sao{s_sao, X >> P.log2_ctb, Y >> P.log2_ctb, nsc};
+        if (sao_on)
+            for (int i = tid; i < nsc * nsc; i += kTileThreads) {
+                const int cx = sao.cx0 + i % nsc, cy = sao.cy0 + i / nsc;
+                if (cx < P.ctb_cols && cy < P.ctb_rows) s_sao[i] = P.sao[(size_t)cy * P.ctb_cols + cx];
+            }
         for (int c = 0; c < ncomp; ++c) {
             const TileComp& k = tc[c];
             const int chunks = k.rw() >> 3;
@@ -715,7 +778,7 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                         const int scan = (vertical ? Y - 4 : X - 4) + 4 * (j / 9);
                         const int emax = vertical ? P.w : P.h, smax = vertical ? P.h : P.w;
                         if (e >= 8 && e <= emax - 4 && scan >= 0 && scan + 4 <= smax)
-                            luma_segment(P, vertical, e, scan, Lc.sp);
+                            luma_segment(P, vertical, e, scan, Lc.sp, cl);
                     } else {
                         const int jj = j - n_luma;
                         const int ne = vertical ? nec_v : nec_h;
@@ -723,7 +786,7 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                         const int scan = (vertical ? Cb.ty - 4 : Cb.tx - 4) + 4 * (jj / ne);
                         const int emax = vertical ? P.cw : P.ch, smax = vertical ? P.ch : P.cw;
                         if (e >= 8 && e <= emax - 2 && scan >= 0 && scan + 4 <= smax)
-                            chroma_segment(P, vertical, e, scan, Cb.sp, tc[2].sp);
+                            chroma_segment(P, vertical, e, scan, Cb.sp, tc[2].sp, cl);
                     }
                 }
                 __syncthreads();
@@ -731,8 +794,9 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
         }
         // ---- 4. SAO: every result computed from the deblocked samples,
         // then written back ----
-        if (P.sao && (P.flags & (HPVCD_PIC_SAO_LUMA | HPVCD_PIC_SAO_CHROMA))) {
+        if (sao_on) {
             for (int c = 0; c < ncomp; ++c) {
+                if (!(P.flags & (c == 0 ? HPVCD_PIC_SAO_LUMA : HPVCD_PIC_SAO_CHROMA))) continue;
                 const TileComp& k = tc[c];
                 constexpr int kMax = kTile * kTile / kTileThreads;  // samples per thread (16)
                 int res[kMax];
@@ -744,7 +808,7 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                     if (i >= n) continue;
                     const int x = k.tx + i % k.tw, y = k.ty + i / k.tw;
                     if (x >= k.pw || y >= k.ph) continue;
-                    res[r] = sao_sample<kGated>(P, c, x, y, k.sp.ld(x, y), k.sp, rmask);
+                    res[r] = sao_sample<kGated>(P, c, x, y, k.sp.ld(x, y), k.sp, cl, sao, rmask);
                 }
                 __syncthreads();
 #pragma unroll
@@ -903,9 +967,9 @@ extern "C" cudaError_t hpvcd_launch_filter_tile(const hpvcd::DevPic* pics, int n
     dim3 grid(std::min(max_tiles, std::max(per_pic, 1)), n_pics, 1);
     const size_t smem = hpvcd::tile_smem_bytes(cfmt);
     if (gated)
-        hpvcd::k_filter_tile<true><<<grid, hpvcd::kTileThreads, smem, stream>>>(pics, out, out ? 1 : 0);
+        hpvcd::k_filter_tile<true><<<grid, hpvcd::kTileThreads, smem, stream>>>(pics, out, out ? 1 : 0, cfmt);
     else
-        hpvcd::k_filter_tile<false><<<grid, hpvcd::kTileThreads, smem, stream>>>(pics, out, out ? 1 : 0);
+        hpvcd::k_filter_tile<false><<<grid, hpvcd::kTileThreads, smem, stream>>>(pics, out, out ? 1 : 0, cfmt);
     hpvcd_note_launches(1);
     return cudaGetLastError();
 }

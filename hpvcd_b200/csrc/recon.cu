@@ -673,8 +673,8 @@ __device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y
     const int yy = lane >> 2, xx = lane & 3;
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
     const bool mine = lane < 16 && xx < vw && yy < vh;
-    // the residual is loaded first: its latency overlaps the prediction
-    const int rv = coded && mine ? (int)k.res[(size_t)(y0 + yy) * k.rs + x0 + xx] : 0;
+    // the residual staged in the TB's canvas area (stage_residual)
+    const int rv = coded && mine ? (int)(int16_t)k.can[cidx(k, x0 + xx, y0 + yy)] : 0;
     int v = 0;
     // lanes past the line repeat the last position and drop it
     bool a = gather_ref(k, stamp, jrec, n2, x0, y0, min(lane, total - 1), &v);
@@ -751,12 +751,12 @@ __device__ __forceinline__ void intra_tb8(const Comp& k, int mode, int x0, int y
                                           const uint32_t* stamp, uint32_t jrec, int lane) {
     constexpr int n = 8, n2 = 16, log2n = 3;
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
-    int rv[2];  // residuals of this lane's two samples, loaded first
+    int rv[2];  // residuals of this lane's two samples, staged in the TB's canvas area
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const int i = lane + 32 * h;
         const int yy = i >> log2n, xx = i & (n - 1);
-        rv[h] = coded && xx < vw && yy < vh ? (int)k.res[(size_t)(y0 + yy) * k.rs + x0 + xx] : 0;
+        rv[h] = coded && xx < vw && yy < vh ? (int)(int16_t)k.can[cidx(k, x0 + xx, y0 + yy)] : 0;
     }
     int v_lo = 0, v_hi = 0;
     const bool a_lo = gather_ref(k, stamp, jrec, n2, x0, y0, lane, &v_lo);
@@ -857,13 +857,25 @@ __device__ __forceinline__ void intra_tb8(const Comp& k, int mode, int x0, int y
     __syncwarp();
 }
 
-// Stages the visible part of a coded n x n TB's residual (n >= 8) into the
-// TB's own canvas area with 16-byte asynchronous copies (the prediction
-// only reads samples outside the TB; each predicting lane then reads its
-// sample's residual in place).
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// Stages the visible part of a coded n x n TB's residual (written by
+// k_residual) into the TB's own canvas area with asynchronous copies: 16
+// bytes per copy, 8 for 4x4 TBs.  The walk stages a few TBs ahead of the one
+// it reconstructs, so the copies' latency overlaps earlier TBs.  The area
+// of a TB not yet reconstructed is never an available reference sample of
+// an earlier TB (its stamp is later), so the staged values are never read
+// as samples; each lane predicting a sample reads its residual in place.
 __device__ __forceinline__ void stage_residual(const Comp& k, int log2n, int x0, int y0, int lane) {
     const int n = 1 << log2n;
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    if (n == 4) {
+        if (lane < vh) cp_async8(k.can + cidx(k, x0, y0 + lane), k.res + (size_t)(y0 + lane) * k.rs + x0);
+        return;
+    }
     const int lc = log2n - 3;  // 8-sample chunks per row: log2
     const int chunks = ((vw + 7) >> 3);
     for (int i = lane; i < (vh << lc); i += 32) {
@@ -871,17 +883,22 @@ __device__ __forceinline__ void stage_residual(const Comp& k, int log2n, int x0,
         if (q < chunks)
             cp_async16(k.can + cidx(k, x0 + 8 * q, y0 + r), k.res + (size_t)(y0 + r) * k.rs + x0 + 8 * q);
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// TBs staged ahead of the one being reconstructed (one cp.async group each).
+constexpr int kStageAhead = 3;
+__device__ __forceinline__ void wait_staged() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(kStageAhead) : "memory");
+    __syncwarp();
 }
 
 // Intra TB of size 8..32, first part, by one warp through shared memory:
 // gather, substitution (intra.rs:84-148), filtering (:151-219) and the
 // per-mode set-up of the prediction (the angular projection into ws.refs,
-// the DC value into ws.dc).  A coded TB's residual is staged meanwhile.
-__device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
+// the DC value into ws.dc).
+__device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode, int x0, int y0,
                                               const uint32_t* stamp, uint32_t jrec, WalkScratch& ws, int lane) {
     const int n = 1 << log2n;
-    if (coded) stage_residual(k, log2n, x0, y0, lane);
     const int total = 4 * n + 1;
     const int n2 = 2 * n;
     uint32_t mask[5];
@@ -997,10 +1014,6 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
     const int max_v = k.max_v;
     const bool edge_filters = k.luma && n < 32;  // is_luma gate of predict_into
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
-    if (coded) {  // the staged residual has arrived for every lane
-        asm volatile("cp.async.wait_all;" ::: "memory");
-        __syncwarp();
-    }
     auto res_at = [&](int xx, int yy) { return (int)(int16_t)k.can[cidx(k, x0 + xx, y0 + yy)]; };
     if (mode >= 2) {
         const int angle = c_intra_angle[mode - 2];
@@ -1065,7 +1078,7 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
 // Intra TB of size 8..32 by one warp.
 __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
                                              const uint32_t* stamp, uint32_t jrec, WalkScratch& ws, int lane) {
-    intra_tb_prep(k, log2n, mode, x0, y0, coded, stamp, jrec, ws, lane);
+    intra_tb_prep(k, log2n, mode, x0, y0, stamp, jrec, ws, lane);
     intra_tb_predict(k, log2n, mode, x0, y0, coded, ws, lane, 32);
     __syncwarp();
 }
@@ -1517,10 +1530,26 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             // edge segments in the canvas, quadrants released
             uint32_t have = s_have[c];
             int prog = 0;
+            // residuals are staged kStageAhead TBs ahead (one copy group per
+            // list entry, empty when it has none to stage)
+            auto stage = [&](uint32_t ei) {
+                if (ei < cnt) {
+                    hpvcd_tu t;
+                    const uint4 w4 = recs[list[ei] & kListRec];
+                    memcpy(&t, &w4, sizeof(t));
+                    const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
+                    if (coded && !(kFeat && (t.flags & HPVCD_TU_PCM)))
+                        stage_residual(k, t.log2n, (int)t.x - k.ox, (int)t.y - k.oy, lane);
+                }
+                asm volatile("cp.async.commit_group;" ::: "memory");
+            };
+#pragma unroll
+            for (int d = 0; d < kStageAhead; ++d) stage((uint32_t)d);
             // the next record is fetched while the current TB is reconstructed
             uint32_t jn = cnt ? list[0] : 0u;
             uint4 wn = cnt ? recs[jn & kListRec] : make_uint4(0u, 0u, 0u, 0u);
             for (uint32_t e = 0; e < cnt; ++e) {
+                stage(e + kStageAhead);
                 const uint32_t j = jn & kListRec;
                 const bool event = (jn & kListEvent) != 0u;
                 hpvcd_tu t;
@@ -1539,6 +1568,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 // a chroma TB with cross-component prediction has a residual
                 // (written by k_ccp) even without coded coefficients
                 const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
+                wait_staged();  // this TB's residual is in its canvas area
                 if (kFeat && (t.flags & HPVCD_TU_PCM)) {
                     pcm_tb(k, t.log2n, x, y, lane);
                 } else if (t.log2n == 2) {
@@ -1549,6 +1579,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     intra_tb_big(k, t.log2n, t.mode, x, y, coded, stamp, j, ws, lane);
                 }
             }
+            asm volatile("cp.async.wait_all;" ::: "memory");  // the trailing (empty) groups
             publish_level(geo(c), P.bps, prog, 4, level + c, lane);
         }
         __syncthreads();

@@ -1042,7 +1042,7 @@ Slot* find_ticket(hpvcd_gpu* g, hpvcd_ticket t) {
 
 hpvcd_status device_status(hpvcd_plan* P, cudaStream_t st) {
     uint32_t err = 0;
-    cudaError_t e = cudaMemcpyAsync(&err, P->d_scratch + P->segs.size(), sizeof(uint32_t),
+    cudaError_t e = cudaMemcpyAsync(&err, P->d_scratch + P->waves.size(), sizeof(uint32_t),
                                     cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_status(e);

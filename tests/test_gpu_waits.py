@@ -5,7 +5,7 @@ there can only end.  Here a CTU waits on flags other CTAs write; every such
 wait is bounded and, when it runs out, sets the device error word and
 returns.  These tests make a wait run out without faulting anything: one CTU
 is left out of the plan's work list (hpvcd_plan_set_wait_test), so it never
-publishes, and the waits of the CTUs predicting from it are cut to 1000
+publishes, and the waits of the CTUs predicting from it are cut to 100 000
 polls.  The launch must complete, report HPVCD_ERR_TIMEOUT, write nothing
 outside the picture's place on the canvas, and leave the CTUs that cannot
 see the missing one bit-exact; restoring the list decodes the whole picture
@@ -27,7 +27,10 @@ if not torch.cuda.is_available():  # pragma: no cover
 from hpvcd_b200.gpu import DevicePlan  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-SPIN = 1000  # polls per wait before it gives up
+# polls per wait before it gives up: short enough for a quick test, far
+# longer than any wait for a CTU that is being reconstructed (one CTU walk
+# is a fraction of a millisecond)
+SPIN = 100_000
 
 
 def wavefront_order(cols: int, rows: int):
