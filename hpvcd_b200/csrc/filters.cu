@@ -625,8 +625,13 @@ __host__ __device__ inline size_t tile_sample_bytes(int cfmt) {
     const int tw = cfmt == 1 ? 64 : 32, th = cfmt == 0 ? 32 : 64;
     return (tile_comp_entries(64, 64) + 2 * tile_comp_entries(tw, th)) * sizeof(uint16_t);
 }
+// The tile's final samples (no halo), component after component.
+__host__ __device__ inline size_t tile_out_bytes(int cfmt) {
+    const int tw = cfmt == 1 ? 64 : 32, th = cfmt == 0 ? 32 : 64;
+    return (size_t)(64 * 64 + 2 * tw * th) * sizeof(uint16_t);
+}
 __host__ __device__ inline size_t tile_smem_bytes(int cfmt) {
-    return tile_sample_bytes(cfmt) + kTileCellsW * kTileCellsH * sizeof(hpvcd_cell) +
+    return tile_sample_bytes(cfmt) + tile_out_bytes(cfmt) + kTileCellsW * kTileCellsH * sizeof(hpvcd_cell) +
            kTileSaoCtbs * sizeof(hpvcd_sao_ctb);
 }
 
@@ -678,6 +683,72 @@ __device__ __forceinline__ int sao_sample(const DevPic& P, int c, int x, int y, 
     return o ? clamp3i(s0 + o, 0, mx) : s0;
 }
 
+template <bool kGated>
+__device__ __noinline__ int sao_sample_slow(const DevPic& P, int c, int x, int y, int s0, const SPlane& src,
+                                            const SCells& cl, const SSao& sao, uint32_t rmask) {
+    return sao_sample<kGated>(P, c, x, y, s0, src, cl, sao, rmask);
+}
+
+// SAO of four horizontally adjacent samples (x0 .. x0 + 3, x0 a multiple of
+// 4, so one CTB) of component c from the staged deblocked region: the 3 x 6
+// neighbourhood is read once (one 8-byte load per row), the CTB's parameters
+// once; out[] receives the results (sao.rs:179-330: band offset, edge offset
+// with picture-border samples unchanged).  Exempt cells and slice / tile
+// boundaries, when the tile has any, go through sao_sample.
+template <bool kGated, class Cl>
+__device__ __forceinline__ void sao_quad(const DevPic& P, int c, const TileComp& k, int x0, int y, const SSao& sao,
+                                         const Cl& cl, bool slow, uint32_t rmask, int out[4]) {
+    const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
+    const int rw = k.rw();
+    const uint16_t* row = k.sp.s + (y - k.sp.y0) * rw + (x0 - k.sp.x0);
+    int w[3][6];  // w[r][j] = sample (x0 - 1 + j, y - 1 + r)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const uint16_t* q = row + (r - 1) * rw;
+        const uint2 v = *(const uint2*)q;
+        w[r][0] = q[-1];
+        w[r][1] = v.x & 0xffff; w[r][2] = v.x >> 16; w[r][3] = v.y & 0xffff; w[r][4] = v.y >> 16;
+        w[r][5] = q[4];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = w[1][i + 1];
+    if (slow) {
+        for (int i = 0; i < 4; ++i)
+            if (x0 + i < k.pw) out[i] = sao_sample_slow<kGated>(P, c, x0 + i, y, w[1][i + 1], k.sp, cl, sao, rmask);
+        return;
+    }
+    const hpvcd_sao_comp sc = sao.at((x0 * sw) >> P.log2_ctb, (y * sh) >> P.log2_ctb, c);
+    const int bd = c ? P.bd_c : P.bd;
+    const int mx = (1 << bd) - 1;
+    if (sc.type_idx == 1) {  // sao.rs:205-233
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint8_t rel = (uint8_t)((uint8_t)(out[i] >> (bd - 5)) - sc.band_pos);
+            if (rel < 4) out[i] = clamp3i(out[i] + sc.offsets[rel], 0, mx);
+        }
+    } else if (sc.type_idx == 2) {  // sao.rs:266-330
+        const int dx = sc.eo_class == 1 ? 0 : 1;
+        const int dy = sc.eo_class == 0 ? 0 : (sc.eo_class == 3 ? -1 : 1);
+        const bool rows_ok = y - dy >= 0 && y + dy >= 0 && y - dy < k.ph && y + dy < k.ph;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int x = x0 + i;
+            if (!rows_ok || x - dx < 0 || x + dx >= k.pw) continue;  // a neighbour outside the picture
+            int n1, n2;  // (x + dx, y + dy) and (x - dx, y - dy)
+            switch (sc.eo_class) {
+                case 0: n1 = w[1][i + 2]; n2 = w[1][i]; break;
+                case 1: n1 = w[2][i + 1]; n2 = w[0][i + 1]; break;
+                case 2: n1 = w[2][i + 2]; n2 = w[0][i]; break;
+                default: n1 = w[0][i + 2]; n2 = w[2][i]; break;
+            }
+            const int s0 = out[i];
+            const int e = ((s0 > n1) - (s0 < n1)) + ((s0 > n2) - (s0 < n2)) + 2;
+            const int o = e == 0 ? sc.offsets[0] : (e == 1 ? sc.offsets[1] : (e == 3 ? sc.offsets[2] : (e == 4 ? sc.offsets[3] : 0)));
+            if (o) out[i] = clamp3i(s0 + o, 0, mx);
+        }
+    }
+}
+
 // Eight horizontally adjacent samples of a plane row at (x, y), as uint16,
 // zero outside the plane.  Vector load when the whole group is inside and
 // 16-byte aligned.
@@ -716,7 +787,8 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
     const bool deblock = (P.flags & HPVCD_PIC_DEBLOCK) && P.cells;
     const bool do_rgb = rgb && out && P.matrix != (int)HPVCD_CANVAS_NATIVE;
     const bool sao_on = P.sao && (P.flags & (HPVCD_PIC_SAO_LUMA | HPVCD_PIC_SAO_CHROMA));
-    const size_t cells_off = tile_sample_bytes(cfmt);
+    const size_t out_off = tile_sample_bytes(cfmt);
+    const size_t cells_off = out_off + tile_out_bytes(cfmt);
     const size_t sao_off = cells_off + kTileCellsW * kTileCellsH * sizeof(hpvcd_cell);
     const uint32_t rmask = (kGated && P.ctb_region) ? (((P.flags & HPVCD_PIC_SAO_NO_ACROSS_SLICES) ? 0xff00u : 0u) |
                                                        ((P.flags & HPVCD_PIC_SAO_NO_ACROSS_TILES) ? 0x00ffu : 0u))
@@ -738,11 +810,15 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
         __syncthreads();  // the previous tile's readers are done
         hpvcd_cell* s_cells = (hpvcd_cell*)((unsigned char*)tsm + cells_off);
         const SCells cl{s_cells, (X - 16) >> 2, (Y - 8) >> 2, kTileCellsW, kTileCellsH, P.cells, P.gw};
+        bool exempt_here = false;  // an exempt cell among the staged ones
         if (P.cells)
             for (int i = tid; i < kTileCellsW * kTileCellsH; i += kTileThreads) {
                 const int gx = cl.gx0 + i % kTileCellsW, gy = cl.gy0 + i / kTileCellsW;
-                s_cells[i] = (gx >= 0 && gy >= 0 && gx < P.gw && gy < P.gh) ? P.cells[(size_t)gy * P.gw + gx]
-                                                                            : hpvcd_cell{};
+                const hpvcd_cell cv = (gx >= 0 && gy >= 0 && gx < P.gw && gy < P.gh)
+                                          ? P.cells[(size_t)gy * P.gw + gx]
+                                          : hpvcd_cell{};
+                s_cells[i] = cv;
+                exempt_here |= (cv.flags & HPVCD_CELL_EXEMPT) != 0;
             }
         hpvcd_sao_ctb* s_sao = (hpvcd_sao_ctb*)((unsigned char*)tsm + sao_off);
         const int nsc = max(1, kTile >> P.log2_ctb);
@@ -761,7 +837,9 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                     load8(P.rec[c], P.bps, k.pw, k.ph, k.sp.x0 + 8 * q, k.sp.y0 + r);
             }
         }
-        __syncthreads();
+        // the SAO of the tile tests exemption and slice / tile boundaries
+        // per sample only when the tile has them
+        const bool sao_slow = __syncthreads_or(exempt_here) || (kGated && rmask);
         if (deblock) {
             // ---- 2. vertical edges, then 3. horizontal edges ----
             const TileComp& Lc = tc[0];
@@ -792,33 +870,36 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                 __syncthreads();
             }
         }
-        // ---- 4. SAO: every result computed from the deblocked samples,
-        // then written back ----
-        if (sao_on) {
-            for (int c = 0; c < ncomp; ++c) {
-                if (!(P.flags & (c == 0 ? HPVCD_PIC_SAO_LUMA : HPVCD_PIC_SAO_CHROMA))) continue;
-                const TileComp& k = tc[c];
-                constexpr int kMax = kTile * kTile / kTileThreads;  // samples per thread (16)
-                int res[kMax];
-                const int n = k.tw * k.th;
-#pragma unroll
-                for (int r = 0; r < kMax; ++r) {
-                    const int i = tid + r * kTileThreads;
-                    res[r] = -1;
-                    if (i >= n) continue;
-                    const int x = k.tx + i % k.tw, y = k.ty + i / k.tw;
-                    if (x >= k.pw || y >= k.ph) continue;
-                    res[r] = sao_sample<kGated>(P, c, x, y, k.sp.ld(x, y), k.sp, cl, sao, rmask);
-                }
-                __syncthreads();
-#pragma unroll
-                for (int r = 0; r < kMax; ++r) {
-                    const int i = tid + r * kTileThreads;
-                    if (i < n && res[r] >= 0) k.sp.st(k.tx + i % k.tw, k.ty + i / k.tw, res[r]);
-                }
-                __syncthreads();
+        // ---- 4. SAO from the deblocked samples into the tile's output
+        // buffer (a copy for components without SAO) ----
+        uint16_t* tout[3];
+        {
+            size_t o = 0;
+            for (int c = 0; c < 3; ++c) {
+                tout[c] = (uint16_t*)((unsigned char*)tsm + out_off) + o;
+                o += (size_t)tc[c].tw * tc[c].th;
             }
         }
+        for (int c = 0; c < ncomp; ++c) {
+            const TileComp& k = tc[c];
+            const bool on = sao_on && (P.flags & (c == 0 ? HPVCD_PIC_SAO_LUMA : HPVCD_PIC_SAO_CHROMA));
+            const int qw = k.tw >> 2, nq = qw * k.th;
+            for (int i = tid; i < nq; i += kTileThreads) {
+                const int xq = 4 * (i % qw), yq = i / qw;
+                const int x0 = k.tx + xq, y = k.ty + yq;
+                if (x0 >= k.pw || y >= k.ph) continue;
+                uint2 v;
+                if (on) {
+                    int r4[4];
+                    sao_quad<kGated>(P, c, k, x0, y, sao, cl, sao_slow, rmask, r4);
+                    v = make_uint2((uint32_t)r4[0] | ((uint32_t)r4[1] << 16), (uint32_t)r4[2] | ((uint32_t)r4[3] << 16));
+                } else {
+                    v = *(const uint2*)(k.sp.s + (y - k.sp.y0) * k.rw() + (x0 - k.sp.x0));
+                }
+                *(uint2*)(tout[c] + yq * k.tw + xq) = v;
+            }
+        }
+        __syncthreads();
         // ---- 5. final planes (8 samples per store) ----
         if (P.write_fin) {
             for (int c = 0; c < ncomp; ++c) {
@@ -828,7 +909,7 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                 for (int i = tid; i < rows * chunks; i += kTileThreads) {
                     const int r = i / chunks, q = i - r * chunks;
                     const int x = k.tx + 8 * q, y = k.ty + r;
-                    const uint16_t* src = k.sp.s + (r + 4) * k.rw() + 8 + 8 * q;
+                    const uint16_t* src = tout[c] + r * k.tw + 8 * q;
                     const size_t idx = (size_t)y * k.pw + x;
                     if (8 * q + 8 <= cols && (idx & 7) == 0) {
                         const uint4 v = *(const uint4*)src;
@@ -858,18 +939,30 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                 const int x0 = X + 4 * (i % (kTile / 4)), yy = Y + i / (kTile / 4);
                 if (x0 >= copy_w || yy >= copy_h) continue;
                 const int cnt = min(4, copy_w - x0);
+                // four luma samples (one 8-byte load) and their chroma
+                const uint2 lv = *(const uint2*)(tout[0] + (yy - Y) * kTile + (x0 - X));
+                const int luma[4] = {(int)(lv.x & 0xffff), (int)(lv.x >> 16), (int)(lv.y & 0xffff), (int)(lv.y >> 16)};
+                int cb[4] = {0, 0, 0, 0}, cr[4] = {0, 0, 0, 0};
+                if (P.idc) {
+                    const TileComp& B = tc[1];
+                    const int cy = yy / P.sub_h - B.ty;
+                    const uint16_t* ob = tout[1] + (size_t)cy * B.tw;
+                    const uint16_t* orr = tout[2] + (size_t)cy * B.tw;
+                    if (P.sub_w == 2) {  // two chroma samples (one 4-byte load each)
+                        const int cx = (x0 >> 1) - B.tx;
+                        const uint32_t b = *(const uint32_t*)(ob + cx), r = *(const uint32_t*)(orr + cx);
+                        cb[0] = cb[1] = b & 0xffff; cb[2] = cb[3] = b >> 16;
+                        cr[0] = cr[1] = r & 0xffff; cr[2] = cr[3] = r >> 16;
+                    } else {
+                        const int cx = x0 - B.tx;
+                        const uint2 b = *(const uint2*)(ob + cx), r = *(const uint2*)(orr + cx);
+                        cb[0] = b.x & 0xffff; cb[1] = b.x >> 16; cb[2] = b.y & 0xffff; cb[3] = b.y >> 16;
+                        cr[0] = r.x & 0xffff; cr[1] = r.x >> 16; cr[2] = r.y & 0xffff; cr[3] = r.y >> 16;
+                    }
+                }
                 uint32_t px[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int x = min(x0 + u, L.pw - 1);
-                    const int luma = L.sp.ld(x, yy);
-                    int cb = 0, cr = 0;
-                    if (P.idc) {
-                        cb = tc[1].sp.ld(x / P.sub_w, yy / P.sub_h);
-                        cr = tc[2].sp.ld(x / P.sub_w, yy / P.sub_h);
-                    }
-                    px[u] = rgb_px(kc, P.idc, luma, cb, cr);
-                }
+                for (int u = 0; u < 4; ++u) px[u] = rgb_px(kc, P.idc, luma[u], cb[u], cr[u]);
                 if (moves_samples(P.orientation)) {  // each pixel to its oriented place
                     for (int u = 0; u < cnt; ++u) {
                         uint8_t* q = canvas + oriented_index(P.dst_x + x0 + u, P.dst_y + yy, P.canvas_w, P.canvas_h,

@@ -525,6 +525,9 @@ __host__ __device__ __forceinline__ int can_size(int S, int Sh) { return can_top
 __device__ __forceinline__ int can_at(int S, int x, int y) {
     return y < 0 ? x + 8 : can_top(S) + y * can_row(S) + x + 8;
 }
+// The same index for a sample of the CTU's own rows (y >= 0), without the
+// test for the row above.
+__device__ __forceinline__ int can_in(int S, int x, int y) { return can_top(S) + y * can_row(S) + x + 8; }
 
 // Shared-memory layout of one CTA: the canvases, one walk scratch per warp,
 // the CTU's staged records, the 16x16 stamp map, the three TB lists.
@@ -594,6 +597,7 @@ struct Comp {
 };
 
 __device__ __forceinline__ int cidx(const Comp& k, int x, int y) { return can_at(k.S, x, y); }
+__device__ __forceinline__ int cin(const Comp& k, int x, int y) { return can_in(k.S, x, y); }
 
 // Reference sample i of the line (i < 2n: left column bottom-up, 2n: the
 // corner, > 2n: above row) with its availability (decode.rs:4651-4690
@@ -661,7 +665,7 @@ __device__ __forceinline__ void pcm_tb(const Comp& k, int log2n, int x0, int y0,
     for (int i = lane; i < n * n; i += 32) {
         const int yy = i >> log2n, xx = i & (n - 1);
         if (xx < vw && yy < vh)
-            k.can[cidx(k, x0 + xx, y0 + yy)] =
+            k.can[cin(k, x0 + xx, y0 + yy)] =
                 (uint16_t)clamp3i(k.res[(size_t)(y0 + yy) * k.rs + x0 + xx], 0, k.max_v);
     }
     __syncwarp();
@@ -674,7 +678,7 @@ __device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
     const bool mine = lane < 16 && xx < vw && yy < vh;
     // the residual staged in the TB's canvas area (stage_residual)
-    const int rv = coded && mine ? (int)(int16_t)k.can[cidx(k, x0 + xx, y0 + yy)] : 0;
+    const int rv = coded && mine ? (int)(int16_t)k.can[cin(k, x0 + xx, y0 + yy)] : 0;
     int v = 0;
     // lanes past the line repeat the last position and drop it
     bool a = gather_ref(k, stamp, jrec, n2, x0, y0, min(lane, total - 1), &v);
@@ -727,7 +731,7 @@ __device__ __forceinline__ void intra_tb4(const Comp& k, int mode, int x0, int y
     }
     if (mine) {
         if (coded) pred = clamp3i(pred + rv, 0, k.max_v);
-        k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)pred;
+        k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)pred;
     }
     __syncwarp();
 }
@@ -756,7 +760,7 @@ __device__ __forceinline__ void intra_tb8(const Comp& k, int mode, int x0, int y
     for (int h = 0; h < 2; ++h) {
         const int i = lane + 32 * h;
         const int yy = i >> log2n, xx = i & (n - 1);
-        rv[h] = coded && xx < vw && yy < vh ? (int)(int16_t)k.can[cidx(k, x0 + xx, y0 + yy)] : 0;
+        rv[h] = coded && xx < vw && yy < vh ? (int)(int16_t)k.can[cin(k, x0 + xx, y0 + yy)] : 0;
     }
     int v_lo = 0, v_hi = 0;
     const bool a_lo = gather_ref(k, stamp, jrec, n2, x0, y0, lane, &v_lo);
@@ -851,7 +855,7 @@ __device__ __forceinline__ void intra_tb8(const Comp& k, int mode, int x0, int y
         if (xx < vw && yy < vh) {
             int v = out[h];
             if (coded) v = clamp3i(v + rv[h], 0, max_v);
-            k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
+            k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
         }
     }
     __syncwarp();
@@ -873,7 +877,7 @@ __device__ __forceinline__ void stage_residual(const Comp& k, int log2n, int x0,
     const int n = 1 << log2n;
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
     if (n == 4) {
-        if (lane < vh) cp_async8(k.can + cidx(k, x0, y0 + lane), k.res + (size_t)(y0 + lane) * k.rs + x0);
+        if (lane < vh) cp_async8(k.can + cin(k, x0, y0 + lane), k.res + (size_t)(y0 + lane) * k.rs + x0);
         return;
     }
     const int lc = log2n - 3;  // 8-sample chunks per row: log2
@@ -881,7 +885,7 @@ __device__ __forceinline__ void stage_residual(const Comp& k, int log2n, int x0,
     for (int i = lane; i < (vh << lc); i += 32) {
         const int r = i >> lc, q = i & ((1 << lc) - 1);
         if (q < chunks)
-            cp_async16(k.can + cidx(k, x0 + 8 * q, y0 + r), k.res + (size_t)(y0 + r) * k.rs + x0 + 8 * q);
+            cp_async16(k.can + cin(k, x0 + 8 * q, y0 + r), k.res + (size_t)(y0 + r) * k.rs + x0 + 8 * q);
     }
 }
 
@@ -1014,7 +1018,7 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
     const int max_v = k.max_v;
     const bool edge_filters = k.luma && n < 32;  // is_luma gate of predict_into
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
-    auto res_at = [&](int xx, int yy) { return (int)(int16_t)k.can[cidx(k, x0 + xx, y0 + yy)]; };
+    auto res_at = [&](int xx, int yy) { return (int)(int16_t)k.can[cin(k, x0 + xx, y0 + yy)]; };
     if (mode >= 2) {
         const int angle = c_intra_angle[mode - 2];
         const bool vertical = mode >= 18;
@@ -1037,7 +1041,7 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
             }
             if (xx < vw && yy < vh) {
                 if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
-                k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
+                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
     } else if (mode == 1) {  // DC
@@ -1056,7 +1060,7 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
             }
             if (xx < vw && yy < vh) {
                 if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
-                k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
+                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
     } else {  // planar
@@ -1069,7 +1073,7 @@ __device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int m
             int v = (hh + vv + n) >> (log2n + 1);
             if (xx < vw && yy < vh) {
                 if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
-                k.can[cidx(k, x0 + xx, y0 + yy)] = (uint16_t)v;
+                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
             }
         }
     }
@@ -1204,7 +1208,7 @@ __device__ __forceinline__ void publish_level(const EdgeGeo& e, int bps, int fro
             x = e.S - 1, y = r0 + i;
         else
             x = b0 + i - nr, y = e.Sh - 1;
-        store_sample(e.plane, bps, (size_t)(e.oy + y) * e.pw + e.ox + x, e.can[can_at(e.S, x, y)]);
+        store_sample(e.plane, bps, (size_t)(e.oy + y) * e.pw + e.ox + x, e.can[can_in(e.S, x, y)]);
     }
     __syncwarp();
     if (lane == 0) st_release(level, (uint32_t)to);
@@ -1444,7 +1448,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     const int ax = ox + x, ay = oy + y;
                     int v = 0;
                     if (ax < pw && ay < ph) v = load_sample(P.rec[c], P.bps, (size_t)ay * pw + ax);
-                    can[can_at(S, x, y)] = (uint16_t)v;
+                    can[can_in(S, x, y)] = (uint16_t)v;
                 }
             }
         }
@@ -1594,7 +1598,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 const int chunks = cols >> 3;
                 for (int i = tid; i < rows * chunks; i += kThreads) {
                     const int y = i / chunks, q = i % chunks;
-                    const uint4 v = *(const uint4*)(can + can_at(S, 8 * q, y));
+                    const uint4 v = *(const uint4*)(can + can_in(S, 8 * q, y));
                     const size_t off = (size_t)(oy + y) * pw + ox + 8 * q;
                     if (P.bps == 2) {
                         *(uint4*)((uint16_t*)P.rec[c] + off) = v;
@@ -1609,7 +1613,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             } else {
                 for (int i = tid; i < rows * cols; i += kThreads) {
                     const int y = i / cols, x = i % cols;
-                    store_sample(P.rec[c], P.bps, (size_t)(oy + y) * pw + ox + x, can[can_at(S, x, y)]);
+                    store_sample(P.rec[c], P.bps, (size_t)(oy + y) * pw + ox + x, can[can_in(S, x, y)]);
                 }
             }
         }
