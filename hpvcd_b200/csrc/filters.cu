@@ -94,6 +94,36 @@ struct SPlane {
     __device__ void st(int x, int y, int v) const { s[(y - y0) * rw + (x - x0)] = (uint16_t)v; }
 };
 
+// The lines of one deblocking segment: sample `tap` (negative: the P side)
+// of line `line`, positioned once per segment (lines across the edge run
+// along x for a vertical edge, along y for a horizontal one).
+struct GLines {
+    void* p;
+    int bps;
+    int base;    // sample index of (line 0, tap 0): planes hold fewer than 2^31 samples
+    int ls, ts;  // line stride, tap stride in samples
+    __device__ GLines(const GPlane& g, bool vertical, int edge, int scan)
+        : p(g.p), bps(g.bps), base(vertical ? scan * g.w + edge : edge * g.w + scan),
+          ls(vertical ? g.w : 1), ts(vertical ? 1 : g.w) {}
+    __device__ int ld(int line, int tap) const { return load_sample(p, bps, (size_t)(base + line * ls + tap * ts)); }
+    __device__ void st(int line, int tap, int v) const { store_sample(p, bps, (size_t)(base + line * ls + tap * ts), v); }
+};
+struct SLines {
+    uint16_t* p;
+    int ls, ts;
+    __device__ SLines(const SPlane& r, bool vertical, int edge, int scan)
+        : p(r.s + (vertical ? (scan - r.y0) * r.rw + (edge - r.x0) : (edge - r.y0) * r.rw + (scan - r.x0))),
+          ls(vertical ? r.rw : 1), ts(vertical ? 1 : r.rw) {}
+    __device__ int ld(int line, int tap) const { return p[line * ls + tap * ts]; }
+    __device__ void st(int line, int tap, int v) const { p[line * ls + tap * ts] = (uint16_t)v; }
+};
+__device__ __forceinline__ GLines lines_of(const GPlane& g, bool vertical, int edge, int scan) {
+    return GLines(g, vertical, edge, scan);
+}
+__device__ __forceinline__ SLines lines_of(const SPlane& r, bool vertical, int edge, int scan) {
+    return SLines(r, vertical, edge, scan);
+}
+
 // Luma segment: 8 taps x 4 lines around the edge, in registers.
 // v[line][tap+4] with tap -4..3 (p3..p0, q0..q3).
 template <class Pl, class Cl>
@@ -112,19 +142,11 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan,
     const int tc = c_tc[clamp3i(avg + 2 * (bs - 1) + 2 * to, 0, 53)] << sh;
     if (tc == 0) return;
     int v[4][8];
-    auto ld = [&](int line, int tap) {
-        return vertical ? pl.ld(edge + tap, scan + line) : pl.ld(scan + line, edge + tap);
-    };
-    auto st = [&](int line, int tap, int val) {
-        if (vertical)
-            pl.st(edge + tap, scan + line, val);
-        else
-            pl.st(scan + line, edge + tap, val);
-    };
+    const auto L = lines_of(pl, vertical, edge, scan);
 #pragma unroll
     for (int l = 0; l < 4; ++l)
 #pragma unroll
-        for (int t = 0; t < 8; ++t) v[l][t] = ld(l, t - 4);
+        for (int t = 0; t < 8; ++t) v[l][t] = L.ld(l, t - 4);
     // deblock.rs:216-238 luma_decision (lines 0 and 3)
     auto g = [&](int l, int tap) { return v[l][tap + 4]; };
     const int dp0 = abs(g(0, -3) - 2 * g(0, -2) + g(0, -1));
@@ -151,31 +173,31 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan,
         if (strong) {  // deblock.rs:605-616
             auto c = [&](int o, int x) { return clamp3i(clamp3i(x, o - 2 * tc, o + 2 * tc), 0, maxv); };
             if (!ex_p) {
-                st(l, -1, c(p0, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3));
-                st(l, -2, c(p1, (p2 + p1 + p0 + q0 + 2) >> 2));
-                st(l, -3, c(p2, (2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3));
+                L.st(l, -1, c(p0, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3));
+                L.st(l, -2, c(p1, (p2 + p1 + p0 + q0 + 2) >> 2));
+                L.st(l, -3, c(p2, (2 * p3 + 3 * p2 + p1 + p0 + q0 + 4) >> 3));
             }
             if (!ex_q) {
-                st(l, 0, c(q0, (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3));
-                st(l, 1, c(q1, (p0 + q0 + q1 + q2 + 2) >> 2));
-                st(l, 2, c(q2, (p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3));
+                L.st(l, 0, c(q0, (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3));
+                L.st(l, 1, c(q1, (p0 + q0 + q1 + q2 + 2) >> 2));
+                L.st(l, 2, c(q2, (p0 + q0 + q1 + 3 * q2 + 2 * q3 + 4) >> 3));
             }
         } else {  // deblock.rs:617-631
             const int delta0 = (9 * (q0 - p0) - 3 * (q1 - p1) + 8) >> 4;
             if (abs(delta0) < tc * 10) {
                 const int delta = clamp3i(delta0, -tc, tc);
                 if (!ex_p) {
-                    st(l, -1, clamp3i(p0 + delta, 0, maxv));
+                    L.st(l, -1, clamp3i(p0 + delta, 0, maxv));
                     if (do_p1) {
                         const int dp1 = clamp3i((((p2 + p0 + 1) >> 1) - p1 + delta) >> 1, -tc2, tc2);
-                        st(l, -2, clamp3i(p1 + dp1, 0, maxv));
+                        L.st(l, -2, clamp3i(p1 + dp1, 0, maxv));
                     }
                 }
                 if (!ex_q) {
-                    st(l, 0, clamp3i(q0 - delta, 0, maxv));
+                    L.st(l, 0, clamp3i(q0 - delta, 0, maxv));
                     if (do_q1) {
                         const int dq1 = clamp3i((((q2 + q0 + 1) >> 1) - q1 - delta) >> 1, -tc2, tc2);
-                        st(l, 1, clamp3i(q1 + dq1, 0, maxv));
+                        L.st(l, 1, clamp3i(q1 + dq1, 0, maxv));
                     }
                 }
             }
@@ -215,20 +237,18 @@ __device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int sca
         const int qc = qpc_map(avg + off, P.idc, P.bd_c);
         const int tc = c_tc[clamp3i(qc + 2 + 2 * to, 0, 53)] << sh;
         if (tc == 0) continue;
-        const Pl& pl = plane == 0 ? cb : cr;
+        const auto L = lines_of(plane == 0 ? cb : cr, vertical, edge, scan);
         for (int s = scan; s < scan + 4; ++s) {
             if (s >= scan_max) continue;
-            // p1, p0 | q0, q1 across the edge, in chroma plane coordinates
-            const int xp0 = vertical ? edge - 1 : s, yp0 = vertical ? s : edge - 1;
-            const int xp1 = vertical ? edge - 2 : s, yp1 = vertical ? s : edge - 2;
-            const int xq0 = vertical ? edge : s, yq0 = vertical ? s : edge;
-            const int xq1 = vertical ? edge + 1 : s, yq1 = vertical ? s : edge + 1;
-            const int p0 = pl.ld(xp0, yp0), p1 = pl.ld(xp1, yp1);
-            const int q0 = pl.ld(xq0, yq0), q1 = pl.ld(xq1, yq1);
+            const int l = s - scan;
+            // p1, p0 | q0, q1 across the edge (taps -2, -1 | 0, 1 of line l)
+            const int p0 = L.ld(l, -1), p1 = L.ld(l, -2), q0 = L.ld(l, 0), q1 = L.ld(l, 1);
             const int delta = clamp3i((((q0 - p0) * 4 + p1 - q1 + 4) >> 3), -tc, tc);
             if (delta != 0) {  // exemption by the luma positions of p0 / q0
-                if (!exempt_of(cl, xp0 * P.sub_w, yp0 * P.sub_h)) pl.st(xp0, yp0, clamp3i(p0 + delta, 0, maxv));
-                if (!exempt_of(cl, xq0 * P.sub_w, yq0 * P.sub_h)) pl.st(xq0, yq0, clamp3i(q0 - delta, 0, maxv));
+                const int xp0 = vertical ? edge - 1 : s, yp0 = vertical ? s : edge - 1;
+                const int xq0 = vertical ? edge : s, yq0 = vertical ? s : edge;
+                if (!exempt_of(cl, xp0 * P.sub_w, yp0 * P.sub_h)) L.st(l, -1, clamp3i(p0 + delta, 0, maxv));
+                if (!exempt_of(cl, xq0 * P.sub_w, yq0 * P.sub_h)) L.st(l, 0, clamp3i(q0 - delta, 0, maxv));
             }
         }
     }
@@ -934,7 +954,6 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
             const int copy_w = min(P.crop_w, max(P.canvas_w - P.dst_x, 0));
             const int copy_h = min(P.crop_h, max(P.canvas_h - P.dst_y, 0));
             const RgbCoef kc = rgb_coef(P);
-            const TileComp& L = tc[0];
             for (int i = tid; i < (kTile / 4) * kTile; i += kTileThreads) {
                 const int x0 = X + 4 * (i % (kTile / 4)), yy = Y + i / (kTile / 4);
                 if (x0 >= copy_w || yy >= copy_h) continue;
