@@ -366,6 +366,15 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
     __syncwarp();
 }
 
+// Records per warp step of k_residual: a warp loads 32 consecutive records
+// at once (one per lane, coalesced), finds their pictures in parallel and
+// prefetches their coefficients into L2, then transforms them one by one.
+constexpr int kResChunk = 32;
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <int kIdct>
 __global__ void __launch_bounds__(kResWarps * 32)
 k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_prefix, uint32_t n_pics,
@@ -374,48 +383,82 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
     __shared__ __align__(16) int16_t scr[kResWarps][2][32 * kScr];  // per warp: buf, tmp (contiguous)
     for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) dct[i] = (int16_t)dct_entry(32, i / 32, i % 32);
     __syncthreads();
+    constexpr unsigned kAll = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t total = rec_prefix[n_pics];
-    for (uint32_t g = rec_prefix[0] + blockIdx.x * kResWarps + warp; g < total; g += gridDim.x * kResWarps) {
-        // picture of global record g (binary search in the prefix)
-        uint32_t lo = 0, hi = n_pics;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (rec_prefix[mid] <= g) lo = mid; else hi = mid;
-        }
-        const DevPic& P = pics[lo];
-        const hpvcd_tu t = P.tus[g - rec_prefix[lo]];
-        if (!(t.flags & HPVCD_TU_CBF)) continue;
-        if ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && t.comp && t.res_scale) continue;  // k_ccp's
-        const int c = t.comp;
-        const int ncomp = P.idc ? 3 : 1;
-        const int n = 1 << t.log2n;
-        const int pw = c < 3 && c ? P.cw : P.w, ph = c < 3 && c ? P.ch : P.h;
-        if (c >= ncomp || t.log2n < 2 || t.log2n > 5 || (int)t.x >= pw || (int)t.y >= ph ||
-            (uint64_t)t.coeff_off + (uint64_t)n * n > P.n_coeffs) {
-            if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
-            continue;
-        }
-        const int x0 = t.x, y0 = t.y;
-        const bool in_plane = (P.flags & HPVCD_PIC_PRED_IN_PLANE) || !(t.flags & HPVCD_TU_INTRA);
-        if (in_plane) {  // prediction already in the plane: add + clip (reconstruct.rs:214-251)
-            void* pl = P.rec[c];
-            const int mx = (1 << (c ? P.bd_c : P.bd)) - 1;
-            const int keep = (t.flags & HPVCD_TU_PCM) ? 0 : 1;  // I_PCM samples replace the plane's
-            tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
-                const int x = x0 + m, y = y0 + r;
-                if (x < pw && y < ph) {
-                    const size_t idx = (size_t)y * pw + x;
-                    store_sample(pl, P.bps, idx, clamp3i(keep * load_sample(pl, P.bps, idx) + v, 0, mx));
+    const uint32_t first = rec_prefix[0], total = rec_prefix[n_pics];
+    const uint32_t n_chunks = (total - first + kResChunk - 1) / kResChunk;
+    for (uint32_t ch = blockIdx.x * kResWarps + warp; ch < n_chunks; ch += gridDim.x * kResWarps) {
+        const uint32_t g0 = first + ch * kResChunk;
+        // ---- this lane's record: its picture (binary search in the prefix),
+        // the record, and an L2 prefetch of its coefficients ----
+        const uint32_t gl = g0 + lane;
+        uint32_t pic = 0;
+        uint4 r4 = make_uint4(0u, 0u, 0u, 0u);
+        if (gl < total) {
+            uint32_t lo = 0, hi = n_pics;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (rec_prefix[mid] <= gl) lo = mid; else hi = mid;
+            }
+            pic = lo;
+            const DevPic& P = pics[lo];
+            r4 = *(const uint4*)(P.tus + (gl - rec_prefix[lo]));  // records are 16-byte aligned
+            hpvcd_tu t;
+            memcpy(&t, &r4, sizeof(t));
+            if ((t.flags & HPVCD_TU_CBF) && t.log2n >= 2 && t.log2n <= 5) {
+                const uint32_t esz = (P.flags & HPVCD_PIC_COEFF8) ? 1u : 2u;
+                const uint64_t n2 = 1ull << (2 * t.log2n);
+                if ((uint64_t)t.coeff_off + n2 <= P.n_coeffs) {
+                    const char* b = (const char*)P.coeffs + (uint64_t)t.coeff_off * esz;
+                    const char* e = b + n2 * esz;
+                    for (const char* q = (const char*)((uintptr_t)b & ~(uintptr_t)127); q < e; q += 128) prefetch_l2(q);
                 }
-            });
-        } else {
-            int16_t* rp = P.res[c];
-            const int rs = P.res_stride[c];
-            tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
-                const int x = x0 + m, y = y0 + r;
-                if (x < pw && y < ph) rp[(size_t)y * rs + x] = (int16_t)sat16(v);
-            });
+            }
+        }
+        // ---- the chunk's records one by one ----
+        const uint32_t nrec = min((uint32_t)kResChunk, total - g0);
+        for (uint32_t j = 0; j < nrec; ++j) {
+            const uint32_t pj = __shfl_sync(kAll, pic, j);
+            uint4 w4;
+            w4.x = __shfl_sync(kAll, r4.x, j);
+            w4.y = __shfl_sync(kAll, r4.y, j);
+            w4.z = __shfl_sync(kAll, r4.z, j);
+            w4.w = __shfl_sync(kAll, r4.w, j);
+            hpvcd_tu t;
+            memcpy(&t, &w4, sizeof(t));
+            const DevPic& P = pics[pj];
+            if (!(t.flags & HPVCD_TU_CBF)) continue;
+            if ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && t.comp && t.res_scale) continue;  // k_ccp's
+            const int c = t.comp;
+            const int ncomp = P.idc ? 3 : 1;
+            const int n = 1 << t.log2n;
+            const int pw = c < 3 && c ? P.cw : P.w, ph = c < 3 && c ? P.ch : P.h;
+            if (c >= ncomp || t.log2n < 2 || t.log2n > 5 || (int)t.x >= pw || (int)t.y >= ph ||
+                (uint64_t)t.coeff_off + (uint64_t)n * n > P.n_coeffs) {
+                if (lane == 0) atomicOr(dev_err, DEV_ERR_BITSTREAM);
+                continue;
+            }
+            const int x0 = t.x, y0 = t.y;
+            const bool in_plane = (P.flags & HPVCD_PIC_PRED_IN_PLANE) || !(t.flags & HPVCD_TU_INTRA);
+            if (in_plane) {  // prediction already in the plane: add + clip (reconstruct.rs:214-251)
+                void* pl = P.rec[c];
+                const int mx = (1 << (c ? P.bd_c : P.bd)) - 1;
+                const int keep = (t.flags & HPVCD_TU_PCM) ? 0 : 1;  // I_PCM samples replace the plane's
+                tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
+                    const int x = x0 + m, y = y0 + r;
+                    if (x < pw && y < ph) {
+                        const size_t idx = (size_t)y * pw + x;
+                        store_sample(pl, P.bps, idx, clamp3i(keep * load_sample(pl, P.bps, idx) + v, 0, mx));
+                    }
+                });
+            } else {
+                int16_t* rp = P.res[c];
+                const int rs = P.res_stride[c];
+                tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
+                    const int x = x0 + m, y = y0 + r;
+                    if (x < pw && y < ph) rp[(size_t)y * rs + x] = (int16_t)sat16(v);
+                });
+            }
         }
     }
 }
@@ -1630,7 +1673,8 @@ extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const ui
                                              uint32_t n_pics, uint32_t total_records, uint32_t* dev_err,
                                              int sms, int idct, cudaStream_t stream) {
     if (total_records == 0) return cudaSuccess;
-    const uint32_t blocks_needed = (total_records + hpvcd::kResWarps - 1) / hpvcd::kResWarps;
+    const uint32_t chunks = (total_records + hpvcd::kResChunk - 1) / hpvcd::kResChunk;
+    const uint32_t blocks_needed = (chunks + hpvcd::kResWarps - 1) / hpvcd::kResWarps;
     const uint32_t cap = (uint32_t)sms * 8u;
     const int grid = (int)(blocks_needed < cap ? blocks_needed : cap);
     if (idct == hpvcd::kIdctButterfly)
