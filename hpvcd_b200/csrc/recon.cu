@@ -52,6 +52,7 @@ constexpr int kScr = 33;  // padded row stride of the transform scratch
 // Inverse-transform variants of k_residual (schedule knob; pixels identical).
 constexpr int kIdctMatrix = 0;     // matrix product, all-zero rows / columns skipped
 constexpr int kIdctButterfly = 1;  // even-odd butterflies for 16x16 and 32x32 TBs
+constexpr int kIdctTensor = 2;     // integer tensor-core products (int8 halves) for 16x16 and 32x32 TBs
 
 __device__ __forceinline__ int dct_entry(int n, int k, int m) {
     if (k == 0) return 64;
@@ -137,6 +138,175 @@ __device__ __forceinline__ void bf_stage_k(int kcount, const int16_t* src, int l
 }
 
 // ===========================================================================
+// Integer tensor-core inverse transform of 16x16 and 32x32 TBs.
+//
+// Both stages are products with the H.265 basis T (entries in [-90, 90], an
+// s8 value): stage 1 tmp = T^T * D over the dequantised coefficients D,
+// stage 2 out = tmp * T.  The int16 operand X of each product is split
+// exactly into a signed high byte and an unsigned low byte, X = 256 * hi +
+// lo, and the product is 256 * (T * hi) + (T * lo): two mma.sync products
+// with s32 accumulation.  No sum overflows (|sum| <= 32 * 90 * 32768 <
+// 2^31), so the result is the reference's integer sum bit for bit; the
+// rounding, shift and clip of each stage are applied to it unchanged.
+// Fragments follow the PTX layouts of mma.m16n8k32 (32x32 TBs) and
+// mma.m16n8k16 (16x16 TBs) with 8-bit operands: lane = 4 * group + t; an A
+// register holds four consecutive K entries of one row (row group or group
+// + 8), a B register four consecutive K entries of one column (group), a
+// C/D register pair two adjacent columns (2t, 2t + 1) of one row.
+// ===========================================================================
+__device__ __forceinline__ void mma32(int (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1, bool a_u8,
+                                      bool b_u8) {
+    // D += A * B, A 16x32 (row), B 32x8 (col), 8-bit operands, s32 accumulation
+    if (!a_u8 && !b_u8)
+        asm volatile("mma.sync.aligned.m16n8k32.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                     "{%0,%1,%2,%3};"
+                     : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+                     : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    else if (!a_u8)
+        asm volatile("mma.sync.aligned.m16n8k32.row.col.s32.s8.u8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                     "{%0,%1,%2,%3};"
+                     : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+                     : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    else
+        asm volatile("mma.sync.aligned.m16n8k32.row.col.s32.u8.s8.s32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                     "{%0,%1,%2,%3};"
+                     : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+                     : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ void mma16(int (&d)[4], uint32_t a0, uint32_t a1, uint32_t b0, bool a_u8, bool b_u8) {
+    // D += A * B, A 16x16 (row), B 16x8 (col), 8-bit operands, s32 accumulation
+    if (!a_u8 && !b_u8)
+        asm volatile("mma.sync.aligned.m16n8k16.row.col.s32.s8.s8.s32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                     : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+                     : "r"(a0), "r"(a1), "r"(b0));
+    else if (!a_u8)
+        asm volatile("mma.sync.aligned.m16n8k16.row.col.s32.s8.u8.s32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                     : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+                     : "r"(a0), "r"(a1), "r"(b0));
+    else
+        asm volatile("mma.sync.aligned.m16n8k16.row.col.s32.u8.s8.s32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                     : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+                     : "r"(a0), "r"(a1), "r"(b0));
+}
+
+// Basis fragments, per lane, in shared memory (index [entry][lane]):
+//   s1a32: T^T as the A operand of stage 1, 32x32: 2 row tiles x 4 registers
+//   s2b32: T as the B operand of stage 2, 32x32: 4 column tiles x 2 registers
+//   s1a16: T^T, 16x16: 2 registers;  s2b16: T, 16x16: 2 column tiles x 1 register
+constexpr int kFragS1A32 = 0, kFragS2B32 = 8, kFragS1A16 = 16, kFragS2B16 = 18, kFragEntries = 20;
+
+__device__ __forceinline__ uint32_t pack4(int a, int b, int c, int d) {
+    return (uint32_t)(a & 0xff) | ((uint32_t)(b & 0xff) << 8) | ((uint32_t)(c & 0xff) << 16) | ((uint32_t)(d & 0xff) << 24);
+}
+
+__device__ void build_basis_frags(uint32_t* frags, int tid, int nthreads) {
+    for (int e = tid; e < kFragEntries * 32; e += nthreads) {
+        const int entry = e >> 5, lane = e & 31, g = lane >> 2, t = lane & 3;
+        int v[4];
+        if (entry < kFragS2B32) {  // A of stage 1, n = 32: A[m][k] = T[k][m]
+            const int mt = entry >> 2, reg = entry & 3;
+            const int m = mt * 16 + g + (reg & 1) * 8, k0 = (reg >> 1) * 16 + 4 * t;
+            for (int i = 0; i < 4; ++i) v[i] = dct_entry(32, k0 + i, m);
+        } else if (entry < kFragS1A16) {  // B of stage 2, n = 32: B[k][m] = T[k][m]
+            const int nt = (entry - kFragS2B32) >> 1, reg = (entry - kFragS2B32) & 1;
+            const int m = nt * 8 + g, k0 = reg * 16 + 4 * t;
+            for (int i = 0; i < 4; ++i) v[i] = dct_entry(32, k0 + i, m);
+        } else if (entry < kFragS2B16) {  // A of stage 1, n = 16
+            const int reg = entry - kFragS1A16;
+            const int m = g + reg * 8, k0 = 4 * t;
+            for (int i = 0; i < 4; ++i) v[i] = dct_entry(16, k0 + i, m);
+        } else {  // B of stage 2, n = 16
+            const int nt = entry - kFragS2B16;
+            const int m = nt * 8 + g, k0 = 4 * t;
+            for (int i = 0; i < 4; ++i) v[i] = dct_entry(16, k0 + i, m);
+        }
+        frags[e] = pack4(v[0], v[1], v[2], v[3]);
+    }
+}
+
+// Four int16 values split into their high bytes (s8) and low bytes (u8).
+__device__ __forceinline__ void split4(int a, int b, int c, int d, uint32_t& hi, uint32_t& lo) {
+    hi = pack4(a >> 8, b >> 8, c >> 8, d >> 8);
+    lo = pack4(a, b, c, d);
+}
+
+// Both stages of an n x n (16 or 32) inverse DCT by one warp: buf holds the
+// dequantised coefficients (row k, column c, stride kScr), tmp receives
+// stage 1; emit(r, m, v) gets every output with the reference's storage.
+template <int N, typename Emit>
+__device__ __forceinline__ void idct_tensor(const int16_t* buf, int16_t* tmp, const uint32_t* frags, int bd, bool i16s,
+                                            int lane, Emit emit) {
+    constexpr int MT = N / 16, NT = N / 8;  // row tiles, column tiles
+    const int g = lane >> 2, t = lane & 3;
+    // ---- stage 1: tmp[m][c] = clip((sum_k T[k][m] D[k][c] + 64) >> 7) ----
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+        const int c = nt * 8 + g;
+        uint32_t bh[2], bl[2];
+#pragma unroll
+        for (int reg = 0; reg < (N == 32 ? 2 : 1); ++reg) {
+            const int k0 = reg * 16 + 4 * t;
+            split4(buf[k0 * kScr + c], buf[(k0 + 1) * kScr + c], buf[(k0 + 2) * kScr + c], buf[(k0 + 3) * kScr + c],
+                   bh[reg], bl[reg]);
+        }
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            int dh[4] = {0, 0, 0, 0}, dl[4] = {0, 0, 0, 0};
+            if constexpr (N == 32) {
+                const uint32_t a[4] = {frags[(kFragS1A32 + mt * 4 + 0) * 32 + lane], frags[(kFragS1A32 + mt * 4 + 1) * 32 + lane],
+                                       frags[(kFragS1A32 + mt * 4 + 2) * 32 + lane], frags[(kFragS1A32 + mt * 4 + 3) * 32 + lane]};
+                mma32(dh, a, bh[0], bh[1], false, false);
+                mma32(dl, a, bl[0], bl[1], false, true);
+            } else {
+                const uint32_t a0 = frags[(kFragS1A16 + 0) * 32 + lane], a1 = frags[(kFragS1A16 + 1) * 32 + lane];
+                mma16(dh, a0, a1, bh[0], false, false);
+                mma16(dl, a0, a1, bl[0], false, true);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int m = mt * 16 + g + (e >> 1) * 8, cc = nt * 8 + 2 * t + (e & 1);
+                const int acc = dh[e] * 256 + dl[e];
+                tmp[m * kScr + cc] = (int16_t)clamp3i((acc + 64) >> 7, -32768, 32767);
+            }
+        }
+    }
+    __syncwarp();
+    // ---- stage 2: out[r][m] = (sum_k tmp[r][k] T[k][m] + add2) >> shift2 ----
+    const int shift2 = 20 - bd;
+    const int add2 = 1 << (shift2 - 1);
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+        uint32_t ah[4], al[4];
+#pragma unroll
+        for (int reg = 0; reg < (N == 32 ? 4 : 2); ++reg) {
+            const int r = mt * 16 + g + (reg & 1) * 8, k0 = (reg >> 1) * 16 + 4 * t;
+            const int16_t* row = tmp + r * kScr + k0;
+            split4(row[0], row[1], row[2], row[3], ah[reg], al[reg]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+            int dh[4] = {0, 0, 0, 0}, dl[4] = {0, 0, 0, 0};
+            if constexpr (N == 32) {
+                const uint32_t b0 = frags[(kFragS2B32 + nt * 2 + 0) * 32 + lane], b1 = frags[(kFragS2B32 + nt * 2 + 1) * 32 + lane];
+                mma32(dh, ah, b0, b1, false, false);
+                mma32(dl, al, b0, b1, true, false);
+            } else {
+                const uint32_t b0 = frags[(kFragS2B16 + nt) * 32 + lane];
+                mma16(dh, ah[0], ah[1], b0, false, false);
+                mma16(dl, al[0], al[1], b0, true, false);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = mt * 16 + g + (e >> 1) * 8, m = nt * 8 + 2 * t + (e & 1);
+                const int v = (dh[e] * 256 + dl[e] + add2) >> shift2;
+                emit(r, m, i16s ? (int)(int16_t)v : v);
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// ===========================================================================
 // k_residual
 // ===========================================================================
 constexpr int kResWarps = 8;
@@ -148,7 +318,8 @@ constexpr int kResWarps = 8;
 // path for chroma TBs with cross-component prediction, decode.rs:5313-5316).
 template <int kIdct, typename Emit>
 __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16_t* dct, int16_t* buf,
-                                 int16_t* tmp, int lane, Emit emit, bool allow16 = true) {
+                                 int16_t* tmp, int lane, Emit emit, bool allow16 = true,
+                                 const uint32_t* frags = nullptr) {
     const int n = 1 << t.log2n;
     const bool luma = t.comp == 0;
     const int bd = luma ? P.bd : P.bd_c;
@@ -303,6 +474,13 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
     for (int o = 16; o; o >>= 1) rows = max(rows, __shfl_xor_sync(0xffffffffu, rows, o));
     __syncwarp();
     const bool dst = luma && n == 4 && (t.flags & HPVCD_TU_INTRA);
+    if (kIdct == kIdctTensor && n >= 16) {
+        if (n == 16)
+            idct_tensor<16>(buf, tmp, frags, bd, i16s, lane, emit);
+        else
+            idct_tensor<32>(buf, tmp, frags, bd, i16s, lane, emit);
+        return;
+    }
     if (kIdct == kIdctButterfly && n >= 16) {
         // stage 1, lane = column: rows >= `rows` are zero
         auto st1 = [](int acc) { return clamp3i((acc + 64) >> 7, -32768, 32767); };
@@ -381,7 +559,9 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
            uint32_t* dev_err) {
     __shared__ int16_t dct[32 * 32];
     __shared__ __align__(16) int16_t scr[kResWarps][2][32 * kScr];  // per warp: buf, tmp (contiguous)
+    __shared__ uint32_t frags[kIdct == kIdctTensor ? kFragEntries * 32 : 1];
     for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) dct[i] = (int16_t)dct_entry(32, i / 32, i % 32);
+    if (kIdct == kIdctTensor) build_basis_frags(frags, threadIdx.x, blockDim.x);
     __syncthreads();
     constexpr unsigned kAll = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -444,20 +624,26 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
                 void* pl = P.rec[c];
                 const int mx = (1 << (c ? P.bd_c : P.bd)) - 1;
                 const int keep = (t.flags & HPVCD_TU_PCM) ? 0 : 1;  // I_PCM samples replace the plane's
-                tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
-                    const int x = x0 + m, y = y0 + r;
-                    if (x < pw && y < ph) {
-                        const size_t idx = (size_t)y * pw + x;
-                        store_sample(pl, P.bps, idx, clamp3i(keep * load_sample(pl, P.bps, idx) + v, 0, mx));
-                    }
-                });
+                tb_residual_warp<kIdct>(
+                    P, t, dct, scr[warp][0], scr[warp][1], lane,
+                    [&](int r, int m, int v) {
+                        const int x = x0 + m, y = y0 + r;
+                        if (x < pw && y < ph) {
+                            const size_t idx = (size_t)y * pw + x;
+                            store_sample(pl, P.bps, idx, clamp3i(keep * load_sample(pl, P.bps, idx) + v, 0, mx));
+                        }
+                    },
+                    true, frags);
             } else {
                 int16_t* rp = P.res[c];
                 const int rs = P.res_stride[c];
-                tb_residual_warp<kIdct>(P, t, dct, scr[warp][0], scr[warp][1], lane, [&](int r, int m, int v) {
-                    const int x = x0 + m, y = y0 + r;
-                    if (x < pw && y < ph) rp[(size_t)y * rs + x] = (int16_t)sat16(v);
-                });
+                tb_residual_warp<kIdct>(
+                    P, t, dct, scr[warp][0], scr[warp][1], lane,
+                    [&](int r, int m, int v) {
+                        const int x = x0 + m, y = y0 + r;
+                        if (x < pw && y < ph) rp[(size_t)y * rs + x] = (int16_t)sat16(v);
+                    },
+                    true, frags);
             }
         }
     }
@@ -1677,7 +1863,10 @@ extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const ui
     const uint32_t blocks_needed = (chunks + hpvcd::kResWarps - 1) / hpvcd::kResWarps;
     const uint32_t cap = (uint32_t)sms * 8u;
     const int grid = (int)(blocks_needed < cap ? blocks_needed : cap);
-    if (idct == hpvcd::kIdctButterfly)
+    if (idct == hpvcd::kIdctTensor)
+        hpvcd::k_residual<hpvcd::kIdctTensor><<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix, n_pics,
+                                                                                        dev_err);
+    else if (idct == hpvcd::kIdctButterfly)
         hpvcd::k_residual<hpvcd::kIdctButterfly><<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix,
                                                                                           n_pics, dev_err);
     else

@@ -481,7 +481,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         P->out.kind = HPVCD_OUT_YUV;
     }
     if (sched) {
-        if (sched->idct > 1 || sched->chroma_warps > 2) {
+        if (sched->idct > 2 || sched->chroma_warps > 2) {
             delete P;
             return HPVCD_ERR_INVALID_ARG;
         }
@@ -1311,7 +1311,7 @@ HPVCD_API hpvcd_status hpvcd_plan_autotune(hpvcd_plan* plan, const hpvcd_sched* 
 HPVCD_API hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched) {
     if (!plan) return HPVCD_ERR_INVALID_ARG;
     const hpvcd_sched next = sched ? *sched : hpvcd_sched{};
-    if (next.idct > 1 || next.chroma_warps > 2 || next.wave > 1) return HPVCD_ERR_INVALID_ARG;
+    if (next.idct > 2 || next.chroma_warps > 2 || next.wave > 1) return HPVCD_ERR_INVALID_ARG;
     if (std::memcmp(&next, &plan->sched, sizeof(next)) == 0) return HPVCD_OK;
     plan->sched = next;
     // graphs captured with the previous schedule hold its kernels

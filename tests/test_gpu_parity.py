@@ -418,7 +418,7 @@ def test_schedule_variants_bit_exact():
     pics = s.pictures()
     ref, _ = O.decode_batch(pics)
     plan = DevicePlan(pics)
-    for idct in (0, 1):
+    for idct in (0, 1, 2):      # matrix, butterflies, integer tensor cores
         for cw in (1, 2):       # chroma warps of the wavefront kernel
             for ctas in (0, 1):
                 for wave in (0, 1):   # quadrant-level / whole-CTU wavefront
@@ -429,6 +429,8 @@ def test_schedule_variants_bit_exact():
                     assert_planes_equal(got, ref, f"idct={idct} chroma_warps={cw} ctas={ctas} wave={wave}")
     with pytest.raises(abi.HpvcdError):
         plan.set_sched(abi.Sched(0, 1, 0, 2))
+    with pytest.raises(abi.HpvcdError):
+        plan.set_sched(abi.Sched(3, 1, 0, 0))
     plan.close()
 
 
