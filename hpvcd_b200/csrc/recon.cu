@@ -1852,7 +1852,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
 }  // namespace hpvcd
 
 extern "C" size_t hpvcd_recon_smem_bytes(int cfmt, int chroma_warps) {
-    return hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(chroma_warps == 2 ? 2 : 1)).total;
+    return hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(chroma_warps == 1 ? 1 : 2)).total;
 }
 
 extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const uint32_t* rec_prefix,
@@ -1863,10 +1863,11 @@ extern "C" cudaError_t hpvcd_launch_residual(const hpvcd::DevPic* pics, const ui
     const uint32_t blocks_needed = (chunks + hpvcd::kResWarps - 1) / hpvcd::kResWarps;
     const uint32_t cap = (uint32_t)sms * 8u;
     const int grid = (int)(blocks_needed < cap ? blocks_needed : cap);
-    if (idct == hpvcd::kIdctTensor)
+    // schedule value: 0 integer tensor cores (the default), 1 butterflies, 2 matrix product
+    if (idct == 0)
         hpvcd::k_residual<hpvcd::kIdctTensor><<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix, n_pics,
                                                                                         dev_err);
-    else if (idct == hpvcd::kIdctButterfly)
+    else if (idct == 1)
         hpvcd::k_residual<hpvcd::kIdctButterfly><<<grid, hpvcd::kResWarps * 32, 0, stream>>>(pics, rec_prefix,
                                                                                           n_pics, dev_err);
     else
@@ -1895,7 +1896,8 @@ extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd
     // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
     // when the plan was built (no non-stream API call here, so launches can
     // be captured into CUDA graphs)
-    const int cw = chroma_warps == 2 ? 2 : 1;
+    // schedule value: 1 one chroma warp (Cb, then Cr), 0 or 2 one warp per chroma component
+    const int cw = chroma_warps == 1 ? 1 : 2;
     const size_t smem = hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(cw)).total;
     const int threads = 32 * hpvcd::recon_warps(cw);
     // default: 2^22 polls of >= 64 ns each bound one neighbour wait to a few
@@ -1922,7 +1924,7 @@ extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd
 // to the 4:4:4 layout of three warps, the largest).
 extern "C" int hpvcd_recon_occupancy(int cfmt, int chroma_warps) {
     int blocks = 0;
-    const int cw = chroma_warps == 2 ? 2 : 1;
+    const int cw = chroma_warps == 1 ? 1 : 2;
     const size_t smem = hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(cw)).total;
     const int lim = (int)hpvcd::ReconLayout(hpvcd::kFmt444, hpvcd::recon_warps(2)).total;
     cudaFuncSetAttribute(hpvcd::k_recon<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);

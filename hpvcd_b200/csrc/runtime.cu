@@ -218,7 +218,7 @@ struct hpvcd_plan {
     };
     std::vector<Wave> waves;
     int occ[3][2] = {{1, 1}, {1, 1}, {1, 1}};  // k_recon CTAs per SM by class and chroma warps (1, 2)
-    int occ_of(int cfmt) const { return occ[cfmt][sched.chroma_warps == 2 ? 1 : 0]; }
+    int occ_of(int cfmt) const { return occ[cfmt][sched.chroma_warps == 1 ? 0 : 1]; }
     int sms = 148;
     int max_rgb = 0;  // largest RGB job of one picture, in 4-pixel quads
     uint32_t launches_per_run = 0;

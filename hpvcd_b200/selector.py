@@ -1,12 +1,11 @@
 """Schedule selection: exhaustive autotuning and the learned selector.
 
 The schedule of a batch (include/hpvcd_gpu.h `hpvcd_sched`) picks kernel
-variants that never change pixels: the inverse transform of k_residual
-(matrix product with zero rows / columns skipped, or even-odd butterflies for
-16x16 / 32x32), the chroma warps of the wavefront kernel k_recon (one warp
-walking Cb then Cr in a CTA of two warps, or one warp per chroma component in
-a CTA of three) and the persistent k_recon CTAs per SM (occupancy maximum, or
-one).  Which is fastest depends on the batch: its TB-size mix,
+variants that never change pixels: the inverse transform of 16x16 / 32x32 TBs
+in k_residual (integer tensor-core products, or even-odd butterflies), the
+chroma warps of the wavefront kernel k_recon (one warp per chroma component
+in a CTA of three, or one warp walking Cb then Cr in a CTA of two) and the
+persistent k_recon CTAs per SM (occupancy maximum, or one).  Which is fastest depends on the batch: its TB-size mix,
 coefficient density, QP, intra share, size and picture count.
 
 * Exhaustive autotuning (`hpvcd_plan_autotune`) times every schedule on the
@@ -39,8 +38,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS_PATH = os.path.join(HERE, "selector_weights.npz")
 
 # The candidate schedules, in output order of the network.
-SCHEDULES = [abi.Sched(idct, cw, ctas, 0) for idct in (0, 1) for cw in (1, 2) for ctas in (0, 1)]
-DEFAULT = 0  # (matrix transform, one-warp walk, occupancy maximum): the all-zero schedule
+SCHEDULES = [abi.Sched(idct, cw, ctas, 0) for idct in (0, 1) for cw in (0, 1) for ctas in (0, 1)]
+DEFAULT = 0  # (tensor-core transform, a warp per chroma component, occupancy maximum): the all-zero schedule
 K = len(SCHEDULES)
 
 

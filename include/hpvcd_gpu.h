@@ -478,12 +478,13 @@ typedef struct hpvcd_plan hpvcd_plan;
 /* Schedule knobs chosen by the autotuner / schedule selector.  They never
  * change pixels, only speed.  All zero is the default schedule. */
 typedef struct hpvcd_sched {
-    uint32_t idct;              /* k_residual inverse transform: 0 matrix product with all-zero
-                                   rows / columns skipped, 1 even-odd butterflies for 16x16 / 32x32,
-                                   2 integer tensor-core products (int16 operands split into
-                                   int8 halves, exact) for 16x16 / 32x32 */
-    uint32_t chroma_warps;      /* chroma walk of the wavefront kernel: 0|1 one warp (Cb, then Cr;
-                                   two warps per CTA), 2 one warp per component (three per CTA) */
+    uint32_t idct;              /* k_residual inverse transform of 16x16 / 32x32 TBs: 0 integer
+                                   tensor-core products (int16 operands split exactly into int8
+                                   halves), 1 even-odd butterflies, 2 matrix product with all-zero
+                                   rows / columns skipped */
+    uint32_t chroma_warps;      /* chroma walk of the wavefront kernel: 0|2 one warp per chroma
+                                   component (three warps per CTA), 1 one warp for Cb, then Cr
+                                   (two warps per CTA: more CTAs per SM) */
     uint32_t recon_ctas_per_sm; /* persistent wavefront CTAs per SM (0 -> occupancy max) */
     uint32_t wave;              /* wavefront synchronisation: 0 per quadrant (a CTU is walked while
                                    its left / above-right neighbours still are), 1 whole CTUs (one
