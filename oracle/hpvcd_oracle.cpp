@@ -7,10 +7,18 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
+#include <functional>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
+
+#include "cpu_simd.h"
 
 namespace {
 
@@ -729,6 +737,36 @@ void yuv_to_rgb16(const uint16_t* Y, const uint16_t* Cb, const uint16_t* Cr, int
 }
 
 // ---------------------------------------------------------------------------
+// Kernel set of a decode (exec.rs:31-77 ExecContext: the reference calls its
+// per-block kernels through a table of function pointers, the SIMD set
+// picked by CPU feature, avx/mod.rs).  The scalar set is the restatement
+// above; the AVX2 set (cpu_simd.cpp) computes the same integers and serves
+// the timed CPU reference arm.  Per thread: a banded decode sets it in every
+// job it runs.
+// ---------------------------------------------------------------------------
+struct Kernels {
+    void (*inv_dct)(const int32_t*, int, int, int, int, bool, int32_t*);
+    void (*add_residual)(uint16_t*, int, const uint16_t*, const int32_t*, int, int, int, int);
+    void (*intra_predict)(int, const uint16_t*, const uint16_t*, int, bool, int, uint16_t*);
+    void (*sao_band)(uint16_t*, const uint16_t*, int, int, int, int, int, const int32_t*, int, int);
+    // edge offset without slice / tile restriction (NULL: the scalar template)
+    void (*sao_edge)(uint16_t*, const uint16_t*, int, int, int, int, int, int, const int32_t*, int, int);
+    bool simd_rgb;
+};
+
+void inv_dct_avx2(const int32_t* coeff, int n, int bd, int max_range, int nx, bool i16s, int32_t* out) {
+    if ((n == 16 || n == 32) && max_range == 15)
+        orc_simd::inv_dct(coeff, n, bd, nx, i16s, out);
+    else
+        inv_dct(coeff, n, bd, max_range, nx, i16s, out);
+}
+
+const Kernels kScalarKernels{inv_dct, add_residual, intra_predict, sao_band, nullptr, false};
+const Kernels kAvx2Kernels{inv_dct_avx2, orc_simd::add_residual, orc_simd::intra_predict, orc_simd::sao_band,
+                           orc_simd::sao_edge, true};
+thread_local const Kernels* tk = &kScalarKernels;
+
+// ---------------------------------------------------------------------------
 // Picture-level state
 // ---------------------------------------------------------------------------
 struct Geo {
@@ -828,12 +866,12 @@ void predict_block(const PicState& st, int comp, int x0, int y0, int n, int mode
     if (luma) {
         const bool strong = (p->flags & HPVCD_PIC_STRONG_SMOOTHING) != 0;
         intra_filter(above, left, n, mode, true, smoothing, strong, bd, fa, fl);
-        intra_predict(mode, fa, fl, n, true, bd, pred);
+        tk->intra_predict(mode, fa, fl, n, true, bd, pred);
     } else if (g.idc == 3) {
         intra_filter(above, left, n, mode, true, smoothing, false, bd, fa, fl);
-        intra_predict(mode, fa, fl, n, false, bd, pred);
+        tk->intra_predict(mode, fa, fl, n, false, bd, pred);
     } else {
-        intra_predict(mode, above, left, n, false, bd, pred);
+        tk->intra_predict(mode, above, left, n, false, bd, pred);
     }
 }
 
@@ -922,7 +960,7 @@ void tb_residual(const hpvcd_picture* p, const Geo& g, const hpvcd_tu& t, int32_
     if (luma && n == 4 && (t.flags & HPVCD_TU_INTRA))
         inv_dst4(deq, bd, 15, i16s, res);
     else
-        inv_dct(deq, n, bd, 15, t.nx ? t.nx : n, i16s, res);
+        tk->inv_dct(deq, n, bd, 15, t.nx ? t.nx : n, i16s, res);
 }
 
 int recon_picture(const hpvcd_picture* p, orc_planes* pl) {
@@ -990,7 +1028,7 @@ int recon_picture(const hpvcd_picture* p, orc_planes* pl) {
             }
         }
         if (vw > 0 && vh > 0)
-            add_residual(plane + (size_t)t.y * pw + t.x, pw, pred, res, n, vw, vh, bd);
+            tk->add_residual(plane + (size_t)t.y * pw + t.x, pw, pred, res, n, vw, vh, bd);
         if (luma) st.mark_decoded(t.x, t.y, n);
     }
     return HPVCD_OK;
@@ -1087,8 +1125,16 @@ int mc_picture(const hpvcd_picture* p, const orc_planes* refs, int n_refs, orc_p
 static uint8_t g_slice_disabled[256];
 static bool g_any_slice_disabled = false;
 
-// decode.rs:1774-2146 apply_deblocking (single slice, PPS-level parameters).
-int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
+// decode.rs:1774-2146 apply_deblocking (single slice, PPS-level parameters):
+// luma vertical, luma horizontal, chroma vertical, chroma horizontal, in
+// that order.  Within a pass the segments of different CTB-row bands touch
+// disjoint rows (a vertical segment its own 4 rows; a horizontal edge e rows
+// e - 4 .. e + 3 of band [r0 - 4, r1 - 4)), so `run(count, body)` may run a
+// pass's bands in any order or at once: serially for apply_deblocking, on
+// the pool for the reference's banded driver (deblock.rs:1118
+// apply_deblocking_parallel).  Exempt samples are restored band by band.
+template <class Run>
+int deblock_picture_t(const hpvcd_picture* p, orc_planes* pl, Run run) {
     int rc = validate(p);
     if (rc) return rc;
     if (!(p->flags & HPVCD_PIC_DEBLOCK) || !p->cells) return HPVCD_OK;
@@ -1139,24 +1185,31 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
     auto exempt = [&](int lx, int ly) {
         return (cells[(size_t)(ly / 4) * g.gw + lx / 4].flags & HPVCD_CELL_EXEMPT) != 0;
     };
-    auto restore_luma = [&]() {
-        for (int y = 0; y < g.h; ++y)
+    auto restore_luma = [&](int y0, int y1) {
+        for (int y = std::max(y0, 0); y < std::min(y1, g.h); ++y)
             for (int x = 0; x < g.w; ++x)
                 if (exempt(x, y)) pl->y[(size_t)y * g.w + x] = sy[(size_t)y * g.w + x];
     };
-    auto restore_chroma = [&]() {
-        for (int cy = 0; cy < g.ch; ++cy)
+    auto restore_chroma = [&](int y0, int y1) {
+        for (int cy = std::max(y0, 0); cy < std::min(y1, g.ch); ++cy)
             for (int cx = 0; cx < g.cw; ++cx)
                 if (exempt(cx * g.sub_w, cy * g.sub_h)) {
                     pl->cb[(size_t)cy * g.cw + cx] = scb[(size_t)cy * g.cw + cx];
                     pl->cr[(size_t)cy * g.cw + cx] = scr[(size_t)cy * g.cw + cx];
                 }
     };
+    const int ctb = 1 << g.log2_ctb;
+    // band b of a pass over `rows` rows with bands `bh` high: rows [r0, r1)
+    // of its vertical segments / horizontal edges, and the rows it restores
+    auto bands_of = [](int rows, int bh) { return (rows + bh - 1) / bh; };
     const int maxv = (1 << g.bd) - 1;
+    const int nbl = bands_of(g.h, ctb);
     for (int pass = 0; pass < 2; ++pass) {
         const int edge_max = pass == 0 ? g.w : g.h, scan_max = pass == 0 ? g.h : g.w;
-        for (int edge = 8; edge <= edge_max - 4; edge += 8) {
-            for (int scan = 0; scan + 4 <= scan_max; scan += 4) {
+        run(nbl, [&](int band) {
+        const int r0 = band * ctb, r1 = std::min((band + 1) * ctb, g.h);
+        for (int edge = pass == 0 ? 8 : std::max(8, r0); edge <= edge_max - 4 && (pass == 0 || edge < r1); edge += 8) {
+            for (int scan = pass == 0 ? r0 : 0; scan + 4 <= scan_max && (pass == 1 || scan < r1); scan += 4) {
                 const int mid = scan + 1;
                 const int bs = pass == 0 ? bs_v(edge, mid) : bs_h(mid, edge);
                 if (bs == 0) continue;
@@ -1176,15 +1229,25 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
                 apply_luma(s, dec, dp1, dq1, tc, maxv);
             }
         }
-        if (any_exempt) restore_luma();
+        if (any_exempt) {
+            if (pass == 0)
+                restore_luma(r0, r1);
+            else
+                restore_luma(r0 - 4, band == nbl - 1 ? g.h : r1 - 4);
+        }
+        });
     }
     if (g.idc == 0) return HPVCD_OK;
     const int maxv_c = (1 << g.bd_c) - 1;
+    const int cband = std::max(ctb / g.sub_h, 8);
+    const int nbc = bands_of(g.ch, cband);
     for (int pass = 0; pass < 2; ++pass) {
         const int scan_max = pass == 0 ? g.ch : g.cw;
         const int cedge_max = pass == 0 ? g.cw : g.ch;
-        for (int edge = 8; edge <= cedge_max - 2; edge += 8) {
-            for (int scan = 0; scan + 4 <= scan_max; scan += 4) {
+        run(nbc, [&](int band) {
+        const int r0 = band * cband, r1 = std::min((band + 1) * cband, g.ch);
+        for (int edge = pass == 0 ? 8 : std::max(8, r0); edge <= cedge_max - 2 && (pass == 0 || edge < r1); edge += 8) {
+            for (int scan = pass == 0 ? r0 : 0; scan + 4 <= scan_max && (pass == 1 || scan < r1); scan += 4) {
                 const int mid = scan + 1;
                 const int lex = pass == 0 ? edge * g.sub_w : mid * g.sub_w;
                 const int ley = pass == 0 ? mid * g.sub_h : edge * g.sub_h;
@@ -1230,13 +1293,30 @@ int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
                 }
             }
         }
-        if (any_exempt) restore_chroma();
+        if (any_exempt) {
+            if (pass == 0)
+                restore_chroma(r0, r1);
+            else
+                restore_chroma(r0 - 4, band == nbc - 1 ? g.ch : r1 - 4);
+        }
+        });
     }
     return HPVCD_OK;
 }
 
+int deblock_picture(const hpvcd_picture* p, orc_planes* pl) {
+    return deblock_picture_t(p, pl, [](int count, const std::function<void(int)>& body) {
+        for (int b = 0; b < count; ++b) body(b);
+    });
+}
+
+
 // decode.rs:2258-2493 apply_sao (serial, boundary-unrestricted path).
-int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
+// Every CTB row reads the pre-SAO snapshot and writes its own rows, so
+// `run(count, body)` may run the CTB rows in any order or at once (sao.rs:807
+// apply_sao_parallel: CTB-row bands on the pool).
+template <class Run>
+int sao_picture_t(const hpvcd_picture* p, orc_planes* pl, Run run) {
     int rc = validate(p);
     if (rc) return rc;
     if (!p->sao) return HPVCD_OK;
@@ -1256,7 +1336,7 @@ int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
         ocb.assign(pl->cb, pl->cb + (size_t)g.cw * g.ch);
         ocr.assign(pl->cr, pl->cr + (size_t)g.cw * g.ch);
     }
-    for (int ry = 0; ry < g.ctb_rows; ++ry)
+    run(g.ctb_rows, [&](int ry) {
         for (int rx = 0; rx < g.ctb_cols; ++rx) {
             const hpvcd_sao_ctb& s = p->sao[(size_t)ry * g.ctb_cols + rx];
             const int x0 = rx * ctb, y0 = ry * ctb;
@@ -1275,7 +1355,9 @@ int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
                 const uint16_t* src = luma ? oy.data() : (c == 1 ? ocb.data() : ocr.data());
                 const int bd = luma ? g.bd : g.bd_c;
                 if (sc.type_idx == 1)
-                    sao_band(dst, src, pw, cx0, cy0, cx1, cy1, off, sc.band_pos, bd);
+                    tk->sao_band(dst, src, pw, cx0, cy0, cx1, cy1, off, sc.band_pos, bd);
+                else if (!p->ctb_region && tk->sao_edge)
+                    tk->sao_edge(dst, src, pw, ph, cx0, cy0, cx1, cy1, off, sc.eo_class, bd);
                 else
                     sao_edge(dst, src, pw, ph, cx0, cy0, cx1, cy1, off, sc.eo_class, bd,
                              [&](int x, int y, int nx, int ny) {  // sao.rs:380-425 (slice / tile part)
@@ -1287,13 +1369,13 @@ int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
                              });
             }
         }
-    // decode.rs:2444-2485: exempt samples keep their pre-SAO value.
-    if (p->cells) {
-        for (int y = 0; y < g.h; ++y)
+        // decode.rs:2444-2485: exempt samples keep their pre-SAO value.
+        if (!p->cells) return;
+        for (int y = ry * ctb; y < std::min((ry + 1) * ctb, g.h); ++y)
             for (int x = 0; x < g.w; ++x)
                 if (p->cells[(size_t)(y / 4) * g.gw + x / 4].flags & HPVCD_CELL_EXEMPT)
                     pl->y[(size_t)y * g.w + x] = oy[(size_t)y * g.w + x];
-        for (int cy = 0; cy < g.ch; ++cy)
+        for (int cy = ry * ctb / g.sub_h; cy < std::min((ry + 1) * ctb / g.sub_h, g.ch); ++cy)
             for (int cx = 0; cx < g.cw; ++cx) {
                 const int lx = cx * g.sub_w, ly = cy * g.sub_h;
                 if (p->cells[(size_t)(ly / 4) * g.gw + lx / 4].flags & HPVCD_CELL_EXEMPT) {
@@ -1301,8 +1383,225 @@ int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
                     pl->cr[(size_t)cy * g.cw + cx] = ocr[(size_t)cy * g.cw + cx];
                 }
             }
-    }
+    });
     return HPVCD_OK;
+}
+
+int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
+    return sao_picture_t(p, pl, [](int count, const std::function<void(int)>& body) {
+        for (int b = 0; b < count; ++b) body(b);
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Work-stealing pool (threadpool.rs:300-520): one job deque per worker; a
+// worker runs its own newest job, or steals the oldest job of another; a
+// thread waiting for the jobs of a parallel_for runs jobs meanwhile, so a
+// job may itself run a parallel_for (the grid rows' tile decodes run their
+// banded filters on the same pool).
+// ---------------------------------------------------------------------------
+class StealPool {
+public:
+    explicit StealPool(int threads) : q_((size_t)std::max(threads, 1)) {
+        for (auto& q : q_) q = std::make_unique<Deque>();
+        for (int i = 1; i < (int)q_.size(); ++i) th_.emplace_back([this, i] { worker(i); });
+    }
+    ~StealPool() {
+        stop_.store(true);
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    // body(i) for i in [0, count), on the pool; returns when all have run.
+    void parallel_for(int count, const std::function<void(int)>& body) {
+        if (count <= 0) return;
+        if (count == 1 || q_.size() == 1) {
+            for (int i = 0; i < count; ++i) body(i);
+            return;
+        }
+        std::atomic<int> left{count};
+        const int me = tls_id_ >= 0 ? tls_id_ : 0;
+        {
+            std::lock_guard<std::mutex> lk(q_[(size_t)me]->mu);
+            for (int i = count - 1; i >= 0; --i) q_[(size_t)me]->d.push_back(Job{&body, i, &left});
+        }
+        queued_.fetch_add(count);
+        cv_.notify_all();
+        while (left.load() > 0)
+            if (!run_one(me)) std::this_thread::yield();
+    }
+
+private:
+    struct Job {
+        const std::function<void(int)>* body;
+        int index;
+        std::atomic<int>* left;
+    };
+    struct Deque {
+        std::mutex mu;
+        std::deque<Job> d;
+    };
+    bool run_one(int me) {
+        Job j{};
+        bool got = false;
+        {
+            std::lock_guard<std::mutex> lk(q_[(size_t)me]->mu);
+            if (!q_[(size_t)me]->d.empty()) {
+                j = q_[(size_t)me]->d.back();
+                q_[(size_t)me]->d.pop_back();
+                got = true;
+            }
+        }
+        for (size_t k = 1; !got && k < q_.size(); ++k) {
+            Deque& o = *q_[(me + k) % q_.size()];
+            std::lock_guard<std::mutex> lk(o.mu);
+            if (!o.d.empty()) {
+                j = o.d.front();
+                o.d.pop_front();
+                got = true;
+            }
+        }
+        if (!got) return false;
+        queued_.fetch_sub(1);
+        (*j.body)(j.index);
+        j.left->fetch_sub(1);
+        return true;
+    }
+    void worker(int id) {
+        tls_id_ = id;
+        while (!stop_.load()) {
+            if (run_one(id)) continue;
+            std::unique_lock<std::mutex> lk(wait_mu_);
+            cv_.wait_for(lk, std::chrono::milliseconds(1), [&] { return queued_.load() > 0 || stop_.load(); });
+        }
+    }
+    std::vector<std::unique_ptr<Deque>> q_;
+    std::vector<std::thread> th_;
+    std::mutex wait_mu_;
+    std::condition_variable cv_;
+    std::atomic<int> queued_{0};
+    std::atomic<bool> stop_{false};
+    static thread_local int tls_id_;
+};
+thread_local int StealPool::tls_id_ = -1;
+
+// Q13 YCbCr -> RGB8 of rows [y0, y1) of a tile's crop onto its canvas
+// (yuv.rs:232 / :327 rows, lib.rs:1964-1978 >> (bd - 8), lib.rs:1610-1660
+// placement with cropping); the AVX2 row kernel for the matrices it covers.
+void tile_rgb_rows(const orc_planes& pl, const Geo& g, int matrix, bool full, int tw, int y0, int y1, uint8_t* canvas,
+                   int canvas_w, int dst_x, int dst_y, int copy_w) {
+    std::vector<uint16_t> buf((size_t)tw * 3);
+    const int shift = g.bd - 8;
+    const bool simd_ok = tk->simd_rgb && g.idc != 0 && g.bd <= 12 && matrix != HPVCD_MATRIX_IDENTITY &&
+                         matrix != HPVCD_MATRIX_YCGCO && g.sub_h <= 2;
+    int64_t cr_r0, cb_g0, cr_g0, cb_b0;
+    switch (matrix) {
+        case HPVCD_MATRIX_BT470BG:
+        case HPVCD_MATRIX_SMPTE170M: cr_r0 = 11485; cb_g0 = -2819; cr_g0 = -5851; cb_b0 = 14516; break;
+        case HPVCD_MATRIX_BT2020NCL: cr_r0 = 12080; cb_g0 = -1348; cr_g0 = -4681; cb_b0 = 17546; break;
+        default: cr_r0 = 12901; cb_g0 = -1534; cr_g0 = -3835; cb_b0 = 15201; break;
+    }
+    const int32_t k_y = full ? 8192 : 9539, k_uv = full ? 8192 : 9326;
+    const int32_t scale = 1 << (g.bd - 8);
+    const int32_t y_black = full ? 0 : 16 * scale, neutral = 128 * scale;
+    const int32_t cmax = g.bd == 8 ? 255 : (1 << g.bd) - 1;
+    for (int y = y0; y < y1; ++y) {
+        if (simd_ok) {
+            const int yr = std::min(y, g.h - 1), cr = std::min(y / g.sub_h, g.ch - 1);
+            orc_simd::rgb_row(pl.y + (size_t)yr * g.w, pl.cb + (size_t)cr * g.cw, pl.cr + (size_t)cr * g.cw, 0, tw, g.w,
+                              g.cw, g.sub_w, g.bd, k_y, y_black, neutral, (int32_t)((cr_r0 * k_uv + 4096) >> 13),
+                              (int32_t)((cb_g0 * k_uv + 4096) >> 13), (int32_t)((cr_g0 * k_uv + 4096) >> 13),
+                              (int32_t)((cb_b0 * k_uv + 4096) >> 13), cmax, buf.data());
+        } else {
+            yuv_to_rgb16(pl.y, pl.cb, pl.cr, g.w, g.h, g.idc, g.bd, tw, 1, 0, y, matrix, full, buf.data());
+        }
+        uint8_t* o = canvas + ((size_t)(dst_y + y) * canvas_w + dst_x) * 3;
+        for (int x = 0; x < copy_w * 3; ++x) o[x] = (uint8_t)(buf[x] >> shift);
+    }
+}
+
+// The reference's grid decode (lib.rs:1724 decode_grid -> :1680
+// fill_grid_bands): one job per grid row of tiles on the pool, each decoding
+// its tiles one after another; per tile the reconstruction (serial: no
+// wavefront parallel processing in these streams), the banded deblocking
+// and SAO drivers, and the banded RGB conversion into the canvas.  Intra /
+// residual pictures onto RGB8 canvases.
+int decode_grid_reference(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out, uint8_t* rgb, int threads,
+                          bool simd) {
+    if (!out || out->kind != HPVCD_OUT_RGB8 || !out->place || !rgb) return HPVCD_ERR_INVALID_ARG;
+    const uint32_t nc = out->n_canvases ? out->n_canvases : 1;
+    std::vector<hpvcd_canvas> cvs;
+    std::vector<size_t> offs;
+    size_t acc = 0;
+    for (uint32_t k = 0; k < nc; ++k) {
+        const hpvcd_canvas cv = out->n_canvases ? out->canvases[k]
+                                                : hpvcd_canvas{out->canvas_w, out->canvas_h, out->matrix,
+                                                               out->full_range, out->orientation};
+        if (cv.matrix == HPVCD_CANVAS_NATIVE || (cv.orientation > 1)) return HPVCD_ERR_UNSUPPORTED;
+        cvs.push_back(cv);
+        offs.push_back(acc);
+        acc += (size_t)cv.width * cv.height * 3;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const int rc = validate(&pics[i]);
+        if (rc) return rc;
+        if ((pics[i].flags & HPVCD_PIC_INTER) || out->place[i].canvas >= nc) return HPVCD_ERR_UNSUPPORTED;
+    }
+    // grid rows: tiles sharing a canvas and a top row, in submission order
+    std::map<std::pair<uint32_t, uint32_t>, std::vector<uint32_t>> row_of;
+    for (uint32_t i = 0; i < n; ++i) row_of[{out->place[i].canvas, out->place[i].dst_y}].push_back(i);
+    std::vector<std::vector<uint32_t>> rows;
+    for (auto& kv : row_of) rows.push_back(kv.second);
+    const Kernels* kset = simd ? &kAvx2Kernels : &kScalarKernels;
+    const Kernels* caller_set = tk;  // the calling thread runs jobs too: restored below
+    StealPool pool(threads);
+    std::atomic<int> err{0};
+    auto on_pool = [&](int count, const std::function<void(int)>& body) {
+        pool.parallel_for(count, [&](int b) {
+            tk = kset;
+            body(b);
+        });
+    };
+    pool.parallel_for((int)rows.size(), [&](int r) {
+        tk = kset;
+        for (const uint32_t i : rows[(size_t)r]) {
+            const hpvcd_picture* p = &pics[i];
+            const Geo g = geo_of(p);
+            std::vector<uint16_t> y((size_t)g.w * g.h), cb((size_t)std::max(g.cw * g.ch, 1)),
+                cr((size_t)std::max(g.cw * g.ch, 1));
+            orc_planes pl{y.data(), cb.data(), cr.data()};
+            if (p->flags & HPVCD_PIC_PRED_IN_PLANE)
+                for (int c = 0; c < (g.idc ? 3 : 1); ++c) {
+                    const size_t cnt = c == 0 ? (size_t)g.w * g.h : (size_t)g.cw * g.ch;
+                    uint16_t* dst = c == 0 ? pl.y : (c == 1 ? pl.cb : pl.cr);
+                    if (!p->pred[c]) continue;
+                    if ((c == 0 ? g.bd : g.bd_c) <= 8)
+                        for (size_t k = 0; k < cnt; ++k) dst[k] = ((const uint8_t*)p->pred[c])[k];
+                    else
+                        std::memcpy(dst, p->pred[c], cnt * 2);
+                }
+            int rc = recon_picture(p, &pl);
+            if (!rc) rc = deblock_picture_t(p, &pl, on_pool);
+            if (!rc) rc = sao_picture_t(p, &pl, on_pool);
+            if (rc) {
+                err.store(rc);
+                continue;
+            }
+            const hpvcd_tile_place& tp = out->place[i];
+            const hpvcd_canvas& cv = cvs[tp.canvas];
+            const int tw = (int)std::min<uint32_t>(tp.crop_w, (uint32_t)g.w);
+            const int th = (int)std::min<uint32_t>(tp.crop_h, (uint32_t)g.h);
+            const int copy_w = std::min(tw, std::max((int)cv.width - (int)tp.dst_x, 0));
+            const int copy_h = std::min(th, std::max((int)cv.height - (int)tp.dst_y, 0));
+            if (copy_w <= 0 || copy_h <= 0) continue;
+            const int band = 64;  // yuv.rs:393 banded: rows per band
+            on_pool((copy_h + band - 1) / band, [&](int b) {
+                tile_rgb_rows(pl, g, (int)cv.matrix, cv.full_range != 0, copy_w, b * band, std::min(copy_h, (b + 1) * band),
+                              rgb + offs[tp.canvas], (int)cv.width, (int)tp.dst_x, (int)tp.dst_y, copy_w);
+            });
+        }
+    });
+    tk = caller_set;
+    return err.load();
 }
 
 }  // namespace
@@ -1311,6 +1610,16 @@ int sao_picture(const hpvcd_picture* p, orc_planes* pl) {
 // C exports
 // ---------------------------------------------------------------------------
 extern "C" {
+
+// The reference's CPU decode of a grid of intra / residual tiles onto RGB8
+// canvases (its parallel structure: grid-row jobs, banded filters and
+// colour conversion on a work-stealing pool), with the scalar kernels or the
+// AVX2 set (simd != 0); `threads` pool threads including the caller.
+int32_t orc_decode_grid_reference(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out, uint8_t* rgb,
+                                  int32_t threads, int32_t simd) {
+    if (simd && !orc_simd::available()) return HPVCD_ERR_UNSUPPORTED;
+    return decode_grid_reference(pics, n, out, rgb, threads, simd != 0);
+}
 
 // Slices whose deblocking is disabled (flags[256], one per slice index;
 // NULL clears them all).  Test input of the oracle only.

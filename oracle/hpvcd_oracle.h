@@ -37,6 +37,11 @@ typedef struct orc_ts_params {
 } orc_ts_params;
 
 /* transform.rs */
+/* The reference's parallel CPU decode of intra / residual tiles onto RGB8
+ * canvases: grid-row jobs on a work-stealing pool, banded deblocking / SAO /
+ * colour conversion, scalar or AVX2 kernels (simd != 0). */
+int32_t orc_decode_grid_reference(const hpvcd_picture* pics, uint32_t n, const hpvcd_output* out, uint8_t* rgb,
+                                  int32_t threads, int32_t simd);
 /* Slices whose deblocking is disabled (flags[256] by slice index, NULL
  * clears): the reference's SliceDeblock.disabled, a test input. */
 void orc_set_disabled_slices(const uint8_t* flags);

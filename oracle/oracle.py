@@ -61,6 +61,8 @@ def lib() -> C.CDLL:
         L.orc_mc_picture.argtypes = [C.POINTER(abi.Picture), C.POINTER(Planes), i32, C.POINTER(Planes)]
         L.orc_set_disabled_slices.argtypes = [vp]
         L.orc_set_disabled_slices.restype = None
+        L.orc_decode_grid_reference.argtypes = [C.POINTER(abi.Picture), u32, C.POINTER(abi.Output), vp, i32, i32]
+        L.orc_decode_grid_reference.restype = i32
         _lib = L
     return _lib
 
@@ -287,3 +289,25 @@ def decode_batch(pics, out=None, want_planes=True, threads=1):
                                 _p(rgb) if rgb is not None else None, i32(threads))
     abi.check(rc, "orc_decode_batch")
     return planes, rgb
+
+
+def canvas_bytes(out) -> int:
+    """Bytes of the RGB8 canvases of an output description."""
+    if out.n_canvases:
+        cv = (abi.Canvas * out.n_canvases).from_address(out.canvases)
+        return sum(c.width * c.height * 3 for c in cv)
+    return out.canvas_w * out.canvas_h * 3
+
+
+def decode_grid_reference(pics, out, threads: int, simd: bool, dst=None):
+    """The reference's parallel CPU decode (grid-row jobs, banded filters and
+    colour conversion on a work-stealing pool) of intra / residual tiles onto
+    RGB8 canvases, with the scalar or the AVX2 kernels; returns the canvas
+    bytes (into `dst` when given)."""
+    n = len(pics)
+    arr = (abi.Picture * n)(*pics)
+    rgb = dst if dst is not None else np.zeros(canvas_bytes(out), np.uint8)
+    rc = lib().orc_decode_grid_reference(arr, n, C.byref(out), _p(rgb), threads, int(simd))
+    if rc != 0:
+        raise abi.HpvcdError(rc, "orc_decode_grid_reference")
+    return rgb
