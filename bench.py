@@ -10,13 +10,19 @@ seeded synthetic buffers with the benchmark's distributions (there is no
 public corpus for this path).
 
 Metric: decoded megapixels (output luma pixels) per second, higher is better.
-  value  -- device time of the reconstruction with inputs resident in HBM,
-            L2 flushed between steps, CUDA events on the launching stream.
+  value  -- device time of the decode with inputs resident in HBM, L2
+            flushed between steps, CUDA events on the launching stream.
   e2e    -- the same decode through the C-ABI host-buffer entry points
             (hpvcd_gpu_submit / wait / read) with the inputs in page-locked
-            host memory and the RGB8 canvas copied back every step.
-`--impl reference` times the CPU reference path (the oracle restatement of
-the reference decoder, all host threads) on the same workload.
+            host memory and the RGB8 canvas copied back every step; beside
+            it the same with ordinary (pageable) per-tile buffers.
+  batched -- the mixed-size serving workload (256 images): one fused plan
+            against one plan per image, device time, its reconstruction
+            roofline, and the serving loop's latency percentiles.
+`--impl reference` times the reference's CPU decode on the host cores: the
+C++ restatement of its parallel structure (grid-row jobs, banded
+deblocking / SAO / colour conversion on a work-stealing pool) with its AVX2
+kernel set, on the same workload and configuration.
 
 One process per GPU (torchrun for N > 1); every rank decodes its own image
 (replicas, weak scaling); the step time is the max over ranks.
@@ -60,6 +66,8 @@ def parse_args():
                          "selector: learned schedule selection on 3840x2160 frames; inter: 1080p GOP")
     ap.add_argument("--frames", type=int, default=60, help="selector: fresh frames to evaluate")
     ap.add_argument("--images", type=int, default=64, help="serving: number of images")
+    ap.add_argument("--batched-images", type=int, default=256,
+                    help="default workload: images of the mixed-size batch block (0 = leave it out)")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: Poisson arrivals per second")
     return ap.parse_args()
 
@@ -133,21 +141,52 @@ class Clocks:
                 "samples": len(rows), "reasons": reasons}
 
 
-def cpu_baseline(pics, out, threads: int, min_seconds: float = 2.0) -> dict:
-    """The oracle (C++ restatement of the reference CPU path) on the host
-    cores: repeated full decodes of the workload for ~min_seconds."""
+CPU_ARM = ("C++ restatement of the hpvcd CPU decode path (Rust toolchain absent): its AVX2 kernel set "
+           "(transforms, intra prediction, residual add, SAO, YCbCr->RGB) and its parallel structure "
+           "(grid-row jobs, banded deblocking / SAO / RGB on a work-stealing pool)")
+
+
+def headline_config(n_int8: int, n_tiles: int) -> dict:
+    """The workload's description, the same in both arms' lines."""
+    return {"workload": WORKLOAD, "tiles": 48, "tile": "512x512 (edge tiles cropped)",
+            "out": f"{OUT_W}x{OUT_H} RGB8 BT.601 full range", "bit_depth": 10, "chroma": "4:2:0",
+            "l2": "flushed between steps (256 MiB write)",
+            "levels": f"int8 pools for {n_int8} of {n_tiles} tiles (every level fits), else int16",
+            "inputs": "seeded synthetic flat buffers (CU/TU quadtrees, modes, QP 22-37, 85% zero levels, "
+                      "Laplacian(8), deblock on, random SAO)"}
+
+
+def reference_decode(pics, out, threads: int, simd: bool = True):
     from oracle import oracle as O
-    O.decode_batch(pics, out, want_planes=False, threads=threads)  # warm
+    return O.decode_grid_reference(pics, out, threads, simd)
+
+
+def cpu_baseline(pics, out, threads: int, min_seconds: float = 3.0) -> dict:
+    """The reference's CPU decode (its parallel structure and AVX2 kernel
+    set, restated) on the host cores: repeated full decodes of the workload
+    for ~min_seconds; beside it the scalar kernels on one thread."""
+    reference_decode(pics, out, threads)  # warm
     reps, t0 = 0, time.perf_counter()
     while True:
-        O.decode_batch(pics, out, want_planes=False, threads=threads)
+        reference_decode(pics, out, threads)
         reps += 1
         el = time.perf_counter() - t0
         if el >= min_seconds and reps >= 2:
             break
+    reference_decode(pics, out, 1, simd=False)
+    r1, t1 = 0, time.perf_counter()
+    while True:
+        reference_decode(pics, out, 1, simd=False)
+        r1 += 1
+        e1 = time.perf_counter() - t1
+        if e1 >= min_seconds / 2 and r1 >= 1:
+            break
     return {"value": round(MPIX * reps / el, 2), "unit": "MPix/s", "cores": threads, "kind": "port",
             "sample": f"{reps} full {OUT_W}x{OUT_H} decodes (48 tiles, recon+deblock+SAO+RGB8) "
-                      f"in {el:.2f} s, {threads} threads"}
+                      f"in {el:.2f} s, {threads} threads, AVX2 kernels",
+            "implementation": CPU_ARM,
+            "scalar_single_thread": {"value": round(MPIX * r1 / e1, 2), "unit": "MPix/s", "cores": 1,
+                                     "sample": f"{r1} full decodes in {e1:.2f} s, scalar kernels, one thread"}}
 
 
 def run_reference(args):
@@ -155,59 +194,63 @@ def run_reference(args):
     if rank != 0:
         return 0
     from hpvcd_b200 import synth
-    from oracle import oracle as O
     threads = os.cpu_count() or 1
     g = synth.config1_grid(seed=0)
     out, keep = synth.grid_output(g)
     pics = g.synth.pictures()
+    c8keep = [] if args.coeff16 else synth.narrow_coeffs(pics)  # same inputs as the GPU arm
     for _ in range(max(args.warmup, 1)):
-        O.decode_batch(pics, out, want_planes=False, threads=threads)
+        reference_decode(pics, out, threads)
     steps = max(1, min(args.steps, 20))
     times = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        O.decode_batch(pics, out, want_planes=False, threads=threads)
+        reference_decode(pics, out, threads)
         times.append(time.perf_counter() - t0)
     total = sum(times)
     value = MPIX * steps / total
     times_ms = sorted(t * 1e3 for t in times)
+    config = headline_config(len(c8keep), len(pics))
+    config["parallelism"] = f"replicas x{world}"
     line = {
         "impl": "reference", "metric": "decoded MPix/s", "value": round(value, 2), "unit": "MPix/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
         "ms_per_step": round(total / steps * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "tiles": 48, "out": f"{OUT_W}x{OUT_H} RGB8",
-                   "implementation": "C++ restatement of the hpvcd CPU reconstruction path "
-                                     "(Rust toolchain absent; scalar kernels, one tile per thread)"},
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic", "config": config,
         "latency_ms": {"p50": round(times_ms[len(times_ms) // 2], 3),
                        "p99": round(times_ms[min(len(times_ms) - 1, int(0.99 * len(times_ms)))], 3)},
         "cpu_baseline": {"value": round(value, 2), "unit": "MPix/s", "cores": threads, "kind": "port",
-                         "sample": f"{steps} full decodes of the workload, {threads} threads"},
+                         "sample": f"{steps} full decodes of the workload, {threads} threads, AVX2 kernels",
+                         "implementation": CPU_ARM},
         "e2e": {"value": round(value, 2), "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="network"):
+def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="network", pageable=False):
     """Same decode through hpvcd_gpu_submit / wait / read: inputs packed in
-    page-locked host memory (one H2D DMA per step), the RGB8 canvas DMA'd
-    back to a page-locked caller buffer every step.  `in_flight` steps are
-    queued (each with its own output buffer), so one step's copies overlap
-    another's decoding; throughput = steps / wall time from the first submit
-    to the last read, latency = submit -> read per step."""
+    page-locked host memory (one H2D DMA per step), or (pageable) the
+    ordinary per-tile host buffers as the host syntax decode leaves them
+    (the context stages them); the RGB8 canvas DMA'd back to a page-locked
+    caller buffer every step.  `in_flight` steps are queued (each with its
+    own output buffer), so one step's copies overlap another's decoding;
+    throughput = steps / wall time from the first submit to the last read,
+    latency = submit -> read per step."""
     import torch
 
-    from hpvcd_b200 import replicas, synth
+    from hpvcd_b200 import abi, replicas, synth
     from hpvcd_b200.gpu import GpuDecoder, pack_pinned, pinned_empty
 
     packed, pkeep = pack_pinned(pics)
     h2d = pkeep[2]
+    src = list(pics) if pageable else packed
     canvas_bytes = OUT_W * OUT_H * 3
     outs = []
     for _ in range(in_flight):
         dst, dkeep = pinned_empty(canvas_bytes)
         o, okeep = synth.grid_output(g)
+        o.options = abi.OUTPUT_CANVAS_ONLY  # the product is the canvas
         o.host_dst = dst.ctypes.data
         o.host_dst_bytes = canvas_bytes
         outs.append((o, dst, dkeep, okeep))
@@ -228,7 +271,7 @@ def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="netwo
                 t, d = warm.pop(0)
                 decd.wait(t)
                 decd.read(t, d)
-            warm.append((decd.submit(packed, o), dst))
+            warm.append((decd.submit(src, o), dst))
         for t, d in warm:
             decd.wait(t)
             decd.read(t, d)
@@ -244,7 +287,7 @@ def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="netwo
                 decd.wait(t)
                 decd.read(t, d)
                 lat.append(time.perf_counter() - ts)
-            pending.append((decd.submit(packed, o), dst, time.perf_counter()))
+            pending.append((decd.submit(src, o), dst, time.perf_counter()))
         for t, d, ts in pending:
             decd.wait(t)
             decd.read(t, d)
@@ -257,7 +300,8 @@ def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="netwo
             "p50_ms": round(lat[len(lat) // 2], 3),
             "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3),
             "in_flight": in_flight,
-            "api": "hpvcd_gpu_submit/wait/read, pinned packed inputs, pinned RGB8 output",
+            "api": "hpvcd_gpu_submit/wait/read, " + ("pageable per-tile inputs" if pageable else "pinned packed inputs")
+                   + ", pinned RGB8 output",
             "schedule": "network pick per submit" if mlp is not None else schedule}
 
 
@@ -281,6 +325,7 @@ def run_ours(args):
 
     g = synth.config1_grid(seed=rank)
     out, keep = synth.grid_output(g)
+    out.options = abi.OUTPUT_CANVAS_ONLY  # the product is the RGB8 canvas (decode_heic_rgb8)
     pics = g.synth.pictures()
     # host transport choice: tiles whose levels all fit in int8 ship an int8
     # pool (half the bytes over PCIe); the pixels are the same
@@ -289,7 +334,10 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    stages = [abi.STAGE_RECON, abi.STAGE_DEBLOCK, abi.STAGE_SAO, abi.STAGE_OUTPUT]
+    # stages: reconstruction (k_residual + k_recon), then deblocking + SAO +
+    # RGB8 (one fused tile kernel when launched together)
+    stage_names = ("recon", "filters")
+    stages = [abi.STAGE_RECON, abi.STAGE_DEBLOCK | abi.STAGE_SAO | abi.STAGE_OUTPUT]
     # the learned schedule: the network picks from the batch's device features
     mlp = _selector_network()
     schedule = {"selected_by": "default"}
@@ -302,7 +350,7 @@ def run_ours(args):
         pick = int(chosen.value)
         sc = selector.SCHEDULES[pick] if pick < selector.K else None
         schedule = {"selected_by": "network", "pick": pick,
-                    "sched": [sc.idct, sc.chroma_warps, sc.recon_ctas_per_sm] if sc is not None else None}
+                    "sched": [sc.idct, sc.chroma_warps, sc.recon_ctas_per_sm, sc.wave] if sc is not None else None}
     for _ in range(args.warmup):
         flush.zero_()
         plan.launch(abi.STAGE_ALL, stream)
@@ -347,7 +395,7 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
         default_ms = sum(a.elapsed_time(b) for a, b in dev_ev) / K4
         if schedule.get("sched") is not None:
-            plan.set_sched(abi.Sched(*schedule["sched"], 0))
+            plan.set_sched(abi.Sched(*schedule["sched"]))
 
     # stage breakdown (separate, untimed for the value): the stages launched
     # one after another, each as its own plan launch
@@ -369,11 +417,7 @@ def run_ours(args):
     # bytes per launch = dense levels of the coded TBs (int16, or int8 in a
     # narrowed pool) + TB records + CTU index + the reconstructed samples
     # written once.
-    coeff_bytes = sum(p.n_coeffs * (1 if p.flags & abi.PIC_COEFF8 else 2) for p in pics)
-    n_tus = sum(p.n_tus for p in pics)
-    ctus = sum(synth.geometry(p)["ctb_cols"] * synth.geometry(p)["ctb_rows"] + 1 for p in pics)
-    written = sum(p.width * p.height * 3 // 2 * synth.geometry(p)["bytes_per_sample"] for p in pics)
-    recon_bytes = coeff_bytes + n_tus * 16 + ctus * 4 + written
+    recon_bytes, written = recon_algorithmic_bytes(pics)
     peak, peak_kind = measured_peaks()
     recon_s = stage_ms[0] / 1e3
     achieved = recon_bytes / recon_s / 1e9
@@ -385,17 +429,18 @@ def run_ours(args):
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": recon_bytes,
                 "traffic": traffic.get("dram_bytes_per_launch") if traffic else None}
-    # whole-pipeline bytes (reconstruction + filters + RGB), for context
-    pipe_bytes = recon_bytes + 2 * written * 2 + written + OUT_W * OUT_H * 3
-    # per-stage algorithmic bytes: deblocking and SAO read + write the planes
-    # once, RGB reads the planes and writes 3 bytes per output pixel
-    stage_bytes = {"recon": recon_bytes, "deblock": 2 * written, "sao": 2 * written,
-                   "rgb": written + OUT_W * OUT_H * 3}
+    # per-stage algorithmic bytes: the fused filter stage reads the
+    # reconstructed planes once and writes the RGB8 canvas (3 bytes per
+    # output pixel; the canvas-only output keeps no final planes)
+    stage_bytes = {"recon": recon_bytes, "filters": written + OUT_W * OUT_H * 3}
+    # whole-pipeline bytes (reconstruction + filters), for context
+    pipe_bytes = stage_bytes["recon"] + stage_bytes["filters"]
     stage_roofline = {}
-    for i, name in enumerate(("recon", "deblock", "sao", "rgb")):
+    for i, name in enumerate(stage_names):
         gbs = stage_bytes[name] / (stage_ms[i] / 1e3) / 1e9 if stage_ms[i] > 0 else 0.0
         stage_roofline[name] = {"bytes": int(stage_bytes[name]), "ms": round(stage_ms[i], 4),
                                 "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    stage_roofline["filters"]["kernel"] = "k_filter_tile (deblocking V + H, SAO, RGB8 per 64x64 tile)"
 
     # ---- end to end through the C ABI (host buffers) ----
     e2e = None
@@ -405,26 +450,26 @@ def run_ours(args):
         other = "network" if args.e2e_schedule == "default" else "default"
         alt = run_e2e(pics, g, K2, args.warmup, local, world, dev, max(1, args.e2e_inflight), other)
         e2e["other_schedule"] = {k: alt[k] for k in ("value", "ms_per_step", "p50_ms", "p99_ms", "schedule")}
+        pg = run_e2e(pics, g, K2, args.warmup, local, world, dev, max(1, args.e2e_inflight), args.e2e_schedule,
+                     pageable=True)
+        e2e["pageable_inputs"] = {k: pg[k] for k in ("value", "ms_per_step", "p50_ms", "p99_ms", "api")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(pics, out, os.cpu_count() or 1)
+    batched = None
+    if world == 1 and args.batched_images > 0:
+        batched = batched_block(args, local)
 
     line = {
         "metric": "decoded MPix/s", "value": round(value, 2), "unit": "MPix/s", "n_gpus": world,
         "steps": K, "warmup": args.warmup, "ms_per_step": round(total_ms / K, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "tiles": 48, "tile": "512x512 (edge tiles cropped)",
-                   "out": f"{OUT_W}x{OUT_H} RGB8 BT.601 full range", "bit_depth": 10, "chroma": "4:2:0",
-                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}",
-                   "levels": f"int8 pools for {len(c8keep)} of {len(pics)} tiles (every level fits), else int16",
-                   "inputs": "seeded synthetic flat buffers (CU/TU quadtrees, modes, QP 22-37, "
-                             "85% zero levels, Laplacian(8), deblock on, random SAO)"},
+        "config": {**headline_config(len(c8keep), len(pics)), "parallelism": f"replicas x{world}"},
         "latency_ms": {"p50": round(lat[len(lat) // 2], 4),
                        "p99": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 4)},
-        "stages_ms": {"recon": round(stage_ms[0], 4), "deblock": round(stage_ms[1], 4),
-                      "sao": round(stage_ms[2], 4), "rgb": round(stage_ms[3], 4),
+        "stages_ms": {"recon": round(stage_ms[0], 4), "filters": round(stage_ms[1], 4),
                       "note": "stages launched one after another (separate pass); the timed step overlaps them"},
         "pipeline_gbs": round(pipe_bytes / (total_ms / K / 1e3) / 1e9, 1),
         "stage_roofline": stage_roofline,
@@ -433,6 +478,7 @@ def run_ours(args):
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "batched": batched,
         "gpu_launches": int(launches),
         "launches_per_step": int(launches // K),
         "clocks": clock_rec,
@@ -443,6 +489,122 @@ def run_ours(args):
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def recon_algorithmic_bytes(pics) -> tuple[int, int]:
+    """Algorithmic bytes of one reconstruction pass over `pics`: the dense
+    levels of the coded TBs (int16, or int8 in a narrowed pool), 16 bytes per
+    TB record, 4 per CTU index entry (+1 per picture), and every reconstructed
+    sample written once.  Returns (total, written sample bytes)."""
+    from hpvcd_b200 import abi, synth
+    coeff_bytes = sum(p.n_coeffs * (1 if p.flags & abi.PIC_COEFF8 else 2) for p in pics)
+    n_tus = sum(p.n_tus for p in pics)
+    ctus = written = 0
+    for p in pics:
+        g = synth.geometry(p)
+        ctus += g["ctb_cols"] * g["ctb_rows"] + 1
+        written += (g["w"] * g["h"] + 2 * g["cw"] * g["ch"]) * g["bytes_per_sample"]
+    return coeff_bytes + n_tus * 16 + ctus * 4 + written, written
+
+
+def batched_block(args, local) -> dict:
+    """The mixed-size serving workload (`args.batched_images` images, sizes
+    256..4096, 8/10-bit, 4:2:0/4:4:4, 512x512 grid tiles, int8 level pools
+    where they fit) as a block of the default line: one fused plan against
+    one plan per image (device time), the fused plan's reconstruction
+    roofline under the learned schedule, and the continuous-batching server's
+    saturation throughput and Poisson latency percentiles (page-locked host
+    buffers, zero copy)."""
+    import ctypes as C
+
+    import torch
+
+    from hpvcd_b200 import abi, serving, synth
+    from hpvcd_b200.gpu import DevicePlan
+
+    keep, imgs = serving.make_images(args.batched_images, seed=0)
+    c8keep = synth.narrow_coeffs([p for im in imgs for p in im.pics])
+    mpix = sum(im.mpix for im in imgs)
+    dev = device_batched_vs_plain(imgs, local)
+
+    # reconstruction roofline of the fused plan: the stages launched one
+    # after another (inputs of 1+ GB: nothing stays in L2 between steps)
+    stream = torch.cuda.Stream(device=local)
+    pics, out, out_keep = serving.fused_output(imgs)
+    plan = DevicePlan(pics, out, device=local)
+    mlp = _selector_network()
+    pick = None
+    if mlp is not None:
+        from hpvcd_b200 import selector
+        chosen = C.c_uint32()
+        with torch.cuda.stream(stream):
+            abi.check(abi.lib().hpvcd_plan_select(plan._h, mlp.handle, selector.schedules_array(), selector.K,
+                                                  C.c_void_p(stream.cuda_stream), C.byref(chosen)),
+                      "hpvcd_plan_select")
+        pick = int(chosen.value)
+    stages = [abi.STAGE_RECON, abi.STAGE_DEBLOCK | abi.STAGE_SAO | abi.STAGE_OUTPUT]
+    reps = 5
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            plan.launch(abi.STAGE_ALL, stream)
+        torch.cuda.synchronize()
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(reps)]
+        for k in range(reps):
+            for i, s_ in enumerate(stages):
+                ev[k][i].record(stream)
+                plan.launch(s_, stream)
+            ev[k][2].record(stream)
+        torch.cuda.synchronize()
+    st = plan.status(stream)
+    plan.close()
+    if st != abi.OK:
+        raise abi.HpvcdError(st, "device status of the fused batch")
+    recon_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / reps
+    filt_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / reps
+    recon_bytes, written = recon_algorithmic_bytes(pics)
+    peak, peak_kind = measured_peaks()
+    gbs = recon_bytes / (recon_ms / 1e3) / 1e9
+    filt_bytes = written + int(round(mpix * 1e6)) * 3
+    filt_gbs = filt_bytes / (filt_ms / 1e3) / 1e9
+    roof = {"kernel": "k_recon", "scope": "reconstruction stage (k_residual + k_recon) of the fused plan",
+            "bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(gbs / peak, 4), "peak_source": peak_kind, "algorithmic_bytes_per_launch": recon_bytes,
+            "ms": round(recon_ms, 3), "schedule_pick": pick}
+    filt = {"kernel": "k_filter_tile", "bytes": filt_bytes, "ms": round(filt_ms, 3), "gbs": round(filt_gbs, 1),
+            "frac": round(filt_gbs / peak, 4)}
+
+    # the serving loop: saturation (all submitted at once) and Poisson arrivals
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    zc = dict(zero_copy=True, warmup=16)
+
+    def brief(r):
+        return {k: (round(r[k], 3) if isinstance(r[k], float) else r[k])
+                for k in ("mpix_per_s", "p50_ms", "p99_ms", "mean_batch_pictures", "errors")}
+    plain_sat = serving.run(imgs, batching=False, arrival_rate=None, device=local, **zc)
+    batched_sat = serving.run(imgs, batching=True, arrival_rate=None, device=local, **zc)
+    learned_sat = (serving.run(imgs, batching=True, arrival_rate=None, device=local, selector=mlp, **zc)
+                   if mlp is not None else None)
+    poi = serving.run(imgs, batching=True, arrival_rate=args.rate, device=local, zero_copy=True,
+                      selector=mlp)
+    del keep, c8keep, out_keep
+    return {
+        "workload": "heic_serving_mixed", "images": len(imgs), "tiles": len(pics), "mpix": round(mpix, 2),
+        "sizes": "256..4096 step 64", "bit_depth": "70% 8 / 30% 10", "chroma": "80% 4:2:0 / 20% 4:4:4",
+        "device": dev,
+        "batched_vs_plain": dev["speedup"],
+        "learned_vs_plain": dev.get("learned_speedup_vs_plain"),
+        "recon_roofline": roof, "filters": filt,
+        "serving_saturation": {"plain": brief(plain_sat), "batched": brief(batched_sat),
+                               "batched_learned": brief(learned_sat) if learned_sat else None},
+        "serving_batched_vs_plain": round(batched_sat["mpix_per_s"] / plain_sat["mpix_per_s"], 3),
+        "serving_learned_vs_plain": (round(learned_sat["mpix_per_s"] / plain_sat["mpix_per_s"], 3)
+                                     if learned_sat else None),
+        "poisson": {"rate_per_s": args.rate, "p50_ms": poi["p50_ms"], "p99_ms": poi["p99_ms"],
+                    "mpix_per_s": poi["mpix_per_s"], "errors": poi["errors"],
+                    "learned_schedule": mlp is not None},
+        "host_buffers": "inputs packed in page-locked memory, page-locked RGB8 outputs (zero copy)",
+    }
 
 
 def device_batched_vs_plain(imgs, local, reps: int = 5):
