@@ -230,10 +230,11 @@ def run_reference(args):
 
 def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="network", pageable=False):
     """Same decode through hpvcd_gpu_submit / wait / read: inputs packed in
-    page-locked host memory (one H2D DMA per step), or (pageable) the
-    ordinary per-tile host buffers as the host syntax decode leaves them
-    (the context stages them); the RGB8 canvas DMA'd back to a page-locked
-    caller buffer every step.  `in_flight` steps are queued (each with its
+    page-locked host memory (one H2D DMA per step) and the RGB8 canvas DMA'd
+    back to a page-locked caller buffer every step; or (pageable) the
+    ordinary per-tile host buffers as the host syntax decode leaves them and
+    an ordinary numpy canvas (the context stages both through its own
+    page-locked buffers with the host copy pool).  `in_flight` steps are queued (each with its
     own output buffer), so one step's copies overlap another's decoding;
     throughput = steps / wall time from the first submit to the last read,
     latency = submit -> read per step."""
@@ -247,8 +248,11 @@ def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="netwo
     src = list(pics) if pageable else packed
     canvas_bytes = OUT_W * OUT_H * 3
     outs = []
+    import numpy as np
     for _ in range(in_flight):
-        dst, dkeep = pinned_empty(canvas_bytes)
+        # pageable: an ordinary numpy canvas (the context DMAs into its own
+        # page-locked buffer and copies out in hpvcd_gpu_read)
+        dst, dkeep = (np.empty(canvas_bytes, np.uint8), None) if pageable else pinned_empty(canvas_bytes)
         o, okeep = synth.grid_output(g)
         o.options = abi.OUTPUT_CANVAS_ONLY  # the product is the canvas
         o.host_dst = dst.ctypes.data
@@ -300,8 +304,8 @@ def run_e2e(pics, g, K2, warmup, local, world, dev, in_flight=2, schedule="netwo
             "p50_ms": round(lat[len(lat) // 2], 3),
             "p99_ms": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3),
             "in_flight": in_flight,
-            "api": "hpvcd_gpu_submit/wait/read, " + ("pageable per-tile inputs" if pageable else "pinned packed inputs")
-                   + ", pinned RGB8 output",
+            "api": "hpvcd_gpu_submit/wait/read, " + ("pageable per-tile inputs, pageable RGB8 output" if pageable
+                                                     else "pinned packed inputs, pinned RGB8 output"),
             "schedule": "network pick per submit" if mlp is not None else schedule}
 
 

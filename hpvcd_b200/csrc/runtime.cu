@@ -12,6 +12,8 @@
 #include <vector>
 
 #include "common.cuh"
+#include "hostcopy.h"
+#include "hpvcd_syntax.h"
 
 #define HPVCD_API extern "C" __attribute__((visibility("default")))
 
@@ -1140,6 +1142,9 @@ HPVCD_API uint64_t hpvcd_kernel_launch_count(void) { return g_launches.load(); }
 
 HPVCD_API const char* hpvcd_last_error_string(void) { return t_last_error; }
 
+// The calling thread's last error, for host code outside this file.
+void hpvcd_note_error(const char* msg) { std::snprintf(t_last_error, sizeof(t_last_error), "%s", msg); }
+
 HPVCD_API hpvcd_status hpvcd_copy(void* dst, const void* src, uint64_t bytes, void* stream) {
     if ((!dst || !src) && bytes) return HPVCD_ERR_INVALID_ARG;
     if (!bytes) return HPVCD_OK;
@@ -1162,7 +1167,7 @@ HPVCD_API uint64_t hpvcd_abi_sizeof(const char* name) {
              {"hpvcd_canvas", sizeof(hpvcd_canvas)}, {"hpvcd_server_cfg", sizeof(hpvcd_server_cfg)},
              {"hpvcd_request", sizeof(hpvcd_request)}, {"hpvcd_completion", sizeof(hpvcd_completion)},
              {"hpvcd_gpu_cfg", sizeof(hpvcd_gpu_cfg)}, {"hpvcd_sched", sizeof(hpvcd_sched)},
-             {"hpvcd_scaling", sizeof(hpvcd_scaling)}};
+             {"hpvcd_scaling", sizeof(hpvcd_scaling)}, {"hpvcd_slice_params", sizeof(hpvcd_slice_params)}};
     for (const auto& e : t)
         if (std::strcmp(e.n, name) == 0) return e.s;
     return 0;
@@ -1639,8 +1644,30 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
             if (e != cudaSuccess) break;
         }
     } else {
-        for (const InputPart& pt : parts) std::memcpy(slot->h_in + pt.off, pt.src, pt.bytes);
-        if (total) e = cudaMemcpyAsync(slot->d_in, slot->h_in, total, cudaMemcpyHostToDevice, slot->stream);
+        // Staged through the slot's page-locked buffer in windows of
+        // kStageWindow bytes: the copy pool fills window k + 1 while window
+        // k's DMA runs.  Parts are laid out in ascending offsets.
+        constexpr size_t kStageWindow = 8u << 20;
+        std::vector<hpvcd_host::CopyTask> tasks;
+        size_t w0 = 0, pi = 0, part_done = 0;
+        while (w0 < total && e == cudaSuccess) {
+            const size_t w1 = std::min(total, w0 + kStageWindow);
+            tasks.clear();
+            while (pi < parts.size() && parts[pi].off + part_done < w1) {
+                const InputPart& pt = parts[pi];
+                const size_t take = std::min(pt.bytes - part_done, w1 - (pt.off + part_done));
+                tasks.push_back(hpvcd_host::CopyTask{slot->h_in + pt.off + part_done,
+                                                     (const unsigned char*)pt.src + part_done, take});
+                part_done += take;
+                if (part_done == pt.bytes) {
+                    ++pi;
+                    part_done = 0;
+                }
+            }
+            hpvcd_host::parallel_copy(tasks.data(), tasks.size());
+            e = cudaMemcpyAsync(slot->d_in + w0, slot->h_in + w0, w1 - w0, cudaMemcpyHostToDevice, slot->stream);
+            w0 = w1;
+        }
     }
     if (e != cudaSuccess) return cuda_status(e);
     for (const InputPart& pt : parts) point_at(dev[pt.pic], pt.kind, slot->d_in + pt.off);
@@ -1781,10 +1808,13 @@ HPVCD_API hpvcd_status hpvcd_gpu_pack_inputs(const hpvcd_picture* pics, uint32_t
     const size_t total = input_layout(pics, n, &parts);
     if (bytes < total) return HPVCD_ERR_INVALID_ARG;
     std::vector<hpvcd_picture> res(pics, pics + n);
+    std::vector<hpvcd_host::CopyTask> tasks;
+    tasks.reserve(parts.size());
     for (const InputPart& pt : parts) {
-        std::memcpy((unsigned char*)dst + pt.off, pt.src, pt.bytes);
+        tasks.push_back(hpvcd_host::CopyTask{(unsigned char*)dst + pt.off, pt.src, pt.bytes});
         point_at(res[pt.pic], pt.kind, (unsigned char*)dst + pt.off);
     }
+    hpvcd_host::parallel_copy(tasks.data(), tasks.size());
     std::memcpy(out_pics, res.data(), sizeof(hpvcd_picture) * n);
     return HPVCD_OK;
 }
@@ -1832,7 +1862,7 @@ HPVCD_API hpvcd_status hpvcd_gpu_read(hpvcd_gpu* g, hpvcd_ticket t, void* dst, u
     hpvcd_status st = cuda_status(e);
     if (st == HPVCD_OK) st = device_status(s->plan, s->stream);
     if (st == HPVCD_OK && s->direct_out != (void*)1 && dst != s->direct_out)
-        std::memcpy(dst, s->direct_out ? (const unsigned char*)s->direct_out : s->h_out, s->out_bytes);
+        hpvcd_host::parallel_copy(dst, s->direct_out ? (const unsigned char*)s->direct_out : s->h_out, s->out_bytes);
     s->busy = false;
     s->ticket = 0;
     return st;

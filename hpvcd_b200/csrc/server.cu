@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include "hpvcd_gpu.h"
+#include "hostcopy.h"
 
 #define HPVCD_API extern "C" __attribute__((visibility("default")))
 
@@ -121,20 +122,31 @@ struct hpvcd_server {
         b.out = Arena{};
     }
 
-    void finish(Batch& b, hpvcd_status st) {
+    // The canvases of a decoded batch from its page-locked output arena into
+    // the callers' buffers (copy pool; needs no lock: the batch is owned by
+    // the worker once it left `running`).
+    static void copy_out(const Batch& b) {
+        if (b.zero_copy) return;
+        std::vector<hpvcd_host::CopyTask> tasks;
+        tasks.reserve(b.reqs.size());
+        for (const ReqMeta& r : b.reqs)
+            tasks.push_back(hpvcd_host::CopyTask{r.dst, b.out.p + r.out_off,
+                                                 (size_t)r.canvas.width * r.canvas.height * 3});
+        hpvcd_host::parallel_copy(tasks.data(), tasks.size());
+    }
+
+    // Completion records for every request of `b` (outputs already copied).
+    void complete(Batch& b, hpvcd_status st) {
         const auto now = Clock::now();
-        for (const ReqMeta& r : b.reqs) {
-            hpvcd_status rs = st;
-            if (rs == HPVCD_OK && !b.zero_copy) {
-                const uint64_t nb = (uint64_t)r.canvas.width * r.canvas.height * 3;
-                std::memcpy(r.dst, b.out.p + r.out_off, nb);
-            }
-            done.push_back(hpvcd_completion{r.user, (int32_t)rs, (uint32_t)b.pics.size(),
+        for (const ReqMeta& r : b.reqs)
+            done.push_back(hpvcd_completion{r.user, (int32_t)st, (uint32_t)b.pics.size(),
                                             ms_between(r.t_submit, now), ms_between(r.t_submit, b.t_launch)});
-        }
         recycle(b);
         cv_done.notify_all();
     }
+
+    // A batch that failed before or at launch: nothing to copy.
+    void finish(Batch& b, hpvcd_status st) { complete(b, st); }
 
     // Launch the front open batch; false when HBM admission asks to wait.
     bool launch_front() {
@@ -190,8 +202,11 @@ struct hpvcd_server {
     void run() {
         cudaSetDevice(cfg.device);
         std::unique_lock<std::mutex> lock(mu);
+        std::vector<std::pair<std::unique_ptr<Batch>, hpvcd_status>> decoded;
         while (true) {
             bool progressed = false;
+            // Decoded batches give back their ticket slot first (the output
+            // is already in the page-locked arena, or the callers' memory)...
             for (size_t i = 0; i < running.size();) {
                 Batch& b = *running[i];
                 const hpvcd_status w = hpvcd_gpu_wait(gpu, b.ticket, 0);
@@ -200,7 +215,7 @@ struct hpvcd_server {
                     continue;
                 }
                 const hpvcd_status st = w == HPVCD_OK ? hpvcd_gpu_read(gpu, b.ticket, b.out.p, b.out.cap) : w;
-                finish(b, st);
+                decoded.emplace_back(std::move(running[i]), st);
                 running.erase(running.begin() + i);
                 progressed = true;
             }
@@ -214,6 +229,16 @@ struct hpvcd_server {
                 if (window_open) break;
                 if (!launch_front()) break;
                 progressed = true;
+            }
+            // ...so the next batches are already decoding while their
+            // canvases go to the callers' buffers, without the lock
+            if (!decoded.empty()) {
+                lock.unlock();
+                for (auto& d : decoded)
+                    if (d.second == HPVCD_OK) copy_out(*d.first);
+                lock.lock();
+                for (auto& d : decoded) complete(*d.first, d.second);
+                decoded.clear();
             }
             if (stop && open.empty() && running.empty()) break;
             if (!progressed) cv_work.wait_for(lock, std::chrono::microseconds(running.empty() ? 500 : 50));
