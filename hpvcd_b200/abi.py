@@ -254,6 +254,33 @@ class SynthCfg(C.Structure):
         ("tu_mix", C.c_float * 4),
         ("scaling", C.c_uint32), ("rext", C.c_uint32), ("tskip_log2_max", C.c_uint32),
         ("ccp_p", C.c_float), ("regions", C.c_uint32), ("pcm_p", C.c_float),
+        ("bitstream", C.c_uint32), ("sign_hiding", C.c_uint32),
+    ]
+
+
+# include/hpvcd_syntax.h
+SLICE_TSKIP = 0x0001
+SLICE_TQ_BYPASS = 0x0002
+SLICE_CU_QP_DELTA = 0x0004
+SLICE_SIGN_HIDING = 0x0008
+SLICE_SAO_LUMA = 0x0010
+SLICE_SAO_CHROMA = 0x0020
+SLICE_DEBLOCK = 0x0040
+SLICE_STRONG_SMOOTHING = 0x0080
+SLICE_EBSP = 0x0100
+
+
+class SliceParams(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32), ("height", C.c_uint32),
+        ("chroma_idc", C.c_uint8), ("bit_depth_y", C.c_uint8), ("bit_depth_c", C.c_uint8),
+        ("log2_ctb", C.c_uint8), ("log2_min_cb", C.c_uint8), ("log2_min_tb", C.c_uint8),
+        ("log2_max_tb", C.c_uint8), ("max_th_depth_intra", C.c_uint8),
+        ("diff_cu_qp_delta_depth", C.c_uint8), ("log2_max_tskip", C.c_uint8),
+        ("pps_cb_qp_offset", C.c_int8), ("pps_cr_qp_offset", C.c_int8),
+        ("slice_qp", C.c_int8), ("slice_cb_qp_offset", C.c_int8), ("slice_cr_qp_offset", C.c_int8),
+        ("beta_offset_div2", C.c_int8), ("tc_offset_div2", C.c_int8), ("rsvd", C.c_uint8 * 3),
+        ("flags", C.c_uint32), ("scaling", C.c_void_p),
     ]
 
 
@@ -330,6 +357,12 @@ def lib() -> C.CDLL:
             "hpvcd_dpb_create": (i32, [i32, u32, C.POINTER(vp)]),
             "hpvcd_dpb_destroy": (i32, [vp]),
             "hpvcd_gpu_set_dpb": (i32, [vp, vp]),
+            "hpvcd_syntax_decode": (i32, [C.POINTER(SliceParams), vp, u64, C.POINTER(vp)]),
+            "hpvcd_syntax_decode_batch": (i32, [u32, C.POINTER(SliceParams), C.POINTER(vp), C.POINTER(u64), u32,
+                                                C.POINTER(vp), C.POINTER(i32)]),
+            "hpvcd_syntax_picture": (i32, [vp, C.POINTER(Picture)]),
+            "hpvcd_syntax_bins": (u64, [vp]),
+            "hpvcd_syntax_free": (None, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -356,6 +389,9 @@ def synth_lib() -> C.CDLL:
         L.hpvcd_synth_count.restype = C.c_uint32
         L.hpvcd_synth_get.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(Picture)]
         L.hpvcd_synth_get.restype = C.c_int32
+        L.hpvcd_synth_slice.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(SliceParams),
+                                        C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]
+        L.hpvcd_synth_slice.restype = C.c_int32
         _synth = L
     return _synth
 

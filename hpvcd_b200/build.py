@@ -37,7 +37,8 @@ def _stale(target: str, sources: list[str]) -> bool:
 def build_synth(force: bool = False) -> str:
     out = os.path.join(HERE, "libhpvcd_synth.so")
     srcs = [os.path.join(CSRC, "synth.cpp"), os.path.join(CSRC, "hpvcd_synth.h"),
-            os.path.join(INCLUDE, "hpvcd_gpu.h")]
+            os.path.join(CSRC, "cabac_tables.h"), os.path.join(INCLUDE, "hpvcd_gpu.h"),
+            os.path.join(INCLUDE, "hpvcd_syntax.h")]
     if force or _stale(out, srcs):
         _run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-Wall", "-Wextra",
               "-o", out, srcs[0]])
@@ -48,11 +49,17 @@ def cuda_sources() -> list[str]:
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
 
+# host-only C++ of the main library (the syntax decode); synth.cpp is the
+# separate generator library
+HOST_SOURCES = ["syntax.cpp"]
+
+
 def build_cuda(force: bool = False, verbose_ptxas: bool = False) -> str:
     out = os.path.join(HERE, "libhpvcd_b200.so")
     cus = cuda_sources()
-    deps = cus + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + [
-        os.path.join(INCLUDE, "hpvcd_gpu.h")]
+    hosts = [os.path.join(CSRC, f) for f in HOST_SOURCES]
+    deps = cus + hosts + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + [
+        os.path.join(INCLUDE, "hpvcd_gpu.h"), os.path.join(INCLUDE, "hpvcd_syntax.h")]
     if not (force or _stale(out, deps)):
         return out
     objdir = os.path.join(HERE, "_build")
@@ -67,6 +74,12 @@ def build_cuda(force: bool = False, verbose_ptxas: bool = False) -> str:
             flags.insert(1, "-Xptxas=-v")
         if force or _stale(obj, [cu] + deps):
             _run(flags)
+        objs.append(obj)
+    for src in hosts:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        if force or _stale(obj, [src] + deps):
+            _run(["g++", "-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-Wextra",
+                  "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj])
         objs.append(obj)
     # static CUDA runtime (nvcc's default): no dependency on a libcudart on
     # the library path; the driver's primary context is shared with torch.

@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include "../../include/hpvcd_gpu.h"
+#include "../../include/hpvcd_syntax.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -76,6 +77,16 @@ typedef struct hpvcd_synth_cfg {
     /* Probability that an 8x8..32x32 intra CU is I_PCM (random samples at a
      * random PCM bit depth, pcm_loop_filter_disabled drawn per CU). */
     float pcm_p;
+    /* 1: also write the picture as the slice data of one H.265 I slice with
+     * the seeded CABAC writer (hpvcd_synth_slice).  The flat buffers are then
+     * exactly what the syntax decode of that slice yields: a coding unit
+     * without coded residual takes the predicted QP (no cu_qp_delta to carry
+     * its own), SAO fields the syntax does not code are zero and, with
+     * sign_hiding, the sign of each hidden level follows the parity rule.
+     * Needs an all-intra picture, chroma 4:0:0 / 4:2:0 / 4:4:4, no PCM,
+     * regions or range-extension tools. */
+    uint32_t bitstream;
+    uint32_t sign_hiding; /* bitstream mode: sign_data_hiding_enabled_flag */
 } hpvcd_synth_cfg;
 
 typedef struct hpvcd_synth hpvcd_synth;
@@ -89,6 +100,12 @@ int32_t hpvcd_synth_add(hpvcd_synth* s, const hpvcd_synth_cfg* cfg);
 uint32_t hpvcd_synth_count(const hpvcd_synth* s);
 /* Descriptor of picture i; pointers stay valid until hpvcd_synth_free. */
 int32_t hpvcd_synth_get(const hpvcd_synth* s, uint32_t i, hpvcd_picture* out);
+/* Slice data of picture i (bitstream mode, with emulation prevention) and the
+ * slice parameters it was written with; HPVCD_ERR_INVALID_ARG when the
+ * picture was generated without it.  The bytes stay valid until
+ * hpvcd_synth_free. */
+int32_t hpvcd_synth_slice(const hpvcd_synth* s, uint32_t i, hpvcd_slice_params* params, const uint8_t** data,
+                          uint64_t* bytes);
 
 #ifdef __cplusplus
 }

@@ -5,6 +5,8 @@
 // distributions instead of a bitstream.
 #include "hpvcd_synth.h"
 
+#include "cabac_tables.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -58,6 +60,26 @@ struct Picture {
     std::vector<int8_t> slice_deblock;  // 256 x {beta, tc} div2
     std::vector<uint8_t> pred8[3];
     std::vector<uint16_t> pred16[3];
+    // bitstream mode: the slice data written for this picture, and the
+    // parameters it was written with
+    std::vector<uint8_t> slice;
+    hpvcd_slice_params slice_params{};
+};
+
+// Coding units of an intra picture as generated, for the bitstream writer:
+// transform-tree leaves in decode order with the range of TB records each
+// produced.
+struct TtLeaf {
+    int x, y, log2;
+    uint32_t tb_first, tb_end;
+};
+struct CuRec {
+    int x, y, log2;
+    bool tqb, nxn;
+    int lm[4], cm[4];
+    int qp;
+    uint32_t tb_first, tb_end;
+    std::vector<TtLeaf> leaves;
 };
 
 struct Gen {
@@ -67,6 +89,7 @@ struct Gen {
     int w, h, idc, sub_w, sub_h, gw, gh, bd, log2_ctb;
     int pic_index;
     std::vector<CellMeta> meta;
+    std::vector<CuRec> cus;  // bitstream mode: intra CUs in decode order
 
     Gen(const hpvcd_synth_cfg& cfg, Picture& pic, int index)
         : c(cfg), rng(cfg.seed), P(pic), pic_index(index) {
@@ -202,6 +225,15 @@ struct Gen {
                                b, intra, nxn, lmodes, cmodes, cu_x, cu_y, cu_size, qp, tqb);
             return;
         }
+        const uint32_t tb0 = (uint32_t)P.tus.size();
+        leaf_tbs(x0, y0, xbase, ybase, log2, blk, intra, nxn, lmodes, cmodes, cu_x, cu_y, cu_size, qp, tqb);
+        if (c.bitstream && intra && !cus.empty())
+            cus.back().leaves.push_back(TtLeaf{x0, y0, log2, tb0, (uint32_t)P.tus.size()});
+    }
+
+    void leaf_tbs(int x0, int y0, int xbase, int ybase, int log2, int blk, bool intra, bool nxn,
+                  const int* lmodes, const int* cmodes, int cu_x, int cu_y, int cu_size, int qp, bool tqb) {
+        const int size = 1 << log2;
         const int pu = nxn ? cu_size / 2 : cu_size;
         const int q = nxn ? ((x0 - cu_x) >= pu ? 1 : 0) + ((y0 - cu_y) >= pu ? 2 : 0) : 0;
         uint8_t base = (intra ? HPVCD_TU_INTRA : 0) | (tqb ? HPVCD_TU_TQB : 0);
@@ -258,7 +290,16 @@ struct Gen {
         if (!nxn || idc != 3)
             for (int i = 1; i < 4; ++i) cmodes[i] = cmodes[0];
         fill_cells(x0, y0, size, qp, tqb, true);
+        if (c.bitstream) {
+            CuRec r{x0, y0, log2, tqb, nxn, {}, {}, qp, (uint32_t)P.tus.size(), 0, {}};
+            for (int i = 0; i < 4; ++i) {
+                r.lm[i] = lmodes[i];
+                r.cm[i] = cmodes[i];
+            }
+            cus.push_back(std::move(r));
+        }
         transform_tree(x0, y0, x0, y0, log2, 0, 0, true, nxn, lmodes, cmodes, x0, y0, size, qp, tqb);
+        if (c.bitstream) cus.back().tb_end = (uint32_t)P.tus.size();
     }
 
     void inter_cu(int x0, int y0, int log2, int qp, bool tqb) {
@@ -607,6 +648,618 @@ struct Gen {
     }
 };
 
+// ---------------------------------------------------------------------------
+// Seeded CABAC writer: the generated intra picture as the slice_segment_data()
+// of one H.265 I slice.  The arithmetic coder is the standard's encoder
+// (H.265 9.3.4.3 decoding, inverted as in the informative encoding process:
+// low / range registers, outstanding bits, flush); the syntax is written in
+// the order the decoder reads it (7.3.8).  It shares only the normative tables
+// (cabac_tables.h) with the decoder in syntax.cpp, so a round trip checks one
+// against the other.
+// ---------------------------------------------------------------------------
+
+struct CabacWriter {
+    std::vector<uint8_t> out;
+    uint32_t cur = 0;
+    int nbits = 0;
+    uint32_t low = 0, range = 510;
+    int outstanding = 0;
+    bool first = true;
+    uint8_t ctx[hpvcd_cabac::kCtxCount];
+
+    void init(int qp) {
+        for (int i = 0; i < hpvcd_cabac::kCtxCount; ++i) ctx[i] = hpvcd_cabac::init_state(hpvcd_cabac::kInitI[i], qp);
+    }
+    void raw(int b) {
+        cur = (cur << 1) | (uint32_t)(b & 1);
+        if (++nbits == 8) {
+            out.push_back((uint8_t)cur);
+            cur = 0;
+            nbits = 0;
+        }
+    }
+    void put(int b) {
+        if (first)
+            first = false;
+        else
+            raw(b);
+        for (; outstanding > 0; --outstanding) raw(1 - b);
+    }
+    void renorm() {
+        while (range < 256) {
+            if (low < 256) {
+                put(0);
+            } else if (low >= 512) {
+                low -= 512;
+                put(1);
+            } else {
+                low -= 256;
+                ++outstanding;
+            }
+            range <<= 1;
+            low <<= 1;
+        }
+    }
+    void bin(int ci, int b) {
+        const int st = ctx[ci] & 63, mps = ctx[ci] >> 6;
+        const uint32_t lps = hpvcd_cabac::kRangeLps[st][(range >> 6) & 3];
+        range -= lps;
+        if (b != mps) {
+            low += range;
+            range = lps;
+            ctx[ci] = (uint8_t)(hpvcd_cabac::kNextLps[st] | ((st == 0 ? 1 - mps : mps) << 6));
+        } else {
+            ctx[ci] = (uint8_t)(hpvcd_cabac::kNextMps[st] | (mps << 6));
+        }
+        renorm();
+    }
+    void bypass(int b) {
+        low <<= 1;
+        if (b) low += range;
+        if (low >= 1024) {
+            put(1);
+            low -= 1024;
+        } else if (low < 512) {
+            put(0);
+        } else {
+            low -= 512;
+            ++outstanding;
+        }
+    }
+    void bypass_bits(uint32_t v, int n) {
+        for (int i = n - 1; i >= 0; --i) bypass((int)((v >> i) & 1));
+    }
+    void terminate(int b) {
+        range -= 2;
+        if (b) {
+            low += range;
+            range = 2;  // flush
+            renorm();
+            put((int)((low >> 9) & 1));
+            raw((int)((low >> 8) & 1));
+            raw(1);  // rbsp_stop_one_bit
+            while (nbits) raw(0);
+        } else {
+            renorm();
+        }
+    }
+};
+
+struct SliceWriter {
+    Gen& G;
+    Picture& P;
+    const hpvcd_synth_cfg& c;
+    hpvcd_slice_params sp{};
+    CabacWriter E;
+    int w, h, idc, log2ctb, ctb, cols, rows, gw, qp_off;
+    std::vector<uint8_t> depth, lmode;
+    std::vector<int8_t> qpmap;
+    size_t ci = 0;
+    int qp_last = 0, qp_pred = 0;
+    bool delta_coded = false;
+
+    explicit SliceWriter(Gen& g) : G(g), P(g.P), c(g.c) {}
+
+    size_t cell(int x, int y) const { return (size_t)(y >> 2) * gw + (x >> 2); }
+    void fill(std::vector<uint8_t>& m, int x0, int y0, int size, uint8_t v) {
+        for (int y = y0; y < std::min(y0 + size, h); y += 4)
+            for (int x = x0; x < std::min(x0 + size, w); x += 4) m[cell(x, y)] = v;
+    }
+
+    void params() {
+        w = G.w;
+        h = G.h;
+        idc = G.idc;
+        log2ctb = G.log2_ctb;
+        ctb = 1 << log2ctb;
+        cols = (w + ctb - 1) / ctb;
+        rows = (h + ctb - 1) / ctb;
+        gw = G.gw;
+        qp_off = 6 * (G.bd - 8);
+        sp.width = (uint32_t)w;
+        sp.height = (uint32_t)h;
+        sp.chroma_idc = (uint8_t)idc;
+        sp.bit_depth_y = sp.bit_depth_c = (uint8_t)G.bd;
+        sp.log2_ctb = (uint8_t)log2ctb;
+        sp.log2_min_cb = 3;
+        sp.log2_min_tb = 2;
+        sp.log2_max_tb = (uint8_t)std::min(5, log2ctb);
+        sp.max_th_depth_intra = (uint8_t)(log2ctb - 2);
+        sp.diff_cu_qp_delta_depth = (uint8_t)(log2ctb - 3);  // one quantization group per CU
+        sp.log2_max_tskip = (uint8_t)std::max<uint32_t>(2, c.tskip_log2_max);
+        sp.pps_cb_qp_offset = (int8_t)c.cb_qp_offset;
+        sp.pps_cr_qp_offset = (int8_t)c.cr_qp_offset;
+        sp.slice_qp = (int8_t)std::clamp((c.qp_min + c.qp_max + 1) / 2, -qp_off, 51);
+        sp.beta_offset_div2 = (int8_t)c.beta_offset_div2;
+        sp.tc_offset_div2 = (int8_t)c.tc_offset_div2;
+        const uint32_t pf = P.desc.flags;
+        sp.flags = HPVCD_SLICE_CU_QP_DELTA | HPVCD_SLICE_EBSP | (c.tskip_p > 0.f ? HPVCD_SLICE_TSKIP : 0) |
+                   (c.tqb_p > 0.f ? HPVCD_SLICE_TQ_BYPASS : 0) | (c.sign_hiding ? HPVCD_SLICE_SIGN_HIDING : 0) |
+                   (pf & HPVCD_PIC_DEBLOCK ? HPVCD_SLICE_DEBLOCK : 0) |
+                   (pf & HPVCD_PIC_STRONG_SMOOTHING ? HPVCD_SLICE_STRONG_SMOOTHING : 0) |
+                   (pf & HPVCD_PIC_SAO_LUMA ? HPVCD_SLICE_SAO_LUMA : 0) |
+                   (pf & HPVCD_PIC_SAO_CHROMA && idc ? HPVCD_SLICE_SAO_CHROMA : 0);
+        sp.scaling = nullptr;  // the caller points it at the picture's lists
+    }
+
+    // SAO fields the syntax does not carry are zero; components whose slice
+    // flag is off are off; no SAO array without a slice flag.
+    void normalise_sao() {
+        const bool luma = sp.flags & HPVCD_SLICE_SAO_LUMA, chroma = sp.flags & HPVCD_SLICE_SAO_CHROMA;
+        if (!luma && !chroma) {
+            P.sao.clear();
+            P.desc.flags &= ~(uint32_t)(HPVCD_PIC_SAO_LUMA | HPVCD_PIC_SAO_CHROMA);
+            return;
+        }
+        P.desc.flags &= ~(uint32_t)(HPVCD_PIC_SAO_LUMA | HPVCD_PIC_SAO_CHROMA);
+        P.desc.flags |= (luma ? HPVCD_PIC_SAO_LUMA : 0) | (chroma ? HPVCD_PIC_SAO_CHROMA : 0);
+        if (P.sao.empty()) P.sao.assign((size_t)cols * rows, hpvcd_sao_ctb{});
+        for (hpvcd_sao_ctb& s : P.sao)
+            for (int k = 0; k < 3; ++k) {
+                hpvcd_sao_comp& sc = s.comp[k];
+                const bool on = k == 0 ? luma : (chroma && idc);
+                if (!on || sc.type_idx == 0) {
+                    sc = hpvcd_sao_comp{};
+                    continue;
+                }
+                sc.rsvd = 0;
+                if (sc.type_idx == 1) sc.eo_class = 0;
+                if (sc.type_idx == 2) sc.band_pos = 0;
+            }
+        if (idc && chroma)
+            for (hpvcd_sao_ctb& s : P.sao) {  // Cr takes Cb's type and class
+                s.comp[2].type_idx = s.comp[1].type_idx;
+                s.comp[2].eo_class = s.comp[1].eo_class;
+                if (!s.comp[2].type_idx) s.comp[2] = hpvcd_sao_comp{};
+            }
+    }
+
+    void write_sao(int rx, int ry) {
+        const size_t at = (size_t)ry * cols + rx;
+        const hpvcd_sao_ctb& s = P.sao[at];
+        if (rx > 0) {
+            const bool m = memcmp(&s, &P.sao[at - 1], sizeof(s)) == 0;
+            E.bin(hpvcd_cabac::kSaoMerge, m);
+            if (m) return;
+        }
+        if (ry > 0) {
+            const bool m = memcmp(&s, &P.sao[at - cols], sizeof(s)) == 0;
+            E.bin(hpvcd_cabac::kSaoMerge, m);
+            if (m) return;
+        }
+        for (int k = 0; k < (idc ? 3 : 1); ++k) {
+            const bool on = k == 0 ? (sp.flags & HPVCD_SLICE_SAO_LUMA) : (sp.flags & HPVCD_SLICE_SAO_CHROMA);
+            if (!on) continue;
+            const hpvcd_sao_comp& sc = s.comp[k];
+            if (k < 2) {
+                E.bin(hpvcd_cabac::kSaoType, sc.type_idx != 0);
+                if (sc.type_idx) E.bypass(sc.type_idx == 2);
+            }
+            if (!sc.type_idx) continue;
+            const int cmax = (1 << (std::min(G.bd, 10) - 5)) - 1;
+            for (int i = 0; i < 4; ++i) {
+                const int a = std::abs((int)sc.offsets[i]);
+                for (int b = 0; b < a; ++b) E.bypass(1);
+                if (a < cmax) E.bypass(0);
+            }
+            if (sc.type_idx == 1) {
+                for (int i = 0; i < 4; ++i)
+                    if (sc.offsets[i]) E.bypass(sc.offsets[i] < 0);
+                E.bypass_bits(sc.band_pos, 5);
+            } else if (k < 2) {
+                E.bypass_bits(sc.eo_class, 2);
+            }
+        }
+    }
+
+    // cbf of component `comp` over the leaves of `cu` inside a square
+    bool cbf_in(const CuRec& cu, int x0, int y0, int log2, int comp) const {
+        const int size = 1 << log2;
+        for (const TtLeaf& l : cu.leaves)
+            if (l.x >= x0 && l.x < x0 + size && l.y >= y0 && l.y < y0 + size)
+                for (uint32_t t = l.tb_first; t < l.tb_end; ++t)
+                    if (P.tus[t].comp == comp && (P.tus[t].flags & HPVCD_TU_CBF)) return true;
+        return false;
+    }
+    bool leaf_cbf(const TtLeaf& l, int comp) const {
+        for (uint32_t t = l.tb_first; t < l.tb_end; ++t)
+            if (P.tus[t].comp == comp && (P.tus[t].flags & HPVCD_TU_CBF)) return true;
+        return false;
+    }
+    // cbf_luma || cbfChroma of a leaf as transform_unit sees them
+    bool leaf_codes(const CuRec& cu, const TtLeaf& l) const {
+        if (leaf_cbf(l, 0)) return true;
+        if (!idc) return false;
+        if (l.log2 > 2 || idc == 3) return leaf_cbf(l, 1) || leaf_cbf(l, 2);
+        const int px = l.x & ~7, py = l.y & ~7;  // 4:2:0 4x4: the parent's chroma flags
+        return cbf_in(cu, px, py, 3, 1) || cbf_in(cu, px, py, 3, 2);
+    }
+
+    void write_qp_delta(int d) {
+        const int a = std::abs(d);
+        for (int b = 0; b < std::min(a, 5); ++b) E.bin(hpvcd_cabac::kQpDelta + (b ? 1 : 0), 1);
+        if (a < 5) {
+            E.bin(hpvcd_cabac::kQpDelta + (a ? 1 : 0), 0);
+        } else {  // EG0 suffix
+            uint32_t v = (uint32_t)(a - 5);
+            int k = 0;
+            while (v >= (1u << k)) {
+                E.bypass(1);
+                v -= 1u << k;
+                ++k;
+            }
+            E.bypass(0);
+            E.bypass_bits(v, k);
+        }
+        if (a) E.bypass(d < 0);
+    }
+
+    void write_remaining(int v, int rice) {
+        const int u = v >> rice;
+        if (u < 4) {
+            for (int i = 0; i < u; ++i) E.bypass(1);
+            E.bypass(0);
+            E.bypass_bits((uint32_t)v & ((1u << rice) - 1), rice);
+            return;
+        }
+        for (int i = 0; i < 4; ++i) E.bypass(1);
+        uint32_t r = (uint32_t)(v - (4 << rice));
+        int k = rice + 1;
+        while (r >= (1u << k)) {
+            E.bypass(1);
+            r -= 1u << k;
+            ++k;
+        }
+        E.bypass(0);
+        E.bypass_bits(r, k);
+    }
+
+    void write_last(int v, int base_ctx, int ctx_off, int ctx_shift, int cmax, int* suffix, int* nb) {
+        int p = v;
+        *nb = 0;
+        *suffix = 0;
+        if (v >= 4)
+            for (p = 4; p <= cmax; ++p) {
+                const int n = (p >> 1) - 1, b = (1 << n) * (2 + (p & 1));
+                if (v >= b && v < b + (1 << n)) {
+                    *nb = n;
+                    *suffix = v - b;
+                    break;
+                }
+            }
+        for (int b = 0; b < p; ++b) E.bin(base_ctx + ctx_off + (b >> ctx_shift), 1);
+        if (p < cmax) E.bin(base_ctx + ctx_off + (p >> ctx_shift), 0);
+    }
+
+    void write_residual(hpvcd_tu& t, bool tqb) {
+        using namespace hpvcd_cabac;
+        const int log2 = t.log2n, n = 1 << log2, comp = t.comp;
+        int16_t* lv = P.coeffs.data() + t.coeff_off;
+        if ((sp.flags & HPVCD_SLICE_TSKIP) && !tqb && log2 <= sp.log2_max_tskip)
+            E.bin(kTskip + (comp ? 1 : 0), (t.flags & HPVCD_TU_TSKIP) != 0);
+        const int scan = scan_idx(true, log2, comp, idc, t.mode);
+        const Scans& S = scans();
+        const int sbl = log2 - 2, nsb = 1 << sbl;
+        auto at = [&](int i, int k) -> int16_t& {
+            const int x = (S.pos[sbl][scan][i][0] << 2) + S.pos[2][scan][k][0];
+            const int y = (S.pos[sbl][scan][i][1] << 2) + S.pos[2][scan][k][1];
+            return lv[y * n + x];
+        };
+        int last_sb = -1, last_pos = -1;
+        for (int i = nsb * nsb - 1; i >= 0 && last_sb < 0; --i)
+            for (int k = 15; k >= 0; --k)
+                if (at(i, k)) {
+                    last_sb = i;
+                    last_pos = k;
+                    break;
+                }
+        int lx = (S.pos[sbl][scan][last_sb][0] << 2) + S.pos[2][scan][last_pos][0];
+        int ly = (S.pos[sbl][scan][last_sb][1] << 2) + S.pos[2][scan][last_pos][1];
+        if (scan == 2) std::swap(lx, ly);
+        int ctx_off, ctx_shift;
+        if (comp == 0) {
+            ctx_off = 3 * (log2 - 2) + ((log2 - 1) >> 2);
+            ctx_shift = (log2 + 1) >> 2;
+        } else {
+            ctx_off = 15;
+            ctx_shift = log2 - 2;
+        }
+        const int cmax = (log2 << 1) - 1;
+        int sx, nbx, sy, nby;
+        write_last(lx, kLastX, ctx_off, ctx_shift, cmax, &sx, &nbx);
+        write_last(ly, kLastY, ctx_off, ctx_shift, cmax, &sy, &nby);
+        E.bypass_bits((uint32_t)sx, nbx);
+        E.bypass_bits((uint32_t)sy, nby);
+        uint8_t csbf[8][8];
+        memset(csbf, 0, sizeof(csbf));
+        int c1 = 1;
+        const bool hiding_on = (sp.flags & HPVCD_SLICE_SIGN_HIDING) && !tqb;
+        for (int i = last_sb; i >= 0; --i) {
+            const int xs = S.pos[sbl][scan][i][0], ys = S.pos[sbl][scan][i][1];
+            bool any = false;
+            for (int k = 0; k < 16; ++k) any |= at(i, k) != 0;
+            bool infer_dc = false;
+            if (i < last_sb && i > 0) {
+                int inc = 0;
+                if (xs < nsb - 1) inc += csbf[xs + 1][ys];
+                if (ys < nsb - 1) inc += csbf[xs][ys + 1];
+                csbf[xs][ys] = any;
+                E.bin(kCsbf + std::min(inc, 1) + (comp ? 2 : 0), any);
+                infer_dc = true;
+            } else {
+                csbf[xs][ys] = 1;
+            }
+            int sig[16], nsig = 0;
+            if (i == last_sb) sig[nsig++] = last_pos;
+            if (csbf[xs][ys]) {
+                int prev = 0;
+                if (xs < nsb - 1) prev |= csbf[xs + 1][ys];
+                if (ys < nsb - 1) prev |= csbf[xs][ys + 1] << 1;
+                for (int k = (i == last_sb ? last_pos - 1 : 15); k >= 0; --k) {
+                    if (k == 0 && infer_dc) {
+                        sig[nsig++] = 0;  // inferred: the only level of the sub-block
+                        break;
+                    }
+                    const int xp = S.pos[2][scan][k][0], yp = S.pos[2][scan][k][1];
+                    const int xc = (xs << 2) + xp, yc = (ys << 2) + yp;
+                    int sc;
+                    if (log2 == 2) {
+                        sc = kSigCtx4x4[(yc << 2) + xc];
+                    } else if (xc + yc == 0) {
+                        sc = 0;
+                    } else {
+                        if (prev == 0)
+                            sc = xp + yp == 0 ? 2 : (xp + yp < 3 ? 1 : 0);
+                        else if (prev == 1)
+                            sc = yp == 0 ? 2 : (yp == 1 ? 1 : 0);
+                        else if (prev == 2)
+                            sc = xp == 0 ? 2 : (xp == 1 ? 1 : 0);
+                        else
+                            sc = 2;
+                        if (comp == 0) {
+                            if (xs > 0 || ys > 0) sc += 3;
+                            sc += log2 == 3 ? (scan == 0 ? 9 : 15) : 21;
+                        } else {
+                            sc += log2 == 3 ? 9 : 12;
+                        }
+                    }
+                    const bool sg = at(i, k) != 0;
+                    E.bin(kSig + (comp ? 27 + sc : sc), sg);
+                    if (sg) {
+                        sig[nsig++] = k;
+                        infer_dc = false;
+                    }
+                }
+            }
+            if (!nsig) continue;
+            const bool hidden = hiding_on && sig[0] - sig[nsig - 1] > 3;
+            if (hidden) {  // the sign of the lowest-position level follows the parity of the sum
+                int sum = 0;
+                for (int k = 0; k < nsig; ++k) sum += std::abs((int)at(i, sig[k]));
+                int16_t& f = at(i, sig[nsig - 1]);
+                const int a = std::abs((int)f);
+                f = (int16_t)((sum & 1) ? -a : a);
+            }
+            int ctx_set = (i == 0 || comp > 0) ? 0 : 2;
+            if (c1 == 0) ++ctx_set;
+            c1 = 1;
+            int a[16], gt1[16] = {0}, first_gt1 = -1;
+            for (int k = 0; k < nsig; ++k) a[k] = std::abs((int)at(i, sig[k]));
+            for (int k = 0; k < std::min(nsig, 8); ++k) {
+                gt1[k] = a[k] > 1;
+                E.bin(kGt1 + ctx_set * 4 + std::min(c1, 3) + (comp ? 16 : 0), gt1[k]);
+                if (gt1[k]) {
+                    c1 = 0;
+                    if (first_gt1 < 0) first_gt1 = k;
+                } else if (c1 > 0 && c1 < 3) {
+                    ++c1;
+                }
+            }
+            int gt2 = 0;
+            if (first_gt1 >= 0) {
+                gt2 = a[first_gt1] > 2;
+                E.bin(kGt2 + ctx_set + (comp ? 4 : 0), gt2);
+            }
+            for (int k = 0; k < nsig; ++k)
+                if (!(hidden && k == nsig - 1)) E.bypass(at(i, sig[k]) < 0);
+            int rice = 0;
+            for (int k = 0; k < nsig; ++k) {
+                const int base = 1 + (k < 8 ? gt1[k] : 0) + (k == first_gt1 ? gt2 : 0);
+                const int thresh = k < 8 ? (k == first_gt1 ? 3 : 2) : 1;
+                if (base == thresh) {
+                    write_remaining(a[k] - base, rice);
+                    if (a[k] > 3 * (1 << rice)) rice = std::min(rice + 1, 4);
+                }
+            }
+        }
+    }
+
+    void write_tt(CuRec& cu, int x0, int y0, int log2, int tdepth, int parent_cb, int parent_cr, size_t& li) {
+        using namespace hpvcd_cabac;
+        const TtLeaf& l = cu.leaves[li];
+        const bool split = !(l.x == x0 && l.y == y0 && l.log2 == log2);
+        const int max_depth = sp.max_th_depth_intra + (cu.nxn ? 1 : 0);
+        if (log2 <= sp.log2_max_tb && log2 > 2 && tdepth < max_depth && !(cu.nxn && tdepth == 0))
+            E.bin(kSplitTf + 5 - log2, split);
+        int cb = 0, cr = 0;
+        if ((log2 > 2 && idc) || idc == 3) {
+            cb = cbf_in(cu, x0, y0, log2, 1);
+            cr = cbf_in(cu, x0, y0, log2, 2);
+            if (tdepth == 0 || parent_cb) E.bin(kCbfChroma + tdepth, cb);
+            if (tdepth == 0 || parent_cr) E.bin(kCbfChroma + tdepth, cr);
+        } else if (idc) {
+            cb = parent_cb;
+            cr = parent_cr;
+        }
+        if (split) {
+            const int half = 1 << (log2 - 1);
+            for (int b = 0; b < 4; ++b)
+                write_tt(cu, x0 + (b & 1) * half, y0 + (b >> 1) * half, log2 - 1, tdepth + 1, cb, cr, li);
+            return;
+        }
+        const bool cbf_l = leaf_cbf(l, 0);
+        E.bin(kCbfLuma + (tdepth == 0 ? 1 : 0), cbf_l);
+        if ((cbf_l || cb || cr) && !delta_coded) {
+            // QpY wraps modulo 52 + QpBdOffsetY (8.6.1): any QP is one delta
+            // inside [-(26 + QpBdOffsetY / 2), 25 + QpBdOffsetY / 2] away
+            int d = cu.qp - qp_pred;
+            while (d > 25 + qp_off / 2) d -= 52 + qp_off;
+            while (d < -(26 + qp_off / 2)) d += 52 + qp_off;
+            write_qp_delta(d);
+            delta_coded = true;
+        }
+        for (uint32_t t = l.tb_first; t < l.tb_end; ++t)
+            if (P.tus[t].flags & HPVCD_TU_CBF) write_residual(P.tus[t], cu.tqb);
+        ++li;
+    }
+
+    void write_cu(CuRec& cu, int cqt_depth) {
+        using namespace hpvcd_cabac;
+        const int size = 1 << cu.log2;
+        // QpY: a coding unit without coded residual has no cu_qp_delta and
+        // takes the prediction
+        bool codes = false;
+        for (const TtLeaf& l : cu.leaves) codes |= leaf_codes(cu, l);
+        if (!codes) {
+            cu.qp = qp_pred;
+            for (uint32_t t = cu.tb_first; t < cu.tb_end; ++t) P.tus[t].qp_y = (int8_t)cu.qp;
+            for (int y = cu.y; y < std::min(cu.y + size, h); y += 4)
+                for (int x = cu.x; x < std::min(cu.x + size, w); x += 4) P.cells[cell(x, y)].qp_y = (int8_t)cu.qp;
+        }
+        if (sp.flags & HPVCD_SLICE_TQ_BYPASS) E.bin(kTqBypass, cu.tqb);
+        if (cu.log2 == 3) E.bin(kPartMode, !cu.nxn);
+        fill(depth, cu.x, cu.y, size, (uint8_t)cqt_depth);
+        const int pb = cu.nxn ? size >> 1 : size, npu = cu.nxn ? 4 : 1;
+        int prev[4], idx[4];
+        for (int k = 0; k < npu; ++k) {
+            const int px = cu.x + (k & 1) * pb, py = cu.y + (k >> 1) * pb;
+            const int a = px > 0 ? lmode[cell(px - 1, py)] : 1;
+            const int b = (py > 0 && ((py - 1) >> log2ctb) == (py >> log2ctb)) ? lmode[cell(px, py - 1)] : 1;
+            int cand[3];
+            mpm_list(a, b, cand);
+            const int m = cu.lm[k];
+            prev[k] = 0;
+            for (int i = 0; i < 3; ++i)
+                if (cand[i] == m) {
+                    prev[k] = 1;
+                    idx[k] = i;
+                }
+            if (!prev[k]) {
+                int r = m;
+                for (int i = 0; i < 3; ++i) r -= cand[i] < m;
+                idx[k] = r;
+            }
+            fill(lmode, px, py, pb, (uint8_t)m);
+        }
+        for (int k = 0; k < npu; ++k) E.bin(kPrevIntra, prev[k]);
+        for (int k = 0; k < npu; ++k) {
+            if (prev[k]) {
+                E.bypass(idx[k] > 0);
+                if (idx[k] > 0) E.bypass(idx[k] > 1);
+            } else {
+                E.bypass_bits((uint32_t)idx[k], 5);
+            }
+        }
+        auto icpm = [&](int cm, int lm) {
+            static const int cand[4] = {0, 26, 10, 1};
+            if (cm == lm) return 4;
+            for (int k = 0; k < 4; ++k)
+                if (cand[k] == cm || (cm == 34 && cand[k] == lm)) return k;
+            return 4;
+        };
+        auto write_icpm = [&](int v) {
+            E.bin(kChromaMode, v != 4);
+            if (v != 4) E.bypass_bits((uint32_t)v, 2);
+        };
+        if (idc == 3)
+            for (int k = 0; k < npu; ++k) write_icpm(icpm(cu.cm[k], cu.lm[k]));
+        else if (idc)
+            write_icpm(icpm(cu.cm[0], cu.lm[0]));
+        size_t li = 0;
+        write_tt(cu, cu.x, cu.y, cu.log2, 0, 0, 0, li);
+        qp_last = cu.qp;
+        for (int y = cu.y; y < std::min(cu.y + size, h); y += 4)
+            for (int x = cu.x; x < std::min(cu.x + size, w); x += 4) qpmap[cell(x, y)] = (int8_t)cu.qp;
+    }
+
+    void write_cqt(int x0, int y0, int log2, int cqt_depth) {
+        const int size = 1 << log2;
+        const CuRec& cu = G.cus[ci];
+        const bool split = !(cu.x == x0 && cu.y == y0 && cu.log2 == log2);
+        if (x0 + size <= w && y0 + size <= h && log2 > 3) {
+            int inc = 0;
+            if (x0 > 0 && depth[cell(x0 - 1, y0)] > cqt_depth) ++inc;
+            if (y0 > 0 && depth[cell(x0, y0 - 1)] > cqt_depth) ++inc;
+            E.bin(hpvcd_cabac::kSplitCu + inc, split);
+        }
+        if (log2 >= log2ctb - sp.diff_cu_qp_delta_depth) {  // quantization group
+            const int mask = ctb - 1;
+            const int qa = (x0 & mask) ? qpmap[cell(x0 - 1, y0)] : qp_last;
+            const int qb = (y0 & mask) ? qpmap[cell(x0, y0 - 1)] : qp_last;
+            qp_pred = (qa + qb + 1) >> 1;
+            delta_coded = false;
+        }
+        if (split) {
+            const int half = size >> 1;
+            for (int b = 0; b < 4; ++b) {
+                const int x = x0 + (b & 1) * half, y = y0 + (b >> 1) * half;
+                if (x < w && y < h) write_cqt(x, y, log2 - 1, cqt_depth + 1);
+            }
+            return;
+        }
+        write_cu(G.cus[ci++], cqt_depth);
+    }
+
+    void run() {
+        params();
+        normalise_sao();
+        depth.assign((size_t)gw * G.gh, 0);
+        lmode.assign((size_t)gw * G.gh, 1);
+        qpmap.assign((size_t)gw * G.gh, 0);
+        E.init(sp.slice_qp);
+        qp_last = qp_pred = sp.slice_qp;
+        for (int ry = 0; ry < rows; ++ry)
+            for (int rx = 0; rx < cols; ++rx) {
+                if (!P.sao.empty()) write_sao(rx, ry);
+                write_cqt(rx << log2ctb, ry << log2ctb, log2ctb, 0);
+                E.terminate(ry == rows - 1 && rx == cols - 1);
+            }
+        // emulation prevention (7.4.2): 0x0000 followed by 0..3 gets a 0x03
+        P.slice.clear();
+        P.slice.reserve(E.out.size() + E.out.size() / 64);
+        int zeros = 0;
+        for (const uint8_t b : E.out) {
+            if (zeros >= 2 && b <= 3) {
+                P.slice.push_back(3);
+                zeros = 0;
+            }
+            P.slice.push_back(b);
+            zeros = b == 0 ? zeros + 1 : 0;
+        }
+        P.slice_params = sp;
+    }
+};
+
 }  // namespace
 
 struct hpvcd_synth {
@@ -652,10 +1305,15 @@ int32_t hpvcd_synth_add(hpvcd_synth* s, const hpvcd_synth_cfg* cfg) {
     if (cfg->chroma_idc > 3 || cfg->bit_depth < 8 || cfg->bit_depth > 12 ||
         cfg->log2_ctb < 4 || cfg->log2_ctb > 6 || cfg->qp_min > cfg->qp_max)
         return -HPVCD_ERR_INVALID_ARG;
+    if (cfg->bitstream && (cfg->kind != HPVCD_SYNTH_INTRA || cfg->chroma_idc == 2 || cfg->pcm_p > 0.f ||
+                           cfg->rext || cfg->ccp_p > 0.f || cfg->regions || cfg->tskip_log2_max > 5 ||
+                           cfg->qp_min < -6 * ((int)cfg->bit_depth - 8) || cfg->qp_max > 51))
+        return -HPVCD_ERR_UNSUPPORTED;
     auto pic = std::make_unique<Picture>();
     const int index = (int)s->pics.size();
     Gen g(*cfg, *pic, index);
     g.run();
+    if (cfg->bitstream) SliceWriter(g).run();
     hpvcd_picture& d = pic->desc;
     d.n_tus = (uint32_t)pic->tus.size();
     d.tus = pic->tus.data();
@@ -679,6 +1337,18 @@ int32_t hpvcd_synth_add(hpvcd_synth* s, const hpvcd_synth_cfg* cfg) {
 }
 
 uint32_t hpvcd_synth_count(const hpvcd_synth* s) { return s ? (uint32_t)s->pics.size() : 0; }
+
+int32_t hpvcd_synth_slice(const hpvcd_synth* s, uint32_t i, hpvcd_slice_params* params, const uint8_t** data,
+                          uint64_t* bytes) {
+    if (!s || !params || !data || !bytes || i >= s->pics.size() || s->pics[i]->slice.empty())
+        return HPVCD_ERR_INVALID_ARG;
+    const Picture& P = *s->pics[i];
+    *params = P.slice_params;
+    params->scaling = P.has_scaling ? &P.scaling : nullptr;
+    *data = P.slice.data();
+    *bytes = P.slice.size();
+    return HPVCD_OK;
+}
 
 int32_t hpvcd_synth_get(const hpvcd_synth* s, uint32_t i, hpvcd_picture* out) {
     if (!s || !out || i >= s->pics.size()) return HPVCD_ERR_INVALID_ARG;

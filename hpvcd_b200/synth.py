@@ -48,6 +48,15 @@ class SynthSet:
     def pictures(self) -> list[abi.Picture]:
         return [self.picture(i) for i in range(len(self))]
 
+    def slice(self, i: int) -> tuple[abi.SliceParams, bytes]:
+        """Slice data of picture i written in bitstream mode (cfg.bitstream)
+        and the slice parameters it was written with."""
+        sp = abi.SliceParams()
+        ptr, n = C.c_void_p(), C.c_uint64()
+        abi.check(abi.synth_lib().hpvcd_synth_slice(self._h, i, C.byref(sp), C.byref(ptr), C.byref(n)),
+                  "hpvcd_synth_slice")
+        return sp, C.string_at(ptr.value, n.value)
+
     def close(self):
         if self._h:
             abi.synth_lib().hpvcd_synth_free(self._h)
@@ -136,10 +145,13 @@ def residual_cfg(seed: int, width=512, height=512, bit_depth=8, chroma_idc=1) ->
 
 
 def intra_cfg(seed: int, width=512, height=512, bit_depth=10, chroma_idc=1, sao=True,
-              deblock=True, tskip_p=0.0, tqb_p=0.0, cbf_p=0.9, scaling=False) -> abi.SynthCfg:
+              deblock=True, tskip_p=0.0, tqb_p=0.0, cbf_p=0.9, scaling=False,
+              bitstream=False) -> abi.SynthCfg:
     """Intra still tile: random CU (64..8) and TU (32..4) quadtrees, modes
     uniform over 35, coefficients as the residual case, deblocking on, SAO
-    with random band/edge types and offsets in [-7, 7]."""
+    with random band/edge types and offsets in [-7, 7].  `bitstream`: also
+    written as an H.265 I slice by the seeded CABAC writer (SynthSet.slice),
+    the flat buffers being what the syntax decode of that slice yields."""
     c = default_cfg()
     c.seed = seed
     c.width, c.height = width, height
@@ -157,6 +169,7 @@ def intra_cfg(seed: int, width=512, height=512, bit_depth=10, chroma_idc=1, sao=
     if sao:
         flags |= abi.PIC_SAO_LUMA | abi.PIC_SAO_CHROMA
     c.pic_flags = flags
+    c.bitstream = int(bitstream)
     return c
 
 
@@ -212,9 +225,15 @@ def grid_output(g: Grid, matrix=abi.MATRIX_SMPTE170M, full_range=True, places=No
     return out, arr
 
 
-def config1_grid(seed: int = 0) -> Grid:
-    """4032x3024 10-bit 4:2:0 still as an 8x6 grid of 512x512 tiles."""
-    return make_grid(4032, 3024, seed, bit_depth=10, chroma_idc=1)
+def config1_grid(seed: int = 0, bitstream: bool = True) -> Grid:
+    """4032x3024 10-bit 4:2:0 still as an 8x6 grid of 512x512 tiles, each
+    tile also written as an I slice by the seeded CABAC writer."""
+    return make_grid(4032, 3024, seed, bit_depth=10, chroma_idc=1, bitstream=bitstream)
+
+
+def grid_slices(g: Grid) -> list:
+    """[(hpvcd_slice_params, slice bytes)] of a grid made in bitstream mode."""
+    return [g.synth.slice(i) for i in range(len(g.synth))]
 
 
 def config2_images(seed: int = 0, n_images: int = 256, max_side: int = 4096):
