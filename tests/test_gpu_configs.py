@@ -13,7 +13,9 @@ benchmark workloads state, through the C ABI, against the CPU oracle:
   8 / 10 bit, 4:2:0 / 4:4:4) including a 4096-wide 10-bit 4:4:4 image,
   through the continuous-batching server with the learned schedule;
 * a slice whose deblocking is disabled, folded by the host into zero
-  boundary strengths, against the reference's own per-slice skip.
+  boundary strengths, against the reference's own per-slice skip;
+* the 4032x3024 grid decoded from its coded I slices (host syntax decode,
+  then the GPU).
 
 Integer work: the tolerance is zero.
 """
@@ -185,3 +187,21 @@ def test_disabled_slice_folded_into_boundary_strengths():
     # and the fold matters: without it the result differs
     plain, _ = O.decode_batch([p])
     assert any(not np.array_equal(a, b) for a, b in zip(plain[0], ref[0]))
+
+
+# --- the 4032x3024 grid from its coded slices ------------------------------
+def test_grid_from_coded_slices_bitstream_to_rgb8():
+    """Bitstream -> pixels: the 48 I slices of the grid parsed by the host
+    syntax decode (hpvcd_syntax_decode_batch), the parsed buffers decoded on
+    the GPU through hpvcd_gpu_submit, against the CPU oracle on the buffers
+    the writer generated."""
+    from hpvcd_b200.syntax import decode_batch
+    g = synth.config1_grid(seed=21)
+    parsed = decode_batch(synth.grid_slices(g), threads=8)
+    out, keep = synth.grid_output(g)
+    with GpuDecoder(0) as d:
+        rgb = d.decode_rgb8([x.picture() for x in parsed], out)
+    _, ref = O.decode_batch(g.synth.pictures(), out, want_planes=False, threads=8)
+    assert np.array_equal(rgb, ref)
+    for x in parsed:
+        x.close()
