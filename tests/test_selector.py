@@ -186,9 +186,10 @@ def test_host_batch_features_match_the_restatement():
 
 def test_trained_selector_gains_on_heldout_frames_cpu():
     """The committed network, evaluated with the numpy oracle forward pass on
-    its bf16 weights over the held-out measured frames: faster in total
-    than the fixed default schedule and than the best single schedule of the
-    training frames, and within 1 % of exhaustive autotuning."""
+    its bf16 weights over the held-out measured frames and batches: faster in
+    total than the fixed default schedule (which is also the best single
+    schedule of the training rows) and within 0.2 % of exhaustive
+    autotuning."""
     if not (os.path.exists(TIMINGS) and os.path.exists(selector.WEIGHTS_PATH)):
         pytest.skip("no committed selector timings / weights")
     z = np.load(TIMINGS)
@@ -203,9 +204,12 @@ def test_trained_selector_gains_on_heldout_frames_cpu():
     s = selector.score_with_fallback(picks, ms[split:])
     fixed = selector.best_fixed(ms[:split])
     s_fixed = selector.score(np.full(len(ms) - split, fixed), ms[split:])
-    assert s["gain_vs_default"] > 0.03
+    # the default schedule is the best single one on these kernels (exhaustive
+    # autotuning is 2.0 % ahead of it on the held-out rows): the network must
+    # take most of that and never cost more than the default
+    assert s["gain_vs_default"] > 0.015
     assert s["ms_selected"] <= s_fixed["ms_selected"]
-    assert s["regret_vs_exhaustive"] < 0.01
+    assert s["regret_vs_exhaustive"] < 0.002
 
 
 # ---------------------------------------------------------------------------
@@ -363,9 +367,12 @@ def test_trained_selector_gains_over_no_network():
     s = selector.score_with_fallback(picks, ms[split:])
     fixed = selector.best_fixed(ms[:split])
     s_fixed = selector.score(np.full(len(ms) - split, fixed), ms[split:])
-    assert s["gain_vs_default"] > 0.03
+    # the default schedule is the best single one on these kernels (exhaustive
+    # autotuning is 2.0 % ahead of it on the held-out rows): the network must
+    # take most of that and never cost more than the default
+    assert s["gain_vs_default"] > 0.015
     assert s["ms_selected"] <= s_fixed["ms_selected"]
-    assert s["regret_vs_exhaustive"] < 0.01
+    assert s["regret_vs_exhaustive"] < 0.002
     # the device picks are the oracle's argmin on the same bf16 weights
     y, _, _ = mlp_ref.forward(m.params(), x[split:], selector.K)
     inside = picks != abi.MLP_NO_PICK
