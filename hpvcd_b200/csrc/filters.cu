@@ -124,10 +124,12 @@ __device__ __forceinline__ SLines lines_of(const SPlane& r, bool vertical, int e
     return SLines(r, vertical, edge, scan);
 }
 
-// Luma segment: 8 taps x 4 lines around the edge, in registers.
-// v[line][tap+4] with tap -4..3 (p3..p0, q0..q3).
+// Luma segment: 8 taps x 4 lines around the edge (tap -4..3 = p3..p0,
+// q0..q3).  The decision reads lines 0 and 3; each line is then loaded,
+// filtered and stored on its own, so only one line's taps are live at a time.
 template <class Pl, class Cl>
-__device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& pl, const Cl& cl) {
+__device__ __forceinline__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& pl,
+                                             const Cl& cl) {
     const int mid = scan + 1;
     const hpvcd_cell q = vertical ? cl.at(edge >> 2, mid >> 2) : cl.at(mid >> 2, edge >> 2);
     const int bs = vertical ? q.bs_v : q.bs_h;
@@ -141,26 +143,26 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan,
     const int beta = c_beta[clamp3i(avg + 2 * bo, 0, 51)] << sh;
     const int tc = c_tc[clamp3i(avg + 2 * (bs - 1) + 2 * to, 0, 53)] << sh;
     if (tc == 0) return;
-    int v[4][8];
     const auto L = lines_of(pl, vertical, edge, scan);
-#pragma unroll
-    for (int l = 0; l < 4; ++l)
-#pragma unroll
-        for (int t = 0; t < 8; ++t) v[l][t] = L.ld(l, t - 4);
     // deblock.rs:216-238 luma_decision (lines 0 and 3)
-    auto g = [&](int l, int tap) { return v[l][tap + 4]; };
-    const int dp0 = abs(g(0, -3) - 2 * g(0, -2) + g(0, -1));
-    const int dp3 = abs(g(3, -3) - 2 * g(3, -2) + g(3, -1));
-    const int dq0 = abs(g(0, 2) - 2 * g(0, 1) + g(0, 0));
-    const int dq3 = abs(g(3, 2) - 2 * g(3, 1) + g(3, 0));
-    if (dp0 + dp3 + dq0 + dq3 >= beta) return;
-    auto dsam = [&](int l, int dpq) {
-        return 2 * dpq < (beta >> 2) && abs(g(l, -4) - g(l, -1)) + abs(g(l, 0) - g(l, 3)) < (beta >> 3) &&
-               abs(g(l, -1) - g(l, 0)) < ((5 * tc + 1) >> 1);
+    int dp[2], dq[2], far[2], near_[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int l = 3 * k;
+        const int p3 = L.ld(l, -4), p2 = L.ld(l, -3), p1 = L.ld(l, -2), p0 = L.ld(l, -1);
+        const int q0 = L.ld(l, 0), q1 = L.ld(l, 1), q2 = L.ld(l, 2), q3 = L.ld(l, 3);
+        dp[k] = abs(p2 - 2 * p1 + p0);
+        dq[k] = abs(q2 - 2 * q1 + q0);
+        far[k] = abs(p3 - p0) + abs(q0 - q3);
+        near_[k] = abs(p0 - q0);
+    }
+    if (dp[0] + dp[1] + dq[0] + dq[1] >= beta) return;
+    auto dsam = [&](int k) {
+        return 2 * (dp[k] + dq[k]) < (beta >> 2) && far[k] < (beta >> 3) && near_[k] < ((5 * tc + 1) >> 1);
     };
-    const bool strong = dsam(0, dp0 + dq0) && dsam(3, dp3 + dq3);
+    const bool strong = dsam(0) && dsam(1);
     const int side_thr = (beta + (beta >> 1)) >> 3;
-    const bool do_p1 = dp0 + dp3 < side_thr, do_q1 = dq0 + dq3 < side_thr;
+    const bool do_p1 = dp[0] + dp[1] < side_thr, do_q1 = dq[0] + dq[1] < side_thr;
     const int maxv = (1 << P.bd) - 1;
     // exemption of the P / Q side (whole 4x4 cells)
     const bool ex_p = vertical ? exempt_of(cl, edge - 1, mid) : exempt_of(cl, mid, edge - 1);
@@ -168,9 +170,10 @@ __device__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan,
     const int tc2 = tc >> 1;
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
-        const int p0 = g(l, -1), p1 = g(l, -2), p2 = g(l, -3), p3 = g(l, -4);
-        const int q0 = g(l, 0), q1 = g(l, 1), q2 = g(l, 2), q3 = g(l, 3);
+        const int p0 = L.ld(l, -1), p1 = L.ld(l, -2), p2 = L.ld(l, -3);
+        const int q0 = L.ld(l, 0), q1 = L.ld(l, 1), q2 = L.ld(l, 2);
         if (strong) {  // deblock.rs:605-616
+            const int p3 = L.ld(l, -4), q3 = L.ld(l, 3);
             auto c = [&](int o, int x) { return clamp3i(clamp3i(x, o - 2 * tc, o + 2 * tc), 0, maxv); };
             if (!ex_p) {
                 L.st(l, -1, c(p0, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3));
@@ -704,8 +707,8 @@ __device__ __forceinline__ int sao_sample(const DevPic& P, int c, int x, int y, 
 }
 
 template <bool kGated>
-__device__ __noinline__ int sao_sample_slow(const DevPic& P, int c, int x, int y, int s0, const SPlane& src,
-                                            const SCells& cl, const SSao& sao, uint32_t rmask) {
+__device__ __noinline__ int sao_sample_slow(const DevPic& P, int c, int x, int y, int s0, const SPlane src,
+                                            const SCells cl, const SSao sao, uint32_t rmask) {
     return sao_sample<kGated>(P, c, x, y, s0, src, cl, sao, rmask);
 }
 
@@ -733,6 +736,7 @@ __device__ __forceinline__ void sao_quad(const DevPic& P, int c, const TileComp&
 #pragma unroll
     for (int i = 0; i < 4; ++i) out[i] = w[1][i + 1];
     if (slow) {
+#pragma unroll
         for (int i = 0; i < 4; ++i)
             if (x0 + i < k.pw) out[i] = sao_sample_slow<kGated>(P, c, x0 + i, y, w[1][i + 1], k.sp, cl, sao, rmask);
         return;
@@ -744,7 +748,9 @@ __device__ __forceinline__ void sao_quad(const DevPic& P, int c, const TileComp&
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const uint8_t rel = (uint8_t)((uint8_t)(out[i] >> (bd - 5)) - sc.band_pos);
-            if (rel < 4) out[i] = clamp3i(out[i] + sc.offsets[rel], 0, mx);
+            // offset of band rel (a select, not an index: the parameters stay in registers)
+            const int o = rel == 0 ? sc.offsets[0] : (rel == 1 ? sc.offsets[1] : (rel == 2 ? sc.offsets[2] : sc.offsets[3]));
+            if (rel < 4) out[i] = clamp3i(out[i] + o, 0, mx);
         }
     } else if (sc.type_idx == 2) {  // sao.rs:266-330
         const int dx = sc.eo_class == 1 ? 0 : 1;
@@ -815,16 +821,22 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                                                     : 0u;
     for (int t = blockIdx.x; t < tiles_x * tiles_y; t += gridDim.x) {
         const int X = (t % tiles_x) * kTile, Y = (t / tiles_x) * kTile;
-        TileComp tc[3];
-        size_t off = 0;
-        for (int c = 0; c < 3; ++c) {
+        // region of component c (computed where it is used: an array of the
+        // three would be indexed by a loop variable and live in local memory)
+        auto tcomp = [&](int c) {
             const int sw = c ? P.sub_w : 1, sh = c ? P.sub_h : 1;
-            TileComp& k = tc[c];
+            TileComp k;
             k.tx = X / sw; k.ty = Y / sh; k.tw = kTile / sw; k.th = kTile / sh;
             k.pw = c ? P.cw : P.w; k.ph = c ? P.ch : P.h;
+            const size_t off = c == 0 ? 0 : tile_comp_entries(64, 64) + (c - 1) * tile_comp_entries(k.tw, k.th);
             k.sp = SPlane{tsm + off, k.tx - 8, k.ty - 4, k.tw + 16};
-            off += tile_comp_entries(k.tw, k.th);
-        }
+            return k;
+        };
+        // the tile's final samples of component c (no halo)
+        auto tout_of = [&](int c) {
+            const int cw_ = kTile / P.sub_w, ch_ = kTile / P.sub_h;
+            return (uint16_t*)((unsigned char*)tsm + out_off) + (c == 0 ? 0 : 64 * 64 + (c - 1) * cw_ * ch_);
+        };
         // ---- 1. stage the tile and its halo (8 samples per copy), the cells
         // around it and the SAO parameters of its CTBs ----
         __syncthreads();  // the previous tile's readers are done
@@ -849,7 +861,7 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                 if (cx < P.ctb_cols && cy < P.ctb_rows) s_sao[i] = P.sao[(size_t)cy * P.ctb_cols + cx];
             }
         for (int c = 0; c < ncomp; ++c) {
-            const TileComp& k = tc[c];
+            const TileComp k = tcomp(c);
             const int chunks = k.rw() >> 3;
             for (int i = tid; i < k.rh() * chunks; i += kTileThreads) {
                 const int r = i / chunks, q = i - r * chunks;
@@ -862,8 +874,9 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
         const bool sao_slow = __syncthreads_or(exempt_here) || (kGated && rmask);
         if (deblock) {
             // ---- 2. vertical edges, then 3. horizontal edges ----
-            const TileComp& Lc = tc[0];
-            const TileComp& Cb = tc[1];
+            const TileComp Lc = tcomp(0);
+            const TileComp Cb = tcomp(1);
+            const SPlane Cr = tcomp(2).sp;
             const int nec_v = Cb.tw / 8 + 1, nsc_v = Cb.rh() / 4;        // chroma V: edges, segments
             const int nec_h = Cb.th / 8 + 1, nsc_h = (Cb.tw + 8) / 4;    // chroma H
             for (int pass = 0; pass < 2; ++pass) {
@@ -884,7 +897,7 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                         const int scan = (vertical ? Cb.ty - 4 : Cb.tx - 4) + 4 * (jj / ne);
                         const int emax = vertical ? P.cw : P.ch, smax = vertical ? P.ch : P.cw;
                         if (e >= 8 && e <= emax - 2 && scan >= 0 && scan + 4 <= smax)
-                            chroma_segment(P, vertical, e, scan, Cb.sp, tc[2].sp, cl);
+                            chroma_segment(P, vertical, e, scan, Cb.sp, Cr, cl);
                     }
                 }
                 __syncthreads();
@@ -892,16 +905,9 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
         }
         // ---- 4. SAO from the deblocked samples into the tile's output
         // buffer (a copy for components without SAO) ----
-        uint16_t* tout[3];
-        {
-            size_t o = 0;
-            for (int c = 0; c < 3; ++c) {
-                tout[c] = (uint16_t*)((unsigned char*)tsm + out_off) + o;
-                o += (size_t)tc[c].tw * tc[c].th;
-            }
-        }
         for (int c = 0; c < ncomp; ++c) {
-            const TileComp& k = tc[c];
+            const TileComp k = tcomp(c);
+            uint16_t* const to = tout_of(c);
             const bool on = sao_on && (P.flags & (c == 0 ? HPVCD_PIC_SAO_LUMA : HPVCD_PIC_SAO_CHROMA));
             const int qw = k.tw >> 2, nq = qw * k.th;
             for (int i = tid; i < nq; i += kTileThreads) {
@@ -916,20 +922,21 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                 } else {
                     v = *(const uint2*)(k.sp.s + (y - k.sp.y0) * k.rw() + (x0 - k.sp.x0));
                 }
-                *(uint2*)(tout[c] + yq * k.tw + xq) = v;
+                *(uint2*)(to + yq * k.tw + xq) = v;
             }
         }
         __syncthreads();
         // ---- 5. final planes (8 samples per store) ----
         if (P.write_fin) {
             for (int c = 0; c < ncomp; ++c) {
-                const TileComp& k = tc[c];
+                const TileComp k = tcomp(c);
+                const uint16_t* const to = tout_of(c);
                 const int rows = min(k.th, k.ph - k.ty), cols = min(k.tw, k.pw - k.tx);
                 const int chunks = (cols + 7) >> 3;
                 for (int i = tid; i < rows * chunks; i += kTileThreads) {
                     const int r = i / chunks, q = i - r * chunks;
                     const int x = k.tx + 8 * q, y = k.ty + r;
-                    const uint16_t* src = tout[c] + r * k.tw + 8 * q;
+                    const uint16_t* src = to + r * k.tw + 8 * q;
                     const size_t idx = (size_t)y * k.pw + x;
                     if (8 * q + 8 <= cols && (idx & 7) == 0) {
                         const uint4 v = *(const uint4*)src;
@@ -954,19 +961,22 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
             const int copy_w = min(P.crop_w, max(P.canvas_w - P.dst_x, 0));
             const int copy_h = min(P.crop_h, max(P.canvas_h - P.dst_y, 0));
             const RgbCoef kc = rgb_coef(P);
+            const TileComp B = tcomp(1);
+            const uint16_t* const tl = tout_of(0);
+            const uint16_t* const tb = tout_of(1);
+            const uint16_t* const tr = tout_of(2);
             for (int i = tid; i < (kTile / 4) * kTile; i += kTileThreads) {
                 const int x0 = X + 4 * (i % (kTile / 4)), yy = Y + i / (kTile / 4);
                 if (x0 >= copy_w || yy >= copy_h) continue;
                 const int cnt = min(4, copy_w - x0);
                 // four luma samples (one 8-byte load) and their chroma
-                const uint2 lv = *(const uint2*)(tout[0] + (yy - Y) * kTile + (x0 - X));
+                const uint2 lv = *(const uint2*)(tl + (yy - Y) * kTile + (x0 - X));
                 const int luma[4] = {(int)(lv.x & 0xffff), (int)(lv.x >> 16), (int)(lv.y & 0xffff), (int)(lv.y >> 16)};
                 int cb[4] = {0, 0, 0, 0}, cr[4] = {0, 0, 0, 0};
                 if (P.idc) {
-                    const TileComp& B = tc[1];
                     const int cy = yy / P.sub_h - B.ty;
-                    const uint16_t* ob = tout[1] + (size_t)cy * B.tw;
-                    const uint16_t* orr = tout[2] + (size_t)cy * B.tw;
+                    const uint16_t* ob = tb + (size_t)cy * B.tw;
+                    const uint16_t* orr = tr + (size_t)cy * B.tw;
                     if (P.sub_w == 2) {  // two chroma samples (one 4-byte load each)
                         const int cx = (x0 >> 1) - B.tx;
                         const uint32_t b = *(const uint32_t*)(ob + cx), r = *(const uint32_t*)(orr + cx);
@@ -983,7 +993,9 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
 #pragma unroll
                 for (int u = 0; u < 4; ++u) px[u] = rgb_px(kc, P.idc, luma[u], cb[u], cr[u]);
                 if (moves_samples(P.orientation)) {  // each pixel to its oriented place
-                    for (int u = 0; u < cnt; ++u) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        if (u >= cnt) break;
                         uint8_t* q = canvas + oriented_index(P.dst_x + x0 + u, P.dst_y + yy, P.canvas_w, P.canvas_h,
                                                              P.orientation) * 3;
                         q[0] = (uint8_t)px[u];
@@ -999,7 +1011,9 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                     o32[1] = (px[1] >> 8) | (px[2] << 16);
                     o32[2] = (px[2] >> 16) | (px[3] << 8);
                 } else {
-                    for (int u = 0; u < cnt; ++u) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        if (u >= cnt) break;
                         o[3 * u] = (uint8_t)px[u];
                         o[3 * u + 1] = (uint8_t)(px[u] >> 8);
                         o[3 * u + 2] = (uint8_t)(px[u] >> 16);

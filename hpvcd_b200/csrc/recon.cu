@@ -1096,36 +1096,29 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 
 // Stages the visible part of a coded n x n TB's residual (written by
-// k_residual) into the TB's own canvas area with asynchronous copies: 16
-// bytes per copy, 8 for 4x4 TBs.  The walk stages a few TBs ahead of the one
-// it reconstructs, so the copies' latency overlaps earlier TBs.  The area
-// of a TB not yet reconstructed is never an available reference sample of
-// an earlier TB (its stamp is later), so the staged values are never read
-// as samples; each lane predicting a sample reads its residual in place.
-__device__ __forceinline__ void stage_residual(const Comp& k, int log2n, int x0, int y0, int lane) {
+// k_residual) into the TB's own canvas area with asynchronous copies issued
+// by one lane: 16 bytes per copy, 8 for 4x4 TBs.  Every coded TB of a CTU is
+// staged before its walk starts (the lanes of the walking warp take the
+// list entries in turn).  The area of a TB not yet reconstructed is never an
+// available reference sample of an earlier TB (its stamp is later), so the
+// staged values are never read as samples; each lane predicting a sample
+// reads its residual in place.
+__device__ __forceinline__ void stage_residual(const Comp& k, int log2n, int x0, int y0) {
     const int n = 1 << log2n;
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
+    const int16_t* src = k.res + (size_t)y0 * k.rs + x0;
+    uint16_t* dst = k.can + cin(k, x0, y0);
+    const int cr = can_row(k.S);
     if (n == 4) {
-        if (lane < vh) cp_async8(k.can + cin(k, x0, y0 + lane), k.res + (size_t)(y0 + lane) * k.rs + x0);
+        for (int r = 0; r < vh; ++r) cp_async8(dst + r * cr, src + (size_t)r * k.rs);
         return;
     }
-    const int lc = log2n - 3;  // 8-sample chunks per row: log2
-    const int chunks = ((vw + 7) >> 3);
-    for (int i = lane; i < (vh << lc); i += 32) {
-        const int r = i >> lc, q = i & ((1 << lc) - 1);
-        if (q < chunks)
-            cp_async16(k.can + cin(k, x0 + 8 * q, y0 + r), k.res + (size_t)(y0 + r) * k.rs + x0 + 8 * q);
-    }
+    const int chunks = (vw + 7) >> 3;
+    for (int r = 0; r < vh; ++r)
+        for (int q = 0; q < chunks; ++q) cp_async16(dst + r * cr + 8 * q, src + (size_t)r * k.rs + 8 * q);
 }
 
-// TBs staged ahead of the one being reconstructed (one cp.async group each).
-constexpr int kStageAhead = 3;
-__device__ __forceinline__ void wait_staged() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(kStageAhead) : "memory");
-    __syncwarp();
-}
-
-// Intra TB of size 8..32, first part, by one warp through shared memory:
+// Intra TB of size 16 or 32, first part, by one warp through shared memory:
 // gather, substitution (intra.rs:84-148), filtering (:151-219) and the
 // per-mode set-up of the prediction (the angular projection into ws.refs,
 // the DC value into ws.dc).
@@ -1235,84 +1228,90 @@ __device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode
     __syncwarp();
 }
 
-// Intra TB of size 8..32, second part: prediction (intra.rs:257-372) and
-// residual add + clip (reconstruct.rs:214-251) of samples tl, tl + ts, ...
-// (one warp: tl = lane, ts = 32).  A coded TB's residual is in its canvas
-// area (stage_residual).
-__device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
-                                                 const WalkScratch& ws, int tl, int ts) {
+// Intra TB of size 16 or 32, second part: prediction (intra.rs:257-372) and
+// residual add + clip (reconstruct.rs:214-251) by one warp, lane l taking
+// samples l, l + 32, ...  in chunks of eight: a chunk's predictions (from the
+// walk scratch) and residuals (staged in the TB's canvas area) are all
+// loaded before any of its samples is stored, so the loads overlap.
+// kKind: 0 planar, 1 DC, 2 angular.
+template <int kKind>
+__device__ __forceinline__ void predict_chunks(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
+                                               const WalkScratch& ws, const int16_t* R, int lane) {
     const int n = 1 << log2n;
     const int n2 = 2 * n;
-    const int16_t* R = ref_filtered(k, n, mode) ? ws.f : ws.s;
     const int max_v = k.max_v;
     const bool edge_filters = k.luma && n < 32;  // is_luma gate of predict_into
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
-    auto res_at = [&](int xx, int yy) { return (int)(int16_t)k.can[cin(k, x0 + xx, y0 + yy)]; };
-    if (mode >= 2) {
-        const int angle = c_intra_angle[mode - 2];
-        const bool vertical = mode >= 18;
-        const int a0 = vertical ? R[n2 + 1] : R[n2 - 1];  // above[1] / left[1]
-        const int c0 = R[n2];
-#pragma unroll 4
-        for (int i = tl; i < n * n; i += ts) {
+    // mode set-up (warp-uniform)
+    const int angle = kKind == 2 ? c_intra_angle[mode - 2] : 0;
+    const bool vertical = mode >= 18;
+    const int a0 = kKind == 2 ? (vertical ? R[n2 + 1] : R[n2 - 1]) : 0;  // above[1] / left[1]
+    const int c0 = kKind == 2 ? R[n2] : 0;
+    const int dc = kKind == 1 ? ws.dc : 0;
+    const int tr = kKind == 0 ? R[n2 + n + 1] : 0, bl = kKind == 0 ? R[n2 - n - 1] : 0;
+    const int per = (n * n) >> 5;  // samples per lane: 8 or 32
+    for (int g = 0; g < per; g += 8) {
+        int v[8], rv[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = lane + 32 * (g + u);
             const int yy = i >> log2n, xx = i & (n - 1);
-            const int a = vertical ? yy : xx;
-            const int b = vertical ? xx : yy;
-            const int pos = (a + 1) * angle;
-            const int iidx = pos >> 5, frac = pos & 31;
-            const int r0 = ws.refs[b + iidx + 1 + n];
-            const int r1 = ws.refs[min(b + iidx + 2, 2 * n) + n];
-            int v = frac ? ((32 - frac) * r0 + frac * r1 + 16) >> 5 : r0;
-            v = clamp3i(v, 0, max_v);
-            if (edge_filters) {
-                if (mode == 26 && xx == 0) v = clamp3i(a0 + ((R[n2 - (yy + 1)] - c0) >> 1), 0, max_v);
-                if (mode == 10 && yy == 0) v = clamp3i(a0 + ((R[n2 + xx + 1] - c0) >> 1), 0, max_v);
+            int p;
+            if (kKind == 2) {
+                const int a = vertical ? yy : xx;
+                const int b = vertical ? xx : yy;
+                const int pos = (a + 1) * angle;
+                const int iidx = pos >> 5, frac = pos & 31;
+                const int r0 = ws.refs[b + iidx + 1 + n];
+                const int r1 = ws.refs[min(b + iidx + 2, 2 * n) + n];
+                p = clamp3i(frac ? ((32 - frac) * r0 + frac * r1 + 16) >> 5 : r0, 0, max_v);
+                if (edge_filters) {
+                    if (mode == 26 && xx == 0) p = clamp3i(a0 + ((R[n2 - (yy + 1)] - c0) >> 1), 0, max_v);
+                    if (mode == 10 && yy == 0) p = clamp3i(a0 + ((R[n2 + xx + 1] - c0) >> 1), 0, max_v);
+                }
+            } else if (kKind == 1) {
+                p = dc;
+                if (edge_filters) {
+                    if (xx == 0 && yy == 0)
+                        p = (R[n2 - 1] + 2 * dc + R[n2 + 1] + 2) >> 2;
+                    else if (yy == 0)
+                        p = (R[n2 + xx + 1] + 3 * dc + 2) >> 2;
+                    else if (xx == 0)
+                        p = (R[n2 - yy - 1] + 3 * dc + 2) >> 2;
+                }
+            } else {
+                const int hh = (n - 1 - xx) * R[n2 - yy - 1] + (xx + 1) * tr;
+                const int vv = (n - 1 - yy) * R[n2 + xx + 1] + (yy + 1) * bl;
+                p = (hh + vv + n) >> (log2n + 1);
             }
-            if (xx < vw && yy < vh) {
-                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
-                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
-            }
+            v[u] = p;
+            rv[u] = coded && xx < vw && yy < vh ? (int)(int16_t)k.can[cin(k, x0 + xx, y0 + yy)] : 0;
         }
-    } else if (mode == 1) {  // DC
-        const int dc = ws.dc;
-#pragma unroll 4
-        for (int i = tl; i < n * n; i += ts) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = lane + 32 * (g + u);
             const int yy = i >> log2n, xx = i & (n - 1);
-            int v = dc;
-            if (edge_filters) {
-                if (xx == 0 && yy == 0)
-                    v = (R[n2 - 1] + 2 * dc + R[n2 + 1] + 2) >> 2;
-                else if (yy == 0)
-                    v = (R[n2 + xx + 1] + 3 * dc + 2) >> 2;
-                else if (xx == 0)
-                    v = (R[n2 - yy - 1] + 3 * dc + 2) >> 2;
-            }
-            if (xx < vw && yy < vh) {
-                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
-                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
-            }
-        }
-    } else {  // planar
-        const int tr = R[n2 + n + 1], bl = R[n2 - n - 1];
-#pragma unroll 4
-        for (int i = tl; i < n * n; i += ts) {
-            const int yy = i >> log2n, xx = i & (n - 1);
-            const int hh = (n - 1 - xx) * R[n2 - yy - 1] + (xx + 1) * tr;
-            const int vv = (n - 1 - yy) * R[n2 + xx + 1] + (yy + 1) * bl;
-            int v = (hh + vv + n) >> (log2n + 1);
-            if (xx < vw && yy < vh) {
-                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
-                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
-            }
+            if (xx < vw && yy < vh) k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)(coded ? clamp3i(v[u] + rv[u], 0, max_v) : v[u]);
         }
     }
 }
 
-// Intra TB of size 8..32 by one warp.
+__device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
+                                                 const WalkScratch& ws, int lane) {
+    const int16_t* R = ref_filtered(k, 1 << log2n, mode) ? ws.f : ws.s;
+    if (mode >= 2)
+        predict_chunks<2>(k, log2n, mode, x0, y0, coded, ws, R, lane);
+    else if (mode == 1)
+        predict_chunks<1>(k, log2n, mode, x0, y0, coded, ws, R, lane);
+    else
+        predict_chunks<0>(k, log2n, mode, x0, y0, coded, ws, R, lane);
+}
+
+// Intra TB of size 16 or 32 by one warp.
 __device__ __forceinline__ void intra_tb_big(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
                                              const uint32_t* stamp, uint32_t jrec, WalkScratch& ws, int lane) {
     intra_tb_prep(k, log2n, mode, x0, y0, stamp, jrec, ws, lane);
-    intra_tb_predict(k, log2n, mode, x0, y0, coded, ws, lane, 32);
+    intra_tb_predict(k, log2n, mode, x0, y0, coded, ws, lane);
     __syncwarp();
 }
 
@@ -1724,17 +1723,8 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             s_lvl[tid] = v;
         }
         __syncthreads();
-        if (tid < ncomp) {
-            uint32_t h = 0;
-            for (int nb = 0; nb < 4; ++nb) h |= segs_at(nb, s_lvl[tid * 4 + nb]);
-            s_have[tid] = h;
-        }
-        __syncthreads();
-        for (int c = 0; c < ncomp; ++c) fetch_edges<(kThreads < 96 ? 4 : 3)>(geo(c), s_have[c], P.bps, tid, kThreads);
-        __syncthreads();
-        // ---- decode-order walk: each warp reconstructs its components ----
-        WalkScratch& ws = *(WalkScratch*)(smem + lay.off_ws + (size_t)warp * kWsBytes);
-        for (int c = c_lo; c <= c_hi && c < ncomp; ++c) {
+        // Everything one walking warp needs about component c of this CTU.
+        auto comp_of = [&](int c) -> Comp {
             Comp k;
             k.S = c ? Scw : ctb;
             k.Sh = c ? Sch : ctb;
@@ -1758,31 +1748,66 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             k.can = can_of(c);
             k.rs = P.res_stride[c];
             k.res = P.res[c] + (size_t)k.oy * k.rs + k.ox;
+            return k;
+        };
+        // ---- residuals into the canvas, before the walk: the copies overlap
+        // the neighbour edge loads below.  In an intra picture every sample
+        // of the CTU comes from the walk, so the whole visible residual block
+        // of each component is copied by all threads (the areas of uncoded
+        // TBs are never read); in an inter picture the canvas holds inter
+        // samples, so only the areas of coded intra TBs are staged (one lane
+        // of the walking warp per list entry) ----
+        if (!(P.flags & HPVCD_PIC_INTER)) {
+            for (int c = 0; c < ncomp; ++c) {
+                const int S = c ? Scw : ctb, Sh = c ? Sch : ctb, ox = c ? ocx : oxl, oy = c ? ocy : oyl;
+                const int rows = min(Sh, (c ? P.ch : P.h) - oy), cols = min(S, (c ? P.cw : P.w) - ox);
+                const int chunks = (cols + 7) >> 3;
+                const int rs = P.res_stride[c];
+                const int16_t* res = P.res[c] + (size_t)oy * rs + ox;
+                uint16_t* can = can_of(c);
+                for (int i = tid; i < rows * chunks; i += kThreads) {
+                    const int r = i / chunks, q = i - r * chunks;
+                    cp_async16(can + can_in(S, 8 * q, r), res + (size_t)r * rs + 8 * q);
+                }
+            }
+        } else {
+            for (int c = c_lo; c <= c_hi && c < ncomp; ++c) {
+                const Comp k = comp_of(c);
+                const uint32_t cnt = counts[c];
+                const uint16_t* list = lists + lay.list_off(c);
+                for (uint32_t e = lane; e < cnt; e += 32) {
+                    hpvcd_tu t;
+                    const uint4 w4 = recs[list[e] & kListRec];
+                    memcpy(&t, &w4, sizeof(t));
+                    const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
+                    if (coded && !(kFeat && (t.flags & HPVCD_TU_PCM)))
+                        stage_residual(k, t.log2n, (int)t.x - k.ox, (int)t.y - k.oy);
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        if (tid < ncomp) {
+            uint32_t h = 0;
+            for (int nb = 0; nb < 4; ++nb) h |= segs_at(nb, s_lvl[tid * 4 + nb]);
+            s_have[tid] = h;
+        }
+        __syncthreads();
+        for (int c = 0; c < ncomp; ++c) fetch_edges<(kThreads < 96 ? 4 : 3)>(geo(c), s_have[c], P.bps, tid, kThreads);
+        cp_async_wait_all();  // this thread's residual copies; the barrier publishes them
+        __syncthreads();
+        // ---- decode-order walk: each warp reconstructs its components ----
+        WalkScratch& ws = *(WalkScratch*)(smem + lay.off_ws + (size_t)warp * kWsBytes);
+        for (int c = c_lo; c <= c_hi && c < ncomp; ++c) {
+            const Comp k = comp_of(c);
             const uint32_t cnt = counts[c];
             const uint16_t* list = lists + lay.list_off(c);
             // edge segments in the canvas, quadrants released
             uint32_t have = s_have[c];
             int prog = 0;
-            // residuals are staged kStageAhead TBs ahead (one copy group per
-            // list entry, empty when it has none to stage)
-            auto stage = [&](uint32_t ei) {
-                if (ei < cnt) {
-                    hpvcd_tu t;
-                    const uint4 w4 = recs[list[ei] & kListRec];
-                    memcpy(&t, &w4, sizeof(t));
-                    const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
-                    if (coded && !(kFeat && (t.flags & HPVCD_TU_PCM)))
-                        stage_residual(k, t.log2n, (int)t.x - k.ox, (int)t.y - k.oy, lane);
-                }
-                asm volatile("cp.async.commit_group;" ::: "memory");
-            };
-#pragma unroll
-            for (int d = 0; d < kStageAhead; ++d) stage((uint32_t)d);
             // the next record is fetched while the current TB is reconstructed
             uint32_t jn = cnt ? list[0] : 0u;
             uint4 wn = cnt ? recs[jn & kListRec] : make_uint4(0u, 0u, 0u, 0u);
             for (uint32_t e = 0; e < cnt; ++e) {
-                stage(e + kStageAhead);
                 const uint32_t j = jn & kListRec;
                 const bool event = (jn & kListEvent) != 0u;
                 hpvcd_tu t;
@@ -1801,7 +1826,6 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                 // a chroma TB with cross-component prediction has a residual
                 // (written by k_ccp) even without coded coefficients
                 const bool coded = (t.flags & HPVCD_TU_CBF) != 0 || (k.ccp && t.res_scale);
-                wait_staged();  // this TB's residual is in its canvas area
                 if (kFeat && (t.flags & HPVCD_TU_PCM)) {
                     pcm_tb(k, t.log2n, x, y, lane);
                 } else if (t.log2n == 2) {
@@ -1812,7 +1836,6 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
                     intra_tb_big(k, t.log2n, t.mode, x, y, coded, stamp, j, ws, lane);
                 }
             }
-            asm volatile("cp.async.wait_all;" ::: "memory");  // the trailing (empty) groups
             publish_level(geo(c), P.bps, prog, 4, level + c, lane);
         }
         __syncthreads();
