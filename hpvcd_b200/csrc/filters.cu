@@ -129,7 +129,7 @@ __device__ __forceinline__ SLines lines_of(const SPlane& r, bool vertical, int e
 // filtered and stored on its own, so only one line's taps are live at a time.
 template <class Pl, class Cl>
 __device__ __forceinline__ void luma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& pl,
-                                             const Cl& cl) {
+                                             const Cl& cl, bool any_exempt = true) {
     const int mid = scan + 1;
     const hpvcd_cell q = vertical ? cl.at(edge >> 2, mid >> 2) : cl.at(mid >> 2, edge >> 2);
     const int bs = vertical ? q.bs_v : q.bs_h;
@@ -165,7 +165,7 @@ __device__ __forceinline__ void luma_segment(const DevPic& P, bool vertical, int
     const bool do_p1 = dp[0] + dp[1] < side_thr, do_q1 = dq[0] + dq[1] < side_thr;
     const int maxv = (1 << P.bd) - 1;
     // exemption of the P / Q side (whole 4x4 cells)
-    const bool ex_p = vertical ? exempt_of(cl, edge - 1, mid) : exempt_of(cl, mid, edge - 1);
+    const bool ex_p = any_exempt && (vertical ? exempt_of(cl, edge - 1, mid) : exempt_of(cl, mid, edge - 1));
     const bool ex_q = (q.flags & HPVCD_CELL_EXEMPT) != 0;
     const int tc2 = tc >> 1;
 #pragma unroll
@@ -211,7 +211,7 @@ __device__ __forceinline__ void luma_segment(const DevPic& P, bool vertical, int
 // Chroma segment (decode.rs:2036-2137): 4 chroma lines, both Cb and Cr.
 template <class Pl, class Cl>
 __device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int scan, const Pl& cb, const Pl& cr,
-                               const Cl& cl) {
+                               const Cl& cl, bool any_exempt = true) {
     const int mid = scan + 1;
     const int lex = vertical ? edge * P.sub_w : mid * P.sub_w;
     const int ley = vertical ? mid * P.sub_h : edge * P.sub_h;
@@ -250,8 +250,8 @@ __device__ void chroma_segment(const DevPic& P, bool vertical, int edge, int sca
             if (delta != 0) {  // exemption by the luma positions of p0 / q0
                 const int xp0 = vertical ? edge - 1 : s, yp0 = vertical ? s : edge - 1;
                 const int xq0 = vertical ? edge : s, yq0 = vertical ? s : edge;
-                if (!exempt_of(cl, xp0 * P.sub_w, yp0 * P.sub_h)) L.st(l, -1, clamp3i(p0 + delta, 0, maxv));
-                if (!exempt_of(cl, xq0 * P.sub_w, yq0 * P.sub_h)) L.st(l, 0, clamp3i(q0 - delta, 0, maxv));
+                if (!(any_exempt && exempt_of(cl, xp0 * P.sub_w, yp0 * P.sub_h))) L.st(l, -1, clamp3i(p0 + delta, 0, maxv));
+                if (!(any_exempt && exempt_of(cl, xq0 * P.sub_w, yq0 * P.sub_h))) L.st(l, 0, clamp3i(q0 - delta, 0, maxv));
             }
         }
     }
@@ -775,6 +775,71 @@ __device__ __forceinline__ void sao_quad(const DevPic& P, int c, const TileComp&
     }
 }
 
+// SAO of one tile component whose samples all lie in one CTB (CTB 64),
+// without exempt cells or region limits: the CTB's parameters, read once,
+// hold for every quad.  kSel: 0..3 edge offset of that class, 4 band
+// offset, 5 off (a copy).  Same arithmetic as sao_quad (sao.rs:179-330).
+template <int kSel>
+__device__ __forceinline__ void sao_fixed(const TileComp& k, uint16_t* to, const hpvcd_sao_comp sc, int bd, int tid) {
+    const int qsh = k.tw == 64 ? 4 : 3;  // quads per row: 16 or 8
+    const int nq = k.th << qsh, rw = k.rw();
+    const int mx = (1 << bd) - 1;
+    const int o0 = sc.offsets[0], o1 = sc.offsets[1], o2 = sc.offsets[2], o3 = sc.offsets[3];
+    for (int i = tid; i < nq; i += kTileThreads) {
+        const int xq = 4 * (i & ((1 << qsh) - 1)), yq = i >> qsh;
+        const int x0 = k.tx + xq, y = k.ty + yq;
+        if (x0 >= k.pw || y >= k.ph) continue;
+        const uint16_t* row = k.sp.s + (yq + 4) * rw + (xq + 8);  // sample (x0, y) of the staged region
+        const uint2 c2 = *(const uint2*)row;
+        int out[4] = {(int)(c2.x & 0xffff), (int)(c2.x >> 16), (int)(c2.y & 0xffff), (int)(c2.y >> 16)};
+        if (kSel == 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint8_t rel = (uint8_t)((uint8_t)(out[u] >> (bd - 5)) - sc.band_pos);
+                const int o = rel == 0 ? o0 : (rel == 1 ? o1 : (rel == 2 ? o2 : o3));
+                if (rel < 4) out[u] = clamp3i(out[u] + o, 0, mx);
+            }
+        } else if (kSel < 4) {
+            constexpr int dx = kSel == 1 ? 0 : 1;
+            constexpr int dy = kSel == 0 ? 0 : (kSel == 3 ? -1 : 1);
+            // n1 = (x + dx, y + dy), n2 = (x - dx, y - dy)
+            int n1[4], n2[4];
+            auto six = [&](const uint16_t* q, int w[6]) {  // samples x0 - 1 .. x0 + 4 of a staged row
+                const uint2 v = *(const uint2*)q;
+                w[0] = q[-1];
+                w[1] = v.x & 0xffff; w[2] = v.x >> 16; w[3] = v.y & 0xffff; w[4] = v.y >> 16;
+                w[5] = q[4];
+            };
+            if (kSel == 1) {
+                const uint2 a = *(const uint2*)(row + rw), b = *(const uint2*)(row - rw);
+                n1[0] = a.x & 0xffff; n1[1] = a.x >> 16; n1[2] = a.y & 0xffff; n1[3] = a.y >> 16;
+                n2[0] = b.x & 0xffff; n2[1] = b.x >> 16; n2[2] = b.y & 0xffff; n2[3] = b.y >> 16;
+            } else {
+                int wa[6], wb[6];
+                six(row + dy * rw, wa);
+                if (dy != 0) six(row - dy * rw, wb);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    n1[u] = wa[u + 2];
+                    n2[u] = dy != 0 ? wb[u] : wa[u];
+                }
+            }
+            const bool rows_ok = y - dy >= 0 && y + dy >= 0 && y - dy < k.ph && y + dy < k.ph;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int x = x0 + u;
+                if (!rows_ok || x - dx < 0 || x + dx >= k.pw) continue;  // a neighbour outside the picture
+                const int s0 = out[u];
+                const int e = ((s0 > n1[u]) - (s0 < n1[u])) + ((s0 > n2[u]) - (s0 < n2[u])) + 2;
+                const int o = e == 0 ? o0 : (e == 1 ? o1 : (e == 3 ? o2 : (e == 4 ? o3 : 0)));
+                if (o) out[u] = clamp3i(s0 + o, 0, mx);
+            }
+        }
+        *(uint2*)(to + yq * k.tw + xq) =
+            make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
+    }
+}
+
 // Eight horizontally adjacent samples of a plane row at (x, y), as uint16,
 // zero outside the plane.  Vector load when the whole group is inside and
 // 16-byte aligned.
@@ -871,7 +936,9 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
         }
         // the SAO of the tile tests exemption and slice / tile boundaries
         // per sample only when the tile has them
-        const bool sao_slow = __syncthreads_or(exempt_here) || (kGated && rmask);
+        // exempt cells (tested per segment and per sample only when present)
+        const bool any_exempt = __syncthreads_or(exempt_here) != 0;
+        const bool sao_slow = any_exempt || (kGated && rmask);
         if (deblock) {
             // ---- 2. vertical edges, then 3. horizontal edges ----
             const TileComp Lc = tcomp(0);
@@ -889,7 +956,7 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                         const int scan = (vertical ? Y - 4 : X - 4) + 4 * (j / 9);
                         const int emax = vertical ? P.w : P.h, smax = vertical ? P.h : P.w;
                         if (e >= 8 && e <= emax - 4 && scan >= 0 && scan + 4 <= smax)
-                            luma_segment(P, vertical, e, scan, Lc.sp, cl);
+                            luma_segment(P, vertical, e, scan, Lc.sp, cl, any_exempt);
                     } else {
                         const int jj = j - n_luma;
                         const int ne = vertical ? nec_v : nec_h;
@@ -897,7 +964,7 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
                         const int scan = (vertical ? Cb.ty - 4 : Cb.tx - 4) + 4 * (jj / ne);
                         const int emax = vertical ? P.cw : P.ch, smax = vertical ? P.ch : P.cw;
                         if (e >= 8 && e <= emax - 2 && scan >= 0 && scan + 4 <= smax)
-                            chroma_segment(P, vertical, e, scan, Cb.sp, Cr, cl);
+                            chroma_segment(P, vertical, e, scan, Cb.sp, Cr, cl, any_exempt);
                     }
                 }
                 __syncthreads();
@@ -909,6 +976,21 @@ k_filter_tile(const DevPic* __restrict__ pics, uint8_t* __restrict__ out, int rg
             const TileComp k = tcomp(c);
             uint16_t* const to = tout_of(c);
             const bool on = sao_on && (P.flags & (c == 0 ? HPVCD_PIC_SAO_LUMA : HPVCD_PIC_SAO_CHROMA));
+            if (!sao_slow && P.log2_ctb >= 6) {  // one CTB covers the tile component
+                hpvcd_sao_comp sc{};
+                if (on) sc = sao.at(X >> P.log2_ctb, Y >> P.log2_ctb, c);
+                const int bd = c ? P.bd_c : P.bd;
+                const int sel = sc.type_idx == 1 ? 4 : (sc.type_idx == 2 ? sc.eo_class : 5);
+                switch (sel) {
+                    case 0: sao_fixed<0>(k, to, sc, bd, tid); break;
+                    case 1: sao_fixed<1>(k, to, sc, bd, tid); break;
+                    case 2: sao_fixed<2>(k, to, sc, bd, tid); break;
+                    case 3: sao_fixed<3>(k, to, sc, bd, tid); break;
+                    case 4: sao_fixed<4>(k, to, sc, bd, tid); break;
+                    default: sao_fixed<5>(k, to, sc, bd, tid); break;
+                }
+                continue;
+            }
             const int qw = k.tw >> 2, nq = qw * k.th;
             for (int i = tid; i < nq; i += kTileThreads) {
                 const int xq = 4 * (i % qw), yq = i / qw;

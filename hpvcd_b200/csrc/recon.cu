@@ -1127,51 +1127,43 @@ __device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode
     const int n = 1 << log2n;
     const int total = 4 * n + 1;
     const int n2 = 2 * n;
-    uint32_t mask[5];
-    int val[5];
-#pragma unroll
-    for (int wd = 0; wd < 5; ++wd) {
+    // The line's words (32 positions each: 3 for n = 16, 5 for n = 32) are
+    // walked in rolled loops, so the code stays small.  Gather: available
+    // samples go to ws.f; lane w keeps the availability word of word w.
+    const int nw = (total + 31) >> 5;
+    uint32_t my_mask = 0u;
+    int first = -1;  // first available position
+#pragma unroll 1
+    for (int wd = 0; wd < nw; ++wd) {
         const int i = wd * 32 + lane;
         int v = 0;
-        bool a = false;
-        if (wd * 32 < total) {  // warp-uniform: every lane joins the shuffle inside
-            a = gather_ref(k, stamp, jrec, n2, x0, y0, min(i, total - 1), &v);
-            a = a && i < total;
-        }
-        val[wd] = v;
-        mask[wd] = __ballot_sync(kFull, a);
-    }
-    int last_upto[5];
-    int first = -1, run = -1;
-#pragma unroll
-    for (int wd = 0; wd < 5; ++wd) {
-        if (mask[wd]) run = wd * 32 + 31 - __clz(mask[wd]);
-        last_upto[wd] = run;
-        if (first < 0 && mask[wd]) first = wd * 32 + __ffs(mask[wd]) - 1;
-    }
-#pragma unroll
-    for (int wd = 0; wd < 5; ++wd) {
-        const int i = wd * 32 + lane;
-        if (i < total && ((mask[wd] >> lane) & 1u)) ws.f[i] = val[wd];
+        bool a = gather_ref(k, stamp, jrec, n2, x0, y0, min(i, total - 1), &v);
+        a = a && i < total;
+        if (a) ws.f[i] = (int16_t)v;
+        const uint32_t m = __ballot_sync(kFull, a);
+        if (lane == wd) my_mask = m;
+        if (first < 0 && m) first = wd * 32 + __ffs(m) - 1;
     }
     __syncwarp();
+    // ---- substitution: an unavailable sample takes the nearest available
+    // one below it in the line, or the first available one ----
     const int neutral = 1 << (k.bd - 1);
-#pragma unroll
-    for (int wd = 0; wd < 5; ++wd) {
+    int run = -1;  // last available position of the words before
+#pragma unroll 1
+    for (int wd = 0; wd < nw; ++wd) {
         const int i = wd * 32 + lane;
-        if (i >= total) continue;
-        int v;
-        if (first < 0) {
-            v = neutral;
-        } else if ((mask[wd] >> lane) & 1u) {
-            v = val[wd];
-        } else {
-            const uint32_t m0 = mask[wd] & ((2u << lane) - 1u);
-            int j = m0 ? wd * 32 + 31 - __clz(m0) : (wd ? last_upto[wd - 1] : -1);
-            if (j < 0) j = first;
-            v = ws.f[j];
+        const uint32_t m = __shfl_sync(kFull, my_mask, wd);
+        if (i < total) {
+            int v = neutral;
+            if (first >= 0) {
+                const uint32_t m0 = m & ((2u << lane) - 1u);
+                int j = m0 ? wd * 32 + 31 - __clz(m0) : run;
+                if (j < 0) j = first;
+                v = ws.f[j];
+            }
+            ws.s[i] = (int16_t)v;
         }
-        ws.s[i] = v;
+        if (m) run = wd * 32 + 31 - __clz(m);
     }
     __syncwarp();
     // ---- filtering (luma, or 4:4:4 chroma without strong smoothing) ----
@@ -1229,82 +1221,78 @@ __device__ __forceinline__ void intra_tb_prep(const Comp& k, int log2n, int mode
 }
 
 // Intra TB of size 16 or 32, second part: prediction (intra.rs:257-372) and
-// residual add + clip (reconstruct.rs:214-251) by one warp, lane l taking
-// samples l, l + 32, ...  in chunks of eight: a chunk's predictions (from the
-// walk scratch) and residuals (staged in the TB's canvas area) are all
-// loaded before any of its samples is stored, so the loads overlap.
-// kKind: 0 planar, 1 DC, 2 angular.
-template <int kKind>
-__device__ __forceinline__ void predict_chunks(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
-                                               const WalkScratch& ws, const int16_t* R, int lane) {
+// residual add + clip (reconstruct.rs:214-251), lane l of one warp taking
+// samples l, l + 32, ...  A coded TB's residual is in its canvas area
+// (stage_residual).  The loops stay compact: the kernel's code competes for
+// the instruction cache with the other walks resident on the SM.
+__device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
+                                                 const WalkScratch& ws, int lane) {
+    const int tl = lane, ts = 32;
     const int n = 1 << log2n;
     const int n2 = 2 * n;
+    const int16_t* R = ref_filtered(k, n, mode) ? ws.f : ws.s;
     const int max_v = k.max_v;
     const bool edge_filters = k.luma && n < 32;  // is_luma gate of predict_into
     const int vw = min(n, k.pw - (k.ox + x0)), vh = min(n, k.ph - (k.oy + y0));
-    // mode set-up (warp-uniform)
-    const int angle = kKind == 2 ? c_intra_angle[mode - 2] : 0;
-    const bool vertical = mode >= 18;
-    const int a0 = kKind == 2 ? (vertical ? R[n2 + 1] : R[n2 - 1]) : 0;  // above[1] / left[1]
-    const int c0 = kKind == 2 ? R[n2] : 0;
-    const int dc = kKind == 1 ? ws.dc : 0;
-    const int tr = kKind == 0 ? R[n2 + n + 1] : 0, bl = kKind == 0 ? R[n2 - n - 1] : 0;
-    const int per = (n * n) >> 5;  // samples per lane: 8 or 32
-    for (int g = 0; g < per; g += 8) {
-        int v[8], rv[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int i = lane + 32 * (g + u);
+    auto res_at = [&](int xx, int yy) { return (int)(int16_t)k.can[cin(k, x0 + xx, y0 + yy)]; };
+    if (mode >= 2) {
+        const int angle = c_intra_angle[mode - 2];
+        const bool vertical = mode >= 18;
+        const int a0 = vertical ? R[n2 + 1] : R[n2 - 1];  // above[1] / left[1]
+        const int c0 = R[n2];
+#pragma unroll 1
+        for (int i = tl; i < n * n; i += ts) {
             const int yy = i >> log2n, xx = i & (n - 1);
-            int p;
-            if (kKind == 2) {
-                const int a = vertical ? yy : xx;
-                const int b = vertical ? xx : yy;
-                const int pos = (a + 1) * angle;
-                const int iidx = pos >> 5, frac = pos & 31;
-                const int r0 = ws.refs[b + iidx + 1 + n];
-                const int r1 = ws.refs[min(b + iidx + 2, 2 * n) + n];
-                p = clamp3i(frac ? ((32 - frac) * r0 + frac * r1 + 16) >> 5 : r0, 0, max_v);
-                if (edge_filters) {
-                    if (mode == 26 && xx == 0) p = clamp3i(a0 + ((R[n2 - (yy + 1)] - c0) >> 1), 0, max_v);
-                    if (mode == 10 && yy == 0) p = clamp3i(a0 + ((R[n2 + xx + 1] - c0) >> 1), 0, max_v);
-                }
-            } else if (kKind == 1) {
-                p = dc;
-                if (edge_filters) {
-                    if (xx == 0 && yy == 0)
-                        p = (R[n2 - 1] + 2 * dc + R[n2 + 1] + 2) >> 2;
-                    else if (yy == 0)
-                        p = (R[n2 + xx + 1] + 3 * dc + 2) >> 2;
-                    else if (xx == 0)
-                        p = (R[n2 - yy - 1] + 3 * dc + 2) >> 2;
-                }
-            } else {
-                const int hh = (n - 1 - xx) * R[n2 - yy - 1] + (xx + 1) * tr;
-                const int vv = (n - 1 - yy) * R[n2 + xx + 1] + (yy + 1) * bl;
-                p = (hh + vv + n) >> (log2n + 1);
+            const int a = vertical ? yy : xx;
+            const int b = vertical ? xx : yy;
+            const int pos = (a + 1) * angle;
+            const int iidx = pos >> 5, frac = pos & 31;
+            const int r0 = ws.refs[b + iidx + 1 + n];
+            const int r1 = ws.refs[min(b + iidx + 2, 2 * n) + n];
+            int v = frac ? ((32 - frac) * r0 + frac * r1 + 16) >> 5 : r0;
+            v = clamp3i(v, 0, max_v);
+            if (edge_filters) {
+                if (mode == 26 && xx == 0) v = clamp3i(a0 + ((R[n2 - (yy + 1)] - c0) >> 1), 0, max_v);
+                if (mode == 10 && yy == 0) v = clamp3i(a0 + ((R[n2 + xx + 1] - c0) >> 1), 0, max_v);
             }
-            v[u] = p;
-            rv[u] = coded && xx < vw && yy < vh ? (int)(int16_t)k.can[cin(k, x0 + xx, y0 + yy)] : 0;
+            if (xx < vw && yy < vh) {
+                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
+                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
+            }
         }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int i = lane + 32 * (g + u);
+    } else if (mode == 1) {  // DC
+        const int dc = ws.dc;
+#pragma unroll 1
+        for (int i = tl; i < n * n; i += ts) {
             const int yy = i >> log2n, xx = i & (n - 1);
-            if (xx < vw && yy < vh) k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)(coded ? clamp3i(v[u] + rv[u], 0, max_v) : v[u]);
+            int v = dc;
+            if (edge_filters) {
+                if (xx == 0 && yy == 0)
+                    v = (R[n2 - 1] + 2 * dc + R[n2 + 1] + 2) >> 2;
+                else if (yy == 0)
+                    v = (R[n2 + xx + 1] + 3 * dc + 2) >> 2;
+                else if (xx == 0)
+                    v = (R[n2 - yy - 1] + 3 * dc + 2) >> 2;
+            }
+            if (xx < vw && yy < vh) {
+                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
+                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
+            }
+        }
+    } else {  // planar
+        const int tr = R[n2 + n + 1], bl = R[n2 - n - 1];
+#pragma unroll 1
+        for (int i = tl; i < n * n; i += ts) {
+            const int yy = i >> log2n, xx = i & (n - 1);
+            const int hh = (n - 1 - xx) * R[n2 - yy - 1] + (xx + 1) * tr;
+            const int vv = (n - 1 - yy) * R[n2 + xx + 1] + (yy + 1) * bl;
+            int v = (hh + vv + n) >> (log2n + 1);
+            if (xx < vw && yy < vh) {
+                if (coded) v = clamp3i(v + res_at(xx, yy), 0, max_v);
+                k.can[cin(k, x0 + xx, y0 + yy)] = (uint16_t)v;
+            }
         }
     }
-}
-
-__device__ __forceinline__ void intra_tb_predict(const Comp& k, int log2n, int mode, int x0, int y0, bool coded,
-                                                 const WalkScratch& ws, int lane) {
-    const int16_t* R = ref_filtered(k, 1 << log2n, mode) ? ws.f : ws.s;
-    if (mode >= 2)
-        predict_chunks<2>(k, log2n, mode, x0, y0, coded, ws, R, lane);
-    else if (mode == 1)
-        predict_chunks<1>(k, log2n, mode, x0, y0, coded, ws, R, lane);
-    else
-        predict_chunks<0>(k, log2n, mode, x0, y0, coded, ws, R, lane);
 }
 
 // Intra TB of size 16 or 32 by one warp.
@@ -1382,6 +1370,7 @@ struct EdgeGeo {
 template <int kPer>
 __device__ __forceinline__ void fetch_edges(const EdgeGeo& e, uint32_t m, int bps, int t, int nt) {
     int total = 0;
+#pragma unroll 1
     for (int s = 0; s < kSegs; ++s)
         if (m >> s & 1u) total += seg_len(s, e.S, e.Sh);
     int v[kPer], dst[kPer];
@@ -1392,6 +1381,7 @@ __device__ __forceinline__ void fetch_edges(const EdgeGeo& e, uint32_t m, int bp
         v[r] = 0;
         if (i >= total) continue;
         int j = i, s = 0;
+#pragma unroll 1
         for (; s < kSegs; ++s) {
             if (!(m >> s & 1u)) continue;
             const int L = seg_len(s, e.S, e.Sh);
