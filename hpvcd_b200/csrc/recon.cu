@@ -1364,22 +1364,17 @@ struct EdgeGeo {
     int ox, oy, S, Sh, pw, ph;
 };
 
-// Loads the segments m of one component into its canvas, thread t of nt;
-// every load of a thread is issued before its first store.  Samples outside
-// the picture read as 0 (they are never available).
-template <int kPer>
+// Loads the segments m of one component into its canvas, thread t of nt
+// taking samples t, t + nt, ... (a rolled loop: this runs inside the walk,
+// whose code competes for the instruction cache).  Samples outside the
+// picture read as 0 (they are never available).
 __device__ __forceinline__ void fetch_edges(const EdgeGeo& e, uint32_t m, int bps, int t, int nt) {
     int total = 0;
 #pragma unroll 1
     for (int s = 0; s < kSegs; ++s)
         if (m >> s & 1u) total += seg_len(s, e.S, e.Sh);
-    int v[kPer], dst[kPer];
-#pragma unroll
-    for (int r = 0; r < kPer; ++r) {
-        const int i = t + r * nt;
-        dst[r] = -1;
-        v[r] = 0;
-        if (i >= total) continue;
+#pragma unroll 1
+    for (int i = t; i < total; i += nt) {
         int j = i, s = 0;
 #pragma unroll 1
         for (; s < kSegs; ++s) {
@@ -1388,7 +1383,7 @@ __device__ __forceinline__ void fetch_edges(const EdgeGeo& e, uint32_t m, int bp
             if (j < L) break;
             j -= L;
         }
-        if (s >= kSegs) continue;  // unreachable: i < total
+        if (s >= kSegs) break;  // unreachable: i < total
         int dx, dy;
         if (s == 0) {
             dx = -1, dy = -1;
@@ -1397,13 +1392,11 @@ __device__ __forceinline__ void fetch_edges(const EdgeGeo& e, uint32_t m, int bp
         } else {
             dx = -1, dy = (s - 5) * (e.Sh >> 1) + j;
         }
-        dst[r] = can_at(e.S, dx, dy);
         const int ax = e.ox + dx, ay = e.oy + dy;
-        if (ax >= 0 && ay >= 0 && ax < e.pw && ay < e.ph) v[r] = load_sample_cg(e.plane, bps, (size_t)ay * e.pw + ax);
+        int v = 0;
+        if (ax >= 0 && ay >= 0 && ax < e.pw && ay < e.ph) v = load_sample_cg(e.plane, bps, (size_t)ay * e.pw + ax);
+        e.can[can_at(e.S, dx, dy)] = (uint16_t)v;
     }
-#pragma unroll
-    for (int r = 0; r < kPer; ++r)
-        if (dst[r] >= 0) e.can[dst[r]] = (uint16_t)v[r];
 }
 
 // Writes the edge samples of quadrants [from, to) of one component to the
@@ -1493,7 +1486,7 @@ __device__ __forceinline__ uint32_t walk_event(const DevPic& P, uint16_t* can, i
 #pragma unroll
         for (int nb = 0; nb < 4; ++nb) got |= segs_at(nb, __shfl_sync(kFull, lv, nb));
         got = (got | miss) & ~have;
-        fetch_edges<7>(e, got, P.bps, lane, 32);
+        fetch_edges(e, got, P.bps, lane, 32);
         have |= got;
         __syncwarp();
     }
@@ -1782,7 +1775,7 @@ k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint
             s_have[tid] = h;
         }
         __syncthreads();
-        for (int c = 0; c < ncomp; ++c) fetch_edges<(kThreads < 96 ? 4 : 3)>(geo(c), s_have[c], P.bps, tid, kThreads);
+        for (int c = 0; c < ncomp; ++c) fetch_edges(geo(c), s_have[c], P.bps, tid, kThreads);
         cp_async_wait_all();  // this thread's residual copies; the barrier publishes them
         __syncthreads();
         // ---- decode-order walk: each warp reconstructs its components ----
