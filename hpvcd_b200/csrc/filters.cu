@@ -1182,10 +1182,20 @@ extern "C" cudaError_t hpvcd_launch_filter_tile(const hpvcd::DevPic* pics, int n
     return cudaGetLastError();
 }
 
+// The shared-memory limit of the largest layout, and the whole unified L1 /
+// shared array as shared memory, like the wavefront kernel: the tile filter
+// of one concurrent group runs beside another group's wavefront, and an SM
+// changes its L1 / shared split only when it holds no CTA.
 extern "C" cudaError_t hpvcd_filter_tile_setup() {
     const int lim = (int)hpvcd::tile_smem_bytes(1);
     cudaError_t e = cudaFuncSetAttribute(hpvcd::k_filter_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(hpvcd::k_filter_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(hpvcd::k_filter_tile<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(hpvcd::k_filter_tile<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
     return e;
 }

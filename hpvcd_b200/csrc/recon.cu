@@ -1498,6 +1498,12 @@ __device__ __forceinline__ uint32_t walk_event(const DevPic& P, uint16_t* can, i
 // Two warps keep eight CTU walks resident per SM at 4:2:0 (shared memory
 // and registers both allow it); the third warp shortens a CTU whose chroma
 // walk is as long as its luma walk (4:4:4).
+// Register-capped build (kDense, three warps only): at most 80 registers
+// per thread so that eight CTAs of three warps fit an SM instead of five.
+// Each walk is a few percent slower, which costs a single picture whose
+// wavefront holds few CTUs at a time; a batch with thousands of CTUs ready
+// at once is bound by the walks resident per SM instead (a fused batch of
+// 256 mixed-size images: reconstruction 73 -> 61 ms).
 __host__ __device__ constexpr int recon_warps(int kCW) { return 1 + kCW; }
 
 // kFeat: some picture of the launch has slices / tiles, constrained intra
@@ -1505,11 +1511,12 @@ __host__ __device__ constexpr int recon_warps(int kCW) { return 1 + kCW; }
 // availability, coded and PCM tests compile to the plain form.  fine: the
 // quadrant-level wavefront; otherwise a CTU waits for its neighbours' last
 // level before its walk and releases only its last level.
-template <int kCW, bool kFeat>
-__global__ void __launch_bounds__(32 * recon_warps(kCW), kCW == 1 ? 8 : 5)
+template <int kCW, bool kFeat, bool kDense = false>
+__global__ void __launch_bounds__(32 * recon_warps(kCW), kDense ? 8 : (kCW == 1 ? 8 : 5))
 k_recon(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items, uint32_t n_items,
         uint32_t* work_counter, uint32_t* dev_err, int cfmt, uint32_t spin_limit, int fine) {
     static_assert(kCW == 1 || kCW == 2, "one or two chroma warps");
+    static_assert(!kDense || kCW == 2, "the register-capped build has three warps");
     constexpr int kWarps = recon_warps(kCW), kThreads = 32 * kWarps;
     extern __shared__ __align__(16) unsigned char smem[];
     const ReconLayout lay(cfmt, kWarps);
@@ -1902,14 +1909,21 @@ extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd
     // the dynamic shared-memory limit was raised by hpvcd_recon_occupancy()
     // when the plan was built (no non-stream API call here, so launches can
     // be captured into CUDA graphs)
-    // schedule value: 1 one chroma warp (Cb, then Cr), 0 or 2 one warp per chroma component
+    // build: 1 one chroma warp (Cb, then Cr), 2 one warp per chroma
+    // component, 3 the same in the register-capped build
     const int cw = chroma_warps == 1 ? 1 : 2;
     const size_t smem = hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(cw)).total;
     const int threads = 32 * hpvcd::recon_warps(cw);
     // default: 2^22 polls of >= 64 ns each bound one neighbour wait to a few
     // hundred ms
     if (spin == 0) spin = 1u << 22;
-    if (cw == 2 && feat)
+    if (chroma_warps == 3 && feat)
+        hpvcd::k_recon<2, true, true><<<grid, threads, smem, stream>>>(pics, items, n_items, work_counter, dev_err,
+                                                                       cfmt, spin, fine);
+    else if (chroma_warps == 3)
+        hpvcd::k_recon<2, false, true><<<grid, threads, smem, stream>>>(pics, items, n_items, work_counter, dev_err,
+                                                                        cfmt, spin, fine);
+    else if (cw == 2 && feat)
         hpvcd::k_recon<2, true><<<grid, threads, smem, stream>>>(pics, items, n_items, work_counter, dev_err, cfmt,
                                                                  spin, fine);
     else if (cw == 2)
@@ -1925,19 +1939,47 @@ extern "C" cudaError_t hpvcd_launch_recon(const hpvcd::DevPic* pics, const hpvcd
     return cudaGetLastError();
 }
 
-// CTAs per SM of the wavefront kernel with the layout of `cfmt` and one or
-// two chroma warps (raises the shared-memory limit of every instantiation
-// to the 4:4:4 layout of three warps, the largest).
+namespace {
+// Every instantiation: the shared-memory limit of the 4:4:4 layout of three
+// warps (the largest) and the whole unified L1 / shared array as shared
+// memory.  The common carveout matters when waves of different layouts
+// (4:2:0 and 4:4:4, one stream per concurrent group of a batch) follow each
+// other on the SMs: an SM changes its L1 / shared split only when it holds
+// no CTA, so a wave that wanted a larger split than the one running could
+// start only once the other groups' waves had drained every SM.
+template <int kCW, bool kFeat, bool kDense>
+void recon_attrs(int lim) {
+    cudaFuncSetAttribute(hpvcd::k_recon<kCW, kFeat, kDense>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+    cudaFuncSetAttribute(hpvcd::k_recon<kCW, kFeat, kDense>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+}
+}  // namespace
+
+// CTAs per SM of the wavefront kernel with the layout of `cfmt` in build
+// `chroma_warps` (1 two warps, 2 three warps, 3 three warps register-capped),
+// after setting the attributes of every instantiation (recon_attrs).
 extern "C" int hpvcd_recon_occupancy(int cfmt, int chroma_warps) {
     int blocks = 0;
     const int cw = chroma_warps == 1 ? 1 : 2;
     const size_t smem = hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(cw)).total;
     const int lim = (int)hpvcd::ReconLayout(hpvcd::kFmt444, hpvcd::recon_warps(2)).total;
-    cudaFuncSetAttribute(hpvcd::k_recon<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(hpvcd::k_recon<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(hpvcd::k_recon<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    cudaFuncSetAttribute(hpvcd::k_recon<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-    if (cw == 2)
+    recon_attrs<1, false, false>(lim);
+    recon_attrs<2, false, false>(lim);
+    recon_attrs<1, true, false>(lim);
+    recon_attrs<2, true, false>(lim);
+    recon_attrs<2, false, true>(lim);
+    recon_attrs<2, true, true>(lim);
+    // the residual pre-pass of one group runs beside another group's waves
+    cudaFuncSetAttribute(hpvcd::k_residual<hpvcd::kIdctMatrix>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(hpvcd::k_residual<hpvcd::kIdctButterfly>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(hpvcd::k_residual<hpvcd::kIdctTensor>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
+    if (chroma_warps == 3)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<2, false, true>,
+                                                      32 * hpvcd::recon_warps(2), smem);
+    else if (cw == 2)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<2, false>, 32 * hpvcd::recon_warps(2),
                                                       smem);
     else

@@ -213,14 +213,29 @@ struct hpvcd_plan {
     // 4:2:2), so the pictures of one class get the CTAs per SM of their own
     // layout.  item_off / n_full: the wave's range of the CTU work list;
     // n_items: entries launched (one fewer while a test drops a CTU).
+    // ready: CTUs of the wave that can be walked at once (per picture, the
+    // longest x + 2y diagonal of its CTB grid), which picks the build.
     struct Wave {
         uint32_t seg;
         int cfmt;
         uint32_t item_off, n_items, n_full;
+        uint32_t ready;
     };
     std::vector<Wave> waves;
-    int occ[3][2] = {{1, 1}, {1, 1}, {1, 1}};  // k_recon CTAs per SM by class and chroma warps (1, 2)
-    int occ_of(int cfmt) const { return occ[cfmt][sched.chroma_warps == 1 ? 0 : 1]; }
+    // k_recon CTAs per SM by class and build (1 two warps, 2 three warps,
+    // 3 three warps register-capped; index build - 1)
+    int occ[3][3] = {{1, 1, 1}, {1, 1, 1}, {1, 1, 1}};
+    // Build of a wave's wavefront kernel (hpvcd_sched.chroma_warps): 0 picks
+    // three warps, register-capped when the wave has more CTUs ready at once
+    // than the plain build's CTAs can hold (its share of them when segments
+    // run concurrently).
+    int build_of(const Wave& wv, int n_seg) const {
+        const uint32_t cw = sched.chroma_warps;
+        if (cw >= 1 && cw <= 3) return (int)cw;
+        const int slots = concurrent ? sms * occ[wv.cfmt][1] / std::max(1, n_seg) : sms * occ[wv.cfmt][1];
+        return wv.ready > (uint32_t)slots ? 3 : 2;
+    }
+    int occ_of(int cfmt, int build) const { return occ[cfmt][build - 1]; }
     int sms = 148;
     int max_rgb = 0;  // largest RGB job of one picture, in 4-pixel quads
     uint32_t launches_per_run = 0;
@@ -483,7 +498,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         P->out.kind = HPVCD_OUT_YUV;
     }
     if (sched) {
-        if (sched->idct > 2 || sched->chroma_warps > 2) {
+        if (sched->idct > 2 || sched->chroma_warps > 3) {
             delete P;
             return HPVCD_ERR_INVALID_ARG;
         }
@@ -572,6 +587,13 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
         }
         for (int cls = 0; cls < 3; ++cls) {
             const uint32_t off = (uint32_t)P->items.size();
+            uint32_t ready = 0;
+            for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
+                const hpvcd_picture& p = pics[i];
+                if ((p.flags & HPVCD_PIC_PRED_IN_PLANE) || recon_class(p) != cls) continue;
+                const Geo g = geo_of(p);
+                ready += (uint32_t)std::min(g.ctb_rows, (g.ctb_cols + 1) / 2);
+            }
             for (int t = 0; t <= max_t; ++t)
                 for (uint32_t i = s.first_pic; i < s.first_pic + s.n_pics; ++i) {
                     const hpvcd_picture& p = pics[i];
@@ -584,7 +606,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
                     }
                 }
             const uint32_t cnt = (uint32_t)P->items.size() - off;
-            if (cnt) P->waves.push_back(hpvcd_plan::Wave{si, cls, off, cnt, cnt});
+            if (cnt) P->waves.push_back(hpvcd_plan::Wave{si, cls, off, cnt, cnt, ready});
         }
         s.n_waves = (uint32_t)P->waves.size() - s.wave_first;
     }
@@ -772,7 +794,7 @@ hpvcd_status plan_build(const hpvcd_picture* pics, uint32_t n, const hpvcd_outpu
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
     P->sms = sms;
     for (int cls = 0; cls < 3; ++cls)
-        for (int cw = 1; cw <= 2; ++cw) P->occ[cls][cw - 1] = std::max(1, hpvcd_recon_occupancy(cls, cw));
+        for (int cw = 1; cw <= 3; ++cw) P->occ[cls][cw - 1] = std::max(1, hpvcd_recon_occupancy(cls, cw));
     {
         const cudaError_t fe = hpvcd_filter_tile_setup();
         if (fe != cudaSuccess) {
@@ -848,13 +870,14 @@ hpvcd_status plan_launch(hpvcd_plan* P, uint32_t stages, cudaStream_t st) {
             // its own layout and work counter
             for (uint32_t w = s.wave_first; w < s.wave_first + s.n_waves; ++w) {
                 const hpvcd_plan::Wave& wv = P->waves[w];
-                int occ = P->occ_of(wv.cfmt);
+                const int build = P->build_of(wv, (int)n_seg);
+                int occ = P->occ_of(wv.cfmt, build);
                 if (P->sched.recon_ctas_per_sm > 0) occ = std::min<int>(occ, (int)P->sched.recon_ctas_per_sm);
                 // concurrent segments share the SMs: each gets its share of the CTAs
                 const int share = P->concurrent ? std::max(1, P->sms * occ / (int)n_seg) : P->sms * occ;
                 const int grid = std::max(1, std::min<int>(share, (int)wv.n_items));
                 e = hpvcd_launch_recon(P->d_pics, P->d_items + wv.item_off, wv.n_items, P->d_scratch + w, d_err,
-                                       wv.cfmt, grid, (int)P->sched.chroma_warps, P->recon_feat ? 1 : 0,
+                                       wv.cfmt, grid, build, P->recon_feat ? 1 : 0,
                                        P->sched.wave ? 0 : 1, P->spin_limit, st);
                 if (e != cudaSuccess) return cuda_status(e);
             }
@@ -1316,7 +1339,7 @@ HPVCD_API hpvcd_status hpvcd_plan_autotune(hpvcd_plan* plan, const hpvcd_sched* 
 HPVCD_API hpvcd_status hpvcd_plan_set_sched(hpvcd_plan* plan, const hpvcd_sched* sched) {
     if (!plan) return HPVCD_ERR_INVALID_ARG;
     const hpvcd_sched next = sched ? *sched : hpvcd_sched{};
-    if (next.idct > 2 || next.chroma_warps > 2 || next.wave > 1) return HPVCD_ERR_INVALID_ARG;
+    if (next.idct > 2 || next.chroma_warps > 3 || next.wave > 1) return HPVCD_ERR_INVALID_ARG;
     if (std::memcmp(&next, &plan->sched, sizeof(next)) == 0) return HPVCD_OK;
     plan->sched = next;
     // graphs captured with the previous schedule hold its kernels
@@ -1743,7 +1766,10 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     {
         if (others > 0) {
             hpvcd_sched s2 = slot->plan->sched;
-            const int occ = std::max(1, slot->plan->occ_of(0));
+            const hpvcd_plan* pl = slot->plan;
+            const int occ = std::max(1, pl->waves.empty() ? pl->occ_of(0, 2)
+                                                           : pl->occ_of(pl->waves[0].cfmt,
+                                                                        pl->build_of(pl->waves[0], 1)));
             const int share = std::max(1, occ / (others + 1));
             const int cur = s2.recon_ctas_per_sm ? (int)s2.recon_ctas_per_sm : occ;
             s2.recon_ctas_per_sm = (uint32_t)std::min(cur, share);

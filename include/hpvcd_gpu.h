@@ -482,9 +482,13 @@ typedef struct hpvcd_sched {
                                    tensor-core products (int16 operands split exactly into int8
                                    halves), 1 even-odd butterflies, 2 matrix product with all-zero
                                    rows / columns skipped */
-    uint32_t chroma_warps;      /* chroma walk of the wavefront kernel: 0|2 one warp per chroma
-                                   component (three warps per CTA), 1 one warp for Cb, then Cr
-                                   (two warps per CTA: more CTAs per SM) */
+    uint32_t chroma_warps;      /* build of the wavefront kernel: 2 one warp per chroma component
+                                   (three warps per CTA), 1 one warp for Cb, then Cr (two warps
+                                   per CTA: more CTAs per SM), 3 three warps with at most 80
+                                   registers per thread (8 CTAs per SM instead of 5: for batches
+                                   with thousands of CTUs ready at once), 0 three warps, the
+                                   register-capped build for a wave with more CTUs ready at once
+                                   than the plain build's CTAs hold */
     uint32_t recon_ctas_per_sm; /* persistent wavefront CTAs per SM (0 -> occupancy max) */
     uint32_t wave;              /* wavefront synchronisation: 0 per quadrant (a CTU is walked while
                                    its left / above-right neighbours still are), 1 whole CTUs (one

@@ -419,7 +419,7 @@ def test_schedule_variants_bit_exact():
     ref, _ = O.decode_batch(pics)
     plan = DevicePlan(pics)
     for idct in (0, 1, 2):      # matrix, butterflies, integer tensor cores
-        for cw in (1, 2):       # chroma warps of the wavefront kernel
+        for cw in (1, 2, 3):    # wavefront build: two warps, three, three register-capped
             for ctas in (0, 1):
                 for wave in (0, 1):   # quadrant-level / whole-CTU wavefront
                     plan.set_sched(abi.Sched(idct, cw, ctas, wave))
@@ -431,6 +431,8 @@ def test_schedule_variants_bit_exact():
         plan.set_sched(abi.Sched(0, 1, 0, 2))
     with pytest.raises(abi.HpvcdError):
         plan.set_sched(abi.Sched(3, 1, 0, 0))
+    with pytest.raises(abi.HpvcdError):
+        plan.set_sched(abi.Sched(0, 4, 0, 0))
     plan.close()
 
 
@@ -803,6 +805,11 @@ def test_slices_and_tiles(dec, regions, idc, no_across):
     plan.launch()
     torch.cuda.synchronize()
     assert_planes_equal([plan.planes(i) for i in range(len(pics))], ref, "regions plan")
+    for cw in (1, 2, 3):  # every wavefront build with the slice / tile tests compiled in
+        plan.set_sched(abi.Sched(0, cw, 0, 0))
+        plan.launch()
+        assert plan.status() == abi.OK
+        assert_planes_equal([plan.planes(i) for i in range(len(pics))], ref, f"regions plan, build {cw}")
     plan.close()
 
 
