@@ -566,6 +566,15 @@ def run_ours(args):
         pg = run_e2e(pics, g, K2, args.warmup, local, world, dev, max(1, args.e2e_inflight), args.e2e_schedule,
                      pageable=True)
         e2e["pageable_inputs"] = {k: pg[k] for k in ("value", "ms_per_step", "p50_ms", "p99_ms", "api")}
+        # the end-to-end rate against the link it crosses: the canvas read
+        # back each step is the larger direction
+        link = pcie_link(dev, int(e2e["h2d_bytes_per_step"]), int(e2e["d2h_bytes_per_step"]))
+        e2e_d2h = e2e["d2h_bytes_per_step"] / (e2e["ms_per_step"] / 1e3) / 1e9
+        e2e_h2d = e2e["h2d_bytes_per_step"] / (e2e["ms_per_step"] / 1e3) / 1e9
+        link.update({"e2e_d2h_gbs": round(e2e_d2h, 1), "e2e_h2d_gbs": round(e2e_h2d, 1),
+                     "frac_of_concurrent_d2h": (round(e2e_d2h / link["concurrent_d2h_gbs"], 3)
+                                                if link["concurrent_d2h_gbs"] else None)})
+        e2e["pcie"] = link
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -606,6 +615,48 @@ def run_ours(args):
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
+
+
+def pcie_link(dev, h2d_bytes: int, d2h_bytes: int, reps: int = 20) -> dict:
+    """Measured host<->device copy bandwidth of this box for one end-to-end
+    step's byte counts (page-locked host buffers, one cudaMemcpyAsync per
+    direction and step, CUDA events): each direction alone and both at once
+    on two streams, as the end-to-end loop runs them."""
+    import torch
+    h_in = torch.empty(h2d_bytes, dtype=torch.uint8, pin_memory=True)
+    h_out = torch.empty(d2h_bytes, dtype=torch.uint8, pin_memory=True)
+    d_in = torch.empty(h2d_bytes, dtype=torch.uint8, device=dev)
+    d_out = torch.empty(d2h_bytes, dtype=torch.uint8, device=dev)
+    s_up, s_down = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+
+    def timed(up: bool, down: bool) -> tuple[float, float]:
+        ev = {k: [torch.cuda.Event(enable_timing=True) for _ in range(2)] for k in ("up", "down")}
+        torch.cuda.synchronize(dev)
+        if up:
+            ev["up"][0].record(s_up)
+            for _ in range(reps):
+                with torch.cuda.stream(s_up):
+                    d_in.copy_(h_in, non_blocking=True)
+            ev["up"][1].record(s_up)
+        if down:
+            ev["down"][0].record(s_down)
+            for _ in range(reps):
+                with torch.cuda.stream(s_down):
+                    h_out.copy_(d_out, non_blocking=True)
+            ev["down"][1].record(s_down)
+        torch.cuda.synchronize(dev)
+        gb_up = h2d_bytes * reps / (ev["up"][0].elapsed_time(ev["up"][1]) / 1e3) / 1e9 if up else 0.0
+        gb_down = d2h_bytes * reps / (ev["down"][0].elapsed_time(ev["down"][1]) / 1e3) / 1e9 if down else 0.0
+        return gb_up, gb_down
+
+    timed(True, True)  # warm-up
+    up, _ = timed(True, False)
+    _, down = timed(False, True)
+    both_up, both_down = timed(True, True)
+    return {"h2d_gbs": round(up, 1), "d2h_gbs": round(down, 1), "concurrent_h2d_gbs": round(both_up, 1),
+            "concurrent_d2h_gbs": round(both_down, 1),
+            "how": f"page-locked copies of one step's bytes ({h2d_bytes} up, {d2h_bytes} down), "
+                   f"{reps} per direction, alone and both directions at once, CUDA events"}
 
 
 def recon_algorithmic_bytes(pics) -> tuple[int, int]:

@@ -549,6 +549,173 @@ __device__ void tb_residual_warp(const DevPic& P, const hpvcd_tu& t, const int16
 // prefetches their coefficients into L2, then transforms them one by one.
 constexpr int kResChunk = 32;
 
+// Dequantisation scale m_levelScale[qs % 6] (transform.rs:701-725) without a
+// table: lanes of one warp index it differently, which a constant-bank read
+// would serialise.
+__device__ __forceinline__ int level_scale(int r) {
+    return r == 0 ? 40 : (r == 1 ? 45 : (r == 2 ? 51 : (r == 3 ? 57 : (r == 4 ? 64 : 72))));
+}
+
+// One 4-point inverse transform, DST-VII (kDst) or DCT, with the basis as
+// immediates: o[m] = sum_k T[k][m] * in[k] (transform.rs:535-603 for the
+// DST, :406-533 for the DCT; the H.265 matrices).
+template <bool kDst>
+__device__ __forceinline__ void inv4(int i0, int i1, int i2, int i3, int& o0, int& o1, int& o2, int& o3) {
+    if (kDst) {
+        o0 = 29 * i0 + 74 * i1 + 84 * i2 + 55 * i3;
+        o1 = 55 * i0 + 74 * i1 - 29 * i2 - 84 * i3;
+        o2 = 74 * i0 - 74 * i2 + 74 * i3;
+        o3 = 84 * i0 - 74 * i1 + 55 * i2 - 29 * i3;
+    } else {
+        const int e0 = 64 * (i0 + i2), e1 = 64 * (i0 - i2);
+        const int q0 = 83 * i1 + 36 * i3, q1 = 36 * i1 - 83 * i3;
+        o0 = e0 + q0;
+        o1 = e1 + q1;
+        o2 = e1 - q1;
+        o3 = e0 - q0;
+    }
+}
+
+// Both stages of a 4x4 inverse transform in one thread's registers: d is
+// the dequantised block (row k, column c at d[4k + c]); on return d holds
+// the residual before the storage wrap.  Stage 1 (columns) clips
+// (sum + 64) >> 7 to int16, stage 2 (rows) adds 2^(shift2 - 1) and shifts
+// by shift2, the same sums as the warp path of tb_residual_warp.
+template <bool kDst>
+__device__ __forceinline__ void idct4_thread(int (&d)[16], int shift2) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        int o0, o1, o2, o3;
+        inv4<kDst>(d[c], d[4 + c], d[8 + c], d[12 + c], o0, o1, o2, o3);
+        d[c] = clamp3i((o0 + 64) >> 7, -32768, 32767);
+        d[4 + c] = clamp3i((o1 + 64) >> 7, -32768, 32767);
+        d[8 + c] = clamp3i((o2 + 64) >> 7, -32768, 32767);
+        d[12 + c] = clamp3i((o3 + 64) >> 7, -32768, 32767);
+    }
+    const int add2 = 1 << (shift2 - 1);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        int o0, o1, o2, o3;
+        inv4<kDst>(d[4 * r], d[4 * r + 1], d[4 * r + 2], d[4 * r + 3], o0, o1, o2, o3);
+        d[4 * r] = (o0 + add2) >> shift2;
+        d[4 * r + 1] = (o1 + add2) >> shift2;
+        d[4 * r + 2] = (o2 + add2) >> shift2;
+        d[4 * r + 3] = (o3 + add2) >> shift2;
+    }
+}
+
+// A record k_residual's per-thread path takes: a coded, valid 4x4 TB with
+// a transform (no transform skip, bypass, I_PCM or RExt residual tool) whose
+// residual is not k_ccp's.
+__device__ __forceinline__ bool tb4_thread_ok(const DevPic& P, const hpvcd_tu& t) {
+    constexpr uint32_t kOther = HPVCD_TU_TSKIP | HPVCD_TU_TQB | HPVCD_TU_ROTATE | HPVCD_TU_RDPCM_H |
+                                HPVCD_TU_RDPCM_V | HPVCD_TU_PCM;
+    if (!(t.flags & HPVCD_TU_CBF) || (t.flags & kOther) || t.log2n != 2) return false;
+    if ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && t.comp && t.res_scale) return false;
+    const int ncomp = P.idc ? 3 : 1;
+    if (t.comp >= ncomp) return false;
+    const int pw = t.comp ? P.cw : P.w, ph = t.comp ? P.ch : P.h;
+    return (int)t.x < pw && (int)t.y < ph && (uint64_t)t.coeff_off + 16 <= P.n_coeffs;
+}
+
+// Residual of one such 4x4 TB by one thread (the 4x4 case of
+// tb_residual_warp: dequantisation transform.rs:764-858 with the same
+// per-coefficient factor, then idct4_thread), stored where the warp path
+// stores it: added to the plane and clipped for TBs predicted in the
+// plane, else into the int16 residual plane.
+__device__ void tb4_thread(const DevPic& P, const hpvcd_tu& t) {
+    const int c = t.comp;
+    const bool luma = c == 0;
+    const int bd = luma ? P.bd : P.bd_c;
+    int qpp;
+    if (luma) {
+        qpp = qp_prime(t.qp_y, bd);
+    } else {
+        const int pps_off = c == 1 ? P.pps_cb_qp_offset : P.pps_cr_qp_offset;
+        qpp = qp_prime(qpc_map(t.qp_y + pps_off + t.cqp_off, P.idc, bd), bd);
+    }
+    const int bd_shift = bd + 2 + 10 - 15;
+    const int qs = clamp3i(qpp, 0, 51 + 6 * (bd - 8));
+    const long long base = (long long)level_scale(qs % 6) * (1ll << (qs / 6));
+    const long long add = 1ll << (bd_shift - 1);
+    const uint8_t* sm = nullptr;
+    if (P.scaling) sm = P.scaling->m[0][min(c, 2) + ((t.flags & HPVCD_TU_INTRA) ? 0 : 3)];
+    const int nx = (t.nx == 0 || t.nx > 4) ? 4 : t.nx;
+    int d[16];
+    const bool c8 = (P.flags & HPVCD_PIC_COEFF8) != 0;
+    if (c8) {
+        const int8_t* lv = (const int8_t*)P.coeffs + t.coeff_off;
+        if (((uintptr_t)lv & 15) == 0) {
+            const int4 w = *(const int4*)lv;
+            const int ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int i = 0; i < 16; ++i) d[i] = (int)(int8_t)(ws[i >> 2] >> (8 * (i & 3)));
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) d[i] = lv[i];
+        }
+    } else {
+        const int16_t* lv = P.coeffs + t.coeff_off;
+        if (((uintptr_t)lv & 15) == 0) {
+            const int4 w0 = *(const int4*)lv, w1 = *(const int4*)(lv + 8);
+            const int ws[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+            for (int i = 0; i < 16; ++i) d[i] = (int)(int16_t)(ws[i >> 1] >> (16 * (i & 1)));
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) d[i] = lv[i];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const long long f = sm ? base * sm[i] : base * 16;
+        const long long v = ((long long)d[i] * f + add) >> bd_shift;
+        d[i] = (i & 3) < nx ? (int)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v)) : 0;
+    }
+    const int shift2 = 20 - bd;
+    if (luma && (t.flags & HPVCD_TU_INTRA))
+        idct4_thread<true>(d, shift2);
+    else
+        idct4_thread<false>(d, shift2);
+    const bool i16s = bd <= 8;
+    const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+    const int x0 = t.x, y0 = t.y;
+    const bool in_plane = (P.flags & HPVCD_PIC_PRED_IN_PLANE) || !(t.flags & HPVCD_TU_INTRA);
+    if (in_plane) {  // reconstruct.rs:214-251: add and clip into the plane
+        void* pl = P.rec[c];
+        const int mx = (1 << bd) - 1;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int x = x0 + (i & 3), y = y0 + (i >> 2);
+            if (x < pw && y < ph) {
+                const int v = i16s ? (int)(int16_t)d[i] : d[i];
+                const size_t idx = (size_t)y * pw + x;
+                store_sample(pl, P.bps, idx, clamp3i(load_sample(pl, P.bps, idx) + v, 0, mx));
+            }
+        }
+    } else {  // the int16 residual plane k_recon adds to its prediction
+        int16_t* rp = P.res[c];
+        const int rs = P.res_stride[c];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int y = y0 + r;
+            if (y >= ph) break;
+            int16_t* row = rp + (size_t)y * rs + x0;
+            int16_t v4[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) v4[m] = (int16_t)sat16(i16s ? (int)(int16_t)d[4 * r + m] : d[4 * r + m]);
+            if (x0 + 4 <= pw && ((uintptr_t)row & 7) == 0) {
+                *(uint2*)row = make_uint2((uint32_t)(uint16_t)v4[0] | ((uint32_t)(uint16_t)v4[1] << 16),
+                                          (uint32_t)(uint16_t)v4[2] | ((uint32_t)(uint16_t)v4[3] << 16));
+            } else {
+#pragma unroll
+                for (int m = 0; m < 4; ++m)
+                    if (x0 + m < pw) row[m] = v4[m];
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
@@ -574,6 +741,7 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
         const uint32_t gl = g0 + lane;
         uint32_t pic = 0;
         uint4 r4 = make_uint4(0u, 0u, 0u, 0u);
+        bool mine4 = false;  // a plain coded 4x4 TB: this lane transforms it on its own
         if (gl < total) {
             uint32_t lo = 0, hi = n_pics;
             while (hi - lo > 1) {
@@ -585,7 +753,9 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
             r4 = *(const uint4*)(P.tus + (gl - rec_prefix[lo]));  // records are 16-byte aligned
             hpvcd_tu t;
             memcpy(&t, &r4, sizeof(t));
-            if ((t.flags & HPVCD_TU_CBF) && t.log2n >= 2 && t.log2n <= 5) {
+            if (tb4_thread_ok(P, t)) {
+                mine4 = true;
+            } else if ((t.flags & HPVCD_TU_CBF) && t.log2n >= 2 && t.log2n <= 5) {
                 const uint32_t esz = (P.flags & HPVCD_PIC_COEFF8) ? 1u : 2u;
                 const uint64_t n2 = 1ull << (2 * t.log2n);
                 if ((uint64_t)t.coeff_off + n2 <= P.n_coeffs) {
@@ -595,9 +765,18 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
                 }
             }
         }
-        // ---- the chunk's records one by one ----
+        // ---- the plain coded 4x4 TBs (most coded TBs): one per lane, in
+        // registers ----
+        if (mine4) {
+            hpvcd_tu t;
+            memcpy(&t, &r4, sizeof(t));
+            tb4_thread(pics[pic], t);
+        }
+        const uint32_t done4 = __ballot_sync(kAll, mine4);
+        // ---- the chunk's other records one by one ----
         const uint32_t nrec = min((uint32_t)kResChunk, total - g0);
         for (uint32_t j = 0; j < nrec; ++j) {
+            if ((done4 >> j) & 1u) continue;
             const uint32_t pj = __shfl_sync(kAll, pic, j);
             uint4 w4;
             w4.x = __shfl_sync(kAll, r4.x, j);

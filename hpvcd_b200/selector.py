@@ -382,6 +382,56 @@ def collect_batches(n_batches: int, seed: int = 0, out_path: str | None = None, 
     return X, T
 
 
+# Photo sizes of grid-coded stills (HEIC): 12 MP in both orientations,
+# 4:3 and 16:9 crops, 48 MP and 8 MP.
+GRID_SIZES = [(4032, 3024), (3024, 4032), (4000, 3000), (4032, 2268), (8064, 6048), (3264, 2448)]
+
+
+def collect_grids(n_grids: int, seed: int = 2, out_path: str | None = None, threads: int = 4,
+                  reps: int = 2, log_every: int = 25, start: int = 0):
+    """Grid-coded stills as the selector sees them: one photo (GRID_SIZES,
+    10-bit in 3 of 4, else 8-bit; 4:2:0) split into 512x512 tiles, int8
+    level pools where every level fits, decoded to an RGB8 canvas only;
+    features over its tiles and the autotuner's time of every schedule.
+    Returns (features, ms)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from . import synth
+    from .gpu import DevicePlan
+
+    rng = np.random.default_rng(seed)
+    specs = [(GRID_SIZES[int(rng.integers(len(GRID_SIZES)))], 8 if rng.random() < 0.25 else 10)
+             for _ in range(start + n_grids)][start:]
+
+    def make(i):
+        (w, h), bd = specs[i]
+        g = synth.make_grid(w, h, seed=seed * 100_019 + start + i, bit_depth=bd, chroma_idc=1)
+        pics = g.synth.pictures()
+        return g, pics, synth.narrow_coeffs(pics)
+
+    X = np.zeros((n_grids, abi.FEATURES), np.float32)
+    T = np.zeros((n_grids, K), np.float32)
+    with ThreadPoolExecutor(threads) as pool:
+        futs = [pool.submit(make, i) for i in range(min(threads, n_grids))]
+        nxt = len(futs)
+        for i in range(n_grids):
+            g, pics, c8 = futs[i].result()
+            futs[i] = None
+            if nxt < n_grids:
+                futs.append(pool.submit(make, nxt))
+                nxt += 1
+            out, okeep = synth.grid_output(g)
+            out.options = abi.OUTPUT_CANVAS_ONLY
+            plan = DevicePlan(pics, out)
+            X[i], T[i] = measure_range(plan, 0, len(pics), reps=reps)
+            plan.close()
+            del g, pics, c8, okeep
+            if out_path and ((i + 1) % log_every == 0 or i + 1 == n_grids):
+                np.savez(out_path, features=X[:i + 1], ms=T[:i + 1], seed=seed, start=start)
+                print(f"[selector] {i + 1}/{n_grids} grids", flush=True)
+    return X, T
+
+
 # ---------------------------------------------------------------------------
 # Training and evaluation
 # ---------------------------------------------------------------------------
@@ -473,6 +523,12 @@ def _main(argv=None):
     b.add_argument("--seed", type=int, default=1)
     b.add_argument("--out", required=True)
     b.add_argument("--threads", type=int, default=4)
+    gq = sub.add_parser("collect-grids")
+    gq.add_argument("--grids", type=int, required=True)
+    gq.add_argument("--start", type=int, default=0)
+    gq.add_argument("--seed", type=int, default=2)
+    gq.add_argument("--out", required=True)
+    gq.add_argument("--threads", type=int, default=4)
     t = sub.add_parser("train")
     t.add_argument("--data", nargs="+", required=True)
     t.add_argument("--holdout", type=float, default=0.2)
@@ -487,6 +543,8 @@ def _main(argv=None):
         collect(a.frames, seed=a.seed, out_path=a.out, threads=a.threads, start=a.start)
     elif a.cmd == "collect-batches":
         collect_batches(a.batches, seed=a.seed, out_path=a.out, threads=a.threads, start=a.start)
+    elif a.cmd == "collect-grids":
+        collect_grids(a.grids, seed=a.seed, out_path=a.out, threads=a.threads, start=a.start)
     elif a.cmd == "train":
         xs, ts = [], []
         for path in a.data:
