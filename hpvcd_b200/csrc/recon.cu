@@ -604,18 +604,18 @@ __device__ __forceinline__ void idct4_thread(int (&d)[16], int shift2) {
     }
 }
 
-// A record k_residual's per-thread path takes: a coded, valid 4x4 TB with
-// a transform (no transform skip, bypass, I_PCM or RExt residual tool) whose
-// residual is not k_ccp's.
-__device__ __forceinline__ bool tb4_thread_ok(const DevPic& P, const hpvcd_tu& t) {
+// A record k_residual's per-lane paths take: a coded, valid TB of size
+// 2^log2n with a transform (no transform skip, bypass, I_PCM or RExt residual
+// tool) whose residual is not k_ccp's.
+__device__ __forceinline__ bool tb_lanes_ok(const DevPic& P, const hpvcd_tu& t, int log2n) {
     constexpr uint32_t kOther = HPVCD_TU_TSKIP | HPVCD_TU_TQB | HPVCD_TU_ROTATE | HPVCD_TU_RDPCM_H |
                                 HPVCD_TU_RDPCM_V | HPVCD_TU_PCM;
-    if (!(t.flags & HPVCD_TU_CBF) || (t.flags & kOther) || t.log2n != 2) return false;
+    if (!(t.flags & HPVCD_TU_CBF) || (t.flags & kOther) || t.log2n != log2n) return false;
     if ((P.flags & HPVCD_PIC_CROSS_COMPONENT) && t.comp && t.res_scale) return false;
     const int ncomp = P.idc ? 3 : 1;
     if (t.comp >= ncomp) return false;
     const int pw = t.comp ? P.cw : P.w, ph = t.comp ? P.ch : P.h;
-    return (int)t.x < pw && (int)t.y < ph && (uint64_t)t.coeff_off + 16 <= P.n_coeffs;
+    return (int)t.x < pw && (int)t.y < ph && (uint64_t)t.coeff_off + (1u << (2 * log2n)) <= P.n_coeffs;
 }
 
 // Residual of one such 4x4 TB by one thread (the 4x4 case of
@@ -720,6 +720,105 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// 8-point inverse DCT with the basis as immediates, even-odd form:
+// o[m] = sum_k T8[k][m] * in[k] (transform.rs:406-533, the H.265 matrix).
+__device__ __forceinline__ void inv8(const int (&in)[8], int (&o)[8]) {
+    const int ee0 = 64 * (in[0] + in[4]), ee1 = 64 * (in[0] - in[4]);
+    const int eo0 = 83 * in[2] + 36 * in[6], eo1 = 36 * in[2] - 83 * in[6];
+    const int e0 = ee0 + eo0, e3 = ee0 - eo0, e1 = ee1 + eo1, e2 = ee1 - eo1;
+    const int o0 = 89 * in[1] + 75 * in[3] + 50 * in[5] + 18 * in[7];
+    const int o1 = 75 * in[1] - 18 * in[3] - 89 * in[5] - 50 * in[7];
+    const int o2 = 50 * in[1] - 89 * in[3] + 18 * in[5] + 75 * in[7];
+    const int o3 = 18 * in[1] - 50 * in[3] + 75 * in[5] - 89 * in[7];
+    o[0] = e0 + o0; o[7] = e0 - o0;
+    o[1] = e1 + o1; o[6] = e1 - o1;
+    o[2] = e2 + o2; o[5] = e2 - o2;
+    o[3] = e3 + o3; o[4] = e3 - o3;
+}
+
+// Stage 1 of a plain coded 8x8 TB by lane q (0..7) of its group of eight:
+// column q dequantised (the 8x8 case of tb_residual_warp: factor
+// base * m[r][q] or base * 16, columns >= nx zero) and inverse transformed,
+// (sum + 64) >> 7 clipped to int16 into the group's scratch S[m * 9 + q].
+__device__ void tb8_cols(const DevPic& P, const hpvcd_tu& t, int q, int16_t* S) {
+    const int c = t.comp;
+    const int bd = c ? P.bd_c : P.bd;
+    int qpp;
+    if (c == 0) {
+        qpp = qp_prime(t.qp_y, bd);
+    } else {
+        const int pps_off = c == 1 ? P.pps_cb_qp_offset : P.pps_cr_qp_offset;
+        qpp = qp_prime(qpc_map(t.qp_y + pps_off + t.cqp_off, P.idc, bd), bd);
+    }
+    const int bd_shift = bd + 3 + 10 - 15;
+    const int qs = clamp3i(qpp, 0, 51 + 6 * (bd - 8));
+    const long long base = (long long)level_scale(qs % 6) * (1ll << (qs / 6));
+    const long long add = 1ll << (bd_shift - 1);
+    const uint8_t* sm = nullptr;
+    if (P.scaling) sm = P.scaling->m[1][min(c, 2) + ((t.flags & HPVCD_TU_INTRA) ? 0 : 3)];
+    const int nx = (t.nx == 0 || t.nx > 8) ? 8 : t.nx;
+    const bool c8 = (P.flags & HPVCD_PIC_COEFF8) != 0;
+    int in[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int i = r * 8 + q;
+        const int l = c8 ? (int)((const int8_t*)P.coeffs + t.coeff_off)[i] : (int)(P.coeffs + t.coeff_off)[i];
+        const long long f = sm ? base * sm[i] : base * 16;
+        const long long v = ((long long)l * f + add) >> bd_shift;
+        in[r] = q < nx ? (int)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v)) : 0;
+    }
+    int o[8];
+    inv8(in, o);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) S[m * 9 + q] = (int16_t)clamp3i((o[m] + 64) >> 7, -32768, 32767);
+}
+
+// Stage 2 of the same TB by lane q: row q of the stage-1 result, inverse
+// transformed, + 2^(shift2 - 1) >> shift2, stored as tb4_thread stores
+// (added to the plane, or into the int16 residual plane).
+__device__ void tb8_rows(const DevPic& P, const hpvcd_tu& t, int q, const int16_t* S) {
+    const int c = t.comp;
+    const int bd = c ? P.bd_c : P.bd;
+    const int shift2 = 20 - bd, add2 = 1 << (shift2 - 1);
+    const bool i16s = bd <= 8;
+    int in[8], o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) in[k] = S[q * 9 + k];
+    inv8(in, o);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int v = (o[m] + add2) >> shift2;
+        o[m] = i16s ? (int)(int16_t)v : v;
+    }
+    const int pw = c ? P.cw : P.w, ph = c ? P.ch : P.h;
+    const int x0 = t.x, y = t.y + q;
+    if (y >= ph) return;
+    const bool in_plane = (P.flags & HPVCD_PIC_PRED_IN_PLANE) || !(t.flags & HPVCD_TU_INTRA);
+    if (in_plane) {  // reconstruct.rs:214-251: add and clip into the plane
+        void* pl = P.rec[c];
+        const int mx = (1 << bd) - 1;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            if (x0 + m >= pw) break;
+            const size_t idx = (size_t)y * pw + x0 + m;
+            store_sample(pl, P.bps, idx, clamp3i(load_sample(pl, P.bps, idx) + o[m], 0, mx));
+        }
+    } else {
+        int16_t* row = P.res[c] + (size_t)y * P.res_stride[c] + x0;
+        if (x0 + 8 <= pw && ((uintptr_t)row & 15) == 0) {
+            uint32_t w[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+                w[h] = (uint32_t)(uint16_t)sat16(o[2 * h]) | ((uint32_t)(uint16_t)sat16(o[2 * h + 1]) << 16);
+            *(uint4*)row = make_uint4(w[0], w[1], w[2], w[3]);
+        } else {
+#pragma unroll
+            for (int m = 0; m < 8; ++m)
+                if (x0 + m < pw) row[m] = (int16_t)sat16(o[m]);
+        }
+    }
+}
+
 template <int kIdct>
 __global__ void __launch_bounds__(kResWarps * 32)
 k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_prefix, uint32_t n_pics,
@@ -742,6 +841,7 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
         uint32_t pic = 0;
         uint4 r4 = make_uint4(0u, 0u, 0u, 0u);
         bool mine4 = false;  // a plain coded 4x4 TB: this lane transforms it on its own
+        bool mine8 = false;  // a plain coded 8x8 TB: a group of eight lanes transforms it
         if (gl < total) {
             uint32_t lo = 0, hi = n_pics;
             while (hi - lo > 1) {
@@ -753,8 +853,10 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
             r4 = *(const uint4*)(P.tus + (gl - rec_prefix[lo]));  // records are 16-byte aligned
             hpvcd_tu t;
             memcpy(&t, &r4, sizeof(t));
-            if (tb4_thread_ok(P, t)) {
+            if (tb_lanes_ok(P, t, 2)) {
                 mine4 = true;
+            } else if (tb_lanes_ok(P, t, 3)) {
+                mine8 = true;
             } else if ((t.flags & HPVCD_TU_CBF) && t.log2n >= 2 && t.log2n <= 5) {
                 const uint32_t esz = (P.flags & HPVCD_PIC_COEFF8) ? 1u : 2u;
                 const uint64_t n2 = 1ull << (2 * t.log2n);
@@ -773,10 +875,35 @@ k_residual(const DevPic* __restrict__ pics, const uint32_t* __restrict__ rec_pre
             tb4_thread(pics[pic], t);
         }
         const uint32_t done4 = __ballot_sync(kAll, mine4);
+        // ---- the plain coded 8x8 TBs: four per pass, eight lanes each
+        // (lane q of a group takes column q, then row q; the transpose goes
+        // through the warp's scratch) ----
+        const uint32_t done8 = __ballot_sync(kAll, mine8);
+        for (uint32_t mask8 = done8; mask8;) {
+            const int grp = lane >> 3, q = lane & 7;
+            uint32_t m = mask8;
+            for (int i = 0; i < grp; ++i) m &= m - 1u;
+            const int src = m ? __ffs(m) - 1 : 0;
+            const uint32_t pj = __shfl_sync(kAll, pic, src);
+            uint4 w4;
+            w4.x = __shfl_sync(kAll, r4.x, src);
+            w4.y = __shfl_sync(kAll, r4.y, src);
+            w4.z = __shfl_sync(kAll, r4.z, src);
+            w4.w = __shfl_sync(kAll, r4.w, src);
+            hpvcd_tu t;
+            memcpy(&t, &w4, sizeof(t));
+            int16_t* S = scr[warp][0] + grp * 72;
+            if (m) tb8_cols(pics[pj], t, q, S);
+            __syncwarp();
+            if (m) tb8_rows(pics[pj], t, q, S);
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 4; ++i) mask8 &= mask8 - 1u;
+        }
         // ---- the chunk's other records one by one ----
         const uint32_t nrec = min((uint32_t)kResChunk, total - g0);
         for (uint32_t j = 0; j < nrec; ++j) {
-            if ((done4 >> j) & 1u) continue;
+            if (((done4 | done8) >> j) & 1u) continue;
             const uint32_t pj = __shfl_sync(kAll, pic, j);
             uint4 w4;
             w4.x = __shfl_sync(kAll, r4.x, j);
