@@ -69,6 +69,8 @@ def parse_args():
     ap.add_argument("--batched-images", type=int, default=256,
                     help="default workload: images of the mixed-size batch block (0 = leave it out)")
     ap.add_argument("--rate", type=float, default=200.0, help="serving: Poisson arrivals per second")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="default workload: leave the serving-loop runs out of the mixed-size batch block")
     ap.add_argument("--sched", default="network",
                     help="default workload: 'network' (the selector's pick) or a fixed schedule "
                          "'idct,chroma_warps,recon_ctas_per_sm,wave' (hpvcd_sched)")
@@ -742,6 +744,12 @@ def batched_block(args, local) -> dict:
     filt = {"kernel": "k_filter_tile", "bytes": filt_bytes, "ms": round(filt_ms, 3), "gbs": round(filt_gbs, 1),
             "frac": round(filt_gbs / peak, 4)}
 
+    if args.no_serving:
+        torch.cuda.nvtx.range_pop()
+        del keep, c8keep, out_keep
+        return {"workload": "heic_serving_mixed", "images": len(imgs), "tiles": len(pics), "mpix": round(mpix, 2),
+                "device": dev, "batched_vs_plain": dev["speedup"],
+                "learned_vs_plain": dev.get("learned_speedup_vs_plain"), "recon_roofline": roof, "filters": filt}
     # the serving loop: saturation (all submitted at once) and Poisson arrivals
     torch.cuda.synchronize()
     torch.cuda.empty_cache()

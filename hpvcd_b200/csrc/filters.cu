@@ -13,6 +13,7 @@
 //
 // RGB (yuv.rs:187-393 Q13 matrix, lib.rs:1964-1978 rgb8 narrowing,
 // lib.rs:1610-1660 tile placement and cropping on the canvas).
+#include <mutex>
 #include <algorithm>
 #include <type_traits>
 
@@ -1186,7 +1187,29 @@ extern "C" cudaError_t hpvcd_launch_filter_tile(const hpvcd::DevPic* pics, int n
 // shared array as shared memory, like the wavefront kernel: the tile filter
 // of one concurrent group runs beside another group's wavefront, and an SM
 // changes its L1 / shared split only when it holds no CTA.
+// Once per device (a plan build calls it for every new batch layout).
+namespace {
+constexpr int kTileSetupDevices = 64;
+std::mutex g_tile_setup_mu;
+bool g_tile_setup_done[kTileSetupDevices];
+}  // namespace
+
+static cudaError_t filter_tile_attrs();
+
 extern "C" cudaError_t hpvcd_filter_tile_setup() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kTileSetupDevices) {
+        cudaGetLastError();
+        return filter_tile_attrs();
+    }
+    std::lock_guard<std::mutex> lock(g_tile_setup_mu);
+    if (g_tile_setup_done[dev]) return cudaSuccess;
+    const cudaError_t e = filter_tile_attrs();
+    g_tile_setup_done[dev] = e == cudaSuccess;
+    return e;
+}
+
+static cudaError_t filter_tile_attrs() {
     const int lim = (int)hpvcd::tile_smem_bytes(1);
     cudaError_t e = cudaFuncSetAttribute(hpvcd::k_filter_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
     if (e == cudaSuccess)

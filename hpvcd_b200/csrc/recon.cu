@@ -28,6 +28,7 @@
 //     needs it (waits bounded), so a CTU starts while its left and
 //     above-right neighbours are still being walked.  Finally the whole CTU
 //     is written out for the filters.
+#include <mutex>
 #include <climits>
 
 #include "common.cuh"
@@ -2259,15 +2260,48 @@ void recon_attrs(int lim) {
     cudaFuncSetAttribute(hpvcd::k_recon<kCW, kFeat, kDense>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxShared);
 }
-}  // namespace
 
-// CTAs per SM of the wavefront kernel with the layout of `cfmt` in build
-// `chroma_warps` (1 two warps, 2 three warps, 3 three warps register-capped),
-// after setting the attributes of every instantiation (recon_attrs).
-extern "C" int hpvcd_recon_occupancy(int cfmt, int chroma_warps) {
+// Occupancy of one build with the layout of `cfmt` (attributes already set).
+int recon_occupancy_of(int cfmt, int chroma_warps) {
     int blocks = 0;
     const int cw = chroma_warps == 1 ? 1 : 2;
     const size_t smem = hpvcd::ReconLayout(cfmt, hpvcd::recon_warps(cw)).total;
+    if (chroma_warps == 3)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<2, false, true>,
+                                                      32 * hpvcd::recon_warps(2), smem);
+    else if (cw == 2)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<2, false>, 32 * hpvcd::recon_warps(2),
+                                                      smem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<1, false>, 32 * hpvcd::recon_warps(1),
+                                                      smem);
+    return blocks;
+}
+
+// Attributes and occupancies are set up once per device: every plan build
+// asks for them, and a serving loop builds a plan for every new batch
+// layout (setting the attributes of every instantiation each time cost
+// milliseconds per plan).
+constexpr int kAttrDevices = 64;
+std::mutex g_attr_mu;
+bool g_attr_done[kAttrDevices];
+int g_attr_occ[kAttrDevices][3][3];
+}  // namespace
+
+// CTAs per SM of the wavefront kernel with the layout of `cfmt` in build
+// `chroma_warps` (1 two warps, 2 three warps, 3 three warps register-capped;
+// 0 counts as 2); the first call on a device sets the attributes of every
+// instantiation (recon_attrs) and of the residual kernel.
+extern "C" int hpvcd_recon_occupancy(int cfmt, int chroma_warps) {
+    const int build = chroma_warps >= 1 && chroma_warps <= 3 ? chroma_warps : 2;
+    const int cf = cfmt >= 0 && cfmt <= 2 ? cfmt : 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kAttrDevices) {
+        cudaGetLastError();
+        dev = -1;
+    }
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    if (dev >= 0 && g_attr_done[dev]) return g_attr_occ[dev][cf][build - 1];
     const int lim = (int)hpvcd::ReconLayout(hpvcd::kFmt444, hpvcd::recon_warps(2)).total;
     recon_attrs<1, false, false>(lim);
     recon_attrs<2, false, false>(lim);
@@ -2282,14 +2316,9 @@ extern "C" int hpvcd_recon_occupancy(int cfmt, int chroma_warps) {
                          (int)cudaSharedmemCarveoutMaxShared);
     cudaFuncSetAttribute(hpvcd::k_residual<hpvcd::kIdctTensor>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxShared);
-    if (chroma_warps == 3)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<2, false, true>,
-                                                      32 * hpvcd::recon_warps(2), smem);
-    else if (cw == 2)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<2, false>, 32 * hpvcd::recon_warps(2),
-                                                      smem);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, hpvcd::k_recon<1, false>, 32 * hpvcd::recon_warps(1),
-                                                      smem);
-    return blocks;
+    if (dev < 0) return recon_occupancy_of(cf, build);
+    for (int f = 0; f < 3; ++f)
+        for (int b = 1; b <= 3; ++b) g_attr_occ[dev][f][b - 1] = recon_occupancy_of(f, b);
+    g_attr_done[dev] = true;
+    return g_attr_occ[dev][cf][build - 1];
 }

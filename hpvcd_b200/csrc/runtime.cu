@@ -1758,22 +1758,24 @@ HPVCD_API hpvcd_status hpvcd_gpu_submit(hpvcd_gpu* g, const hpvcd_picture* pics,
     // Tickets already in flight share the SMs with this one: the wavefront
     // kernel's persistent grid keeps to its share of the CTA slots (its CTAs
     // wait for their neighbour CTUs in place, holding slots the other
-    // tickets' kernels need), and it waits for whole neighbour CTUs: with the
-    // SMs busy, starting a CTU early only trades its slot for mid-walk polls.
-    // At three tickets in flight on the 4032x3024 grid the share is worth
-    // about 15 % of throughput; a ticket alone keeps the full grid and the
-    // quadrant-level wavefront, which shortens its critical path.
+    // tickets' kernels need).  At three tickets in flight on the 4032x3024
+    // grid the share is worth about 15 % of throughput; a ticket alone keeps
+    // the full grid.  Sharing, the default build is the register-capped one:
+    // eight CTAs per SM split between the tickets instead of five (at four
+    // tickets in flight one CTA per SM each with the plain build, a quarter
+    // of that per group of the grid, fewer than the group's ready CTUs).
+    // With two CTAs per SM per ticket the quadrant-level wavefront also pays
+    // while sharing (four grids in flight: 1.19 against 1.29 ms per image
+    // with whole-CTU waits, same box).
     {
         if (others > 0) {
             hpvcd_sched s2 = slot->plan->sched;
             const hpvcd_plan* pl = slot->plan;
-            const int occ = std::max(1, pl->waves.empty() ? pl->occ_of(0, 2)
-                                                           : pl->occ_of(pl->waves[0].cfmt,
-                                                                        pl->build_of(pl->waves[0], 1)));
+            if (s2.chroma_warps == 0) s2.chroma_warps = 3;
+            const int occ = std::max(1, pl->occ_of(pl->waves.empty() ? 0 : pl->waves[0].cfmt, (int)s2.chroma_warps));
             const int share = std::max(1, occ / (others + 1));
             const int cur = s2.recon_ctas_per_sm ? (int)s2.recon_ctas_per_sm : occ;
             s2.recon_ctas_per_sm = (uint32_t)std::min(cur, share);
-            s2.wave = 1;
             st = hpvcd_plan_set_sched(slot->plan, &s2);
             if (st != HPVCD_OK) return st;
         }
