@@ -2281,7 +2281,9 @@ int recon_occupancy_of(int cfmt, int chroma_warps) {
 // Attributes and occupancies are set up once per device: every plan build
 // asks for them, and a serving loop builds a plan for every new batch
 // layout (setting the attributes of every instantiation each time cost
-// milliseconds per plan).
+// milliseconds per plan).  Like the no-allocation entry point's per-device
+// set-up, this assumes the device's primary context lives until the process
+// exits (no cudaDeviceReset while the library is in use).
 constexpr int kAttrDevices = 64;
 std::mutex g_attr_mu;
 bool g_attr_done[kAttrDevices];
